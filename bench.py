@@ -1,0 +1,316 @@
+#!/usr/bin/env python
+"""Benchmark of the interpolation-grid build (path a) on the configuration-2 workload.
+
+Workload (one "step"): the three tricubic grids of the charged synthetic framework — C_co2 Lennard-Jones, O_co2
+Lennard-Jones and the unit-charge real-space Ewald grid — 133 x 133 x 89 = 1,574,321 points each (0.15 Angstrom
+spacing over the 20.0 x 19.9 x 13.4 Angstrom cell, 96 T + 192 O atoms, rc = 12 Angstrom, alpha = 0.265), computed in
+FP32 with compensated accumulation (FP32C). Metric: grid points per second over the whole job.
+
+* value: device-resident output buffers, CUDA events on the launching stream, an L2 flush (a 256 MiB write) between
+  timed steps (the per-step output of 302 MB also exceeds the 126 MB L2), max over ranks.
+* e2e: the same steps through the C-ABI with host buffers: the framework upload and the 302 MB device-to-host copy of
+  the grids are inside the timed region.
+* roofline: the dominant kernel's achieved FP32 throughput (in-cutoff pairs x FLOPs per pair / launch time) against
+  the FP32 FMA throughput measured by rg_probe_fma_peak in the same run.
+* cpu_baseline: the FP64 CPU oracle (the reference's grid loop restated) on a sample of points, all host cores.
+
+--impl reference times the CPU oracle alone on the same workload (rank 0 only).
+Multi-GPU: the grid build is replicated (independent frameworks per rank, no collective), so scaling is weak.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid pts/s"
+UNIT = "grid points/s"
+# FLOPs per in-cutoff pair of the restated formulas (add/mul = 1, FMA = 2, reciprocal/sqrt/erfc/exp = 1 each).
+FLOPS_PER_PAIR = {"lj": 55, "ewald": 65}
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the cpu_baseline sample")
+    return ap.parse_args()
+
+
+def workload():
+    from raspa3_b200.synthetic import config1_grid_dims, synthetic_forcefield, synthetic_framework
+
+    ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=8)
+    cell, atoms = synthetic_framework(ff, seed=42)
+    dims = config1_grid_dims(cell)
+    grids = [("C_co2-LJ", 0, ff.index("C_co2")), ("O_co2-LJ", 0, ff.index("O_co2")), ("Ewald-real", 1, 0)]
+    return ff, cell, atoms, dims, grids
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_oracle_rate(ff, cell, atoms, dims, grids, target_seconds, threads=0, seed=5):
+    """FP64 oracle on a random sample of grid points of every grid; returns (points/s, points, seconds, threads)."""
+    import oracle
+
+    nx, ny, nz = dims
+    total = nx * ny * nz
+    rng = np.random.default_rng(seed)
+    threads = threads or os.cpu_count() or 1
+
+    def run(n):
+        pts = np.sort(rng.choice(total, size=min(n, total), replace=False)).astype(np.int64)
+        t0 = time.perf_counter()
+        for _, gt, probe in grids:
+            oracle.make_grid(gt, ff, cell, atoms, probe, 12.0, dims, points=pts, threads=threads)
+        return len(pts) * len(grids), time.perf_counter() - t0
+
+    n0 = 64 * threads
+    pts0, t0 = run(n0)
+    n1 = int(n0 * max(1.0, target_seconds / max(t0, 1e-3)))
+    pts1, t1 = run(n1)
+    return pts1 / t1, pts1, t1, threads
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+
+    oracle.lib()
+    ff, cell, atoms, dims, grids = workload()
+    threads = os.cpu_count() or 1
+    # size one step so that W + K steps take a few minutes at most
+    per_step = max(2.0, min(8.0, 150.0 / max(1, args.steps + args.warmup)))
+    rate0, _, _, _ = cpu_oracle_rate(ff, cell, atoms, dims, grids, 1.0, threads)
+    n_pts = max(256, int(rate0 * per_step / len(grids)))
+    rng = np.random.default_rng(99)
+    total = dims[0] * dims[1] * dims[2]
+    done, secs = 0, 0.0
+    for s in range(args.warmup + args.steps):
+        pts = np.sort(rng.choice(total, size=min(n_pts, total), replace=False)).astype(np.int64)
+        t0 = time.perf_counter()
+        for _, gt, probe in grids:
+            oracle.make_grid(gt, ff, cell, atoms, probe, 12.0, dims, points=pts, threads=threads)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            done += len(pts) * len(grids)
+            secs += dt
+    value = done / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "config2 grid build: C_co2-LJ + O_co2-LJ + unit-charge Ewald-real tricubic grids, "
+                               "133x133x89 points each", "grid_points_per_step_full": 3 * total,
+                   "parallelism": "cpu"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{n_pts} random grid points x 3 grids per step (FP64 oracle restating "
+                                   f"makeFrameworkInterpolationGrid, OpenMP over points)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    from raspa3_b200 import native
+
+    ff, cell, atoms, dims, grids = workload()
+    npts = dims[0] * dims[1] * dims[2]
+    ctx = native.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    outs = [torch.empty(8 * npts, dtype=torch.float64, device="cuda") for _ in grids]
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def build(gi, out_device=None, out_host=None, count=False):
+        _, gt, probe = grids[gi]
+        return ctx.grid_build(gt, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP32C,
+                              out_device=out_device, host=out_host is not None, out_host=out_host,
+                              count_pairs=count)
+
+    # work per grid (pair counts) outside the timed region
+    stats = [build(g, out_device=outs[g].data_ptr(), count=True)[1] for g in range(len(grids))]
+    peak_fp32 = ctx.probe_fma_peak(native.PRECISION_FP32C)
+
+    for _ in range(args.warmup):
+        for g in range(len(grids)):
+            build(g, out_device=outs[g].data_ptr())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(grids) + 1)] for _ in range(args.steps)]
+    for s in range(args.steps):
+        flush.zero_()
+        ev[s][0].record(stream)
+        for g in range(len(grids)):
+            build(g, out_device=outs[g].data_ptr())
+            ev[s][g + 1].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    step_ms = [ev[s][0].elapsed_time(ev[s][-1]) for s in range(args.steps)]
+    kern_ms = [[ev[s][g].elapsed_time(ev[s][g + 1]) for s in range(args.steps)] for g in range(len(grids))]
+    total_s = sum(step_ms) / 1e3
+    if world > 1:
+        t = torch.tensor([total_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_s = float(t.item())
+    value = world * len(grids) * npts * args.steps / total_s
+
+    # e2e through the C-ABI with pinned host output buffers (framework upload + grid download inside the region)
+    e2e_steps = max(1, min(args.steps, 5))
+    host_bufs = [torch.empty(8 * npts, dtype=torch.float64, pin_memory=True) for _ in grids]
+    host_np = [b.numpy() for b in host_bufs]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    h2d = d2h = 0
+    t0 = time.perf_counter()
+    for s in range(e2e_steps):
+        for g in range(len(grids)):
+            _, st = build(g, out_host=host_np[g], count=(s == 0))
+            if s == 0:
+                h2d += st["h2d_bytes"]
+                d2h += st["d2h_bytes"]
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * len(grids) * npts * e2e_steps / e2e_s
+
+    # roofline of the dominant kernel
+    mean_ms = [statistics.mean(k) for k in kern_ms]
+    dom = int(np.argmax(mean_ms))
+    kind = "ewald" if grids[dom][1] == 1 else "lj"
+    achieved = stats[dom]["pair_count"] * FLOPS_PER_PAIR[kind] / (mean_ms[dom] * 1e-3) / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "grid_build_config2_traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(grids[dom][0])
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "config2 grid build: C_co2-LJ + O_co2-LJ + unit-charge Ewald-real tricubic grids, "
+                               "133x133x89 points each, FP32C", "grid_points_per_step": len(grids) * npts,
+                   "framework_atoms": int(len(atoms)), "cutoff": 12.0, "precision": "FP32 pairs, compensated FP32 "
+                   "accumulation, FP64 epilogue", "l2": "256 MiB flush between timed steps; 302 MB output per step",
+                   "parallelism": f"replicas x{world}"},
+        "kernels": {grids[g][0]: {"ms": mean_ms[g], "pairs": stats[g]["pair_count"], "images": stats[g]["n_images"],
+                                  "tflops": stats[g]["pair_count"] * FLOPS_PER_PAIR["ewald" if grids[g][1] == 1
+                                                                                   else "lj"] / (mean_ms[g] * 1e-3) / 1e12}
+                    for g in range(len(grids))},
+        "roofline": {"kernel": f"gridKernel<float> ({grids[dom][0]})", "bound": "fp32", "achieved": achieved,
+                     "peak": peak_fp32, "unit": "TFLOP/s", "frac": achieved / peak_fp32, "traffic": traffic,
+                     "peak_source": "rg_probe_fma_peak: FP32 FMA chains on all SMs, measured in this run",
+                     "flops_per_pair": FLOPS_PER_PAIR[kind]},
+        "clocks": clocks,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps, "path": "rg_grid_build with pinned host output"},
+        "gpu_launches": len(grids) * args.steps,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, pts, secs, threads = cpu_oracle_rate(ff, cell, atoms, dims, grids, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{pts // len(grids)} random grid points x {len(grids)} grids in {secs:.1f} s "
+                                          f"(FP64 oracle of makeFrameworkInterpolationGrid, OpenMP over points)"}
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

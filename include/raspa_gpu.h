@@ -1,0 +1,137 @@
+/*
+ * raspa_gpu.h — C-ABI of the B200 (sm_100a) implementation of RASPA3's data-parallel energy paths.
+ *
+ * Every entry point takes plain pointers and sizes and returns an rg_status. Host pointers stay owned by the
+ * caller; device buffers passed in (out_device, ...) stay owned by the caller; buffers the library allocates
+ * belong to the rg_ctx that allocated them and are freed by rg_ctx_destroy. One rg_ctx per host thread (or per
+ * System): the library keeps no mutable global state besides the CUDA device context, so the calls are
+ * re-entrant per context, matching the reference's one-System-per-thread drivers.
+ *
+ * A molecule overlap is a result (a flag in the output), never an error, as in the reference where it is a
+ * std::nullopt. Units are the reference's internal units (energy 10 J/mol, length Angstrom, charge e).
+ */
+#ifndef RASPA_GPU_H
+#define RASPA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t rg_status;
+enum
+{
+  RG_OK = 0,
+  RG_ERR_INVALID_ARGUMENT = 1,
+  RG_ERR_CUDA = 2,
+  RG_ERR_TIMEOUT = 3,
+  RG_ERR_UNSUPPORTED = 4,
+  RG_ERR_OUT_OF_MEMORY = 5,
+  RG_ERR_NO_DEVICE = 6
+};
+
+/* Byte-for-byte the reference Atom (src/raspakit/atom.ixx:28-39, 64 bytes): a std::span<const Atom> can be passed
+ * as (const rg_atom*, size) without repacking. */
+typedef struct rg_atom
+{
+  double x, y, z, w; /* double3 position (w: the union's padding lane, unused) */
+  double charge;
+  double scaling_vdw;
+  double scaling_coulomb;
+  uint32_t molecule_id;
+  uint16_t type;
+  uint8_t component_id;
+  uint8_t group_fractional; /* low nibble: groupId (1-based dU/dlambda group, 0 = none); high nibble: isFractional */
+} rg_atom;
+
+/* SimulationBox (src/raspakit/simulationbox.ixx): cell[3*c + r] is component r of lattice vector c (the reference
+ * double3x3 is column-major). triclinic != 0 selects the general minimum image. */
+typedef struct rg_box
+{
+  double cell[9];
+  int32_t triclinic;
+} rg_box;
+
+/* The ForceField fields these paths read (src/raspakit/forcefield/forcefield.ixx:88-174): the mixed, shifted
+ * Lennard-Jones pair table (epsilon in internal units) and the cutoff / Ewald / overlap parameters. */
+typedef struct rg_forcefield
+{
+  int32_t n_types;
+  const double* epsilon; /* [n_types*n_types] */
+  const double* sigma;   /* [n_types*n_types] */
+  const double* shift;   /* [n_types*n_types] */
+  const int32_t* lj;     /* [n_types*n_types] 1 = Lennard-Jones, 0 = None */
+  double cutoff_framework_vdw;
+  double cutoff_molecule_vdw;
+  double cutoff_coulomb;
+  double ewald_alpha;
+  int32_t kmax_x, kmax_y, kmax_z;
+  uint64_t recip_int_cutoff_sq; /* integer k-sphere bound; UINT64_MAX = full half-box */
+  double recip_cutoff_sq;
+  double overlap_criteria;
+  int32_t use_charge;
+  int32_t omit_inter;
+} rg_forcefield;
+
+typedef struct rg_ctx rg_ctx;
+
+/* ---- context ---- */
+rg_status rg_ctx_create(int device, rg_ctx** out);
+rg_status rg_ctx_destroy(rg_ctx* ctx);
+/* Use the caller's CUDA stream (a cudaStream_t; NULL restores the context's own stream). */
+rg_status rg_ctx_set_stream(rg_ctx* ctx, void* stream);
+void* rg_ctx_stream(rg_ctx* ctx);
+rg_status rg_ctx_synchronize(rg_ctx* ctx);
+/* Message of the last failing call on this context ("" if none). */
+const char* rg_ctx_last_error(rg_ctx* ctx);
+const char* rg_version(void);
+
+/* ---- (a) interpolation-grid build ---- */
+enum
+{
+  RG_GRID_LENNARD_JONES = 0,
+  RG_GRID_EWALD_REAL = 1, /* unit-charge real-space Ewald grid */
+  RG_GRID_LENNARD_JONES_REPULSION = 2,
+  RG_GRID_LENNARD_JONES_ATTRACTION = 3
+};
+enum
+{
+  RG_PRECISION_FP64 = 0,  /* FP64 pair terms and accumulation */
+  RG_PRECISION_FP32C = 1  /* FP32 pair terms, compensated FP32 accumulation, FP64 epilogue */
+};
+
+/* Replaces InterpolationEnergyGrid::makeFrameworkInterpolationGrid, tricubic scheme
+ * (src/raspakit/interpolation_energy_grid.cpp:3800-3978), with the per-point sums of
+ * Interactions::calculateTricubicFractionalAtPosition (src/raspakit/interactions/framework_molecule_grid.cpp:168-282).
+ * Called from System::createFrameworkInterpolationGrids (src/raspakit/system_interpolation_grids.cpp:211, 236).
+ *
+ * unit_atoms: the framework's unit-cell atoms (Cartesian, host memory); unit_cell: the framework unit cell;
+ * cutoff: the cutoff that sizes the reference's supercell (cutOffFrameworkVDW for VDW grids, cutOffCoulomb for
+ * the Ewald grid); the pair cutoff is ff->cutoff_framework_vdw, as in the reference. nx, ny, nz include the
+ * duplicate periodic end-point. The result, 8 doubles per point in the reference layout
+ * data[l + 8*(i + nx*(j + ny*k))], goes to out_device (a device buffer of 8*nx*ny*nz doubles) and/or out_host.
+ * If stats is non-NULL it receives the work and traffic of the call; pair counting adds one integer add per pair. */
+typedef struct rg_grid_stats
+{
+  int64_t pair_count;  /* in-cutoff pair evaluations (rr < rc^2, nonzero parameter): the algorithmic unit */
+  int64_t n_images;    /* periodic images of the unit-cell atoms staged on the device */
+  int64_t h2d_bytes;   /* host-to-device bytes copied by the call */
+  int64_t d2h_bytes;   /* device-to-host bytes copied by the call */
+} rg_grid_stats;
+
+rg_status rg_grid_build(rg_ctx* ctx, int grid_type, const rg_forcefield* ff, const rg_box* unit_cell,
+                        const rg_atom* unit_atoms, int n_unit_atoms, int probe_type, double cutoff, int nx, int ny,
+                        int nz, int precision, double* out_device, double* out_host, rg_grid_stats* stats);
+
+/* ---- measurement ---- */
+/* FP32 (precision = RG_PRECISION_FP32C) or FP64 FMA throughput of this device in TFLOP/s, from independent FMA chains
+ * on every SM: the SIMT-pipe denominator for the pair kernels' rooflines. No counterpart in the reference. */
+rg_status rg_probe_fma_peak(rg_ctx* ctx, int precision, double* tflops, double* seconds);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,287 @@
+"""ctypes wrapper of the FP64 CPU oracle (oracle/_build/liboracle.so) — TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu-baseline / reference arms import this module. It is the
+checker the CUDA path is compared against; the product never imports it.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build(quiet: bool = True) -> str:
+    subprocess.run(["make", "-C", _HERE], check=True, capture_output=quiet)
+    return _LIB_PATH
+
+
+class OAtomPtr(ctypes.c_void_p):
+    pass
+
+
+class OBox(ctypes.Structure):
+    _fields_ = [("cell", ctypes.c_double * 9), ("triclinic", ctypes.c_int32)]
+
+
+class OFF(ctypes.Structure):
+    _fields_ = [
+        ("n_types", ctypes.c_int32),
+        ("epsilon", ctypes.POINTER(ctypes.c_double)),
+        ("sigma", ctypes.POINTER(ctypes.c_double)),
+        ("shift", ctypes.POINTER(ctypes.c_double)),
+        ("lj", ctypes.POINTER(ctypes.c_int32)),
+        ("cutoff_framework_vdw", ctypes.c_double),
+        ("cutoff_molecule_vdw", ctypes.c_double),
+        ("cutoff_coulomb", ctypes.c_double),
+        ("ewald_alpha", ctypes.c_double),
+        ("kmax_x", ctypes.c_int32), ("kmax_y", ctypes.c_int32), ("kmax_z", ctypes.c_int32),
+        ("recip_int_cutoff_sq", ctypes.c_uint64),
+        ("recip_cutoff_sq", ctypes.c_double),
+        ("overlap_criteria", ctypes.c_double),
+        ("use_charge", ctypes.c_int32),
+        ("omit_inter", ctypes.c_int32),
+    ]
+
+
+ENERGY_FIELDS = ["framework_molecule_vdw", "framework_molecule_charge", "molecule_molecule_vdw",
+                 "molecule_molecule_charge", "ewald_fourier", "ewald_self", "ewald_exclusion"]
+
+
+class OEnergy(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_double) for f in ENERGY_FIELDS] + [
+        ("dudlambda_vdw", ctypes.c_double * 4), ("dudlambda_charge", ctypes.c_double * 4),
+        ("dudlambda_ewald", ctypes.c_double * 4)]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f in ENERGY_FIELDS}
+        d["dudlambda_vdw"] = list(self.dudlambda_vdw)
+        d["dudlambda_charge"] = list(self.dudlambda_charge)
+        d["dudlambda_ewald"] = list(self.dudlambda_ewald)
+        return d
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.POINTER
+        d, i32, i64, vp = ctypes.c_double, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p
+        L.oracle_energy_to_kelvin.restype = d
+        L.oracle_kelvin_to_energy.restype = d
+        L.oracle_coulomb_factor.restype = d
+        L.oracle_make_tricubic_grid.argtypes = [i32, P(OFF), P(OBox), vp, i32, i32, d, i32, i32, i32, vp, i64, i32, vp]
+        L.oracle_make_tricubic_grid.restype = i32
+        L.oracle_grid_pair_count.argtypes = [i32, P(OFF), P(OBox), vp, i32, i32, d, i32, i32, i32, vp, i64, i32]
+        L.oracle_grid_pair_count.restype = i64
+        L.oracle_tricubic_fractional_at_position.argtypes = [i32, P(OFF), P(OBox), vp, i32, P(OBox), vp, i32, vp]
+        L.oracle_tricubic_matrix.argtypes = [vp]
+        L.oracle_grid_interpolate.argtypes = [vp, i32, i32, i32, P(OBox), vp]
+        L.oracle_grid_interpolate.restype = d
+        L.oracle_pair_vdw.argtypes = [P(OFF), d, d, d, i32, i32, vp]
+        L.oracle_pair_coulomb.argtypes = [P(OFF), d, d, d, d, d, vp]
+        L.oracle_cbmc_framework_molecule.argtypes = [P(OFF), P(OBox), vp, i32, i32, i32, P(OBox), vp, i32, d, d, vp,
+                                                     i32, i32, P(OEnergy)]
+        L.oracle_cbmc_framework_molecule.restype = i32
+        L.oracle_cbmc_intermolecular.argtypes = [P(OFF), P(OBox), vp, i32, d, d, vp, i32, i32, i64, P(OEnergy)]
+        L.oracle_cbmc_intermolecular.restype = i32
+        L.oracle_ewald_kvectors.argtypes = [P(OFF), P(OBox), vp, vp, vp]
+        L.oracle_ewald_kvectors.restype = i64
+        L.oracle_ewald_rigid.argtypes = [P(OFF), P(OBox), vp, i32, vp]
+        L.oracle_ewald_fourier_energy.argtypes = [P(OFF), P(OBox), vp, vp, i32, vp, i32, d, vp, P(OEnergy)]
+        L.oracle_ewald_delta.argtypes = [P(OFF), P(OBox), vp, vp, i32, vp, i32, d, vp, vp, P(OEnergy)]
+        L.oracle_ewald_single_ion.argtypes = [P(OFF), P(OBox), vp, d]
+        L.oracle_ewald_single_ion.restype = d
+        L.oracle_select_trial.argtypes = [vp, i32, d]
+        L.oracle_select_trial.restype = i32
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def off(ff) -> OFF:
+    """OFF struct from a raspa3_b200.forcefield.ForceField (keeps the arrays alive on the struct)."""
+    eps = np.ascontiguousarray(ff.epsilon, dtype=np.float64)
+    sig = np.ascontiguousarray(ff.sigma, dtype=np.float64)
+    sh = np.ascontiguousarray(ff.shift, dtype=np.float64)
+    lj = np.ascontiguousarray(ff.lj, dtype=np.int32)
+    P = ctypes.POINTER
+    s = OFF(ff.n_types, eps.ctypes.data_as(P(ctypes.c_double)), sig.ctypes.data_as(P(ctypes.c_double)),
+            sh.ctypes.data_as(P(ctypes.c_double)), lj.ctypes.data_as(P(ctypes.c_int32)),
+            ff.cutoff_framework_vdw, ff.cutoff_molecule_vdw, ff.cutoff_coulomb, ff.ewald_alpha,
+            int(ff.kmax[0]), int(ff.kmax[1]), int(ff.kmax[2]), int(ff.recip_int_cutoff_sq), ff.recip_cutoff_sq,
+            ff.overlap_criteria, 1 if ff.use_charge else 0, 1 if ff.omit_inter else 0)
+    s._keep = (eps, sig, sh, lj)
+    return s
+
+
+def obox(cell, triclinic=None) -> OBox:
+    cell = np.asarray(cell, dtype=np.float64).reshape(3, 3)
+    if triclinic is None:
+        triclinic = bool(np.any(cell - np.diag(np.diag(cell)) != 0.0))
+    b = OBox()
+    for i in range(9):
+        b.cell[i] = float(cell.reshape(-1)[i])
+    b.triclinic = 1 if triclinic else 0
+    return b
+
+
+def energy_to_kelvin() -> float:
+    return lib().oracle_energy_to_kelvin()
+
+
+def make_grid(grid_type, ff, cell, atoms, probe_type, cutoff, dims, points=None, threads=0):
+    """Full tricubic grid (flat, reference layout) or the 8 values at the listed flat point indices."""
+    nx, ny, nz = dims
+    o, b = off(ff), obox(cell)
+    atoms = np.ascontiguousarray(atoms)
+    if points is None:
+        out = np.empty(8 * nx * ny * nz)
+        lib().oracle_make_tricubic_grid(grid_type, o, b, _ptr(atoms), len(atoms), probe_type, cutoff, nx, ny, nz,
+                                        None, 0, threads, _ptr(out))
+        return out
+    pts = np.ascontiguousarray(points, dtype=np.int64)
+    out = np.empty((len(pts), 8))
+    lib().oracle_make_tricubic_grid(grid_type, o, b, _ptr(atoms), len(atoms), probe_type, cutoff, nx, ny, nz,
+                                    _ptr(pts), len(pts), threads, _ptr(out))
+    return out
+
+
+def grid_pair_count(grid_type, ff, cell, atoms, probe_type, cutoff, dims, points=None, threads=0) -> int:
+    nx, ny, nz = dims
+    atoms = np.ascontiguousarray(atoms)
+    if points is None:
+        return lib().oracle_grid_pair_count(grid_type, off(ff), obox(cell), _ptr(atoms), len(atoms), probe_type,
+                                            cutoff, nx, ny, nz, None, 0, threads)
+    pts = np.ascontiguousarray(points, dtype=np.int64)
+    return lib().oracle_grid_pair_count(grid_type, off(ff), obox(cell), _ptr(atoms), len(atoms), probe_type, cutoff,
+                                        nx, ny, nz, _ptr(pts), len(pts), threads)
+
+
+def tricubic_fractional(grid_type, ff, super_cell, pos, type_a, unit_cell, super_atoms):
+    out = np.empty(8)
+    p = np.ascontiguousarray(pos, dtype=np.float64)
+    sa = np.ascontiguousarray(super_atoms)
+    lib().oracle_tricubic_fractional_at_position(grid_type, off(ff), obox(super_cell), _ptr(p), type_a,
+                                                 obox(unit_cell), _ptr(sa), len(sa), _ptr(out))
+    return out
+
+
+def tricubic_matrix() -> np.ndarray:
+    m = np.empty(64 * 64)
+    lib().oracle_tricubic_matrix(_ptr(m))
+    return m.reshape(64, 64)
+
+
+def interpolate(grid, dims, cell, pos) -> float:
+    g = np.ascontiguousarray(grid, dtype=np.float64)
+    p = np.ascontiguousarray(pos, dtype=np.float64)
+    return lib().oracle_grid_interpolate(_ptr(g), dims[0], dims[1], dims[2], obox(cell), _ptr(p))
+
+
+def cbmc_framework_molecule(ff, cell, fw_atoms, atoms, cutoff_vdw, cutoff_coulomb, grids=None, grid_dims=None,
+                            grid_cell=None, skip=-1):
+    """Returns (ok, energy dict). grids: list of length n_types+1 of flat grids or None."""
+    e = OEnergy()
+    fw = np.ascontiguousarray(fw_atoms)
+    at = np.ascontiguousarray(atoms)
+    gptr = None
+    keep = None
+    gnx = gny = gnz = 0
+    gbox = None
+    if grids is not None:
+        arr = (ctypes.c_void_p * len(grids))()
+        keep = [None if g is None else np.ascontiguousarray(g, dtype=np.float64) for g in grids]
+        for i, g in enumerate(keep):
+            arr[i] = None if g is None else g.ctypes.data
+        gptr = ctypes.cast(arr, ctypes.c_void_p)
+        gnx, gny, gnz = grid_dims
+        gbox = obox(grid_cell if grid_cell is not None else cell)
+    ok = lib().oracle_cbmc_framework_molecule(off(ff), obox(cell), gptr, gnx, gny, gnz, gbox, _ptr(fw), len(fw),
+                                              cutoff_vdw, cutoff_coulomb, _ptr(at), len(at), skip, ctypes.byref(e))
+    del keep
+    return bool(ok), e.as_dict()
+
+
+def cbmc_intermolecular(ff, cell, molecule_atoms, atoms, cutoff_vdw, cutoff_coulomb, skip=-1, skip_background=-1):
+    e = OEnergy()
+    ma = np.ascontiguousarray(molecule_atoms)
+    at = np.ascontiguousarray(atoms)
+    ok = lib().oracle_cbmc_intermolecular(off(ff), obox(cell), _ptr(ma), len(ma), cutoff_vdw, cutoff_coulomb,
+                                          _ptr(at), len(at), skip, skip_background, ctypes.byref(e))
+    return bool(ok), e.as_dict()
+
+
+def pair_vdw(ff, sa, sb, rr, ta, tb):
+    out = np.empty(2)
+    lib().oracle_pair_vdw(off(ff), sa, sb, rr, ta, tb, _ptr(out))
+    return out
+
+
+def pair_coulomb(ff, sa, sb, r, qa, qb):
+    out = np.empty(2)
+    lib().oracle_pair_coulomb(off(ff), sa, sb, r, qa, qb, _ptr(out))
+    return out
+
+
+def ewald_kvectors(ff, cell):
+    o, b = off(ff), obox(cell)
+    n = lib().oracle_ewald_kvectors(o, b, None, None, None)
+    kv = np.empty((n, 3), dtype=np.int32)
+    temp = np.empty(n)
+    s = ctypes.c_double()
+    lib().oracle_ewald_kvectors(o, b, _ptr(kv), _ptr(temp), ctypes.c_void_p(ctypes.addressof(s)))
+    return kv, temp, s.value
+
+
+def ewald_rigid(ff, cell, fw_atoms):
+    n = ewald_kvectors(ff, cell)[0].shape[0]
+    out = np.zeros(2 * n)
+    fw = np.ascontiguousarray(fw_atoms)
+    lib().oracle_ewald_rigid(off(ff), obox(cell), _ptr(fw), len(fw), _ptr(out))
+    return out
+
+
+def ewald_fourier_energy(ff, cell, atoms, molecule_sizes, s_rigid=None, net_charge_framework=0.0):
+    n = ewald_kvectors(ff, cell)[0].shape[0]
+    stored = np.zeros(10 * n)
+    at = np.ascontiguousarray(atoms)
+    ms = np.ascontiguousarray(molecule_sizes, dtype=np.int32)
+    e = OEnergy()
+    sr = None if s_rigid is None else np.ascontiguousarray(s_rigid, dtype=np.float64)
+    lib().oracle_ewald_fourier_energy(off(ff), obox(cell), _ptr(sr), _ptr(at), len(at), _ptr(ms), len(ms),
+                                      net_charge_framework, _ptr(stored), ctypes.byref(e))
+    return e.as_dict(), stored
+
+
+def ewald_delta(ff, cell, stored, new_atoms, old_atoms, net_charge=0.0, net_charge_derivative_ext=None):
+    trial = np.zeros_like(stored)
+    na = np.ascontiguousarray(new_atoms)
+    oa = np.ascontiguousarray(old_atoms)
+    e = OEnergy()
+    nd = None if net_charge_derivative_ext is None else np.ascontiguousarray(net_charge_derivative_ext, np.float64)
+    st = np.ascontiguousarray(stored, dtype=np.float64)
+    lib().oracle_ewald_delta(off(ff), obox(cell), _ptr(st), _ptr(na), len(na), _ptr(oa), len(oa), net_charge,
+                             _ptr(nd), _ptr(trial), ctypes.byref(e))
+    return e.as_dict(), trial
+
+
+def ewald_single_ion(ff, cell, pos, charge) -> float:
+    p = np.ascontiguousarray(pos, dtype=np.float64)
+    return lib().oracle_ewald_single_ion(off(ff), obox(cell), _ptr(p), charge)
+
+
+def select_trial(log_boltzmann, uniform) -> int:
+    lb = np.ascontiguousarray(log_boltzmann, dtype=np.float64)
+    return lib().oracle_select_trial(_ptr(lb), len(lb), uniform)

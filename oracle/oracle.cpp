@@ -1,0 +1,1166 @@
+// FP64 CPU oracle for the RASPA3 energy paths — TEST INFRASTRUCTURE ONLY (see oracle.h).
+//
+// Each function restates the cited reference function in double precision, keeping its loop structure,
+// its edge semantics (rr = max(0.1, rr), overlap clamps, duplicate periodic end-points, fractional derivative
+// scaling, supercell minimum image) and its expression order where that order is visible in the source.
+// Citations are file:line within the RASPA3 tree (src/raspakit/...).
+
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace
+{
+constexpr double kPi = 3.141592653589793238462643383279502884;
+constexpr double kInvSqrtPi = 0.564189583547756286948079451560772586;
+
+// ---- units.cpp:14-98 (base constants from foundationkit/units.ixx:29-55) ----
+constexpr double kAngstrom = 1e-10;
+constexpr double kPicoSecond = 1e-12;
+constexpr double kAtomicMassUnit = 1.6605402e-27;
+constexpr double kElectronicChargeUnit = 1.60217733e-19;
+constexpr double kMolarGasConstant = 8.314464919;
+constexpr double kAvogadroConstant = 6.0221419947e23;
+constexpr double kDielectricConstantVacuum = 8.8541878176e-12;
+
+double energyConversionFactor()
+{
+  return kAtomicMassUnit * kAngstrom * kAngstrom / (kPicoSecond * kPicoSecond);
+}
+double coulombFactor()
+{
+  return kElectronicChargeUnit * kElectronicChargeUnit /
+         (4.0 * kPi * kDielectricConstantVacuum * kAngstrom * energyConversionFactor());
+}
+
+// ---- boxes: SimulationBox (simulationbox.ixx:131-161, simulationbox.cpp:120-156) ----
+struct Box
+{
+  double c[3][3];   // c[col][row]; column col is lattice vector col
+  double ic[3][3];  // inverse, same convention
+  bool triclinic;
+  double volume;
+};
+
+void invert(const double m[3][3], double inv[3][3], double* det_out)
+{
+  // double3x3::inverse (mathkit/double3x3.cpp:102-118); mRC = row R, column C = m[C-1][R-1].
+  double m11 = m[0][0], m12 = m[1][0], m13 = m[2][0];
+  double m21 = m[0][1], m22 = m[1][1], m23 = m[2][1];
+  double m31 = m[0][2], m32 = m[1][2], m33 = m[2][2];
+  double det = m11 * (m22 * m33 - m23 * m32) - m12 * (m21 * m33 - m23 * m31) + m13 * (m21 * m32 - m22 * m31);
+  inv[0][0] = (m22 * m33 - m32 * m23) / det;
+  inv[0][1] = -(m21 * m33 - m31 * m23) / det;
+  inv[0][2] = (m21 * m32 - m31 * m22) / det;
+  inv[1][0] = -(m12 * m33 - m32 * m13) / det;
+  inv[1][1] = (m11 * m33 - m31 * m13) / det;
+  inv[1][2] = -(m11 * m32 - m31 * m12) / det;
+  inv[2][0] = (m12 * m23 - m22 * m13) / det;
+  inv[2][1] = -(m11 * m23 - m21 * m13) / det;
+  inv[2][2] = (m11 * m22 - m21 * m12) / det;
+  if (det_out) *det_out = det;
+}
+
+Box makeBox(const obox* b)
+{
+  Box box{};
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) box.c[c][r] = b->cell[3 * c + r];
+  double det;
+  invert(box.c, box.ic, &det);
+  box.volume = det;
+  box.triclinic = b->triclinic != 0;
+  return box;
+}
+
+Box scaledBox(const Box& b, int nx, int ny, int nz)
+{
+  obox o{};
+  int n[3] = {nx, ny, nz};
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) o.cell[3 * c + r] = b.c[c][r] * static_cast<double>(n[c]);
+  o.triclinic = b.triclinic ? 1 : 0;
+  return makeBox(&o);
+}
+
+inline void matvec(const double m[3][3], const double v[3], double out[3])
+{
+  for (int r = 0; r < 3; ++r) out[r] = m[0][r] * v[0] + m[1][r] * v[1] + m[2][r] * v[2];
+}
+
+inline double roundHalfAway(double x) { return static_cast<double>(static_cast<long long>(x + ((x >= 0.0) ? 0.5 : -0.5))); }
+
+// SimulationBox::applyPeriodicBoundaryConditions (simulationbox.ixx:131-161)
+inline void pbc(const Box& b, double dr[3])
+{
+  if (!b.triclinic)
+  {
+    dr[0] = dr[0] - roundHalfAway(dr[0] * b.ic[0][0]) * b.c[0][0];
+    dr[1] = dr[1] - roundHalfAway(dr[1] * b.ic[1][1]) * b.c[1][1];
+    dr[2] = dr[2] - roundHalfAway(dr[2] * b.ic[2][2]) * b.c[2][2];
+    return;
+  }
+  double s[3];
+  matvec(b.ic, dr, s);
+  for (int d = 0; d < 3; ++d) s[d] -= roundHalfAway(s[d]);
+  matvec(b.c, s, dr);
+}
+
+// SimulationBox::perpendicularWidths (simulationbox.cpp:137-148)
+void perpendicularWidths(const Box& b, double w[3])
+{
+  auto cross = [](const double* u, const double* v, double* o)
+  {
+    o[0] = u[1] * v[2] - u[2] * v[1];
+    o[1] = u[2] * v[0] - u[0] * v[2];
+    o[2] = u[0] * v[1] - u[1] * v[0];
+  };
+  double c1[3], c2[3], c3[3];
+  cross(b.c[0], b.c[1], c1);
+  cross(b.c[1], b.c[2], c2);
+  cross(b.c[0], b.c[2], c3);
+  double v = std::fabs(b.c[0][0] * c2[0] + b.c[0][1] * c2[1] + b.c[0][2] * c2[2]);
+  w[0] = v / std::sqrt(c2[0] * c2[0] + c2[1] * c2[1] + c2[2] * c2[2]);
+  w[1] = v / std::sqrt(c3[0] * c3[0] + c3[1] * c3[1] + c3[2] * c3[2]);
+  w[2] = v / std::sqrt(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);
+}
+
+// double3::fract (mathkit/double3.cpp:22-50)
+inline double fract1(double x)
+{
+  double s = x - std::rint(x);
+  if (s < 0.0) s += 1.0;
+  if (s > 1.0) s -= 1.0;
+  return s;
+}
+
+struct Factor
+{
+  double e, f1, f2, f3;
+};
+
+// potentialLennardJonesTricubicDerivative (potentials/interpolation/tricubic_derivative_lj.ixx:33-46) and the
+// repulsion/attraction variants (:48-78).
+inline Factor ljTricubic(int kind, double eps, double sigma, double shift, double r2)
+{
+  double arg1 = 4.0 * eps;
+  double arg2 = sigma * sigma;
+  double temp3 = (arg2 / r2) * (arg2 / r2) * (arg2 / r2);
+  double r4 = r2 * r2;
+  double r6 = r4 * r2;
+  switch (kind)
+  {
+    case 2:
+      return {arg1 * temp3 * temp3 - 0.0, -12.0 * arg1 * temp3 * temp3 / r2, 168.0 * arg1 * temp3 * temp3 / r4,
+              -2688.0 * arg1 * temp3 * temp3 / r6};
+    case 3:
+      return {arg1 * temp3 - 0.0, -6.0 * arg1 * temp3 / r2, 48.0 * arg1 * temp3 / r4, -480.0 * arg1 * temp3 / r6};
+    default:
+      return {arg1 * (temp3 * temp3 - temp3) - shift, -6.0 * arg1 * (2.0 * temp3 * temp3 - temp3) / r2,
+              24.0 * arg1 * (7.0 * temp3 * temp3 - 2.0 * temp3) / r4,
+              -96.0 * arg1 * (28.0 * temp3 * temp3 - 5.0 * temp3) / r6};
+  }
+}
+
+// potentialRealEwaldTricubicDerivative (potentials/interpolation/tricubic_derivative_real_ewald.ixx:32-56)
+inline Factor ewaldTricubic(double alpha, double rr, double r, double qa, double qb)
+{
+  const double C = coulombFactor();
+  double exp_factor = std::erfc(alpha * r);
+  double temp = C * qa * qb * exp_factor / r;
+  double exp_term_rr = 2.0 * alpha * r * std::exp(-alpha * alpha * rr) * kInvSqrtPi;
+  double alpha_r = alpha * r;
+  double alpha_r_2 = alpha_r * alpha_r;
+  double alpha_r_4 = alpha_r_2 * alpha_r_2;
+  double r3 = rr * r;
+  double r5 = r3 * rr;
+  double r7 = r5 * rr;
+  return {temp, -C * qa * qb * ((exp_term_rr + exp_factor) / r3),
+          C * qa * qb * ((exp_term_rr * (2.0 * alpha_r_2 + 3.0) + 3.0 * exp_factor) / r5),
+          -C * qa * qb * ((exp_term_rr * (4.0 * alpha_r_4 + 10 * alpha_r_2 + 15.0) + 15.0 * exp_factor) / r7)};
+}
+
+inline Factor gridFactor(int grid_type, const off* ff, double rr, int typeA, const oatom& b)
+{
+  int n = ff->n_types;
+  int idx = typeA * n + b.type;
+  if (grid_type == 1) return ewaldTricubic(ff->ewald_alpha, rr, std::sqrt(rr), 1.0, b.charge);
+  return ljTricubic(grid_type, ff->epsilon[idx], ff->sigma[idx], ff->shift[idx], rr);
+}
+
+// Interactions::calculateTricubicDerivativeAtPosition (interactions/framework_molecule_grid.cpp:76-144):
+// Cartesian energy, gradient, Hessian and third-derivative tensor.
+void tricubicCartesian(int grid_type, const off* ff, const Box& superBox, const double* posA, int typeA,
+                       const oatom* atoms, int n, double& energy, double g[3], double h[3][3], double t[3][3][3])
+{
+  const double rc2 = ff->cutoff_framework_vdw * ff->cutoff_framework_vdw;
+  energy = 0.0;
+  std::memset(g, 0, 3 * sizeof(double));
+  std::memset(h, 0, 9 * sizeof(double));
+  std::memset(t, 0, 27 * sizeof(double));
+  for (int a = 0; a < n; ++a)
+  {
+    double dr[3] = {posA[0] - atoms[a].x, posA[1] - atoms[a].y, posA[2] - atoms[a].z};
+    pbc(superBox, dr);
+    double rr = std::max(0.1, dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+    if (rr < rc2)
+    {
+      Factor v = gridFactor(grid_type, ff, rr, typeA, atoms[a]);
+      energy += v.e;
+      for (int i = 0; i != 3; ++i)
+      {
+        g[i] += dr[i] * v.f1;
+        for (int j = 0; j != 3; ++j)
+        {
+          h[i][j] += v.f2 * dr[i] * dr[j] + (i == j ? v.f1 : 0.0);
+          for (int k = 0; k != 3; ++k)
+          {
+            t[i][j][k] += v.f3 * dr[i] * dr[j] * dr[k] + (j == k ? v.f2 * dr[i] : 0.0) +
+                          (i == k ? v.f2 * dr[j] : 0.0) + (i == j ? v.f2 * dr[k] : 0.0);
+          }
+        }
+      }
+    }
+  }
+}
+
+void tricubicFractional(int grid_type, const off* ff, const Box& superBox, const double* posA, int typeA,
+                        const Box& unitBox, const oatom* atoms, int n, double out[8])
+{
+  const double rc2 = ff->cutoff_framework_vdw * ff->cutoff_framework_vdw;
+  if (!unitBox.triclinic)
+  {
+    // rectangular branch, framework_molecule_grid.cpp:192-243
+    double energy = 0.0, fx = 0.0, fy = 0.0, fz = 0.0, fxy = 0.0, fxz = 0.0, fyz = 0.0, fxyz = 0.0;
+    for (int a = 0; a < n; ++a)
+    {
+      double dr[3] = {posA[0] - atoms[a].x, posA[1] - atoms[a].y, posA[2] - atoms[a].z};
+      pbc(superBox, dr);
+      double rr = std::max(0.1, dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+      if (rr < rc2)
+      {
+        Factor v = gridFactor(grid_type, ff, rr, typeA, atoms[a]);
+        energy += v.e;
+        fx += dr[0] * v.f1;
+        fy += dr[1] * v.f1;
+        fz += dr[2] * v.f1;
+        fxy += v.f2 * dr[0] * dr[1];
+        fxz += v.f2 * dr[0] * dr[2];
+        fyz += v.f2 * dr[1] * dr[2];
+        fxyz += v.f3 * dr[0] * dr[1] * dr[2];
+      }
+    }
+    const double cx = unitBox.c[0][0], cy = unitBox.c[1][1], cz = unitBox.c[2][2];
+    out[0] = energy;
+    out[1] = fx * cx;
+    out[2] = fy * cy;
+    out[3] = fz * cz;
+    out[4] = fxy * cx * cy;
+    out[5] = fxz * cx * cz;
+    out[6] = fyz * cy * cz;
+    out[7] = fxyz * cx * cy * cz;
+    return;
+  }
+  // triclinic branch, framework_molecule_grid.cpp:244-279
+  double energy, g[3], h[3][3], t[3][3][3];
+  tricubicCartesian(grid_type, ff, superBox, posA, typeA, atoms, n, energy, g, h, t);
+  const auto& C = unitBox.c;  // C[row-vector index][p] = frameworkCell[index][p]
+  double f[3] = {0, 0, 0}, s01 = 0, s02 = 0, s12 = 0, t012 = 0;
+  for (int p = 0; p < 3; ++p)
+  {
+    f[0] += C[0][p] * g[p];
+    f[1] += C[1][p] * g[p];
+    f[2] += C[2][p] * g[p];
+    for (int q = 0; q < 3; ++q)
+    {
+      s01 += C[0][p] * C[1][q] * h[p][q];
+      s02 += C[0][p] * C[2][q] * h[p][q];
+      s12 += C[1][p] * C[2][q] * h[p][q];
+      for (int r = 0; r < 3; ++r) t012 += C[0][p] * C[1][q] * C[2][r] * t[p][q][r];
+    }
+  }
+  out[0] = energy;
+  out[1] = f[0];
+  out[2] = f[1];
+  out[3] = f[2];
+  out[4] = s01;
+  out[5] = s02;
+  out[6] = s12;
+  out[7] = t012;
+}
+
+struct GridSetup
+{
+  Box unit, super;
+  std::vector<oatom> atoms;
+  int ncx, ncy, ncz;
+};
+
+GridSetup gridSetup(const obox* unit_box, const oatom* unit_atoms, int n_unit, double cutoff, int nx, int ny, int nz)
+{
+  GridSetup s;
+  s.unit = makeBox(unit_box);
+  // SimulationBox::smallestNumberOfUnitCellsForMinimumImagesConvention (simulationbox.cpp:150-156)
+  double w[3];
+  perpendicularWidths(s.unit, w);
+  int n[3];
+  for (int d = 0; d < 3; ++d) n[d] = static_cast<int>(std::ceil(2.0 * cutoff / w[d]));
+  // Framework::makeSuperCell(int3) (framework.cpp:1105-1127): i outer, k inner, atoms innermost
+  for (int i = 0; i < n[0]; ++i)
+    for (int j = 0; j < n[1]; ++j)
+      for (int k = 0; k < n[2]; ++k)
+        for (int a = 0; a < n_unit; ++a)
+        {
+          oatom c = unit_atoms[a];
+          double f[3] = {static_cast<double>(i), static_cast<double>(j), static_cast<double>(k)}, d[3];
+          matvec(s.unit.c, f, d);
+          c.x += d[0];
+          c.y += d[1];
+          c.z += d[2];
+          s.atoms.push_back(c);
+        }
+  s.super = scaledBox(s.unit, n[0], n[1], n[2]);
+  s.ncx = nx - 1;
+  s.ncy = ny - 1;
+  s.ncz = nz - 1;
+  return s;
+}
+
+// One grid point of makeFrameworkInterpolationGrid, tricubic branch (interpolation_energy_grid.cpp:3826-3874).
+void gridPoint(int grid_type, const off* ff, const GridSetup& s, int probe_type, int64_t i, int64_t j, int64_t k,
+               double* dst)
+{
+  double delta[3] = {1.0 / static_cast<double>(s.ncx), 1.0 / static_cast<double>(s.ncy),
+                     1.0 / static_cast<double>(s.ncz)};
+  double frac[3] = {static_cast<double>(i) * delta[0], static_cast<double>(j) * delta[1],
+                    static_cast<double>(k) * delta[2]};
+  double pos[3];
+  matvec(s.unit.c, frac, pos);
+  double values[8];
+  tricubicFractional(grid_type, ff, s.super, pos, probe_type, s.unit, s.atoms.data(), static_cast<int>(s.atoms.size()),
+                     values);
+  const double cx = static_cast<double>(s.ncx), cy = static_cast<double>(s.ncy), cz = static_cast<double>(s.ncz);
+  values[1] /= cx;
+  values[2] /= cy;
+  values[3] /= cz;
+  values[4] /= cx * cy;
+  values[5] /= cx * cz;
+  values[6] /= cy * cz;
+  values[7] /= cx * cy * cz;
+  const double oc = ff->overlap_criteria;
+  if (values[0] > oc)
+  {
+    dst[0] = 2.0 * oc;
+    dst[1] = std::clamp(values[1], -oc, oc);
+    dst[2] = std::clamp(values[2], -oc, oc);
+    dst[3] = std::clamp(values[3], -oc, oc);
+    for (int l = 4; l < 8; ++l) dst[l] = 0.0;
+  }
+  else
+  {
+    for (int l = 0; l < 8; ++l) dst[l] = values[l];
+  }
+}
+
+// Tricubic coefficient matrix: inverse of the map from the 64 monomial coefficients a[i+4j+16k] to the 64 corner
+// values X[8*v + corner] (v = f, fx, fy, fz, fxy, fxz, fyz, fxyz; corner bit 0 = x, bit 1 = y, bit 2 = z).
+struct TricubicMatrix
+{
+  double m[64][64];
+  TricubicMatrix()
+  {
+    static const int dv[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                                 {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+    auto dmono = [](int p, int d, int x) -> double
+    {
+      // d-th derivative of t^p at t = x (x in {0,1})
+      if (d > p) return 0.0;
+      double c = 1.0;
+      for (int q = 0; q < d; ++q) c *= static_cast<double>(p - q);
+      if (x == 0) return (p == d) ? c : 0.0;
+      return c;
+    };
+    double B[64][128];
+    for (int v = 0; v < 8; ++v)
+      for (int corner = 0; corner < 8; ++corner)
+      {
+        int row = 8 * v + corner;
+        int x = corner & 1, y = (corner >> 1) & 1, z = (corner >> 2) & 1;
+        for (int k = 0; k < 4; ++k)
+          for (int j = 0; j < 4; ++j)
+            for (int i = 0; i < 4; ++i)
+              B[row][i + 4 * j + 16 * k] = dmono(i, dv[v][0], x) * dmono(j, dv[v][1], y) * dmono(k, dv[v][2], z);
+        for (int c = 0; c < 64; ++c) B[row][64 + c] = (c == row) ? 1.0 : 0.0;
+      }
+    // Gauss-Jordan with partial pivoting; the inverse has small integer entries and is rounded to them.
+    for (int col = 0; col < 64; ++col)
+    {
+      int piv = col;
+      for (int r = col + 1; r < 64; ++r)
+        if (std::fabs(B[r][col]) > std::fabs(B[piv][col])) piv = r;
+      if (piv != col)
+        for (int c = 0; c < 128; ++c) std::swap(B[piv][c], B[col][c]);
+      double p = B[col][col];
+      for (int c = 0; c < 128; ++c) B[col][c] /= p;
+      for (int r = 0; r < 64; ++r)
+      {
+        if (r == col) continue;
+        double f = B[r][col];
+        if (f == 0.0) continue;
+        for (int c = 0; c < 128; ++c) B[r][c] -= f * B[col][c];
+      }
+    }
+    for (int r = 0; r < 64; ++r)
+      for (int c = 0; c < 64; ++c) m[r][c] = std::rint(B[r][64 + c]);
+  }
+};
+
+const TricubicMatrix& tricubicMatrix()
+{
+  static const TricubicMatrix tm;
+  return tm;
+}
+
+double interpolateTricubic(const double* data, int nx, int ny, int nz, const Box& unit, const double* pos)
+{
+  // InterpolationEnergyGrid::interpolate, tricubic branch (interpolation_energy_grid.cpp:3980-4118)
+  double sraw[3], s[3];
+  matvec(unit.ic, pos, sraw);
+  for (int d = 0; d < 3; ++d) s[d] = fract1(sraw[d]);
+  const int ncx = nx - 1, ncy = ny - 1, ncz = nz - 1;
+  int64_t x0 = std::min(static_cast<int64_t>(s[0] * static_cast<double>(ncx)), static_cast<int64_t>(ncx - 1));
+  int64_t y0 = std::min(static_cast<int64_t>(s[1] * static_cast<double>(ncy)), static_cast<int64_t>(ncy - 1));
+  int64_t z0 = std::min(static_cast<int64_t>(s[2] * static_cast<double>(ncz)), static_cast<int64_t>(ncz - 1));
+  int64_t x1 = x0 + 1, y1 = y0 + 1, z1 = z0 + 1;
+  s[0] = (s[0] * static_cast<double>(ncx)) - static_cast<double>(x0);
+  s[1] = (s[1] * static_cast<double>(ncy)) - static_cast<double>(y0);
+  s[2] = (s[2] * static_cast<double>(ncz)) - static_cast<double>(z0);
+  auto at = [&](int l, int64_t i, int64_t j, int64_t k) { return data[l + 8 * (i + nx * (j + ny * k))]; };
+  double X[64], a[64];
+  for (int l = 0; l != 8; ++l)
+  {
+    X[8 * l + 0] = at(l, x0, y0, z0);
+    X[8 * l + 1] = at(l, x1, y0, z0);
+    X[8 * l + 2] = at(l, x0, y1, z0);
+    X[8 * l + 3] = at(l, x1, y1, z0);
+    X[8 * l + 4] = at(l, x0, y0, z1);
+    X[8 * l + 5] = at(l, x1, y0, z1);
+    X[8 * l + 6] = at(l, x0, y1, z1);
+    X[8 * l + 7] = at(l, x1, y1, z1);
+  }
+  const auto& M = tricubicMatrix().m;
+  for (int r = 0; r < 64; ++r)
+  {
+    double acc = 0.0;
+    for (int c = 0; c < 64; ++c) acc += M[r][c] * X[c];
+    a[r] = acc;
+  }
+  double value = 0.0;
+  for (int k = 0; k != 4; ++k)
+    for (int j = 0; j != 4; ++j)
+      for (int i = 0; i != 4; ++i)
+        value += a[i + 4 * j + 16 * k] * std::pow(s[0], i) * std::pow(s[1], j) * std::pow(s[2], k);
+  return value;
+}
+
+inline int groupOf(const oatom& a) { return a.group_fractional & 0x0f; }
+inline bool fractionalOf(const oatom& a) { return (a.group_fractional >> 4) != 0; }
+
+inline void addDud(double* arr, int gA, int gB, double sA, double sB, double factor)
+{
+  // RunningEnergy::addDudlambda* (running_energy.ixx:258-279)
+  if (gA != 0) arr[gA - 1] += sB * factor;
+  if (gB != 0) arr[gB - 1] += sA * factor;
+}
+
+void pairVDW(const off* ff, double sA, double sB, double rr, int tA, int tB, double out[2])
+{
+  // potentialVDW<0>, Lennard-Jones branch (potentials/pair_vdw.ixx:85-101); other types -> zero
+  int idx = tA * ff->n_types + tB;
+  if (!ff->lj[idx])
+  {
+    out[0] = 0.0;
+    out[1] = 0.0;
+    return;
+  }
+  double scaling = sA * sB;
+  double arg1 = 4.0 * ff->epsilon[idx];
+  double arg2 = ff->sigma[idx] * ff->sigma[idx];
+  double arg3 = ff->shift[idx];
+  double temp = (rr / arg2);
+  double temp3 = temp * temp * temp;
+  double inv_scaling = 1.0 - scaling;
+  double rri3 = 1.0 / (temp3 + 0.5 * inv_scaling * inv_scaling);
+  double rri6 = rri3 * rri3;
+  double term = arg1 * (rri3 * (rri3 - 1.0)) - arg3;
+  double dlambda_term = arg1 * scaling * inv_scaling * (2.0 * rri6 * rri3 - rri6);
+  out[0] = scaling * term;
+  out[1] = term + dlambda_term;
+}
+
+void pairCoulomb(const off* ff, double sA, double sB, double r, double qA, double qB, double out[2])
+{
+  // potentialCoulomb<0>, Ewald branch (potentials/pair_coulomb.ixx:51-77)
+  double scaling = sA * sB;
+  double alpha = ff->ewald_alpha;
+  double prefactor = coulombFactor() * qA * qB;
+  double s = r + 0.01 * (1.0 - scaling);
+  double inverseS = 1.0 / s;
+  double inverseSS = inverseS * inverseS;
+  double erfcTerm = std::erfc(alpha * s);
+  double gaussian = std::exp(-alpha * alpha * s * s) * kInvSqrtPi;
+  double phi = erfcTerm * inverseS;
+  double phiPrime = -(erfcTerm * inverseSS + 2.0 * alpha * gaussian * inverseS);
+  out[0] = scaling * prefactor * phi;
+  out[1] = prefactor * (phi - scaling * 0.01 * phiPrime);
+}
+
+// ---- Ewald (interactions/ewald.cpp, interactions/ewald_kvector.ixx) ----
+struct Cplx
+{
+  double re, im;
+};
+inline Cplx cmul(Cplx a, Cplx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+inline Cplx conjIf(Cplx a, bool c) { return c ? Cplx{a.re, -a.im} : a; }
+inline double norm2(Cplx a) { return a.re * a.re + a.im * a.im; }
+
+struct EikTables
+{
+  int n, kx, ky, kz;
+  std::vector<Cplx> x, y, z;
+  // Ewald::buildEikTables (ewald_kvector.ixx): atom-major eik_x[i + kx*N], k = 0,1 explicit, then recurrence
+  EikTables(const Box& b, const std::vector<const oatom*>& atoms, int kxm, int kym, int kzm)
+      : n(static_cast<int>(atoms.size())), kx(kxm), ky(kym), kz(kzm)
+  {
+    x.resize(static_cast<size_t>(n) * (kxm + 1));
+    y.resize(static_cast<size_t>(n) * (kym + 1));
+    z.resize(static_cast<size_t>(n) * (kzm + 1));
+    for (int i = 0; i < n; ++i)
+    {
+      x[i] = y[i] = z[i] = Cplx{1.0, 0.0};
+      double p[3] = {atoms[i]->x, atoms[i]->y, atoms[i]->z}, s[3];
+      matvec(b.ic, p, s);
+      for (int d = 0; d < 3; ++d) s[d] *= 2.0 * kPi;
+      if (kxm >= 1) x[i + n] = Cplx{std::cos(s[0]), std::sin(s[0])};
+      if (kym >= 1) y[i + n] = Cplx{std::cos(s[1]), std::sin(s[1])};
+      if (kzm >= 1) z[i + n] = Cplx{std::cos(s[2]), std::sin(s[2])};
+    }
+    for (int k = 2; k <= kxm; ++k)
+      for (int i = 0; i < n; ++i) x[i + k * n] = cmul(x[i + (k - 1) * n], x[i + n]);
+    for (int k = 2; k <= kym; ++k)
+      for (int i = 0; i < n; ++i) y[i + k * n] = cmul(y[i + (k - 1) * n], y[i + n]);
+    for (int k = 2; k <= kzm; ++k)
+      for (int i = 0; i < n; ++i) z[i + k * n] = cmul(z[i + (k - 1) * n], z[i + n]);
+  }
+  // fillEikXYRow + eikPhase
+  Cplx xy(int i, int kxv, int kyv) const { return cmul(x[i + n * kxv], conjIf(y[i + n * std::abs(kyv)], kyv < 0)); }
+  Cplx zf(int i, int kzv) const { return conjIf(z[i + n * std::abs(kzv)], kzv < 0); }
+};
+
+// Iterates the k-vectors in the reference order, calling body(kx, ky, kz, rksq, factor) for each accepted one.
+template <typename F>
+void forEachK(const off* ff, const Box& b, F&& body)
+{
+  double ax[3] = {b.ic[0][0], b.ic[1][0], b.ic[2][0]};
+  double ay[3] = {b.ic[0][1], b.ic[1][1], b.ic[2][1]};
+  double az[3] = {b.ic[0][2], b.ic[1][2], b.ic[2][2]};
+  const double prefactor = coulombFactor() * (2.0 * kPi / b.volume);
+  for (int kx = 0; kx <= ff->kmax_x; ++kx)
+  {
+    double kvx[3];
+    for (int d = 0; d < 3; ++d) kvx[d] = 2.0 * kPi * static_cast<double>(kx) * ax[d];
+    double factor = (kx == 0) ? (1.0 * prefactor) : (2.0 * prefactor);
+    for (int ky = -ff->kmax_y; ky <= ff->kmax_y; ++ky)
+    {
+      double kvy[3];
+      for (int d = 0; d < 3; ++d) kvy[d] = 2.0 * kPi * static_cast<double>(ky) * ay[d];
+      for (int kz = -ff->kmax_z; kz <= ff->kmax_z; ++kz)
+      {
+        double kvz[3];
+        for (int d = 0; d < 3; ++d) kvz[d] = 2.0 * kPi * static_cast<double>(kz) * az[d];
+        double kv[3] = {kvx[0] + kvy[0] + kvz[0], kvx[1] + kvy[1] + kvz[1], kvx[2] + kvy[2] + kvz[2]};
+        double rksq = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
+        uint64_t ksq = static_cast<uint64_t>(kx * kx + ky * ky + kz * kz);
+        if ((ksq != 0) && (ksq <= ff->recip_int_cutoff_sq) && (rksq < ff->recip_cutoff_sq))
+          body(kx, ky, kz, rksq, factor);
+      }
+    }
+  }
+}
+
+// Potentials::ewaldExclusionFactors (potentials/coulomb_real_space.ixx:49-65): potential and dU/dlambda factor
+inline void exclusionFactors(double alpha, double scalingTotal, double r, double& potential, double& dudl)
+{
+  const double offset = 0.01 * (1.0 - scalingTotal);
+  const double s = r + offset;
+  const double inverseS = 1.0 / s;
+  potential = std::erf(alpha * s) * inverseS;
+  const double gaussianTerm = 2.0 * alpha * kInvSqrtPi * std::exp(-alpha * alpha * s * s);
+  const double firstDerivative = (gaussianTerm - potential) * inverseS;
+  dudl = potential - scalingTotal * 0.01 * firstDerivative;
+}
+
+void addFourierDUdlambda(oenergy* e, double factor, Cplx sk, const Cplx* dsk)
+{
+  // ewald.cpp:166-173
+  for (int g = 0; g != 4; ++g) e->dudlambda_ewald[g] += factor * (sk.re * dsk[g].re + sk.im * dsk[g].im);
+}
+
+}  // namespace
+
+extern "C"
+{
+double oracle_energy_to_kelvin(void) { return energyConversionFactor() * kAvogadroConstant / kMolarGasConstant; }
+double oracle_kelvin_to_energy(void) { return kMolarGasConstant / (energyConversionFactor() * kAvogadroConstant); }
+double oracle_coulomb_factor(void) { return coulombFactor(); }
+
+void oracle_tricubic_fractional_at_position(int grid_type, const off* ff, const obox* super_box, const double* pos,
+                                            int type_a, const obox* unit_box, const oatom* super_atoms, int n,
+                                            double out[8])
+{
+  Box sb = makeBox(super_box), ub = makeBox(unit_box);
+  tricubicFractional(grid_type, ff, sb, pos, type_a, ub, super_atoms, n, out);
+}
+
+int oracle_make_tricubic_grid(int grid_type, const off* ff, const obox* unit_box, const oatom* unit_atoms, int n_unit,
+                              int probe_type, double cutoff, int nx, int ny, int nz, const int64_t* points,
+                              int64_t n_points, int threads, double* out)
+{
+  GridSetup s = gridSetup(unit_box, unit_atoms, n_unit, cutoff, nx, ny, nz);
+  const int64_t total = points ? n_points : static_cast<int64_t>(nx) * ny * nz;
+#ifdef _OPENMP
+  if (threads < 1) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+#endif
+  for (int64_t p = 0; p < total; ++p)
+  {
+    int64_t flat = points ? points[p] : p;
+    int64_t i = flat % nx, j = (flat / nx) % ny, k = flat / (static_cast<int64_t>(nx) * ny);
+    double* dst = points ? out + 8 * p : out + 8 * flat;
+    gridPoint(grid_type, ff, s, probe_type, i, j, k, dst);
+  }
+  (void)threads;
+  return static_cast<int>(s.atoms.size());
+}
+
+int64_t oracle_grid_pair_count(int grid_type, const off* ff, const obox* unit_box, const oatom* unit_atoms, int n_unit,
+                               int probe_type, double cutoff, int nx, int ny, int nz, const int64_t* points,
+                               int64_t n_points, int threads)
+{
+  GridSetup s = gridSetup(unit_box, unit_atoms, n_unit, cutoff, nx, ny, nz);
+  const int64_t total = points ? n_points : static_cast<int64_t>(nx) * ny * nz;
+  const double rc2 = ff->cutoff_framework_vdw * ff->cutoff_framework_vdw;
+  std::vector<char> active(s.atoms.size());
+  for (size_t a = 0; a < s.atoms.size(); ++a)
+  {
+    const oatom& b = s.atoms[a];
+    active[a] = (grid_type == 1) ? (b.charge != 0.0) : (ff->epsilon[probe_type * ff->n_types + b.type] != 0.0);
+  }
+  int64_t count = 0;
+#ifdef _OPENMP
+  if (threads < 1) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : count) num_threads(threads)
+#endif
+  for (int64_t p = 0; p < total; ++p)
+  {
+    int64_t flat = points ? points[p] : p;
+    int64_t i = flat % nx, j = (flat / nx) % ny, k = flat / (static_cast<int64_t>(nx) * ny);
+    double frac[3] = {static_cast<double>(i) / s.ncx, static_cast<double>(j) / s.ncy, static_cast<double>(k) / s.ncz};
+    double pos[3];
+    matvec(s.unit.c, frac, pos);
+    for (size_t a = 0; a < s.atoms.size(); ++a)
+    {
+      if (!active[a]) continue;
+      double dr[3] = {pos[0] - s.atoms[a].x, pos[1] - s.atoms[a].y, pos[2] - s.atoms[a].z};
+      pbc(s.super, dr);
+      double rr = std::max(0.1, dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+      if (rr < rc2) ++count;
+    }
+  }
+  (void)threads;
+  return count;
+}
+
+void oracle_tricubic_matrix(double* m)
+{
+  const auto& M = tricubicMatrix().m;
+  for (int r = 0; r < 64; ++r)
+    for (int c = 0; c < 64; ++c) m[64 * r + c] = M[r][c];
+}
+
+double oracle_grid_interpolate(const double* data, int nx, int ny, int nz, const obox* unit_box, const double* pos)
+{
+  Box ub = makeBox(unit_box);
+  return interpolateTricubic(data, nx, ny, nz, ub, pos);
+}
+
+void oracle_pair_vdw(const off* ff, double scaling_a, double scaling_b, double rr, int type_a, int type_b,
+                     double out[2])
+{
+  pairVDW(ff, scaling_a, scaling_b, rr, type_a, type_b, out);
+}
+
+void oracle_pair_coulomb(const off* ff, double scaling_a, double scaling_b, double r, double qa, double qb,
+                         double out[2])
+{
+  pairCoulomb(ff, scaling_a, scaling_b, r, qa, qb, out);
+}
+
+int oracle_cbmc_framework_molecule(const off* ff, const obox* box, const double* const* grids, int gnx, int gny,
+                                   int gnz, const obox* grid_box, const oatom* fw, int n_fw, double cutoff_vdw,
+                                   double cutoff_coulomb, const oatom* atoms, int n_atoms, int skip, oenergy* e)
+{
+  // cbmc/interactions_framework_molecule.cpp:31-104 (serial variant)
+  std::memset(e, 0, sizeof(oenergy));
+  Box b = makeBox(box);
+  Box gb = grid_box ? makeBox(grid_box) : b;
+  const bool useCharge = ff->use_charge != 0;
+  const double overlap = ff->overlap_criteria;
+  const double rcv2 = cutoff_vdw * cutoff_vdw;
+  const double rcc2 = cutoff_coulomb * cutoff_coulomb;
+  for (int index = 0; index < n_atoms; ++index)
+  {
+    if (index == skip) continue;
+    const oatom& B = atoms[index];
+    double posB[3] = {B.x, B.y, B.z};
+    if (grids && grids[B.type] && !fractionalOf(B))
+    {
+      double energy = interpolateTricubic(grids[B.type], gnx, gny, gnz, gb, posB);
+      if (energy > overlap) return 0;
+      e->framework_molecule_vdw += energy;
+      if (useCharge && grids[ff->n_types])
+        e->framework_molecule_charge += B.charge * interpolateTricubic(grids[ff->n_types], gnx, gny, gnz, gb, posB);
+      continue;
+    }
+    for (int a = 0; a < n_fw; ++a)
+    {
+      const oatom& A = fw[a];
+      double dr[3] = {A.x - B.x, A.y - B.y, A.z - B.z};
+      pbc(b, dr);
+      double rr = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+      if (rr < rcv2)
+      {
+        double f[2];
+        pairVDW(ff, A.scaling_vdw, B.scaling_vdw, rr, A.type, B.type, f);
+        if (f[0] > overlap) return 0;
+        e->framework_molecule_vdw += f[0];
+        addDud(e->dudlambda_vdw, groupOf(A), groupOf(B), A.scaling_vdw, B.scaling_vdw, f[1]);
+      }
+      if (useCharge && rr < rcc2)
+      {
+        double r = std::sqrt(rr);
+        double f[2];
+        pairCoulomb(ff, A.scaling_coulomb, B.scaling_coulomb, r, A.charge, B.charge, f);
+        e->framework_molecule_charge += f[0];
+        addDud(e->dudlambda_charge, groupOf(A), groupOf(B), A.scaling_coulomb, B.scaling_coulomb, f[1]);
+      }
+    }
+  }
+  return 1;
+}
+
+int oracle_cbmc_intermolecular(const off* ff, const obox* box, const oatom* molecule_atoms, int n_mol,
+                               double cutoff_vdw, double cutoff_coulomb, const oatom* atoms, int n_atoms, int skip,
+                               int64_t skip_background_molecule, oenergy* e)
+{
+  // cbmc/interactions_intermolecular.cpp:22-95
+  std::memset(e, 0, sizeof(oenergy));
+  Box b = makeBox(box);
+  const bool useCharge = ff->use_charge != 0;
+  const double overlap = ff->overlap_criteria;
+  const double rcv2 = cutoff_vdw * cutoff_vdw;
+  const double rcc2 = cutoff_coulomb * cutoff_coulomb;
+  for (int m = 0; m < n_mol; ++m)
+  {
+    const oatom& A = molecule_atoms[m];
+    if (skip_background_molecule >= 0 && A.molecule_id == static_cast<uint64_t>(skip_background_molecule)) continue;
+    for (int index = 0; index < n_atoms; ++index)
+    {
+      if (index == skip) continue;
+      const oatom& B = atoms[index];
+      if (A.molecule_id == B.molecule_id) continue;
+      double dr[3] = {A.x - B.x, A.y - B.y, A.z - B.z};
+      pbc(b, dr);
+      double rr = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+      if (rr < rcv2)
+      {
+        double f[2];
+        pairVDW(ff, A.scaling_vdw, B.scaling_vdw, rr, A.type, B.type, f);
+        if (f[0] > overlap) return 0;
+        e->molecule_molecule_vdw += f[0];
+        addDud(e->dudlambda_vdw, groupOf(A), groupOf(B), A.scaling_vdw, B.scaling_vdw, f[1]);
+      }
+      if (useCharge && rr < rcc2)
+      {
+        double r = std::sqrt(rr);
+        double f[2];
+        pairCoulomb(ff, A.scaling_coulomb, B.scaling_coulomb, r, A.charge, B.charge, f);
+        e->molecule_molecule_charge += f[0];
+        addDud(e->dudlambda_charge, groupOf(A), groupOf(B), A.scaling_coulomb, B.scaling_coulomb, f[1]);
+      }
+    }
+  }
+  return 1;
+}
+
+int64_t oracle_ewald_kvectors(const off* ff, const obox* box, int32_t* kvec, double* temp, double* single_ion_sum)
+{
+  Box b = makeBox(box);
+  const double alpha_squared = ff->ewald_alpha * ff->ewald_alpha;
+  int64_t n = 0;
+  double sum = 0.0;
+  forEachK(ff, b,
+           [&](int kx, int ky, int kz, double rksq, double factor)
+           {
+             double t = factor * std::exp((-0.25 / alpha_squared) * rksq) / rksq;
+             if (kvec)
+             {
+               kvec[3 * n + 0] = kx;
+               kvec[3 * n + 1] = ky;
+               kvec[3 * n + 2] = kz;
+             }
+             if (temp) temp[n] = t;
+             sum += t;
+             ++n;
+           });
+  if (single_ion_sum) *single_ion_sum = sum;
+  return n;
+}
+
+void oracle_ewald_rigid(const off* ff, const obox* box, const oatom* fw, int n_fw, double* s_rigid)
+{
+  // precomputeEwaldFourierRigid, ewald.cpp:276-348
+  Box b = makeBox(box);
+  std::vector<const oatom*> ptr(n_fw);
+  for (int i = 0; i < n_fw; ++i) ptr[i] = &fw[i];
+  EikTables eik(b, ptr, ff->kmax_x, ff->kmax_y, ff->kmax_z);
+  int64_t nvec = 0;
+  int lastKx = -1, lastKy = 1 << 30;
+  std::vector<Cplx> xy(n_fw);
+  forEachK(ff, b,
+           [&](int kx, int ky, int kz, double, double)
+           {
+             if (kx != lastKx || ky != lastKy)
+             {
+               for (int i = 0; i < n_fw; ++i) xy[i] = eik.xy(i, kx, ky);
+               lastKx = kx;
+               lastKy = ky;
+             }
+             Cplx sum{0.0, 0.0};
+             for (int i = 0; i < n_fw; ++i)
+             {
+               Cplx e = cmul(xy[i], eik.zf(i, kz));
+               double w = fw[i].scaling_coulomb * fw[i].charge;
+               sum.re += w * e.re;
+               sum.im += w * e.im;
+             }
+             s_rigid[2 * nvec] = sum.re;
+             s_rigid[2 * nvec + 1] = sum.im;
+             ++nvec;
+           });
+}
+
+void oracle_ewald_fourier_energy(const off* ff, const obox* box, const double* s_rigid, const oatom* atoms, int n,
+                                 const int32_t* molecule_sizes, int n_molecules, double net_charge_framework,
+                                 double* stored, oenergy* e)
+{
+  // computeEwaldFourierEnergy, ewald.cpp:352-563 (Ewald charge method)
+  std::memset(e, 0, sizeof(oenergy));
+  if (!ff->use_charge) return;
+  Box b = makeBox(box);
+  const double alpha = ff->ewald_alpha;
+  const double alpha_squared = alpha * alpha;
+  const double C = coulombFactor();
+  std::vector<const oatom*> ptr(n);
+  for (int i = 0; i < n; ++i) ptr[i] = &atoms[i];
+  EikTables eik(b, ptr, ff->kmax_x, ff->kmax_y, ff->kmax_z);
+  double singleIonFourierSum = 0.0;
+  int64_t nvec = 0;
+  int lastKx = -1, lastKy = 1 << 30;
+  std::vector<Cplx> xy(n);
+  forEachK(ff, b,
+           [&](int kx, int ky, int kz, double rksq, double factor)
+           {
+             if (kx != lastKx || ky != lastKy)
+             {
+               for (int i = 0; i < n; ++i) xy[i] = eik.xy(i, kx, ky);
+               lastKx = kx;
+               lastKy = ky;
+             }
+             double temp = factor * std::exp((-0.25 / alpha_squared) * rksq) / rksq;
+             singleIonFourierSum += temp;
+             Cplx ck{0.0, 0.0};
+             Cplx cg[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+             for (int i = 0; i < n; ++i)
+             {
+               Cplx ei = cmul(xy[i], eik.zf(i, kz));
+               double q = atoms[i].charge, sc = atoms[i].scaling_coulomb;
+               ck.re += sc * q * ei.re;
+               ck.im += sc * q * ei.im;
+               int g = groupOf(atoms[i]);
+               if (g != 0)
+               {
+                 cg[g - 1].re += q * ei.re;
+                 cg[g - 1].im += q * ei.im;
+               }
+             }
+             Cplx rigid{0.0, 0.0};
+             if (s_rigid) rigid = Cplx{s_rigid[2 * nvec], s_rigid[2 * nvec + 1]};
+             Cplx rigidG[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+             Cplx total{rigid.re + ck.re, rigid.im + ck.im};
+             Cplx totalG[4];
+             for (int g = 0; g < 4; ++g) totalG[g] = Cplx{rigidG[g].re + cg[g].re, rigidG[g].im + cg[g].im};
+             double rigidEnergy = temp * (rigid.re * rigid.re + rigid.im * rigid.im);
+             e->ewald_fourier += temp * (total.re * total.re + total.im * total.im) - rigidEnergy;
+             if (ff->omit_inter) e->ewald_fourier -= temp * (ck.re * ck.re + ck.im * ck.im);
+             addFourierDUdlambda(e, 2.0 * temp, total, totalG);
+             addFourierDUdlambda(e, -2.0 * temp, rigid, rigidG);
+             if (stored)
+             {
+               double* s = stored + 10 * nvec;
+               s[0] = total.re;
+               s[1] = total.im;
+               for (int g = 0; g < 4; ++g)
+               {
+                 s[2 + 2 * g] = totalG[g].re;
+                 s[3 + 2 * g] = totalG[g].im;
+               }
+             }
+             ++nvec;
+           });
+  if (!ff->omit_inter)
+  {
+    double prefactor_self = C * alpha / std::sqrt(kPi);
+    for (int i = 0; i < n; ++i)
+    {
+      double q = atoms[i].charge, sc = atoms[i].scaling_coulomb;
+      int g = groupOf(atoms[i]);
+      e->ewald_self -= prefactor_self * sc * q * sc * q;
+      if (g != 0) e->dudlambda_ewald[g - 1] -= 2.0 * prefactor_self * sc * q * q;
+    }
+    int index = 0;
+    for (int m = 0; m < n_molecules; ++m)
+    {
+      int size = molecule_sizes[m];
+      const oatom* span = atoms + index;
+      for (int i = 0; i + 1 < size; ++i)
+        for (int j = i + 1; j < size; ++j)
+        {
+          double dr[3] = {span[i].x - span[j].x, span[i].y - span[j].y, span[i].z - span[j].z};
+          pbc(b, dr);
+          double r = std::sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+          double sA = span[i].scaling_coulomb, sB = span[j].scaling_coulomb;
+          double pot, dudl;
+          exclusionFactors(alpha, sA * sB, r, pot, dudl);
+          double prefactor = C * span[i].charge * span[j].charge;
+          e->ewald_exclusion -= sA * sB * prefactor * pot;
+          addDud(e->dudlambda_ewald, groupOf(span[i]), groupOf(span[j]), sA, sB, -prefactor * dudl);
+        }
+      index += size;
+    }
+  }
+  // net-charge correction (ewald.cpp:526-560)
+  double netChargeAdsorbates = 0.0;
+  double netChargeDerivative[4] = {0, 0, 0, 0};
+  for (int i = 0; i < n; ++i)
+  {
+    netChargeAdsorbates += atoms[i].scaling_coulomb * atoms[i].charge;
+    int g = groupOf(atoms[i]);
+    if (g != 0) netChargeDerivative[g - 1] += atoms[i].charge;
+  }
+  double uIon = -(singleIonFourierSum - C * alpha / std::sqrt(kPi));
+  if (ff->omit_inter)
+  {
+    e->ewald_fourier += 2.0 * uIon * net_charge_framework * netChargeAdsorbates;
+    for (int g = 0; g < 4; ++g) e->dudlambda_ewald[g] += 2.0 * uIon * net_charge_framework * netChargeDerivative[g];
+  }
+  else
+  {
+    e->ewald_fourier += uIon * (2.0 * net_charge_framework + netChargeAdsorbates) * netChargeAdsorbates;
+    for (int g = 0; g < 4; ++g)
+      e->dudlambda_ewald[g] += 2.0 * uIon * (net_charge_framework + netChargeAdsorbates) * netChargeDerivative[g];
+  }
+}
+
+void oracle_ewald_delta(const off* ff, const obox* box, const double* stored, const oatom* new_atoms, int n_new,
+                        const oatom* old_atoms, int n_old, double net_charge, const double* net_charge_derivative_ext,
+                        double* trial, oenergy* e)
+{
+  // energyDifferenceEwaldFourier, ewald.cpp:1043-1244 (Ewald charge method)
+  std::memset(e, 0, sizeof(oenergy));
+  if (!ff->use_charge) return;
+  Box b = makeBox(box);
+  const double alpha = ff->ewald_alpha;
+  const double alpha_squared = alpha * alpha;
+  const double C = coulombFactor();
+  const int n = n_new + n_old;
+  std::vector<const oatom*> ptr(n);  // old atoms first, then new (ewald_kvector.ixx buildEikTables overload)
+  for (int i = 0; i < n_old; ++i) ptr[i] = &old_atoms[i];
+  for (int i = 0; i < n_new; ++i) ptr[n_old + i] = &new_atoms[i];
+  EikTables eik(b, ptr, ff->kmax_x, ff->kmax_y, ff->kmax_z);
+  double singleIonFourierSum = 0.0;
+  int64_t nvec = 0;
+  int lastKx = -1, lastKy = 1 << 30;
+  std::vector<Cplx> xy(n);
+  forEachK(ff, b,
+           [&](int kx, int ky, int kz, double rksq, double factor)
+           {
+             if (kx != lastKx || ky != lastKy)
+             {
+               for (int i = 0; i < n; ++i) xy[i] = eik.xy(i, kx, ky);
+               lastKx = kx;
+               lastKy = ky;
+             }
+             Cplx co{0, 0}, cn{0, 0};
+             Cplx go[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}}, gn[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+             for (int i = 0; i < n; ++i)
+             {
+               Cplx ei = cmul(xy[i], eik.zf(i, kz));
+               const oatom& A = *ptr[i];
+               double q = A.charge, sc = A.scaling_coulomb;
+               Cplx& c = (i < n_old) ? co : cn;
+               Cplx* g = (i < n_old) ? go : gn;
+               c.re += sc * q * ei.re;
+               c.im += sc * q * ei.im;
+               int gi = groupOf(A);
+               if (gi != 0)
+               {
+                 g[gi - 1].re += q * ei.re;
+                 g[gi - 1].im += q * ei.im;
+               }
+             }
+             double temp = factor * std::exp((-0.25 / alpha_squared) * rksq) / rksq;
+             singleIonFourierSum += temp;
+             const double* s = stored + 10 * nvec;
+             Cplx S{s[0], s[1]};
+             Cplx SG[4];
+             for (int g = 0; g < 4; ++g) SG[g] = Cplx{s[2 + 2 * g], s[3 + 2 * g]};
+             Cplx T{S.re + cn.re - co.re, S.im + cn.im - co.im};
+             Cplx TG[4];
+             for (int g = 0; g < 4; ++g) TG[g] = Cplx{SG[g].re + gn[g].re - go[g].re, SG[g].im + gn[g].im - go[g].im};
+             e->ewald_fourier += temp * norm2(T);
+             e->ewald_fourier -= temp * norm2(S);
+             addFourierDUdlambda(e, 2.0 * temp, T, TG);
+             addFourierDUdlambda(e, -2.0 * temp, S, SG);
+             if (trial)
+             {
+               double* t = trial + 10 * nvec;
+               t[0] = T.re;
+               t[1] = T.im;
+               for (int g = 0; g < 4; ++g)
+               {
+                 t[2 + 2 * g] = TG[g].re;
+                 t[3 + 2 * g] = TG[g].im;
+               }
+             }
+             ++nvec;
+           });
+  // intramolecular exclusion, ewald.cpp:1164-1219
+  auto exclusion = [&](const oatom* atoms, int count, double sign)
+  {
+    for (int i = 0; i < count; ++i)
+      for (int j = i + 1; j < count; ++j)
+      {
+        if (atoms[i].molecule_id != atoms[j].molecule_id) continue;
+        double dr[3] = {atoms[i].x - atoms[j].x, atoms[i].y - atoms[j].y, atoms[i].z - atoms[j].z};
+        pbc(b, dr);
+        double r = std::sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+        double sA = atoms[i].scaling_coulomb, sB = atoms[j].scaling_coulomb;
+        double pot, dudl;
+        exclusionFactors(alpha, sA * sB, r, pot, dudl);
+        double prefactor = C * atoms[i].charge * atoms[j].charge;
+        e->ewald_exclusion += sign * sA * sB * prefactor * pot;
+        addDud(e->dudlambda_ewald, groupOf(atoms[i]), groupOf(atoms[j]), sA, sB, sign * prefactor * dudl);
+      }
+  };
+  exclusion(old_atoms, n_old, 1.0);
+  exclusion(new_atoms, n_new, -1.0);
+  // self energy, ewald.cpp:1221-1238
+  double prefactor_self = C * ff->ewald_alpha / std::sqrt(kPi);
+  for (int i = 0; i < n_old; ++i)
+  {
+    double q = old_atoms[i].charge, sc = old_atoms[i].scaling_coulomb;
+    int g = groupOf(old_atoms[i]);
+    e->ewald_self += prefactor_self * sc * q * sc * q;
+    if (g != 0) e->dudlambda_ewald[g - 1] += 2.0 * prefactor_self * sc * q * q;
+  }
+  for (int i = 0; i < n_new; ++i)
+  {
+    double q = new_atoms[i].charge, sc = new_atoms[i].scaling_coulomb;
+    int g = groupOf(new_atoms[i]);
+    e->ewald_self -= prefactor_self * sc * q * sc * q;
+    if (g != 0) e->dudlambda_ewald[g - 1] -= 2.0 * prefactor_self * sc * q * q;
+  }
+  // net-charge correction difference, ewald.cpp:181-208
+  double deltaCharge = 0.0;
+  double dNew[4], dOld[4];
+  for (int g = 0; g < 4; ++g) dNew[g] = dOld[g] = net_charge_derivative_ext ? net_charge_derivative_ext[g] : 0.0;
+  for (int i = 0; i < n_old; ++i)
+  {
+    deltaCharge -= old_atoms[i].scaling_coulomb * old_atoms[i].charge;
+    int g = groupOf(old_atoms[i]);
+    if (g != 0) dOld[g - 1] += old_atoms[i].charge;
+  }
+  for (int i = 0; i < n_new; ++i)
+  {
+    deltaCharge += new_atoms[i].scaling_coulomb * new_atoms[i].charge;
+    int g = groupOf(new_atoms[i]);
+    if (g != 0) dNew[g - 1] += new_atoms[i].charge;
+  }
+  double uIon = -(singleIonFourierSum - C * alpha / std::sqrt(kPi));
+  double netChargeNew = net_charge + deltaCharge;
+  e->ewald_fourier += uIon * (netChargeNew * netChargeNew - net_charge * net_charge);
+  for (int g = 0; g < 4; ++g)
+    e->dudlambda_ewald[g] += 2.0 * uIon * (netChargeNew * dNew[g] - net_charge * dOld[g]);
+}
+
+double oracle_ewald_single_ion(const off* ff, const obox* box, const double* pos, double charge)
+{
+  // computeEwaldFourierEnergySingleIon, ewald.cpp:210-274
+  Box b = makeBox(box);
+  const double alpha = ff->ewald_alpha;
+  const double alpha_squared = alpha * alpha;
+  oatom a{};
+  a.x = pos[0];
+  a.y = pos[1];
+  a.z = pos[2];
+  std::vector<const oatom*> ptr{&a};
+  EikTables eik(b, ptr, ff->kmax_x, ff->kmax_y, ff->kmax_z);
+  double energy_sum = 0.0;
+  forEachK(ff, b,
+           [&](int kx, int ky, int kz, double rksq, double)
+           {
+             double factor = (kx == 0) ? 1.0 : 2.0;
+             Cplx e = cmul(eik.xy(0, kx, ky), eik.zf(0, kz));
+             Cplx ck{charge * e.re, charge * e.im};
+             energy_sum += factor * norm2(ck) * std::exp((-0.25 / alpha_squared) * rksq) / rksq;
+           });
+  return -coulombFactor() * ((2.0 * kPi / b.volume) * energy_sum - alpha / std::sqrt(kPi));
+}
+
+int oracle_select_trial(const double* log_boltzmann, int n, double uniform)
+{
+  // CBMC::selectTrialPosition, cbmc/util.cpp:14-47
+  double largest = log_boltzmann[0];
+  for (int i = 1; i < n; ++i) largest = std::max(largest, log_boltzmann[i]);
+  std::vector<double> shifted(n);
+  double sum = 0.0;
+  for (int i = 0; i < n; ++i)
+  {
+    shifted[i] = std::exp(log_boltzmann[i] - largest);
+    sum += shifted[i];
+  }
+  int selected = 0;
+  double cumw = shifted[0];
+  double ws = uniform * sum;
+  while (selected + 1 < n && cumw < ws) cumw += shifted[++selected];
+  return selected;
+}
+}

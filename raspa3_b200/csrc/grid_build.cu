@@ -1,0 +1,630 @@
+// (a) Rigid-framework interpolation-grid build on sm_100a.
+//
+// Replaces InterpolationEnergyGrid::makeFrameworkInterpolationGrid (src/raspakit/interpolation_energy_grid.cpp:
+// 3800-3978) and the per-point sums of Interactions::calculateTricubicFractionalAtPosition
+// (src/raspakit/interactions/framework_molecule_grid.cpp:168-282).
+//
+// Algorithm. The reference sums, for every grid point, over all atoms of a supercell of ceil(2 rc / width) unit
+// cells with the minimum image in that supercell. Because the supercell is at least 2 rc wide, exactly one image of
+// every lattice-translate class lies within rc, so that sum equals the sum over ALL periodic images of the unit-cell
+// atoms with r < rc. We enumerate those images once on the host (only atoms with a nonzero parameter: eps != 0 for
+// Lennard-Jones grids, q != 0 for the Ewald grid), then every CTA owns a brick of BX*BY*BZ grid points (one point per
+// thread) and compacts, chunk by chunk and in image order, the images within rc + R of its brick centre (R = brick
+// half-diagonal) into shared memory. All threads then stream the staged candidates (shared-memory broadcast reads)
+// and accumulate energy and the seven derivative channels. Edge semantics kept from the reference: rr = max(0.1, rr),
+// the strict rr < rc^2 test, fractional scaling by the cell and division by the cell counts, and the overlap clamp.
+//
+// Precisions: FP64 throughout; or FP32C — coordinates relative to the brick centre (formed in FP64, rounded once),
+// FP32 pair terms, FP32 partial sums per staged chunk folded into a compensated (TwoSum) hi/lo FP32 pair, and an
+// FP64 epilogue.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace
+{
+constexpr int kPer = 2;  // images tested per thread per chunk
+
+struct GridParams
+{
+  double cell[3][3];  // c[col][row]
+  double delta[3];
+  double ncells[3];
+  int nx, ny, nz;
+  int n_images;
+  double rc2;
+  double filter2;
+  double alpha;
+  double coul;
+  double overlap;
+  unsigned long long* pair_count;
+  double* out;
+};
+
+__device__ __forceinline__ double rcpRn(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcpRn(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double sqrtT(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqrtT(float x) { return sqrtf(x); }
+__device__ __forceinline__ double erfcT(double x) { return erfc(x); }
+__device__ __forceinline__ float erfcT(float x) { return erfcf(x); }
+__device__ __forceinline__ double expT(double x) { return exp(x); }
+__device__ __forceinline__ float expT(float x) { return expf(x); }
+
+template <typename Real>
+struct Factor
+{
+  Real e, f1, f2, f3;
+};
+
+// potentialLennardJonesTricubicDerivative and its repulsion/attraction variants
+// (src/raspakit/potentials/interpolation/tricubic_derivative_lj.ixx:33-78), written with one reciprocal.
+template <int TYPE, typename Real>
+__device__ __forceinline__ Factor<Real> ljFactor(Real rr, Real a1, Real s2, Real shift)
+{
+  Real inv = rcpRn(rr);
+  Real q = s2 * inv;
+  Real t3 = q * q * q;
+  Real t6 = t3 * t3;
+  Real inv2 = inv * inv;
+  Real inv3 = inv2 * inv;
+  Factor<Real> f;
+  if constexpr (TYPE == RG_GRID_LENNARD_JONES_REPULSION)
+  {
+    f.e = a1 * t6;
+    f.f1 = Real(-12) * a1 * t6 * inv;
+    f.f2 = Real(168) * a1 * t6 * inv2;
+    f.f3 = Real(-2688) * a1 * t6 * inv3;
+  }
+  else if constexpr (TYPE == RG_GRID_LENNARD_JONES_ATTRACTION)
+  {
+    f.e = a1 * t3;
+    f.f1 = Real(-6) * a1 * t3 * inv;
+    f.f2 = Real(48) * a1 * t3 * inv2;
+    f.f3 = Real(-480) * a1 * t3 * inv3;
+  }
+  else
+  {
+    f.e = a1 * (t6 - t3) - shift;
+    f.f1 = Real(-6) * a1 * (Real(2) * t6 - t3) * inv;
+    f.f2 = Real(24) * a1 * (Real(7) * t6 - Real(2) * t3) * inv2;
+    f.f3 = Real(-96) * a1 * (Real(28) * t6 - Real(5) * t3) * inv3;
+  }
+  return f;
+}
+
+// potentialRealEwaldTricubicDerivative with q_A = 1 (src/raspakit/potentials/interpolation/
+// tricubic_derivative_real_ewald.ixx:32-56); cq = CoulombicConversionFactor * q_B.
+template <typename Real>
+__device__ __forceinline__ Factor<Real> ewaldFactor(Real rr, Real cq, Real alpha)
+{
+  Real r = sqrtT(rr);
+  Real ec = erfcT(alpha * r);
+  Real ex = expT(-alpha * alpha * rr);
+  Real etr = Real(2) * alpha * r * ex * Real(0.564189583547756286948079451560772586);
+  Real ar2 = alpha * alpha * rr;
+  Real invr = rcpRn(r);
+  Real invrr = invr * invr;
+  Real i3 = invr * invrr;
+  Real i5 = i3 * invrr;
+  Real i7 = i5 * invrr;
+  Factor<Real> f;
+  f.e = cq * ec * invr;
+  f.f1 = -cq * (etr + ec) * i3;
+  f.f2 = cq * (etr * (Real(2) * ar2 + Real(3)) + Real(3) * ec) * i5;
+  f.f3 = -cq * (etr * (Real(4) * ar2 * ar2 + Real(10) * ar2 + Real(15)) + Real(15) * ec) * i7;
+  return f;
+}
+
+// Accumulators: FP64 plain sums, or FP32 chunk partials folded into a TwoSum-compensated hi/lo pair.
+template <int N>
+struct AccF64
+{
+  double v[N];
+  __device__ void init()
+  {
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = 0.0;
+  }
+  __device__ __forceinline__ void add(int i, double x) { v[i] += x; }
+  __device__ __forceinline__ void flush() {}
+  __device__ __forceinline__ double get(int i) const { return v[i]; }
+};
+
+template <int N>
+struct AccF32C
+{
+  float p[N], hi[N], lo[N];
+  __device__ void init()
+  {
+#pragma unroll
+    for (int i = 0; i < N; ++i) p[i] = hi[i] = lo[i] = 0.0f;
+  }
+  __device__ __forceinline__ void add(int i, float x) { p[i] += x; }
+  __device__ __forceinline__ void flush()
+  {
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+    {
+      // Knuth TwoSum of hi + p (exact error term), error carried in lo
+      float s = __fadd_rn(hi[i], p[i]);
+      float bp = __fsub_rn(s, hi[i]);
+      float err = __fadd_rn(__fsub_rn(hi[i], __fsub_rn(s, bp)), __fsub_rn(p[i], bp));
+      hi[i] = s;
+      lo[i] = __fadd_rn(lo[i], err);
+      p[i] = 0.0f;
+    }
+  }
+  __device__ __forceinline__ double get(int i) const { return static_cast<double>(hi[i]) + static_cast<double>(lo[i]); }
+};
+
+template <typename Real>
+struct Vec4;
+template <>
+struct Vec4<double>
+{
+  using T = double4;
+};
+template <>
+struct Vec4<float>
+{
+  using T = float4;
+};
+
+template <typename Real, int N>
+struct AccOf;
+template <int N>
+struct AccOf<double, N>
+{
+  using T = AccF64<N>;
+};
+template <int N>
+struct AccOf<float, N>
+{
+  using T = AccF32C<N>;
+};
+
+// Index of the symmetric 3-tensor component (i<=j<=k) in the 10-slot layout xxx,xxy,xxz,xyy,xyz,xzz,yyy,yyz,yzz,zzz.
+__device__ __forceinline__ int sym3(int i, int j, int k)
+{
+  // sort
+  int a = min(i, min(j, k)), c = max(i, max(j, k)), b = i + j + k - a - c;
+  const int table[27] = {0, 1, 2, 0, 3, 4, 0, 0, 5, 0, 0, 0, 0, 6, 7, 0, 0, 8, 0, 0, 0, 0, 0, 0, 0, 0, 9};
+  return table[a * 9 + b * 3 + c];
+}
+__device__ __forceinline__ int sym2(int i, int j)
+{
+  int a = min(i, j), b = max(i, j);
+  const int table[9] = {0, 1, 2, 0, 3, 4, 0, 0, 5};
+  return table[a * 3 + b];
+}
+
+template <typename Real, int TYPE, bool TRICLINIC, bool COUNT>
+__global__ void __launch_bounds__(256) gridKernel(GridParams p, const double4* __restrict__ ipos,
+                                                  const double4* __restrict__ ipar, int bx, int by, int bz)
+{
+  using V4 = typename Vec4<Real>::T;
+  constexpr bool EWALD = (TYPE == RG_GRID_EWALD_REAL);
+  constexpr int NCH = TRICLINIC ? 20 : 8;
+  extern __shared__ unsigned char smem_raw[];
+  const int nt = blockDim.x;
+  const int chunk = nt * kPer;
+  V4* cpos = reinterpret_cast<V4*>(smem_raw);
+  V4* cpar = cpos + chunk;
+  __shared__ int warp_sums[33];
+
+  const int tid = threadIdx.x;
+  const int lx = tid % bx, ly = (tid / bx) % by, lz = tid / (bx * by);
+  const int i = blockIdx.x * bx + lx, j = blockIdx.y * by + ly, k = blockIdx.z * bz + lz;
+  const bool valid = (i < p.nx) && (j < p.ny) && (k < p.nz) && (lz < bz);
+
+  // grid point (interpolation_energy_grid.cpp:3827-3829): s = (i,j,k)*delta, pos = cell * s
+  double s[3] = {static_cast<double>(i) * p.delta[0], static_cast<double>(j) * p.delta[1],
+                 static_cast<double>(k) * p.delta[2]};
+  double pos[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) pos[r] = p.cell[0][r] * s[0] + p.cell[1][r] * s[1] + p.cell[2][r] * s[2];
+  // brick centre
+  double sc[3] = {(blockIdx.x * bx + 0.5 * (bx - 1)) * p.delta[0], (blockIdx.y * by + 0.5 * (by - 1)) * p.delta[1],
+                  (blockIdx.z * bz + 0.5 * (bz - 1)) * p.delta[2]};
+  double ctr[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) ctr[r] = p.cell[0][r] * sc[0] + p.cell[1][r] * sc[1] + p.cell[2][r] * sc[2];
+  // the point relative to the brick centre, in the working precision
+  const Real px = static_cast<Real>(pos[0] - ctr[0]);
+  const Real py = static_cast<Real>(pos[1] - ctr[1]);
+  const Real pz = static_cast<Real>(pos[2] - ctr[2]);
+  const Real rc2 = static_cast<Real>(p.rc2);
+  const Real alpha = static_cast<Real>(p.alpha);
+
+  typename AccOf<Real, NCH>::T acc;
+  acc.init();
+  unsigned long long npairs = 0;
+
+  for (int base = 0; base < p.n_images; base += chunk)
+  {
+    // stage: each thread tests kPer consecutive images; a block scan keeps image order (deterministic sums)
+    double4 ip[kPer];
+    bool ok[kPer];
+    int cnt = 0;
+#pragma unroll
+    for (int r = 0; r < kPer; ++r)
+    {
+      int idx = base + tid * kPer + r;
+      ok[r] = false;
+      if (idx < p.n_images)
+      {
+        ip[r] = ipos[idx];
+        double dx = ip[r].x - ctr[0], dy = ip[r].y - ctr[1], dz = ip[r].z - ctr[2];
+        ok[r] = (dx * dx + dy * dy + dz * dz) < p.filter2;
+        cnt += ok[r] ? 1 : 0;
+      }
+    }
+    int total;
+    int off = blockExclusiveScan(cnt, warp_sums, &total);
+#pragma unroll
+    for (int r = 0; r < kPer; ++r)
+    {
+      if (ok[r])
+      {
+        int idx = base + tid * kPer + r;
+        V4 c;
+        c.x = static_cast<Real>(ip[r].x - ctr[0]);
+        c.y = static_cast<Real>(ip[r].y - ctr[1]);
+        c.z = static_cast<Real>(ip[r].z - ctr[2]);
+        c.w = static_cast<Real>(ip[r].w);
+        cpos[off] = c;
+        if (!EWALD)
+        {
+          double4 q = ipar[idx];
+          V4 pr;
+          pr.x = static_cast<Real>(q.x);
+          pr.y = static_cast<Real>(q.y);
+          pr.z = static_cast<Real>(q.z);
+          pr.w = Real(0);
+          cpar[off] = pr;
+        }
+        ++off;
+      }
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int c = 0; c < total; ++c)
+    {
+      V4 a = cpos[c];
+      Real dx = px - a.x, dy = py - a.y, dz = pz - a.z;
+      Real rr = dx * dx + dy * dy + dz * dz;
+      rr = rr > Real(0.1) ? rr : Real(0.1);
+      if (rr < rc2)
+      {
+        Factor<Real> f;
+        if constexpr (EWALD)
+          f = ewaldFactor<Real>(rr, a.w, alpha);
+        else
+        {
+          V4 q = cpar[c];
+          f = ljFactor<TYPE, Real>(rr, q.x, q.y, q.z);
+        }
+        if (COUNT && valid) ++npairs;
+        acc.add(0, f.e);
+        if constexpr (!TRICLINIC)
+        {
+          acc.add(1, dx * f.f1);
+          acc.add(2, dy * f.f1);
+          acc.add(3, dz * f.f1);
+          acc.add(4, f.f2 * dx * dy);
+          acc.add(5, f.f2 * dx * dz);
+          acc.add(6, f.f2 * dy * dz);
+          acc.add(7, f.f3 * dx * dy * dz);
+        }
+        else
+        {
+          // full Cartesian tensors (framework_molecule_grid.cpp:76-144), symmetric storage
+          const Real d[3] = {dx, dy, dz};
+          acc.add(1, dx * f.f1);
+          acc.add(2, dy * f.f1);
+          acc.add(3, dz * f.f1);
+#pragma unroll
+          for (int u = 0; u < 3; ++u)
+#pragma unroll
+            for (int v = u; v < 3; ++v) acc.add(4 + sym2(u, v), f.f2 * d[u] * d[v] + (u == v ? f.f1 : Real(0)));
+#pragma unroll
+          for (int u = 0; u < 3; ++u)
+#pragma unroll
+            for (int v = u; v < 3; ++v)
+#pragma unroll
+              for (int w = v; w < 3; ++w)
+                acc.add(10 + sym3(u, v, w), f.f3 * d[u] * d[v] * d[w] + (v == w ? f.f2 * d[u] : Real(0)) +
+                                                (u == w ? f.f2 * d[v] : Real(0)) + (u == v ? f.f2 * d[w] : Real(0)));
+        }
+      }
+    }
+    acc.flush();
+    __syncthreads();
+  }
+
+  if (COUNT)
+  {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) npairs += __shfl_down_sync(0xffffffffu, npairs, o);
+    if ((tid & 31) == 0 && npairs) atomicAdd(p.pair_count, npairs);
+  }
+  if (!valid) return;
+
+  double v[8];
+  v[0] = acc.get(0);
+  if constexpr (!TRICLINIC)
+  {
+    // rectangular scaling by the cell diagonal (framework_molecule_grid.cpp:236-243)
+    const double cx = p.cell[0][0], cy = p.cell[1][1], cz = p.cell[2][2];
+    v[1] = acc.get(1) * cx;
+    v[2] = acc.get(2) * cy;
+    v[3] = acc.get(3) * cz;
+    v[4] = acc.get(4) * cx * cy;
+    v[5] = acc.get(5) * cx * cz;
+    v[6] = acc.get(6) * cy * cz;
+    v[7] = acc.get(7) * cx * cy * cz;
+  }
+  else
+  {
+    // contraction with the cell vectors (framework_molecule_grid.cpp:244-279)
+    double g[3] = {acc.get(1), acc.get(2), acc.get(3)};
+    double f0 = 0, f1 = 0, f2 = 0, s01 = 0, s02 = 0, s12 = 0, t012 = 0;
+    for (int a = 0; a < 3; ++a)
+    {
+      f0 += p.cell[0][a] * g[a];
+      f1 += p.cell[1][a] * g[a];
+      f2 += p.cell[2][a] * g[a];
+      for (int b = 0; b < 3; ++b)
+      {
+        double h = acc.get(4 + sym2(a, b));
+        s01 += p.cell[0][a] * p.cell[1][b] * h;
+        s02 += p.cell[0][a] * p.cell[2][b] * h;
+        s12 += p.cell[1][a] * p.cell[2][b] * h;
+        for (int c = 0; c < 3; ++c) t012 += p.cell[0][a] * p.cell[1][b] * p.cell[2][c] * acc.get(10 + sym3(a, b, c));
+      }
+    }
+    v[1] = f0;
+    v[2] = f1;
+    v[3] = f2;
+    v[4] = s01;
+    v[5] = s02;
+    v[6] = s12;
+    v[7] = t012;
+  }
+  // division by the cell counts and the overlap clamp (interpolation_energy_grid.cpp:3847-3874)
+  v[1] /= p.ncells[0];
+  v[2] /= p.ncells[1];
+  v[3] /= p.ncells[2];
+  v[4] /= p.ncells[0] * p.ncells[1];
+  v[5] /= p.ncells[0] * p.ncells[2];
+  v[6] /= p.ncells[1] * p.ncells[2];
+  v[7] /= p.ncells[0] * p.ncells[1] * p.ncells[2];
+  const double oc = p.overlap;
+  if (v[0] > oc)
+  {
+    v[0] = 2.0 * oc;
+    v[1] = fmin(fmax(v[1], -oc), oc);
+    v[2] = fmin(fmax(v[2], -oc), oc);
+    v[3] = fmin(fmax(v[3], -oc), oc);
+    v[4] = v[5] = v[6] = v[7] = 0.0;
+  }
+  double2* dst = reinterpret_cast<double2*>(p.out + 8 * (static_cast<long long>(i) +
+                                                         static_cast<long long>(p.nx) *
+                                                             (static_cast<long long>(j) + static_cast<long long>(p.ny) * k)));
+  dst[0] = make_double2(v[0], v[1]);
+  dst[1] = make_double2(v[2], v[3]);
+  dst[2] = make_double2(v[4], v[5]);
+  dst[3] = make_double2(v[6], v[7]);
+}
+
+template <typename Real, int TYPE, bool TRI>
+cudaError_t launchTyped(const GridParams& p, const double4* ipos, const double4* ipar, int bx, int by, int bz,
+                        bool count, cudaStream_t stream)
+{
+  dim3 grid((p.nx + bx - 1) / bx, (p.ny + by - 1) / by, (p.nz + bz - 1) / bz);
+  int nt = bx * by * bz;
+  size_t shmem = 2 * sizeof(typename Vec4<Real>::T) * static_cast<size_t>(nt) * kPer;
+  if (count)
+  {
+    auto kern = gridKernel<Real, TYPE, TRI, true>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shmem));
+    kern<<<grid, nt, shmem, stream>>>(p, ipos, ipar, bx, by, bz);
+  }
+  else
+  {
+    auto kern = gridKernel<Real, TYPE, TRI, false>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shmem));
+    kern<<<grid, nt, shmem, stream>>>(p, ipos, ipar, bx, by, bz);
+  }
+  return cudaGetLastError();
+}
+
+template <typename Real, bool TRI>
+cudaError_t launchPrec(int type, const GridParams& p, const double4* ipos, const double4* ipar, int bx, int by, int bz,
+                       bool count, cudaStream_t stream)
+{
+  switch (type)
+  {
+    case RG_GRID_LENNARD_JONES:
+      return launchTyped<Real, RG_GRID_LENNARD_JONES, TRI>(p, ipos, ipar, bx, by, bz, count, stream);
+    case RG_GRID_EWALD_REAL:
+      return launchTyped<Real, RG_GRID_EWALD_REAL, TRI>(p, ipos, ipar, bx, by, bz, count, stream);
+    case RG_GRID_LENNARD_JONES_REPULSION:
+      return launchTyped<Real, RG_GRID_LENNARD_JONES_REPULSION, TRI>(p, ipos, ipar, bx, by, bz, count, stream);
+    default:
+      return launchTyped<Real, RG_GRID_LENNARD_JONES_ATTRACTION, TRI>(p, ipos, ipar, bx, by, bz, count, stream);
+  }
+}
+}  // namespace
+
+namespace rg
+{
+// Periodic images of the unit-cell atoms that can lie within rc of some point of the closed unit cell.
+// pos.w carries C*q for the Ewald grid; par = (4 eps, sigma^2, shift) for Lennard-Jones grids.
+int buildGridImages(int grid_type, const rg_forcefield* ff, const HostBox& box, const rg_atom* atoms, int n,
+                    int probe_type, std::vector<double4>& pos, std::vector<double4>& par)
+{
+  double w[3];
+  perpendicularWidths(box, w);
+  const double rc = ff->cutoff_framework_vdw;
+  const double C = coulombFactor();
+  pos.clear();
+  par.clear();
+  for (int a = 0; a < n; ++a)
+  {
+    const rg_atom& at = atoms[a];
+    double4 pr = make_double4(0, 0, 0, 0);
+    double wq = 0.0;
+    if (grid_type == RG_GRID_EWALD_REAL)
+    {
+      if (at.charge == 0.0) continue;
+      wq = C * at.charge;
+    }
+    else
+    {
+      int idx = probe_type * ff->n_types + at.type;
+      double eps = ff->epsilon[idx];
+      if (eps == 0.0) continue;
+      pr = make_double4(4.0 * eps, ff->sigma[idx] * ff->sigma[idx], ff->shift[idx], 0.0);
+    }
+    double r[3] = {at.x, at.y, at.z}, s[3];
+    matvec(box.ic, r, s);
+    int lo[3], hi[3];
+    for (int d = 0; d < 3; ++d)
+    {
+      double f = rc / w[d] + 1e-9;
+      lo[d] = static_cast<int>(std::ceil(-s[d] - f));
+      hi[d] = static_cast<int>(std::floor(1.0 - s[d] + f));
+    }
+    for (int mx = lo[0]; mx <= hi[0]; ++mx)
+      for (int my = lo[1]; my <= hi[1]; ++my)
+        for (int mz = lo[2]; mz <= hi[2]; ++mz)
+        {
+          double m[3] = {static_cast<double>(mx), static_cast<double>(my), static_cast<double>(mz)}, d[3];
+          matvec(box.c, m, d);
+          pos.push_back(make_double4(r[0] + d[0], r[1] + d[1], r[2] + d[2], wq));
+          par.push_back(pr);
+        }
+  }
+  return static_cast<int>(pos.size());
+}
+}  // namespace rg
+
+extern "C" rg_status rg_grid_build(rg_ctx* ctx, int grid_type, const rg_forcefield* ff, const rg_box* unit_cell,
+                                   const rg_atom* unit_atoms, int n_unit_atoms, int probe_type, double cutoff, int nx,
+                                   int ny, int nz, int precision, double* out_device, double* out_host,
+                                   rg_grid_stats* stats)
+{
+  if (!ctx) return RG_ERR_INVALID_ARGUMENT;
+  if (!ff || !unit_cell || (n_unit_atoms > 0 && !unit_atoms) || n_unit_atoms < 0)
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build: null argument");
+  if (grid_type < 0 || grid_type > 3) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build: bad grid_type");
+  if (precision != RG_PRECISION_FP64 && precision != RG_PRECISION_FP32C)
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build: bad precision");
+  if (nx < 2 || ny < 2 || nz < 2) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build: need >= 2 points per axis");
+  if (grid_type != RG_GRID_EWALD_REAL && (probe_type < 0 || probe_type >= ff->n_types))
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build: probe_type out of range");
+  if (!out_device && !out_host) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build: no output");
+  (void)cutoff;  // the supercell size only selects which images the reference visits; all images within rc are used
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+
+  rg::HostBox box = rg::makeHostBox(unit_cell);
+  std::vector<double4> hpos, hpar;
+  int n_images = rg::buildGridImages(grid_type, ff, box, unit_atoms, n_unit_atoms, probe_type, hpos, hpar);
+
+  const size_t npts = static_cast<size_t>(nx) * ny * nz;
+  const size_t out_bytes = npts * 8 * sizeof(double);
+  double* dout = out_device;
+  void* p = nullptr;
+  if (!dout)
+  {
+    rg_status st = rg::scratch(ctx, 0, out_bytes, &p);
+    if (st) return st;
+    dout = static_cast<double*>(p);
+  }
+  // images + pair counter in scratch slot 1
+  size_t img_bytes = 2 * sizeof(double4) * static_cast<size_t>(n_images > 0 ? n_images : 1);
+  rg_status st = rg::scratch(ctx, 1, img_bytes + 64, &p);
+  if (st) return st;
+  double4* dpos = static_cast<double4*>(p);
+  double4* dpar = dpos + (n_images > 0 ? n_images : 1);
+  unsigned long long* dcount = reinterpret_cast<unsigned long long*>(dpar + (n_images > 0 ? n_images : 1));
+  if (n_images > 0)
+  {
+    // stage through pinned memory so the upload is asynchronous on the context stream; the staging slot is reused by
+    // the next call only after this stream has passed the copy
+    void* hp = nullptr;
+    RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    st = rg::pinnedScratch(ctx, 0, 2 * sizeof(double4) * n_images, &hp);
+    if (st) return st;
+    double4* stage = static_cast<double4*>(hp);
+    std::memcpy(stage, hpos.data(), sizeof(double4) * n_images);
+    std::memcpy(stage + n_images, hpar.data(), sizeof(double4) * n_images);
+    RG_CUDA(ctx, cudaMemcpyAsync(dpos, stage, 2 * sizeof(double4) * n_images, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  RG_CUDA(ctx, cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), ctx->stream));
+
+  // brick shape and its half-diagonal
+  const int bx = 8, by = 8, bz = 4;
+  GridParams gp{};
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) gp.cell[c][r] = box.c[c][r];
+  gp.ncells[0] = static_cast<double>(nx - 1);
+  gp.ncells[1] = static_cast<double>(ny - 1);
+  gp.ncells[2] = static_cast<double>(nz - 1);
+  gp.delta[0] = 1.0 / gp.ncells[0];
+  gp.delta[1] = 1.0 / gp.ncells[1];
+  gp.delta[2] = 1.0 / gp.ncells[2];
+  gp.nx = nx;
+  gp.ny = ny;
+  gp.nz = nz;
+  gp.n_images = n_images;
+  gp.rc2 = ff->cutoff_framework_vdw * ff->cutoff_framework_vdw;
+  double R = 0.0;
+  for (int sx = -1; sx <= 1; sx += 2)
+    for (int sy = -1; sy <= 1; sy += 2)
+      for (int sz = -1; sz <= 1; sz += 2)
+      {
+        double f[3] = {sx * 0.5 * (bx - 1) * gp.delta[0], sy * 0.5 * (by - 1) * gp.delta[1],
+                       sz * 0.5 * (bz - 1) * gp.delta[2]},
+               d[3];
+        rg::matvec(box.c, f, d);
+        R = std::fmax(R, std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
+      }
+  double rf = ff->cutoff_framework_vdw + R + 1e-6;
+  gp.filter2 = rf * rf;
+  gp.alpha = ff->ewald_alpha;
+  gp.coul = rg::coulombFactor();
+  gp.overlap = ff->overlap_criteria;
+  gp.pair_count = dcount;
+  gp.out = dout;
+
+  cudaError_t err;
+  const bool count = stats != nullptr;
+  if (precision == RG_PRECISION_FP64)
+    err = box.triclinic ? launchPrec<double, true>(grid_type, gp, dpos, dpar, bx, by, bz, count, ctx->stream)
+                        : launchPrec<double, false>(grid_type, gp, dpos, dpar, bx, by, bz, count, ctx->stream);
+  else
+    err = box.triclinic ? launchPrec<float, true>(grid_type, gp, dpos, dpar, bx, by, bz, count, ctx->stream)
+                        : launchPrec<float, false>(grid_type, gp, dpos, dpar, bx, by, bz, count, ctx->stream);
+  if (err != cudaSuccess) return rg::cudaFail(ctx, err, "gridKernel launch");
+
+  if (out_host) RG_CUDA(ctx, cudaMemcpyAsync(out_host, dout, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (stats)
+  {
+    unsigned long long c = 0;
+    RG_CUDA(ctx, cudaMemcpyAsync(&c, dcount, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+    RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    stats->pair_count = static_cast<int64_t>(c);
+    stats->n_images = n_images;
+    stats->h2d_bytes = static_cast<int64_t>(2 * sizeof(double4)) * n_images;
+    stats->d2h_bytes = out_host ? static_cast<int64_t>(out_bytes) : 0;
+  }
+  else if (out_host)
+  {
+    RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return RG_OK;
+}

@@ -1,0 +1,137 @@
+"""(a) Grid build on the GPU through the C-ABI vs the FP64 oracle (the reference's grid loop restated)."""
+
+import numpy as np
+import pytest
+
+from raspa3_b200 import native
+from raspa3_b200.forcefield import KELVIN_TO_ENERGY, make_atoms
+from raspa3_b200.synthetic import (config1_grid_dims, synthetic_forcefield, synthetic_framework)
+from reference_systems import itq29, zeolite_forcefield
+
+pytestmark = pytest.mark.gpu
+
+E_LIMIT = 1e4 * KELVIN_TO_ENERGY  # north-star tolerance applies where |E| < 1e4 K
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = native.Context(0)
+    yield c
+    c.close()
+
+
+def sample_points(dims, n, seed=7):
+    nx, ny, nz = dims
+    rng = np.random.default_rng(seed)
+    pts = set(rng.integers(0, nx * ny * nz, size=n).tolist())
+    # the duplicate periodic end-points and the corners
+    for i in (0, nx - 1):
+        for j in (0, ny - 1):
+            for k in (0, nz - 1):
+                pts.add(i + nx * (j + ny * k))
+    return np.array(sorted(pts), dtype=np.int64)
+
+
+def grid_errors(gpu, ref):
+    """Per-channel max error over points with |E| < 1e4 K: relative to max(|ref|, floor) with floor = 1e-2 * RMS of the
+    channel (derivative channels cancel to ~0 at symmetric points), and relative to max(|ref|, 1 K) for the energy."""
+    mask = np.abs(ref[:, 0]) < E_LIMIT
+    g, r = gpu[mask], ref[mask]
+    errs = []
+    for l in range(8):
+        floor = KELVIN_TO_ENERGY if l == 0 else 1e-2 * np.sqrt(np.mean(r[:, l] ** 2)) + 1e-300
+        errs.append(float(np.max(np.abs(g[:, l] - r[:, l]) / np.maximum(np.abs(r[:, l]), floor))))
+    return np.array(errs), int(mask.sum())
+
+
+def test_config1_lj_fp64_full_grid_vs_oracle_sample(ctx, oracle):
+    ff = synthetic_forcefield(charges=False)
+    cell, atoms = synthetic_framework(ff)
+    dims = config1_grid_dims(cell)
+    assert dims == (133, 133, 89)
+    probe = ff.index("CH4")
+    out, stats = ctx.grid_build(native.GRID_LENNARD_JONES, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP64,
+                                count_pairs=True)
+    pts = sample_points(dims, 1500)
+    ref = oracle.make_grid(0, ff, cell, atoms, probe, 12.0, dims, points=pts)
+    gpu = out.reshape(-1, 8)[pts]
+    errs, n = grid_errors(gpu, ref)
+    assert n > 100
+    assert np.all(errs < 1e-10), errs
+    assert stats["pair_count"] > 0 and stats["n_images"] > 0
+
+
+def test_config1_pair_count_small_grid(ctx, oracle):
+    ff = synthetic_forcefield(charges=False)
+    cell, atoms = synthetic_framework(ff)
+    dims = (21, 20, 14)
+    probe = ff.index("CH4")
+    _, stats = ctx.grid_build(0, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP64, count_pairs=True)
+    assert stats["pair_count"] == oracle.grid_pair_count(0, ff, cell, atoms, probe, 12.0, dims)
+
+
+@pytest.mark.parametrize("grid_type,probe_name", [(0, "C_co2"), (0, "O_co2"), (1, None)])
+def test_config2_fp32c_vs_oracle_sample(ctx, oracle, grid_type, probe_name):
+    ff = synthetic_forcefield(charges=True)
+    cell, atoms = synthetic_framework(ff)
+    dims = config1_grid_dims(cell)
+    probe = 0 if probe_name is None else ff.index(probe_name)
+    out, _ = ctx.grid_build(grid_type, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP32C)
+    pts = sample_points(dims, 1500, seed=11)
+    ref = oracle.make_grid(grid_type, ff, cell, atoms, probe, 12.0, dims, points=pts)
+    gpu = out.reshape(-1, 8)[pts]
+    errs, n = grid_errors(gpu, ref)
+    print("fp32c errors per channel", grid_type, probe_name, errs)
+    assert n > 100
+    assert np.all(errs < 1e-5), errs
+
+
+@pytest.mark.parametrize("precision,tol", [(native.PRECISION_FP64, 1e-10), (native.PRECISION_FP32C, 1e-5)])
+def test_itq29_small_full_grid(ctx, oracle, precision, tol):
+    """Known framework (zeolite force field: Si and O both Lennard-Jones), every point of a coarse grid."""
+    ff = zeolite_forcefield(12.0, True, use_charge=True)
+    cell, fw = itq29(ff)
+    dims = (24, 24, 24)
+    for grid_type, probe in ((0, ff.index("CH4")), (1, 0)):
+        out, _ = ctx.grid_build(grid_type, ff, cell, fw, probe, 12.0, dims, precision)
+        ref = oracle.make_grid(grid_type, ff, cell, fw, probe, 12.0, dims).reshape(-1, 8)
+        errs, _ = grid_errors(out.reshape(-1, 8), ref)
+        assert np.all(errs < tol), (grid_type, errs)
+        # overlap-clamped points reproduce the reference clamp exactly
+        clamp = ref[:, 0] == 2.0 * ff.overlap_criteria
+        np.testing.assert_array_equal(out.reshape(-1, 8)[clamp, 0], ref[clamp, 0])
+
+
+def test_triclinic_cell_fp64(ctx, oracle):
+    """Triclinic branch: Cartesian tensors contracted with the cell vectors (framework_molecule_grid.cpp:244-279)."""
+    ff = synthetic_forcefield(charges=True)
+    rng = np.random.default_rng(3)
+    cell = np.array([[14.0, 0.0, 0.0], [3.0, 13.0, 0.0], [2.0, 1.5, 12.5]])
+    frac = rng.random((60, 3))
+    pos = frac @ cell
+    types = np.where(np.arange(60) % 3 == 0, ff.index("T"), ff.index("O")).astype(np.uint16)
+    q = np.where(types == ff.index("T"), 2.05, -1.025)
+    atoms = make_atoms(pos, types, q)
+    dims = (12, 11, 10)
+    for grid_type, probe in ((0, ff.index("CH4")), (1, 0)):
+        out, _ = ctx.grid_build(grid_type, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP64)
+        ref = oracle.make_grid(grid_type, ff, cell, atoms, probe, 12.0, dims).reshape(-1, 8)
+        errs, _ = grid_errors(out.reshape(-1, 8), ref)
+        assert np.all(errs < 1e-9), (grid_type, errs)
+
+
+def test_empty_framework_and_minimum_grid(ctx):
+    ff = synthetic_forcefield(charges=False)
+    cell = np.diag([10.0, 10.0, 10.0])
+    empty = make_atoms(np.zeros((0, 3)), np.zeros(0, dtype=np.uint16), np.zeros(0))
+    out, _ = ctx.grid_build(0, ff, cell, empty, ff.index("CH4"), 12.0, (2, 2, 2))
+    assert out.shape == (64,) and np.all(out == 0.0)
+
+
+def test_invalid_arguments_raise(ctx):
+    ff = synthetic_forcefield(charges=False)
+    cell, atoms = synthetic_framework(ff)
+    with pytest.raises(native.RaspaGpuError):
+        ctx.grid_build(0, ff, cell, atoms, 99, 12.0, (10, 10, 10))
+    with pytest.raises(native.RaspaGpuError):
+        ctx.grid_build(0, ff, cell, atoms, 2, 12.0, (1, 10, 10))

@@ -44,7 +44,7 @@ L2_FLUSH_BYTES = 256 << 20
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -192,7 +192,9 @@ def run_ours(args):
     ff, cell, atoms, dims, grids = workload()
     npts = dims[0] * dims[1] * dims[2]
     ctx = native.Context(local)
-    stream = torch.cuda.current_stream()
+    # a created stream (not the legacy NULL stream) shared by the library and the timing events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     outs = [torch.empty(8 * npts, dtype=torch.float64, device="cuda") for _ in grids]
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")

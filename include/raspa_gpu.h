@@ -80,7 +80,8 @@ typedef struct rg_ctx rg_ctx;
 /* ---- context ---- */
 rg_status rg_ctx_create(int device, rg_ctx** out);
 rg_status rg_ctx_destroy(rg_ctx* ctx);
-/* Use the caller's CUDA stream (a cudaStream_t; NULL restores the context's own stream). */
+/* Use the caller's CUDA stream (a created cudaStream_t or cudaStreamPerThread; NULL restores the context's own
+ * non-blocking stream, so the legacy NULL stream itself cannot be selected). */
 rg_status rg_ctx_set_stream(rg_ctx* ctx, void* stream);
 void* rg_ctx_stream(rg_ctx* ctx);
 rg_status rg_ctx_synchronize(rg_ctx* ctx);
@@ -124,6 +125,49 @@ typedef struct rg_grid_stats
 rg_status rg_grid_build(rg_ctx* ctx, int grid_type, const rg_forcefield* ff, const rg_box* unit_cell,
                         const rg_atom* unit_atoms, int n_unit_atoms, int probe_type, double cutoff, int nx, int ny,
                         int nz, int precision, double* out_device, double* out_host, rg_grid_stats* stats);
+
+/* ---- (c) Ewald Fourier energy of a move ---- */
+typedef struct rg_ewald rg_ewald; /* device-resident k-vectors, prefactors and structure factors of one system */
+
+/* The Ewald part of RunningEnergy (src/raspakit/running_energy.ixx:500-540) in internal units. */
+typedef struct rg_ewald_energy
+{
+  double ewald_fourier;
+  double ewald_self;
+  double ewald_exclusion;
+  double dudlambda_ewald[4];
+} rg_ewald_energy;
+
+/* Builds the k-vector set of the box (kx in [0,kmax_x], ky, kz in [-kmax,kmax], k != 0, kx^2+ky^2+kz^2 <=
+ * ff->recip_int_cutoff_sq, |k|^2 < ff->recip_cutoff_sq; ewald.cpp:1098-1146) and zeroed structure factors with
+ * n_groups (0..4) dU/dlambda group sums. The state lives on ctx's device and stream. */
+rg_status rg_ewald_create(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* box, int n_groups, rg_ewald** out);
+rg_status rg_ewald_destroy(rg_ewald* ewald);
+/* Number of k-vectors and the single-ion Fourier sum sum_k temp(k) (ewald.cpp:1146). */
+rg_status rg_ewald_info(rg_ewald* ewald, int64_t* n_kvectors, double* single_ion_sum);
+/* Replaces Interactions::precomputeEwaldFourierRigid (src/raspakit/interactions/ewald.cpp:276-348): the rigid
+ * framework's structure factor, subtracted as a constant from every energy. */
+rg_status rg_ewald_set_framework(rg_ewald* ewald, const rg_atom* framework_atoms, int n_framework_atoms);
+/* Replaces Interactions::computeEwaldFourierEnergy (ewald.cpp:352-563): full recompute of the adsorbate structure
+ * factors (stored), Fourier energy minus the framework-framework part, self, exclusion and net-charge terms.
+ * molecule_sizes: atom counts of the consecutive molecules in atoms (for the intramolecular exclusion). Called at
+ * initialisation, for drift checks and for volume moves. */
+rg_status rg_ewald_full(rg_ewald* ewald, const rg_atom* atoms, int n_atoms, const int32_t* molecule_sizes,
+                        int n_molecules, double net_charge_framework, rg_ewald_energy* out);
+/* Replaces Interactions::energyDifferenceEwaldFourier (ewald.cpp:1043-1244), called from every charged move
+ * (e.g. mc_moves/component/translation.cpp, insertion_cbmc.cpp:99-101): the energy change of replacing old_atoms by
+ * new_atoms (at most 512 together), leaving the trial structure factors on the device. net_charge: system net charge
+ * before the move; net_charge_derivative_ext: 4 doubles or NULL (ewald.cpp:175-208). */
+rg_status rg_ewald_delta(rg_ewald* ewald, const rg_atom* new_atoms, int n_new, const rg_atom* old_atoms, int n_old,
+                         double net_charge, const double* net_charge_derivative_ext, rg_ewald_energy* out);
+/* Replaces Interactions::acceptEwaldMove (ewald.cpp:1565-1574): the trial structure factors become the stored ones
+ * (a pointer swap, no copy). */
+rg_status rg_ewald_accept(rg_ewald* ewald);
+/* Copies structure factors to the host, 2*(1+n_groups) doubles per k-vector in the reference's storedEik order
+ * (total, then group sums; re, im). which: 0 = stored, 1 = trial, 2 = framework (2 doubles per k). */
+rg_status rg_ewald_get_structure_factors(rg_ewald* ewald, int which, double* host, int64_t n_doubles);
+/* Overwrites the stored structure factors (e.g. from a restart file); n_doubles must equal 2*nk*(1+n_groups). */
+rg_status rg_ewald_set_structure_factors(rg_ewald* ewald, const double* host, int64_t n_doubles);
 
 /* ---- measurement ---- */
 /* FP32 (precision = RG_PRECISION_FP32C) or FP64 FMA throughput of this device in TFLOP/s, from independent FMA chains

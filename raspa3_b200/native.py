@@ -31,6 +31,15 @@ class RaspaGpuError(RuntimeError):
     pass
 
 
+class EwaldEnergy(ctypes.Structure):
+    _fields_ = [("ewald_fourier", ctypes.c_double), ("ewald_self", ctypes.c_double),
+                ("ewald_exclusion", ctypes.c_double), ("dudlambda_ewald", ctypes.c_double * 4)]
+
+    def as_dict(self):
+        return {"ewald_fourier": self.ewald_fourier, "ewald_self": self.ewald_self,
+                "ewald_exclusion": self.ewald_exclusion, "dudlambda_ewald": list(self.dudlambda_ewald)}
+
+
 class GridStats(ctypes.Structure):
     _fields_ = [("pair_count", ctypes.c_int64), ("n_images", ctypes.c_int64), ("h2d_bytes", ctypes.c_int64),
                 ("d2h_bytes", ctypes.c_int64)]
@@ -59,6 +68,15 @@ def lib():
         L.rg_grid_build.argtypes = [vp, i32, P(RgForceField), P(RgBox), vp, i32, i32, d, i32, i32, i32, i32, vp, vp,
                                     P(GridStats)]
         L.rg_probe_fma_peak.argtypes = [vp, i32, P(d), P(d)]
+        L.rg_ewald_create.argtypes = [vp, P(RgForceField), P(RgBox), i32, P(vp)]
+        L.rg_ewald_destroy.argtypes = [vp]
+        L.rg_ewald_info.argtypes = [vp, P(i64), P(d)]
+        L.rg_ewald_set_framework.argtypes = [vp, vp, i32]
+        L.rg_ewald_full.argtypes = [vp, vp, i32, vp, i32, d, P(EwaldEnergy)]
+        L.rg_ewald_delta.argtypes = [vp, vp, i32, vp, i32, d, vp, P(EwaldEnergy)]
+        L.rg_ewald_accept.argtypes = [vp]
+        L.rg_ewald_get_structure_factors.argtypes = [vp, i32, vp, i64]
+        L.rg_ewald_set_structure_factors.argtypes = [vp, vp, i64]
         _lib = L
     return _lib
 
@@ -125,3 +143,77 @@ class Context:
         check(self.handle, lib().rg_probe_fma_peak(self.handle, precision, ctypes.byref(t), ctypes.byref(s)),
               "rg_probe_fma_peak")
         return t.value
+
+
+def _atoms_ptr(a):
+    a = np.ascontiguousarray(a, dtype=ATOM_DTYPE)
+    return a, (ctypes.c_void_p(a.ctypes.data) if len(a) else None)
+
+
+class Ewald:
+    """Device-resident Ewald state of one system (k-vectors, prefactors, stored/trial structure factors)."""
+
+    def __init__(self, ctx: Context, ff: ForceField, cell, n_groups: int = 0):
+        self.ctx = ctx
+        self._ff = ff_struct(ff)
+        self._box = box_struct(cell)
+        h = ctypes.c_void_p()
+        check(ctx.handle, lib().rg_ewald_create(ctx.handle, ctypes.byref(self._ff), ctypes.byref(self._box), n_groups,
+                                                ctypes.byref(h)), "rg_ewald_create")
+        self.handle = h
+        self.n_groups = n_groups
+        nk, s = ctypes.c_int64(), ctypes.c_double()
+        check(ctx.handle, lib().rg_ewald_info(h, ctypes.byref(nk), ctypes.byref(s)), "rg_ewald_info")
+        self.n_kvectors = nk.value
+        self.single_ion_sum = s.value
+
+    def close(self):
+        if self.handle:
+            lib().rg_ewald_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_framework(self, fw_atoms):
+        a, p = _atoms_ptr(fw_atoms)
+        check(self.ctx.handle, lib().rg_ewald_set_framework(self.handle, p, len(a)), "rg_ewald_set_framework")
+
+    def full(self, atoms, molecule_sizes, net_charge_framework=0.0) -> dict:
+        a, p = _atoms_ptr(atoms)
+        ms = np.ascontiguousarray(molecule_sizes, dtype=np.int32)
+        e = EwaldEnergy()
+        check(self.ctx.handle, lib().rg_ewald_full(self.handle, p, len(a), ctypes.c_void_p(ms.ctypes.data) if len(ms)
+                                                   else None, len(ms), net_charge_framework, ctypes.byref(e)),
+              "rg_ewald_full")
+        return e.as_dict()
+
+    def delta(self, new_atoms, old_atoms, net_charge=0.0, net_charge_derivative_ext=None) -> dict:
+        na, pn = _atoms_ptr(new_atoms)
+        oa, po = _atoms_ptr(old_atoms)
+        nd = None
+        if net_charge_derivative_ext is not None:
+            nd = np.ascontiguousarray(net_charge_derivative_ext, dtype=np.float64)
+        e = EwaldEnergy()
+        check(self.ctx.handle, lib().rg_ewald_delta(self.handle, pn, len(na), po, len(oa), net_charge,
+                                                    None if nd is None else ctypes.c_void_p(nd.ctypes.data),
+                                                    ctypes.byref(e)), "rg_ewald_delta")
+        return e.as_dict()
+
+    def accept(self):
+        check(self.ctx.handle, lib().rg_ewald_accept(self.handle), "rg_ewald_accept")
+
+    def structure_factors(self, which: int = 0) -> np.ndarray:
+        n = 2 * self.n_kvectors * (1 + self.n_groups)
+        out = np.empty(n)
+        check(self.ctx.handle, lib().rg_ewald_get_structure_factors(self.handle, which, ctypes.c_void_p(out.ctypes.data),
+                                                                    n), "rg_ewald_get_structure_factors")
+        return out if which != 2 else out[: 2 * self.n_kvectors]
+
+    def set_structure_factors(self, s: np.ndarray):
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        check(self.ctx.handle, lib().rg_ewald_set_structure_factors(self.handle, ctypes.c_void_p(s.ctypes.data),
+                                                                    len(s)), "rg_ewald_set_structure_factors")

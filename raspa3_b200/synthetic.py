@@ -149,3 +149,34 @@ def random_rotation(rng) -> np.ndarray:
     return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
                      [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
                      [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+
+
+def rigid_molecule(ff: ForceField, names, offsets, center, rotation, molecule_id, lam: float = 1.0, group: int = 0,
+                   fractional: bool = False):
+    """Atoms of a rigid molecule: body-frame offsets rotated and translated to `center`."""
+    from .forcefield import lambda_scaling
+
+    offsets = np.asarray(offsets, dtype=np.float64)
+    pos = np.asarray(center, dtype=np.float64)[None, :] + offsets @ np.asarray(rotation).T
+    types = np.array([ff.index(n) for n in names], dtype=np.uint16)
+    charges = np.array([ff.pseudo_atoms[t].charge for t in types])
+    svdw, scoul = lambda_scaling(lam) if lam != 1.0 else (1.0, 1.0)
+    n = len(names)
+    return make_atoms(pos, types, charges, molecule_ids=np.full(n, molecule_id), scaling_vdw=svdw,
+                      scaling_coulomb=scoul, group_ids=np.full(n, group), fractional=np.full(n, 1 if fractional else 0))
+
+
+CO2_NAMES = ("O_co2", "C_co2", "O_co2")
+CO2_OFFSETS = ((0.0, 0.0, 1.16), (0.0, 0.0, 0.0), (0.0, 0.0, -1.16))
+N2_NAMES = ("N_n2", "N_com", "N_n2")
+N2_OFFSETS = ((0.0, 0.0, 0.55), (0.0, 0.0, 0.0), (0.0, 0.0, -0.55))
+
+
+def random_molecules(ff: ForceField, cell, n: int, names=CO2_NAMES, offsets=CO2_OFFSETS, seed: int = 0,
+                     first_id: int = 0):
+    """n rigid molecules at uniform random positions and orientations (no overlap test)."""
+    rng = np.random.default_rng(seed)
+    cell = np.asarray(cell, dtype=np.float64)
+    mols = [rigid_molecule(ff, names, offsets, rng.random(3) @ cell, random_rotation(rng), first_id + i)
+            for i in range(n)]
+    return np.concatenate(mols) if mols else make_atoms(np.zeros((0, 3)), np.zeros(0, np.uint16), np.zeros(0))

@@ -126,6 +126,20 @@ rg_status rg_grid_build(rg_ctx* ctx, int grid_type, const rg_forcefield* ff, con
                         const rg_atom* unit_atoms, int n_unit_atoms, int probe_type, double cutoff, int nx, int ny,
                         int nz, int precision, double* out_device, double* out_host, rg_grid_stats* stats);
 
+/* Grid build that allocates nothing, for callers that cannot allocate device memory: applications whose device memory
+ * is owned by another allocator (a host framework that reserves the whole device up front, or a memory pool with a hard
+ * budget) where any cudaMalloc by a library would fail or break the budget. No counterpart in the reference.
+ * Same arguments and result as rg_grid_build, minus the context: the caller passes the device, a stream (NULL = the
+ * legacy default stream) and the device output buffer; there is no host output. The working memory is one fixed
+ * file-scope device array that every GPU loading the library holds until exit; it holds at most 32768 periodic images
+ * of the unit-cell atoms (RG_ERR_INVALID_ARGUMENT beyond that). The first call on a device looks up the array's device
+ * address, so make that first call before any stream capture. All calls share the array: calls whose work overlaps on
+ * the GPU (from several threads or streams) race; serialise them. */
+rg_status rg_grid_build_noalloc(int device, void* stream, int grid_type, const rg_forcefield* ff,
+                                const rg_box* unit_cell, const rg_atom* unit_atoms, int n_unit_atoms, int probe_type,
+                                double cutoff, int nx, int ny, int nz, int precision, double* out_device,
+                                rg_grid_stats* stats);
+
 /* ---- (c) Ewald Fourier energy of a move ---- */
 typedef struct rg_ewald rg_ewald; /* device-resident k-vectors, prefactors and structure factors of one system */
 

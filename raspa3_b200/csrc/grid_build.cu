@@ -19,6 +19,7 @@
 // FP64 epilogue.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -650,6 +651,191 @@ extern "C" rg_status rg_grid_build(rg_ctx* ctx, int grid_type, const rg_forcefie
   else if (out_host)
   {
     RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return RG_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Grid build without any allocation by the library.
+//
+// For callers that cannot allocate device memory themselves or let a library do it: an application whose device
+// memory is owned by another allocator (a host framework that reserves the whole device up front, or a pool with a
+// hard budget), where an extra cudaMalloc would fail or break the budget. The caller passes the inputs and the device
+// output; the only working memory is the file-scope array below, whose size is fixed at load time.
+// ---------------------------------------------------------------------------------------------------------------------
+namespace
+{
+// Scratch of the no-allocation grid build: up to kNoAllocMaxImages staged periodic images (position + parameters,
+// 2 x 32 bytes each) followed by the 8-byte pair counter. Every GPU that loads this library holds it until exit.
+constexpr int kNoAllocMaxImages = 32768;
+constexpr size_t kNoAllocBytes = 2 * sizeof(double4) * kNoAllocMaxImages + 256;
+__device__ __align__(256) unsigned char g_grid_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_address[kMaxDevices] = {};
+
+// The device address of g_grid_noalloc_scratch on `device` (looked up once per device with that device current; in
+// host code the symbol itself is only a host-side stand-in and must never be passed to a kernel).
+cudaError_t noallocScratchAddress(int device, void** out)
+{
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_address[device])
+  {
+    void* p = nullptr;
+    cudaError_t err = cudaGetSymbolAddress(&p, g_grid_noalloc_scratch);
+    if (err != cudaSuccess) return err;
+    g_noalloc_address[device] = p;
+  }
+  *out = g_noalloc_address[device];
+  return cudaSuccess;
+}
+}  // namespace
+
+extern "C" rg_status rg_grid_build_noalloc(int device, void* stream, int grid_type, const rg_forcefield* ff,
+                                           const rg_box* unit_cell, const rg_atom* unit_atoms, int n_unit_atoms,
+                                           int probe_type, double cutoff, int nx, int ny, int nz, int precision,
+                                           double* out_device, rg_grid_stats* stats)
+{
+  (void)cutoff;
+  if (!ff || !unit_cell || (n_unit_atoms > 0 && !unit_atoms) || n_unit_atoms < 0 || !out_device)
+    return RG_ERR_INVALID_ARGUMENT;
+  if (grid_type < 0 || grid_type > 3 || (precision != RG_PRECISION_FP64 && precision != RG_PRECISION_FP32C))
+    return RG_ERR_INVALID_ARGUMENT;
+  if (nx < 2 || ny < 2 || nz < 2) return RG_ERR_INVALID_ARGUMENT;
+  if (grid_type != RG_GRID_EWALD_REAL && (probe_type < 0 || probe_type >= ff->n_types)) return RG_ERR_INVALID_ARGUMENT;
+  if (device < 0 || device >= kMaxDevices) return RG_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(device) != cudaSuccess) return RG_ERR_CUDA;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  void* base = nullptr;
+  if (noallocScratchAddress(device, &base) != cudaSuccess) return RG_ERR_CUDA;
+  double4* dpos = static_cast<double4*>(base);
+  double4* dpar = dpos + kNoAllocMaxImages;
+  unsigned long long* dcount = reinterpret_cast<unsigned long long*>(dpar + kNoAllocMaxImages);
+
+  const rg::HostBox box = rg::makeHostBox(unit_cell);
+  double w[3];
+  rg::perpendicularWidths(box, w);
+  const double rc = ff->cutoff_framework_vdw;
+  const double C = rg::coulombFactor();
+
+  // Enumerate the images in the order of rg_grid_build and stream them to the scratch array through a fixed stack
+  // buffer (copies from pageable memory return once the buffer may be reused). Sizes beyond the array are rejected.
+  constexpr int kChunk = 256;
+  double4 cpos[kChunk], cpar[kChunk];
+  int in_chunk = 0, n_images = 0;
+  bool too_many = false;
+  auto flush = [&]() -> bool
+  {
+    if (in_chunk == 0) return true;
+    if (cudaMemcpyAsync(dpos + n_images - in_chunk, cpos, sizeof(double4) * in_chunk, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(dpar + n_images - in_chunk, cpar, sizeof(double4) * in_chunk, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess)
+      return false;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return false;
+    in_chunk = 0;
+    return true;
+  };
+  for (int a = 0; a < n_unit_atoms && !too_many; ++a)
+  {
+    const rg_atom& at = unit_atoms[a];
+    double4 pr = make_double4(0, 0, 0, 0);
+    double wq = 0.0;
+    if (grid_type == RG_GRID_EWALD_REAL)
+    {
+      if (at.charge == 0.0) continue;
+      wq = C * at.charge;
+    }
+    else
+    {
+      const int idx = probe_type * ff->n_types + at.type;
+      if (ff->epsilon[idx] == 0.0) continue;
+      pr = make_double4(4.0 * ff->epsilon[idx], ff->sigma[idx] * ff->sigma[idx], ff->shift[idx], 0.0);
+    }
+    double r[3] = {at.x, at.y, at.z}, s[3];
+    rg::matvec(box.ic, r, s);
+    int lo[3], hi[3];
+    for (int d = 0; d < 3; ++d)
+    {
+      const double f = rc / w[d] + 1e-9;
+      lo[d] = static_cast<int>(std::ceil(-s[d] - f));
+      hi[d] = static_cast<int>(std::floor(1.0 - s[d] + f));
+    }
+    for (int mx = lo[0]; mx <= hi[0] && !too_many; ++mx)
+      for (int my = lo[1]; my <= hi[1] && !too_many; ++my)
+        for (int mz = lo[2]; mz <= hi[2] && !too_many; ++mz)
+        {
+          if (n_images == kNoAllocMaxImages)
+          {
+            too_many = true;
+            break;
+          }
+          double m[3] = {static_cast<double>(mx), static_cast<double>(my), static_cast<double>(mz)}, d[3];
+          rg::matvec(box.c, m, d);
+          cpos[in_chunk] = make_double4(r[0] + d[0], r[1] + d[1], r[2] + d[2], wq);
+          cpar[in_chunk] = pr;
+          ++in_chunk;
+          ++n_images;
+          if (in_chunk == kChunk && !flush()) return RG_ERR_CUDA;
+        }
+  }
+  if (too_many) return RG_ERR_INVALID_ARGUMENT;  // more than kNoAllocMaxImages periodic images
+  if (!flush()) return RG_ERR_CUDA;
+  // the counter must start at zero; the array keeps whatever the previous call left
+  if (cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), st) != cudaSuccess) return RG_ERR_CUDA;
+
+  const int bx = 8, by = 8, bz = 4;
+  GridParams gp{};
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) gp.cell[c][r] = box.c[c][r];
+  gp.ncells[0] = static_cast<double>(nx - 1);
+  gp.ncells[1] = static_cast<double>(ny - 1);
+  gp.ncells[2] = static_cast<double>(nz - 1);
+  gp.delta[0] = 1.0 / gp.ncells[0];
+  gp.delta[1] = 1.0 / gp.ncells[1];
+  gp.delta[2] = 1.0 / gp.ncells[2];
+  gp.nx = nx;
+  gp.ny = ny;
+  gp.nz = nz;
+  gp.n_images = n_images;
+  gp.rc2 = rc * rc;
+  double R = 0.0;
+  for (int sx = -1; sx <= 1; sx += 2)
+    for (int sy = -1; sy <= 1; sy += 2)
+      for (int sz = -1; sz <= 1; sz += 2)
+      {
+        double f[3] = {sx * 0.5 * (bx - 1) * gp.delta[0], sy * 0.5 * (by - 1) * gp.delta[1],
+                       sz * 0.5 * (bz - 1) * gp.delta[2]},
+               d[3];
+        rg::matvec(box.c, f, d);
+        R = std::fmax(R, std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
+      }
+  const double rf = rc + R + 1e-6;
+  gp.filter2 = rf * rf;
+  gp.alpha = ff->ewald_alpha;
+  gp.coul = C;
+  gp.overlap = ff->overlap_criteria;
+  gp.pair_count = dcount;
+  gp.out = out_device;
+  const bool count = stats != nullptr;
+  cudaError_t err;
+  if (precision == RG_PRECISION_FP64)
+    err = box.triclinic ? launchPrec<double, true>(grid_type, gp, dpos, dpar, bx, by, bz, count, st)
+                        : launchPrec<double, false>(grid_type, gp, dpos, dpar, bx, by, bz, count, st);
+  else
+    err = box.triclinic ? launchPrec<float, true>(grid_type, gp, dpos, dpar, bx, by, bz, count, st)
+                        : launchPrec<float, false>(grid_type, gp, dpos, dpar, bx, by, bz, count, st);
+  if (err != cudaSuccess) return RG_ERR_CUDA;
+  if (stats)
+  {
+    unsigned long long c = 0;
+    if (cudaMemcpyAsync(&c, dcount, sizeof(c), cudaMemcpyDeviceToHost, st) != cudaSuccess) return RG_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return RG_ERR_CUDA;
+    stats->pair_count = static_cast<int64_t>(c);
+    stats->n_images = n_images;
+    stats->h2d_bytes = static_cast<int64_t>(2 * sizeof(double4)) * n_images;
+    stats->d2h_bytes = 0;
   }
   return RG_OK;
 }

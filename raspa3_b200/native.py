@@ -68,6 +68,8 @@ def lib():
         L.rg_grid_build.argtypes = [vp, i32, P(RgForceField), P(RgBox), vp, i32, i32, d, i32, i32, i32, i32, vp, vp,
                                     P(GridStats)]
         L.rg_probe_fma_peak.argtypes = [vp, i32, P(d), P(d)]
+        L.rg_grid_build_noalloc.argtypes = [i32, vp, i32, P(RgForceField), P(RgBox), vp, i32, i32, d, i32, i32, i32,
+                                            i32, vp, P(GridStats)]
         L.rg_ewald_create.argtypes = [vp, P(RgForceField), P(RgBox), i32, P(vp)]
         L.rg_ewald_destroy.argtypes = [vp]
         L.rg_ewald_info.argtypes = [vp, P(i64), P(d)]
@@ -217,3 +219,4 @@ class Ewald:
         s = np.ascontiguousarray(s, dtype=np.float64)
         check(self.ctx.handle, lib().rg_ewald_set_structure_factors(self.handle, ctypes.c_void_p(s.ctypes.data),
                                                                     len(s)), "rg_ewald_set_structure_factors")
+

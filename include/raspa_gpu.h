@@ -76,9 +76,12 @@ typedef struct rg_forcefield
 } rg_forcefield;
 
 typedef struct rg_ctx rg_ctx;
+typedef struct rg_system rg_system; /* device-resident framework, grids, adsorbates and pair table of one system */
+typedef struct rg_ewald rg_ewald;   /* device-resident k-vectors, prefactors and structure factors of one system */
 
 /* ---- context ---- */
 rg_status rg_ctx_create(int device, rg_ctx** out);
+/* Objects created on a context (rg_system, rg_ewald, rg_gcmc) must be destroyed before it. */
 rg_status rg_ctx_destroy(rg_ctx* ctx);
 /* Use the caller's CUDA stream (a created cudaStream_t or cudaStreamPerThread; NULL restores the context's own
  * non-blocking stream, so the legacy NULL stream itself cannot be selected). */
@@ -140,9 +143,95 @@ rg_status rg_grid_build_noalloc(int device, void* stream, int grid_type, const r
                                 double cutoff, int nx, int ny, int nz, int precision, double* out_device,
                                 rg_grid_stats* stats);
 
-/* ---- (c) Ewald Fourier energy of a move ---- */
-typedef struct rg_ewald rg_ewald; /* device-resident k-vectors, prefactors and structure factors of one system */
+/* ---- (b) CBMC / CFCMC trial energies ---- */
+/* External energy of one trial (the RunningEnergy fields of CBMC::FirstBeadTrial / ChainTrial), internal units. */
+typedef struct rg_trial_energy
+{
+  double framework_vdw;
+  double framework_charge;
+  double molecule_vdw;
+  double molecule_charge;
+  double dudlambda_vdw[4];
+  double dudlambda_charge[4];
+  int32_t overlap; /* 1: the trial overlaps (the reference drops it: std::nullopt) */
+  int32_t pad;
+} rg_trial_energy;
 
+/* A System's framework atoms (Cartesian, simulation-box frame), pair table and simulation box on ctx's device. */
+rg_status rg_system_create(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* box, const rg_atom* framework_atoms,
+                           int n_framework_atoms, rg_system** out);
+rg_status rg_system_destroy(rg_system* system);
+/* Attaches the tricubic grid of pseudo-atom `index` (index == ff->n_types: the unit-charge Ewald grid), the
+ * System::interpolationGrids slots (src/raspakit/system.cpp:142). data: 8*nx*ny*nz doubles in the layout
+ * rg_grid_build writes; data_on_device != 0 borrows a device buffer the caller keeps alive, else it is copied. */
+rg_status rg_system_set_grid(rg_system* system, int index, const rg_box* unit_cell, int nx, int ny, int nz,
+                             const double* data, int data_on_device);
+/* Uploads the adsorbate atoms (System::spanOfMoleculeAtoms, the moleculeAtoms of CBMC::GrowContext). */
+rg_status rg_system_set_molecules(rg_system* system, const rg_atom* atoms, int n_atoms);
+/* Replaces CBMC::computeExternalNonOverlappingEnergies (src/raspakit/cbmc/interactions.cpp:54-179) and its callees
+ * CBMC::computeFrameworkMoleculeEnergy (cbmc/interactions_framework_molecule.cpp:31-104) and
+ * CBMC::computeInterMolecularEnergy (cbmc/interactions_intermolecular.cpp:22-95); called from the first-bead schemes
+ * (cbmc/multiple_first_bead.cpp) and the chain growth (cbmc/flexible_molecules/insertion.cpp:63-64).
+ * trials: n_trials consecutive sets of atoms_per_trial atoms (<= 64 per set, <= 4096 in total); skip: index within a
+ * set to leave out (-1: none); skip_background_molecule: moleculeId of adsorbate atoms to leave out (-1: none).
+ * out[t] gets trial t's energies; overlapping trials are flagged, not removed. */
+rg_status rg_cbmc_external_energies(rg_system* system, const rg_atom* trials, int n_trials, int atoms_per_trial,
+                                    int skip, int64_t skip_background_molecule, double cutoff_framework_vdw,
+                                    double cutoff_molecule_vdw, double cutoff_coulomb, rg_trial_energy* out);
+
+/* ---- device-resident GCMC of a rigid component (many independent chains) ---- */
+typedef struct rg_gcmc rg_gcmc;
+
+/* A rigid component (Component, src/raspakit/component.ixx): body-frame positions relative to the centre of mass. */
+typedef struct rg_gcmc_component
+{
+  int32_t n_atoms; /* <= 8 */
+  int32_t starting_bead;
+  int32_t types[8];
+  double charges[8];
+  double masses[8];
+  double offsets[24];
+} rg_gcmc_component;
+
+typedef struct rg_gcmc_params
+{
+  double beta;     /* 1/(kB T), internal units (System::beta, system.cpp:98) */
+  double fugacity; /* internal pressure units (pressure / PressureConversionFactor, system.cpp:96) */
+  double cutoff_framework_vdw, cutoff_molecule_vdw, cutoff_coulomb;
+  double max_translation; /* Angstrom, one Cartesian direction per move (translation.cpp:42-48) */
+  double max_rotation;    /* radians, about one Cartesian axis (rotation.cpp:42-53) */
+  double p_translation, p_rotation, p_swap; /* relative move probabilities; a swap is insertion or deletion 50/50 */
+  int32_t n_first_bead_trials;              /* numberOfFirstBeadPositions (<= 16) */
+  int32_t n_orientation_trials;             /* numberOfTrialDirections (<= 16) */
+  int32_t max_molecules;                    /* molecules per chain */
+  uint64_t seed;
+} rg_gcmc_params;
+
+typedef struct rg_gcmc_chain_result
+{
+  int64_t n_molecules;
+  double energy; /* running total energy (framework + molecule-molecule + Ewald) */
+  int64_t attempted[4], accepted[4]; /* translation, rotation, insertion, deletion */
+  double sum_n, sum_n2, sum_energy;
+  int64_t samples;
+  double block_n[5]; /* loading averaged over 5 consecutive blocks of the recorded moves */
+} rg_gcmc_chain_result;
+
+/* n_chains independent GCMC chains of one rigid component in `system` (framework grids, pair table, simulation box),
+ * each starting from an empty box; with charges, `ewald` (same box, rg_ewald_set_framework already called) provides
+ * the k-vectors and the framework structure factor that every chain starts from. Moves: translation
+ * (mc_moves/component/translation.cpp), rotation (rotation.cpp), CBMC insertion (insertion_cbmc.cpp:34-207) and
+ * deletion (deletion_cbmc.cpp:34-195) with the first-bead and rigid-orientation trials of the reference's CBMC. */
+rg_status rg_gcmc_create(rg_system* system, rg_ewald* ewald, const rg_gcmc_component* component,
+                         const rg_gcmc_params* params, int n_chains, rg_gcmc** out);
+rg_status rg_gcmc_destroy(rg_gcmc* gcmc);
+/* Advances every chain by `moves` move attempts; record != 0 accumulates the statistics. Asynchronous on the ctx stream. */
+rg_status rg_gcmc_run(rg_gcmc* gcmc, int64_t moves, int record);
+rg_status rg_gcmc_results(rg_gcmc* gcmc, rg_gcmc_chain_result* out);
+/* Positions (x, y, z per atom, molecules consecutive) of one chain, for recomputation checks. */
+rg_status rg_gcmc_get_positions(rg_gcmc* gcmc, int chain, double* xyz, int capacity_atoms, int* n_molecules);
+
+/* ---- (c) Ewald Fourier energy of a move ---- */
 /* The Ewald part of RunningEnergy (src/raspakit/running_energy.ixx:500-540) in internal units. */
 typedef struct rg_ewald_energy
 {

@@ -285,3 +285,109 @@ def ewald_single_ion(ff, cell, pos, charge) -> float:
 def select_trial(log_boltzmann, uniform) -> int:
     lb = np.ascontiguousarray(log_boltzmann, dtype=np.float64)
     return lib().oracle_select_trial(_ptr(lb), len(lb), uniform)
+
+
+class OGcmcSetup(ctypes.Structure):
+    _fields_ = [
+        ("ff", ctypes.POINTER(OFF)),
+        ("box", OBox),
+        ("grid_cell", OBox),
+        ("gnx", ctypes.c_int32), ("gny", ctypes.c_int32), ("gnz", ctypes.c_int32),
+        ("grids", ctypes.c_void_p),
+        ("s_framework", ctypes.c_void_p),
+        ("n_atoms", ctypes.c_int32),
+        ("starting_bead", ctypes.c_int32),
+        ("offsets", ctypes.c_double * 24),
+        ("masses", ctypes.c_double * 8),
+        ("types", ctypes.c_int32 * 8),
+        ("charges", ctypes.c_double * 8),
+        ("beta", ctypes.c_double),
+        ("fugacity", ctypes.c_double),
+        ("max_translation", ctypes.c_double),
+        ("max_rotation", ctypes.c_double),
+        ("p_translation", ctypes.c_double),
+        ("p_rotation", ctypes.c_double),
+        ("p_swap", ctypes.c_double),
+        ("n_first_bead_trials", ctypes.c_int32),
+        ("n_orientation_trials", ctypes.c_int32),
+        ("max_molecules", ctypes.c_int32),
+        ("use_ewald", ctypes.c_int32),
+    ]
+
+
+class OGcmcResult(ctypes.Structure):
+    _fields_ = [
+        ("n_molecules", ctypes.c_int64),
+        ("running_energy", ctypes.c_double),
+        ("recomputed_energy", ctypes.c_double),
+        ("sum_n", ctypes.c_double),
+        ("sum_n2", ctypes.c_double),
+        ("sum_energy", ctypes.c_double),
+        ("samples", ctypes.c_int64),
+        ("attempted", ctypes.c_int64 * 4),
+        ("accepted", ctypes.c_int64 * 4),
+        ("block_n", ctypes.c_double * 5),
+    ]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("attempted", "accepted", "block_n")}
+        d["attempted"] = list(self.attempted)
+        d["accepted"] = list(self.accepted)
+        d["block_n"] = list(self.block_n)
+        return d
+
+
+def gcmc_run(ff, cell, component, beta, fugacity, n_chains, steps, equilibration=0, seed=1, threads=0, grids=None,
+             grid_dims=None, grid_cell=None, s_framework=None, use_ewald=True, max_translation=1.0,
+             max_rotation=0.5235987755982988, probabilities=(1.0, 1.0, 1.0), n_first=10, n_orient=10,
+             max_molecules=512):
+    """Independent GCMC chains of one rigid component; returns (list of result dicts, seconds)."""
+    L = lib()
+    if not hasattr(L, "_gcmc_declared"):
+        L.oracle_gcmc_run.argtypes = [ctypes.POINTER(OGcmcSetup), ctypes.c_int, ctypes.c_int64, ctypes.c_int64,
+                                      ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        L._gcmc_declared = True
+    o = off(ff)
+    s = OGcmcSetup()
+    s.ff = ctypes.pointer(o)
+    s.box = obox(cell)
+    keep = [o]
+    if grids is not None:
+        arr = (ctypes.c_void_p * len(grids))()
+        gk = [None if g is None else np.ascontiguousarray(g, dtype=np.float64) for g in grids]
+        for i, g in enumerate(gk):
+            arr[i] = None if g is None else g.ctypes.data
+        keep += [arr, gk]
+        s.grids = ctypes.cast(arr, ctypes.c_void_p)
+        s.gnx, s.gny, s.gnz = grid_dims
+        s.grid_cell = obox(grid_cell)
+    if s_framework is not None:
+        sf = np.ascontiguousarray(s_framework, dtype=np.float64)
+        keep.append(sf)
+        s.s_framework = sf.ctypes.data
+    n = component.n_atoms
+    s.n_atoms = n
+    s.starting_bead = component.starting_bead
+    types = component.types(ff)
+    charges = component.charges(ff)
+    for i in range(n):
+        for d in range(3):
+            s.offsets[3 * i + d] = float(component.offsets[i][d])
+        s.masses[i] = float(component.masses[i])
+        s.types[i] = int(types[i])
+        s.charges[i] = float(charges[i])
+    s.beta = beta
+    s.fugacity = fugacity
+    s.max_translation = max_translation
+    s.max_rotation = max_rotation
+    s.p_translation, s.p_rotation, s.p_swap = probabilities
+    s.n_first_bead_trials = n_first
+    s.n_orientation_trials = n_orient
+    s.max_molecules = max_molecules
+    s.use_ewald = 1 if use_ewald else 0
+    out = (OGcmcResult * n_chains)()
+    secs = ctypes.c_double()
+    L.oracle_gcmc_run(ctypes.byref(s), n_chains, steps, equilibration, seed, threads, ctypes.cast(out, ctypes.c_void_p),
+                      ctypes.c_void_p(ctypes.addressof(secs)))
+    del keep
+    return [out[i].as_dict() for i in range(n_chains)], secs.value

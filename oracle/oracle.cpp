@@ -419,7 +419,23 @@ struct TricubicMatrix
     }
     for (int r = 0; r < 64; ++r)
       for (int c = 0; c < 64; ++c) m[r][c] = std::rint(B[r][64 + c]);
+    // nonzero pattern per row: the reference evaluates the map unrolled over its ~1000 nonzeros
+    // (interpolation_energy_grid.cpp:195-358), so the oracle does the same amount of work
+    for (int r = 0; r < 64; ++r)
+    {
+      start[r] = static_cast<int>(nzc.size());
+      for (int c = 0; c < 64; ++c)
+        if (m[r][c] != 0.0)
+        {
+          nzc.push_back(c);
+          nzv.push_back(m[r][c]);
+        }
+    }
+    start[64] = static_cast<int>(nzc.size());
   }
+  int start[65];
+  std::vector<int> nzc;
+  std::vector<double> nzv;
 };
 
 const TricubicMatrix& tricubicMatrix()
@@ -455,11 +471,11 @@ double interpolateTricubic(const double* data, int nx, int ny, int nz, const Box
     X[8 * l + 6] = at(l, x0, y1, z1);
     X[8 * l + 7] = at(l, x1, y1, z1);
   }
-  const auto& M = tricubicMatrix().m;
+  const TricubicMatrix& T = tricubicMatrix();
   for (int r = 0; r < 64; ++r)
   {
     double acc = 0.0;
-    for (int c = 0; c < 64; ++c) acc += M[r][c] * X[c];
+    for (int q = T.start[r]; q < T.start[r + 1]; ++q) acc += T.nzv[q] * X[T.nzc[q]];
     a[r] = acc;
   }
   double value = 0.0;

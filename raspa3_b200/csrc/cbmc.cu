@@ -1,0 +1,466 @@
+// (b) Energies of CBMC / CFCMC trial positions and orientations on sm_100a.
+//
+// Replaces CBMC::computeExternalNonOverlappingEnergies (src/raspakit/cbmc/interactions.cpp:54-179) with its two
+// callees CBMC::computeFrameworkMoleculeEnergy (cbmc/interactions_framework_molecule.cpp:31-104) and
+// CBMC::computeInterMolecularEnergy (cbmc/interactions_intermolecular.cpp:22-95).
+//
+// A system (rg_system) keeps on the device: the pair table, the simulation box, the framework atoms, the tricubic
+// grids (one per pseudo-atom type plus the unit-charge Ewald grid) and the adsorbate atoms. One launch evaluates all
+// trials of a growth step: the grid is (trial, partner chunk); each CTA stages the trial's atoms in shared memory,
+// the threads stride over their chunk of partners (framework atoms for trial atoms without a grid, then adsorbate
+// atoms from other molecules), and the per-trial totals are reduced in a fixed order by the last CTA of the trial.
+// Trial atoms with a grid (and not fractional) take the grid branch: one tricubic interpolation of their VDW grid and,
+// with charges, q times the unit-charge Ewald grid. A trial is flagged as overlapping if any VDW pair energy or
+// interpolated VDW energy exceeds the overlap criterion, which is the reference's std::nullopt. Arithmetic is FP64:
+// these launches are latency-bound and FP64 keeps them exact against the FP64 path.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "energy.cuh"
+
+namespace
+{
+constexpr int kThreads = 256;
+constexpr int kChunk = 2048;           // partner atoms per CTA
+constexpr int kMaxTrialAtoms = 64;     // atoms of one trial set
+constexpr int kNumOut = 12;            // fmVDW, fmCharge, mmVDW, mmCharge, dudl VDW[4], dudl charge[4]
+}  // namespace
+
+struct rg_system
+{
+  rg_ctx* ctx = nullptr;
+  int n_types = 0;
+  rgd::FF ff{};
+  rgd::Box box{};
+  double overlap = 1e6;
+  // device buffers
+  double* tables = nullptr;   // eps4, sig2, shift (3*n*n) followed by lj as ints
+  rg_atom* fw = nullptr;
+  int n_fw = 0;
+  rg_atom* mol = nullptr;
+  int n_mol = 0;
+  int mol_cap = 0;
+  std::vector<double*> grids;   // n_types + 1 slots (last = unit-charge Ewald grid); owned device copies
+  std::vector<int> grid_owned;
+  int gnx = 0, gny = 0, gnz = 0;
+  double gic[3][3]{};
+  // per-launch scratch
+  rg_atom* trials = nullptr;
+  int trial_cap = 0;
+  double* partial = nullptr;
+  int partial_cap = 0;
+  unsigned int* counters = nullptr;
+  int counter_cap = 0;
+  rg_trial_energy* out = nullptr;
+  int out_cap = 0;
+  rg_atom* trials_host = nullptr;     // pinned
+  rg_trial_energy* out_host = nullptr;  // pinned
+};
+
+namespace
+{
+struct TrialArgs
+{
+  rgd::FF ff;
+  rgd::Box box;
+  const rg_atom* fw;
+  int n_fw;
+  const rg_atom* mol;
+  int n_mol;
+  const rg_atom* trials;
+  int atoms_per_trial;
+  int skip;
+  long long skip_background;
+  double rcv_fw2, rcv_mol2, rcc2;
+  const double* grid[64];  // per type, null = no grid (types >= 64 have none)
+  const double* ewald_grid;
+  int gnx, gny, gnz;
+  double gic[3][3];
+  int n_chunks;
+  int fw_partners;         // framework atoms scanned (0 if every trial atom has a grid)
+  double* partial;         // [trial][chunk][kNumOut + 1]
+  unsigned int* counters;  // per trial
+  rg_trial_energy* out;
+};
+
+__global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a)
+{
+  const int trial = blockIdx.x;
+  const int chunk = blockIdx.y;
+  __shared__ rg_atom sT[kMaxTrialAtoms];
+  __shared__ int sGridBranch[kMaxTrialAtoms];
+  __shared__ double red[kThreads / 32][kNumOut + 1];
+  __shared__ bool last;
+  const int nA = a.atoms_per_trial;
+  for (int i = threadIdx.x; i < nA; i += blockDim.x)
+  {
+    sT[i] = a.trials[static_cast<long long>(trial) * nA + i];
+    const int t = sT[i].type;
+    sGridBranch[i] = (t < 64 && a.grid[t] != nullptr && !rgd::fractionalOf(sT[i])) ? 1 : 0;
+  }
+  __syncthreads();
+
+  double acc[kNumOut];
+#pragma unroll
+  for (int c = 0; c < kNumOut; ++c) acc[c] = 0.0;
+  double overlap = 0.0;
+
+  // grid branch: one thread per trial atom, in chunk 0 only
+  if (chunk == 0)
+  {
+    for (int i = threadIdx.x; i < nA; i += blockDim.x)
+    {
+      if (i == a.skip || !sGridBranch[i]) continue;
+      rgd::Grid g{a.grid[sT[i].type], a.gnx, a.gny, a.gnz, {}};
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) g.ic[r][c] = a.gic[r][c];
+      const double e = rgd::interpolate(g, sT[i].x, sT[i].y, sT[i].z);
+      if (e > a.ff.overlap) overlap = 1.0;
+      acc[0] += e;
+      if (a.ff.use_charge && a.ewald_grid)
+      {
+        rgd::Grid ge = g;
+        ge.data = a.ewald_grid;
+        acc[1] += sT[i].charge * rgd::interpolate(ge, sT[i].x, sT[i].y, sT[i].z);
+      }
+    }
+  }
+
+  const long long total = static_cast<long long>(a.fw_partners) + a.n_mol;
+  const long long begin = static_cast<long long>(chunk) * kChunk;
+  const long long end = begin + kChunk < total ? begin + kChunk : total;
+  for (long long p = begin + threadIdx.x; p < end; p += blockDim.x)
+  {
+    const bool isFw = p < a.fw_partners;
+    const rg_atom B = isFw ? a.fw[p] : a.mol[p - a.fw_partners];
+    if (!isFw && a.skip_background >= 0 && static_cast<long long>(B.molecule_id) == a.skip_background) continue;
+    const int gB = rgd::groupOf(B);
+    for (int i = 0; i < nA; ++i)
+    {
+      if (i == a.skip) continue;
+      const rg_atom& A = sT[i];
+      if (isFw && sGridBranch[i]) continue;
+      if (!isFw && A.molecule_id == B.molecule_id) continue;
+      // dr = partner - trial in both loops (interactions_framework_molecule.cpp:86-88,
+      // interactions_intermolecular.cpp:66-68)
+      double dx = B.x - A.x, dy = B.y - A.y, dz = B.z - A.z;
+      rgd::pbc(a.box, dx, dy, dz);
+      const double rr = dx * dx + dy * dy + dz * dz;
+      const double rcv2 = isFw ? a.rcv_fw2 : a.rcv_mol2;
+      const int gA = rgd::groupOf(A);
+      if (rr < rcv2)
+      {
+        const double2 f = rgd::pairVDW(a.ff, B.scaling_vdw, A.scaling_vdw, rr, B.type, A.type);
+        if (f.x > a.ff.overlap) overlap = 1.0;
+        acc[isFw ? 0 : 2] += f.x;
+        // addDudlambdaVDW(groupIdA(partner), groupIdB(trial), ...) (running_energy.ixx:258-263)
+        if (gB != 0) acc[4 + gB - 1] += A.scaling_vdw * f.y;
+        if (gA != 0) acc[4 + gA - 1] += B.scaling_vdw * f.y;
+      }
+      if (a.ff.use_charge && rr < a.rcc2)
+      {
+        const double r = sqrt(rr);
+        const double2 f = rgd::pairCoulomb(a.ff, B.scaling_coulomb, A.scaling_coulomb, r, B.charge, A.charge);
+        acc[isFw ? 1 : 3] += f.x;
+        if (gB != 0) acc[8 + gB - 1] += A.scaling_coulomb * f.y;
+        if (gA != 0) acc[8 + gA - 1] += B.scaling_coulomb * f.y;
+      }
+    }
+  }
+
+  // block reduction (fixed order), then the last CTA of this trial sums the chunks in order
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c <= kNumOut; ++c)
+  {
+    double x = c < kNumOut ? acc[c] : overlap;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+      const double y = __shfl_down_sync(0xffffffffu, x, o);
+      x = (c < kNumOut) ? x + y : fmax(x, y);
+    }
+    if (lane == 0) red[warp][c] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    double* dst = a.partial + (static_cast<long long>(trial) * a.n_chunks + chunk) * (kNumOut + 1);
+    for (int c = 0; c <= kNumOut; ++c)
+    {
+      double x = 0.0;
+      for (int w = 0; w < kThreads / 32; ++w) x = (c < kNumOut) ? x + red[w][c] : fmax(x, red[w][c]);
+      dst[c] = x;
+    }
+    __threadfence();
+    const unsigned int done = atomicAdd(a.counters + trial, 1u);
+    last = (done == static_cast<unsigned int>(a.n_chunks - 1));
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0)
+  {
+    __threadfence();
+    double tot[kNumOut + 1];
+    for (int c = 0; c <= kNumOut; ++c) tot[c] = 0.0;
+    const volatile double* src = a.partial + static_cast<long long>(trial) * a.n_chunks * (kNumOut + 1);
+    for (int ch = 0; ch < a.n_chunks; ++ch)
+      for (int c = 0; c <= kNumOut; ++c)
+        tot[c] = (c < kNumOut) ? tot[c] + src[ch * (kNumOut + 1) + c] : fmax(tot[c], src[ch * (kNumOut + 1) + c]);
+    rg_trial_energy o;
+    o.framework_vdw = tot[0];
+    o.framework_charge = tot[1];
+    o.molecule_vdw = tot[2];
+    o.molecule_charge = tot[3];
+    for (int g = 0; g < 4; ++g)
+    {
+      o.dudlambda_vdw[g] = tot[4 + g];
+      o.dudlambda_charge[g] = tot[8 + g];
+    }
+    o.overlap = tot[kNumOut] > 0.0 ? 1 : 0;
+    o.pad = 0;
+    a.out[trial] = o;
+    a.counters[trial] = 0u;
+  }
+}
+
+template <typename T>
+rg_status growDevice(rg_ctx* ctx, T** p, int* cap, int need)
+{
+  if (*cap >= need && *p) return RG_OK;
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (*p) RG_CUDA(ctx, cudaFree(*p));
+  *p = nullptr;
+  int grow = need + need / 2 + 16;
+  RG_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * static_cast<size_t>(grow)));
+  *cap = grow;
+  return RG_OK;
+}
+}  // namespace
+
+extern "C"
+{
+rg_status rg_system_create(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* box, const rg_atom* framework_atoms,
+                           int n_framework_atoms, rg_system** out)
+{
+  if (!ctx || !ff || !box || !out || n_framework_atoms < 0 || (n_framework_atoms > 0 && !framework_atoms))
+    return RG_ERR_INVALID_ARGUMENT;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  rg_system* s = new rg_system();
+  s->ctx = ctx;
+  const int n = ff->n_types;
+  s->n_types = n;
+  std::vector<double> tab(3 * n * n);
+  std::vector<int> lj(n * n);
+  for (int i = 0; i < n * n; ++i)
+  {
+    tab[i] = 4.0 * ff->epsilon[i];
+    tab[n * n + i] = ff->sigma[i] * ff->sigma[i];
+    tab[2 * n * n + i] = ff->shift[i];
+    lj[i] = ff->lj[i];
+  }
+  cudaError_t err = cudaMalloc(reinterpret_cast<void**>(&s->tables), sizeof(double) * 3 * n * n + sizeof(int) * n * n);
+  if (!err) err = cudaMemcpy(s->tables, tab.data(), sizeof(double) * 3 * n * n, cudaMemcpyHostToDevice);
+  if (!err) err = cudaMemcpy(s->tables + 3 * n * n, lj.data(), sizeof(int) * n * n, cudaMemcpyHostToDevice);
+  if (!err && n_framework_atoms > 0)
+  {
+    err = cudaMalloc(reinterpret_cast<void**>(&s->fw), sizeof(rg_atom) * n_framework_atoms);
+    if (!err) err = cudaMemcpy(s->fw, framework_atoms, sizeof(rg_atom) * n_framework_atoms, cudaMemcpyHostToDevice);
+  }
+  if (!err) err = cudaMallocHost(reinterpret_cast<void**>(&s->trials_host), sizeof(rg_atom) * 4096);
+  if (!err) err = cudaMallocHost(reinterpret_cast<void**>(&s->out_host), sizeof(rg_trial_energy) * 4096);
+  if (err)
+  {
+    rg_status st = rg::cudaFail(ctx, err, "rg_system_create");
+    rg_system_destroy(s);
+    return st;
+  }
+  s->n_fw = n_framework_atoms;
+  s->ff.n = n;
+  s->ff.eps4 = s->tables;
+  s->ff.sig2 = s->tables + n * n;
+  s->ff.shift = s->tables + 2 * n * n;
+  s->ff.lj = reinterpret_cast<const int*>(s->tables + 3 * n * n);
+  s->ff.alpha = ff->ewald_alpha;
+  s->ff.coul = rg::coulombFactor();
+  s->ff.overlap = ff->overlap_criteria;
+  s->ff.use_charge = ff->use_charge;
+  rg::HostBox hb = rg::makeHostBox(box);
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r)
+    {
+      s->box.c[c][r] = hb.c[c][r];
+      s->box.ic[c][r] = hb.ic[c][r];
+    }
+  s->box.triclinic = hb.triclinic ? 1 : 0;
+  s->box.volume = hb.volume;
+  s->grids.assign(n + 1, nullptr);
+  s->grid_owned.assign(n + 1, 0);
+  *out = s;
+  return RG_OK;
+}
+
+rg_status rg_system_destroy(rg_system* s)
+{
+  if (!s) return RG_OK;
+  if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
+  cudaFree(s->tables);
+  cudaFree(s->fw);
+  cudaFree(s->mol);
+  for (size_t i = 0; i < s->grids.size(); ++i)
+    if (s->grid_owned[i]) cudaFree(s->grids[i]);
+  cudaFree(s->trials);
+  cudaFree(s->partial);
+  cudaFree(s->counters);
+  cudaFree(s->out);
+  if (s->trials_host) cudaFreeHost(s->trials_host);
+  if (s->out_host) cudaFreeHost(s->out_host);
+  delete s;
+  return RG_OK;
+}
+
+rg_status rg_system_set_grid(rg_system* s, int index, const rg_box* unit_cell, int nx, int ny, int nz,
+                             const double* data, int data_on_device)
+{
+  if (!s || !unit_cell || !data || index < 0 || index > s->n_types || nx < 2 || ny < 2 || nz < 2)
+    return RG_ERR_INVALID_ARGUMENT;
+  if (index < s->n_types && index >= 64)
+    return rg::fail(s->ctx, RG_ERR_UNSUPPORTED, "rg_system_set_grid: grids only for pseudo-atom types < 64");
+  rg_ctx* ctx = s->ctx;
+  bool first = true;
+  for (int i = 0; i <= s->n_types; ++i)
+    if (s->grids[i]) first = false;
+  if (!first && (nx != s->gnx || ny != s->gny || nz != s->gnz))
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_system_set_grid: all grids of a system share one shape");
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t bytes = sizeof(double) * 8 * static_cast<size_t>(nx) * ny * nz;
+  if (s->grid_owned[index]) RG_CUDA(ctx, cudaFree(s->grids[index]));
+  s->grids[index] = nullptr;
+  s->grid_owned[index] = 0;
+  if (data_on_device)
+  {
+    s->grids[index] = const_cast<double*>(data);  // borrowed: the caller keeps it alive
+  }
+  else
+  {
+    RG_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&s->grids[index]), bytes));
+    s->grid_owned[index] = 1;
+    RG_CUDA(ctx, cudaMemcpy(s->grids[index], data, bytes, cudaMemcpyHostToDevice));
+  }
+  rg::HostBox hb = rg::makeHostBox(unit_cell);
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) s->gic[c][r] = hb.ic[c][r];
+  s->gnx = nx;
+  s->gny = ny;
+  s->gnz = nz;
+  return RG_OK;
+}
+
+rg_status rg_system_set_molecules(rg_system* s, const rg_atom* atoms, int n)
+{
+  if (!s || n < 0 || (n > 0 && !atoms)) return RG_ERR_INVALID_ARGUMENT;
+  rg_ctx* ctx = s->ctx;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  rg_status st = growDevice(ctx, &s->mol, &s->mol_cap, n > 0 ? n : 1);
+  if (st) return st;
+  if (n > 0) RG_CUDA(ctx, cudaMemcpyAsync(s->mol, atoms, sizeof(rg_atom) * n, cudaMemcpyHostToDevice, ctx->stream));
+  s->n_mol = n;
+  return RG_OK;
+}
+
+rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_trials, int atoms_per_trial, int skip,
+                                    int64_t skip_background_molecule, double cutoff_framework_vdw,
+                                    double cutoff_molecule_vdw, double cutoff_coulomb, rg_trial_energy* out)
+{
+  if (!s || !trials || !out || n_trials < 0 || atoms_per_trial < 1) return RG_ERR_INVALID_ARGUMENT;
+  rg_ctx* ctx = s->ctx;
+  if (atoms_per_trial > kMaxTrialAtoms)
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_cbmc_external_energies: at most 64 atoms per trial");
+  if (static_cast<long long>(n_trials) * atoms_per_trial > 4096 || n_trials > 4096)
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_cbmc_external_energies: at most 4096 trial atoms per call");
+  if (n_trials == 0) return RG_OK;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int nt_atoms = n_trials * atoms_per_trial;
+  // does any trial atom need the framework pair loop?
+  bool needFw = false;
+  for (int i = 0; i < nt_atoms && !needFw; ++i)
+  {
+    if (i % atoms_per_trial == skip) continue;
+    const int t = trials[i].type;
+    const bool grid = t < 64 && t < s->n_types && s->grids[t] && !((trials[i].group_fractional >> 4) != 0);
+    if (!grid) needFw = true;
+  }
+  const int fw_partners = needFw ? s->n_fw : 0;
+  const long long total = static_cast<long long>(fw_partners) + s->n_mol;
+  const int n_chunks = static_cast<int>(total > 0 ? (total + kChunk - 1) / kChunk : 1);
+  rg_status st = growDevice(ctx, &s->trials, &s->trial_cap, nt_atoms);
+  if (!st) st = growDevice(ctx, &s->partial, &s->partial_cap, n_trials * n_chunks * (kNumOut + 1));
+  if (!st && s->counter_cap < n_trials)
+  {
+    st = growDevice(ctx, &s->counters, &s->counter_cap, n_trials);
+    if (!st) RG_CUDA(ctx, cudaMemsetAsync(s->counters, 0, sizeof(unsigned int) * s->counter_cap, ctx->stream));
+  }
+  if (!st) st = growDevice(ctx, &s->out, &s->out_cap, n_trials);
+  if (st) return st;
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // pinned staging of the previous call is free again
+  std::memcpy(s->trials_host, trials, sizeof(rg_atom) * nt_atoms);
+  RG_CUDA(ctx, cudaMemcpyAsync(s->trials, s->trials_host, sizeof(rg_atom) * nt_atoms, cudaMemcpyHostToDevice,
+                               ctx->stream));
+  TrialArgs a{};
+  a.ff = s->ff;
+  a.box = s->box;
+  a.fw = s->fw;
+  a.n_fw = s->n_fw;
+  a.mol = s->mol;
+  a.n_mol = s->n_mol;
+  a.trials = s->trials;
+  a.atoms_per_trial = atoms_per_trial;
+  a.skip = skip;
+  a.skip_background = skip_background_molecule;
+  a.rcv_fw2 = cutoff_framework_vdw * cutoff_framework_vdw;
+  a.rcv_mol2 = cutoff_molecule_vdw * cutoff_molecule_vdw;
+  a.rcc2 = cutoff_coulomb * cutoff_coulomb;
+  for (int t = 0; t < 64; ++t) a.grid[t] = t < s->n_types ? s->grids[t] : nullptr;
+  a.ewald_grid = s->grids[s->n_types];
+  a.gnx = s->gnx;
+  a.gny = s->gny;
+  a.gnz = s->gnz;
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) a.gic[c][r] = s->gic[c][r];
+  a.n_chunks = n_chunks;
+  a.fw_partners = fw_partners;
+  a.partial = s->partial;
+  a.counters = s->counters;
+  a.out = s->out;
+  dim3 grid(n_trials, n_chunks);
+  trialEnergyKernel<<<grid, kThreads, 0, ctx->stream>>>(a);
+  RG_CUDA(ctx, cudaGetLastError());
+  RG_CUDA(ctx, cudaMemcpyAsync(s->out_host, s->out, sizeof(rg_trial_energy) * n_trials, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  std::memcpy(out, s->out_host, sizeof(rg_trial_energy) * n_trials);
+  return RG_OK;
+}
+}
+
+namespace rgd
+{
+rg_status systemExport(rg_system* s, FF* ff, Box* box, const double** type_grids, const double** ewald_grid,
+                       int* n_types, int gdims[3], double gic[3][3], rg_ctx** ctx)
+{
+  if (!s) return RG_ERR_INVALID_ARGUMENT;
+  *ff = s->ff;
+  *box = s->box;
+  for (int t = 0; t < 64; ++t) type_grids[t] = t < s->n_types ? s->grids[t] : nullptr;
+  *ewald_grid = s->grids[s->n_types];
+  *n_types = s->n_types;
+  gdims[0] = s->gnx;
+  gdims[1] = s->gny;
+  gdims[2] = s->gnz;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) gic[a][b] = s->gic[a][b];
+  *ctx = s->ctx;
+  return RG_OK;
+}
+}  // namespace rgd

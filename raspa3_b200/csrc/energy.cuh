@@ -1,0 +1,176 @@
+// Device-side pair potentials, periodic boundaries and tricubic grid interpolation shared by the CBMC trial-energy
+// kernels and the device-resident Monte Carlo kernels. All FP64.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/raspa_gpu.h"
+
+namespace rgd
+{
+// Force-field tables on the device (n x n, row = type A).
+struct FF
+{
+  int n;
+  const double* eps4;   // 4 * epsilon
+  const double* sig2;   // sigma^2
+  const double* shift;
+  const int* lj;
+  double alpha;
+  double coul;          // CoulombicConversionFactor
+  double overlap;
+  int use_charge;
+};
+
+struct Box
+{
+  double c[3][3];   // c[col][row]
+  double ic[3][3];
+  int triclinic;
+  double volume;
+};
+
+__device__ __forceinline__ double roundHalfAway(double x)
+{
+  return static_cast<double>(static_cast<long long>(x + ((x >= 0.0) ? 0.5 : -0.5)));
+}
+
+// SimulationBox::applyPeriodicBoundaryConditions (src/raspakit/simulationbox.ixx:131-161)
+__device__ __forceinline__ void pbc(const Box& b, double& dx, double& dy, double& dz)
+{
+  if (!b.triclinic)
+  {
+    dx -= roundHalfAway(dx * b.ic[0][0]) * b.c[0][0];
+    dy -= roundHalfAway(dy * b.ic[1][1]) * b.c[1][1];
+    dz -= roundHalfAway(dz * b.ic[2][2]) * b.c[2][2];
+    return;
+  }
+  double s0 = b.ic[0][0] * dx + b.ic[1][0] * dy + b.ic[2][0] * dz;
+  double s1 = b.ic[0][1] * dx + b.ic[1][1] * dy + b.ic[2][1] * dz;
+  double s2 = b.ic[0][2] * dx + b.ic[1][2] * dy + b.ic[2][2] * dz;
+  s0 -= roundHalfAway(s0);
+  s1 -= roundHalfAway(s1);
+  s2 -= roundHalfAway(s2);
+  dx = b.c[0][0] * s0 + b.c[1][0] * s1 + b.c[2][0] * s2;
+  dy = b.c[0][1] * s0 + b.c[1][1] * s1 + b.c[2][1] * s2;
+  dz = b.c[0][2] * s0 + b.c[1][2] * s1 + b.c[2][2] * s2;
+}
+
+// potentialVDW<0>, Lennard-Jones branch (src/raspakit/potentials/pair_vdw.ixx:85-101): {energy, dU/dlambda}
+__device__ __forceinline__ double2 pairVDW(const FF& ff, double sA, double sB, double rr, int tA, int tB)
+{
+  const int idx = tA * ff.n + tB;
+  if (!ff.lj[idx]) return make_double2(0.0, 0.0);
+  const double scaling = sA * sB;
+  const double arg1 = ff.eps4[idx];
+  const double arg2 = ff.sig2[idx];
+  const double arg3 = ff.shift[idx];
+  const double temp = rr / arg2;
+  const double temp3 = temp * temp * temp;
+  const double inv_scaling = 1.0 - scaling;
+  const double rri3 = 1.0 / (temp3 + 0.5 * inv_scaling * inv_scaling);
+  const double rri6 = rri3 * rri3;
+  const double term = arg1 * (rri3 * (rri3 - 1.0)) - arg3;
+  const double dlambda_term = arg1 * scaling * inv_scaling * (2.0 * rri6 * rri3 - rri6);
+  return make_double2(scaling * term, term + dlambda_term);
+}
+
+// potentialCoulomb<0>, Ewald branch (src/raspakit/potentials/pair_coulomb.ixx:51-77): {energy, dU/dlambda}
+__device__ __forceinline__ double2 pairCoulomb(const FF& ff, double sA, double sB, double r, double qA, double qB)
+{
+  const double scaling = sA * sB;
+  const double alpha = ff.alpha;
+  const double prefactor = ff.coul * qA * qB;
+  const double s = r + 0.01 * (1.0 - scaling);
+  const double inverseS = 1.0 / s;
+  const double inverseSS = inverseS * inverseS;
+  const double erfcTerm = erfc(alpha * s);
+  const double gaussian = exp(-alpha * alpha * s * s) * 0.564189583547756286948079451560772586;
+  const double phi = erfcTerm * inverseS;
+  const double phiPrime = -(erfcTerm * inverseSS + 2.0 * alpha * gaussian * inverseS);
+  return make_double2(scaling * prefactor * phi, prefactor * (phi - scaling * 0.01 * phiPrime));
+}
+
+struct Grid
+{
+  const double* data;  // 8 doubles per point, data[l + 8*(i + nx*(j + ny*k))]
+  int nx, ny, nz;
+  double ic[3][3];     // inverse of the grid's unit cell
+};
+
+__device__ __forceinline__ double fract1(double x)
+{
+  // double3::fract (src/mathkit/double3.cpp:22-50)
+  double s = x - rint(x);
+  if (s < 0.0) s += 1.0;
+  if (s > 1.0) s -= 1.0;
+  return s;
+}
+
+// InterpolationEnergyGrid::interpolate, tricubic scheme (src/raspakit/interpolation_energy_grid.cpp:3980-4118).
+// The reference maps the 64 corner values (f, fx, fy, fz, fxy, fxz, fyz, fxyz at 8 corners) through the Lekien-Marsden
+// 64x64 matrix to monomial coefficients and sums the polynomial; that interpolant is the tensor product of 1D cubic
+// Hermite bases, evaluated here directly as 64 products (identical up to rounding).
+__device__ __forceinline__ double interpolate(const Grid& g, double px, double py, double pz)
+{
+  double s[3];
+  s[0] = fract1(g.ic[0][0] * px + g.ic[1][0] * py + g.ic[2][0] * pz);
+  s[1] = fract1(g.ic[0][1] * px + g.ic[1][1] * py + g.ic[2][1] * pz);
+  s[2] = fract1(g.ic[0][2] * px + g.ic[1][2] * py + g.ic[2][2] * pz);
+  const int nc[3] = {g.nx - 1, g.ny - 1, g.nz - 1};
+  int i0[3];
+  double t[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    long long c = static_cast<long long>(s[d] * static_cast<double>(nc[d]));
+    i0[d] = static_cast<int>(c < nc[d] - 1 ? c : nc[d] - 1);
+    t[d] = s[d] * static_cast<double>(nc[d]) - static_cast<double>(i0[d]);
+  }
+  // h[d][corner][order]: corner 0/1, order 0 = value basis, 1 = derivative basis
+  double h[3][2][2];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    const double x = t[d], x2 = x * x, x3 = x2 * x;
+    h[d][0][0] = 2.0 * x3 - 3.0 * x2 + 1.0;
+    h[d][1][0] = -2.0 * x3 + 3.0 * x2;
+    h[d][0][1] = x3 - 2.0 * x2 + x;
+    h[d][1][1] = x3 - x2;
+  }
+  // derivative orders (x, y, z) of the 8 stored channels
+  const int ox[8] = {0, 1, 0, 0, 1, 1, 0, 1};
+  const int oy[8] = {0, 0, 1, 0, 1, 0, 1, 1};
+  const int oz[8] = {0, 0, 0, 1, 0, 1, 1, 1};
+  double value = 0.0;
+#pragma unroll
+  for (int corner = 0; corner < 8; ++corner)
+  {
+    const int cx = corner & 1, cy = (corner >> 1) & 1, cz = (corner >> 2) & 1;
+    const double* p = g.data + 8 * (static_cast<long long>(i0[0] + cx) +
+                                    static_cast<long long>(g.nx) * (static_cast<long long>(i0[1] + cy) +
+                                                                   static_cast<long long>(g.ny) * (i0[2] + cz)));
+    const double2* p2 = reinterpret_cast<const double2*>(p);
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+    {
+      double2 u = __ldg(p2 + q);
+      v[2 * q] = u.x;
+      v[2 * q + 1] = u.y;
+    }
+#pragma unroll
+    for (int l = 0; l < 8; ++l) value += v[l] * h[0][cx][ox[l]] * h[1][cy][oy[l]] * h[2][cz][oz[l]];
+  }
+  return value;
+}
+
+// Internal accessors between translation units: the device data of a system and of an Ewald state.
+rg_status systemExport(rg_system* s, FF* ff, Box* box, const double** type_grids /*[64]*/, const double** ewald_grid,
+                       int* n_types, int gdims[3], double gic[3][3], rg_ctx** ctx);
+rg_status ewaldExport(rg_ewald* e, const char4** kvec, const double** temp, const double2** s_rigid, int64_t* nk,
+                      int kmax[3], double* alpha, double* single_ion_sum);
+
+__device__ __forceinline__ int groupOf(const rg_atom& a) { return a.group_fractional & 0x0f; }
+__device__ __forceinline__ bool fractionalOf(const rg_atom& a) { return (a.group_fractional >> 4) != 0; }
+}  // namespace rgd

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "energy.cuh"
 
 struct rg_ewald
 {
@@ -770,3 +771,22 @@ rg_status rg_ewald_set_structure_factors(rg_ewald* e, const double* host, int64_
   return RG_OK;
 }
 }
+
+namespace rgd
+{
+rg_status ewaldExport(rg_ewald* e, const char4** kvec, const double** temp, const double2** s_rigid, int64_t* nk,
+                      int kmax[3], double* alpha, double* single_ion_sum)
+{
+  if (!e) return RG_ERR_INVALID_ARGUMENT;
+  *kvec = e->kvec;
+  *temp = e->temp;
+  *s_rigid = e->s_rigid;
+  *nk = e->nk;
+  kmax[0] = e->ff.kmax_x;
+  kmax[1] = e->ff.kmax_y;
+  kmax[2] = e->ff.kmax_z;
+  *alpha = e->alpha;
+  *single_ion_sum = e->single_ion_sum;
+  return RG_OK;
+}
+}  // namespace rgd

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -40,6 +41,39 @@ class EwaldEnergy(ctypes.Structure):
                 "ewald_exclusion": self.ewald_exclusion, "dudlambda_ewald": list(self.dudlambda_ewald)}
 
 
+class TrialEnergy(ctypes.Structure):
+    _fields_ = [("framework_vdw", ctypes.c_double), ("framework_charge", ctypes.c_double),
+                ("molecule_vdw", ctypes.c_double), ("molecule_charge", ctypes.c_double),
+                ("dudlambda_vdw", ctypes.c_double * 4), ("dudlambda_charge", ctypes.c_double * 4),
+                ("overlap", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+class GcmcComponent(ctypes.Structure):
+    _fields_ = [("n_atoms", ctypes.c_int32), ("starting_bead", ctypes.c_int32), ("types", ctypes.c_int32 * 8),
+                ("charges", ctypes.c_double * 8), ("masses", ctypes.c_double * 8), ("offsets", ctypes.c_double * 24)]
+
+
+class GcmcParams(ctypes.Structure):
+    _fields_ = [("beta", ctypes.c_double), ("fugacity", ctypes.c_double),
+                ("cutoff_framework_vdw", ctypes.c_double), ("cutoff_molecule_vdw", ctypes.c_double),
+                ("cutoff_coulomb", ctypes.c_double), ("max_translation", ctypes.c_double),
+                ("max_rotation", ctypes.c_double), ("p_translation", ctypes.c_double),
+                ("p_rotation", ctypes.c_double), ("p_swap", ctypes.c_double),
+                ("n_first_bead_trials", ctypes.c_int32), ("n_orientation_trials", ctypes.c_int32),
+                ("max_molecules", ctypes.c_int32), ("seed", ctypes.c_uint64)]
+
+
+class GcmcChainResult(ctypes.Structure):
+    _fields_ = [("n_molecules", ctypes.c_int64), ("energy", ctypes.c_double), ("attempted", ctypes.c_int64 * 4),
+                ("accepted", ctypes.c_int64 * 4), ("sum_n", ctypes.c_double), ("sum_n2", ctypes.c_double),
+                ("sum_energy", ctypes.c_double), ("samples", ctypes.c_int64), ("block_n", ctypes.c_double * 5)]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f not in ("attempted", "accepted", "block_n")}
+        d["attempted"], d["accepted"], d["block_n"] = list(self.attempted), list(self.accepted), list(self.block_n)
+        return d
+
+
 class GridStats(ctypes.Structure):
     _fields_ = [("pair_count", ctypes.c_int64), ("n_images", ctypes.c_int64), ("h2d_bytes", ctypes.c_int64),
                 ("d2h_bytes", ctypes.c_int64)]
@@ -70,6 +104,16 @@ def lib():
         L.rg_probe_fma_peak.argtypes = [vp, i32, P(d), P(d)]
         L.rg_grid_build_noalloc.argtypes = [i32, vp, i32, P(RgForceField), P(RgBox), vp, i32, i32, d, i32, i32, i32,
                                             i32, vp, P(GridStats)]
+        L.rg_system_create.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, P(vp)]
+        L.rg_system_destroy.argtypes = [vp]
+        L.rg_system_set_grid.argtypes = [vp, i32, P(RgBox), i32, i32, i32, vp, i32]
+        L.rg_system_set_molecules.argtypes = [vp, vp, i32]
+        L.rg_cbmc_external_energies.argtypes = [vp, vp, i32, i32, i32, i64, d, d, d, vp]
+        L.rg_gcmc_create.argtypes = [vp, vp, P(GcmcComponent), P(GcmcParams), i32, P(vp)]
+        L.rg_gcmc_destroy.argtypes = [vp]
+        L.rg_gcmc_run.argtypes = [vp, i64, i32]
+        L.rg_gcmc_results.argtypes = [vp, vp]
+        L.rg_gcmc_get_positions.argtypes = [vp, i32, vp, i32, P(i32)]
         L.rg_ewald_create.argtypes = [vp, P(RgForceField), P(RgBox), i32, P(vp)]
         L.rg_ewald_destroy.argtypes = [vp]
         L.rg_ewald_info.argtypes = [vp, P(i64), P(d)]
@@ -99,9 +143,16 @@ class Context:
             raise RaspaGpuError(f"rg_ctx_create({device}) failed with status {st} (no CUDA device?)")
         self.handle = h
         self.device = device
+        self._children = weakref.WeakSet()
+
+    def adopt(self, child):
+        """Objects created on this context (systems, Ewald states, GCMC runs) are closed before it."""
+        self._children.add(child)
 
     def close(self):
         if self.handle:
+            for child in list(self._children):
+                child.close()
             lib().rg_ctx_destroy(self.handle)
             self.handle = None
 
@@ -163,6 +214,7 @@ class Ewald:
         check(ctx.handle, lib().rg_ewald_create(ctx.handle, ctypes.byref(self._ff), ctypes.byref(self._box), n_groups,
                                                 ctypes.byref(h)), "rg_ewald_create")
         self.handle = h
+        ctx.adopt(self)
         self.n_groups = n_groups
         nk, s = ctypes.c_int64(), ctypes.c_double()
         check(ctx.handle, lib().rg_ewald_info(h, ctypes.byref(nk), ctypes.byref(s)), "rg_ewald_info")
@@ -220,3 +272,123 @@ class Ewald:
         check(self.ctx.handle, lib().rg_ewald_set_structure_factors(self.handle, ctypes.c_void_p(s.ctypes.data),
                                                                     len(s)), "rg_ewald_set_structure_factors")
 
+
+class System:
+    """Device-resident framework, grids and adsorbates of one system (the CBMC::GrowContext data)."""
+
+    def __init__(self, ctx: Context, ff: ForceField, cell, framework_atoms):
+        self.ctx = ctx
+        self.ff = ff
+        self._ff = ff_struct(ff)
+        self._box = box_struct(cell)
+        fw, p = _atoms_ptr(framework_atoms)
+        self._fw = fw
+        h = ctypes.c_void_p()
+        check(ctx.handle, lib().rg_system_create(ctx.handle, ctypes.byref(self._ff), ctypes.byref(self._box), p,
+                                                 len(fw), ctypes.byref(h)), "rg_system_create")
+        self.handle = h
+        ctx.adopt(self)
+        self._grids = {}
+
+    def close(self):
+        if self.handle:
+            lib().rg_system_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_grid(self, index: int, unit_cell, dims, data, on_device: bool = False):
+        box = box_struct(unit_cell)
+        if on_device:
+            ptr = ctypes.c_void_p(int(data))
+        else:
+            data = np.ascontiguousarray(data, dtype=np.float64)
+            self._grids[index] = data
+            ptr = ctypes.c_void_p(data.ctypes.data)
+        check(self.ctx.handle, lib().rg_system_set_grid(self.handle, index, ctypes.byref(box), dims[0], dims[1],
+                                                        dims[2], ptr, 1 if on_device else 0), "rg_system_set_grid")
+
+    def set_molecules(self, atoms):
+        a, p = _atoms_ptr(atoms)
+        check(self.ctx.handle, lib().rg_system_set_molecules(self.handle, p, len(a)), "rg_system_set_molecules")
+
+    def external_energies(self, trials, atoms_per_trial: int, skip: int = -1, skip_background: int = -1,
+                          cutoff_framework_vdw: float | None = None, cutoff_molecule_vdw: float | None = None,
+                          cutoff_coulomb: float | None = None):
+        t, p = _atoms_ptr(trials)
+        n = len(t) // atoms_per_trial
+        out = (TrialEnergy * max(n, 1))()
+        ff = self.ff
+        check(self.ctx.handle, lib().rg_cbmc_external_energies(
+            self.handle, p, n, atoms_per_trial, skip, skip_background,
+            ff.cutoff_framework_vdw if cutoff_framework_vdw is None else cutoff_framework_vdw,
+            ff.cutoff_molecule_vdw if cutoff_molecule_vdw is None else cutoff_molecule_vdw,
+            ff.cutoff_coulomb if cutoff_coulomb is None else cutoff_coulomb, ctypes.cast(out, ctypes.c_void_p)),
+            "rg_cbmc_external_energies")
+        return [out[i] for i in range(n)]
+
+
+class Gcmc:
+    """Independent device-resident GCMC chains of one rigid component (rg_gcmc)."""
+
+    def __init__(self, system: System, ewald, component, beta: float, fugacity: float, n_chains: int, seed: int = 1,
+                 max_translation: float = 1.0, max_rotation: float = 0.5235987755982988,
+                 probabilities=(1.0, 1.0, 1.0), n_first: int = 10, n_orient: int = 10, max_molecules: int = 256):
+        self.ctx = system.ctx
+        self.system = system
+        self.ewald = ewald
+        self.component = component
+        self.n_chains = n_chains
+        ff = system.ff
+        c = GcmcComponent()
+        c.n_atoms = component.n_atoms
+        c.starting_bead = component.starting_bead
+        types, charges = component.types(ff), component.charges(ff)
+        for i in range(component.n_atoms):
+            c.types[i] = int(types[i])
+            c.charges[i] = float(charges[i])
+            c.masses[i] = float(component.masses[i])
+            for d in range(3):
+                c.offsets[3 * i + d] = float(component.offsets[i][d])
+        p = GcmcParams(beta, fugacity, ff.cutoff_framework_vdw, ff.cutoff_molecule_vdw, ff.cutoff_coulomb,
+                       max_translation, max_rotation, probabilities[0], probabilities[1], probabilities[2], n_first,
+                       n_orient, max_molecules, seed)
+        h = ctypes.c_void_p()
+        check(self.ctx.handle, lib().rg_gcmc_create(system.handle, ewald.handle if ewald is not None else None,
+                                                    ctypes.byref(c), ctypes.byref(p), n_chains, ctypes.byref(h)),
+              "rg_gcmc_create")
+        self.handle = h
+        self.ctx.adopt(self)
+        self.max_molecules = max_molecules
+
+    def close(self):
+        if self.handle:
+            lib().rg_gcmc_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, moves: int, record: bool = True):
+        check(self.ctx.handle, lib().rg_gcmc_run(self.handle, moves, 1 if record else 0), "rg_gcmc_run")
+
+    def results(self):
+        out = (GcmcChainResult * self.n_chains)()
+        check(self.ctx.handle, lib().rg_gcmc_results(self.handle, ctypes.cast(out, ctypes.c_void_p)),
+              "rg_gcmc_results")
+        return [out[i].as_dict() for i in range(self.n_chains)]
+
+    def positions(self, chain: int) -> np.ndarray:
+        cap = self.max_molecules * self.component.n_atoms
+        buf = np.empty(3 * cap)
+        n = ctypes.c_int32()
+        check(self.ctx.handle, lib().rg_gcmc_get_positions(self.handle, chain, ctypes.c_void_p(buf.ctypes.data), cap,
+                                                           ctypes.byref(n)), "rg_gcmc_get_positions")
+        return buf[: 3 * n.value * self.component.n_atoms].reshape(-1, 3)

@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gcmc", action="store_true", help="skip the GCMC steps/s section")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the cpu_baseline sample")
     return ap.parse_args()
 
@@ -133,6 +134,93 @@ def cpu_oracle_rate(ff, cell, atoms, dims, grids, target_seconds, threads=0, see
     return pts1 / t1, pts1, t1, threads
 
 
+GCMC_CHAINS_PER_SM = 8
+GCMC_MOVES = 2000
+GCMC_EQUIL = 500
+
+
+def gcmc_setup(ff, cell, atoms):
+    from raspa3_b200.synthetic import replicate
+
+    scell, sfw = replicate(cell, atoms, (2, 2, 3))
+    return scell, sfw
+
+
+def run_gcmc(args, ctx, ff, cell, atoms, dims, grids, outs, world, rank, dist, torch):
+    """Device-resident GCMC of CO2 at 300 K and 1e5 Pa (configuration 2): move attempts per second over all chains."""
+    from raspa3_b200 import native
+    from raspa3_b200.gcmc import beta_of, co2_component, fugacity_of
+
+    scell, sfw = gcmc_setup(ff, cell, atoms)
+    sysg = native.System(ctx, ff, scell, sfw)
+    for (name, gt, probe), out in zip(grids, outs):
+        idx = probe if gt == 0 else ff.n_types
+        sysg.set_grid(idx, cell, dims, out.data_ptr(), on_device=True)
+    ew = native.Ewald(ctx, ff, scell)
+    ew.set_framework(sfw)
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    chains = GCMC_CHAINS_PER_SM * sms
+    g = native.Gcmc(sysg, ew, co2_component(), beta_of(300.0), fugacity_of(1e5), n_chains=chains, seed=1 + rank)
+    g.run(GCMC_EQUIL, record=False)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream()
+    e0.record(stream)
+    g.run(GCMC_MOVES, record=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3
+    if world > 1:
+        t = torch.tensor([secs], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        secs = float(t.item())
+    # e2e: the same run call plus the read-back of every chain's statistics through the C-ABI
+    t0 = time.perf_counter()
+    g.run(GCMC_MOVES, record=True)
+    res = g.results()
+    e2e_secs = time.perf_counter() - t0
+    moves = world * chains * GCMC_MOVES
+    mean_n = float(np.mean([r["sum_n"] / max(1, r["samples"]) for r in res]))
+    out = {"metric": "GCMC steps/s", "value": moves / secs, "unit": "MC move attempts/s", "chains": chains,
+           "moves_per_chain": GCMC_MOVES, "ms": secs * 1e3,
+           "workload": "CO2 (rigid 3-site), 300 K, 1e5 Pa, 2x2x3 box of the charged framework, FP32C grids, "
+                       "Ewald alpha 0.265 kmax 8 (1152 k), translation/rotation/CBMC swap 1:1:1, 10+10 trials",
+           "mean_loading": mean_n, "n_kvectors": ew.n_kvectors,
+           "e2e": {"value": world * chains * GCMC_MOVES / e2e_secs, "unit": "MC move attempts/s",
+                   "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": chains * 8 * 24 + chains * 12}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_gcmc_rate(ff, cell, scell, sfw, dims, grids, outs, args.cpu_seconds)
+    g.close()
+    ew.close()
+    sysg.close()
+    return out
+
+
+def cpu_gcmc_rate(ff, cell, scell, sfw, dims, grids, outs, target_seconds):
+    """The oracle GCMC (the reference's moves restated) on all host cores, one chain per core, same grids."""
+    import oracle
+    from raspa3_b200.gcmc import beta_of, co2_component, fugacity_of
+
+    threads = os.cpu_count() or 1
+    host_grids = [None] * (ff.n_types + 1)
+    for (name, gt, probe), out in zip(grids, outs):
+        host_grids[probe if gt == 0 else ff.n_types] = out.cpu().numpy()
+    s_fw = oracle.ewald_rigid(ff, scell, sfw)
+    kw = dict(grids=host_grids, grid_dims=dims, grid_cell=cell, s_framework=s_fw, threads=threads)
+    _, t0 = oracle.gcmc_run(ff, scell, co2_component(), beta_of(300.0), fugacity_of(1e5), n_chains=threads,
+                            steps=200, equilibration=0, seed=3, **kw)
+    steps = int(max(200, 200 * target_seconds / max(t0, 1e-3)))
+    _, t1 = oracle.gcmc_run(ff, scell, co2_component(), beta_of(300.0), fugacity_of(1e5), n_chains=threads,
+                            steps=steps, equilibration=0, seed=4, **kw)
+    return {"value": threads * steps / t1, "unit": "MC move attempts/s", "cores": threads, "kind": "port",
+            "sample": f"{threads} chains x {steps} moves from an empty box in {t1:.1f} s (FP64 oracle GCMC, one chain "
+                      f"per thread)"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -199,19 +287,27 @@ def run_ours(args):
     outs = [torch.empty(8 * npts, dtype=torch.float64, device="cuda") for _ in grids]
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
-    def build(gi, out_device=None, out_host=None, count=False):
-        _, gt, probe = grids[gi]
-        return ctx.grid_build(gt, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP32C,
-                              out_device=out_device, host=out_host is not None, out_host=out_host,
-                              count_pairs=count)
+    # one step = two calls of the grid-set entry point: the two Lennard-Jones grids (one two-probe kernel) and the
+    # unit-charge Ewald grid
+    calls = [[0, 1], [2]]
+    call_names = ["LJ C_co2+O_co2 (two-probe kernel)", "Ewald-real"]
+
+    def build_call(ci, out_host=None, count=False):
+        idx = calls[ci]
+        return ctx.grid_build_set(ff, cell, atoms, 12.0, dims, native.PRECISION_FP32C, [grids[g][1] for g in idx],
+                                  [grids[g][2] for g in idx], [outs[g].data_ptr() for g in idx], count_pairs=count,
+                                  out_host=None if out_host is None else [out_host[g] for g in idx])
 
     # work per grid (pair counts) outside the timed region
-    stats = [build(g, out_device=outs[g].data_ptr(), count=True)[1] for g in range(len(grids))]
+    stats = [None] * len(grids)
+    for ci, idx in enumerate(calls):
+        for g, st in zip(idx, build_call(ci, count=True)):
+            stats[g] = st
     peak_fp32 = ctx.probe_fma_peak(native.PRECISION_FP32C)
 
     for _ in range(args.warmup):
-        for g in range(len(grids)):
-            build(g, out_device=outs[g].data_ptr())
+        for ci in range(len(calls)):
+            build_call(ci)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -220,17 +316,17 @@ def run_ours(args):
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(grids) + 1)] for _ in range(args.steps)]
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(calls) + 1)] for _ in range(args.steps)]
     for s in range(args.steps):
         flush.zero_()
         ev[s][0].record(stream)
-        for g in range(len(grids)):
-            build(g, out_device=outs[g].data_ptr())
-            ev[s][g + 1].record(stream)
+        for ci in range(len(calls)):
+            build_call(ci)
+            ev[s][ci + 1].record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
     step_ms = [ev[s][0].elapsed_time(ev[s][-1]) for s in range(args.steps)]
-    kern_ms = [[ev[s][g].elapsed_time(ev[s][g + 1]) for s in range(args.steps)] for g in range(len(grids))]
+    kern_ms = [[ev[s][c].elapsed_time(ev[s][c + 1]) for s in range(args.steps)] for c in range(len(calls))]
     total_s = sum(step_ms) / 1e3
     if world > 1:
         t = torch.tensor([total_s], dtype=torch.float64, device="cuda")
@@ -246,13 +342,15 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     h2d = d2h = 0
+    all_idx = list(range(len(grids)))
     t0 = time.perf_counter()
     for s in range(e2e_steps):
-        for g in range(len(grids)):
-            _, st = build(g, out_host=host_np[g], count=(s == 0))
-            if s == 0:
-                h2d += st["h2d_bytes"]
-                d2h += st["d2h_bytes"]
+        st = ctx.grid_build_set(ff, cell, atoms, 12.0, dims, native.PRECISION_FP32C, [g[1] for g in grids],
+                                [g[2] for g in grids], [outs[g].data_ptr() for g in all_idx], count_pairs=(s == 0),
+                                out_host=host_np)
+        if s == 0:
+            h2d = sum(x["h2d_bytes"] for x in st)
+            d2h = sum(x["d2h_bytes"] for x in st)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if world > 1:
@@ -261,15 +359,16 @@ def run_ours(args):
         e2e_s = float(t.item())
     e2e_value = world * len(grids) * npts * e2e_steps / e2e_s
 
-    # roofline of the dominant kernel
+    # roofline of the dominant kernel: algorithmic FLOPs = in-cutoff pairs x FLOPs per pair, per grid built
     mean_ms = [statistics.mean(k) for k in kern_ms]
+    call_flops = [sum(stats[g]["pair_count"] * FLOPS_PER_PAIR["ewald" if grids[g][1] == 1 else "lj"] for g in idx)
+                  for idx in calls]
     dom = int(np.argmax(mean_ms))
-    kind = "ewald" if grids[dom][1] == 1 else "lj"
-    achieved = stats[dom]["pair_count"] * FLOPS_PER_PAIR[kind] / (mean_ms[dom] * 1e-3) / 1e12
+    achieved = call_flops[dom] / (mean_ms[dom] * 1e-3) / 1e12
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "grid_build_config2_traffic.json")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(grids[dom][0])
+        traffic = json.load(open(tpath)).get(call_names[dom])
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -280,19 +379,24 @@ def run_ours(args):
                    "framework_atoms": int(len(atoms)), "cutoff": 12.0, "precision": "FP32 pairs, compensated FP32 "
                    "accumulation, FP64 epilogue", "l2": "256 MiB flush between timed steps; 302 MB output per step",
                    "parallelism": f"replicas x{world}"},
-        "kernels": {grids[g][0]: {"ms": mean_ms[g], "pairs": stats[g]["pair_count"], "images": stats[g]["n_images"],
-                                  "tflops": stats[g]["pair_count"] * FLOPS_PER_PAIR["ewald" if grids[g][1] == 1
-                                                                                   else "lj"] / (mean_ms[g] * 1e-3) / 1e12}
-                    for g in range(len(grids))},
-        "roofline": {"kernel": f"gridKernel<float> ({grids[dom][0]})", "bound": "fp32", "achieved": achieved,
+        "kernels": {call_names[c]: {"ms": mean_ms[c], "grids": [grids[g][0] for g in calls[c]],
+                                    "pairs_per_grid": stats[calls[c][0]]["pair_count"],
+                                    "images": stats[calls[c][0]]["n_images"],
+                                    "tflops": call_flops[c] / (mean_ms[c] * 1e-3) / 1e12}
+                    for c in range(len(calls))},
+        "roofline": {"kernel": f"gridKernel<float> ({call_names[dom]})", "bound": "fp32", "achieved": achieved,
                      "peak": peak_fp32, "unit": "TFLOP/s", "frac": achieved / peak_fp32, "traffic": traffic,
                      "peak_source": "rg_probe_fma_peak: FP32 FMA chains on all SMs, measured in this run",
-                     "flops_per_pair": FLOPS_PER_PAIR[kind]},
+                     "flops_per_pair": FLOPS_PER_PAIR},
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "steps": e2e_steps, "path": "rg_grid_build with pinned host output"},
-        "gpu_launches": len(grids) * args.steps,
+                "steps": e2e_steps, "path": "rg_grid_build_set with pinned host outputs"},
+        "gpu_launches": len(calls) * args.steps,
     }
+    # ---- GCMC steps/s on the same workload: CO2 in the 2x2x3 simulation box, the FP32C grids just built ----
+    if not args.no_gcmc:
+        line["gcmc"] = run_gcmc(args, ctx, ff, cell, atoms, dims, grids, outs, world, rank, dist, torch)
+
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, pts, secs, threads = cpu_oracle_rate(ff, cell, atoms, dims, grids, args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",

@@ -78,6 +78,8 @@ typedef struct rg_forcefield
 typedef struct rg_ctx rg_ctx;
 typedef struct rg_system rg_system; /* device-resident framework, grids, adsorbates and pair table of one system */
 typedef struct rg_ewald rg_ewald;   /* device-resident k-vectors, prefactors and structure factors of one system */
+typedef struct rg_mlp rg_mlp;       /* the learned proposal's network: parameters and optimizer state on the device */
+typedef struct rg_proposal rg_proposal; /* a tabulated, exactly normalised first-bead proposal density */
 
 /* ---- context ---- */
 rg_status rg_ctx_create(int device, rg_ctx** out);
@@ -128,6 +130,16 @@ typedef struct rg_grid_stats
 rg_status rg_grid_build(rg_ctx* ctx, int grid_type, const rg_forcefield* ff, const rg_box* unit_cell,
                         const rg_atom* unit_atoms, int n_unit_atoms, int probe_type, double cutoff, int nx, int ny,
                         int nz, int precision, double* out_device, double* out_host, rg_grid_stats* stats);
+
+/* Several grids of one framework in one call, replacing the grid loop of System::createFrameworkInterpolationGrids
+ * (src/raspakit/system_interpolation_grids.cpp:202-238): grid g has type grid_types[g], probe probe_types[g] and goes
+ * to the device buffer out_device[g] (8*nx*ny*nz doubles each) and, if out_host and out_host[g] are non-NULL, to that
+ * host buffer too (the call then returns after the copies). Lennard-Jones grids whose probes see the same framework
+ * atoms are computed two at a time in one pass over the candidate atoms. stats: n_grids entries or NULL. */
+rg_status rg_grid_build_set(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* unit_cell, const rg_atom* unit_atoms,
+                            int n_unit_atoms, double cutoff, int nx, int ny, int nz, int precision, int n_grids,
+                            const int* grid_types, const int* probe_types, double* const* out_device,
+                            double* const* out_host, rg_grid_stats* stats);
 
 /* Grid build that allocates nothing, for callers that cannot allocate device memory: applications whose device memory
  * is owned by another allocator (a host framework that reserves the whole device up front, or a memory pool with a hard
@@ -230,6 +242,42 @@ rg_status rg_gcmc_run(rg_gcmc* gcmc, int64_t moves, int record);
 rg_status rg_gcmc_results(rg_gcmc* gcmc, rg_gcmc_chain_result* out);
 /* Positions (x, y, z per atom, molecules consecutive) of one chain, for recomputation checks. */
 rg_status rg_gcmc_get_positions(rg_gcmc* gcmc, int chain, double* xyz, int capacity_atoms, int* n_molecules);
+
+/* Uses a learned first-bead proposal for the CBMC insertion and deletion trials of every chain (NULL: back to uniform
+ * positions). The trial weights become exp(-beta U) / q with q the proposal density relative to uniform; the
+ * acceptance rules are unchanged, so the sampled ensemble is the same. The simulation box must be an integer
+ * replication of unit_cell, the cell the proposal is defined on. No counterpart in the reference. */
+rg_status rg_gcmc_set_proposal(rg_gcmc* gcmc, rg_proposal* proposal, const rg_box* unit_cell);
+
+/* ---- learned first-bead proposal (no counterpart in the reference; plugs into the uniform first-bead sampling of
+ * CBMC::growMoleculeMultipleFirstBeadSwapInsertion, src/raspakit/cbmc/multiple_first_bead.cpp:23-27) ---- */
+/* A Fourier-feature MLP (96 inputs: sin, cos of 2 pi n s_a, n = 1..16, a = x, y, z; 2 SiLU layers of 64; 1 output,
+ * 10,433 FP32 parameters) with He-uniform initial weights from `seed`. */
+rg_status rg_mlp_create(rg_ctx* ctx, uint64_t seed, rg_mlp** out);
+rg_status rg_mlp_destroy(rg_mlp* mlp);
+int32_t rg_mlp_num_params(void);
+/* Parameter vector order: W1 (64x96 row-major), b1, W2 (64x64), b2, w3 (64), b3. */
+rg_status rg_mlp_get_params(rg_mlp* mlp, float* host, int32_t n);
+rg_status rg_mlp_set_params(rg_mlp* mlp, const float* host, int32_t n);
+/* Loss (1/n) sum (f(s_i) - t_i)^2 and its gradient over n samples (device arrays s: 3 per sample, t: 1). */
+rg_status rg_mlp_loss_and_gradient(rg_mlp* mlp, const float* s_device, const float* target_device, int32_t n,
+                                   float* loss, float* grad_host);
+/* `steps` Adam steps on random minibatches of `batch` samples drawn from the n_samples device arrays. */
+rg_status rg_mlp_train(rg_mlp* mlp, const float* s_device, const float* target_device, int64_t n_samples,
+                       int32_t steps, int32_t batch, float learning_rate, uint64_t seed, float* final_loss);
+/* f(s) for n fractional positions (device arrays). */
+rg_status rg_mlp_evaluate(rg_mlp* mlp, const float* s_device, int64_t n, float* out_device);
+/* Training data: n uniform fractional positions s of the unit cell and targets t = max(-beta U(s), t_min) with U the
+ * framework energy of one bead of pseudo-atom type `pseudo_atom` and charge `charge` from the system's grids. */
+rg_status rg_proposal_sample_targets(rg_system* system, int pseudo_atom, double charge, double beta, double t_min,
+                                     const rg_box* unit_cell, int64_t n, uint64_t seed, float* s_device,
+                                     float* t_device);
+/* Tabulates exp(f) over cells_per_axis^3 cells of the unit cell into an exactly normalised density mixed with the
+ * uniform density (weight eps_uniform > 0, so q > 0 everywhere). */
+rg_status rg_proposal_create(rg_mlp* mlp, int32_t cells_per_axis, double eps_uniform, rg_proposal** out);
+rg_status rg_proposal_destroy(rg_proposal* proposal);
+/* The density relative to uniform at n fractional positions (host arrays, 3 per position). */
+rg_status rg_proposal_density(rg_proposal* proposal, const double* s, int64_t n, double* q_out);
 
 /* ---- (c) Ewald Fourier energy of a move ---- */
 /* The Ewald part of RunningEnergy (src/raspakit/running_energy.ixx:500-540) in internal units. */

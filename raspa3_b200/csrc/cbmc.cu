@@ -260,14 +260,20 @@ rg_status rg_system_create(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* b
     tab[2 * n * n + i] = ff->shift[i];
     lj[i] = ff->lj[i];
   }
+  // all copies on the context stream, synchronised before returning (the legacy default stream does not order with it)
   cudaError_t err = cudaMalloc(reinterpret_cast<void**>(&s->tables), sizeof(double) * 3 * n * n + sizeof(int) * n * n);
-  if (!err) err = cudaMemcpy(s->tables, tab.data(), sizeof(double) * 3 * n * n, cudaMemcpyHostToDevice);
-  if (!err) err = cudaMemcpy(s->tables + 3 * n * n, lj.data(), sizeof(int) * n * n, cudaMemcpyHostToDevice);
+  if (!err)
+    err = cudaMemcpyAsync(s->tables, tab.data(), sizeof(double) * 3 * n * n, cudaMemcpyHostToDevice, ctx->stream);
+  if (!err)
+    err = cudaMemcpyAsync(s->tables + 3 * n * n, lj.data(), sizeof(int) * n * n, cudaMemcpyHostToDevice, ctx->stream);
   if (!err && n_framework_atoms > 0)
   {
     err = cudaMalloc(reinterpret_cast<void**>(&s->fw), sizeof(rg_atom) * n_framework_atoms);
-    if (!err) err = cudaMemcpy(s->fw, framework_atoms, sizeof(rg_atom) * n_framework_atoms, cudaMemcpyHostToDevice);
+    if (!err)
+      err = cudaMemcpyAsync(s->fw, framework_atoms, sizeof(rg_atom) * n_framework_atoms, cudaMemcpyHostToDevice,
+                            ctx->stream);
   }
+  if (!err) err = cudaStreamSynchronize(ctx->stream);
   if (!err) err = cudaMallocHost(reinterpret_cast<void**>(&s->trials_host), sizeof(rg_atom) * 4096);
   if (!err) err = cudaMallocHost(reinterpret_cast<void**>(&s->out_host), sizeof(rg_trial_energy) * 4096);
   if (err)
@@ -346,7 +352,8 @@ rg_status rg_system_set_grid(rg_system* s, int index, const rg_box* unit_cell, i
   {
     RG_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&s->grids[index]), bytes));
     s->grid_owned[index] = 1;
-    RG_CUDA(ctx, cudaMemcpy(s->grids[index], data, bytes, cudaMemcpyHostToDevice));
+    RG_CUDA(ctx, cudaMemcpyAsync(s->grids[index], data, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   rg::HostBox hb = rg::makeHostBox(unit_cell);
   for (int c = 0; c < 3; ++c)
@@ -365,6 +372,7 @@ rg_status rg_system_set_molecules(rg_system* s, const rg_atom* atoms, int n)
   rg_status st = growDevice(ctx, &s->mol, &s->mol_cap, n > 0 ? n : 1);
   if (st) return st;
   if (n > 0) RG_CUDA(ctx, cudaMemcpyAsync(s->mol, atoms, sizeof(rg_atom) * n, cudaMemcpyHostToDevice, ctx->stream));
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // the caller's atom buffer is pageable
   s->n_mol = n;
   return RG_OK;
 }

@@ -62,6 +62,15 @@ struct Params
   const char4* kvec;
   const double* temp;
   unsigned long long seed;
+  // learned first-bead proposal (null: uniform): inclusive cumulative cell probabilities and the density relative to
+  // uniform, over G^3 cells of the unit cell; the simulation box is rep[0] x rep[1] x rep[2] unit cells
+  const double* prop_cdf;
+  const double* prop_q;
+  int prop_G;
+  double prop_eps;
+  double uc[3][3];   // unit cell c[col][row]
+  double uic[3][3];  // its inverse
+  int rep[3];
   // per-chain state
   double4* pos;              // [chain][capacity * n_atoms]
   double2* sk;               // [chain][nk] structure factors (framework included)
@@ -109,8 +118,8 @@ enum Slot
   kSlotPick = 1,       // (molecule, direction)
   kSlotChange = 2,     // (displacement or angle, acceptance)
   kSlotSelect = 3,     // (first-bead selection, orientation selection)
-  kSlotFirst = 16,     // + 2 t: first-bead position t (3 numbers)
-  kSlotOrient = 64     // + 2 t: orientation t (3 numbers)
+  kSlotFirst = 16,     // + 4 t: first-bead position t (up to 8 numbers)
+  kSlotOrient = 128    // + 2 t: orientation t (3 numbers)
 };
 
 __device__ __forceinline__ void rotationFromUniforms(double u1, double u2, double u3, double R[3][3])
@@ -134,6 +143,7 @@ struct Shared
   double trial[kMaxTrials][kMaxAtoms][3];  // positions of the trial sets
   double setE[kMaxTrials];
   int setOv[kMaxTrials];
+  double logq[kMaxTrials];
   double newPos[kMaxAtoms][3];
   double oldPos[kMaxAtoms][3];
   double red[kWarps];
@@ -278,14 +288,15 @@ __device__ void blockAcceptEwald(const Params& p, int chain)
 
 // CBMC::selectTrialPosition (cbmc/util.cpp:14-47) over the non-overlapping trials; returns the chosen trial index and
 // the Rosenbluth weight sum_i exp(-beta U_i) / k, or -1 if every trial overlaps.
-__device__ int selectTrial(const double* E, const int* ov, int k, double beta, double u, double* W)
+// With a proposal density, trial t's log weight is -beta U_t - log q_t (logq may be null: uniform, q = 1).
+__device__ int selectTrial(const double* E, const int* ov, const double* logq, int k, double beta, double u, double* W)
 {
   double largest = -1e300;
   bool any = false;
   for (int t = 0; t < k; ++t)
     if (!ov[t])
     {
-      largest = fmax(largest, -beta * E[t]);
+      largest = fmax(largest, -beta * E[t] - (logq ? logq[t] : 0.0));
       any = true;
     }
   if (!any)
@@ -297,8 +308,9 @@ __device__ int selectTrial(const double* E, const int* ov, int k, double beta, d
   for (int t = 0; t < k; ++t)
     if (!ov[t])
     {
-      sum += exp(-beta * E[t] - largest);
-      w += exp(-beta * E[t]);
+      const double lw = -beta * E[t] - (logq ? logq[t] : 0.0);
+      sum += exp(lw - largest);
+      w += exp(lw);
     }
   *W = w / static_cast<double>(k);
   const double ws = u * sum;
@@ -307,20 +319,33 @@ __device__ int selectTrial(const double* E, const int* ov, int k, double beta, d
   for (int t = 0; t < k; ++t)
   {
     if (ov[t]) continue;
+    const double lw = -beta * E[t] - (logq ? logq[t] : 0.0);
     if (first < 0)
     {
       first = t;
       selected = t;
-      cumw = exp(-beta * E[t] - largest);
+      cumw = exp(lw - largest);
       continue;
     }
     if (cumw < ws)
     {
-      cumw += exp(-beta * E[t] - largest);
+      cumw += exp(lw - largest);
       selected = t;
     }
   }
   return selected;
+}
+
+// Proposal density (relative to uniform) of a position: the cell of its unit-cell fractional coordinates.
+__device__ __forceinline__ double proposalDensity(const Params& p, const double r[3])
+{
+  int c[3];
+  for (int a = 0; a < 3; ++a)
+  {
+    const double s = rgd::fract1(p.uic[0][a] * r[0] + p.uic[1][a] * r[1] + p.uic[2][a] * r[2]);
+    c[a] = min(p.prop_G - 1, static_cast<int>(s * p.prop_G));
+  }
+  return p.prop_q[c[0] + p.prop_G * (c[1] + p.prop_G * c[2])];
 }
 
 extern __shared__ double2 gcmcDyn[];
@@ -441,12 +466,43 @@ __global__ void __launch_bounds__(kThreads) gcmcKernel(Params p, long long move0
             sh.trial[0][0][2] = o.z;
             continue;
           }
-          const double2 a = uniform2(p.seed, chain, mv, kSlotFirst + 2 * t);
-          const double2 b = uniform2(p.seed, chain, mv, kSlotFirst + 2 * t + 1);
-          const double s0 = a.x, s1 = a.y, s2 = b.x;
-          for (int r = 0; r < 3; ++r) sh.trial[t][0][r] = p.box.c[0][r] * s0 + p.box.c[1][r] * s1 + p.box.c[2][r] * s2;
+          const double2 a = uniform2(p.seed, chain, mv, kSlotFirst + 4 * t);
+          const double2 b = uniform2(p.seed, chain, mv, kSlotFirst + 4 * t + 1);
+          const double2 u = uniform2(p.seed, chain, mv, kSlotFirst + 4 * t + 2);
+          if (!p.prop_cdf || u.x < p.prop_eps)
+          {
+            // SimulationBox::randomPosition (simulationbox.cpp:132-135)
+            const double s0 = a.x, s1 = a.y, s2 = b.x;
+            for (int r = 0; r < 3; ++r)
+              sh.trial[t][0][r] = p.box.c[0][r] * s0 + p.box.c[1][r] * s1 + p.box.c[2][r] * s2;
+          }
+          else
+          {
+            // a cell of the tabulated proposal (binary search of the cumulative probabilities), a uniform point in
+            // it, and a uniformly chosen unit-cell replica of the simulation box
+            const double2 v = uniform2(p.seed, chain, mv, kSlotFirst + 4 * t + 3);
+            const int G = p.prop_G;
+            const int ncell = G * G * G;
+            int lo = 0, hi = ncell - 1;
+            while (lo < hi)
+            {
+              const int mid = (lo + hi) >> 1;
+              if (p.prop_cdf[mid] < u.y)
+                lo = mid + 1;
+              else
+                hi = mid;
+            }
+            const int ci = lo % G, cj = (lo / G) % G, ck = lo / (G * G);
+            const double sf[3] = {(ci + a.x) / G + static_cast<double>(min(p.rep[0] - 1, static_cast<int>(b.y * p.rep[0]))),
+                                  (cj + a.y) / G + static_cast<double>(min(p.rep[1] - 1, static_cast<int>(v.x * p.rep[1]))),
+                                  (ck + b.x) / G + static_cast<double>(min(p.rep[2] - 1, static_cast<int>(v.y * p.rep[2])))};
+            for (int r = 0; r < 3; ++r)
+              sh.trial[t][0][r] = p.uc[0][r] * sf[0] + p.uc[1][r] * sf[1] + p.uc[2][r] * sf[2];
+          }
         }
         __syncthreads();
+        for (int t = threadIdx.x; t < p.k1; t += blockDim.x)
+          sh.logq[t] = p.prop_cdf ? log(proposalDensity(p, sh.trial[t][0])) : 0.0;
         int one[1] = {sb};
         for (int t = warp; t < p.k1; t += kWarps)
         {
@@ -462,7 +518,7 @@ __global__ void __launch_bounds__(kThreads) gcmcKernel(Params p, long long move0
         if (threadIdx.x == 0)
         {
           double W1;
-          int sel = selectTrial(sh.setE, sh.setOv, p.k1, p.beta, uSel.x, &W1);
+          int sel = selectTrial(sh.setE, sh.setOv, sh.logq, p.k1, p.beta, uSel.x, &W1);
           if (retrace) sel = sh.setOv[0] ? -1 : 0;
           sh.ints[0] = sel;
           sh.dbl[0] = W1;
@@ -526,7 +582,7 @@ __global__ void __launch_bounds__(kThreads) gcmcKernel(Params p, long long move0
           if (threadIdx.x == 0)
           {
             double W2;
-            int sel = selectTrial(sh.setE, sh.setOv, p.k2, p.beta, uSel.y, &W2);
+            int sel = selectTrial(sh.setE, sh.setOv, nullptr, p.k2, p.beta, uSel.y, &W2);
             if (retrace) sel = sh.setOv[0] ? -1 : 0;
             sh.ints[1] = sel;
             sh.dbl[5] = W2;
@@ -831,4 +887,48 @@ rg_status rg_gcmc_get_positions(rg_gcmc* g, int chain, double* xyz, int capacity
   *n_molecules = n;
   return RG_OK;
 }
+}
+
+extern "C" rg_status rg_gcmc_set_proposal(rg_gcmc* g, rg_proposal* proposal, const rg_box* unit_cell)
+{
+  if (!g) return RG_ERR_INVALID_ARGUMENT;
+  Params& p = g->p;
+  if (!proposal)
+  {
+    p.prop_cdf = nullptr;
+    p.prop_q = nullptr;
+    return RG_OK;
+  }
+  if (!unit_cell) return RG_ERR_INVALID_ARGUMENT;
+  rg_status st = rgd::proposalExport(proposal, &p.prop_cdf, &p.prop_q, &p.prop_G, &p.prop_eps);
+  if (st) return st;
+  const rg::HostBox ub = rg::makeHostBox(unit_cell);
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+    {
+      p.uc[a][b] = ub.c[a][b];
+      p.uic[a][b] = ub.ic[a][b];
+    }
+  // the simulation box must be an integer replication of the unit cell along each lattice vector
+  for (int d = 0; d < 3; ++d)
+  {
+    double ratio = 0.0, n2 = 0.0;
+    for (int r = 0; r < 3; ++r)
+    {
+      ratio += p.box.c[d][r] * ub.c[d][r];
+      n2 += ub.c[d][r] * ub.c[d][r];
+    }
+    ratio /= n2;
+    const int rep = static_cast<int>(std::lround(ratio));
+    double err = 0.0;
+    for (int r = 0; r < 3; ++r) err += std::fabs(p.box.c[d][r] - rep * ub.c[d][r]);
+    if (rep < 1 || err > 1e-6)
+    {
+      p.prop_cdf = nullptr;
+      p.prop_q = nullptr;
+      return rg::fail(g->ctx, RG_ERR_INVALID_ARGUMENT, "rg_gcmc_set_proposal: box is not a replication of the unit cell");
+    }
+    p.rep[d] = rep;
+  }
+  return RG_OK;
 }

@@ -41,17 +41,47 @@ struct GridParams
   double coul;
   double overlap;
   unsigned long long* pair_count;
-  double* out;
+  double* out[2];  // one output grid per Lennard-Jones probe sharing the candidate set (out[0] otherwise)
 };
 
 __device__ __forceinline__ double rcpRn(double x) { return __drcp_rn(x); }
-__device__ __forceinline__ float rcpRn(float x) { return __frcp_rn(x); }
+// FP32 reciprocal: the hardware approximation refined by one Newton step (x (2 - a x)), ~0.5 ulp
+__device__ __forceinline__ float rcpRn(float a)
+{
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  const float e = fmaf(-a, r, 1.0f);
+  return fmaf(r, e, r);
+}
+// FP32 reciprocal square root, refined by one Newton step (r (3 - a r^2) / 2)
+__device__ __forceinline__ float rsqrtRn(float a)
+{
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  const float h = 0.5f * a * r;
+  return r * fmaf(-h, r, 1.5f);
+}
+// erfc(x) = exp(-x^2) R(x) for 0 <= x <= 4, with R(x) = exp(x^2) erfc(x) fitted (weighted least squares in Chebyshev
+// form, relative error 4e-8 in FP64, ~2 ulp in FP32) as a degree-9 polynomial in t = 1 / (1 + x/2); the caller passes
+// exp(-x^2), which the derivative factors need anyway.
+__device__ __forceinline__ float erfcFromExp(float x, float expmx2)
+{
+  const float t = rcpRn(fmaf(0.5f, x, 1.0f));
+  float r = -0.02496027760207653f;
+  r = fmaf(r, t, 0.09420006722211838f);
+  r = fmaf(r, t, -0.024484887719154358f);
+  r = fmaf(r, t, -0.36430737376213074f);
+  r = fmaf(r, t, 0.534475564956665f);
+  r = fmaf(r, t, -0.11705945432186127f);
+  r = fmaf(r, t, 0.3620023727416992f);
+  r = fmaf(r, t, 0.25453805923461914f);
+  r = fmaf(r, t, 0.2858136296272278f);
+  r = fmaf(r, t, -0.00021772264153696597f);
+  return expmx2 * r;
+}
 __device__ __forceinline__ double sqrtT(double x) { return sqrt(x); }
-__device__ __forceinline__ float sqrtT(float x) { return sqrtf(x); }
 __device__ __forceinline__ double erfcT(double x) { return erfc(x); }
-__device__ __forceinline__ float erfcT(float x) { return erfcf(x); }
 __device__ __forceinline__ double expT(double x) { return exp(x); }
-__device__ __forceinline__ float expT(float x) { return expf(x); }
 
 template <typename Real>
 struct Factor
@@ -87,10 +117,14 @@ __device__ __forceinline__ Factor<Real> ljFactor(Real rr, Real a1, Real s2, Real
   }
   else
   {
-    f.e = a1 * (t6 - t3) - shift;
-    f.f1 = Real(-6) * a1 * (Real(2) * t6 - t3) * inv;
-    f.f2 = Real(24) * a1 * (Real(7) * t6 - Real(2) * t3) * inv2;
-    f.f3 = Real(-96) * a1 * (Real(28) * t6 - Real(5) * t3) * inv3;
+    // with A = 4 eps t3 and B = 4 eps t6: U = B - A - shift, F1 = (6A - 12B)/r^2, F2 = (168B - 48A)/r^4,
+    // F3 = (480A - 2688B)/r^6 (the reference's factors, tricubic_derivative_lj.ixx:38-45, regrouped)
+    const Real A = a1 * t3;
+    const Real B = A * t3;
+    f.e = B - A - shift;
+    f.f1 = (Real(6) * A - Real(12) * B) * inv;
+    f.f2 = (Real(168) * B - Real(48) * A) * inv2;
+    f.f3 = (Real(480) * A - Real(2688) * B) * inv3;
   }
   return f;
 }
@@ -98,8 +132,34 @@ __device__ __forceinline__ Factor<Real> ljFactor(Real rr, Real a1, Real s2, Real
 // potentialRealEwaldTricubicDerivative with q_A = 1 (src/raspakit/potentials/interpolation/
 // tricubic_derivative_real_ewald.ixx:32-56); cq = CoulombicConversionFactor * q_B.
 template <typename Real>
-__device__ __forceinline__ Factor<Real> ewaldFactor(Real rr, Real cq, Real alpha)
+__device__ __forceinline__ Factor<Real> ewaldFactor(Real rr, Real cq, Real alpha);
+
+// FP32: 1/r from one reciprocal square root, erfc from the shared exp(-alpha^2 r^2)
+template <>
+__device__ __forceinline__ Factor<float> ewaldFactor<float>(float rr, float cq, float alpha)
 {
+  const float invr = rsqrtRn(rr);
+  const float r = rr * invr;
+  const float ex = expf(-alpha * alpha * rr);
+  const float ec = erfcFromExp(alpha * r, ex);
+  const float etr = 2.0f * alpha * r * ex * 0.564189583547756286948079451560772586f;
+  const float ar2 = alpha * alpha * rr;
+  const float invrr = invr * invr;
+  const float i3 = invr * invrr;
+  const float i5 = i3 * invrr;
+  const float i7 = i5 * invrr;
+  Factor<float> f;
+  f.e = cq * ec * invr;
+  f.f1 = -cq * (etr + ec) * i3;
+  f.f2 = cq * (etr * (2.0f * ar2 + 3.0f) + 3.0f * ec) * i5;
+  f.f3 = -cq * (etr * (4.0f * ar2 * ar2 + 10.0f * ar2 + 15.0f) + 15.0f * ec) * i7;
+  return f;
+}
+
+template <>
+__device__ __forceinline__ Factor<double> ewaldFactor<double>(double rr, double cq, double alpha)
+{
+  using Real = double;
   Real r = sqrtT(rr);
   Real ec = erfcT(alpha * r);
   Real ex = expT(-alpha * alpha * rr);
@@ -201,7 +261,9 @@ __device__ __forceinline__ int sym2(int i, int j)
   return table[a * 3 + b];
 }
 
-template <typename Real, int TYPE, bool TRICLINIC, bool COUNT>
+// NP Lennard-Jones probes (1 or 2) share one candidate set: the distances, the reciprocal and the staging are computed
+// once per pair and each probe adds its own factors (ipar holds NP parameter sets per image).
+template <typename Real, int TYPE, bool TRICLINIC, bool COUNT, int NP>
 __global__ void __launch_bounds__(256) gridKernel(GridParams p, const double4* __restrict__ ipos,
                                                   const double4* __restrict__ ipar, int bx, int by, int bz)
 {
@@ -212,8 +274,8 @@ __global__ void __launch_bounds__(256) gridKernel(GridParams p, const double4* _
   const int nt = blockDim.x;
   const int chunk = nt * kPer;
   V4* cpos = reinterpret_cast<V4*>(smem_raw);
-  V4* cpar = cpos + chunk;
-  float4* clo = reinterpret_cast<float4*>(cpar + chunk);  // FP32C only: low parts of the candidate coordinates
+  V4* cpar = cpos + chunk;                                     // NP * chunk parameter sets
+  float4* clo = reinterpret_cast<float4*>(cpar + NP * chunk);  // FP32C only: low parts of the candidate coordinates
   __shared__ int warp_sums[33];
 
   const int tid = threadIdx.x;
@@ -245,8 +307,9 @@ __global__ void __launch_bounds__(256) gridKernel(GridParams p, const double4* _
   const Real rc2 = static_cast<Real>(p.rc2);
   const Real alpha = static_cast<Real>(p.alpha);
 
-  typename AccOf<Real, NCH>::T acc;
-  acc.init();
+  typename AccOf<Real, NCH>::T accs[NP];
+#pragma unroll
+  for (int q = 0; q < NP; ++q) accs[q].init();
   unsigned long long npairs = 0;
 
   for (int base = 0; base < p.n_images; base += chunk)
@@ -289,13 +352,17 @@ __global__ void __launch_bounds__(256) gridKernel(GridParams p, const double4* _
                                  static_cast<float>(rz - static_cast<double>(c.z)), 0.0f);
         if (!EWALD)
         {
-          double4 q = ipar[idx];
-          V4 pr;
-          pr.x = static_cast<Real>(q.x);
-          pr.y = static_cast<Real>(q.y);
-          pr.z = static_cast<Real>(q.z);
-          pr.w = Real(0);
-          cpar[off] = pr;
+#pragma unroll
+          for (int q = 0; q < NP; ++q)
+          {
+            const double4 pq = ipar[static_cast<long long>(idx) * NP + q];
+            V4 pr;
+            pr.x = static_cast<Real>(pq.x);
+            pr.y = static_cast<Real>(pq.y);
+            pr.z = static_cast<Real>(pq.z);
+            pr.w = Real(0);
+            cpar[q * chunk + off] = pr;
+          }
         }
         ++off;
       }
@@ -323,49 +390,55 @@ __global__ void __launch_bounds__(256) gridKernel(GridParams p, const double4* _
       rr = rr > Real(0.1) ? rr : Real(0.1);
       if (rr < rc2)
       {
-        Factor<Real> f;
-        if constexpr (EWALD)
-          f = ewaldFactor<Real>(rr, a.w, alpha);
-        else
-        {
-          V4 q = cpar[c];
-          f = ljFactor<TYPE, Real>(rr, q.x, q.y, q.z);
-        }
         if (COUNT && valid) ++npairs;
-        acc.add(0, f.e);
-        if constexpr (!TRICLINIC)
+#pragma unroll
+        for (int q = 0; q < NP; ++q)
         {
-          acc.add(1, dx * f.f1);
-          acc.add(2, dy * f.f1);
-          acc.add(3, dz * f.f1);
-          acc.add(4, f.f2 * dx * dy);
-          acc.add(5, f.f2 * dx * dz);
-          acc.add(6, f.f2 * dy * dz);
-          acc.add(7, f.f3 * dx * dy * dz);
-        }
-        else
-        {
-          // full Cartesian tensors (framework_molecule_grid.cpp:76-144), symmetric storage
-          const Real d[3] = {dx, dy, dz};
-          acc.add(1, dx * f.f1);
-          acc.add(2, dy * f.f1);
-          acc.add(3, dz * f.f1);
+          Factor<Real> f;
+          if constexpr (EWALD)
+            f = ewaldFactor<Real>(rr, a.w, alpha);
+          else
+          {
+            V4 pq = cpar[q * chunk + c];
+            f = ljFactor<TYPE, Real>(rr, pq.x, pq.y, pq.z);
+          }
+          auto& acc = accs[q];
+          acc.add(0, f.e);
+          if constexpr (!TRICLINIC)
+          {
+            acc.add(1, dx * f.f1);
+            acc.add(2, dy * f.f1);
+            acc.add(3, dz * f.f1);
+            acc.add(4, f.f2 * dx * dy);
+            acc.add(5, f.f2 * dx * dz);
+            acc.add(6, f.f2 * dy * dz);
+            acc.add(7, f.f3 * dx * dy * dz);
+          }
+          else
+          {
+            // full Cartesian tensors (framework_molecule_grid.cpp:76-144), symmetric storage
+            const Real d[3] = {dx, dy, dz};
+            acc.add(1, dx * f.f1);
+            acc.add(2, dy * f.f1);
+            acc.add(3, dz * f.f1);
 #pragma unroll
-          for (int u = 0; u < 3; ++u)
+            for (int u = 0; u < 3; ++u)
 #pragma unroll
-            for (int v = u; v < 3; ++v) acc.add(4 + sym2(u, v), f.f2 * d[u] * d[v] + (u == v ? f.f1 : Real(0)));
+              for (int v = u; v < 3; ++v) acc.add(4 + sym2(u, v), f.f2 * d[u] * d[v] + (u == v ? f.f1 : Real(0)));
 #pragma unroll
-          for (int u = 0; u < 3; ++u)
+            for (int u = 0; u < 3; ++u)
 #pragma unroll
-            for (int v = u; v < 3; ++v)
+              for (int v = u; v < 3; ++v)
 #pragma unroll
-              for (int w = v; w < 3; ++w)
-                acc.add(10 + sym3(u, v, w), f.f3 * d[u] * d[v] * d[w] + (v == w ? f.f2 * d[u] : Real(0)) +
-                                                (u == w ? f.f2 * d[v] : Real(0)) + (u == v ? f.f2 * d[w] : Real(0)));
+                for (int w = v; w < 3; ++w)
+                  acc.add(10 + sym3(u, v, w), f.f3 * d[u] * d[v] * d[w] + (v == w ? f.f2 * d[u] : Real(0)) +
+                                                  (u == w ? f.f2 * d[v] : Real(0)) + (u == v ? f.f2 * d[w] : Real(0)));
+          }
         }
       }
     }
-    acc.flush();
+#pragma unroll
+    for (int q = 0; q < NP; ++q) accs[q].flush();
     __syncthreads();
   }
 
@@ -377,6 +450,10 @@ __global__ void __launch_bounds__(256) gridKernel(GridParams p, const double4* _
   }
   if (!valid) return;
 
+#pragma unroll
+  for (int q = 0; q < NP; ++q)
+  {
+  const auto& acc = accs[q];
   double v[8];
   v[0] = acc.get(0);
   if constexpr (!TRICLINIC)
@@ -435,32 +512,33 @@ __global__ void __launch_bounds__(256) gridKernel(GridParams p, const double4* _
     v[3] = fmin(fmax(v[3], -oc), oc);
     v[4] = v[5] = v[6] = v[7] = 0.0;
   }
-  double2* dst = reinterpret_cast<double2*>(p.out + 8 * (static_cast<long long>(i) +
+  double2* dst = reinterpret_cast<double2*>(p.out[q] + 8 * (static_cast<long long>(i) +
                                                          static_cast<long long>(p.nx) *
                                                              (static_cast<long long>(j) + static_cast<long long>(p.ny) * k)));
   dst[0] = make_double2(v[0], v[1]);
   dst[1] = make_double2(v[2], v[3]);
   dst[2] = make_double2(v[4], v[5]);
   dst[3] = make_double2(v[6], v[7]);
+  }
 }
 
-template <typename Real, int TYPE, bool TRI>
+template <typename Real, int TYPE, bool TRI, int NP = 1>
 cudaError_t launchTyped(const GridParams& p, const double4* ipos, const double4* ipar, int bx, int by, int bz,
                         bool count, cudaStream_t stream)
 {
   dim3 grid((p.nx + bx - 1) / bx, (p.ny + by - 1) / by, (p.nz + bz - 1) / bz);
   int nt = bx * by * bz;
-  size_t shmem = (2 * sizeof(typename Vec4<Real>::T) + (sizeof(Real) == 4 ? sizeof(float4) : 0)) *
+  size_t shmem = ((1 + NP) * sizeof(typename Vec4<Real>::T) + (sizeof(Real) == 4 ? sizeof(float4) : 0)) *
                  static_cast<size_t>(nt) * kPer;
   if (count)
   {
-    auto kern = gridKernel<Real, TYPE, TRI, true>;
+    auto kern = gridKernel<Real, TYPE, TRI, true, NP>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shmem));
     kern<<<grid, nt, shmem, stream>>>(p, ipos, ipar, bx, by, bz);
   }
   else
   {
-    auto kern = gridKernel<Real, TYPE, TRI, false>;
+    auto kern = gridKernel<Real, TYPE, TRI, false, NP>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shmem));
     kern<<<grid, nt, shmem, stream>>>(p, ipos, ipar, bx, by, bz);
   }
@@ -483,6 +561,7 @@ cudaError_t launchPrec(int type, const GridParams& p, const double4* ipos, const
       return launchTyped<Real, RG_GRID_LENNARD_JONES_ATTRACTION, TRI>(p, ipos, ipar, bx, by, bz, count, stream);
   }
 }
+
 }  // namespace
 
 namespace rg
@@ -625,7 +704,8 @@ extern "C" rg_status rg_grid_build(rg_ctx* ctx, int grid_type, const rg_forcefie
   gp.coul = rg::coulombFactor();
   gp.overlap = ff->overlap_criteria;
   gp.pair_count = dcount;
-  gp.out = dout;
+  gp.out[0] = dout;
+  gp.out[1] = nullptr;
 
   cudaError_t err;
   const bool count = stats != nullptr;
@@ -817,7 +897,8 @@ extern "C" rg_status rg_grid_build_noalloc(int device, void* stream, int grid_ty
   gp.coul = C;
   gp.overlap = ff->overlap_criteria;
   gp.pair_count = dcount;
-  gp.out = out_device;
+  gp.out[0] = out_device;
+  gp.out[1] = nullptr;
   const bool count = stats != nullptr;
   cudaError_t err;
   if (precision == RG_PRECISION_FP64)
@@ -837,5 +918,162 @@ extern "C" rg_status rg_grid_build_noalloc(int device, void* stream, int grid_ty
     stats->h2d_bytes = static_cast<int64_t>(2 * sizeof(double4)) * n_images;
     stats->d2h_bytes = 0;
   }
+  return RG_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Several grids of one framework in one call: the loop of System::createFrameworkInterpolationGrids
+// (src/raspakit/system_interpolation_grids.cpp:202-238). Lennard-Jones grids whose probes see the same framework atoms
+// (nonzero epsilon for the same atoms) are built two at a time by one kernel that shares the candidate staging, the
+// distances and the reciprocal between the two probes.
+// ---------------------------------------------------------------------------------------------------------------------
+extern "C" rg_status rg_grid_build_set(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* unit_cell,
+                                       const rg_atom* unit_atoms, int n_unit_atoms, double cutoff, int nx, int ny,
+                                       int nz, int precision, int n_grids, const int* grid_types,
+                                       const int* probe_types, double* const* out_device, double* const* out_host,
+                                       rg_grid_stats* stats)
+{
+  if (!ctx) return RG_ERR_INVALID_ARGUMENT;
+  if (!ff || !unit_cell || (n_unit_atoms > 0 && !unit_atoms) || n_unit_atoms < 0 || n_grids < 0 ||
+      (n_grids > 0 && (!grid_types || !probe_types || !out_device)))
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_set: null argument");
+  if (precision != RG_PRECISION_FP64 && precision != RG_PRECISION_FP32C)
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_set: bad precision");
+  if (nx < 2 || ny < 2 || nz < 2) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_set: grid shape");
+  for (int g = 0; g < n_grids; ++g)
+  {
+    if (grid_types[g] < 0 || grid_types[g] > 3 || !out_device[g])
+      return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_set: bad grid type or output");
+    if (grid_types[g] != RG_GRID_EWALD_REAL && (probe_types[g] < 0 || probe_types[g] >= ff->n_types))
+      return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_set: probe_type out of range");
+  }
+  (void)cutoff;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  const rg::HostBox box = rg::makeHostBox(unit_cell);
+  // which framework atoms a Lennard-Jones probe sees
+  auto mask = [&](int probe)
+  {
+    std::vector<char> m(n_unit_atoms);
+    for (int a = 0; a < n_unit_atoms; ++a) m[a] = ff->epsilon[probe * ff->n_types + unit_atoms[a].type] != 0.0;
+    return m;
+  };
+  std::vector<int> done(n_grids, 0);
+  const size_t grid_bytes = sizeof(double) * 8 * static_cast<size_t>(nx) * ny * nz;
+  auto download = [&](int q) -> rg_status
+  {
+    if (out_host && out_host[q])
+      RG_CUDA(ctx, cudaMemcpyAsync(out_host[q], out_device[q], grid_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    if (stats && out_host && out_host[q]) stats[q].d2h_bytes = static_cast<int64_t>(grid_bytes);
+    return RG_OK;
+  };
+  for (int g = 0; g < n_grids; ++g)
+  {
+    if (done[g]) continue;
+    int partner = -1;
+    if (grid_types[g] == RG_GRID_LENNARD_JONES)
+    {
+      const std::vector<char> mg = mask(probe_types[g]);
+      for (int h = g + 1; h < n_grids && partner < 0; ++h)
+        if (!done[h] && grid_types[h] == RG_GRID_LENNARD_JONES && mask(probe_types[h]) == mg) partner = h;
+    }
+    if (partner < 0)
+    {
+      rg_status st = rg_grid_build(ctx, grid_types[g], ff, unit_cell, unit_atoms, n_unit_atoms, probe_types[g], cutoff,
+                                   nx, ny, nz, precision, out_device[g], nullptr, stats ? &stats[g] : nullptr);
+      if (!st) st = download(g);
+      if (st) return st;
+      done[g] = 1;
+      continue;
+    }
+    // fused pair: positions from probe g, parameters of both probes interleaved per image
+    std::vector<double4> pos, par0, pos1, par1;
+    const int n_images = rg::buildGridImages(RG_GRID_LENNARD_JONES, ff, box, unit_atoms, n_unit_atoms,
+                                             probe_types[g], pos, par0);
+    rg::buildGridImages(RG_GRID_LENNARD_JONES, ff, box, unit_atoms, n_unit_atoms, probe_types[partner], pos1, par1);
+    void* p = nullptr;
+    const int nimg = n_images > 0 ? n_images : 1;
+    rg_status st = rg::scratch(ctx, 1, 3 * sizeof(double4) * static_cast<size_t>(nimg) + 64, &p);
+    if (st) return st;
+    double4* dpos = static_cast<double4*>(p);
+    double4* dpar = dpos + nimg;
+    unsigned long long* dcount = reinterpret_cast<unsigned long long*>(dpar + 2 * static_cast<size_t>(nimg));
+    if (n_images > 0)
+    {
+      void* hp = nullptr;
+      RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      st = rg::pinnedScratch(ctx, 0, 3 * sizeof(double4) * n_images, &hp);
+      if (st) return st;
+      double4* stage = static_cast<double4*>(hp);
+      std::memcpy(stage, pos.data(), sizeof(double4) * n_images);
+      for (int i = 0; i < n_images; ++i)
+      {
+        stage[n_images + 2 * i] = par0[i];
+        stage[n_images + 2 * i + 1] = par1[i];
+      }
+      RG_CUDA(ctx, cudaMemcpyAsync(dpos, stage, 3 * sizeof(double4) * n_images, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    RG_CUDA(ctx, cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), ctx->stream));
+    const int bx = 8, by = 8, bz = 4;
+    GridParams gp{};
+    for (int c = 0; c < 3; ++c)
+      for (int r = 0; r < 3; ++r) gp.cell[c][r] = box.c[c][r];
+    gp.ncells[0] = static_cast<double>(nx - 1);
+    gp.ncells[1] = static_cast<double>(ny - 1);
+    gp.ncells[2] = static_cast<double>(nz - 1);
+    for (int d = 0; d < 3; ++d) gp.delta[d] = 1.0 / gp.ncells[d];
+    gp.nx = nx;
+    gp.ny = ny;
+    gp.nz = nz;
+    gp.n_images = n_images;
+    gp.rc2 = ff->cutoff_framework_vdw * ff->cutoff_framework_vdw;
+    double R = 0.0;
+    for (int sx = -1; sx <= 1; sx += 2)
+      for (int sy = -1; sy <= 1; sy += 2)
+        for (int sz = -1; sz <= 1; sz += 2)
+        {
+          double f[3] = {sx * 0.5 * (bx - 1) * gp.delta[0], sy * 0.5 * (by - 1) * gp.delta[1],
+                         sz * 0.5 * (bz - 1) * gp.delta[2]},
+                 d[3];
+          rg::matvec(box.c, f, d);
+          R = std::fmax(R, std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
+        }
+    const double rf = ff->cutoff_framework_vdw + R + 1e-6;
+    gp.filter2 = rf * rf;
+    gp.alpha = ff->ewald_alpha;
+    gp.coul = rg::coulombFactor();
+    gp.overlap = ff->overlap_criteria;
+    gp.pair_count = dcount;
+    gp.out[0] = out_device[g];
+    gp.out[1] = out_device[partner];
+    const bool count = stats != nullptr;
+    cudaError_t err;
+    if (precision == RG_PRECISION_FP64)
+      err = box.triclinic
+                ? launchTyped<double, RG_GRID_LENNARD_JONES, true, 2>(gp, dpos, dpar, bx, by, bz, count, ctx->stream)
+                : launchTyped<double, RG_GRID_LENNARD_JONES, false, 2>(gp, dpos, dpar, bx, by, bz, count, ctx->stream);
+    else
+      err = box.triclinic
+                ? launchTyped<float, RG_GRID_LENNARD_JONES, true, 2>(gp, dpos, dpar, bx, by, bz, count, ctx->stream)
+                : launchTyped<float, RG_GRID_LENNARD_JONES, false, 2>(gp, dpos, dpar, bx, by, bz, count, ctx->stream);
+    if (err != cudaSuccess) return rg::cudaFail(ctx, err, "gridKernel (two probes) launch");
+    if (stats)
+    {
+      unsigned long long c = 0;
+      RG_CUDA(ctx, cudaMemcpyAsync(&c, dcount, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+      RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      for (int q : {g, partner})
+      {
+        stats[q].pair_count = static_cast<int64_t>(c);
+        stats[q].n_images = n_images;
+        stats[q].h2d_bytes = static_cast<int64_t>(3 * sizeof(double4)) * n_images / 2;
+        stats[q].d2h_bytes = 0;
+      }
+    }
+    rg_status dst = download(g);
+    if (!dst) dst = download(partner);
+    if (dst) return dst;
+    done[g] = done[partner] = 1;
+  }
+  if (out_host) RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return RG_OK;
 }

@@ -102,6 +102,8 @@ def lib():
         L.rg_grid_build.argtypes = [vp, i32, P(RgForceField), P(RgBox), vp, i32, i32, d, i32, i32, i32, i32, vp, vp,
                                     P(GridStats)]
         L.rg_probe_fma_peak.argtypes = [vp, i32, P(d), P(d)]
+        L.rg_grid_build_set.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, d, i32, i32, i32, i32, i32, vp, vp, vp,
+                                        vp, vp]
         L.rg_grid_build_noalloc.argtypes = [i32, vp, i32, P(RgForceField), P(RgBox), vp, i32, i32, d, i32, i32, i32,
                                             i32, vp, P(GridStats)]
         L.rg_system_create.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, P(vp)]
@@ -114,6 +116,19 @@ def lib():
         L.rg_gcmc_run.argtypes = [vp, i64, i32]
         L.rg_gcmc_results.argtypes = [vp, vp]
         L.rg_gcmc_get_positions.argtypes = [vp, i32, vp, i32, P(i32)]
+        L.rg_gcmc_set_proposal.argtypes = [vp, vp, P(RgBox)]
+        L.rg_mlp_create.argtypes = [vp, ctypes.c_uint64, P(vp)]
+        L.rg_mlp_destroy.argtypes = [vp]
+        L.rg_mlp_num_params.restype = i32
+        L.rg_mlp_get_params.argtypes = [vp, vp, i32]
+        L.rg_mlp_set_params.argtypes = [vp, vp, i32]
+        L.rg_mlp_loss_and_gradient.argtypes = [vp, vp, vp, i32, P(ctypes.c_float), vp]
+        L.rg_mlp_train.argtypes = [vp, vp, vp, i64, i32, i32, ctypes.c_float, ctypes.c_uint64, P(ctypes.c_float)]
+        L.rg_mlp_evaluate.argtypes = [vp, vp, i64, vp]
+        L.rg_proposal_sample_targets.argtypes = [vp, i32, d, d, d, P(RgBox), i64, ctypes.c_uint64, vp, vp]
+        L.rg_proposal_create.argtypes = [vp, i32, d, P(vp)]
+        L.rg_proposal_destroy.argtypes = [vp]
+        L.rg_proposal_density.argtypes = [vp, vp, i64, vp]
         L.rg_ewald_create.argtypes = [vp, P(RgForceField), P(RgBox), i32, P(vp)]
         L.rg_ewald_destroy.argtypes = [vp]
         L.rg_ewald_info.argtypes = [vp, P(i64), P(d)]
@@ -190,6 +205,30 @@ class Context:
                                  ctypes.byref(stats) if count_pairs else None)
         check(self.handle, st, "rg_grid_build")
         return out, (stats.as_dict() if count_pairs else None)
+
+    def grid_build_set(self, ff: ForceField, cell, unit_atoms: np.ndarray, cutoff: float, dims, precision: int,
+                       grid_types, probe_types, out_device_ptrs, count_pairs: bool = False, out_host=None):
+        """Several grids of one framework into device buffers (Lennard-Jones probes fused in pairs); out_host: optional
+        list of host float64 arrays that also receive the grids."""
+        nx, ny, nz = (int(v) for v in dims)
+        atoms = np.ascontiguousarray(unit_atoms, dtype=ATOM_DTYPE)
+        ffs, box = ff_struct(ff), box_struct(cell)
+        n = len(grid_types)
+        gt = np.ascontiguousarray(grid_types, dtype=np.int32)
+        pt = np.ascontiguousarray(probe_types, dtype=np.int32)
+        outs = (ctypes.c_void_p * n)(*[int(p) for p in out_device_ptrs])
+        hosts = None
+        if out_host is not None:
+            hosts = (ctypes.c_void_p * n)(*[None if h is None else h.ctypes.data for h in out_host])
+        stats = (GridStats * n)()
+        check(self.handle, lib().rg_grid_build_set(self.handle, ctypes.byref(ffs), ctypes.byref(box),
+                                                   ctypes.c_void_p(atoms.ctypes.data), len(atoms), cutoff, nx, ny, nz,
+                                                   precision, n, ctypes.c_void_p(gt.ctypes.data),
+                                                   ctypes.c_void_p(pt.ctypes.data), ctypes.cast(outs, ctypes.c_void_p),
+                                                   None if hosts is None else ctypes.cast(hosts, ctypes.c_void_p),
+                                                   ctypes.cast(stats, ctypes.c_void_p) if count_pairs else None),
+              "rg_grid_build_set")
+        return [stats[i].as_dict() for i in range(n)] if count_pairs else None
 
     def probe_fma_peak(self, precision: int = PRECISION_FP32C) -> float:
         t, s = ctypes.c_double(), ctypes.c_double()
@@ -379,6 +418,16 @@ class Gcmc:
     def run(self, moves: int, record: bool = True):
         check(self.ctx.handle, lib().rg_gcmc_run(self.handle, moves, 1 if record else 0), "rg_gcmc_run")
 
+    def set_proposal(self, proposal, unit_cell=None):
+        """Learned first-bead proposal (None: uniform positions)."""
+        self._proposal = proposal
+        if proposal is None:
+            check(self.ctx.handle, lib().rg_gcmc_set_proposal(self.handle, None, None), "rg_gcmc_set_proposal")
+        else:
+            box = box_struct(unit_cell)
+            check(self.ctx.handle, lib().rg_gcmc_set_proposal(self.handle, proposal.handle, ctypes.byref(box)),
+                  "rg_gcmc_set_proposal")
+
     def results(self):
         out = (GcmcChainResult * self.n_chains)()
         check(self.ctx.handle, lib().rg_gcmc_results(self.handle, ctypes.cast(out, ctypes.c_void_p)),
@@ -392,3 +441,94 @@ class Gcmc:
         check(self.ctx.handle, lib().rg_gcmc_get_positions(self.handle, chain, ctypes.c_void_p(buf.ctypes.data), cap,
                                                            ctypes.byref(n)), "rg_gcmc_get_positions")
         return buf[: 3 * n.value * self.component.n_atoms].reshape(-1, 3)
+
+
+class Mlp:
+    """The learned proposal's Fourier-feature MLP on the device (rg_mlp)."""
+
+    def __init__(self, ctx: Context, seed: int = 1):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        check(ctx.handle, lib().rg_mlp_create(ctx.handle, seed, ctypes.byref(h)), "rg_mlp_create")
+        self.handle = h
+        ctx.adopt(self)
+        self.n_params = lib().rg_mlp_num_params()
+
+    def close(self):
+        if self.handle:
+            lib().rg_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.n_params, dtype=np.float32)
+        check(self.ctx.handle, lib().rg_mlp_get_params(self.handle, ctypes.c_void_p(out.ctypes.data), self.n_params),
+              "rg_mlp_get_params")
+        return out
+
+    def set_params(self, theta):
+        theta = np.ascontiguousarray(theta, dtype=np.float32)
+        check(self.ctx.handle, lib().rg_mlp_set_params(self.handle, ctypes.c_void_p(theta.ctypes.data), len(theta)),
+              "rg_mlp_set_params")
+
+    def loss_and_gradient(self, s_ptr: int, t_ptr: int, n: int):
+        loss = ctypes.c_float()
+        grad = np.empty(self.n_params, dtype=np.float32)
+        check(self.ctx.handle, lib().rg_mlp_loss_and_gradient(self.handle, s_ptr, t_ptr, n, ctypes.byref(loss),
+                                                              ctypes.c_void_p(grad.ctypes.data)),
+              "rg_mlp_loss_and_gradient")
+        return loss.value, grad
+
+    def train(self, s_ptr: int, t_ptr: int, n: int, steps: int, batch: int = 4096, lr: float = 1e-3, seed: int = 1):
+        loss = ctypes.c_float()
+        check(self.ctx.handle, lib().rg_mlp_train(self.handle, s_ptr, t_ptr, n, steps, batch, lr, seed,
+                                                  ctypes.byref(loss)), "rg_mlp_train")
+        return loss.value
+
+    def evaluate(self, s_ptr: int, n: int, out_ptr: int):
+        check(self.ctx.handle, lib().rg_mlp_evaluate(self.handle, s_ptr, n, out_ptr), "rg_mlp_evaluate")
+
+
+def sample_targets(system: System, pseudo_atom: int, charge: float, beta: float, t_min: float, unit_cell, n: int,
+                   seed: int, s_ptr: int, t_ptr: int):
+    box = box_struct(unit_cell)
+    check(system.ctx.handle, lib().rg_proposal_sample_targets(system.handle, pseudo_atom, charge, beta, t_min,
+                                                              ctypes.byref(box), n, seed, s_ptr, t_ptr),
+          "rg_proposal_sample_targets")
+
+
+class Proposal:
+    """A tabulated, exactly normalised first-bead proposal (rg_proposal) built from an Mlp."""
+
+    def __init__(self, mlp: Mlp, cells_per_axis: int = 64, eps_uniform: float = 0.1):
+        self.ctx = mlp.ctx
+        h = ctypes.c_void_p()
+        check(self.ctx.handle, lib().rg_proposal_create(mlp.handle, cells_per_axis, eps_uniform, ctypes.byref(h)),
+              "rg_proposal_create")
+        self.handle = h
+        self.ctx.adopt(self)
+        self.cells = cells_per_axis
+        self.eps = eps_uniform
+
+    def close(self):
+        if self.handle:
+            lib().rg_proposal_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def density(self, s) -> np.ndarray:
+        s = np.ascontiguousarray(s, dtype=np.float64).reshape(-1, 3)
+        out = np.empty(len(s))
+        check(self.ctx.handle, lib().rg_proposal_density(self.handle, ctypes.c_void_p(s.ctypes.data), len(s),
+                                                         ctypes.c_void_p(out.ctypes.data)), "rg_proposal_density")
+        return out

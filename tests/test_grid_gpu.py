@@ -153,3 +153,23 @@ def test_invalid_arguments_raise(ctx):
         ctx.grid_build(0, ff, cell, atoms, 99, 12.0, (10, 10, 10))
     with pytest.raises(native.RaspaGpuError):
         ctx.grid_build(0, ff, cell, atoms, 2, 12.0, (1, 10, 10))
+
+
+@pytest.mark.parametrize("precision", [native.PRECISION_FP64, native.PRECISION_FP32C])
+def test_grid_build_set_matches_single_builds(ctx, precision):
+    """rg_grid_build_set (Lennard-Jones probes fused two per kernel) gives the grids of separate rg_grid_build calls."""
+    torch = pytest.importorskip("torch")
+    ff = synthetic_forcefield(charges=True)
+    cell, atoms = synthetic_framework(ff)
+    dims = (45, 45, 30)
+    types = [0, 0, 1]
+    probes = [ff.index("C_co2"), ff.index("O_co2"), 0]
+    outs = [torch.empty(8 * dims[0] * dims[1] * dims[2], dtype=torch.float64, device="cuda") for _ in types]
+    hosts = [np.empty(8 * dims[0] * dims[1] * dims[2]) for _ in types]
+    stats = ctx.grid_build_set(ff, cell, atoms, 12.0, dims, precision, types, probes, [o.data_ptr() for o in outs],
+                               count_pairs=True, out_host=hosts)
+    for g, (gt, pr) in enumerate(zip(types, probes)):
+        ref, rs = ctx.grid_build(gt, ff, cell, atoms, pr, 12.0, dims, precision, count_pairs=True)
+        np.testing.assert_array_equal(outs[g].cpu().numpy(), ref)
+        np.testing.assert_array_equal(hosts[g], ref)
+        assert stats[g]["pair_count"] == rs["pair_count"]

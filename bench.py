@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gcmc", action="store_true", help="skip the GCMC steps/s section")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-uniform proposal section")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the cpu_baseline sample")
     return ap.parse_args()
 
@@ -195,6 +196,110 @@ def run_gcmc(args, ctx, ff, cell, atoms, dims, grids, outs, world, rank, dist, t
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_gcmc_rate(ff, cell, scell, sfw, dims, grids, outs, args.cpu_seconds)
     g.close()
+    ew.close()
+    sysg.close()
+    return out
+
+
+LEARNED_SAMPLES = 1 << 22
+LEARNED_TRAIN_STEPS = 3000
+LEARNED_EQUIL = 4000
+LEARNED_MOVES = 40000
+
+
+def run_learned(args, ctx, world, rank, dist, torch):
+    """Learned vs uniform first-bead proposal (configuration 4): CO2 at 300 K and 1e6 Pa in the 2x2x3 box of the
+    synthetic framework, with the framework charges set to zero (with them the binding wells of about -1e4 K make the
+    system non-ergodic for every sampler); CO2 keeps its charges, Ewald on. The MLP is trained on 2^22 grid-sampled
+    Boltzmann factors of the C atom. Both arms run the same number of chains and moves; the statistical error of the
+    loading is the standard error over independent chains. GPU-seconds to reach the uniform run's error:
+    t_train + t_learned * (se_learned / se_uniform)^2, against t_uniform."""
+    from raspa3_b200 import native
+    from raspa3_b200.gcmc import beta_of, co2_component, fugacity_of
+    from raspa3_b200.synthetic import config1_grid_dims, replicate, synthetic_forcefield, synthetic_framework
+
+    ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=8)
+    for pa in ff.pseudo_atoms[:2]:
+        pa.charge = 0.0
+    ucell, ufw = synthetic_framework(ff, seed=42)
+    scell, sfw = replicate(ucell, ufw, (2, 2, 3))
+    dims = config1_grid_dims(ucell)
+    stream = torch.cuda.current_stream()
+    sysg = native.System(ctx, ff, scell, sfw)
+    keep = []
+    for idx, gt in ((ff.index("C_co2"), 0), (ff.index("O_co2"), 0), (ff.n_types, 1)):
+        buf = torch.empty(8 * dims[0] * dims[1] * dims[2], dtype=torch.float64, device="cuda")
+        ctx.grid_build(gt, ff, ucell, ufw, idx if gt == 0 else 0, 12.0, dims, native.PRECISION_FP32C,
+                       out_device=buf.data_ptr(), host=False)
+        sysg.set_grid(idx, ucell, dims, buf.data_ptr(), on_device=True)
+        keep.append(buf)
+    ew = native.Ewald(ctx, ff, scell)
+    ew.set_framework(sfw)
+    beta = beta_of(300.0)
+    comp = co2_component()
+    c_atom = comp.starting_bead
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    chains = GCMC_CHAINS_PER_SM * sms
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1) / 1e3
+
+    # training: target sampling from the grids, MLP training, tabulation of the proposal density
+    n = LEARNED_SAMPLES
+    ds = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+    dt = torch.empty(n, dtype=torch.float32, device="cuda")
+    m = native.Mlp(ctx, seed=1)
+    _, t_sample = timed(lambda: native.sample_targets(sysg, int(comp.types(ff)[c_atom]), float(comp.charges(ff)[c_atom]),
+                                                      beta, -15.0, ucell, n, 9, ds.data_ptr(), dt.data_ptr()))
+    loss, t_fit = timed(lambda: m.train(ds.data_ptr(), dt.data_ptr(), n, steps=LEARNED_TRAIN_STEPS, batch=4096,
+                                        lr=2e-3))
+    prop, t_table = timed(lambda: native.Proposal(m, cells_per_axis=48, eps_uniform=0.05))
+    t_train = t_sample + t_fit + t_table
+
+    arms = {}
+    for name, use in (("uniform", False), ("learned", True)):
+        g = native.Gcmc(sysg, ew, comp, beta, fugacity_of(1e6), n_chains=chains, seed=(31 if use else 32) + 100 * rank)
+        if use:
+            g.set_proposal(prop, ucell)
+        g.run(LEARNED_EQUIL, record=False)
+        _, secs = timed(lambda: g.run(LEARNED_MOVES, record=True))
+        res = g.results()
+        g.close()
+        means = np.array([r["sum_n"] / r["samples"] for r in res])
+        emeans = np.array([r["sum_energy"] / r["samples"] for r in res])
+        blocks = np.array([r["block_n"] for r in res], dtype=np.float64)
+        acc = np.sum([r["accepted"] for r in res], axis=0)
+        att = np.sum([r["attempted"] for r in res], axis=0)
+        arms[name] = {"gpu_seconds": secs, "loading": float(means.mean()),
+                      "loading_se": float(means.std(ddof=1) / np.sqrt(len(means))),
+                      "loading_block_se": float(blocks.mean(axis=0).std(ddof=1) / np.sqrt(blocks.shape[1])),
+                      "energy_K": float(emeans.mean()), "energy_se_K": float(emeans.std(ddof=1) / np.sqrt(len(means))),
+                      "swap_acceptance": float((acc[2] + acc[3]) / max(1, att[2] + att[3])),
+                      "moves_per_s": chains * LEARNED_MOVES / secs}
+    u, l = arms["uniform"], arms["learned"]
+    var_ratio = (l["loading_se"] / u["loading_se"]) ** 2
+    t_equal = t_train + l["gpu_seconds"] * var_ratio
+    out = {"metric": "GPU-seconds to equal loading error, learned vs uniform first-bead proposal",
+           "workload": "CO2 (charged, Ewald alpha 0.265 kmax 8) at 300 K and 1e6 Pa in the 2x2x3 box of the synthetic "
+                       "framework with framework charges off, 133x133x89 FP32C grids; MLP 96-64-64-1 SiLU trained on "
+                       f"2^22 grid Boltzmann factors, proposal tabulated on 48^3 cells with 5% uniform mixing; "
+                       f"{chains} chains x {LEARNED_MOVES} moves after {LEARNED_EQUIL} equilibration moves per arm",
+           "train": {"sample_s": t_sample, "fit_s": t_fit, "table_s": t_table, "total_s": t_train,
+                     "final_loss": loss, "steps": LEARNED_TRAIN_STEPS, "batch": 4096},
+           "uniform": u, "learned": l,
+           "loading_difference_sigmas": abs(l["loading"] - u["loading"]) / float(np.hypot(u["loading_se"],
+                                                                                           l["loading_se"])),
+           "sampling_efficiency_ratio": u["gpu_seconds"] / (l["gpu_seconds"] * var_ratio),
+           "learned_seconds_to_uniform_error": t_equal,
+           "speedup_at_equal_error_incl_training": u["gpu_seconds"] / t_equal}
+    prop.close()
+    m.close()
     ew.close()
     sysg.close()
     return out
@@ -396,6 +501,10 @@ def run_ours(args):
     # ---- GCMC steps/s on the same workload: CO2 in the 2x2x3 simulation box, the FP32C grids just built ----
     if not args.no_gcmc:
         line["gcmc"] = run_gcmc(args, ctx, ff, cell, atoms, dims, grids, outs, world, rank, dist, torch)
+    # ---- learned vs uniform first-bead proposal at equal loading error (configuration 4) ----
+    if not args.no_learned:
+        del flush
+        line["learned_proposal"] = run_learned(args, ctx, world, rank, dist, torch)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, pts, secs, threads = cpu_oracle_rate(ff, cell, atoms, dims, grids, args.cpu_seconds)

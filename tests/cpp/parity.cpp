@@ -237,8 +237,16 @@ int main()
     context.setMoleculeAtoms({});
     const std::vector<rg_atom> one{atom(0.5 * a, 0.5 * a, 0.5 * a, 0.0, CH4, 0)};
     auto e = CBMC::computeExternalNonOverlappingEnergies(context, one);
-    // interpolated vs exact pair sum at the cage centre: within the grid's interpolation error (0.25 A spacing)
-    if (!e.empty()) EXPECT_NEAR(e[0].energy.frameworkMoleculeVDW * EnergyToKelvin, -337.77056357, 1.0);
+    // The grid holds the sum over every periodic image within the cutoff. In the 11.87 A cell the minimum-image pair
+    // loop (and the -337.77 K golden) misses the images beyond half a cell, so the exact value is the pair loop in the
+    // 3x3x3 supercell, where the minimum image reaches all of them. Tolerance: interpolation error at 0.25 A spacing.
+    CBMC::GrowContext exact(ctx, ff, cubic(3.0 * a), itq29(3));
+    exact.setMoleculeAtoms({});
+    auto ex = CBMC::computeExternalNonOverlappingEnergies(exact, one);
+    EXPECT_NEAR(ex.size(), 1.0, 0.0);
+    if (!e.empty() && !ex.empty())
+      EXPECT_NEAR(e[0].energy.frameworkMoleculeVDW, ex[0].energy.frameworkMoleculeVDW,
+                  1e-3 * std::fabs(ex[0].energy.frameworkMoleculeVDW));
   }
 
   std::printf("%s (%d failures)\n", failures ? "FAILED" : "PASSED", failures);

@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gcmc", action="store_true", help="skip the GCMC steps/s section")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-uniform proposal section")
+    ap.add_argument("--no-alkane", action="store_true", help="skip the batched flexible-chain CBMC section")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the cpu_baseline sample")
     return ap.parse_args()
 
@@ -198,6 +199,86 @@ def run_gcmc(args, ctx, ff, cell, atoms, dims, grids, outs, world, rank, dist, t
     g.close()
     ew.close()
     sysg.close()
+    return out
+
+
+ALKANE_SYSTEMS = 64
+ALKANE_EQUIL = 2000
+ALKANE_MOVES = 1000
+# FLOPs per in-cutoff pair of the FP32 Lennard-Jones trial term: displacement scaling and r^2 (8), sigma^2/r^2 (1),
+# t^3 (2), 4 eps t^3 (t^3 - 1) - shift (4), accumulation (1), counted as in the grid kernels (reciprocal = 1)
+ALKANE_FLOPS_PER_PAIR = 16
+
+
+def run_alkane(args, ctx, peak_fp32, world, rank, dist, torch):
+    """Batched CBMC of flexible alkanes (configuration 3): 64 independent systems of uneven size (cells 12-40 A,
+    96-1536 framework atoms, 4-8 bead chains) in one graph replay of persistent cluster kernels, GCMC at 300 K and
+    1e5 Pa with translation and CBMC swap moves. Metric: move attempts per second over all systems, after
+    equilibration, with the launch plan chosen by the autotuner."""
+    from raspa3_b200 import native
+    from raspa3_b200.alkane import alkane_forcefield, config3_systems
+
+    ff = alkane_forcefield()
+    systems = config3_systems(ff, n_systems=ALKANE_SYSTEMS, seed=1234, max_molecules=128)
+    stream = torch.cuda.current_stream()
+    w_ig = {}
+    for q in systems:
+        nb = q.chain.n_beads
+        if nb not in w_ig:
+            w_ig[nb] = native.alkane_grow_vacuum(ctx, ff, q.chain, q.beta, 200000, seed=17)
+        q.w_ig = w_ig[nb]
+    a = native.Alkane(ctx, ff, systems, seed=5 + rank)
+    a.run(ALKANE_EQUIL, record=False)
+    plan = a.autotune(moves_per_candidate=16)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    pairs0 = a.pair_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    a.run(ALKANE_MOVES, record=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3
+    pairs = a.pair_count() - pairs0
+    if world > 1:
+        t = torch.tensor([secs], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        secs = float(t.item())
+    res = a.results()
+    # e2e: the run call plus the read-back of every system's statistics through the C-ABI
+    t0 = time.perf_counter()
+    a.run(ALKANE_MOVES, record=True)
+    a.results()
+    e2e_secs = time.perf_counter() - t0
+    achieved = pairs * ALKANE_FLOPS_PER_PAIR / secs / 1e12
+    loading = [r["n_molecules"] for r in res]
+    out = {"metric": "batched CBMC steps/s", "value": world * ALKANE_SYSTEMS * ALKANE_MOVES / secs,
+           "unit": "MC move attempts/s", "systems": ALKANE_SYSTEMS, "moves_per_system": ALKANE_MOVES,
+           "ms": secs * 1e3, "plan": plan, "w_ig": {str(k): v for k, v in sorted(w_ig.items())},
+           "workload": "64 synthetic cells (lengths U[12,40] A, 0.025 atoms/A^3 clipped to 96-1536 atoms, replicated "
+                       "for rc = 12 A), one 4-8 bead TraPPE-UA alkane per system, 300 K, 1e5 Pa, translation : CBMC "
+                       "swap 1 : 1, 10 first-bead trials, 10 directions x 100 torsion spins per bead",
+           "loading_min_mean_max": [min(loading), float(np.mean(loading)), max(loading)],
+           "pairs_per_move": pairs / (ALKANE_SYSTEMS * ALKANE_MOVES),
+           "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
+                        "frac": achieved / peak_fp32, "flops_per_pair": ALKANE_FLOPS_PER_PAIR},
+           "e2e": {"value": world * ALKANE_SYSTEMS * ALKANE_MOVES / e2e_secs, "unit": "MC move attempts/s",
+                   "h2d_bytes_per_step": 16, "d2h_bytes_per_step": ALKANE_SYSTEMS * (8 * 24 + 12)}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        start = [a.positions(s) for s in range(ALKANE_SYSTEMS)]
+        threads = os.cpu_count() or 1
+        _, _, t_probe = oracle.alkane_run(ff, systems, steps=20, seed=3, threads=threads, initial=start)
+        steps = int(max(20, 20 * args.cpu_seconds / max(t_probe, 1e-3)))
+        _, _, t_cpu = oracle.alkane_run(ff, systems, steps=steps, seed=4, threads=threads, initial=start)
+        out["cpu_baseline"] = {"value": ALKANE_SYSTEMS * steps / t_cpu, "unit": "MC move attempts/s",
+                               "cores": threads, "kind": "port",
+                               "sample": f"64 systems x {steps} moves from the device's equilibrated state in "
+                                         f"{t_cpu:.1f} s (FP64 oracle restating the flexible CBMC, one system per "
+                                         f"thread)"}
+    a.close()
     return out
 
 
@@ -501,6 +582,9 @@ def run_ours(args):
     # ---- GCMC steps/s on the same workload: CO2 in the 2x2x3 simulation box, the FP32C grids just built ----
     if not args.no_gcmc:
         line["gcmc"] = run_gcmc(args, ctx, ff, cell, atoms, dims, grids, outs, world, rank, dist, torch)
+    # ---- batched CBMC of flexible chains in 64 uneven systems (configuration 3) ----
+    if not args.no_alkane:
+        line["batched_cbmc"] = run_alkane(args, ctx, peak_fp32, world, rank, dist, torch)
     # ---- learned vs uniform first-bead proposal at equal loading error (configuration 4) ----
     if not args.no_learned:
         del flush

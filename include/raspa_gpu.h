@@ -320,6 +320,88 @@ rg_status rg_ewald_get_structure_factors(rg_ewald* ewald, int which, double* hos
 /* Overwrites the stored structure factors (e.g. from a restart file); n_doubles must equal 2*nk*(1+n_groups). */
 rg_status rg_ewald_set_structure_factors(rg_ewald* ewald, const double* host, int64_t n_doubles);
 
+/* ---- batched CBMC of flexible chains in many independent systems ---- */
+/* A batch of independent systems of uneven size (framework atoms, chain length, trial counts), each running GCMC of
+ * one flexible united-atom chain component with translation and CBMC swap moves. The whole batch advances in one
+ * CUDA-graph replay of persistent kernels: one thread-block cluster per system keeps the system's framework atoms
+ * (fixed-point fractional coordinates) and its molecules in shared memory for all moves of a launch. Replaces, per
+ * system, the reference's CBMC::growFlexibleMoleculeChainInsertion (cbmc/flexible_molecules/insertion.cpp:32-126),
+ * CBMC::retraceFlexibleMoleculeChainDeletion (deletion.cpp:30-104) with CBMC::generateGrowTrials /
+ * generateRetraceTrials (cbmc/operators.cpp:951-1078) and the external energies of the trials
+ * (CBMC::computeExternalNonOverlappingEnergies, cbmc/interactions.cpp:54-179), driven by
+ * MC_Moves::insertionMoveCBMC / deletionMoveCBMC / translationMove. Pair terms are FP32 from exact fixed-point
+ * displacements, reduced in FP64; Rosenbluth weights, acceptance and running energies are FP64. */
+typedef struct rg_alkane rg_alkane;
+
+/* A linear chain grown from bead 0 (Component with a fixed-bond / harmonic-bend / TraPPE-torsion definition). */
+typedef struct rg_alkane_chain
+{
+  int32_t n_beads;              /* 2..8 */
+  int32_t types[8];             /* pseudo-atom type of each bead */
+  double bond_length;           /* BondType::Fixed, Angstrom */
+  double bend_k, bend_theta0;   /* BendType::Harmonic 0.5 k (theta - theta0)^2: internal energy units, radians */
+  double torsion[4];            /* TorsionType::TraPPE p0..p3, internal energy units */
+  int32_t n_first_bead_trials;  /* 1..16 */
+  int32_t n_trial_directions;   /* 1..16 (ForceField::numberOfTrialDirections) */
+  int32_t n_torsion_trials;     /* 1..128 (ForceField::numberOfTorsionTrialDirections) */
+  int32_t reserved;
+} rg_alkane_chain;
+
+typedef struct rg_alkane_system
+{
+  rg_box box;                   /* simulation box (already replicated for the minimum image of the cutoffs) */
+  const rg_atom* framework;     /* framework atoms of the simulation box, Cartesian */
+  int32_t n_framework;
+  int32_t max_molecules;        /* 1..256 */
+  rg_alkane_chain chain;
+  double beta, fugacity;        /* 1/(kB T) and fugacity, internal units */
+  double w_ig;                  /* ideal-gas Rosenbluth weight (Component::idealGasRosenbluthWeight) */
+  double max_translation;       /* Angstrom */
+  double p_translation, p_swap; /* relative move probabilities */
+} rg_alkane_system;
+
+/* The launch plan: systems sorted by work; the first `split` run as clusters of cluster_big CTAs, the rest as
+ * clusters of cluster_small; `threads` per CTA; `moves_per_launch` moves per persistent launch. */
+typedef struct rg_alkane_plan
+{
+  int32_t cluster_big, cluster_small, threads, split, moves_per_launch, reserved;
+  double ms_per_move; /* measured by rg_alkane_autotune (device time per move of every system) */
+} rg_alkane_plan;
+
+/* Uploads the batch; every system starts empty. Pair parameters come from ff (mixed, shifted Lennard-Jones; the
+ * framework and molecule VDW cutoffs and the overlap criterion). Framework atoms whose type has no Lennard-Jones
+ * interaction with any bead type are dropped (they contribute nothing). */
+rg_status rg_alkane_create(rg_ctx* ctx, const rg_forcefield* ff, const rg_alkane_system* systems, int n_systems,
+                           uint64_t seed, rg_alkane** out);
+rg_status rg_alkane_destroy(rg_alkane* batch);
+/* Times candidate plans on the batch (each from the same snapshot of the state, restored afterwards so tuning does
+ * not advance the simulation), keeps the fastest and returns it in *chosen (may be NULL). */
+rg_status rg_alkane_autotune(rg_alkane* batch, int moves_per_candidate, rg_alkane_plan* chosen);
+rg_status rg_alkane_set_plan(rg_alkane* batch, const rg_alkane_plan* plan);
+rg_status rg_alkane_get_plan(rg_alkane* batch, rg_alkane_plan* plan);
+/* Advances every system by `moves` move attempts (graph replays on the context stream); record != 0 accumulates the
+ * statistics returned by rg_alkane_results. Asynchronous: returns once the work is enqueued. */
+rg_status rg_alkane_run(rg_alkane* batch, int64_t moves, int record);
+/* Per-system statistics (attempted/accepted [0] translation, [2] insertion, [3] deletion) and running energy. */
+rg_status rg_alkane_results(rg_alkane* batch, rg_gcmc_chain_result* out);
+/* Positions of system s: n_molecules * n_beads * 3 doubles (Cartesian, each molecule unwrapped). */
+rg_status rg_alkane_get_positions(rg_alkane* batch, int system, double* xyz, int capacity_doubles, int* n_molecules);
+/* Replaces the molecules of system s (e.g. a restart) and its running energy. */
+rg_status rg_alkane_set_positions(rg_alkane* batch, int system, const double* xyz, int n_molecules, double energy);
+/* External energies of single beads in system s against its framework and molecules (skipping molecule `skip`, or
+ * -1): the trial-energy kernel of the batch on one system, the counterpart of
+ * CBMC::computeExternalNonOverlappingEnergies for single-bead trials. fw, mm: per-bead energies; overlap: 1 where a
+ * pair exceeds the overlap criterion. n_beads <= 16. */
+rg_status rg_alkane_bead_energies(rg_alkane* batch, int system, const double* xyz_beads, const int32_t* types,
+                                  int n_beads, int skip, double* fw, double* mm, int32_t* overlap);
+/* In-cutoff pair evaluations (trial bead x framework atom or molecule bead with r < rc) since creation, summed
+ * over the systems: the algorithmic unit of the trial energies. */
+rg_status rg_alkane_pair_count(rg_alkane* batch, uint64_t* total);
+/* Grows n chains in vacuum on the device: the ideal-gas Rosenbluth weight <W> (*w_mean; the W_IG of the acceptance
+ * rule) and optionally per chain w[n], the bend angles theta[n*(nb-2)] and torsion cosines cos_phi[n*(nb-3)]. */
+rg_status rg_alkane_grow_vacuum(rg_ctx* ctx, const rg_forcefield* ff, const rg_alkane_chain* chain, double beta,
+                                int64_t n, uint64_t seed, double* w_mean, double* w, double* theta, double* cos_phi);
+
 /* ---- measurement ---- */
 /* FP32 (precision = RG_PRECISION_FP32C) or FP64 FMA throughput of this device in TFLOP/s, from independent FMA chains
  * on every SM: the SIMT-pipe denominator for the pair kernels' rooflines. No counterpart in the reference. */

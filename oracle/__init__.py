@@ -391,3 +391,141 @@ def gcmc_run(ff, cell, component, beta, fugacity, n_chains, steps, equilibration
                       ctypes.c_void_p(ctypes.addressof(secs)))
     del keep
     return [out[i].as_dict() for i in range(n_chains)], secs.value
+
+
+# ---- flexible alkane GCMC (oracle/alkane.cpp) ----
+class OAlkane(ctypes.Structure):
+    _fields_ = [("n_beads", ctypes.c_int32), ("types", ctypes.c_int32 * 8), ("bond_length", ctypes.c_double),
+                ("bend_k", ctypes.c_double), ("bend_theta0", ctypes.c_double), ("torsion", ctypes.c_double * 4),
+                ("n_first_bead_trials", ctypes.c_int32), ("n_trial_directions", ctypes.c_int32),
+                ("n_torsion_trials", ctypes.c_int32), ("n_moves_per_open_bead", ctypes.c_int32)]
+
+
+class OAlkaneSetup(ctypes.Structure):
+    _fields_ = [("ff", ctypes.POINTER(OFF)), ("box", OBox), ("framework", ctypes.c_void_p),
+                ("n_framework", ctypes.c_int32), ("chain", OAlkane), ("beta", ctypes.c_double),
+                ("fugacity", ctypes.c_double), ("w_ig", ctypes.c_double), ("max_translation", ctypes.c_double),
+                ("p_translation", ctypes.c_double), ("p_swap", ctypes.c_double), ("max_molecules", ctypes.c_int32)]
+
+
+def _alkane_lib():
+    L = lib()
+    if not hasattr(L, "_alkane_declared"):
+        P, vp, i32, i64, d = ctypes.POINTER, ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_double
+        L.oracle_alkane_run.argtypes = [vp, i32, i64, i64, ctypes.c_uint64, i32, vp, vp, vp, vp, vp]
+        L.oracle_alkane_grow_vacuum.argtypes = [P(OFF), P(OAlkane), d, i64, ctypes.c_uint64, i32, vp, vp, vp]
+        L.oracle_alkane_energy.argtypes = [P(OAlkaneSetup), vp, i32, vp]
+        L.oracle_alkane_bead_energies.argtypes = [P(OAlkaneSetup), vp, i32, vp, vp, i32, i32, vp, vp, vp]
+        L._alkane_declared = True
+    return L
+
+
+def oalkane(chain, ff) -> OAlkane:
+    """OAlkane from a raspa3_b200.alkane.AlkaneChain (internal units)."""
+    from raspa3_b200.alkane import chain_struct
+
+    c = chain_struct(chain, ff)
+    o = OAlkane()
+    o.n_beads = c.n_beads
+    for i in range(8):
+        o.types[i] = c.types[i]
+    o.bond_length, o.bend_k, o.bend_theta0 = c.bond_length, c.bend_k, c.bend_theta0
+    for k in range(4):
+        o.torsion[k] = c.torsion[k]
+    o.n_first_bead_trials, o.n_trial_directions = c.n_first_bead_trials, c.n_trial_directions
+    o.n_torsion_trials = c.n_torsion_trials
+    o.n_moves_per_open_bead = chain.n_moves_per_open_bead
+    return o
+
+
+def _alkane_setups(ff, systems):
+    o = off(ff)
+    arr = (OAlkaneSetup * len(systems))()
+    keep = [o]
+    for i, q in enumerate(systems):
+        fw = np.ascontiguousarray(q.framework)
+        keep.append(fw)
+        arr[i].ff = ctypes.pointer(o)
+        arr[i].box = obox(q.cell)
+        arr[i].framework = fw.ctypes.data if len(fw) else None
+        arr[i].n_framework = len(fw)
+        arr[i].chain = oalkane(q.chain, ff)
+        arr[i].beta, arr[i].fugacity, arr[i].w_ig = q.beta, q.fugacity, q.w_ig
+        arr[i].max_translation, arr[i].p_translation, arr[i].p_swap = q.max_translation, q.p_translation, q.p_swap
+        arr[i].max_molecules = q.max_molecules
+    return arr, keep
+
+
+def alkane_run(ff, systems, steps, equilibration=0, seed=1, threads=0, initial=None):
+    """One oracle GCMC chain per system; returns (result dicts, final positions per system, seconds).
+    initial: optional list of starting positions per system (arrays [n, nb, 3])."""
+    L = _alkane_lib()
+    arr, keep = _alkane_setups(ff, systems)
+    n = len(systems)
+    out = (OGcmcResult * n)()
+    offs = []
+    o = 0
+    for q in systems:
+        offs.append(o)
+        o += q.max_molecules * q.chain.n_beads * 3
+    xyz = np.zeros(o)
+    xin, nin = None, None
+    if initial is not None:
+        xin = np.zeros(o)
+        nin = np.zeros(n, dtype=np.int32)
+        for i, x in enumerate(initial):
+            x = np.asarray(x, dtype=np.float64).reshape(-1)
+            xin[offs[i]: offs[i] + len(x)] = x
+            nin[i] = len(x) // (3 * systems[i].chain.n_beads)
+    secs = ctypes.c_double()
+    L.oracle_alkane_run(ctypes.cast(arr, ctypes.c_void_p), n, steps, equilibration, seed, threads,
+                        ctypes.cast(out, ctypes.c_void_p), ctypes.c_void_p(xyz.ctypes.data),
+                        ctypes.c_void_p(ctypes.addressof(secs)), _ptr(xin), _ptr(nin))
+    res = [out[i].as_dict() for i in range(n)]
+    pos = []
+    for i, q in enumerate(systems):
+        nm = res[i]["n_molecules"]
+        pos.append(xyz[offs[i]: offs[i] + nm * q.chain.n_beads * 3].reshape(nm, q.chain.n_beads, 3))
+    del keep
+    return res, pos, secs.value
+
+
+def alkane_grow_vacuum(ff, chain, beta, n, seed=1, threads=0):
+    """Chains grown in vacuum: (w[n], theta[n, nb-2], cos_phi[n, nb-3])."""
+    L = _alkane_lib()
+    o = off(ff)
+    c = oalkane(chain, ff)
+    nb = chain.n_beads
+    w = np.empty(n)
+    th = np.empty(n * max(0, nb - 2))
+    cp = np.empty(n * max(0, nb - 3))
+    L.oracle_alkane_grow_vacuum(ctypes.byref(o), ctypes.byref(c), beta, n, seed, threads, _ptr(w),
+                                _ptr(th) if th.size else None, _ptr(cp) if cp.size else None)
+    return w, th.reshape(n, max(0, nb - 2)), cp.reshape(n, max(0, nb - 3))
+
+
+def alkane_energy(ff, system, xyz):
+    """(framework-molecule VDW, molecule-molecule VDW, internal) of molecules xyz[n, nb, 3] in the system."""
+    L = _alkane_lib()
+    arr, keep = _alkane_setups(ff, [system])
+    x = np.ascontiguousarray(xyz, dtype=np.float64)
+    out = np.empty(3)
+    L.oracle_alkane_energy(ctypes.byref(arr[0]), _ptr(x), int(x.size // (3 * system.chain.n_beads)), _ptr(out))
+    del keep
+    return tuple(out)
+
+
+def alkane_bead_energies(ff, system, xyz, beads, types, skip=-1):
+    """Per-bead (framework, molecule, overlap) energies of single beads against the framework and molecules xyz."""
+    L = _alkane_lib()
+    arr, keep = _alkane_setups(ff, [system])
+    x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1)
+    b = np.ascontiguousarray(beads, dtype=np.float64).reshape(-1)
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    n = len(t)
+    fw, mm, ov = np.empty(n), np.empty(n), np.empty(n, dtype=np.int32)
+    L.oracle_alkane_bead_energies(ctypes.byref(arr[0]), _ptr(x) if x.size else None,
+                                  int(x.size // (3 * system.chain.n_beads)), _ptr(b), _ptr(t), n, skip, _ptr(fw),
+                                  _ptr(mm), _ptr(ov))
+    del keep
+    return fw, mm, ov

@@ -74,6 +74,15 @@ class GcmcChainResult(ctypes.Structure):
         return d
 
 
+class AlkanePlan(ctypes.Structure):
+    _fields_ = [("cluster_big", ctypes.c_int32), ("cluster_small", ctypes.c_int32), ("threads", ctypes.c_int32),
+                ("split", ctypes.c_int32), ("moves_per_launch", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("ms_per_move", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+
+
 class GridStats(ctypes.Structure):
     _fields_ = [("pair_count", ctypes.c_int64), ("n_images", ctypes.c_int64), ("h2d_bytes", ctypes.c_int64),
                 ("d2h_bytes", ctypes.c_int64)]
@@ -138,6 +147,20 @@ def lib():
         L.rg_ewald_accept.argtypes = [vp]
         L.rg_ewald_get_structure_factors.argtypes = [vp, i32, vp, i64]
         L.rg_ewald_set_structure_factors.argtypes = [vp, vp, i64]
+        from .alkane import RgAlkaneChain
+        L.rg_alkane_create.argtypes = [vp, P(RgForceField), vp, i32, ctypes.c_uint64, P(vp)]
+        L.rg_alkane_destroy.argtypes = [vp]
+        L.rg_alkane_autotune.argtypes = [vp, i32, P(AlkanePlan)]
+        L.rg_alkane_set_plan.argtypes = [vp, P(AlkanePlan)]
+        L.rg_alkane_get_plan.argtypes = [vp, P(AlkanePlan)]
+        L.rg_alkane_run.argtypes = [vp, i64, i32]
+        L.rg_alkane_results.argtypes = [vp, vp]
+        L.rg_alkane_get_positions.argtypes = [vp, i32, vp, i32, P(i32)]
+        L.rg_alkane_set_positions.argtypes = [vp, i32, vp, i32, d]
+        L.rg_alkane_pair_count.argtypes = [vp, P(ctypes.c_uint64)]
+        L.rg_alkane_bead_energies.argtypes = [vp, i32, vp, vp, i32, i32, vp, vp, vp]
+        L.rg_alkane_grow_vacuum.argtypes = [vp, P(RgForceField), P(RgAlkaneChain), d, i64, ctypes.c_uint64, P(d), vp,
+                                            vp, vp]
         _lib = L
     return _lib
 
@@ -532,3 +555,129 @@ class Proposal:
         check(self.ctx.handle, lib().rg_proposal_density(self.handle, ctypes.c_void_p(s.ctypes.data), len(s),
                                                          ctypes.c_void_p(out.ctypes.data)), "rg_proposal_density")
         return out
+
+
+class Alkane:
+    """A batch of independent systems running GCMC of flexible chains (rg_alkane)."""
+
+    def __init__(self, ctx: Context, ff: ForceField, systems, seed: int = 1):
+        from .alkane import RgAlkaneChain, chain_struct
+
+        class RgAlkaneSystem(ctypes.Structure):
+            _fields_ = [("box", RgBox), ("framework", ctypes.c_void_p), ("n_framework", ctypes.c_int32),
+                        ("max_molecules", ctypes.c_int32), ("chain", RgAlkaneChain), ("beta", ctypes.c_double),
+                        ("fugacity", ctypes.c_double), ("w_ig", ctypes.c_double), ("max_translation", ctypes.c_double),
+                        ("p_translation", ctypes.c_double), ("p_swap", ctypes.c_double)]
+
+        self.ctx = ctx
+        self.ff = ff
+        self.systems = list(systems)
+        n = len(self.systems)
+        arr = (RgAlkaneSystem * n)()
+        self._keep = []
+        for i, q in enumerate(self.systems):
+            fw = np.ascontiguousarray(q.framework, dtype=ATOM_DTYPE)
+            self._keep.append(fw)
+            arr[i].box = box_struct(q.cell)
+            arr[i].framework = fw.ctypes.data if len(fw) else None
+            arr[i].n_framework = len(fw)
+            arr[i].max_molecules = q.max_molecules
+            arr[i].chain = chain_struct(q.chain, ff)
+            arr[i].beta, arr[i].fugacity, arr[i].w_ig = q.beta, q.fugacity, q.w_ig
+            arr[i].max_translation, arr[i].p_translation, arr[i].p_swap = q.max_translation, q.p_translation, q.p_swap
+        ffs = ff_struct(ff)
+        h = ctypes.c_void_p()
+        check(ctx.handle, lib().rg_alkane_create(ctx.handle, ctypes.byref(ffs), ctypes.cast(arr, ctypes.c_void_p), n,
+                                                 seed, ctypes.byref(h)), "rg_alkane_create")
+        self.handle = h
+        ctx.adopt(self)
+
+    def close(self):
+        if self.handle:
+            lib().rg_alkane_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def autotune(self, moves_per_candidate: int = 8) -> dict:
+        pl = AlkanePlan()
+        check(self.ctx.handle, lib().rg_alkane_autotune(self.handle, moves_per_candidate, ctypes.byref(pl)),
+              "rg_alkane_autotune")
+        return pl.as_dict()
+
+    def plan(self) -> dict:
+        pl = AlkanePlan()
+        check(self.ctx.handle, lib().rg_alkane_get_plan(self.handle, ctypes.byref(pl)), "rg_alkane_get_plan")
+        return pl.as_dict()
+
+    def set_plan(self, cluster_big=1, cluster_small=1, threads=128, split=0, moves_per_launch=64):
+        pl = AlkanePlan(cluster_big, cluster_small, threads, split, moves_per_launch, 0, 0.0)
+        check(self.ctx.handle, lib().rg_alkane_set_plan(self.handle, ctypes.byref(pl)), "rg_alkane_set_plan")
+
+    def run(self, moves: int, record: bool = True):
+        check(self.ctx.handle, lib().rg_alkane_run(self.handle, moves, 1 if record else 0), "rg_alkane_run")
+
+    def pair_count(self) -> int:
+        v = ctypes.c_uint64()
+        check(self.ctx.handle, lib().rg_alkane_pair_count(self.handle, ctypes.byref(v)), "rg_alkane_pair_count")
+        return int(v.value)
+
+    def results(self):
+        n = len(self.systems)
+        out = (GcmcChainResult * n)()
+        check(self.ctx.handle, lib().rg_alkane_results(self.handle, ctypes.cast(out, ctypes.c_void_p)),
+              "rg_alkane_results")
+        return [out[i].as_dict() for i in range(n)]
+
+    def positions(self, system: int) -> np.ndarray:
+        q = self.systems[system]
+        cap = 3 * q.max_molecules * q.chain.n_beads
+        buf = np.empty(cap)
+        n = ctypes.c_int32()
+        check(self.ctx.handle, lib().rg_alkane_get_positions(self.handle, system, ctypes.c_void_p(buf.ctypes.data),
+                                                             cap, ctypes.byref(n)), "rg_alkane_get_positions")
+        return buf[: 3 * n.value * q.chain.n_beads].reshape(n.value, q.chain.n_beads, 3)
+
+    def set_positions(self, system: int, xyz, energy: float = 0.0):
+        x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1)
+        nb = self.systems[system].chain.n_beads
+        check(self.ctx.handle, lib().rg_alkane_set_positions(self.handle, system, ctypes.c_void_p(x.ctypes.data),
+                                                             len(x) // (3 * nb), energy), "rg_alkane_set_positions")
+
+    def bead_energies(self, system: int, xyz, types, skip: int = -1):
+        x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1)
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        n = len(t)
+        fw, mm, ov = np.empty(n), np.empty(n), np.empty(n, dtype=np.int32)
+        check(self.ctx.handle, lib().rg_alkane_bead_energies(self.handle, system, ctypes.c_void_p(x.ctypes.data),
+                                                             ctypes.c_void_p(t.ctypes.data), n, skip,
+                                                             ctypes.c_void_p(fw.ctypes.data),
+                                                             ctypes.c_void_p(mm.ctypes.data),
+                                                             ctypes.c_void_p(ov.ctypes.data)),
+              "rg_alkane_bead_energies")
+        return fw, mm, ov
+
+
+def alkane_grow_vacuum(ctx: Context, ff: ForceField, chain, beta: float, n: int, seed: int = 1, details: bool = False):
+    """Chains grown in vacuum on the device: returns <W> (the ideal-gas Rosenbluth weight), or with details
+    (<W>, w[n], theta[n, nb-2], cos_phi[n, nb-3])."""
+    from .alkane import chain_struct
+
+    c = chain_struct(chain, ff)
+    ffs = ff_struct(ff)
+    nb = chain.n_beads
+    mean = ctypes.c_double()
+    w = np.empty(n) if details else None
+    th = np.empty(n * max(0, nb - 2)) if details else None
+    cp = np.empty(n * max(0, nb - 3)) if details else None
+    ptr = (lambda a: None if a is None or a.size == 0 else ctypes.c_void_p(a.ctypes.data))
+    check(ctx.handle, lib().rg_alkane_grow_vacuum(ctx.handle, ctypes.byref(ffs), ctypes.byref(c), beta, n, seed,
+                                                  ctypes.byref(mean), ptr(w), ptr(th), ptr(cp)),
+          "rg_alkane_grow_vacuum")
+    if not details:
+        return mean.value
+    return mean.value, w, th.reshape(n, max(0, nb - 2)), cp.reshape(n, max(0, nb - 3))

@@ -234,6 +234,7 @@ def run_alkane(args, ctx, peak_fp32, world, rank, dist, torch):
     if world > 1:
         dist.barrier()
     pairs0 = a.pair_count()
+    launches0 = a.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     a.run(ALKANE_MOVES, record=True)
@@ -241,6 +242,7 @@ def run_alkane(args, ctx, peak_fp32, world, rank, dist, torch):
     torch.cuda.synchronize()
     secs = e0.elapsed_time(e1) / 1e3
     pairs = a.pair_count() - pairs0
+    launches = a.launch_count() - launches0
     if world > 1:
         t = torch.tensor([secs], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -261,6 +263,7 @@ def run_alkane(args, ctx, peak_fp32, world, rank, dist, torch):
                        "swap 1 : 1, 10 first-bead trials, 10 directions x 100 torsion spins per bead",
            "loading_min_mean_max": [min(loading), float(np.mean(loading)), max(loading)],
            "pairs_per_move": pairs / (ALKANE_SYSTEMS * ALKANE_MOVES),
+           "gpu_launches": launches, "kernel_launches_before_timed": launches0,
            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                         "frac": achieved / peak_fp32, "flops_per_pair": ALKANE_FLOPS_PER_PAIR},
            "e2e": {"value": world * ALKANE_SYSTEMS * ALKANE_MOVES / e2e_secs, "unit": "MC move attempts/s",

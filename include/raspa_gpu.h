@@ -374,8 +374,9 @@ typedef struct rg_alkane_plan
 rg_status rg_alkane_create(rg_ctx* ctx, const rg_forcefield* ff, const rg_alkane_system* systems, int n_systems,
                            uint64_t seed, rg_alkane** out);
 rg_status rg_alkane_destroy(rg_alkane* batch);
-/* Times candidate plans on the batch (each from the same snapshot of the state, restored afterwards so tuning does
- * not advance the simulation), keeps the fastest and returns it in *chosen (may be NULL). */
+/* Times candidate plans on the batch (cluster sizes 1/2/4 per class, 128/256/512 threads; each from the same snapshot
+ * of the state, restored afterwards so tuning does not advance the simulation), keeps the fastest and returns it in
+ * *chosen (may be NULL). */
 rg_status rg_alkane_autotune(rg_alkane* batch, int moves_per_candidate, rg_alkane_plan* chosen);
 rg_status rg_alkane_set_plan(rg_alkane* batch, const rg_alkane_plan* plan);
 rg_status rg_alkane_get_plan(rg_alkane* batch, rg_alkane_plan* plan);
@@ -397,6 +398,8 @@ rg_status rg_alkane_bead_energies(rg_alkane* batch, int system, const double* xy
 /* In-cutoff pair evaluations (trial bead x framework atom or molecule bead with r < rc) since creation, summed
  * over the systems: the algorithmic unit of the trial energies. */
 rg_status rg_alkane_pair_count(rg_alkane* batch, uint64_t* total);
+/* Monte Carlo kernel launches enqueued by this batch so far (each kernel node of a graph replay counts once). */
+rg_status rg_alkane_launch_count(rg_alkane* batch, int64_t* launches);
 /* Grows n chains in vacuum on the device: the ideal-gas Rosenbluth weight <W> (*w_mean; the W_IG of the acceptance
  * rule) and optionally per chain w[n], the bend angles theta[n*(nb-2)] and torsion cosines cos_phi[n*(nb-3)]. */
 rg_status rg_alkane_grow_vacuum(rg_ctx* ctx, const rg_forcefield* ff, const rg_alkane_chain* chain, double beta,

@@ -40,7 +40,7 @@ constexpr int kMaxTrials = 16;
 constexpr int kMaxTorsion = 128;
 constexpr int kMaxMolecules = 256;
 constexpr int kMaxTypes = 16;
-constexpr int kMaxWarps = 8;  // up to 256 threads per CTA
+constexpr int kMaxWarps = 16;  // up to 512 threads per CTA
 constexpr int kStats = 24;    // the rg_gcmc_chain_result record of gcmc.cu
 constexpr double kMinimumRosenbluth = 1e-150;  // ForceField::minimumRosenbluthFactor (forcefield.ixx:143)
 constexpr double kPi = 3.141592653589793238462643383279502884;
@@ -108,7 +108,7 @@ struct Shared
 {
   float4 tab[kMaxTypes * kMaxTypes];
   int4 bead[kMaxTrials];  // beads evaluated (fixed point, .w = type)
-  double red[kMaxWarps][2 * kMaxTrials];
+  double red[2][32 * kMaxWarps];  // per-thread framework / molecule partial sums
   unsigned red_ovl[kMaxWarps];
   double xch[2][2 * kMaxTrials];  // per-CTA sums exchanged across the cluster (double-buffered)
   unsigned xch_ovl[2];
@@ -119,11 +119,12 @@ struct Shared
   double3 dir[kMaxTrials];
   double tw[kMaxTrials];
   double intra[kMaxTrials];
-  int sel[kMaxTrials];
-  double lbf[kMaxTrials][kMaxTorsion];
-  double3 base;
+  double theta[kMaxBeads], psi[kMaxBeads];   // base-conformation bend angle and azimuth / pi per step (insertion)
+  double tD[kMaxBeads];                      // retrace: cosine of the old dihedral at step j
+  double ttw[kMaxBeads][kMaxTrials];         // torsion weight per step and direction
+  int tsel[kMaxBeads][kMaxTrials];           // selected spin per step and direction
   double W, eext, dU, stats[kStats];
-  int fail, kind, m, axis, n, accept, eval;
+  int fail, kind, m, axis, n, accept;
   unsigned long long pairs;
   double energy, disp, u_acc;
 };
@@ -144,11 +145,10 @@ __device__ __forceinline__ double3 cross(double3 a, double3 b)
 }
 __device__ __forceinline__ double3 normalized(double3 a) { return scale(1.0 / sqrt(dot(a, a)), a); }
 
-// double3::rotateAroundAxis (mathkit/double3.ixx:163-178): rotates v about the unit axis a
-__device__ __forceinline__ double3 rotateAround(double3 a, double3 v, double ang)
+// double3::rotateAroundAxis (mathkit/double3.ixx:163-178): rotates v about the unit axis a by the angle whose sine
+// and cosine are s and c
+__device__ __forceinline__ double3 rotateAroundSC(double3 a, double3 v, double s, double c)
 {
-  double s, c;
-  sincos(ang, &s, &c);
   const double w = 1.0 - c;
   return d3(v.x * (a.x * a.x * w + c) + v.y * (a.x * a.y * w + a.z * s) + v.z * (a.x * a.z * w - a.y * s),
             v.x * (a.x * a.y * w - a.z * s) + v.y * (a.y * a.y * w + c) + v.z * (a.y * a.z * w + a.x * s),
@@ -205,7 +205,7 @@ __device__ __forceinline__ double intraVdw(const Params& p, const SysDev& S, con
 }
 
 // all internal terms of a chain: bends, torsions, intra-molecular VDW (bonds are fixed)
-__device__ double internalEnergy(const Params& p, const SysDev& S, const double3* x)
+__device__ __noinline__ double internalEnergy(const Params& p, const SysDev& S, const double3* x)
 {
   double e = 0.0;
   for (int j = 2; j < S.nb; ++j) e += bendEnergy(S, x[j - 2], x[j - 1], x[j]);
@@ -214,156 +214,125 @@ __device__ double internalEnergy(const Params& p, const SysDev& S, const double3
   return e;
 }
 
-// CBMC::selectTrialPosition (cbmc/util.cpp:14-47) over the entries of lbf flagged in `ok`
-__device__ int selectShifted(const double* lbf, unsigned ok, int n, double u)
-{
-  double largest = -1e300;
-  for (int i = 0; i < n; ++i)
-    if ((ok >> i) & 1u) largest = fmax(largest, lbf[i]);
-  double sum = 0.0;
-  for (int i = 0; i < n; ++i)
-    if ((ok >> i) & 1u) sum += exp(lbf[i] - largest);
-  const double target = u * sum;
-  double cum = 0.0;
-  int last = -1;
-  for (int i = 0; i < n; ++i)
-  {
-    if (!((ok >> i) & 1u)) continue;
-    last = i;
-    cum += exp(lbf[i] - largest);
-    if (cum >= target) return i;
-  }
-  return last;
-}
-
-// Reduce-scatter of 16 per-lane values over a warp: afterwards lane l holds the warp sum of value
-// 8*b4 + 4*b3 + 2*b2 + b1 (b = bits of l); lanes l and l^1 hold the same sum.
-__device__ __forceinline__ double warpReduceScatter16(double v[16])
+// Trial selection by one warp, lane i holding trial i (i < 32): *sum = sum over the non-overlapping trials of
+// exp(lbf) (the Rosenbluth sum), and the index chosen by CBMC::selectTrialPosition (cbmc/util.cpp:14-47): the first
+// trial whose cumulative shifted Boltzmann factor reaches u times the total. retrace: trial 0 (the old position).
+// Returns -1 when every trial overlaps. Called by all 32 lanes of warp 0.
+__device__ __forceinline__ int warpSelect(double lbf, bool ok, bool retrace, double u, double* sum)
 {
   const int lane = threadIdx.x & 31;
+  const unsigned okMask = __ballot_sync(0xffffffffu, ok);
+  double mx = ok ? lbf : -1e300;
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
-  {
-    const bool hi = (lane >> 4) & 1;
-    const double send = hi ? v[i] : v[i + 8], keep = hi ? v[i + 8] : v[i];
-    v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  double direct = ok ? exp(lbf) : 0.0;
+  const double shifted = ok ? exp(lbf - mx) : 0.0;
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-  {
-    const bool hi = (lane >> 3) & 1;
-    const double send = hi ? v[i] : v[i + 4], keep = hi ? v[i + 4] : v[i];
-    v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-  }
+  for (int o = 16; o > 0; o >>= 1) direct += __shfl_xor_sync(0xffffffffu, direct, o);
+  double incl = shifted;
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+  for (int o = 1; o < 32; o <<= 1)
   {
-    const bool hi = (lane >> 2) & 1;
-    const double send = hi ? v[i] : v[i + 2], keep = hi ? v[i + 2] : v[i];
-    v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    const double t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
   }
-  {
-    const bool hi = (lane >> 1) & 1;
-    const double send = hi ? v[0] : v[1], keep = hi ? v[1] : v[0];
-    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
-  }
-  return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
-}
-__device__ __forceinline__ int scatterIndex(int lane)
-{
-  return 8 * ((lane >> 4) & 1) + 4 * ((lane >> 3) & 1) + 2 * ((lane >> 2) & 1) + ((lane >> 1) & 1);
+  const double total = __shfl_sync(0xffffffffu, incl, 31);
+  *sum = direct;
+  if (okMask == 0u) return -1;
+  if (retrace) return 0;
+  const unsigned hit = __ballot_sync(0xffffffffu, ok && incl >= u * total);
+  return hit ? __ffs(hit) - 1 : 31 - __clz(okMask);
 }
 
-// Pair terms of up to 16 beads (sh.bead) against `n` partners; per-thread FP32 partials in acc.
+// One bead against the partners partners[begin, n) with the given stride: FP32 pair terms from the fixed-point
+// displacement, accumulated in FP64. Bit b of ovl is set if a pair exceeds the overlap criterion.
 template <bool TRI, bool SKIP>
-__device__ __forceinline__ void pairLoop(const Shared& sh, const SysDev& S, const int4* partners, int begin, int n,
-                                         int stride, int nbd, int skip, float rc2, float ovlf, float acc[16],
-                                         unsigned& ovl, unsigned& inside)
+__device__ __forceinline__ void beadPartners(const Shared& sh, const SysDev& S, int4 B, const int4* partners,
+                                             int begin, int n, int stride, int skip, float rc2, float ovlf,
+                                             double& acc, unsigned& ovl, unsigned& inside, int b)
 {
+  const int bt = (B.w & 0xff) * kMaxTypes;
+#pragma unroll 4
   for (int i = begin; i < n; i += stride)
   {
     const int4 P = partners[i];
     if (SKIP && (P.w >> 8) == skip) continue;
-    const int pt = P.w & 0xff;
-#pragma unroll
-    for (int b = 0; b < kMaxTrials; ++b)
+    const float f0 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.x) - static_cast<uint32_t>(P.x))) * kFix;
+    const float f1 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.y) - static_cast<uint32_t>(P.y))) * kFix;
+    const float f2 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.z) - static_cast<uint32_t>(P.z))) * kFix;
+    float rx, ry, rz;
+    if (TRI)
     {
-      if (b >= nbd) break;
-      const int4 B = sh.bead[b];
-      const float f0 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.x) - static_cast<uint32_t>(P.x))) * kFix;
-      const float f1 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.y) - static_cast<uint32_t>(P.y))) * kFix;
-      const float f2 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.z) - static_cast<uint32_t>(P.z))) * kFix;
-      float rx, ry, rz;
-      if (TRI)
-      {
-        rx = fmaf(S.hf[0][0], f0, fmaf(S.hf[1][0], f1, S.hf[2][0] * f2));
-        ry = fmaf(S.hf[0][1], f0, fmaf(S.hf[1][1], f1, S.hf[2][1] * f2));
-        rz = fmaf(S.hf[0][2], f0, fmaf(S.hf[1][2], f1, S.hf[2][2] * f2));
-      }
-      else
-      {
-        rx = S.hf[0][0] * f0;
-        ry = S.hf[1][1] * f1;
-        rz = S.hf[2][2] * f2;
-      }
-      const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-      if (r2 < rc2)
-      {
-        const float4 q = sh.tab[(B.w & 0xff) * kMaxTypes + pt];
-        const float t = q.y * __frcp_rn(r2);
-        const float t3 = t * t * t;
-        const float e = q.x * (t3 * (t3 - 1.0f)) - q.z;
-        acc[b] += e;
-        inside += 1u;
-        if (e > ovlf) ovl |= 1u << b;
-      }
+      rx = fmaf(S.hf[0][0], f0, fmaf(S.hf[1][0], f1, S.hf[2][0] * f2));
+      ry = fmaf(S.hf[0][1], f0, fmaf(S.hf[1][1], f1, S.hf[2][1] * f2));
+      rz = fmaf(S.hf[0][2], f0, fmaf(S.hf[1][2], f1, S.hf[2][2] * f2));
+    }
+    else
+    {
+      rx = S.hf[0][0] * f0;
+      ry = S.hf[1][1] * f1;
+      rz = S.hf[2][2] * f2;
+    }
+    const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+    if (r2 < rc2)
+    {
+      const float4 q = sh.tab[bt + (P.w & 0xff)];
+      const float t = q.y * __frcp_rn(r2);
+      const float t3 = t * t * t;
+      const float e = q.x * (t3 * (t3 - 1.0f)) - q.z;
+      acc += static_cast<double>(e);
+      inside += 1u;
+      if (e > ovlf) ovl |= 1u << b;
     }
   }
 }
 
 // Framework + molecule energies of the nbd beads in sh.bead, summed over the cluster into sh.efw / sh.emm / sh.ovl.
-// The framework slice of this CTA is fwS[0, nfw); molecule beads are molS[0, nmb) (interleaved over the cluster
-// ranks). Called by every thread of every CTA of the cluster.
-__device__ void evalBeads(Shared& sh, const Params& p, const SysDev& S, const int4* fwS, int nfw, const int4* molS,
-                          int nmb, int nbd, int skip, Cl cl)
+// Thread t works on bead t % nbd with partner stream t / nbd: the framework slice of this CTA is fwS[0, nfw), the
+// molecule beads molS[0, nmb) are interleaved over the cluster ranks. The per-thread sums are reduced per bead in a
+// fixed order, the CTAs' sums in rank order, so every CTA ends with identical totals. Called by every thread of every
+// CTA of the cluster.
+__device__ __noinline__ void evalBeads(Shared& sh, const Params& p, const SysDev& S, const int4* fwS, int nfw, const int4* molS,
+                          int nmb, int nbd, int skip, Cl cl, int& eval)
 {
   const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = T >> 5;
   const int rank = cl.rank, C = cl.C;
-  float acc[16];
+  const int streams = T / nbd, b = tid % nbd, st = tid / nbd;
+  double afw = 0.0, amm = 0.0;
   unsigned ovl = 0, inside = 0;
-#pragma unroll
-  for (int b = 0; b < 16; ++b) acc[b] = 0.0f;
-  if (S.triclinic)
-    pairLoop<true, false>(sh, S, fwS, tid, nfw, T, nbd, -1, p.rc2_fw, p.overlap_f, acc, ovl, inside);
-  else
-    pairLoop<false, false>(sh, S, fwS, tid, nfw, T, nbd, -1, p.rc2_fw, p.overlap_f, acc, ovl, inside);
-  double v[16];
-#pragma unroll
-  for (int b = 0; b < 16; ++b) v[b] = static_cast<double>(acc[b]);
-  double r = warpReduceScatter16(v);
-  if (!(lane & 1)) sh.red[warp][scatterIndex(lane)] = r;
-#pragma unroll
-  for (int b = 0; b < 16; ++b) acc[b] = 0.0f;
-  if (S.triclinic)
-    pairLoop<true, true>(sh, S, molS, rank * T + tid, nmb, C * T, nbd, skip, p.rc2_mm, p.overlap_f, acc, ovl, inside);
-  else
-    pairLoop<false, true>(sh, S, molS, rank * T + tid, nmb, C * T, nbd, skip, p.rc2_mm, p.overlap_f, acc, ovl,
-                          inside);
+  if (st < streams)
+  {
+    const int4 B = sh.bead[b];
+    if (S.triclinic)
+    {
+      beadPartners<true, false>(sh, S, B, fwS, st, nfw, streams, -1, p.rc2_fw, p.overlap_f, afw, ovl, inside, b);
+      beadPartners<true, true>(sh, S, B, molS, rank * streams + st, nmb, C * streams, skip, p.rc2_mm, p.overlap_f,
+                               amm, ovl, inside, b);
+    }
+    else
+    {
+      beadPartners<false, false>(sh, S, B, fwS, st, nfw, streams, -1, p.rc2_fw, p.overlap_f, afw, ovl, inside, b);
+      beadPartners<false, true>(sh, S, B, molS, rank * streams + st, nmb, C * streams, skip, p.rc2_mm, p.overlap_f,
+                                amm, ovl, inside, b);
+    }
+  }
+  sh.red[0][tid] = afw;
+  sh.red[1][tid] = amm;
   inside = __reduce_add_sync(0xffffffffu, inside);
   if (lane == 0 && inside) atomicAdd(&sh.pairs, static_cast<unsigned long long>(inside));
-#pragma unroll
-  for (int b = 0; b < 16; ++b) v[b] = static_cast<double>(acc[b]);
-  r = warpReduceScatter16(v);
-  if (!(lane & 1)) sh.red[warp][kMaxTrials + scatterIndex(lane)] = r;
   ovl = __reduce_or_sync(0xffffffffu, ovl);
   if (lane == 0) sh.red_ovl[warp] = ovl;
   __syncthreads();
-  const int buf = sh.eval & 1;
+  const int buf = eval & 1;
+  eval += 1;
   if (tid < 2 * kMaxTrials)
   {
-    double s = 0.0;
-    for (int w = 0; w < nw; ++w) s += sh.red[w][tid];
-    sh.xch[buf][tid] = s;
+    // thread t < 16 sums the framework part of bead t, thread 16 + t its molecule part
+    const int which = tid >= kMaxTrials, bb = tid - which * kMaxTrials;
+    double sum = 0.0;
+    if (bb < nbd)
+      for (int k = 0; k < streams; ++k) sum += sh.red[which][bb + nbd * k];
+    sh.xch[buf][tid] = sum;
   }
   if (tid == 2 * kMaxTrials)
   {
@@ -378,12 +347,12 @@ __device__ void evalBeads(Shared& sh, const Params& p, const SysDev& S, const in
     cluster.sync();
     if (tid < 2 * kMaxTrials)
     {
-      double s = 0.0;
-      for (int q = 0; q < C; ++q) s += cluster.map_shared_rank(&sh.xch[buf][0], q)[tid];
+      double sum = 0.0;
+      for (int q = 0; q < C; ++q) sum += cluster.map_shared_rank(&sh.xch[buf][0], q)[tid];
       if (tid < kMaxTrials)
-        sh.efw[tid] = s;
+        sh.efw[tid] = sum;
       else
-        sh.emm[tid - kMaxTrials] = s;
+        sh.emm[tid - kMaxTrials] = sum;
     }
     if (tid == 2 * kMaxTrials)
     {
@@ -400,24 +369,66 @@ __device__ void evalBeads(Shared& sh, const Params& p, const SysDev& S, const in
     if (tid == 2 * kMaxTrials) sh.ovl = sh.xch_ovl[buf];
   }
   __syncthreads();
-  if (tid == 0) sh.eval += 1;
-  __syncthreads();
 }
 
-// Generates the trial positions of step j >= 2 (base conformation + torsion selection per direction) into sh.dir
-// and sh.tw. retrace: the old orientation is the base and torsion trial 0 of direction 0.
-__device__ void torsionTrials(Shared& sh, const Params& p, const SysDev& S, int s, long long move, int j, bool retrace)
+// Four spin angles per Philox draw: word k of draw (j, i, q) gives spin 4q + k of direction i at step j, the angle
+// (2u - 1) pi with u = (word + 1/2) 2^-32; sincospi returns its sine and cosine.
+__device__ __forceinline__ uint4 spinWords(const Params& p, int s, long long move, int j, int i, int q)
 {
-  const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = T >> 5;
+  uint32_t c[4] = {slot(kKindSpin, j, i, q), static_cast<uint32_t>(move), static_cast<uint32_t>(move >> 32),
+                   static_cast<uint32_t>(s)};
+  rgd::philox(c, static_cast<uint32_t>(p.seed), static_cast<uint32_t>(p.seed >> 32));
+  return make_uint4(c[0], c[1], c[2], c[3]);
+}
+__device__ __forceinline__ void spinAngle(uint32_t word, double* sa, double* ca)
+{
+  const double u = (static_cast<double>(word) + 0.5) * 0x1.0p-32;
+  sincospi(2.0 * u - 1.0, sa, ca);
+}
+
+// TraPPE torsion energy from the torsion cosine (torsion_potential.cpp:464-473)
+__device__ __forceinline__ double trappe(const SysDev& S, double cp)
+{
+  const double* q = S.torsion;
+  return q[0] + (1.0 + cp) * (q[1] + q[3] - 2.0 * (cp - 1.0) * (q[2] - 2.0 * q[3] * cp));
+}
+
+// Signed dihedral (cos D, sin D) about the unit axis a = normalized(x2 - x3) of the position y grown from x3, with
+// reference atom x1 (the torsion x1-x2-x3-y): cos D is TorsionPotential's cos(phi), and a spin of y by alpha about a
+// (rotateAroundAxis) turns D into D - alpha.
+__device__ __forceinline__ void signedDihedral(double3 x1, double3 x2, double3 x3, double3 y, double3 a, double* cD,
+                                               double* sD)
+{
+  const double3 dcb = scale(-1.0, a);
+  const double3 dab = sub(x1, x2), ddc = sub(y, x3);
+  const double3 dr = normalized(sub(dab, scale(dot(dab, dcb), dcb)));
+  const double3 ds = normalized(sub(ddc, scale(dot(ddc, dcb), dcb)));
+  *cD = dot(dr, ds);
+  *sD = dot(cross(dr, ds), a);
+}
+
+// Everything of a growth or retrace that does not depend on where the chain goes, done once per move by the warps
+// in parallel (no barrier inside):
+//  * insertion: the bend angle and azimuth of every step j >= 2, drawn exactly from sin(theta) exp(-beta U_bend) by
+//    a warp vote over Gaussian proposals;
+//  * every step j >= 3 and direction i: the coupled-decoupled torsion selection of selectTorsionOrientation
+//    (operators.cpp:135-196). A spin by a uniform angle alpha about the bond gives the dihedral D - alpha, itself
+//    uniform whatever D is, so the spins are drawn directly as uniform dihedrals phi: the torsion weight
+//    (1/n) sum exp(-beta U(phi_s)) and the selected phi do not depend on the chain; the step then turns its base by
+//    alpha = D - phi_sel. In a retrace, spin 0 of direction 0 is the old dihedral itself (sh.tD holds its cosine).
+//  * step 2 has no torsion: its weight is 1 and its spin is uniform.
+__device__ __noinline__ void precomputeGrowth(Shared& sh, const Params& p, const SysDev& S, int s, long long move, bool retrace)
+{
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int nb = S.nb, kd = S.n_dir, nt = S.n_tors;
   const double beta = S.beta;
-  const int kd = S.n_dir, nt = S.n_tors;
-  const double3 cur = sh.x[j - 1];
-  const double3 a = normalized(sub(sh.x[j - 2], cur));
-  if (!retrace)
+  const int nTheta = retrace ? 0 : max(0, nb - 2);
+  const int nTors = max(0, nb - 2) * kd;  // steps j = 2..nb-1
+  for (int task = warp; task < nTheta + nTors; task += nw)
   {
-    // exact base-conformation sample: Gaussian proposals around theta0 accepted with probability sin(theta)
-    if (warp == 0)
+    if (task < nTheta)
     {
+      const int j = 2 + task;
       double theta = S.bend_theta0, psi = 0.0;
       for (int round = 0; round < 64; ++round)
       {
@@ -425,75 +436,68 @@ __device__ void torsionTrials(Shared& sh, const Params& p, const SysDev& S, int 
         const double2 v = urand(p, s, move, slot(kKindTheta, j, round, 2 * lane + 1));
         const double g = sqrt(-2.0 * log(1.0 - u.x)) * cospi(2.0 * u.y);
         const double th = S.bend_theta0 + S.sigma_theta * g;
-        const bool ok = th > 0.0 && th < kPi && v.x < sin(th);
+        const bool ok = th > 0.0 && th < kPi && v.x < sinpi(th / kPi);
         const unsigned bal = __ballot_sync(0xffffffffu, ok);
         if (bal)
         {
           const int l = __ffs(bal) - 1;
           theta = __shfl_sync(0xffffffffu, th, l);
-          psi = 2.0 * kPi * __shfl_sync(0xffffffffu, v.y, l);
+          psi = 2.0 * __shfl_sync(0xffffffffu, v.y, l);  // azimuth / pi
           break;
         }
       }
       if (lane == 0)
       {
-        // orthonormal e1, e2 perpendicular to a; direction at angle theta from a, azimuth psi
-        const double3 h = fabs(a.x) < 0.6 ? d3(1, 0, 0) : (fabs(a.y) < 0.6 ? d3(0, 1, 0) : d3(0, 0, 1));
-        const double3 e1 = normalized(cross(a, h));
-        const double3 e2 = cross(a, e1);
-        double sp, cp, st, ct;
-        sincos(psi, &sp, &cp);
-        sincos(theta, &st, &ct);
-        const double3 u = add(scale(ct, a), scale(st, add(scale(cp, e1), scale(sp, e2))));
-        sh.base = add(cur, scale(S.bond, u));
+        sh.theta[j] = theta;
+        sh.psi[j] = psi;
       }
+      continue;
     }
-  }
-  else if (tid == 0)
-  {
-    sh.base = sh.old[j];
-  }
-  __syncthreads();
-  const double3 base = sub(sh.base, cur);
-  // torsion energies of every spin of every direction
-  for (int idx = tid; idx < kd * nt; idx += T)
-  {
-    const int i = idx / nt, sp = idx - i * nt;
-    double lb = 0.0;
-    if (j >= 3)
+    const int t = task - nTheta, j = 2 + t / kd, i = t - (j - 2) * kd;
+    if (j == 2)
     {
-      const double ang = (retrace && i == 0 && sp == 0)
-                             ? 0.0
-                             : (2.0 * urand(p, s, move, slot(kKindSpin, j, i, sp)).x - 1.0) * kPi;
-      const double3 pos = add(cur, rotateAround(a, base, ang));
-      lb = -beta * torsionEnergy(S, sh.x[j - 3], sh.x[j - 2], cur, pos);
+      // no torsion: all spins weigh 1; the selected one is uniform
+      if (lane == 0)
+      {
+        sh.ttw[j][i] = 1.0;
+        sh.tsel[j][i] = static_cast<int>(urand(p, s, move, slot(kKindSelect, j, i, 0)).x * nt) % nt;
+      }
+      continue;
     }
-    sh.lbf[i][sp] = lb;
-  }
-  __syncthreads();
-  // per direction: torsion weight and Boltzmann selection (one warp per direction)
-  for (int i = warp; i < kd; i += nw)
-  {
+    // lane owns spins 4 lane .. 4 lane + 3 (one Philox draw, four 32-bit words)
+    double lbf[4];
+    const uint4 w = spinWords(p, s, move, j, i, lane);
+    const uint32_t words[4] = {w.x, w.y, w.z, w.w};
     double mx = -1e300;
+#pragma unroll
     for (int k = 0; k < 4; ++k)
     {
       const int sp = 4 * lane + k;
-      if (sp < nt) mx = fmax(mx, sh.lbf[i][sp]);
+      lbf[k] = -1e300;
+      if (sp < nt)
+      {
+        const double cp = (retrace && i == 0 && sp == 0)
+                              ? sh.tD[j]
+                              : cospi(2.0 * ((static_cast<double>(words[k]) + 0.5) * 0x1.0p-32) - 1.0);
+        lbf[k] = -beta * trappe(S, fmin(1.0, fmax(-1.0, cp)));
+        mx = fmax(mx, lbf[k]);
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    double local = 0.0;
+    double e[4], local = 0.0;
+#pragma unroll
     for (int k = 0; k < 4; ++k)
     {
-      const int sp = 4 * lane + k;
-      if (sp < nt) local += exp(sh.lbf[i][sp] - mx);
+      e[k] = (4 * lane + k < nt) ? exp(lbf[k] - mx) : 0.0;
+      local += e[k];
     }
     double incl = local;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1)
     {
-      const double t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
+      const double v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
     }
     const double total = __shfl_sync(0xffffffffu, incl, 31);
     int sel = 0;
@@ -502,54 +506,100 @@ __device__ void torsionTrials(Shared& sh, const Params& p, const SysDev& S, int 
       const double target = urand(p, s, move, slot(kKindSelect, j, i, 0)).x * total;
       const unsigned bal = __ballot_sync(0xffffffffu, incl >= target && local > 0.0);
       const int l = bal ? __ffs(bal) - 1 : 31;
+      int mine = -1;
       if (lane == l)
       {
         double cum = incl - local;
-        sel = -1;
+#pragma unroll
         for (int k = 0; k < 4; ++k)
         {
-          const int sp = 4 * lane + k;
-          if (sp >= nt) break;
-          cum += exp(sh.lbf[i][sp] - mx);
-          sel = sp;
-          if (cum >= target) break;
+          if (4 * lane + k >= nt || mine >= 0) continue;
+          cum += e[k];
+          if (cum >= target) mine = 4 * lane + k;
         }
+        if (mine < 0) mine = min(4 * lane + 3, nt - 1);
       }
-      sel = __shfl_sync(0xffffffffu, sel, l);
-      if (sel < 0) sel = nt - 1;
+      sel = __shfl_sync(0xffffffffu, mine, l);
     }
     if (lane == 0)
     {
-      sh.tw[i] = exp(mx) * total / static_cast<double>(nt);
-      sh.sel[i] = sel;
+      sh.ttw[j][i] = exp(mx) * total / static_cast<double>(nt);
+      sh.tsel[j][i] = sel;
     }
   }
-  __syncthreads();
-  if (tid < kd)
+}
+
+// Trial positions of step j >= 2 from the precomputed selections: direction i turns the step's base by
+// alpha = D - phi_sel (retrace: direction 0 is the old position). Threads i < kd; ends with a barrier.
+__device__ __noinline__ void stepTrials(Shared& sh, const Params& p, const SysDev& S, int s, long long move, int j, bool retrace)
+{
+  const int tid = threadIdx.x;
+  if (tid < S.n_dir)
   {
-    const int i = tid, sp = sh.sel[i];
+    const int i = tid;
+    const double3 cur = sh.x[j - 1];
+    const double3 a = normalized(sub(sh.x[j - 2], cur));
+    double3 base;
+    if (retrace)
+      base = sh.old[j];
+    else
+    {
+      // direction at angle theta from a with azimuth psi about a
+      const double3 h = fabs(a.x) < 0.6 ? d3(1, 0, 0) : (fabs(a.y) < 0.6 ? d3(0, 1, 0) : d3(0, 0, 1));
+      const double3 e1 = normalized(cross(a, h));
+      const double3 e2 = cross(a, e1);
+      double sp, cp, st, ct;
+      sincospi(sh.psi[j], &sp, &cp);
+      sincospi(sh.theta[j] / kPi, &st, &ct);
+      base = add(cur, scale(S.bond, add(scale(ct, a), scale(st, add(scale(cp, e1), scale(sp, e2))))));
+    }
     double3 pos;
     if (retrace && i == 0)
       pos = sh.old[j];
     else
     {
-      const double ang = (2.0 * urand(p, s, move, slot(kKindSpin, j, i, sp)).x - 1.0) * kPi;
-      pos = add(cur, rotateAround(a, base, ang));
+      const int sel = sh.tsel[j][i];
+      const uint4 w = spinWords(p, s, move, j, i, sel >> 2);
+      const uint32_t words[4] = {w.x, w.y, w.z, w.w};
+      double sphi, cphi;
+      spinAngle(words[sel & 3], &sphi, &cphi);
+      double sa = sphi, ca = cphi;  // step 2: any uniform angle (no dihedral)
+      if (j >= 3)
+      {
+        double cD, sD;
+        signedDihedral(sh.x[j - 3], sh.x[j - 2], cur, base, a, &cD, &sD);
+        ca = cD * cphi + sD * sphi;  // cos(D - phi)
+        sa = sD * cphi - cD * sphi;  // sin(D - phi)
+      }
+      pos = add(cur, rotateAroundSC(a, sub(base, cur), sa, ca));
     }
     sh.dir[i] = pos;
+    sh.tw[i] = sh.ttw[j][i];
+    sh.bead[i] = toFixed(S, pos, S.types[j]);
   }
   __syncthreads();
 }
 
 // One growth (insertion: retrace = false) or retrace of molecule m (its positions in sh.old). On return sh.fail,
 // sh.W (Rosenbluth weight), sh.eext (external energy of the chain) and sh.x (grown chain) are set.
-__device__ void growChain(Shared& sh, const Params& p, const SysDev& S, int s, long long move, bool retrace, int m,
-                          const int4* fwS, int nfw, const int4* molS, int nmb, Cl cl)
+__device__ __noinline__ void growChain(Shared& sh, const Params& p, const SysDev& S, int s, long long move, bool retrace, int m,
+                          const int4* fwS, int nfw, const int4* molS, int nmb, Cl cl, int& eval)
 {
   const int tid = threadIdx.x;
   const double beta = S.beta;
   const int skip = retrace ? m : -1;
   const int k1 = S.n_first, kd = S.n_dir, nb = S.nb;
+  if (retrace && tid >= 3 && tid < nb)
+  {
+    // the old dihedral of every step (spin 0 of direction 0 of the retrace)
+    const int j = tid;
+    double cD, sD;
+    signedDihedral(sh.old[j - 3], sh.old[j - 2], sh.old[j - 1], sh.old[j],
+                   normalized(sub(sh.old[j - 2], sh.old[j - 1])), &cD, &sD);
+    sh.tD[j] = cD;
+  }
+  __syncthreads();
+  precomputeGrowth(sh, p, S, s, move, retrace);
   // first bead (multiple_first_bead.cpp:20-76)
   if (tid < k1)
   {
@@ -573,27 +623,22 @@ __device__ void growChain(Shared& sh, const Params& p, const SysDev& S, int s, l
     sh.bead[tid] = f;
   }
   __syncthreads();
-  evalBeads(sh, p, S, fwS, nfw, molS, nmb, k1, skip, cl);
-  if (tid == 0)
+  evalBeads(sh, p, S, fwS, nfw, molS, nmb, k1, skip, cl, eval);
+  if (tid < 32)
   {
-    unsigned ok = 0;
-    double lbf[kMaxTrials], sum = 0.0;
-    for (int t = 0; t < k1; ++t)
+    const bool ok = tid < k1 && !((sh.ovl >> tid) & 1u);
+    const double lbf = ok ? -beta * (sh.efw[tid] + sh.emm[tid]) : 0.0;
+    double sum;
+    const int sel = warpSelect(lbf, ok, retrace, urand(p, s, move, slot(kKindMove, 0, 0, 3)).x, &sum);
+    if (tid == 0)
     {
-      lbf[t] = -beta * (sh.efw[t] + sh.emm[t]);
-      if (!((sh.ovl >> t) & 1u))
+      sh.fail = (sel < 0) || (retrace && ((sh.ovl & 1u) != 0u));
+      if (!sh.fail)
       {
-        ok |= 1u << t;
-        sum += exp(lbf[t]);
+        sh.W = sum / static_cast<double>(k1);
+        sh.x[0] = sh.dir[sel];
+        sh.eext = sh.efw[sel] + sh.emm[sel];
       }
-    }
-    sh.fail = (ok == 0u) || (retrace && !(ok & 1u));
-    if (!sh.fail)
-    {
-      const int sel = retrace ? 0 : selectShifted(lbf, ok, k1, urand(p, s, move, slot(kKindMove, 0, 0, 3)).x);
-      sh.W = sum / static_cast<double>(k1);
-      sh.x[0] = sh.dir[sel];
-      sh.eext = sh.efw[sel] + sh.emm[sel];
     }
   }
   __syncthreads();
@@ -619,41 +664,34 @@ __device__ void growChain(Shared& sh, const Params& p, const SysDev& S, int s, l
         }
         sh.dir[tid] = r;
         sh.tw[tid] = 1.0;
+        sh.bead[tid] = toFixed(S, r, S.types[1]);
       }
       __syncthreads();
     }
     else
     {
-      torsionTrials(sh, p, S, s, move, j, retrace);
+      stepTrials(sh, p, S, s, move, j, retrace);
     }
-    if (tid < kd) sh.bead[tid] = toFixed(S, sh.dir[tid], S.types[j]);
-    __syncthreads();
-    evalBeads(sh, p, S, fwS, nfw, molS, nmb, kd, skip, cl);
-    if (tid < kd) sh.intra[tid] = (j >= 4) ? intraVdw(p, S, sh.x, j, sh.dir[tid]) : 0.0;
-    __syncthreads();
-    if (tid == 0)
+    evalBeads(sh, p, S, fwS, nfw, molS, nmb, kd, skip, cl, eval);
+    if (tid < 32)
     {
-      unsigned ok = 0;
-      double lbf[kMaxTrials], sum = 0.0;
-      for (int i = 0; i < kd; ++i)
+      const bool ok = tid < kd && !((sh.ovl >> tid) & 1u);
+      const double intra = (ok && j >= 4) ? intraVdw(p, S, sh.x, j, sh.dir[tid]) : 0.0;
+      const double lbf = ok ? -beta * (sh.efw[tid] + sh.emm[tid] + intra) : 0.0;
+      double sum;
+      const int sel = warpSelect(lbf, ok, retrace, urand(p, s, move, slot(kKindSelect, j, 255, 0)).x, &sum);
+      if (tid == 0)
       {
-        lbf[i] = -beta * (sh.efw[i] + sh.emm[i] + sh.intra[i]);
-        if (!((sh.ovl >> i) & 1u))
+        sh.fail = (sel < 0) || (retrace && ((sh.ovl & 1u) != 0u));
+        if (!sh.fail)
         {
-          ok |= 1u << i;
-          sum += exp(lbf[i]);
+          Wc *= sh.tw[sel] * sum / static_cast<double>(kd);
+          if (!retrace && Wc < kMinimumRosenbluth) sh.fail = 1;
+          sh.x[j] = sh.dir[sel];
+          sh.eext += sh.efw[sel] + sh.emm[sel];
         }
+        if (j == nb - 1 && !sh.fail) sh.W *= Wc;
       }
-      sh.fail = (ok == 0u) || (retrace && !(ok & 1u));
-      if (!sh.fail)
-      {
-        const int sel = retrace ? 0 : selectShifted(lbf, ok, kd, urand(p, s, move, slot(kKindSelect, j, 255, 0)).x);
-        Wc *= sh.tw[sel] * sum / static_cast<double>(kd);
-        if (!retrace && Wc < kMinimumRosenbluth) sh.fail = 1;
-        sh.x[j] = sh.dir[sel];
-        sh.eext += sh.efw[sel] + sh.emm[sel];
-      }
-      if (j == nb - 1 && !sh.fail) sh.W *= Wc;
     }
     __syncthreads();
     if (sh.fail) return;
@@ -667,7 +705,7 @@ __device__ __forceinline__ int4* dynamicBase(unsigned char* smem)
 
 // The persistent Monte Carlo kernel: one cluster per system, `moves` move attempts per system.
 template <int T>
-__global__ void __launch_bounds__(T) alkaneKernel(Params p, const int* __restrict__ order, int fw_cap, int moves)
+__global__ void __launch_bounds__(T, 1) alkaneKernel(Params p, const int* __restrict__ order, int fw_cap, int moves)
 {
   extern __shared__ __align__(16) unsigned char smem[];
   Shared& sh = *reinterpret_cast<Shared*>(smem);
@@ -699,11 +737,11 @@ __global__ void __launch_bounds__(T) alkaneKernel(Params p, const int* __restric
   {
     sh.n = n0;
     sh.energy = p.energy[s];
-    sh.eval = 0;
     sh.pairs = 0ull;
     for (int k = 0; k < kStats; ++k) sh.stats[k] = st[k];
   }
   const long long move0 = p.move_base[s];
+  int eval = 0;  // evaluation counter (selects the exchange buffer), identical in every thread
   __syncthreads();
 
   for (int mv = 0; mv < moves; ++mv)
@@ -741,7 +779,7 @@ __global__ void __launch_bounds__(T) alkaneKernel(Params p, const int* __restric
         sh.bead[nb + tid] = make_int4(q.x, q.y, q.z, S.types[tid]);
       }
       __syncthreads();
-      evalBeads(sh, p, S, fwS, nfw, molS, nmb, 2 * nb, m, cl);
+      evalBeads(sh, p, S, fwS, nfw, molS, nmb, 2 * nb, m, cl, eval);
       if (tid == 0)
       {
         const unsigned newMask = (1u << nb) - 1u;
@@ -770,7 +808,7 @@ __global__ void __launch_bounds__(T) alkaneKernel(Params p, const int* __restric
     else if (kind == 2 && n < S.max_molecules)
     {
       // CBMC insertion (insertion_cbmc.cpp:34-207): Pacc = beta f V / (N+1) W / W_IG
-      growChain(sh, p, S, s, move, false, -1, fwS, nfw, molS, nmb, cl);
+      growChain(sh, p, S, s, move, false, -1, fwS, nfw, molS, nmb, cl, eval);
       if (tid == 0 && !sh.fail)
       {
         const double pacc = S.beta * S.fugacity * S.volume / static_cast<double>(n + 1) * sh.W / S.w_ig;
@@ -800,7 +838,7 @@ __global__ void __launch_bounds__(T) alkaneKernel(Params p, const int* __restric
         sh.old[tid] = d3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
       }
       __syncthreads();
-      growChain(sh, p, S, s, move, true, m, fwS, nfw, molS, nmb, cl);
+      growChain(sh, p, S, s, move, true, m, fwS, nfw, molS, nmb, cl, eval);
       if (tid == 0 && !sh.fail)
       {
         const double pacc = static_cast<double>(n) / (S.beta * S.fugacity * S.volume) * S.w_ig / sh.W;
@@ -870,13 +908,10 @@ __global__ void __launch_bounds__(128) beadKernel(Params p, int s, int fw_cap, c
     molS[i] = toFixed(S, d3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]), S.types[b] | (m << 8));
   }
   if (tid < nbd) sh.bead[tid] = toFixed(S, d3(xyz[3 * tid], xyz[3 * tid + 1], xyz[3 * tid + 2]), types[tid]);
-  if (tid == 0)
-  {
-    sh.eval = 0;
-    sh.pairs = 0ull;
-  }
+  if (tid == 0) sh.pairs = 0ull;
   __syncthreads();
-  evalBeads(sh, p, S, fwS, S.n_fw, molS, n * nb, nbd, skip, cl);
+  int eval = 0;
+  evalBeads(sh, p, S, fwS, S.n_fw, molS, n * nb, nbd, skip, cl, eval);
   if (tid < nbd)
   {
     out_fw[tid] = sh.efw[tid];
@@ -894,15 +929,12 @@ __global__ void __launch_bounds__(128) vacuumKernel(Params p, long long n, doubl
   const SysDev& S = p.sys[0];
   const int tid = threadIdx.x, nb = S.nb;
   for (int i = tid; i < kMaxTypes * kMaxTypes; i += blockDim.x) sh.tab[i] = p.ljf[i];
-  if (tid == 0)
-  {
-    sh.eval = 0;
-    sh.pairs = 0ull;
-  }
+  if (tid == 0) sh.pairs = 0ull;
+  int eval = 0;
   __syncthreads();
   for (long long c = blockIdx.x; c < n; c += gridDim.x)
   {
-    growChain(sh, p, S, 0, c, false, -1, nullptr, 0, nullptr, 0, cl);
+    growChain(sh, p, S, 0, c, false, -1, nullptr, 0, nullptr, 0, cl, eval);
     if (tid == 0)
     {
       w[c] = sh.fail ? 0.0 : sh.W;
@@ -945,6 +977,8 @@ struct rg_alkane
   cudaEvent_t fork = nullptr, join = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_moves = 0;
+  int graph_kernels = 0;
+  int64_t launches = 0;  // Monte Carlo kernel launches enqueued (graph kernel nodes included)
   int max_smem = 0;
 };
 
@@ -1005,7 +1039,10 @@ bool planFits(const rg_alkane* a, const rg_alkane_plan& pl)
     classCaps(a, c[0], c[1], c[2], &f, &m);
     const size_t smem = sharedBytes(f, m);
     if (smem > static_cast<size_t>(a->max_smem)) return false;
-    if (!(pl.threads == 256 ? clusterFits<256>(c[2], smem) : clusterFits<128>(c[2], smem))) return false;
+    const bool fits = pl.threads == 512   ? clusterFits<512>(c[2], smem)
+                      : pl.threads == 256 ? clusterFits<256>(c[2], smem)
+                                          : clusterFits<128>(c[2], smem);
+    if (!fits) return false;
   }
   return true;
 }
@@ -1032,14 +1069,17 @@ cudaError_t launchClass(rg_alkane* a, cudaStream_t stream, int b, int e, int C, 
   return cudaLaunchKernelEx(&cfg, alkaneKernel<T>, a->p, static_cast<const int*>(a->d_order + b), fw_cap, moves);
 }
 
-cudaError_t launchPlan(rg_alkane* a, const rg_alkane_plan& pl, int moves)
+cudaError_t launchPlan(rg_alkane* a, const rg_alkane_plan& pl, int moves, bool count = true)
 {
   const int split = std::min(std::max(pl.split, 0), a->n_systems);
+  if (count) a->launches += (split > 0 ? 1 : 0) + (split < a->n_systems ? 1 : 0);
   cudaStream_t main = a->ctx->stream;
   cudaError_t err = cudaEventRecord(a->fork, main);
   if (err == cudaSuccess) err = cudaStreamWaitEvent(a->side, a->fork, 0);
   auto go = [&](cudaStream_t st, int b, int e, int C) {
-    return pl.threads == 256 ? launchClass<256>(a, st, b, e, C, moves) : launchClass<128>(a, st, b, e, C, moves);
+    return pl.threads == 512   ? launchClass<512>(a, st, b, e, C, moves)
+           : pl.threads == 256 ? launchClass<256>(a, st, b, e, C, moves)
+                               : launchClass<128>(a, st, b, e, C, moves);
   };
   if (err == cudaSuccess) err = go(main, 0, split, pl.cluster_big);
   if (err == cudaSuccess) err = go(a->side, split, a->n_systems, pl.cluster_small);
@@ -1058,7 +1098,7 @@ rg_status rebuildGraph(rg_alkane* a)
   }
   cudaGraph_t g = nullptr;
   RG_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-  const cudaError_t le = launchPlan(a, a->plan, a->plan.moves_per_launch);
+  const cudaError_t le = launchPlan(a, a->plan, a->plan.moves_per_launch, false);
   const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
   if (le != cudaSuccess) return rg::cudaFail(ctx, le, "alkane graph capture");
   if (ce != cudaSuccess) return rg::cudaFail(ctx, ce, "cudaStreamEndCapture");
@@ -1066,6 +1106,8 @@ rg_status rebuildGraph(rg_alkane* a)
   cudaGraphDestroy(g);
   if (ie != cudaSuccess) return rg::cudaFail(ctx, ie, "cudaGraphInstantiate");
   a->graph_moves = a->plan.moves_per_launch;
+  const int split = std::min(std::max(a->plan.split, 0), a->n_systems);
+  a->graph_kernels = (split > 0 ? 1 : 0) + (split < a->n_systems ? 1 : 0);
   return RG_OK;
 }
 
@@ -1264,6 +1306,8 @@ extern "C" rg_status rg_alkane_create(rg_ctx* ctx, const rg_forcefield* ff, cons
     err = cudaFuncSetAttribute(alkaneKernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, a->max_smem);
   if (err == cudaSuccess)
     err = cudaFuncSetAttribute(alkaneKernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, a->max_smem);
+  if (err == cudaSuccess)
+    err = cudaFuncSetAttribute(alkaneKernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, a->max_smem);
   if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&a->side, cudaStreamNonBlocking);
   if (err == cudaSuccess) err = cudaEventCreateWithFlags(&a->fork, cudaEventDisableTiming);
   if (err == cudaSuccess) err = cudaEventCreateWithFlags(&a->join, cudaEventDisableTiming);
@@ -1317,9 +1361,10 @@ extern "C" rg_status rg_alkane_set_plan(rg_alkane* a, const rg_alkane_plan* plan
   rg_ctx* ctx = a->ctx;
   const int okC[3] = {1, 2, 4};
   auto validC = [&](int c) { return std::find(okC, okC + 3, c) != okC + 3; };
-  if (!validC(plan->cluster_big) || !validC(plan->cluster_small) || (plan->threads != 128 && plan->threads != 256) ||
+  if (!validC(plan->cluster_big) || !validC(plan->cluster_small) ||
+      (plan->threads != 128 && plan->threads != 256 && plan->threads != 512) ||
       plan->moves_per_launch < 1 || plan->split < 0 || plan->split > a->n_systems)
-    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_alkane_set_plan: clusters 1/2/4, threads 128/256");
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_alkane_set_plan: clusters 1/2/4, threads 128/256/512");
   if (!planFits(a, *plan)) return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_alkane_set_plan: exceeds shared memory");
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
   a->plan = *plan;
@@ -1345,6 +1390,7 @@ extern "C" rg_status rg_alkane_run(rg_alkane* a, int64_t moves, int record)
   while (left >= a->graph_moves)
   {
     RG_CUDA(ctx, cudaGraphLaunch(a->graph, ctx->stream));
+    a->launches += a->graph_kernels;
     left -= a->graph_moves;
   }
   // (the control block is copied from pageable memory: staged before cudaMemcpyAsync returns)
@@ -1390,7 +1436,7 @@ extern "C" rg_status rg_alkane_autotune(rg_alkane* a, int moves_per_candidate, r
   std::vector<rg_alkane_plan> cands;
   const int quarter = std::max(1, n / 4), half = std::max(1, n / 2);
   const int combos[][3] = {{1, 1, 0}, {2, 2, 0}, {4, 4, 0}, {2, 1, 0}, {2, 1, 1}, {4, 1, 0}, {4, 2, 0}, {4, 2, 1}};
-  for (int t : {128, 256})
+  for (int t : {128, 256, 512})
     for (auto& cb : combos)
     {
       rg_alkane_plan pl{cb[0], cb[1], t, cb[0] == cb[1] ? n : (cb[2] ? half : quarter), a->plan.moves_per_launch, 0,
@@ -1602,6 +1648,13 @@ extern "C" rg_status rg_alkane_grow_vacuum(rg_ctx* ctx, const rg_forcefield* ff,
   for (double v : hw) sum += v;
   if (w) std::memcpy(w, hw.data(), sizeof(double) * n);
   if (w_mean) *w_mean = sum / static_cast<double>(n);
+  return RG_OK;
+}
+
+extern "C" rg_status rg_alkane_launch_count(rg_alkane* a, int64_t* launches)
+{
+  if (!a || !launches) return RG_ERR_INVALID_ARGUMENT;
+  *launches = a->launches;
   return RG_OK;
 }
 

@@ -158,6 +158,7 @@ def lib():
         L.rg_alkane_get_positions.argtypes = [vp, i32, vp, i32, P(i32)]
         L.rg_alkane_set_positions.argtypes = [vp, i32, vp, i32, d]
         L.rg_alkane_pair_count.argtypes = [vp, P(ctypes.c_uint64)]
+        L.rg_alkane_launch_count.argtypes = [vp, P(ctypes.c_int64)]
         L.rg_alkane_bead_energies.argtypes = [vp, i32, vp, vp, i32, i32, vp, vp, vp]
         L.rg_alkane_grow_vacuum.argtypes = [vp, P(RgForceField), P(RgAlkaneChain), d, i64, ctypes.c_uint64, P(d), vp,
                                             vp, vp]
@@ -620,6 +621,11 @@ class Alkane:
 
     def run(self, moves: int, record: bool = True):
         check(self.ctx.handle, lib().rg_alkane_run(self.handle, moves, 1 if record else 0), "rg_alkane_run")
+
+    def launch_count(self) -> int:
+        v = ctypes.c_int64()
+        check(self.ctx.handle, lib().rg_alkane_launch_count(self.handle, ctypes.byref(v)), "rg_alkane_launch_count")
+        return int(v.value)
 
     def pair_count(self) -> int:
         v = ctypes.c_uint64()

@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--no-gcmc", action="store_true", help="skip the GCMC steps/s section")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-uniform proposal section")
     ap.add_argument("--no-alkane", action="store_true", help="skip the batched flexible-chain CBMC section")
+    ap.add_argument("--no-mixture", action="store_true", help="skip the large two-component system section")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the cpu_baseline sample")
     return ap.parse_args()
 
@@ -282,6 +283,130 @@ def run_alkane(args, ctx, peak_fp32, world, rank, dist, torch):
                                          f"{t_cpu:.1f} s (FP64 oracle restating the flexible CBMC, one system per "
                                          f"thread)"}
     a.close()
+    return out
+
+
+MIXTURE_EQUIL = 2000
+MIXTURE_MOVES = 20000
+
+
+def run_mixture(args, ctx, world, rank, dist, torch):
+    """The large mixture (configuration 5): 2,000 CO2 + 2,000 N2 in the 18,432-atom framework, Ewald kmax 12
+    (3,796 k-vectors), translation : rotation : CBMC swap : identity change = 1 : 1 : 1 : 1 with the learned first-bead
+    proposal of each component, one system advanced by all SMs. Metric: move attempts per second."""
+    from raspa3_b200 import native
+    from raspa3_b200.gcmc import beta_of, fugacity_of
+    from raspa3_b200.mixture import config5, total_energy
+
+    d = config5(ctx, torch)
+    ff, comps = d["ff"], d["components"]
+    beta = beta_of(300.0)
+    e0 = total_energy(d["system"], d["ewald"], ff, comps, d["xyz"], d["comp"])
+    sk0 = d["ewald"].structure_factors(0)
+    # learned first-bead proposals (C of CO2, N of N2), trained on the unit-cell grids
+    t0 = time.perf_counter()
+    props, mlps = [], []
+    for c, comp in enumerate(comps):
+        sb = comp.starting_bead
+        n = 1 << 20
+        ds = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+        dt = torch.empty(n, dtype=torch.float32, device="cuda")
+        native.sample_targets(d["system"], int(comp.types(ff)[sb]), float(comp.charges(ff)[sb]), beta, -15.0,
+                              d["unit_cell"], n, 11 + c, ds.data_ptr(), dt.data_ptr())
+        m = native.Mlp(ctx, seed=1 + c)
+        m.train(ds.data_ptr(), dt.data_ptr(), n, steps=1500, batch=4096, lr=2e-3)
+        props.append(native.Proposal(m, cells_per_axis=48, eps_uniform=0.05))
+        mlps.append(m)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    mx = native.Mixture(d["system"], d["ewald"], comps, beta, [fugacity_of(1e5), fugacity_of(1e5)], d["xyz"],
+                        d["comp"], max_molecules=6000, seed=3 + rank)
+    mx.set_state(e0, sk0)
+    for c, pr in enumerate(props):
+        mx.set_proposal(c, pr, d["unit_cell"])
+    mx.run(MIXTURE_EQUIL, record=False)
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0_, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0_.record(stream)
+    mx.run(MIXTURE_MOVES, record=True)
+    e1_.record(stream)
+    torch.cuda.synchronize()
+    secs = e0_.elapsed_time(e1_) / 1e3
+    if world > 1:
+        t = torch.tensor([secs], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        secs = float(t.item())
+    r = mx.results()
+    # e2e: the run call plus the read-back of the statistics
+    t1 = time.perf_counter()
+    mx.run(MIXTURE_MOVES // 4, record=True)
+    mx.results()
+    e2e_secs = time.perf_counter() - t1
+    xyz, comp = mx.positions()
+    e_check = total_energy(d["system"], d["ewald"], ff, comps, xyz, comp)
+    info = mx.info()
+    nk = info["n_kvectors"]
+    # structure-factor traffic of one move: every CTA reads its S(k) range once per phase and, on acceptance, reads and
+    # writes it again (16 bytes each per k-vector); S(k) and temp(k) (8 B) stay in L2
+    phases = 1.0 + r["attempted"][2] / max(1, sum(r["attempted"]))  # a second phase for insertions
+    acc_frac = sum(r["accepted"]) / max(1, sum(r["attempted"]))
+    sk_bytes = nk * (phases * (16 + 8) + acc_frac * 32)
+    moves_per_s = world * MIXTURE_MOVES / secs
+    hbm = None
+    try:
+        hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs")
+    except (OSError, ValueError):
+        hbm = None
+    out = {"metric": "mixture GCMC steps/s", "value": moves_per_s, "unit": "MC move attempts/s",
+           "moves": MIXTURE_MOVES, "ms": secs * 1e3, "blocks": info["blocks"], "n_kvectors": nk,
+           "workload": "2,000 CO2 + 2,000 N2 (12,000 sites) in the 4x4x4 replica (18,432 atoms) of the synthetic "
+                       "charged cell at 1.5x the configuration-1 lengths, Ewald alpha 0.265 kmax 12, 300 K, 1e5 Pa "
+                       "each, translation : rotation : CBMC swap : identity change 1:1:1:1, 10 + 10 trials, learned "
+                       "first-bead proposal per component",
+           "n_molecules": r["n_molecules"][:2], "attempted": r["attempted"], "accepted": r["accepted"],
+           "proposal_training_s": t_train, "status": r["status"],
+           "drift_relative": abs(r["energy"] - e_check) / max(1.0, abs(e_check)),
+           "structure_factor_update": {"bytes_per_move": sk_bytes, "achieved_gbs": sk_bytes * moves_per_s / 1e9,
+                                       "hbm_peak_gbs": hbm,
+                                       "frac_of_hbm": (sk_bytes * moves_per_s / 1e9 / hbm) if hbm else None,
+                                       "note": "the per-move S(k) traffic is L2-resident; the move is latency-bound "
+                                               "by its grid barriers, not by memory"},
+           "e2e": {"value": world * (MIXTURE_MOVES // 4) / e2e_secs, "unit": "MC move attempts/s",
+                   "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 176}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        from concurrent.futures import ThreadPoolExecutor
+
+        host_grids = [None] * (ff.n_types + 1)
+        for name, buf in zip(("C_co2", "O_co2", "N_n2", None), d["grids"]):
+            host_grids[ff.index(name) if name else ff.n_types] = buf.cpu().numpy()
+        s_fw = d["ewald"].structure_factors(2)
+        threads = os.cpu_count() or 1
+
+        def one(seed, steps):
+            rr, _, _, s_ = oracle.mixture_run(ff, d["cell"], comps, beta, [fugacity_of(1e5), fugacity_of(1e5)],
+                                             d["xyz"], d["comp"], steps, seed=seed, grids=host_grids,
+                                             grid_dims=d["dims"], grid_cell=d["unit_cell"], s_framework=s_fw,
+                                             max_molecules=6000)
+            return s_
+
+        t_probe = one(1, 20)
+        steps = int(max(20, 20 * args.cpu_seconds / max(t_probe, 1e-3)))
+        with ThreadPoolExecutor(threads) as pool:
+            secs_cpu = list(pool.map(lambda s: one(s + 2, steps), range(threads)))
+        out["cpu_baseline"] = {"value": threads * steps / max(secs_cpu), "unit": "MC move attempts/s",
+                               "cores": threads, "kind": "port",
+                               "sample": f"{threads} independent copies x {steps} moves from the same starting "
+                                         f"configuration (FP64 oracle mixture GCMC, one copy per thread, uniform "
+                                         f"first beads) in {max(secs_cpu):.1f} s"}
+    mx.close()
+    for pr in props:
+        pr.close()
+    for m in mlps:
+        m.close()
     return out
 
 
@@ -588,6 +713,9 @@ def run_ours(args):
     # ---- batched CBMC of flexible chains in 64 uneven systems (configuration 3) ----
     if not args.no_alkane:
         line["batched_cbmc"] = run_alkane(args, ctx, peak_fp32, world, rank, dist, torch)
+    # ---- one large two-component system on the whole GPU (configuration 5) ----
+    if not args.no_mixture:
+        line["mixture"] = run_mixture(args, ctx, world, rank, dist, torch)
     # ---- learned vs uniform first-bead proposal at equal loading error (configuration 4) ----
     if not args.no_learned:
         del flush

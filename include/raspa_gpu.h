@@ -405,6 +405,60 @@ rg_status rg_alkane_launch_count(rg_alkane* batch, int64_t* launches);
 rg_status rg_alkane_grow_vacuum(rg_ctx* ctx, const rg_forcefield* ff, const rg_alkane_chain* chain, double beta,
                                 int64_t n, uint64_t seed, double* w_mean, double* w, double* theta, double* cos_phi);
 
+/* ---- one large system of several rigid components on the whole GPU ---- */
+/* GCMC of a mixture in one system: translation, rotation, CBMC insertion / deletion and identity change
+ * (mc_moves/component/translation.cpp, rotation.cpp, insertion_cbmc.cpp, deletion_cbmc.cpp, identity_change.cpp). Every
+ * move runs on all SMs: molecule sites and k-vectors are split between the CTAs of one cooperative persistent kernel,
+ * which meet at a grid barrier once per phase (one phase per move, two for an insertion). Framework energies come from
+ * the grids of `system`, molecule-molecule pairs are FP32 from exact fixed-point displacements with FP64 sums, the
+ * Fourier part uses `ewald`'s k-vectors (FP64). */
+typedef struct rg_mixture rg_mixture;
+
+typedef struct rg_mixture_params
+{
+  double beta;
+  double fugacity[4];     /* per component, internal units */
+  double w_ig[4];         /* ideal-gas Rosenbluth weight per component (0 = 1) */
+  double cutoff_molecule_vdw, cutoff_coulomb;
+  double max_translation, max_rotation;
+  double p_translation, p_rotation, p_swap, p_identity; /* a component is chosen uniformly, then the move */
+  int32_t n_first_bead_trials, n_orientation_trials;    /* 1..12 */
+  int32_t max_molecules;
+  int32_t n_blocks;       /* CTAs of the cooperative launch (0: one per SM) */
+  uint64_t seed;
+} rg_mixture_params;
+
+typedef struct rg_mixture_result
+{
+  int64_t n_molecules[4];
+  double energy;                     /* running total energy */
+  int64_t attempted[5], accepted[5]; /* translation, rotation, insertion, deletion, identity change */
+  double sum_n[4];                   /* sum over recorded moves of each component's count */
+  double sum_energy;
+  int64_t samples;
+  int32_t status;                    /* RG_OK, or RG_ERR_TIMEOUT if a grid barrier gave up */
+  int32_t reserved;
+} rg_mixture_result;
+
+/* components: all with the same atom count (2-4); the starting configuration is n_molecules molecules at xyz
+ * (n_atoms * 3 doubles each) of components comp_of_molecule. Set the running energy and the structure factors of
+ * that configuration with rg_mixture_set_state before running. */
+rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const rg_gcmc_component* components, int n_components,
+                            const rg_mixture_params* params, const double* xyz, const int32_t* comp_of_molecule,
+                            int n_molecules, rg_mixture** out);
+rg_status rg_mixture_destroy(rg_mixture* mixture);
+/* energy: total energy of the configuration; sk: its structure factors (framework included), 2 doubles per k-vector
+ * in the rg_ewald order (NULL: leave them). */
+rg_status rg_mixture_set_state(rg_mixture* mixture, double energy, const double* sk, int64_t n_doubles);
+rg_status rg_mixture_run(rg_mixture* mixture, int64_t moves, int record);
+rg_status rg_mixture_results(rg_mixture* mixture, rg_mixture_result* out);
+rg_status rg_mixture_get_positions(rg_mixture* mixture, double* xyz, int32_t* comp, int capacity_molecules,
+                                   int* n_molecules);
+rg_status rg_mixture_get_structure_factors(rg_mixture* mixture, double* host, int64_t n_doubles);
+/* Learned first-bead proposal of one component (NULL: uniform). */
+rg_status rg_mixture_set_proposal(rg_mixture* mixture, int component, rg_proposal* proposal, const rg_box* unit_cell);
+rg_status rg_mixture_info(rg_mixture* mixture, int* blocks, int64_t* nk);
+
 /* ---- measurement ---- */
 /* FP32 (precision = RG_PRECISION_FP32C) or FP64 FMA throughput of this device in TFLOP/s, from independent FMA chains
  * on every SM: the SIMT-pipe denominator for the pair kernels' rooflines. No counterpart in the reference. */

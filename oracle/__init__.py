@@ -529,3 +529,98 @@ def alkane_bead_energies(ff, system, xyz, beads, types, skip=-1):
                                   _ptr(mm), _ptr(ov))
     del keep
     return fw, mm, ov
+
+
+# ---- mixture GCMC with identity change (oracle/mixture.cpp) ----
+class OMixComponent(ctypes.Structure):
+    _fields_ = [("n_atoms", ctypes.c_int32), ("starting_bead", ctypes.c_int32), ("offsets", ctypes.c_double * 24),
+                ("masses", ctypes.c_double * 8), ("types", ctypes.c_int32 * 8), ("charges", ctypes.c_double * 8),
+                ("fugacity", ctypes.c_double), ("w_ig", ctypes.c_double)]
+
+
+class OMixSetup(ctypes.Structure):
+    _fields_ = [("ff", ctypes.POINTER(OFF)), ("box", OBox), ("grid_cell", OBox), ("gnx", ctypes.c_int32),
+                ("gny", ctypes.c_int32), ("gnz", ctypes.c_int32), ("grids", ctypes.c_void_p),
+                ("s_framework", ctypes.c_void_p), ("n_components", ctypes.c_int32), ("comps", OMixComponent * 4),
+                ("beta", ctypes.c_double), ("max_translation", ctypes.c_double), ("max_rotation", ctypes.c_double),
+                ("p_translation", ctypes.c_double), ("p_rotation", ctypes.c_double), ("p_swap", ctypes.c_double),
+                ("p_identity", ctypes.c_double), ("n_first_bead_trials", ctypes.c_int32),
+                ("n_orientation_trials", ctypes.c_int32), ("max_molecules", ctypes.c_int32),
+                ("use_ewald", ctypes.c_int32)]
+
+
+class OMixResult(ctypes.Structure):
+    _fields_ = [("n_molecules", ctypes.c_int64 * 4), ("running_energy", ctypes.c_double),
+                ("recomputed_energy", ctypes.c_double), ("sum_n", ctypes.c_double * 4), ("samples", ctypes.c_int64),
+                ("attempted", ctypes.c_int64 * 5), ("accepted", ctypes.c_int64 * 5)]
+
+    def as_dict(self):
+        return {"n_molecules": list(self.n_molecules), "running_energy": self.running_energy,
+                "recomputed_energy": self.recomputed_energy, "sum_n": list(self.sum_n), "samples": self.samples,
+                "attempted": list(self.attempted), "accepted": list(self.accepted)}
+
+
+def mixture_run(ff, cell, components, beta, fugacities, xyz, comp, steps, seed=1, grids=None, grid_dims=None,
+                grid_cell=None, s_framework=None, use_ewald=True, max_translation=1.0,
+                max_rotation=0.5235987755982988, probabilities=(1.0, 1.0, 1.0, 1.0), n_first=10, n_orient=10,
+                max_molecules=512, w_ig=None):
+    """One oracle mixture run from the molecules xyz[n, na, 3] of components comp[n]; returns (result dict, final xyz,
+    final comp, seconds)."""
+    L = lib()
+    if not hasattr(L, "_mixture_declared"):
+        L.oracle_mixture_run.argtypes = [ctypes.POINTER(OMixSetup), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.c_int64, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p]
+        L._mixture_declared = True
+    o = off(ff)
+    s = OMixSetup()
+    s.ff = ctypes.pointer(o)
+    s.box = obox(cell)
+    keep = [o]
+    if grids is not None:
+        arr = (ctypes.c_void_p * len(grids))()
+        gk = [None if g is None else np.ascontiguousarray(g, dtype=np.float64) for g in grids]
+        for i, g in enumerate(gk):
+            arr[i] = None if g is None else g.ctypes.data
+        keep += [arr, gk]
+        s.grids = ctypes.cast(arr, ctypes.c_void_p)
+        s.gnx, s.gny, s.gnz = grid_dims
+        s.grid_cell = obox(grid_cell)
+    if s_framework is not None:
+        sf = np.ascontiguousarray(s_framework, dtype=np.float64)
+        keep.append(sf)
+        s.s_framework = sf.ctypes.data
+    s.n_components = len(components)
+    for k, comp_k in enumerate(components):
+        c = s.comps[k]
+        c.n_atoms = comp_k.n_atoms
+        c.starting_bead = comp_k.starting_bead
+        types, charges = comp_k.types(ff), comp_k.charges(ff)
+        for i in range(comp_k.n_atoms):
+            for d in range(3):
+                c.offsets[3 * i + d] = float(comp_k.offsets[i][d])
+            c.masses[i] = float(comp_k.masses[i])
+            c.types[i] = int(types[i])
+            c.charges[i] = float(charges[i])
+        c.fugacity = fugacities[k]
+        c.w_ig = 1.0 if w_ig is None else w_ig[k]
+    s.beta = beta
+    s.max_translation, s.max_rotation = max_translation, max_rotation
+    s.p_translation, s.p_rotation, s.p_swap, s.p_identity = probabilities
+    s.n_first_bead_trials, s.n_orientation_trials = n_first, n_orient
+    s.max_molecules = max_molecules
+    s.use_ewald = 1 if use_ewald else 0
+    x = np.ascontiguousarray(xyz, dtype=np.float64)
+    cc = np.ascontiguousarray(comp, dtype=np.int32)
+    na = components[0].n_atoms
+    out = OMixResult()
+    xo = np.zeros(max_molecules * na * 3)
+    co = np.zeros(max_molecules, dtype=np.int32)
+    secs = ctypes.c_double()
+    L.oracle_mixture_run(ctypes.byref(s), _ptr(x) if len(cc) else None, _ptr(cc) if len(cc) else None, len(cc), steps,
+                         seed, ctypes.c_void_p(ctypes.addressof(out)), _ptr(xo), _ptr(co),
+                         ctypes.c_void_p(ctypes.addressof(secs)))
+    r = out.as_dict()
+    n = sum(r["n_molecules"])
+    del keep
+    return r, xo[: n * na * 3].reshape(n, na, 3), co[:n].copy(), secs.value

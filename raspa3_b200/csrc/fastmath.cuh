@@ -1,0 +1,41 @@
+// FP32 reciprocal, reciprocal square root and erfc for the FP32 pair kernels (own code: hardware approximations
+// refined by one Newton step, and erfc as exp(-x^2) times a fitted rational-in-t polynomial).
+#pragma once
+
+namespace rgd
+{
+// FP32 reciprocal: the hardware approximation refined by one Newton step (x (2 - a x)), ~0.5 ulp
+__device__ __forceinline__ float rcpRn(float a)
+{
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  const float e = fmaf(-a, r, 1.0f);
+  return fmaf(r, e, r);
+}
+// FP32 reciprocal square root, refined by one Newton step (r (3 - a r^2) / 2)
+__device__ __forceinline__ float rsqrtRn(float a)
+{
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  const float h = 0.5f * a * r;
+  return r * fmaf(-h, r, 1.5f);
+}
+// erfc(x) = exp(-x^2) R(x) for 0 <= x <= 4, with R(x) = exp(x^2) erfc(x) fitted (weighted least squares in Chebyshev
+// form, relative error 4e-8 in FP64, ~2 ulp in FP32) as a degree-9 polynomial in t = 1 / (1 + x/2); the caller passes
+// exp(-x^2), which the derivative factors need anyway.
+__device__ __forceinline__ float erfcFromExp(float x, float expmx2)
+{
+  const float t = rcpRn(fmaf(0.5f, x, 1.0f));
+  float r = -0.02496027760207653f;
+  r = fmaf(r, t, 0.09420006722211838f);
+  r = fmaf(r, t, -0.024484887719154358f);
+  r = fmaf(r, t, -0.36430737376213074f);
+  r = fmaf(r, t, 0.534475564956665f);
+  r = fmaf(r, t, -0.11705945432186127f);
+  r = fmaf(r, t, 0.3620023727416992f);
+  r = fmaf(r, t, 0.25453805923461914f);
+  r = fmaf(r, t, 0.2858136296272278f);
+  r = fmaf(r, t, -0.00021772264153696597f);
+  return expmx2 * r;
+}
+}  // namespace rgd

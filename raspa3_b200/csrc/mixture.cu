@@ -1,0 +1,1521 @@
+// Monte Carlo of one large system of several rigid components on the whole GPU (rg_mixture_*).
+//
+// A single system (tens of thousands of atoms, thousands of k-vectors) has too little work per move for one CTA and
+// too much for a CPU core, so every move runs on all SMs: a cooperative persistent kernel of one CTA per SM.
+//  * The molecule sites are split into contiguous slices, one per CTA; the k-vectors into ranges, one per CTA. Each
+//    CTA keeps its range of the structure factors S(k) and the structure-factor changes of the move's candidates in
+//    shared memory, and updates its range on acceptance: S(k) never crosses the GPU.
+//  * A phase evaluates a set of trial atoms (framework energy from the tricubic grids, molecule-molecule Lennard-Jones
+//    and real-space Ewald over the CTA's slice in FP32 from exact fixed-point displacements, accumulated in FP64) and
+//    a set of Ewald candidates (energy change over the CTA's k-range, FP64). Each CTA writes one row of partial sums;
+//    after a grid barrier every CTA adds the rows in CTA order, so every CTA holds identical totals, draws the same
+//    counter-based random numbers and takes the same decision: nothing else is exchanged, and every CTA applies the
+//    (identical) updates of positions and molecule lists itself. Every value such an update reads is read before the
+//    phase's barrier, when no CTA can have started writing it.
+//  * Moves with all trial positions known up front need one phase: translation, rotation, CBMC deletion (the retrace
+//    orientations sit on the old first bead) and identity change (the new first bead sits on the old one). A CBMC
+//    insertion needs two (first bead, then orientations).
+//  * The grid barrier is this file's own: a generation counter in global memory, spin-waits bounded by an iteration
+//    limit after which an error flag is raised and every CTA leaves; the host reports RG_ERR_TIMEOUT.
+// Reference moves (file:line in the RASPA3 tree): mc_moves/component/translation.cpp:30-200, rotation.cpp:30-190,
+// insertion_cbmc.cpp:34-207, deletion_cbmc.cpp:34-195, identity_change.cpp:33-290 with
+// cbmc/multiple_first_bead.cpp:20-76, 136-168; energies cbmc/interactions_framework_molecule.cpp,
+// cbmc/interactions_intermolecular.cpp, interactions/ewald.cpp:1043-1244 (Fourier difference) and :1164-1238 (self
+// and exclusion terms of inserted / deleted rigid molecules, constant per component).
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "energy.cuh"
+#include "fastmath.cuh"
+#include "rng.cuh"
+
+namespace
+{
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxComp = 4;
+constexpr int kMaxAtoms = 4;
+constexpr int kMaxTrials = 12;
+constexpr int kMaxItems = 96;          // trial atoms of one phase
+constexpr int kMaxCand = kMaxTrials;   // Ewald candidates of one phase
+constexpr int kMaxCandAtoms = 2 * kMaxAtoms;
+constexpr int kMaxKPerCta = 64;
+constexpr int kMaxTypes = 16;
+constexpr int kRow = kMaxItems + kMaxCand + 4;  // doubles per CTA row of partial sums (last 4: overlap bits)
+constexpr long long kSpinLimit = 1ll << 22;
+constexpr int kStats = 24;
+constexpr double kPi = 3.141592653589793238462643383279502884;
+constexpr float kFix = 2.3283064365386963e-10f;  // 2^-32
+
+struct Comp
+{
+  int n_atoms, starting_bead;
+  int types[kMaxAtoms];
+  double charges[kMaxAtoms], masses[kMaxAtoms], offsets[kMaxAtoms][3];
+  double fugacity, w_ig, self_excl;
+  const double* vdw_grid[kMaxAtoms];
+  // learned first-bead proposal (null: uniform)
+  const double* prop_cdf;
+  const double* prop_q;
+  int prop_G;
+  double prop_eps;
+};
+
+struct Params
+{
+  rgd::Box box;
+  rgd::Grid grid;  // shape and inverse cell of the grids; data per atom in Comp::vdw_grid
+  const double* ewald_grid;
+  double overlap;
+  float overlap_f;
+  int use_charge;
+  float hf[3][3];
+  float rc2_mm, rc2_c, alpha, coul;
+  int n_comp;
+  Comp comp[kMaxComp];
+  double beta, volume;
+  double max_translation, max_rotation;
+  double p_translation, p_rotation, p_swap, p_identity;
+  int k1, k2, capacity, na;
+  int nk;
+  const char4* kvec;
+  const double* temp;
+  double uc[3][3], uic[3][3];
+  int rep[3];
+  unsigned long long seed;
+  const float4* ljf;  // [kMaxTypes^2]: 4 eps, sigma^2, shift, lj flag
+  const float* qtype; // charge per type (the pseudo-atom charge)
+  // state
+  double4* pos;    // [capacity * na] Cartesian
+  int4* fx;        // [capacity * na] fixed point, .w = type | molecule << 8
+  int* comp_of;    // [capacity]
+  int* list;       // [kMaxComp][capacity]
+  int* slot;       // [capacity]
+  int* n_state;    // n, count[kMaxComp]
+  double* energy;
+  long long* move_base;
+  double* stats;   // attempted[5], accepted[5], sum_n[4], sum_energy, samples
+  double2* sk;     // [nk]
+  double* part;    // [gridDim][kRow]
+  unsigned* bar;   // count, generation, error
+  int record;
+};
+
+enum : uint32_t
+{
+  kKindMove = 1,
+  kKindFirst = 2,
+  kKindOrient = 3,
+  kKindNewOrient = 4,
+  kKindOldOrient = 5
+};
+__host__ __device__ constexpr uint32_t slot(uint32_t kind, uint32_t index, uint32_t sub)
+{
+  return (kind << 28) | (index << 8) | sub;
+}
+
+struct Shared
+{
+  float4 tab[kMaxTypes * kMaxTypes];
+  float qt[kMaxTypes];
+  double3 ta[kMaxItems];  // trial atoms: Cartesian position
+  int4 tf[kMaxItems];     // fixed point, .w = type
+  int nta;
+  double3 cpos[kMaxCand][kMaxCandAtoms];  // Ewald candidates: atoms and signed charges
+  double cq[kMaxCand][kMaxCandAtoms];
+  int cn[kMaxCand];
+  int ncand;
+  double2 dk[kMaxCand][kMaxKPerCta];  // structure-factor change of each candidate over this CTA's k-range
+  double red[kThreads];
+  unsigned ovl_bits[4];
+  double tot[kMaxItems + kMaxCand];  // totals over the grid
+  unsigned ovl[4];
+  // move state
+  int kind, c, c2, m, axis, accept, fail, n, count[kMaxComp], gen;
+  int phases;  // phases run by this CTA: its parity selects the buffer of partial-sum rows
+  // molecule-list state an accepted deletion / identity change rewrites, read before the phase's barrier (no CTA
+  // writes it before every CTA has passed that barrier, so every CTA reads the same values and writes the same update)
+  int preSlot, preLastC, preCl, preSl;
+  double3 preLast[kMaxAtoms];
+  double u[8];
+  double energy, dU;
+  double3 mol[kMaxAtoms];   // new molecule (selected)
+  double W, W2;
+  int selFirst, selOrient;
+  double3 first;
+  double logq[kMaxTrials];
+  double stats[kStats];
+};
+
+__device__ __forceinline__ double2 urand(const Params& p, long long move, uint32_t sl)
+{
+  return rgd::uniform2(p.seed, 0, move, sl);
+}
+
+__device__ __forceinline__ uint32_t fixOf(double s)
+{
+  s -= floor(s);
+  return static_cast<uint32_t>(static_cast<unsigned long long>(s * 4294967296.0));
+}
+__device__ __forceinline__ int4 toFixed(const Params& p, double3 r, int w)
+{
+  const rgd::Box& b = p.box;
+  const double s0 = b.ic[0][0] * r.x + b.ic[1][0] * r.y + b.ic[2][0] * r.z;
+  const double s1 = b.ic[0][1] * r.x + b.ic[1][1] * r.y + b.ic[2][1] * r.z;
+  const double s2 = b.ic[0][2] * r.x + b.ic[1][2] * r.y + b.ic[2][2] * r.z;
+  return make_int4(static_cast<int>(fixOf(s0)), static_cast<int>(fixOf(s1)), static_cast<int>(fixOf(s2)), w);
+}
+
+// uniform rotation from three uniforms (Shoemake's unit quaternion)
+__device__ void rotationFromUniforms(double u1, double u2, double u3, double R[3][3])
+{
+  double s2, c2, s3, c3;
+  sincospi(2.0 * u2, &s2, &c2);
+  sincospi(2.0 * u3, &s3, &c3);
+  const double a = sqrt(1.0 - u1), b = sqrt(u1);
+  const double x = a * s2, y = a * c2, z = b * s3, w = b * c3;
+  R[0][0] = 1 - 2 * (y * y + z * z);
+  R[0][1] = 2 * (x * y - z * w);
+  R[0][2] = 2 * (x * z + y * w);
+  R[1][0] = 2 * (x * y + z * w);
+  R[1][1] = 1 - 2 * (x * x + z * z);
+  R[1][2] = 2 * (y * z - x * w);
+  R[2][0] = 2 * (x * z - y * w);
+  R[2][1] = 2 * (y * z + x * w);
+  R[2][2] = 1 - 2 * (x * x + y * y);
+}
+
+// Grid barrier over all CTAs of the cooperative launch. Spin-waits are bounded: on timeout the error flag is raised
+// and false returned; every CTA then leaves the kernel. Returns false as well once any CTA has raised the flag.
+__device__ bool gridBarrier(const Params& p, Shared& sh)
+{
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    const unsigned g = static_cast<unsigned>(sh.gen);
+    __threadfence();
+    const unsigned arrived = atomicAdd(&p.bar[0], 1u);
+    if (arrived == gridDim.x - 1)
+    {
+      atomicExch(&p.bar[0], 0u);
+      __threadfence();
+      atomicExch(&p.bar[1], g + 1u);
+    }
+    else
+    {
+      long long spins = 0;
+      while (atomicAdd(&p.bar[1], 0u) == g)
+      {
+        if (++spins > kSpinLimit || atomicAdd(&p.bar[2], 0u) != 0u)
+        {
+          atomicExch(&p.bar[2], 1u);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    sh.gen = static_cast<int>(g + 1u);
+    sh.fail = atomicAdd(&p.bar[2], 0u) != 0u;
+  }
+  __syncthreads();
+  return !sh.fail;
+}
+
+// framework energy of one trial atom from the grids (FP64); overlap flag if the VDW part exceeds the criterion
+__device__ double gridEnergy(const Params& p, int type, double q, double3 r, const double* vdw, bool* ovl)
+{
+  double e = 0.0;
+  if (vdw)
+  {
+    rgd::Grid g = p.grid;
+    g.data = vdw;
+    const double v = rgd::interpolate(g, r.x, r.y, r.z);
+    if (v > p.overlap) *ovl = true;
+    e += v;
+  }
+  if (p.use_charge && p.ewald_grid && q != 0.0)
+  {
+    rgd::Grid g = p.grid;
+    g.data = p.ewald_grid;
+    e += q * rgd::interpolate(g, r.x, r.y, r.z);
+  }
+  return e;
+}
+
+// One phase: energies of sh.nta trial atoms (framework + molecules other than `skip`) and the Ewald energy change of
+// sh.ncand candidates, each summed over the whole grid into sh.tot[0, nta) and sh.tot[nta, nta + ncand); overlap bits
+// per trial atom in sh.ovl. vdwOf/qOf: the framework grid and charge of each trial atom (set by the caller in
+// sh.tf[].w = type; the grids come from the type). Returns false if a barrier failed.
+__device__ bool phase(const Params& p, Shared& sh, int skip, const double* const* atomGrid)
+{
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int G = gridDim.x, cta = blockIdx.x;
+  const int nta = sh.nta, ncand = sh.ncand;
+  if (tid < 4) sh.ovl_bits[tid] = 0u;
+  __syncthreads();
+  // 1. molecule-molecule pairs over this CTA's slice of sites
+  const int ns = sh.n * p.na;
+  const int chunk = (ns + G - 1) / G, s0 = cta * chunk, s1 = min(ns, s0 + chunk);
+  double acc = 0.0;
+  bool ov = false;
+  const int streams = nta > 0 ? kThreads / nta : 0;
+  const int b = nta > 0 ? tid % nta : 0, st = nta > 0 ? tid / nta : 0;
+  if (nta > 0 && st < streams)
+  {
+    const int4 B = sh.tf[b];
+    const int bt = B.w & 0xff;
+    const float qb = sh.qt[bt];
+    for (int i = s0 + st; i < s1; i += streams)
+    {
+      const int4 P = __ldcg(p.fx + i);
+      if ((P.w >> 8) == skip) continue;
+      const int pt = P.w & 0xff;
+      const float f0 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.x) - static_cast<uint32_t>(P.x))) * kFix;
+      const float f1 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.y) - static_cast<uint32_t>(P.y))) * kFix;
+      const float f2 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.z) - static_cast<uint32_t>(P.z))) * kFix;
+      const float rx = fmaf(p.hf[0][0], f0, fmaf(p.hf[1][0], f1, p.hf[2][0] * f2));
+      const float ry = fmaf(p.hf[0][1], f0, fmaf(p.hf[1][1], f1, p.hf[2][1] * f2));
+      const float rz = fmaf(p.hf[0][2], f0, fmaf(p.hf[1][2], f1, p.hf[2][2] * f2));
+      const float rr = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+      if (rr < p.rc2_mm)
+      {
+        const float4 q = sh.tab[bt * kMaxTypes + pt];
+        if (q.w != 0.0f)
+        {
+          const float t = q.y * rgd::rcpRn(rr);
+          const float t3 = t * t * t;
+          const float e = q.x * (t3 * (t3 - 1.0f)) - q.z;
+          if (e > p.overlap_f) ov = true;
+          acc += static_cast<double>(e);
+        }
+      }
+      if (p.use_charge && rr < p.rc2_c)
+      {
+        const float qq = qb * sh.qt[pt];
+        if (qq != 0.0f)
+        {
+          // potentialCoulomb<0>, Ewald branch at full scaling: C qA qB erfc(alpha r) / r
+          const float invr = rgd::rsqrtRn(rr);
+          const float r = rr * invr;
+          const float ex = expf(-p.alpha * p.alpha * rr);
+          acc += static_cast<double>(p.coul * qq * rgd::erfcFromExp(p.alpha * r, ex) * invr);
+        }
+      }
+    }
+  }
+  // framework part of trial atom b, by the CTA b mod G (thread b)
+  if (tid < nta && tid % G == cta)
+  {
+    const int bt = sh.tf[tid].w & 0xff;
+    acc += gridEnergy(p, bt, static_cast<double>(sh.qt[bt]), sh.ta[tid], atomGrid[tid], &ov);
+  }
+  sh.red[tid] = acc;
+  if (ov) atomicOr(&sh.ovl_bits[b >> 5], 1u << (b & 31));
+  __syncthreads();
+  // two buffers of rows, alternating by phase: a CTA writes the next phase's row only after every CTA has passed
+  // this phase's barrier and read this phase's rows, which lie in the other buffer
+  const int buf = sh.phases & 1;
+  double* rows = p.part + static_cast<long long>(buf) * G * kRow;
+  double* row = rows + static_cast<long long>(cta) * kRow;
+  if (tid < nta)
+  {
+    double s = 0.0;
+    for (int k = 0; k < streams; ++k) s += sh.red[tid + nta * k];
+    row[tid] = s;
+  }
+  if (tid < 4) reinterpret_cast<unsigned*>(row + kMaxItems + kMaxCand)[tid] = sh.ovl_bits[tid];
+  // 2. Ewald candidates over this CTA's k-range: one warp per candidate, lanes over the k-vectors
+  const int kchunk = (p.nk + G - 1) / G, k0 = cta * kchunk, k1 = min(p.nk, k0 + kchunk);
+  for (int c = warp; c < ncand; c += kWarps)
+  {
+    double e = 0.0;
+    for (int kk = lane; kk < k1 - k0; kk += 32)
+    {
+      const int k = k0 + kk;
+      const char4 kv = p.kvec[k];
+      double2 d = make_double2(0.0, 0.0);
+      for (int a = 0; a < sh.cn[c]; ++a)
+      {
+        const double3 r = sh.cpos[c][a];
+        const rgd::Box& bx = p.box;
+        const double sx = bx.ic[0][0] * r.x + bx.ic[1][0] * r.y + bx.ic[2][0] * r.z;
+        const double sy = bx.ic[0][1] * r.x + bx.ic[1][1] * r.y + bx.ic[2][1] * r.z;
+        const double sz = bx.ic[0][2] * r.x + bx.ic[1][2] * r.y + bx.ic[2][2] * r.z;
+        double sn, cs;
+        sincospi(2.0 * (kv.x * sx + kv.y * sy + kv.z * sz), &sn, &cs);
+        d.x += sh.cq[c][a] * cs;
+        d.y += sh.cq[c][a] * sn;
+      }
+      const double2 s = p.sk[k];
+      e += p.temp[k] * (2.0 * (s.x * d.x + s.y * d.y) + (d.x * d.x + d.y * d.y));
+      sh.dk[c][kk] = d;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if (lane == 0) row[kMaxItems + c] = e;
+  }
+  if (!gridBarrier(p, sh)) return false;
+  // 3. totals: one warp per item, rows added in CTA order (lane partials over a fixed CTA stride, then a fixed tree)
+  const int nitems = nta + ncand;
+  for (int it = warp; it < nitems; it += kWarps)
+  {
+    const int col = it < nta ? it : kMaxItems + (it - nta);
+    double s = 0.0;
+    for (int q = lane; q < G; q += 32) s += __ldcg(rows + static_cast<long long>(q) * kRow + col);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) sh.tot[it] = s;
+  }
+  if (tid < 4)
+  {
+    unsigned o = 0u;
+    for (int q = 0; q < G; ++q)
+      o |= __ldcg(reinterpret_cast<const unsigned*>(rows + static_cast<long long>(q) * kRow + kMaxItems + kMaxCand) + tid);
+    sh.ovl[tid] = o;
+  }
+  if (tid == 0) sh.phases += 1;
+  __syncthreads();
+  return true;
+}
+
+__device__ __forceinline__ bool ovlOf(const Shared& sh, int i) { return (sh.ovl[i >> 5] >> (i & 31)) & 1u; }
+
+// Proposal density (relative to uniform) of a position for component c
+__device__ double proposalDensity(const Params& p, const Comp& c, double3 r)
+{
+  const double v[3] = {r.x, r.y, r.z};
+  int ci[3];
+  for (int a = 0; a < 3; ++a)
+  {
+    const double s = rgd::fract1(p.uic[0][a] * v[0] + p.uic[1][a] * v[1] + p.uic[2][a] * v[2]);
+    ci[a] = min(c.prop_G - 1, static_cast<int>(s * c.prop_G));
+  }
+  return c.prop_q[ci[0] + c.prop_G * (ci[1] + c.prop_G * ci[2])];
+}
+
+// First-bead trial position t of component c: uniform in the box, or from the component's tabulated proposal
+__device__ double3 firstBeadPosition(const Params& p, const Comp& c, long long move, int t)
+{
+  const double2 a = urand(p, move, slot(kKindFirst, t, 0));
+  const double2 b = urand(p, move, slot(kKindFirst, t, 1));
+  const double2 u = urand(p, move, slot(kKindFirst, t, 2));
+  double sf[3];
+  const double(*cell)[3] = p.box.c;
+  if (!c.prop_cdf || u.x < c.prop_eps)
+  {
+    sf[0] = a.x;
+    sf[1] = a.y;
+    sf[2] = b.x;
+  }
+  else
+  {
+    const double2 v = urand(p, move, slot(kKindFirst, t, 3));
+    const int G = c.prop_G, ncell = G * G * G;
+    int lo = 0, hi = ncell - 1;
+    while (lo < hi)
+    {
+      const int mid = (lo + hi) >> 1;
+      if (c.prop_cdf[mid] < u.y)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    const int ci = lo % G, cj = (lo / G) % G, ck = lo / (G * G);
+    sf[0] = (ci + a.x) / G + static_cast<double>(min(p.rep[0] - 1, static_cast<int>(b.y * p.rep[0])));
+    sf[1] = (cj + a.y) / G + static_cast<double>(min(p.rep[1] - 1, static_cast<int>(v.x * p.rep[1])));
+    sf[2] = (ck + b.x) / G + static_cast<double>(min(p.rep[2] - 1, static_cast<int>(v.y * p.rep[2])));
+    cell = p.uc;
+  }
+  return make_double3(cell[0][0] * sf[0] + cell[1][0] * sf[1] + cell[2][0] * sf[2],
+                      cell[0][1] * sf[0] + cell[1][1] * sf[1] + cell[2][1] * sf[2],
+                      cell[0][2] * sf[0] + cell[1][2] * sf[1] + cell[2][2] * sf[2]);
+}
+
+// the atoms of component c with its starting bead at `first`, orientation from (kind, t)
+__device__ void orientedMolecule(const Params& p, const Comp& c, double3 first, long long move, uint32_t kind, int t,
+                                 double3* out)
+{
+  const double2 a = urand(p, move, slot(kind, t, 0));
+  const double2 b = urand(p, move, slot(kind, t, 1));
+  double R[3][3];
+  rotationFromUniforms(a.x, a.y, b.x, R);
+  const double* o0 = c.offsets[c.starting_bead];
+  const double rc[3] = {R[0][0] * o0[0] + R[0][1] * o0[1] + R[0][2] * o0[2],
+                        R[1][0] * o0[0] + R[1][1] * o0[1] + R[1][2] * o0[2],
+                        R[2][0] * o0[0] + R[2][1] * o0[1] + R[2][2] * o0[2]};
+  for (int i = 0; i < c.n_atoms; ++i)
+  {
+    const double* o = c.offsets[i];
+    out[i] = make_double3(first.x - rc[0] + R[0][0] * o[0] + R[0][1] * o[1] + R[0][2] * o[2],
+                          first.y - rc[1] + R[1][0] * o[0] + R[1][1] * o[1] + R[1][2] * o[2],
+                          first.z - rc[2] + R[2][0] * o[0] + R[2][1] * o[1] + R[2][2] * o[2]);
+  }
+}
+
+// Boltzmann selection among the trials with ok bit set (CBMC::selectTrialPosition, cbmc/util.cpp:14-47);
+// *W = sum exp(lw) / k; returns -1 if none. Thread-level (k <= 12).
+__device__ int selectTrial(const double* lw, unsigned ok, int k, double u, double* W)
+{
+  double largest = -1e300;
+  for (int t = 0; t < k; ++t)
+    if ((ok >> t) & 1u) largest = fmax(largest, lw[t]);
+  if (largest == -1e300)
+  {
+    *W = 0.0;
+    return -1;
+  }
+  double sum = 0.0, w = 0.0;
+  for (int t = 0; t < k; ++t)
+    if ((ok >> t) & 1u)
+    {
+      sum += exp(lw[t] - largest);
+      w += exp(lw[t]);
+    }
+  *W = w / static_cast<double>(k);
+  const double target = u * sum;
+  double cum = 0.0;
+  int last = -1;
+  for (int t = 0; t < k; ++t)
+  {
+    if (!((ok >> t) & 1u)) continue;
+    last = t;
+    cum += exp(lw[t] - largest);
+    if (cum >= target) return t;
+  }
+  return last;
+}
+
+__device__ __forceinline__ double3 loadPos(const Params& p, int site)
+{
+  const double2* q = reinterpret_cast<const double2*>(p.pos + site);
+  const double2 a = __ldcg(q), b = __ldcg(q + 1);
+  return make_double3(a.x, a.y, b.x);
+}
+
+// write the atoms of molecule m (every CTA writes the same values; each reads back only its own writes)
+__device__ void storeMolecule(const Params& p, int m, int cidx, const double3* x)
+{
+  const Comp& c = p.comp[cidx];
+  for (int i = 0; i < p.na; ++i)
+  {
+    p.pos[m * p.na + i] = make_double4(x[i].x, x[i].y, x[i].z, 0.0);
+    p.fx[m * p.na + i] = toFixed(p, x[i], c.types[i] | (m << 8));
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves)
+{
+  __shared__ Shared sh;
+  const int tid = threadIdx.x;
+  const int na = p.na;
+  for (int i = tid; i < kMaxTypes * kMaxTypes; i += kThreads) sh.tab[i] = p.ljf[i];
+  for (int i = tid; i < kMaxTypes; i += kThreads) sh.qt[i] = p.qtype[i];
+  if (tid == 0)
+  {
+    sh.n = p.n_state[0];
+    for (int c = 0; c < kMaxComp; ++c) sh.count[c] = p.n_state[1 + c];
+    sh.energy = *p.energy;
+    sh.gen = static_cast<int>(atomicAdd(&p.bar[1], 0u));
+    sh.fail = 0;
+    sh.phases = 0;
+    for (int k = 0; k < kStats; ++k) sh.stats[k] = p.stats[k];
+  }
+  // this CTA's k-range
+  const int G = gridDim.x;
+  const int kchunk = (p.nk + G - 1) / G, k0 = blockIdx.x * kchunk, k1 = min(p.nk, k0 + kchunk);
+  const long long move0 = *p.move_base;
+  __shared__ const double* atomGrid[kMaxItems];
+  __syncthreads();
+  for (int mv = 0; mv < moves; ++mv)
+  {
+    const long long move = move0 + mv;
+    if (tid == 0)
+    {
+      for (int q = 0; q < 4; ++q)
+      {
+        const double2 u = urand(p, move, slot(kKindMove, 0, q));
+        sh.u[2 * q] = u.x;
+        sh.u[2 * q + 1] = u.y;
+      }
+      sh.c = min(p.n_comp - 1, static_cast<int>(sh.u[0] * p.n_comp));
+      const double ptot = p.p_translation + p.p_rotation + p.p_swap + p.p_identity;
+      const double v = sh.u[1] * ptot;
+      sh.kind = v < p.p_translation ? 0
+                : v < p.p_translation + p.p_rotation ? 1
+                : v < p.p_translation + p.p_rotation + p.p_swap ? (sh.u[2] < 0.5 ? 2 : 3)
+                                                                 : 4;
+      sh.accept = 0;
+      sh.nta = 0;
+      sh.ncand = 0;
+    }
+    __syncthreads();
+    const int kind = sh.kind;
+    int c = sh.c;
+    bool ran = false;
+    if ((kind == 0 || kind == 1) && sh.count[c] > 0)
+    {
+      // translation (one Cartesian direction) or rotation (one Cartesian axis about the centre of mass)
+      if (tid == 0)
+      {
+        const Comp& cc = p.comp[c];
+        const int m = __ldcg(p.list + c * p.capacity + min(sh.count[c] - 1, static_cast<int>(sh.u[3] * sh.count[c])));
+        sh.m = m;
+        const int dir = min(2, static_cast<int>(3.0 * sh.u[4]));
+        double3 old[kMaxAtoms], nw[kMaxAtoms];
+        for (int i = 0; i < na; ++i) old[i] = nw[i] = loadPos(p, m * na + i);
+        if (kind == 0)
+        {
+          const double d = p.max_translation * 2.0 * (sh.u[5] - 0.5);
+          for (int i = 0; i < na; ++i)
+          {
+            if (dir == 0) nw[i].x += d;
+            if (dir == 1) nw[i].y += d;
+            if (dir == 2) nw[i].z += d;
+          }
+        }
+        else
+        {
+          const double ang = p.max_rotation * 2.0 * (sh.u[5] - 0.5);
+          double sn, cs;
+          sincos(ang, &sn, &cs);
+          double ctr[3] = {0, 0, 0}, w = 0.0;
+          for (int i = 0; i < na; ++i)
+          {
+            ctr[0] += cc.masses[i] * old[i].x;
+            ctr[1] += cc.masses[i] * old[i].y;
+            ctr[2] += cc.masses[i] * old[i].z;
+            w += cc.masses[i];
+          }
+          for (int d = 0; d < 3; ++d) ctr[d] /= w;
+          const int a1 = (dir + 1) % 3, a2 = (dir + 2) % 3;
+          for (int i = 0; i < na; ++i)
+          {
+            const double dv[3] = {old[i].x - ctr[0], old[i].y - ctr[1], old[i].z - ctr[2]};
+            double r[3] = {dv[0], dv[1], dv[2]};
+            r[a1] = cs * dv[a1] - sn * dv[a2];
+            r[a2] = sn * dv[a1] + cs * dv[a2];
+            nw[i] = make_double3(ctr[0] + r[0], ctr[1] + r[1], ctr[2] + r[2]);
+          }
+        }
+        for (int i = 0; i < na; ++i)
+        {
+          sh.ta[i] = nw[i];
+          sh.tf[i] = toFixed(p, nw[i], cc.types[i]);
+          atomGrid[i] = cc.vdw_grid[i];
+          sh.ta[na + i] = old[i];
+          sh.tf[na + i] = toFixed(p, old[i], cc.types[i]);
+          atomGrid[na + i] = cc.vdw_grid[i];
+          sh.cpos[0][i] = nw[i];
+          sh.cq[0][i] = cc.charges[i];
+          sh.cpos[0][na + i] = old[i];
+          sh.cq[0][na + i] = -cc.charges[i];
+          sh.mol[i] = nw[i];
+        }
+        sh.cn[0] = 2 * na;
+        sh.nta = 2 * na;
+        sh.ncand = p.use_charge ? 1 : 0;
+      }
+      __syncthreads();
+      if (!phase(p, sh, sh.m, atomGrid)) break;
+      if (tid == 0)
+      {
+        bool ovn = false;
+        double dU = 0.0;
+        for (int i = 0; i < na; ++i)
+        {
+          ovn |= ovlOf(sh, i);
+          dU += sh.tot[i] - sh.tot[na + i];
+        }
+        if (p.use_charge) dU += sh.tot[sh.nta];
+        if (!ovn && sh.u[6] < exp(-p.beta * dU))
+        {
+          sh.accept = 1;
+          sh.energy += dU;
+        }
+      }
+      __syncthreads();
+      if (sh.accept)
+      {
+        if (tid == 0) storeMolecule(p, sh.m, c, sh.mol);
+        if (p.use_charge)
+          for (int kk = tid; kk < k1 - k0; kk += kThreads)
+          {
+            const double2 d = sh.dk[0][kk];
+            p.sk[k0 + kk].x += d.x;
+            p.sk[k0 + kk].y += d.y;
+          }
+      }
+      ran = true;
+    }
+    else if (kind == 2 && sh.n < p.capacity)
+    {
+      // CBMC insertion: first-bead trials, then orientations about the selected bead
+      const Comp& cc = p.comp[c];
+      const int sb = cc.starting_bead;
+      if (tid < p.k1)
+      {
+        const double3 r = firstBeadPosition(p, cc, move, tid);
+        sh.ta[tid] = r;
+        sh.tf[tid] = toFixed(p, r, cc.types[sb]);
+        atomGrid[tid] = cc.vdw_grid[sb];
+        sh.logq[tid] = cc.prop_cdf ? log(proposalDensity(p, cc, r)) : 0.0;
+      }
+      if (tid == 0)
+      {
+        sh.nta = p.k1;
+        sh.ncand = 0;
+      }
+      __syncthreads();
+      if (!phase(p, sh, -1, atomGrid)) break;
+      if (tid == 0)
+      {
+        double lw[kMaxTrials];
+        unsigned ok = 0u;
+        for (int t = 0; t < p.k1; ++t)
+        {
+          lw[t] = -p.beta * sh.tot[t] - sh.logq[t];
+          if (!ovlOf(sh, t)) ok |= 1u << t;
+        }
+        double W;
+        const int sel = selectTrial(lw, ok, p.k1, urand(p, move, slot(kKindMove, 1, 0)).x, &W);
+        sh.selFirst = sel;
+        sh.W = W;
+        if (sel >= 0)
+        {
+          sh.first = sh.ta[sel];
+          sh.dU = sh.tot[sel];
+          // orientation trials: the other atoms of each orientation; Ewald candidates: whole molecules
+          int a = 0;
+          for (int t = 0; t < p.k2; ++t)
+          {
+            double3 x[kMaxAtoms];
+            orientedMolecule(p, cc, sh.first, move, kKindOrient, t, x);
+            for (int i = 0; i < na; ++i)
+            {
+              sh.cpos[t][i] = x[i];
+              sh.cq[t][i] = cc.charges[i];
+              if (i == sb) continue;
+              sh.ta[a] = x[i];
+              sh.tf[a] = toFixed(p, x[i], cc.types[i]);
+              atomGrid[a] = cc.vdw_grid[i];
+              ++a;
+            }
+            sh.cn[t] = na;
+          }
+          sh.nta = a;
+          sh.ncand = p.use_charge ? p.k2 : 0;
+        }
+      }
+      __syncthreads();
+      if (sh.selFirst >= 0)
+      {
+        if (!phase(p, sh, -1, atomGrid)) break;
+        if (tid == 0)
+        {
+          double lw[kMaxTrials];
+          unsigned ok = 0u;
+          const int per = na - 1;
+          for (int t = 0; t < p.k2; ++t)
+          {
+            double e = 0.0;
+            bool o = false;
+            for (int i = 0; i < per; ++i)
+            {
+              e += sh.tot[t * per + i];
+              o |= ovlOf(sh, t * per + i);
+            }
+            lw[t] = -p.beta * e;
+            if (!o) ok |= 1u << t;
+          }
+          double W2;
+          const int sel = selectTrial(lw, ok, p.k2, urand(p, move, slot(kKindMove, 2, 0)).x, &W2);
+          if (sel >= 0 && sh.W * W2 >= 1e-150)
+          {
+            const double dEw = p.use_charge ? sh.tot[sh.nta + sel] + cc.self_excl : 0.0;
+            const double W = sh.W * W2;
+            const double pacc = exp(-p.beta * dEw) * p.beta * cc.fugacity * p.volume /
+                                static_cast<double>(sh.count[c] + 1) * W / cc.w_ig;
+            if (sh.u[6] < pacc)
+            {
+              double e = 0.0;
+              for (int i = 0; i < per; ++i) e += sh.tot[sel * per + i];
+              sh.accept = 1;
+              sh.energy += sh.dU + e + dEw;
+              sh.selOrient = sel;
+              for (int i = 0; i < na; ++i) sh.mol[i] = sh.cpos[sel][i];
+            }
+          }
+        }
+        __syncthreads();
+        if (sh.accept)
+        {
+          if (tid == 0)
+          {
+            const int m = sh.n;
+            storeMolecule(p, m, c, sh.mol);
+            p.comp_of[m] = c;
+            p.slot[m] = sh.count[c];
+            p.list[c * p.capacity + sh.count[c]] = m;
+            sh.count[c] += 1;
+            sh.n += 1;
+          }
+          if (p.use_charge)
+            for (int kk = tid; kk < k1 - k0; kk += kThreads)
+            {
+              const double2 d = sh.dk[sh.selOrient][kk];
+              p.sk[k0 + kk].x += d.x;
+              p.sk[k0 + kk].y += d.y;
+            }
+        }
+      }
+      ran = true;
+    }
+    else if (kind == 3 && sh.count[c] > 0)
+    {
+      // CBMC deletion: first-bead retrace (trial 0 = old bead) and orientation retrace about the old bead
+      const Comp& cc = p.comp[c];
+      const int sb = cc.starting_bead;
+      if (tid == 0) sh.m = __ldcg(p.list + c * p.capacity + min(sh.count[c] - 1, static_cast<int>(sh.u[3] * sh.count[c])));
+      __syncthreads();
+      const int m = sh.m;
+      if (tid < p.k1)
+      {
+        const double3 r = tid == 0 ? loadPos(p, m * na + sb) : firstBeadPosition(p, cc, move, tid);
+        sh.ta[tid] = r;
+        sh.tf[tid] = toFixed(p, r, cc.types[sb]);
+        atomGrid[tid] = cc.vdw_grid[sb];
+        sh.logq[tid] = cc.prop_cdf ? log(proposalDensity(p, cc, r)) : 0.0;
+      }
+      if (tid == 0)
+      {
+        const int last = sh.n - 1;
+        sh.preSlot = __ldcg(p.slot + m);
+        sh.preLastC = __ldcg(p.list + c * p.capacity + sh.count[c] - 1);
+        sh.preCl = __ldcg(p.comp_of + last);
+        sh.preSl = __ldcg(p.slot + last);
+        for (int i = 0; i < na; ++i) sh.preLast[i] = loadPos(p, last * na + i);
+        const double3 first = loadPos(p, m * na + sb);
+        int a = p.k1;
+        for (int t = 0; t < p.k2; ++t)
+        {
+          double3 x[kMaxAtoms];
+          if (t == 0)
+            for (int i = 0; i < na; ++i) x[i] = loadPos(p, m * na + i);
+          else
+            orientedMolecule(p, cc, first, move, kKindOrient, t, x);
+          for (int i = 0; i < na; ++i)
+          {
+            if (i == sb) continue;
+            sh.ta[a] = x[i];
+            sh.tf[a] = toFixed(p, x[i], cc.types[i]);
+            atomGrid[a] = cc.vdw_grid[i];
+            ++a;
+          }
+        }
+        for (int i = 0; i < na; ++i)
+        {
+          sh.cpos[0][i] = loadPos(p, m * na + i);
+          sh.cq[0][i] = -cc.charges[i];
+        }
+        sh.cn[0] = na;
+        sh.nta = a;
+        sh.ncand = p.use_charge ? 1 : 0;
+      }
+      __syncthreads();
+      if (!phase(p, sh, m, atomGrid)) break;
+      if (tid == 0)
+      {
+        double lw[kMaxTrials];
+        unsigned ok = 0u;
+        for (int t = 0; t < p.k1; ++t)
+        {
+          lw[t] = -p.beta * sh.tot[t] - sh.logq[t];
+          if (!ovlOf(sh, t)) ok |= 1u << t;
+        }
+        double W1, W2;
+        selectTrial(lw, ok, p.k1, 0.0, &W1);
+        unsigned ok2 = 0u;
+        double lw2[kMaxTrials], e0 = 0.0;
+        const int per = na - 1;
+        for (int t = 0; t < p.k2; ++t)
+        {
+          double e = 0.0;
+          bool o = false;
+          for (int i = 0; i < per; ++i)
+          {
+            e += sh.tot[p.k1 + t * per + i];
+            o |= ovlOf(sh, p.k1 + t * per + i);
+          }
+          if (t == 0) e0 = e;
+          lw2[t] = -p.beta * e;
+          if (!o) ok2 |= 1u << t;
+        }
+        selectTrial(lw2, ok2, p.k2, 0.0, &W2);
+        if ((ok & 1u) && (ok2 & 1u))
+        {
+          const double dEw = p.use_charge ? sh.tot[sh.nta] - cc.self_excl : 0.0;
+          const double W = W1 * W2;
+          const double pacc = exp(-p.beta * dEw) * static_cast<double>(sh.count[c]) /
+                              (p.beta * cc.fugacity * p.volume) * cc.w_ig / W;
+          if (sh.u[6] < pacc)
+          {
+            sh.accept = 1;
+            sh.energy += -(sh.tot[0] + e0) + dEw;
+          }
+        }
+      }
+      __syncthreads();
+      if (sh.accept)
+      {
+        if (tid == 0)
+        {
+          // remove m from its component list, then move the last molecule into slot m (from the values read before
+          // the barrier)
+          const int k = sh.preSlot, lastC = sh.preLastC;
+          p.list[c * p.capacity + k] = lastC;
+          p.slot[lastC] = k;
+          sh.count[c] -= 1;
+          const int last = sh.n - 1;
+          if (m != last)
+          {
+            const int cl = sh.preCl;
+            const int sl = (lastC == last) ? k : sh.preSl;
+            storeMolecule(p, m, cl, sh.preLast);
+            p.comp_of[m] = cl;
+            p.slot[m] = sl;
+            p.list[cl * p.capacity + sl] = m;
+          }
+          sh.n -= 1;
+        }
+        if (p.use_charge)
+          for (int kk = tid; kk < k1 - k0; kk += kThreads)
+          {
+            const double2 d = sh.dk[0][kk];
+            p.sk[k0 + kk].x += d.x;
+            p.sk[k0 + kk].y += d.y;
+          }
+      }
+      ran = true;
+    }
+    else if (kind == 4 && p.n_comp > 1)
+    {
+      // identity change: old and new component swapped with probability 1/2 (identity_change.cpp:62-66)
+      if (tid == 0)
+      {
+        int oldC = c, newC = (c + 1 + min(p.n_comp - 2, static_cast<int>(sh.u[3] * (p.n_comp - 1)))) % p.n_comp;
+        if (sh.u[4] < 0.5)
+        {
+          const int t = oldC;
+          oldC = newC;
+          newC = t;
+        }
+        sh.c = oldC;
+        sh.c2 = newC;
+        sh.m = sh.count[oldC] > 0
+                   ? __ldcg(p.list + oldC * p.capacity +
+                            min(sh.count[oldC] - 1, static_cast<int>(sh.u[5] * sh.count[oldC])))
+                   : -1;
+      }
+      __syncthreads();
+      if (sh.m >= 0)
+      {
+        const int m = sh.m, oldC = sh.c, newC = sh.c2;
+        const Comp& co = p.comp[oldC];
+        const Comp& cn = p.comp[newC];
+        if (tid == 0)
+        {
+          sh.preSlot = __ldcg(p.slot + m);
+          sh.preLastC = __ldcg(p.list + oldC * p.capacity + sh.count[oldC] - 1);
+          // trial atoms: new first bead (on the old starting bead), new orientations, old first bead, old retrace
+          const double3 first = loadPos(p, m * na + co.starting_bead);
+          int a = 0;
+          sh.ta[a] = first;
+          sh.tf[a] = toFixed(p, first, cn.types[cn.starting_bead]);
+          atomGrid[a] = cn.vdw_grid[cn.starting_bead];
+          ++a;
+          for (int t = 0; t < p.k2; ++t)
+          {
+            double3 x[kMaxAtoms];
+            orientedMolecule(p, cn, first, move, kKindNewOrient, t, x);
+            for (int i = 0; i < na; ++i)
+            {
+              sh.cpos[t][i] = x[i];
+              sh.cq[t][i] = cn.charges[i];
+              if (i == cn.starting_bead) continue;
+              sh.ta[a] = x[i];
+              sh.tf[a] = toFixed(p, x[i], cn.types[i]);
+              atomGrid[a] = cn.vdw_grid[i];
+              ++a;
+            }
+            for (int i = 0; i < na; ++i)
+            {
+              sh.cpos[t][na + i] = loadPos(p, m * na + i);
+              sh.cq[t][na + i] = -co.charges[i];
+            }
+            sh.cn[t] = 2 * na;
+          }
+          sh.ta[a] = first;
+          sh.tf[a] = toFixed(p, first, co.types[co.starting_bead]);
+          atomGrid[a] = co.vdw_grid[co.starting_bead];
+          ++a;
+          const double3 firstOld = first;
+          for (int t = 0; t < p.k2; ++t)
+          {
+            double3 x[kMaxAtoms];
+            if (t == 0)
+              for (int i = 0; i < na; ++i) x[i] = loadPos(p, m * na + i);
+            else
+              orientedMolecule(p, co, firstOld, move, kKindOldOrient, t, x);
+            for (int i = 0; i < na; ++i)
+            {
+              if (i == co.starting_bead) continue;
+              sh.ta[a] = x[i];
+              sh.tf[a] = toFixed(p, x[i], co.types[i]);
+              atomGrid[a] = co.vdw_grid[i];
+              ++a;
+            }
+          }
+          sh.nta = a;
+          sh.ncand = p.use_charge ? p.k2 : 0;
+        }
+        __syncthreads();
+        if (!phase(p, sh, m, atomGrid)) break;
+        if (tid == 0)
+        {
+          const int per = na - 1;
+          const int base2 = 1 + p.k2 * per;  // index of the old first bead
+          double lw[kMaxTrials], lw2[kMaxTrials];
+          unsigned ok = 0u, ok2 = 0u;
+          double e0 = 0.0;
+          for (int t = 0; t < p.k2; ++t)
+          {
+            double e = 0.0, eo = 0.0;
+            bool o = false, oo = false;
+            for (int i = 0; i < per; ++i)
+            {
+              e += sh.tot[1 + t * per + i];
+              o |= ovlOf(sh, 1 + t * per + i);
+              eo += sh.tot[base2 + 1 + t * per + i];
+              oo |= ovlOf(sh, base2 + 1 + t * per + i);
+            }
+            lw[t] = -p.beta * e;
+            lw2[t] = -p.beta * eo;
+            if (!o) ok |= 1u << t;
+            if (!oo) ok2 |= 1u << t;
+            if (t == 0) e0 = eo;
+          }
+          double Wn2, Wo2;
+          const int sel = selectTrial(lw, ok, p.k2, urand(p, move, slot(kKindMove, 3, 0)).x, &Wn2);
+          selectTrial(lw2, ok2, p.k2, 0.0, &Wo2);
+          const bool newFirstOk = !ovlOf(sh, 0), oldOk = !ovlOf(sh, base2) && (ok2 & 1u);
+          const double Wn = exp(-p.beta * sh.tot[0]) * Wn2, Wo = exp(-p.beta * sh.tot[base2]) * Wo2;
+          if (newFirstOk && sel >= 0 && oldOk && Wn >= 1e-150)
+          {
+            const double dEw = p.use_charge ? sh.tot[sh.nta + sel] + cn.self_excl - co.self_excl : 0.0;
+            const double pacc = exp(-p.beta * dEw) * (Wn / cn.w_ig) * cn.fugacity *
+                                static_cast<double>(sh.count[oldC]) /
+                                ((Wo / co.w_ig) * co.fugacity * static_cast<double>(sh.count[newC] + 1));
+            if (sh.u[6] < pacc)
+            {
+              double en = sh.tot[0];
+              for (int i = 0; i < per; ++i) en += sh.tot[1 + sel * per + i];
+              sh.accept = 1;
+              sh.energy += (en - (sh.tot[base2] + e0)) + dEw;
+              sh.selOrient = sel;
+              for (int i = 0; i < na; ++i) sh.mol[i] = sh.cpos[sel][i];
+            }
+          }
+        }
+        __syncthreads();
+        if (sh.accept)
+        {
+          if (tid == 0)
+          {
+            storeMolecule(p, m, newC, sh.mol);
+            // move m from the old component's list to the new one's (from the values read before the barrier)
+            const int k = sh.preSlot, lastC = sh.preLastC;
+            p.list[oldC * p.capacity + k] = lastC;
+            p.slot[lastC] = k;
+            sh.count[oldC] -= 1;
+            p.comp_of[m] = newC;
+            p.slot[m] = sh.count[newC];
+            p.list[newC * p.capacity + sh.count[newC]] = m;
+            sh.count[newC] += 1;
+          }
+          if (p.use_charge)
+            for (int kk = tid; kk < k1 - k0; kk += kThreads)
+            {
+              const double2 d = sh.dk[sh.selOrient][kk];
+              p.sk[k0 + kk].x += d.x;
+              p.sk[k0 + kk].y += d.y;
+            }
+        }
+        c = oldC;
+      }
+      ran = true;
+    }
+    (void)ran;
+    __syncthreads();
+    if (tid == 0 && p.record)
+    {
+      sh.stats[kind] += 1.0;
+      sh.stats[5 + kind] += sh.accept ? 1.0 : 0.0;
+      for (int q = 0; q < p.n_comp && q < 4; ++q) sh.stats[10 + q] += sh.count[q];
+      sh.stats[14] += sh.energy;
+      sh.stats[15] += 1.0;
+    }
+    __syncthreads();
+  }
+  if (blockIdx.x == 0 && tid == 0 && !sh.fail)
+  {
+    p.n_state[0] = sh.n;
+    for (int c = 0; c < kMaxComp; ++c) p.n_state[1 + c] = sh.count[c];
+    *p.energy = sh.energy;
+    *p.move_base = move0 + moves;
+    for (int k = 0; k < kStats; ++k) p.stats[k] = sh.stats[k];
+  }
+}
+}  // namespace
+
+struct rg_mixture
+{
+  rg_ctx* ctx = nullptr;
+  rg_system* system = nullptr;
+  rg_ewald* ewald = nullptr;
+  Params p{};
+  int blocks = 0;
+  int n_comp = 0;
+  std::vector<void*> allocs;
+};
+
+namespace
+{
+void freeAll(rg_mixture* x)
+{
+  for (void* q : x->allocs) cudaFree(q);
+  x->allocs.clear();
+}
+}  // namespace
+
+extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const rg_gcmc_component* comps,
+                                       int n_components, const rg_mixture_params* params, const double* xyz,
+                                       const int32_t* comp_of_molecule, int n_molecules, rg_mixture** out)
+{
+  if (!system || !comps || !params || !out || n_components < 1 || n_components > kMaxComp || n_molecules < 0 ||
+      (n_molecules > 0 && (!xyz || !comp_of_molecule)))
+    return RG_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  rgd::FF ff{};
+  rgd::Box box{};
+  const double* tg[64] = {};
+  const double* eg = nullptr;
+  int nt = 0, gd[3] = {0, 0, 0};
+  double gic[3][3];
+  rg_ctx* ctx = nullptr;
+  rg_status st = rgd::systemExport(system, &ff, &box, tg, &eg, &nt, gd, gic, &ctx);
+  if (st) return st;
+  if (nt > kMaxTypes) return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: at most 16 pseudo-atom types");
+  const int na = comps[0].n_atoms;
+  if (na < 2 || na > kMaxAtoms) return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: molecules of 2-4 atoms");
+  for (int c = 0; c < n_components; ++c)
+    if (comps[c].n_atoms != na || comps[c].starting_bead < 0 || comps[c].starting_bead >= na)
+      return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: every component needs the same atom count");
+  if (params->n_first_bead_trials < 1 || params->n_first_bead_trials > kMaxTrials ||
+      params->n_orientation_trials < 1 || params->n_orientation_trials > kMaxTrials)
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture: 1..12 first-bead and orientation trials");
+  if (2 + 2 * params->n_orientation_trials * (na - 1) > kMaxItems ||
+      params->n_first_bead_trials + params->n_orientation_trials * (na - 1) > kMaxItems)
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture: too many trial atoms per phase");
+  if (params->max_molecules < n_molecules || params->max_molecules < 1 || params->max_molecules > (1 << 22))
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture: max_molecules");
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  auto* x = new rg_mixture();
+  x->ctx = ctx;
+  x->system = system;
+  x->ewald = ewald;
+  x->n_comp = n_components;
+  Params& p = x->p;
+  p.box = box;
+  p.grid.nx = gd[0];
+  p.grid.ny = gd[1];
+  p.grid.nz = gd[2];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+    {
+      p.grid.ic[i][j] = gic[i][j];
+      p.hf[i][j] = static_cast<float>(box.c[i][j]);
+    }
+  p.ewald_grid = eg;
+  p.overlap = ff.overlap;
+  p.overlap_f = static_cast<float>(ff.overlap);
+  p.use_charge = (ff.use_charge && ewald) ? 1 : 0;
+  p.beta = params->beta;
+  p.volume = box.volume;
+  p.max_translation = params->max_translation;
+  p.max_rotation = params->max_rotation;
+  p.p_translation = params->p_translation;
+  p.p_rotation = params->p_rotation;
+  p.p_swap = params->p_swap;
+  p.p_identity = params->p_identity;
+  p.k1 = params->n_first_bead_trials;
+  p.k2 = params->n_orientation_trials;
+  p.capacity = params->max_molecules;
+  p.na = na;
+  p.n_comp = n_components;
+  p.seed = params->seed;
+  // pair table (FP32) and the charge of each type
+  std::vector<float4> ljf(kMaxTypes * kMaxTypes, make_float4(0, 0, 0, 0));
+  std::vector<float> qtype(kMaxTypes, 0.0f);
+  {
+    std::vector<double> eps4(nt * nt), sig2(nt * nt), shift(nt * nt);
+    std::vector<int> lj(nt * nt);
+    cudaError_t e = cudaMemcpy(eps4.data(), ff.eps4, sizeof(double) * nt * nt, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(sig2.data(), ff.sig2, sizeof(double) * nt * nt, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(shift.data(), ff.shift, sizeof(double) * nt * nt, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(lj.data(), ff.lj, sizeof(int) * nt * nt, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+    {
+      delete x;
+      return rg::cudaFail(ctx, e, "rg_mixture_create: pair table");
+    }
+    for (int a = 0; a < nt; ++a)
+      for (int b = 0; b < nt; ++b)
+        if (lj[a * nt + b])
+          ljf[a * kMaxTypes + b] = make_float4(static_cast<float>(eps4[a * nt + b]), static_cast<float>(sig2[a * nt + b]),
+                                               static_cast<float>(shift[a * nt + b]), 1.0f);
+  }
+  const double rcv_mol = params->cutoff_molecule_vdw, rcc = params->cutoff_coulomb;
+  p.rc2_mm = static_cast<float>(rcv_mol * rcv_mol);
+  p.rc2_c = static_cast<float>(rcc * rcc);
+  p.alpha = static_cast<float>(ff.alpha);
+  p.coul = static_cast<float>(ff.coul);
+  // components
+  double ewaldAlpha = ff.alpha;
+  for (int c = 0; c < n_components; ++c)
+  {
+    const rg_gcmc_component& q = comps[c];
+    Comp& cc = p.comp[c];
+    cc.n_atoms = q.n_atoms;
+    cc.starting_bead = q.starting_bead;
+    for (int i = 0; i < q.n_atoms; ++i)
+    {
+      cc.types[i] = q.types[i];
+      cc.charges[i] = q.charges[i];
+      cc.masses[i] = q.masses[i];
+      for (int d = 0; d < 3; ++d) cc.offsets[i][d] = q.offsets[3 * i + d];
+      cc.vdw_grid[i] = (q.types[i] >= 0 && q.types[i] < 64) ? tg[q.types[i]] : nullptr;
+      if (q.types[i] < 0 || q.types[i] >= nt)
+      {
+        delete x;
+        return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture: component atom type");
+      }
+      qtype[q.types[i]] = static_cast<float>(q.charges[i]);
+    }
+    cc.fugacity = params->fugacity[c];
+    cc.w_ig = params->w_ig[c] > 0.0 ? params->w_ig[c] : 1.0;
+    // Ewald self + intramolecular exclusion energy of one molecule (ewald.cpp:1164-1238, new-atom terms)
+    double self = 0.0, excl = 0.0;
+    const double C = rg::coulombFactor();
+    for (int i = 0; i < q.n_atoms; ++i) self -= C * ewaldAlpha * rg::kInvSqrtPi * q.charges[i] * q.charges[i];
+    for (int i = 0; i < q.n_atoms; ++i)
+      for (int j = i + 1; j < q.n_atoms; ++j)
+      {
+        double d2 = 0.0;
+        for (int k = 0; k < 3; ++k)
+        {
+          const double d = q.offsets[3 * i + k] - q.offsets[3 * j + k];
+          d2 += d * d;
+        }
+        const double r = std::sqrt(d2);
+        excl -= C * q.charges[i] * q.charges[j] * std::erf(ewaldAlpha * r) / r;
+      }
+    cc.self_excl = self + excl;
+  }
+  // Ewald tables
+  if (p.use_charge)
+  {
+    const char4* kv = nullptr;
+    const double* temp = nullptr;
+    const double2* srig = nullptr;
+    int64_t nk = 0;
+    int kmax[3];
+    double alpha, sis;
+    st = rgd::ewaldExport(ewald, &kv, &temp, &srig, &nk, kmax, &alpha, &sis);
+    if (st)
+    {
+      delete x;
+      return st;
+    }
+    p.kvec = kv;
+    p.temp = temp;
+    p.nk = static_cast<int>(nk);
+  }
+  // launch geometry: one CTA per SM, co-resident
+  int sms = 0, perSM = 0;
+  cudaError_t err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, mixtureKernel, kThreads, 0);
+  if (err != cudaSuccess || perSM < 1)
+  {
+    delete x;
+    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: kernel does not fit on an SM");
+  }
+  x->blocks = params->n_blocks > 0 ? std::min(params->n_blocks, sms * perSM) : sms;
+  if (p.use_charge && (p.nk + x->blocks - 1) / x->blocks > kMaxKPerCta)
+  {
+    delete x;
+    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: more than 64 k-vectors per CTA");
+  }
+  // device state
+  const int cap = p.capacity;
+  auto alloc = [&](void** ptr, size_t bytes) {
+    if (err == cudaSuccess) err = cudaMalloc(ptr, std::max<size_t>(bytes, 16));
+    if (err == cudaSuccess) x->allocs.push_back(*ptr);
+  };
+  float4* dljf = nullptr;
+  float* dq = nullptr;
+  alloc(reinterpret_cast<void**>(&dljf), sizeof(float4) * ljf.size());
+  alloc(reinterpret_cast<void**>(&dq), sizeof(float) * qtype.size());
+  alloc(reinterpret_cast<void**>(&p.pos), sizeof(double4) * cap * na);
+  alloc(reinterpret_cast<void**>(&p.fx), sizeof(int4) * cap * na);
+  alloc(reinterpret_cast<void**>(&p.comp_of), sizeof(int) * cap);
+  alloc(reinterpret_cast<void**>(&p.list), sizeof(int) * cap * kMaxComp);
+  alloc(reinterpret_cast<void**>(&p.slot), sizeof(int) * cap);
+  alloc(reinterpret_cast<void**>(&p.n_state), sizeof(int) * (1 + kMaxComp));
+  alloc(reinterpret_cast<void**>(&p.energy), sizeof(double));
+  alloc(reinterpret_cast<void**>(&p.move_base), sizeof(long long));
+  alloc(reinterpret_cast<void**>(&p.stats), sizeof(double) * kStats);
+  alloc(reinterpret_cast<void**>(&p.sk), sizeof(double2) * std::max(1, p.nk));
+  alloc(reinterpret_cast<void**>(&p.part), sizeof(double) * kRow * 2 * x->blocks);
+  alloc(reinterpret_cast<void**>(&p.bar), sizeof(unsigned) * 4);
+  p.ljf = dljf;
+  p.qtype = dq;
+  // host copies of the starting configuration
+  std::vector<double4> hpos(static_cast<size_t>(cap) * na);
+  std::vector<int4> hfx(static_cast<size_t>(cap) * na);
+  std::vector<int> hcomp(cap, 0), hlist(static_cast<size_t>(cap) * kMaxComp, 0), hslot(cap, 0);
+  int counts[kMaxComp] = {0, 0, 0, 0};
+  for (int m = 0; m < n_molecules; ++m)
+  {
+    const int c = comp_of_molecule[m];
+    if (c < 0 || c >= n_components)
+    {
+      freeAll(x);
+      delete x;
+      return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture: component index");
+    }
+    hcomp[m] = c;
+    hslot[m] = counts[c];
+    hlist[static_cast<size_t>(c) * cap + counts[c]] = m;
+    counts[c] += 1;
+    for (int i = 0; i < na; ++i)
+    {
+      const double* r = xyz + 3 * (static_cast<size_t>(m) * na + i);
+      hpos[m * na + i] = make_double4(r[0], r[1], r[2], 0.0);
+      double s[3];
+      for (int a = 0; a < 3; ++a) s[a] = box.ic[0][a] * r[0] + box.ic[1][a] * r[1] + box.ic[2][a] * r[2];
+      int f[3];
+      for (int a = 0; a < 3; ++a)
+      {
+        const double v = s[a] - std::floor(s[a]);
+        f[a] = static_cast<int>(static_cast<uint32_t>(static_cast<unsigned long long>(v * 4294967296.0)));
+      }
+      hfx[m * na + i] = make_int4(f[0], f[1], f[2], comps[c].types[i] | (m << 8));
+    }
+  }
+  int nstate[1 + kMaxComp] = {n_molecules, counts[0], counts[1], counts[2], counts[3]};
+  const double zero = 0.0;
+  const long long zl = 0;
+  cudaStream_t sm = ctx->stream;
+  if (err == cudaSuccess) err = cudaMemcpyAsync(dljf, ljf.data(), sizeof(float4) * ljf.size(), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(dq, qtype.data(), sizeof(float) * qtype.size(), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(p.pos, hpos.data(), sizeof(double4) * hpos.size(), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(p.fx, hfx.data(), sizeof(int4) * hfx.size(), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(p.comp_of, hcomp.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(p.list, hlist.data(), sizeof(int) * hlist.size(), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(p.slot, hslot.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(p.n_state, nstate, sizeof(nstate), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(p.energy, &zero, sizeof(double), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(p.move_base, &zl, sizeof(long long), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemsetAsync(p.stats, 0, sizeof(double) * kStats, sm);
+  if (err == cudaSuccess) err = cudaMemsetAsync(p.sk, 0, sizeof(double2) * std::max(1, p.nk), sm);
+  if (err == cudaSuccess) err = cudaMemsetAsync(p.bar, 0, sizeof(unsigned) * 4, sm);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(sm);
+  if (err != cudaSuccess)
+  {
+    freeAll(x);
+    delete x;
+    return rg::cudaFail(ctx, err, "rg_mixture_create");
+  }
+  *out = x;
+  return RG_OK;
+}
+
+extern "C" rg_status rg_mixture_destroy(rg_mixture* x)
+{
+  if (!x) return RG_OK;
+  cudaSetDevice(x->ctx->device);
+  cudaStreamSynchronize(x->ctx->stream);
+  freeAll(x);
+  delete x;
+  return RG_OK;
+}
+
+extern "C" rg_status rg_mixture_set_state(rg_mixture* x, double energy, const double* sk, int64_t n_doubles)
+{
+  if (!x) return RG_ERR_INVALID_ARGUMENT;
+  rg_ctx* ctx = x->ctx;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (sk)
+  {
+    if (n_doubles != 2ll * x->p.nk) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_set_state: 2 nk doubles");
+    RG_CUDA(ctx, cudaMemcpyAsync(x->p.sk, sk, sizeof(double) * n_doubles, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  RG_CUDA(ctx, cudaMemcpyAsync(x->p.energy, &energy, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
+}
+
+extern "C" rg_status rg_mixture_run(rg_mixture* x, int64_t moves, int record)
+{
+  if (!x || moves < 0) return RG_ERR_INVALID_ARGUMENT;
+  rg_ctx* ctx = x->ctx;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  x->p.record = record ? 1 : 0;
+  const int64_t per = 8192;
+  for (int64_t done = 0; done < moves; done += per)
+  {
+    int m = static_cast<int>(std::min<int64_t>(per, moves - done));
+    void* args[] = {&x->p, &m};
+    RG_CUDA(ctx, cudaLaunchCooperativeKernel(reinterpret_cast<void*>(mixtureKernel), dim3(x->blocks), dim3(kThreads),
+                                             args, 0, ctx->stream));
+  }
+  return RG_OK;
+}
+
+extern "C" rg_status rg_mixture_results(rg_mixture* x, rg_mixture_result* out)
+{
+  if (!x || !out) return RG_ERR_INVALID_ARGUMENT;
+  rg_ctx* ctx = x->ctx;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  int ns[1 + kMaxComp];
+  double e, st[kStats];
+  unsigned bar[4];
+  RG_CUDA(ctx, cudaMemcpyAsync(ns, x->p.n_state, sizeof(ns), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaMemcpyAsync(&e, x->p.energy, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaMemcpyAsync(st, x->p.stats, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaMemcpyAsync(bar, x->p.bar, sizeof(bar), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  std::memset(out, 0, sizeof(*out));
+  for (int c = 0; c < kMaxComp; ++c)
+  {
+    out->n_molecules[c] = ns[1 + c];
+    out->sum_n[c] = st[10 + c];
+  }
+  out->energy = e;
+  for (int k = 0; k < 5; ++k)
+  {
+    out->attempted[k] = static_cast<int64_t>(st[k]);
+    out->accepted[k] = static_cast<int64_t>(st[5 + k]);
+  }
+  out->sum_energy = st[14];
+  out->samples = static_cast<int64_t>(st[15]);
+  out->status = bar[2] ? RG_ERR_TIMEOUT : RG_OK;
+  return RG_OK;
+}
+
+extern "C" rg_status rg_mixture_get_positions(rg_mixture* x, double* xyz, int32_t* comp, int capacity_molecules,
+                                              int* n_molecules)
+{
+  if (!x || !xyz || !comp || !n_molecules) return RG_ERR_INVALID_ARGUMENT;
+  rg_ctx* ctx = x->ctx;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  int n = 0;
+  RG_CUDA(ctx, cudaMemcpyAsync(&n, x->p.n_state, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (n > capacity_molecules) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_get_positions: capacity");
+  std::vector<double4> pos(static_cast<size_t>(n) * x->p.na);
+  if (n > 0)
+  {
+    RG_CUDA(ctx, cudaMemcpyAsync(pos.data(), x->p.pos, sizeof(double4) * pos.size(), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    RG_CUDA(ctx, cudaMemcpyAsync(comp, x->p.comp_of, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (size_t i = 0; i < pos.size(); ++i)
+  {
+    xyz[3 * i] = pos[i].x;
+    xyz[3 * i + 1] = pos[i].y;
+    xyz[3 * i + 2] = pos[i].z;
+  }
+  *n_molecules = n;
+  return RG_OK;
+}
+
+extern "C" rg_status rg_mixture_get_structure_factors(rg_mixture* x, double* host, int64_t n_doubles)
+{
+  if (!x || !host || n_doubles != 2ll * x->p.nk) return RG_ERR_INVALID_ARGUMENT;
+  rg_ctx* ctx = x->ctx;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  RG_CUDA(ctx, cudaMemcpyAsync(host, x->p.sk, sizeof(double) * n_doubles, cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
+}
+
+extern "C" rg_status rg_mixture_set_proposal(rg_mixture* x, int component, rg_proposal* proposal,
+                                             const rg_box* unit_cell)
+{
+  if (!x || component < 0 || component >= x->n_comp) return RG_ERR_INVALID_ARGUMENT;
+  Comp& c = x->p.comp[component];
+  if (!proposal)
+  {
+    c.prop_cdf = nullptr;
+    c.prop_q = nullptr;
+    return RG_OK;
+  }
+  if (!unit_cell) return RG_ERR_INVALID_ARGUMENT;
+  rg_status st = rgd::proposalExport(proposal, &c.prop_cdf, &c.prop_q, &c.prop_G, &c.prop_eps);
+  if (st) return st;
+  // the simulation box must be rep[0] x rep[1] x rep[2] unit cells
+  const rg::HostBox ub = rg::makeHostBox(unit_cell);
+  for (int a = 0; a < 3; ++a)
+  {
+    double ratio = 0.0, norm = 0.0;
+    for (int r = 0; r < 3; ++r)
+    {
+      ratio += x->p.box.c[a][r] * ub.c[a][r];
+      norm += ub.c[a][r] * ub.c[a][r];
+    }
+    const double rep = ratio / norm;
+    x->p.rep[a] = static_cast<int>(std::lround(rep));
+    if (x->p.rep[a] < 1 || std::fabs(rep - x->p.rep[a]) > 1e-9 * rep)
+    {
+      c.prop_cdf = nullptr;
+      c.prop_q = nullptr;
+      return rg::fail(x->ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_set_proposal: box is not a replication of the cell");
+    }
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+    {
+      x->p.uc[i][j] = ub.c[i][j];
+      x->p.uic[i][j] = ub.ic[i][j];
+    }
+  return RG_OK;
+}
+
+extern "C" rg_status rg_mixture_info(rg_mixture* x, int* blocks, int64_t* nk)
+{
+  if (!x) return RG_ERR_INVALID_ARGUMENT;
+  if (blocks) *blocks = x->blocks;
+  if (nk) *nk = x->p.nk;
+  return RG_OK;
+}

@@ -49,10 +49,11 @@ def co2_component(bond: float = 1.16) -> RigidComponent:
 
 
 def n2_component(bond: float = 1.10) -> RigidComponent:
-    """3-site N2: N-N 1.10 A with the massless charge site N_com at the centre."""
+    """3-site N2: N-N 1.10 A with the massless charge site N_com at the centre; grown from atom 0 (an N), the
+    reference's default starting bead (Component::startingBead, component.ixx:195)."""
     m = np.array([14.00674, 0.0, 14.00674])
     return RigidComponent("N2", ("N_n2", "N_com", "N_n2"),
-                          _centred([(0, 0, 0.5 * bond), (0, 0, 0), (0, 0, -0.5 * bond)], m), m, 1)
+                          _centred([(0, 0, 0.5 * bond), (0, 0, 0), (0, 0, -0.5 * bond)], m), m, 0)
 
 
 def methane_component() -> RigidComponent:

@@ -74,6 +74,27 @@ class GcmcChainResult(ctypes.Structure):
         return d
 
 
+class MixtureParams(ctypes.Structure):
+    _fields_ = [("beta", ctypes.c_double), ("fugacity", ctypes.c_double * 4), ("w_ig", ctypes.c_double * 4),
+                ("cutoff_molecule_vdw", ctypes.c_double), ("cutoff_coulomb", ctypes.c_double),
+                ("max_translation", ctypes.c_double), ("max_rotation", ctypes.c_double),
+                ("p_translation", ctypes.c_double), ("p_rotation", ctypes.c_double), ("p_swap", ctypes.c_double),
+                ("p_identity", ctypes.c_double), ("n_first_bead_trials", ctypes.c_int32),
+                ("n_orientation_trials", ctypes.c_int32), ("max_molecules", ctypes.c_int32),
+                ("n_blocks", ctypes.c_int32), ("seed", ctypes.c_uint64)]
+
+
+class MixtureResult(ctypes.Structure):
+    _fields_ = [("n_molecules", ctypes.c_int64 * 4), ("energy", ctypes.c_double), ("attempted", ctypes.c_int64 * 5),
+                ("accepted", ctypes.c_int64 * 5), ("sum_n", ctypes.c_double * 4), ("sum_energy", ctypes.c_double),
+                ("samples", ctypes.c_int64), ("status", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+    def as_dict(self):
+        return {"n_molecules": list(self.n_molecules), "energy": self.energy, "attempted": list(self.attempted),
+                "accepted": list(self.accepted), "sum_n": list(self.sum_n), "sum_energy": self.sum_energy,
+                "samples": self.samples, "status": self.status}
+
+
 class AlkanePlan(ctypes.Structure):
     _fields_ = [("cluster_big", ctypes.c_int32), ("cluster_small", ctypes.c_int32), ("threads", ctypes.c_int32),
                 ("split", ctypes.c_int32), ("moves_per_launch", ctypes.c_int32), ("reserved", ctypes.c_int32),
@@ -147,6 +168,15 @@ def lib():
         L.rg_ewald_accept.argtypes = [vp]
         L.rg_ewald_get_structure_factors.argtypes = [vp, i32, vp, i64]
         L.rg_ewald_set_structure_factors.argtypes = [vp, vp, i64]
+        L.rg_mixture_create.argtypes = [vp, vp, vp, i32, P(MixtureParams), vp, vp, i32, P(vp)]
+        L.rg_mixture_destroy.argtypes = [vp]
+        L.rg_mixture_set_state.argtypes = [vp, d, vp, i64]
+        L.rg_mixture_run.argtypes = [vp, i64, i32]
+        L.rg_mixture_results.argtypes = [vp, P(MixtureResult)]
+        L.rg_mixture_get_positions.argtypes = [vp, vp, vp, i32, P(i32)]
+        L.rg_mixture_get_structure_factors.argtypes = [vp, vp, i64]
+        L.rg_mixture_set_proposal.argtypes = [vp, i32, vp, P(RgBox)]
+        L.rg_mixture_info.argtypes = [vp, P(i32), P(i64)]
         from .alkane import RgAlkaneChain
         L.rg_alkane_create.argtypes = [vp, P(RgForceField), vp, i32, ctypes.c_uint64, P(vp)]
         L.rg_alkane_destroy.argtypes = [vp]
@@ -687,3 +717,111 @@ def alkane_grow_vacuum(ctx: Context, ff: ForceField, chain, beta: float, n: int,
     if not details:
         return mean.value
     return mean.value, w, th.reshape(n, max(0, nb - 2)), cp.reshape(n, max(0, nb - 3))
+
+
+def component_struct(component, ff: ForceField) -> GcmcComponent:
+    c = GcmcComponent()
+    c.n_atoms = component.n_atoms
+    c.starting_bead = component.starting_bead
+    types, charges = component.types(ff), component.charges(ff)
+    for i in range(component.n_atoms):
+        c.types[i] = int(types[i])
+        c.charges[i] = float(charges[i])
+        c.masses[i] = float(component.masses[i])
+        for d in range(3):
+            c.offsets[3 * i + d] = float(component.offsets[i][d])
+    return c
+
+
+class Mixture:
+    """One large system of several rigid components advanced on the whole GPU (rg_mixture)."""
+
+    def __init__(self, system: System, ewald, components, beta: float, fugacities, xyz, comp, max_molecules: int,
+                 seed: int = 1, probabilities=(1.0, 1.0, 1.0, 1.0), n_first: int = 10, n_orient: int = 10,
+                 max_translation: float = 1.0, max_rotation: float = 0.5235987755982988, n_blocks: int = 0,
+                 w_ig=None):
+        self.ctx = system.ctx
+        self.system = system
+        self.components = list(components)
+        ff = system.ff
+        arr = (GcmcComponent * len(self.components))()
+        for i, c in enumerate(self.components):
+            arr[i] = component_struct(c, ff)
+        p = MixtureParams()
+        p.beta = beta
+        for i, f in enumerate(fugacities):
+            p.fugacity[i] = f
+            p.w_ig[i] = 1.0 if w_ig is None else w_ig[i]
+        p.cutoff_molecule_vdw, p.cutoff_coulomb = ff.cutoff_molecule_vdw, ff.cutoff_coulomb
+        p.max_translation, p.max_rotation = max_translation, max_rotation
+        p.p_translation, p.p_rotation, p.p_swap, p.p_identity = probabilities
+        p.n_first_bead_trials, p.n_orientation_trials = n_first, n_orient
+        p.max_molecules, p.n_blocks, p.seed = max_molecules, n_blocks, seed
+        x = np.ascontiguousarray(xyz, dtype=np.float64)
+        cc = np.ascontiguousarray(comp, dtype=np.int32)
+        self.na = self.components[0].n_atoms
+        self.max_molecules = max_molecules
+        h = ctypes.c_void_p()
+        check(self.ctx.handle, lib().rg_mixture_create(system.handle, ewald.handle if ewald is not None else None,
+                                                       ctypes.cast(arr, ctypes.c_void_p), len(self.components),
+                                                       ctypes.byref(p), ctypes.c_void_p(x.ctypes.data) if len(cc) else None,
+                                                       ctypes.c_void_p(cc.ctypes.data) if len(cc) else None, len(cc),
+                                                       ctypes.byref(h)), "rg_mixture_create")
+        self.handle = h
+        self.ctx.adopt(self)
+
+    def close(self):
+        if self.handle:
+            lib().rg_mixture_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, energy: float, sk=None):
+        s = None if sk is None else np.ascontiguousarray(sk, dtype=np.float64)
+        check(self.ctx.handle, lib().rg_mixture_set_state(self.handle, energy,
+                                                          None if s is None else ctypes.c_void_p(s.ctypes.data),
+                                                          0 if s is None else len(s)), "rg_mixture_set_state")
+
+    def run(self, moves: int, record: bool = True):
+        check(self.ctx.handle, lib().rg_mixture_run(self.handle, moves, 1 if record else 0), "rg_mixture_run")
+
+    def results(self) -> dict:
+        r = MixtureResult()
+        check(self.ctx.handle, lib().rg_mixture_results(self.handle, ctypes.byref(r)), "rg_mixture_results")
+        return r.as_dict()
+
+    def positions(self):
+        xyz = np.empty(3 * self.max_molecules * self.na)
+        comp = np.empty(self.max_molecules, dtype=np.int32)
+        n = ctypes.c_int32()
+        check(self.ctx.handle, lib().rg_mixture_get_positions(self.handle, ctypes.c_void_p(xyz.ctypes.data),
+                                                              ctypes.c_void_p(comp.ctypes.data), self.max_molecules,
+                                                              ctypes.byref(n)), "rg_mixture_get_positions")
+        return xyz[: 3 * n.value * self.na].reshape(n.value, self.na, 3), comp[: n.value].copy()
+
+    def structure_factors(self) -> np.ndarray:
+        b, nk = ctypes.c_int32(), ctypes.c_int64()
+        check(self.ctx.handle, lib().rg_mixture_info(self.handle, ctypes.byref(b), ctypes.byref(nk)), "rg_mixture_info")
+        out = np.empty(2 * nk.value)
+        check(self.ctx.handle, lib().rg_mixture_get_structure_factors(self.handle, ctypes.c_void_p(out.ctypes.data),
+                                                                      len(out)), "rg_mixture_get_structure_factors")
+        return out
+
+    def info(self):
+        b, nk = ctypes.c_int32(), ctypes.c_int64()
+        check(self.ctx.handle, lib().rg_mixture_info(self.handle, ctypes.byref(b), ctypes.byref(nk)), "rg_mixture_info")
+        return {"blocks": b.value, "n_kvectors": nk.value}
+
+    def set_proposal(self, component: int, proposal, unit_cell=None):
+        if proposal is None:
+            check(self.ctx.handle, lib().rg_mixture_set_proposal(self.handle, component, None, None),
+                  "rg_mixture_set_proposal")
+        else:
+            box = box_struct(unit_cell)
+            check(self.ctx.handle, lib().rg_mixture_set_proposal(self.handle, component, proposal.handle,
+                                                                 ctypes.byref(box)), "rg_mixture_set_proposal")

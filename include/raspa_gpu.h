@@ -420,6 +420,7 @@ typedef struct rg_mixture_params
   double fugacity[4];     /* per component, internal units */
   double w_ig[4];         /* ideal-gas Rosenbluth weight per component (0 = 1) */
   double cutoff_molecule_vdw, cutoff_coulomb;
+  double cutoff_framework_vdw; /* explicit framework pairs of atom types without a VDW grid */
   double max_translation, max_rotation;
   double p_translation, p_rotation, p_swap, p_identity; /* a component is chosen uniformly, then the move */
   int32_t n_first_bead_trials, n_orientation_trials;    /* 1..12 */

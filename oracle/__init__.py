@@ -546,7 +546,7 @@ class OMixSetup(ctypes.Structure):
                 ("p_translation", ctypes.c_double), ("p_rotation", ctypes.c_double), ("p_swap", ctypes.c_double),
                 ("p_identity", ctypes.c_double), ("n_first_bead_trials", ctypes.c_int32),
                 ("n_orientation_trials", ctypes.c_int32), ("max_molecules", ctypes.c_int32),
-                ("use_ewald", ctypes.c_int32)]
+                ("use_ewald", ctypes.c_int32), ("framework", ctypes.c_void_p), ("n_framework", ctypes.c_int32)]
 
 
 class OMixResult(ctypes.Structure):
@@ -563,9 +563,9 @@ class OMixResult(ctypes.Structure):
 def mixture_run(ff, cell, components, beta, fugacities, xyz, comp, steps, seed=1, grids=None, grid_dims=None,
                 grid_cell=None, s_framework=None, use_ewald=True, max_translation=1.0,
                 max_rotation=0.5235987755982988, probabilities=(1.0, 1.0, 1.0, 1.0), n_first=10, n_orient=10,
-                max_molecules=512, w_ig=None):
+                max_molecules=512, w_ig=None, framework=None):
     """One oracle mixture run from the molecules xyz[n, na, 3] of components comp[n]; returns (result dict, final xyz,
-    final comp, seconds)."""
+    final comp, seconds). framework: atom records of the framework, seen explicitly by atom types without a grid."""
     L = lib()
     if not hasattr(L, "_mixture_declared"):
         L.oracle_mixture_run.argtypes = [ctypes.POINTER(OMixSetup), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
@@ -610,6 +610,10 @@ def mixture_run(ff, cell, components, beta, fugacities, xyz, comp, steps, seed=1
     s.n_first_bead_trials, s.n_orientation_trials = n_first, n_orient
     s.max_molecules = max_molecules
     s.use_ewald = 1 if use_ewald else 0
+    if framework is not None and len(framework):
+        fw = np.ascontiguousarray(framework)
+        keep.append(fw)
+        s.framework, s.n_framework = fw.ctypes.data, len(fw)
     x = np.ascontiguousarray(xyz, dtype=np.float64)
     cc = np.ascontiguousarray(comp, dtype=np.int32)
     na = components[0].n_atoms

@@ -77,7 +77,8 @@ struct Mixture
   bool external(const oatom* set, int cnt, int64_t skip, double& e)
   {
     oenergy ef, em;
-    if (!oracle_cbmc_framework_molecule(p->ff, &p->box, p->grids, p->gnx, p->gny, p->gnz, &p->grid_cell, nullptr, 0,
+    if (!oracle_cbmc_framework_molecule(p->ff, &p->box, p->grids, p->gnx, p->gny, p->gnz, &p->grid_cell, p->framework,
+                                        p->n_framework,
                                         p->ff->cutoff_framework_vdw, p->ff->cutoff_coulomb, set, cnt, -1, &ef))
       return false;
     if (!oracle_cbmc_intermolecular(p->ff, &p->box, atoms.data(), n * na, p->ff->cutoff_molecule_vdw,
@@ -396,7 +397,8 @@ struct Mixture
     for (int m = 0; m < n; ++m)
     {
       oenergy ef;
-      oracle_cbmc_framework_molecule(p->ff, &p->box, p->grids, p->gnx, p->gny, p->gnz, &p->grid_cell, nullptr, 0,
+      oracle_cbmc_framework_molecule(p->ff, &p->box, p->grids, p->gnx, p->gny, p->gnz, &p->grid_cell, p->framework,
+                                        p->n_framework,
                                      p->ff->cutoff_framework_vdw, p->ff->cutoff_coulomb, &atoms[m * na], na, -1, &ef);
       e += ef.framework_molecule_vdw + ef.framework_molecule_charge;
       if (m + 1 < n)
@@ -426,15 +428,39 @@ extern "C" void oracle_mixture_run(const omix_setup* setup, const double* xyz_in
 {
   Mixture mx(setup, seed * 0x100000001b3ULL + 0x51ed270b27ULL);
   const int na = mx.na;
+  // inverse of the cell (columns = lattice vectors) for the minimum image of intramolecular separations
+  const double(&h)[3][3] = mx.cell;  // h[c][r]: component r of lattice vector c
+  const double det = h[0][0] * (h[1][1] * h[2][2] - h[1][2] * h[2][1]) - h[1][0] * (h[0][1] * h[2][2] - h[0][2] * h[2][1]) +
+                     h[2][0] * (h[0][1] * h[1][2] - h[0][2] * h[1][1]);
+  double M[3][3], inv[3][3];  // M[r][c] = h[c][r]; inv = M^-1: fractional k = sum_r inv[k][r] * cartesian r
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) M[r][c] = h[c][r];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+    {
+      // inv[i][j] = cofactor(j, i) / det, cofactors from cyclic indices
+      const int j1 = (j + 1) % 3, j2 = (j + 2) % 3, i1 = (i + 1) % 3, i2 = (i + 2) % 3;
+      inv[i][j] = (M[j1][i1] * M[j2][i2] - M[j1][i2] * M[j2][i1]) / det;
+    }
   for (int m = 0; m < n_in; ++m)
   {
     const omix_component& c = setup->comps[comp_in[m]];
+    const double* r0 = xyz_in + 3 * (m * na);
     for (int i = 0; i < na; ++i)
     {
+      // molecules are kept whole: atom i = atom 0 + the minimum image of their separation
+      const double* ri = xyz_in + 3 * (m * na + i);
+      const double dr[3] = {ri[0] - r0[0], ri[1] - r0[1], ri[2] - r0[2]};
+      double sd[3];
+      for (int k = 0; k < 3; ++k)
+      {
+        sd[k] = inv[k][0] * dr[0] + inv[k][1] * dr[1] + inv[k][2] * dr[2];
+        sd[k] -= std::nearbyint(sd[k]);
+      }
       oatom a{};
-      a.x = xyz_in[3 * (m * na + i)];
-      a.y = xyz_in[3 * (m * na + i) + 1];
-      a.z = xyz_in[3 * (m * na + i) + 2];
+      a.x = r0[0] + h[0][0] * sd[0] + h[1][0] * sd[1] + h[2][0] * sd[2];
+      a.y = r0[1] + h[0][1] * sd[0] + h[1][1] * sd[1] + h[2][1] * sd[2];
+      a.z = r0[2] + h[0][2] * sd[0] + h[1][2] * sd[1] + h[2][2] * sd[2];
       a.charge = c.charges[i];
       a.scaling_vdw = a.scaling_coulomb = 1.0;
       a.molecule_id = static_cast<uint32_t>(m);

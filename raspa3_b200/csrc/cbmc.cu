@@ -471,4 +471,12 @@ rg_status systemExport(rg_system* s, FF* ff, Box* box, const double** type_grids
   *ctx = s->ctx;
   return RG_OK;
 }
+
+rg_status systemFramework(rg_system* s, const rg_atom** fw, int* n_fw)
+{
+  if (!s) return RG_ERR_INVALID_ARGUMENT;
+  *fw = s->fw;
+  *n_fw = s->n_fw;
+  return RG_OK;
+}
 }  // namespace rgd

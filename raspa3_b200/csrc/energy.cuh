@@ -168,6 +168,8 @@ __device__ __forceinline__ double interpolate(const Grid& g, double px, double p
 // Internal accessors between translation units: the device data of a system and of an Ewald state.
 rg_status systemExport(rg_system* s, FF* ff, Box* box, const double** type_grids /*[64]*/, const double** ewald_grid,
                        int* n_types, int gdims[3], double gic[3][3], rg_ctx** ctx);
+// the framework atoms of a system (device rg_atom array, count)
+rg_status systemFramework(rg_system* s, const rg_atom** fw, int* n_fw);
 rg_status proposalExport(rg_proposal* p, const double** cdf, const double** density, int* G, double* eps);
 rg_status ewaldExport(rg_ewald* e, const char4** kvec, const double** temp, const double2** s_rigid, int64_t* nk,
                       int kmax[3], double* alpha, double* single_ion_sum);

@@ -90,6 +90,11 @@ struct Params
   unsigned long long seed;
   const float4* ljf;  // [kMaxTypes^2]: 4 eps, sigma^2, shift, lj flag
   const float* qtype; // charge per type (the pseudo-atom charge)
+  // framework atoms, for trial atoms whose type has no VDW grid (explicit pairs; n_fw = 0 when every type has one)
+  const int4* fwx;    // [n_fw] fixed point, .w = type
+  const float* fwq;   // [n_fw] charges
+  int n_fw;
+  float rc2_fw;
   // state
   double4* pos;    // [capacity * na] Cartesian
   int4* fx;        // [capacity * na] fixed point, .w = type | molecule << 8
@@ -227,11 +232,13 @@ __device__ bool gridBarrier(const Params& p, Shared& sh)
   return !sh.fail;
 }
 
-// framework energy of one trial atom from the grids (FP64); overlap flag if the VDW part exceeds the criterion
+// framework energy of one trial atom from the grids (FP64); overlap flag if the VDW part exceeds the criterion. The
+// grid branch of interactions_framework_molecule.cpp: only an atom whose type has a VDW grid takes it (the unit-charge
+// Ewald grid then gives its charge term); any other atom sees the framework atoms explicitly (phase()).
 __device__ double gridEnergy(const Params& p, int type, double q, double3 r, const double* vdw, bool* ovl)
 {
+  if (!vdw) return 0.0;
   double e = 0.0;
-  if (vdw)
   {
     rgd::Grid g = p.grid;
     g.data = vdw;
@@ -305,6 +312,46 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
           const float r = rr * invr;
           const float ex = expf(-p.alpha * p.alpha * rr);
           acc += static_cast<double>(p.coul * qq * rgd::erfcFromExp(p.alpha * r, ex) * invr);
+        }
+      }
+    }
+    // trial atom without a VDW grid: explicit pairs with this CTA's slice of the framework atoms
+    if (p.n_fw > 0 && atomGrid[b] == nullptr)
+    {
+      const int fchunk = (p.n_fw + G - 1) / G, fa = cta * fchunk, fb = min(p.n_fw, fa + fchunk);
+      for (int i = fa + st; i < fb; i += streams)
+      {
+        const int4 P = __ldg(p.fwx + i);
+        const int pt = P.w;
+        const float f0 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.x) - static_cast<uint32_t>(P.x))) * kFix;
+        const float f1 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.y) - static_cast<uint32_t>(P.y))) * kFix;
+        const float f2 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.z) - static_cast<uint32_t>(P.z))) * kFix;
+        const float rx = fmaf(p.hf[0][0], f0, fmaf(p.hf[1][0], f1, p.hf[2][0] * f2));
+        const float ry = fmaf(p.hf[0][1], f0, fmaf(p.hf[1][1], f1, p.hf[2][1] * f2));
+        const float rz = fmaf(p.hf[0][2], f0, fmaf(p.hf[1][2], f1, p.hf[2][2] * f2));
+        const float rr = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+        if (rr < p.rc2_fw)
+        {
+          const float4 q = sh.tab[bt * kMaxTypes + pt];
+          if (q.w != 0.0f)
+          {
+            const float t = q.y * rgd::rcpRn(rr);
+            const float t3 = t * t * t;
+            const float e = q.x * (t3 * (t3 - 1.0f)) - q.z;
+            if (e > p.overlap_f) ov = true;
+            acc += static_cast<double>(e);
+          }
+        }
+        if (p.use_charge && rr < p.rc2_c)
+        {
+          const float qq = qb * __ldg(p.fwq + i);
+          if (qq != 0.0f)
+          {
+            const float invr = rgd::rsqrtRn(rr);
+            const float r = rr * invr;
+            const float ex = expf(-p.alpha * p.alpha * rr);
+            acc += static_cast<double>(p.coul * qq * rgd::erfcFromExp(p.alpha * r, ex) * invr);
+          }
         }
       }
     }
@@ -1193,6 +1240,7 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   const double rcv_mol = params->cutoff_molecule_vdw, rcc = params->cutoff_coulomb;
   p.rc2_mm = static_cast<float>(rcv_mol * rcv_mol);
   p.rc2_c = static_cast<float>(rcc * rcc);
+  p.rc2_fw = static_cast<float>(params->cutoff_framework_vdw * params->cutoff_framework_vdw);
   p.alpha = static_cast<float>(ff.alpha);
   p.coul = static_cast<float>(ff.coul);
   // components
@@ -1237,6 +1285,53 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
       }
     cc.self_excl = self + excl;
   }
+  // framework atoms in fixed point, needed only if some component atom type has no VDW grid
+  bool gridless = false;
+  for (int c = 0; c < n_components; ++c)
+    for (int i = 0; i < na; ++i) gridless |= p.comp[c].vdw_grid[i] == nullptr;
+  std::vector<int4> hfw;
+  std::vector<float> hfq;
+  {
+    const rg_atom* dfw = nullptr;
+    int nfw = 0;
+    st = rgd::systemFramework(system, &dfw, &nfw);
+    if (st)
+    {
+      delete x;
+      return st;
+    }
+    if (gridless && nfw > 0)
+    {
+      std::vector<rg_atom> fw(nfw);
+      const cudaError_t e = cudaMemcpy(fw.data(), dfw, sizeof(rg_atom) * nfw, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess)
+      {
+        delete x;
+        return rg::cudaFail(ctx, e, "rg_mixture_create: framework atoms");
+      }
+      hfw.resize(nfw);
+      hfq.resize(nfw);
+      for (int i = 0; i < nfw; ++i)
+      {
+        if (fw[i].type >= nt)
+        {
+          delete x;
+          return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture: framework atom type");
+        }
+        const double r[3] = {fw[i].x, fw[i].y, fw[i].z};
+        int f[3];
+        for (int a = 0; a < 3; ++a)
+        {
+          const double sa = box.ic[0][a] * r[0] + box.ic[1][a] * r[1] + box.ic[2][a] * r[2];
+          const double v = sa - std::floor(sa);
+          f[a] = static_cast<int>(static_cast<uint32_t>(static_cast<unsigned long long>(v * 4294967296.0)));
+        }
+        hfw[i] = make_int4(f[0], f[1], f[2], fw[i].type);
+        hfq[i] = static_cast<float>(fw[i].charge);
+      }
+    }
+  }
+  p.n_fw = static_cast<int>(hfw.size());
   // Ewald tables
   if (p.use_charge)
   {
@@ -1293,6 +1388,12 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   alloc(reinterpret_cast<void**>(&p.sk), sizeof(double2) * std::max(1, p.nk));
   alloc(reinterpret_cast<void**>(&p.part), sizeof(double) * kRow * 2 * x->blocks);
   alloc(reinterpret_cast<void**>(&p.bar), sizeof(unsigned) * 4);
+  int4* dfwx = nullptr;
+  float* dfwq = nullptr;
+  alloc(reinterpret_cast<void**>(&dfwx), sizeof(int4) * hfw.size());
+  alloc(reinterpret_cast<void**>(&dfwq), sizeof(float) * hfq.size());
+  p.fwx = dfwx;
+  p.fwq = dfwq;
   p.ljf = dljf;
   p.qtype = dq;
   // host copies of the starting configuration
@@ -1313,9 +1414,22 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
     hslot[m] = counts[c];
     hlist[static_cast<size_t>(c) * cap + counts[c]] = m;
     counts[c] += 1;
+    // every molecule is stored whole (atom i = atom 0 + the minimum image of their separation), as the reference keeps
+    // molecules: a molecule split by per-atom wrapping would have a wrong centre of mass in a rotation
+    const double* r0 = xyz + 3 * (static_cast<size_t>(m) * na);
     for (int i = 0; i < na; ++i)
     {
-      const double* r = xyz + 3 * (static_cast<size_t>(m) * na + i);
+      const double* ri = xyz + 3 * (static_cast<size_t>(m) * na + i);
+      double dr[3] = {ri[0] - r0[0], ri[1] - r0[1], ri[2] - r0[2]};
+      double sd[3];
+      for (int a = 0; a < 3; ++a)
+      {
+        sd[a] = box.ic[0][a] * dr[0] + box.ic[1][a] * dr[1] + box.ic[2][a] * dr[2];
+        sd[a] -= std::nearbyint(sd[a]);
+      }
+      const double r[3] = {r0[0] + box.c[0][0] * sd[0] + box.c[1][0] * sd[1] + box.c[2][0] * sd[2],
+                           r0[1] + box.c[0][1] * sd[0] + box.c[1][1] * sd[1] + box.c[2][1] * sd[2],
+                           r0[2] + box.c[0][2] * sd[0] + box.c[1][2] * sd[1] + box.c[2][2] * sd[2]};
       hpos[m * na + i] = make_double4(r[0], r[1], r[2], 0.0);
       double s[3];
       for (int a = 0; a < 3; ++a) s[a] = box.ic[0][a] * r[0] + box.ic[1][a] * r[1] + box.ic[2][a] * r[2];
@@ -1334,6 +1448,10 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   cudaStream_t sm = ctx->stream;
   if (err == cudaSuccess) err = cudaMemcpyAsync(dljf, ljf.data(), sizeof(float4) * ljf.size(), cudaMemcpyHostToDevice, sm);
   if (err == cudaSuccess) err = cudaMemcpyAsync(dq, qtype.data(), sizeof(float) * qtype.size(), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess && !hfw.empty())
+    err = cudaMemcpyAsync(dfwx, hfw.data(), sizeof(int4) * hfw.size(), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess && !hfq.empty())
+    err = cudaMemcpyAsync(dfwq, hfq.data(), sizeof(float) * hfq.size(), cudaMemcpyHostToDevice, sm);
   if (err == cudaSuccess)
     err = cudaMemcpyAsync(p.pos, hpos.data(), sizeof(double4) * hpos.size(), cudaMemcpyHostToDevice, sm);
   if (err == cudaSuccess) err = cudaMemcpyAsync(p.fx, hfx.data(), sizeof(int4) * hfx.size(), cudaMemcpyHostToDevice, sm);

@@ -4,7 +4,8 @@ The framework is the configuration-1/2 generator (96 T + 192 O per cell, T +2.05
 the configuration-1/2 lengths (30.0 x 29.85 x 20.1 A), replicated 4 x 4 x 4: 18,432 atoms, holding 2,000 rigid CO2
 and 2,000 rigid 3-site N2 (N-N 1.10 A, N 36 K / 3.31 A / -0.482 e, massless centre +0.964 e); Ewald alpha = 0.265 per
 Angstrom with kmax 12 (integer sphere: 3,796 k-vectors). Framework energies come from the unit-cell grids (C_co2, O_co2,
-N_n2 Lennard-Jones and the unit-charge real-space Ewald grid, 0.15 A spacing). The larger cell is what makes room for
+N_n2 and N_com Lennard-Jones -- every adsorbate type has one, N_com's being zero -- and the unit-charge real-space Ewald
+grid, 0.15 A spacing). The larger cell is what makes room for
 4,000 molecules: in the 20.0 x 19.9 x 13.4 A cell with randomly placed atoms only 0.7 % of the volume is farther than
 2.6 A from an atom, too little for 62.5 molecules per cell; at 1.5 times the lengths it is 44 %.
 """
@@ -21,8 +22,8 @@ from .synthetic import random_rotation, replicate, synthetic_forcefield, synthet
 def random_mixture(cell, framework, components, counts, seed: int = 5, min_fw: float = 2.6, min_mol: float = 2.8,
                    max_tries: int = 2_000_000):
     """Random non-overlapping rigid molecules: counts[c] of components[c] with no atom closer than min_fw to a
-    framework atom or min_mol to another molecule's atom (periodic orthorhombic box). Returns (xyz[n, na, 3],
-    comp[n])."""
+    framework atom or min_mol to another molecule's atom (periodic orthorhombic box). Every molecule is whole: its
+    atoms are the rigid offsets about a point in the box, not wrapped one by one. Returns (xyz[n, na, 3], comp[n])."""
     from scipy.spatial import cKDTree
 
     rng = np.random.default_rng(seed)
@@ -56,14 +57,16 @@ def random_mixture(cell, framework, components, counts, seed: int = 5, min_fw: f
             tries += 1
             if tries > max_tries:
                 raise RuntimeError("random_mixture: could not place the molecules")
-            x = (comp.offsets @ random_rotation(rng).T + rng.random(3) * L) % L
-            if fw_tree.query(x, k=1)[0].min() < min_fw:
+            # the molecule stays whole (atoms may lie outside the box); distances use the wrapped copy
+            x = comp.offsets @ random_rotation(rng).T + rng.random(3) * L
+            xw = x % L
+            if fw_tree.query(xw, k=1)[0].min() < min_fw:
                 continue
-            if any(near(a) for a in x):
+            if any(near(a) for a in xw):
                 continue
             break
         dims = np.maximum(1, (L // grid_size).astype(int))
-        for a in x:
+        for a in xw:
             k = tuple(((a // grid_size).astype(int)) % dims)
             cells.setdefault(k, []).append(a)
         placed.append(x)
@@ -110,24 +113,26 @@ def config5(ctx, torch, reps=(4, 4, 4), counts=(2000, 2000), kmax: int = 12, see
     scell, sfw = replicate(ucell, ufw, reps)
     dims = dims or grid_points_for_spacing(ucell, spacing)
     system = native.System(ctx, ff, scell, sfw)
-    bufs = []
-    for name in ("C_co2", "O_co2", "N_n2"):
+    bufs, grid_types = [], []
+    for name in ("C_co2", "O_co2", "N_n2", "N_com"):
         idx = ff.index(name)
         buf = torch.empty(8 * dims[0] * dims[1] * dims[2], dtype=torch.float64, device="cuda")
         ctx.grid_build(0, ff, ucell, ufw, idx, 12.0, dims, native.PRECISION_FP32C, out_device=buf.data_ptr(),
                        host=False)
         system.set_grid(idx, ucell, dims, buf.data_ptr(), on_device=True)
         bufs.append(buf)
+        grid_types.append(idx)
     buf = torch.empty(8 * dims[0] * dims[1] * dims[2], dtype=torch.float64, device="cuda")
     ctx.grid_build(1, ff, ucell, ufw, 0, 12.0, dims, native.PRECISION_FP32C, out_device=buf.data_ptr(), host=False)
     system.set_grid(ff.n_types, ucell, dims, buf.data_ptr(), on_device=True)
     bufs.append(buf)
+    grid_types.append(ff.n_types)
     ewald = native.Ewald(ctx, ff, scell)
     ewald.set_framework(sfw)
     components = [co2_component(), n2_component()]
     xyz, comp = random_mixture(scell, sfw, components, counts, seed=seed)
     return {"ff": ff, "unit_cell": ucell, "unit_framework": ufw, "cell": scell, "framework": sfw, "grids": bufs,
-            "system": system, "ewald": ewald, "components": components, "xyz": xyz, "comp": comp, "dims": dims}
+            "grid_types": grid_types, "system": system, "ewald": ewald, "components": components, "xyz": xyz, "comp": comp, "dims": dims}
 
 
 def kelvin(e: float) -> float:

@@ -77,7 +77,7 @@ class GcmcChainResult(ctypes.Structure):
 class MixtureParams(ctypes.Structure):
     _fields_ = [("beta", ctypes.c_double), ("fugacity", ctypes.c_double * 4), ("w_ig", ctypes.c_double * 4),
                 ("cutoff_molecule_vdw", ctypes.c_double), ("cutoff_coulomb", ctypes.c_double),
-                ("max_translation", ctypes.c_double), ("max_rotation", ctypes.c_double),
+                ("cutoff_framework_vdw", ctypes.c_double), ("max_translation", ctypes.c_double), ("max_rotation", ctypes.c_double),
                 ("p_translation", ctypes.c_double), ("p_rotation", ctypes.c_double), ("p_swap", ctypes.c_double),
                 ("p_identity", ctypes.c_double), ("n_first_bead_trials", ctypes.c_int32),
                 ("n_orientation_trials", ctypes.c_int32), ("max_molecules", ctypes.c_int32),
@@ -753,6 +753,7 @@ class Mixture:
             p.fugacity[i] = f
             p.w_ig[i] = 1.0 if w_ig is None else w_ig[i]
         p.cutoff_molecule_vdw, p.cutoff_coulomb = ff.cutoff_molecule_vdw, ff.cutoff_coulomb
+        p.cutoff_framework_vdw = ff.cutoff_framework_vdw
         p.max_translation, p.max_rotation = max_translation, max_rotation
         p.p_translation, p.p_rotation, p.p_swap, p.p_identity = probabilities
         p.n_first_bead_trials, p.n_orientation_trials = n_first, n_orient

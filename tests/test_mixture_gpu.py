@@ -1,9 +1,10 @@
 """One large mixture system on the whole GPU (rg_mixture_*) against exact results and the FP64 CPU oracle.
 
 * Ideal-gas mixture with translation, rotation, CBMC swap and identity change: <N_c> = beta f_c V per component.
-* CO2 + N2 in the synthetic framework (framework charges off, the adsorbates charged, Ewald on): the running energy and
-  the structure factors after thousands of moves equal an FP64 recomputation of the final configuration, and the
-  loading of each component agrees with independent oracle runs on the same grids.
+* CO2 + N2 in the synthetic framework (the adsorbates charged, Ewald on; framework charges off and on): the running
+  energy and the structure factors after thousands of moves equal an FP64 recomputation of the final configuration,
+  and the loading of each component agrees with independent oracle runs on the same grids. N2's massless charge site
+  has no grid, so it sees the framework atoms explicitly (the reference's non-grid branch), on both sides.
 * The large configuration (4 x 4 x 4 framework cells, 2,000 CO2 + 2,000 N2, kmax 12) runs without a barrier
   timeout and without drift.
 """
@@ -22,6 +23,8 @@ from raspa3_b200.synthetic import replicate, synthetic_forcefield, synthetic_fra
 
 pytestmark = pytest.mark.gpu
 BETA = beta_of(300.0)
+N_RUNS = 8  # independent runs per side in the loading comparison
+RECORDED = 50000  # recorded moves per run after 3000 discarded equilibration moves
 
 
 @pytest.fixture(scope="module")
@@ -63,10 +66,11 @@ def test_ideal_gas_mixture_with_identity_change(ctx):
         assert abs(means[:, c].mean() - t) < 4 * se + 0.03 * t, (c, means[:, c].mean(), t, se)
 
 
-def framework_system(ctx, torch, kmax=6):
+def framework_system(ctx, torch, kmax=6, framework_charges=False):
     ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=kmax)
-    for pa in ff.pseudo_atoms[:2]:
-        pa.charge = 0.0
+    if not framework_charges:
+        for pa in ff.pseudo_atoms[:2]:
+            pa.charge = 0.0
     ucell, ufw = synthetic_framework(ff, seed=42)
     scell, sfw = replicate(ucell, ufw, (2, 2, 3))
     dims = (34, 34, 23)
@@ -79,23 +83,28 @@ def framework_system(ctx, torch, kmax=6):
                        out_device=buf.data_ptr(), host=False)
         sysg.set_grid(idx, ucell, dims, buf.data_ptr(), on_device=True)
         bufs.append(buf)
+    # the builds ran on the context's own stream; torch's copies below run on torch's stream
+    ctx.synchronize()
+    for idx, buf in zip([ff.index("C_co2"), ff.index("O_co2"), ff.index("N_n2"), ff.n_types], bufs):
         host[idx] = buf.cpu().numpy()
     ew = native.Ewald(ctx, ff, scell)
     ew.set_framework(sfw)
     return ff, ucell, ufw, scell, sfw, dims, sysg, ew, bufs, host
 
 
-def test_framework_mixture_drift_and_loading(ctx, torch, oracle):
-    ff, ucell, ufw, scell, sfw, dims, sysg, ew, bufs, host = framework_system(ctx, torch)
+@pytest.mark.parametrize("framework_charges", [False, True])
+def test_framework_mixture_drift_and_loading(ctx, torch, oracle, framework_charges):
+    ff, ucell, ufw, scell, sfw, dims, sysg, ew, bufs, host = framework_system(ctx, torch,
+                                                                               framework_charges=framework_charges)
     comps = [co2_component(), n2_component()]
     fug = [fugacity_of(1e6), fugacity_of(1e6)]
     runs = []
-    for seed in range(4):
+    for seed in range(N_RUNS):
         mx = native.Mixture(sysg, ew, comps, BETA, fug, np.zeros((0, 3, 3)), np.zeros(0, dtype=np.int32),
                             max_molecules=256, seed=seed + 11)
         mx.set_state(0.0, ew.structure_factors(2))
         mx.run(3000, record=False)
-        mx.run(20000, record=True)
+        mx.run(RECORDED, record=True)
         r = mx.results()
         assert r["status"] == 0
         runs.append([s / r["samples"] for s in r["sum_n"][:2]])
@@ -111,19 +120,47 @@ def test_framework_mixture_drift_and_loading(ctx, torch, oracle):
     gpu = np.array(runs)
     s_fw = ew.structure_factors(2)
 
+    kw = dict(grids=host, grid_dims=dims, grid_cell=ucell, s_framework=s_fw, max_molecules=256, framework=sfw)
+
     def one(seed):
-        r, _, _, _ = oracle.mixture_run(ff, scell, comps, BETA, fug, np.zeros((0, 3, 3)), np.zeros(0, dtype=np.int32),
-                                        23000, seed=seed, grids=host, grid_dims=dims, grid_cell=ucell,
-                                        s_framework=s_fw, max_molecules=256)
+        # the same 3000 equilibration moves, discarded, then RECORDED from the equilibrated configuration
+        _, xyz0, comp0, _ = oracle.mixture_run(ff, scell, comps, BETA, fug, np.zeros((0, 3, 3)),
+                                               np.zeros(0, dtype=np.int32), 3000, seed=seed, **kw)
+        r, _, _, _ = oracle.mixture_run(ff, scell, comps, BETA, fug, xyz0, comp0, RECORDED, seed=seed + 100, **kw)
         return r
 
-    with ThreadPoolExecutor(4) as pool:
-        ores = list(pool.map(one, range(4)))
-    # the oracle records every move including the first 3000 (equilibration is short next to the run at this loading)
+    with ThreadPoolExecutor(N_RUNS) as pool:
+        ores = list(pool.map(one, range(N_RUNS)))
     cpu = np.array([[s / r["samples"] for s in r["sum_n"][:2]] for r in ores])
     for c in range(2):
-        se = math.hypot(gpu[:, c].std(ddof=1) / 2, cpu[:, c].std(ddof=1) / 2)
+        se = math.hypot(gpu[:, c].std(ddof=1), cpu[:, c].std(ddof=1)) / math.sqrt(N_RUNS)
         assert abs(gpu[:, c].mean() - cpu[:, c].mean()) < 4 * se + 0.05 * cpu[:, c].mean(), (c, gpu, cpu)
+
+
+def test_split_molecules_are_kept_whole(ctx, torch):
+    """Molecules handed in wrapped atom by atom (split across the box faces): rg_mixture_create makes them whole, so
+    rotations keep the rigid geometry and the running energy equals the recomputed one."""
+    ff, ucell, ufw, scell, sfw, dims, sysg, ew, bufs, host = framework_system(ctx, torch, framework_charges=True)
+    comps = [co2_component(), n2_component()]
+    xyz, comp = random_mixture(scell, sfw, comps, (20, 20), seed=3)
+    split = xyz % np.diag(np.asarray(scell))
+    assert np.any(np.abs(split - xyz) > 1.0)
+    e0 = total_energy(sysg, ew, ff, comps, xyz, comp)
+    sk0 = ew.structure_factors(0)
+    mx = native.Mixture(sysg, ew, comps, BETA, [fugacity_of(1e5), fugacity_of(1e5)], split, comp, max_molecules=256,
+                        seed=5, probabilities=(0.2, 1.0, 0.0, 0.0))
+    mx.set_state(e0, sk0)
+    mx.run(3000, record=True)
+    r = mx.results()
+    assert r["status"] == 0 and r["accepted"][1] > 100
+    out, comp_out = mx.positions()
+    for m, c in enumerate(comp_out):
+        d_out = np.linalg.norm(out[m][:, None] - out[m][None], axis=-1)
+        d_ref = np.linalg.norm(comps[c].offsets[:, None] - comps[c].offsets[None], axis=-1)
+        assert np.allclose(d_out, d_ref, atol=1e-9)
+    e = total_energy(sysg, ew, ff, comps, out, comp_out)
+    assert abs(r["energy"] - e) < 1e-6 * max(1.0, abs(e)) + 1e-3, (r["energy"], e)
+    mx.close()
 
 
 def test_large_mixture_runs_without_drift(ctx, torch):

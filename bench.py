@@ -292,7 +292,7 @@ MIXTURE_MOVES = 20000
 
 def run_mixture(args, ctx, world, rank, dist, torch):
     """The large mixture (configuration 5): 2,000 CO2 + 2,000 N2 in the 18,432-atom framework, Ewald kmax 12
-    (3,796 k-vectors), translation : rotation : CBMC swap : identity change = 1 : 1 : 1 : 1 with the learned first-bead
+    (8,124 k-vectors), translation : rotation : CBMC swap : identity change = 1 : 1 : 1 : 1 with the learned first-bead
     proposal of each component, one system advanced by all SMs. Metric: move attempts per second."""
     from raspa3_b200 import native
     from raspa3_b200.gcmc import beta_of, fugacity_of

@@ -111,57 +111,73 @@ __device__ __forceinline__ double fract1(double x)
 // The reference maps the 64 corner values (f, fx, fy, fz, fxy, fxz, fyz, fxyz at 8 corners) through the Lekien-Marsden
 // 64x64 matrix to monomial coefficients and sums the polynomial; that interpolant is the tensor product of 1D cubic
 // Hermite bases, evaluated here directly as 64 products (identical up to rounding).
-__device__ __forceinline__ double interpolate(const Grid& g, double px, double py, double pz)
+// The grid cell of a position and the 1D cubic Hermite bases of its local coordinates.
+struct GridCell
 {
+  int i0[3];
+  double h[3][2][2];  // h[d][corner][order]: corner 0/1, order 0 = value basis, 1 = derivative basis
+};
+
+__device__ __forceinline__ GridCell gridCell(const Grid& g, double px, double py, double pz)
+{
+  GridCell cl;
   double s[3];
   s[0] = fract1(g.ic[0][0] * px + g.ic[1][0] * py + g.ic[2][0] * pz);
   s[1] = fract1(g.ic[0][1] * px + g.ic[1][1] * py + g.ic[2][1] * pz);
   s[2] = fract1(g.ic[0][2] * px + g.ic[1][2] * py + g.ic[2][2] * pz);
   const int nc[3] = {g.nx - 1, g.ny - 1, g.nz - 1};
-  int i0[3];
   double t[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d)
   {
     long long c = static_cast<long long>(s[d] * static_cast<double>(nc[d]));
-    i0[d] = static_cast<int>(c < nc[d] - 1 ? c : nc[d] - 1);
-    t[d] = s[d] * static_cast<double>(nc[d]) - static_cast<double>(i0[d]);
+    cl.i0[d] = static_cast<int>(c < nc[d] - 1 ? c : nc[d] - 1);
+    t[d] = s[d] * static_cast<double>(nc[d]) - static_cast<double>(cl.i0[d]);
   }
-  // h[d][corner][order]: corner 0/1, order 0 = value basis, 1 = derivative basis
-  double h[3][2][2];
 #pragma unroll
   for (int d = 0; d < 3; ++d)
   {
     const double x = t[d], x2 = x * x, x3 = x2 * x;
-    h[d][0][0] = 2.0 * x3 - 3.0 * x2 + 1.0;
-    h[d][1][0] = -2.0 * x3 + 3.0 * x2;
-    h[d][0][1] = x3 - 2.0 * x2 + x;
-    h[d][1][1] = x3 - x2;
+    cl.h[d][0][0] = 2.0 * x3 - 3.0 * x2 + 1.0;
+    cl.h[d][1][0] = -2.0 * x3 + 3.0 * x2;
+    cl.h[d][0][1] = x3 - 2.0 * x2 + x;
+    cl.h[d][1][1] = x3 - x2;
   }
-  // derivative orders (x, y, z) of the 8 stored channels
+  return cl;
+}
+
+// The share of one corner (0..7: bit 0 = x, 1 = y, 2 = z) of the cell: its 8 stored channels (f, fx, fy, fz, fxy,
+// fxz, fyz, fxyz) times their basis products.
+__device__ __forceinline__ double interpolateCorner(const Grid& g, const GridCell& cl, int corner)
+{
   const int ox[8] = {0, 1, 0, 0, 1, 1, 0, 1};
   const int oy[8] = {0, 0, 1, 0, 1, 0, 1, 1};
   const int oz[8] = {0, 0, 0, 1, 0, 1, 1, 1};
+  const int cx = corner & 1, cy = (corner >> 1) & 1, cz = (corner >> 2) & 1;
+  const double* p = g.data + 8 * (static_cast<long long>(cl.i0[0] + cx) +
+                                  static_cast<long long>(g.nx) * (static_cast<long long>(cl.i0[1] + cy) +
+                                                                 static_cast<long long>(g.ny) * (cl.i0[2] + cz)));
+  const double2* p2 = reinterpret_cast<const double2*>(p);
+  double v[8];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+  {
+    double2 u = __ldg(p2 + q);
+    v[2 * q] = u.x;
+    v[2 * q + 1] = u.y;
+  }
   double value = 0.0;
 #pragma unroll
-  for (int corner = 0; corner < 8; ++corner)
-  {
-    const int cx = corner & 1, cy = (corner >> 1) & 1, cz = (corner >> 2) & 1;
-    const double* p = g.data + 8 * (static_cast<long long>(i0[0] + cx) +
-                                    static_cast<long long>(g.nx) * (static_cast<long long>(i0[1] + cy) +
-                                                                   static_cast<long long>(g.ny) * (i0[2] + cz)));
-    const double2* p2 = reinterpret_cast<const double2*>(p);
-    double v[8];
+  for (int l = 0; l < 8; ++l) value += v[l] * cl.h[0][cx][ox[l]] * cl.h[1][cy][oy[l]] * cl.h[2][cz][oz[l]];
+  return value;
+}
+
+__device__ __forceinline__ double interpolate(const Grid& g, double px, double py, double pz)
+{
+  const GridCell cl = gridCell(g, px, py, pz);
+  double value = 0.0;
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
-    {
-      double2 u = __ldg(p2 + q);
-      v[2 * q] = u.x;
-      v[2 * q + 1] = u.y;
-    }
-#pragma unroll
-    for (int l = 0; l < 8; ++l) value += v[l] * h[0][cx][ox[l]] * h[1][cy][oy[l]] * h[2][cz][oz[l]];
-  }
+  for (int corner = 0; corner < 8; ++corner) value += interpolateCorner(g, cl, corner);
   return value;
 }
 

@@ -46,7 +46,8 @@ constexpr int kMaxCand = kMaxTrials;   // Ewald candidates of one phase
 constexpr int kMaxCandAtoms = 2 * kMaxAtoms;
 constexpr int kMaxKPerCta = 64;
 constexpr int kMaxTypes = 16;
-constexpr int kRow = kMaxItems + kMaxCand + 4;  // doubles per CTA row of partial sums (last 4: overlap bits)
+constexpr int kRow = kMaxItems + kMaxCand + 4;  // columns of partial sums per CTA (last 4: overlap-bit words)
+constexpr int kMaxBlocks = 256;                 // CTAs of the cooperative launch (lanes x 8 in the column sums)
 constexpr long long kSpinLimit = 1ll << 22;
 constexpr int kStats = 24;
 constexpr double kPi = 3.141592653589793238462643383279502884;
@@ -106,8 +107,10 @@ struct Params
   long long* move_base;
   double* stats;   // attempted[5], accepted[5], sum_n[4], sum_energy, samples
   double2* sk;     // [nk]
-  double* part;    // [gridDim][kRow]
-  unsigned* bar;   // count, generation, error
+  int km[3];       // kmax per axis: the phasor tables hold exp(2 pi i j s) for j = 0..km[d]
+  int tabK;        // table stride: max(km) + 1
+  double* part;    // [2][kRow][gridDim]: partial sums, column-major, two buffers alternating by phase
+  unsigned long long* bar;  // [0] barrier arrivals in this launch (zeroed before each launch), [1] error flag
   int record;
 };
 
@@ -136,6 +139,8 @@ struct Shared
   int cn[kMaxCand];
   int ncand;
   double2 dk[kMaxCand][kMaxKPerCta];  // structure-factor change of each candidate over this CTA's k-range
+  double ek[kMaxCand][kMaxKPerCta];   // its energy change per k
+  double fwE[kMaxItems];              // framework (grid) energy of the trial atoms this CTA owns
   double red[kThreads];
   unsigned ovl_bits[4];
   double tot[kMaxItems + kMaxCand];  // totals over the grid
@@ -195,64 +200,58 @@ __device__ void rotationFromUniforms(double u1, double u2, double u3, double R[3
   R[2][2] = 1 - 2 * (x * x + y * y);
 }
 
-// Grid barrier over all CTAs of the cooperative launch. Spin-waits are bounded: on timeout the error flag is raised
-// and false returned; every CTA then leaves the kernel. Returns false as well once any CTA has raised the flag.
+__device__ __forceinline__ unsigned long long loadAcquire(const unsigned long long* a)
+{
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(a) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long loadRelaxed(const unsigned long long* a)
+{
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(a) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long addRelease(unsigned long long* a, unsigned long long x)
+{
+  unsigned long long old;
+  asm volatile("atom.add.release.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(a), "l"(x) : "memory");
+  return old;
+}
+
+// Grid barrier over all CTAs of the cooperative launch: a monotonic arrival counter (zeroed before each launch); the
+// n-th barrier of the launch is passed once the counter reaches n x gridDim. One release add per CTA, then acquire
+// polls: no reset, no second round trip. Spin-waits are bounded: on timeout the error flag is raised and false
+// returned, and every CTA leaves the kernel; a CTA waiting on a barrier that a failed CTA will never reach sees the
+// flag (polled every 64 spins) and leaves too.
 __device__ bool gridBarrier(const Params& p, Shared& sh)
 {
   __syncthreads();
   if (threadIdx.x == 0)
   {
-    const unsigned g = static_cast<unsigned>(sh.gen);
-    __threadfence();
-    const unsigned arrived = atomicAdd(&p.bar[0], 1u);
-    if (arrived == gridDim.x - 1)
+    const unsigned long long target = static_cast<unsigned long long>(sh.gen + 1) * gridDim.x;
+    unsigned long long v = addRelease(&p.bar[0], 1ull) + 1ull;
+    long long spins = 0;
+    while (v < target)
     {
-      atomicExch(&p.bar[0], 0u);
-      __threadfence();
-      atomicExch(&p.bar[1], g + 1u);
-    }
-    else
-    {
-      long long spins = 0;
-      while (atomicAdd(&p.bar[1], 0u) == g)
+      if (++spins > kSpinLimit)
       {
-        if (++spins > kSpinLimit || atomicAdd(&p.bar[2], 0u) != 0u)
-        {
-          atomicExch(&p.bar[2], 1u);
-          break;
-        }
-        __nanosleep(64);
+        atomicExch(&p.bar[1], 1ull);
+        sh.fail = 1;
+        break;
       }
+      if ((spins & 63) == 0 && loadRelaxed(&p.bar[1]) != 0ull)
+      {
+        sh.fail = 1;
+        break;
+      }
+      __nanosleep(32);
+      v = loadAcquire(&p.bar[0]);
     }
-    __threadfence();
-    sh.gen = static_cast<int>(g + 1u);
-    sh.fail = atomicAdd(&p.bar[2], 0u) != 0u;
+    sh.gen += 1;
   }
   __syncthreads();
   return !sh.fail;
-}
-
-// framework energy of one trial atom from the grids (FP64); overlap flag if the VDW part exceeds the criterion. The
-// grid branch of interactions_framework_molecule.cpp: only an atom whose type has a VDW grid takes it (the unit-charge
-// Ewald grid then gives its charge term); any other atom sees the framework atoms explicitly (phase()).
-__device__ double gridEnergy(const Params& p, int type, double q, double3 r, const double* vdw, bool* ovl)
-{
-  if (!vdw) return 0.0;
-  double e = 0.0;
-  {
-    rgd::Grid g = p.grid;
-    g.data = vdw;
-    const double v = rgd::interpolate(g, r.x, r.y, r.z);
-    if (v > p.overlap) *ovl = true;
-    e += v;
-  }
-  if (p.use_charge && p.ewald_grid && q != 0.0)
-  {
-    rgd::Grid g = p.grid;
-    g.data = p.ewald_grid;
-    e += q * rgd::interpolate(g, r.x, r.y, r.z);
-  }
-  return e;
 }
 
 // One phase: energies of sh.nta trial atoms (framework + molecules other than `skip`) and the Ewald energy change of
@@ -264,8 +263,42 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int G = gridDim.x, cta = blockIdx.x;
   const int nta = sh.nta, ncand = sh.ncand;
-  if (tid < 4) sh.ovl_bits[tid] = 0u;
+  if (tid < 4)
+  {
+    sh.ovl_bits[tid] = 0u;
+    sh.ovl[tid] = 0u;
+  }
+  if (tid < nta) sh.fwE[tid] = 0.0;
   __syncthreads();
+  // 0. framework grids of the trial atoms this CTA owns (b = cta, cta + G, ..), by 16 lanes of the last warp: lane l
+  //    takes corner l & 7 of the VDW grid (l < 8) or of the unit-charge Ewald grid (l >= 8). Started first, so its
+  //    grid loads overlap the pair loop of the other warps. The grid branch of interactions_framework_molecule.cpp:
+  //    only an atom whose type has a VDW grid takes it (its charge term then comes from the Ewald grid); any other
+  //    atom sees the framework atoms explicitly (below).
+  if (warp == kWarps - 1 && lane < 16)
+    for (int b = cta; b < nta; b += G)
+    {
+      const double* vdw = atomGrid[b];
+      const double q = static_cast<double>(sh.qt[sh.tf[b].w & 0xff]);
+      const bool charged = p.use_charge && p.ewald_grid != nullptr && q != 0.0;
+      double v = 0.0;
+      if (vdw != nullptr && (lane < 8 || charged))
+      {
+        rgd::Grid g = p.grid;
+        g.data = lane < 8 ? vdw : p.ewald_grid;
+        const double3 r = sh.ta[b];
+        v = rgd::interpolateCorner(g, rgd::gridCell(g, r.x, r.y, r.z), lane & 7);
+      }
+      v += __shfl_xor_sync(0x0000ffffu, v, 1);
+      v += __shfl_xor_sync(0x0000ffffu, v, 2);
+      v += __shfl_xor_sync(0x0000ffffu, v, 4);
+      const double ew = __shfl_sync(0x0000ffffu, v, 8);
+      if (lane == 0)
+      {
+        sh.fwE[b] = v + q * ew;
+        if (v > p.overlap) atomicOr(&sh.ovl_bits[b >> 5], 1u << (b & 31));
+      }
+    }
   // 1. molecule-molecule pairs over this CTA's slice of sites
   const int ns = sh.n * p.na;
   const int chunk = (ns + G - 1) / G, s0 = cta * chunk, s1 = min(ns, s0 + chunk);
@@ -356,75 +389,110 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
       }
     }
   }
-  // framework part of trial atom b, by the CTA b mod G (thread b)
-  if (tid < nta && tid % G == cta)
-  {
-    const int bt = sh.tf[tid].w & 0xff;
-    acc += gridEnergy(p, bt, static_cast<double>(sh.qt[bt]), sh.ta[tid], atomGrid[tid], &ov);
-  }
   sh.red[tid] = acc;
   if (ov) atomicOr(&sh.ovl_bits[b >> 5], 1u << (b & 31));
   __syncthreads();
-  // two buffers of rows, alternating by phase: a CTA writes the next phase's row only after every CTA has passed
-  // this phase's barrier and read this phase's rows, which lie in the other buffer
+  // partial sums column-major ([column][CTA]), in two buffers alternating by phase: a CTA writes the next phase's
+  // partials only after every CTA has passed this phase's barrier and read this phase's, which lie in the other buffer
   const int buf = sh.phases & 1;
-  double* rows = p.part + static_cast<long long>(buf) * G * kRow;
-  double* row = rows + static_cast<long long>(cta) * kRow;
+  double* cols = p.part + static_cast<long long>(buf) * kRow * G;
   if (tid < nta)
   {
     double s = 0.0;
     for (int k = 0; k < streams; ++k) s += sh.red[tid + nta * k];
-    row[tid] = s;
+    cols[static_cast<long long>(tid) * G + cta] = s + sh.fwE[tid];
   }
-  if (tid < 4) reinterpret_cast<unsigned*>(row + kMaxItems + kMaxCand)[tid] = sh.ovl_bits[tid];
-  // 2. Ewald candidates over this CTA's k-range: one warp per candidate, lanes over the k-vectors
-  const int kchunk = (p.nk + G - 1) / G, k0 = cta * kchunk, k1 = min(p.nk, k0 + kchunk);
-  for (int c = warp; c < ncand; c += kWarps)
+  if (tid < 4) cols[static_cast<long long>(kMaxItems + kMaxCand + tid) * G + cta] = static_cast<double>(sh.ovl_bits[tid]);
+  // 2. Ewald candidates over this CTA's k-range. Per candidate atom (c, a) and axis d a phasor table
+  //    tab[j] = exp(2 pi i j s_d), j = 0..kmax_d (j < 0: the conjugate), built by powers of tab[1] (one thread per
+  //    table); then per (candidate, k) the structure-factor change sum_a q_a tab_x[kx] tab_y[ky] tab_z[kz] and its
+  //    energy change (ewald.cpp:1043-1244), one thread each; then per candidate the sum over k in a fixed order.
+  extern __shared__ double2 phasor[];
+  const int kchunk = (p.nk + G - 1) / G, k0 = cta * kchunk, nkr = max(0, min(p.nk, k0 + kchunk) - k0);
+  if (ncand > 0)
   {
-    double e = 0.0;
-    for (int kk = lane; kk < k1 - k0; kk += 32)
+    const rgd::Box& bx = p.box;
+    for (int task = tid; task < ncand * kMaxCandAtoms * 3; task += kThreads)
     {
-      const int k = k0 + kk;
+      const int c = task / (kMaxCandAtoms * 3), a = (task / 3) % kMaxCandAtoms, d = task % 3;
+      if (a >= sh.cn[c]) continue;
+      const double3 r = sh.cpos[c][a];
+      const double sd = bx.ic[0][d] * r.x + bx.ic[1][d] * r.y + bx.ic[2][d] * r.z;
+      double sn, cs;
+      sincospi(2.0 * sd, &sn, &cs);
+      double2* t = phasor + (static_cast<long long>(c * kMaxCandAtoms + a) * 3 + d) * p.tabK;
+      double2 w = make_double2(1.0, 0.0);
+      t[0] = w;
+      for (int j = 1; j <= p.km[d]; ++j)
+      {
+        w = make_double2(w.x * cs - w.y * sn, w.x * sn + w.y * cs);
+        t[j] = w;
+      }
+    }
+    __syncthreads();
+    for (int task = tid; task < ncand * nkr; task += kThreads)
+    {
+      const int c = task / nkr, kk = task - c * nkr, k = k0 + kk;
       const char4 kv = p.kvec[k];
       double2 d = make_double2(0.0, 0.0);
       for (int a = 0; a < sh.cn[c]; ++a)
       {
-        const double3 r = sh.cpos[c][a];
-        const rgd::Box& bx = p.box;
-        const double sx = bx.ic[0][0] * r.x + bx.ic[1][0] * r.y + bx.ic[2][0] * r.z;
-        const double sy = bx.ic[0][1] * r.x + bx.ic[1][1] * r.y + bx.ic[2][1] * r.z;
-        const double sz = bx.ic[0][2] * r.x + bx.ic[1][2] * r.y + bx.ic[2][2] * r.z;
-        double sn, cs;
-        sincospi(2.0 * (kv.x * sx + kv.y * sy + kv.z * sz), &sn, &cs);
-        d.x += sh.cq[c][a] * cs;
-        d.y += sh.cq[c][a] * sn;
+        const double2* t = phasor + static_cast<long long>(c * kMaxCandAtoms + a) * 3 * p.tabK;
+        double2 ex = t[abs(kv.x)], ey = t[p.tabK + abs(kv.y)], ez = t[2 * p.tabK + abs(kv.z)];
+        if (kv.x < 0) ex.y = -ex.y;
+        if (kv.y < 0) ey.y = -ey.y;
+        if (kv.z < 0) ez.y = -ez.y;
+        const double2 exy = make_double2(ex.x * ey.x - ex.y * ey.y, ex.x * ey.y + ex.y * ey.x);
+        const double q = sh.cq[c][a];
+        d.x += q * (exy.x * ez.x - exy.y * ez.y);
+        d.y += q * (exy.x * ez.y + exy.y * ez.x);
       }
-      const double2 s = p.sk[k];
-      e += p.temp[k] * (2.0 * (s.x * d.x + s.y * d.y) + (d.x * d.x + d.y * d.y));
+      const double2 sk = p.sk[k];
+      sh.ek[c][kk] = p.temp[k] * (2.0 * (sk.x * d.x + sk.y * d.y) + (d.x * d.x + d.y * d.y));
       sh.dk[c][kk] = d;
     }
+    __syncthreads();
+    for (int c = warp; c < ncand; c += kWarps)
+    {
+      double e = 0.0;
+      for (int kk = lane; kk < nkr; kk += 32) e += sh.ek[c][kk];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
-    if (lane == 0) row[kMaxItems + c] = e;
+      for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+      if (lane == 0) cols[static_cast<long long>(kMaxItems + c) * G + cta] = e;
+    }
   }
   if (!gridBarrier(p, sh)) return false;
-  // 3. totals: one warp per item, rows added in CTA order (lane partials over a fixed CTA stride, then a fixed tree)
-  const int nitems = nta + ncand;
-  for (int it = warp; it < nitems; it += kWarps)
+  // 3. totals: columns spread over the warps, lanes over the CTAs; all loads of a column are issued before any sum.
+  //    The order is fixed (lane partials over j, then a fixed shuffle tree), so every CTA gets identical totals.
+  const int nitems = nta + ncand, nwords = (nta + 31) >> 5;
+  for (int it = warp; it < nitems + nwords; it += kWarps)
   {
-    const int col = it < nta ? it : kMaxItems + (it - nta);
-    double s = 0.0;
-    for (int q = lane; q < G; q += 32) s += __ldcg(rows + static_cast<long long>(q) * kRow + col);
+    const int col = it < nta ? it : it < nitems ? kMaxItems + (it - nta) : kMaxItems + kMaxCand + (it - nitems);
+    const double* src = cols + static_cast<long long>(col) * G;
+    double v[kMaxBlocks / 32];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) sh.tot[it] = s;
-  }
-  if (tid < 4)
-  {
-    unsigned o = 0u;
-    for (int q = 0; q < G; ++q)
-      o |= __ldcg(reinterpret_cast<const unsigned*>(rows + static_cast<long long>(q) * kRow + kMaxItems + kMaxCand) + tid);
-    sh.ovl[tid] = o;
+    for (int j = 0; j < kMaxBlocks / 32; ++j)
+    {
+      const int q = lane + 32 * j;
+      v[j] = q < G ? __ldcg(src + q) : 0.0;
+    }
+    if (it < nitems)
+    {
+      double s = 0.0;
+#pragma unroll
+      for (int j = 0; j < kMaxBlocks / 32; ++j) s += v[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) sh.tot[it] = s;
+    }
+    else
+    {
+      unsigned o = 0u;
+#pragma unroll
+      for (int j = 0; j < kMaxBlocks / 32; ++j) o |= static_cast<unsigned>(v[j]);
+      o = __reduce_or_sync(0xffffffffu, o);
+      if (lane == 0) sh.ovl[it - nitems] = o;
+    }
   }
   if (tid == 0) sh.phases += 1;
   __syncthreads();
@@ -505,37 +573,34 @@ __device__ void orientedMolecule(const Params& p, const Comp& c, double3 first, 
   }
 }
 
-// Boltzmann selection among the trials with ok bit set (CBMC::selectTrialPosition, cbmc/util.cpp:14-47);
-// *W = sum exp(lw) / k; returns -1 if none. Thread-level (k <= 12).
-__device__ int selectTrial(const double* lw, unsigned ok, int k, double u, double* W)
+// Boltzmann selection among up to 32 trials held one per lane (CBMC::selectTrialPosition, cbmc/util.cpp:14-47): lane t
+// holds the log-weight lw of trial t and whether it is allowed. Returns in every lane the selected trial (-1 if none)
+// and W = sum over the allowed trials of exp(lw) / k. The maximum, the prefix sums and the total come from fixed
+// shuffle patterns, so every CTA takes the same decision.
+__device__ int warpSelect(double lw, bool ok, int k, double u, double* W)
 {
-  double largest = -1e300;
-  for (int t = 0; t < k; ++t)
-    if ((ok >> t) & 1u) largest = fmax(largest, lw[t]);
-  if (largest == -1e300)
+  const int lane = threadIdx.x & 31;
+  const bool on = ok && lane < k;
+  double m = on ? lw : -1e300;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (m == -1e300)
   {
     *W = 0.0;
     return -1;
   }
-  double sum = 0.0, w = 0.0;
-  for (int t = 0; t < k; ++t)
-    if ((ok >> t) & 1u)
-    {
-      sum += exp(lw[t] - largest);
-      w += exp(lw[t]);
-    }
-  *W = w / static_cast<double>(k);
-  const double target = u * sum;
-  double cum = 0.0;
-  int last = -1;
-  for (int t = 0; t < k; ++t)
+  double pre = on ? exp(lw - m) : 0.0;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1)
   {
-    if (!((ok >> t) & 1u)) continue;
-    last = t;
-    cum += exp(lw[t] - largest);
-    if (cum >= target) return t;
+    const double y = __shfl_up_sync(0xffffffffu, pre, o);
+    if (lane >= o) pre += y;
   }
-  return last;
+  const double sum = __shfl_sync(0xffffffffu, pre, 31);
+  *W = exp(m) * sum / static_cast<double>(k);
+  const unsigned onMask = __ballot_sync(0xffffffffu, on);
+  const unsigned hit = __ballot_sync(0xffffffffu, on && pre >= u * sum);
+  return hit ? __ffs(hit) - 1 : 31 - __clz(onMask);
 }
 
 __device__ __forceinline__ double3 loadPos(const Params& p, int site)
@@ -556,6 +621,21 @@ __device__ void storeMolecule(const Params& p, int m, int cidx, const double3* x
   }
 }
 
+// the atoms of one orientation trial other than the starting bead, in atom order, into trial-atom slots base, base+1, ..
+__device__ void storeOrientation(const Params& p, Shared& sh, const double** atomGrid, const Comp& cc,
+                                 const double3* x, int base)
+{
+  int a = base;
+  for (int i = 0; i < p.na; ++i)
+  {
+    if (i == cc.starting_bead) continue;
+    sh.ta[a] = x[i];
+    sh.tf[a] = toFixed(p, x[i], cc.types[i]);
+    atomGrid[a] = cc.vdw_grid[i];
+    ++a;
+  }
+}
+
 __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves)
 {
   __shared__ Shared sh;
@@ -568,8 +648,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
     sh.n = p.n_state[0];
     for (int c = 0; c < kMaxComp; ++c) sh.count[c] = p.n_state[1 + c];
     sh.energy = *p.energy;
-    sh.gen = static_cast<int>(atomicAdd(&p.bar[1], 0u));
-    sh.fail = 0;
+    sh.gen = 0;
+    sh.fail = loadRelaxed(&p.bar[1]) != 0ull;  // a barrier of an earlier launch timed out: do nothing
     sh.phases = 0;
     for (int k = 0; k < kStats; ++k) sh.stats[k] = p.stats[k];
   }
@@ -579,6 +659,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
   const long long move0 = *p.move_base;
   __shared__ const double* atomGrid[kMaxItems];
   __syncthreads();
+  if (sh.fail) return;
   for (int mv = 0; mv < moves; ++mv)
   {
     const long long move = move0 + mv;
@@ -720,69 +801,57 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
       }
       __syncthreads();
       if (!phase(p, sh, -1, atomGrid)) break;
-      if (tid == 0)
+      if (tid < 32)
       {
-        double lw[kMaxTrials];
-        unsigned ok = 0u;
-        for (int t = 0; t < p.k1; ++t)
-        {
-          lw[t] = -p.beta * sh.tot[t] - sh.logq[t];
-          if (!ovlOf(sh, t)) ok |= 1u << t;
-        }
+        const int t = tid;
+        const double lw = t < p.k1 ? -p.beta * sh.tot[t] - sh.logq[t] : 0.0;
         double W;
-        const int sel = selectTrial(lw, ok, p.k1, urand(p, move, slot(kKindMove, 1, 0)).x, &W);
-        sh.selFirst = sel;
-        sh.W = W;
-        if (sel >= 0)
+        const int sel = warpSelect(lw, t < p.k1 && !ovlOf(sh, t), p.k1, urand(p, move, slot(kKindMove, 1, 0)).x, &W);
+        if (tid == 0)
+        {
+          sh.selFirst = sel;
+          sh.W = W;
+        }
+        if (tid == 0 && sel >= 0)
         {
           sh.first = sh.ta[sel];
           sh.dU = sh.tot[sel];
-          // orientation trials: the other atoms of each orientation; Ewald candidates: whole molecules
-          int a = 0;
-          for (int t = 0; t < p.k2; ++t)
-          {
-            double3 x[kMaxAtoms];
-            orientedMolecule(p, cc, sh.first, move, kKindOrient, t, x);
-            for (int i = 0; i < na; ++i)
-            {
-              sh.cpos[t][i] = x[i];
-              sh.cq[t][i] = cc.charges[i];
-              if (i == sb) continue;
-              sh.ta[a] = x[i];
-              sh.tf[a] = toFixed(p, x[i], cc.types[i]);
-              atomGrid[a] = cc.vdw_grid[i];
-              ++a;
-            }
-            sh.cn[t] = na;
-          }
-          sh.nta = a;
+          sh.nta = p.k2 * (na - 1);
           sh.ncand = p.use_charge ? p.k2 : 0;
         }
       }
       __syncthreads();
       if (sh.selFirst >= 0)
       {
-        if (!phase(p, sh, -1, atomGrid)) break;
-        if (tid == 0)
+        // orientation trials, one per thread: the other atoms of each orientation; Ewald candidates: whole molecules
+        if (tid < p.k2)
         {
-          double lw[kMaxTrials];
-          unsigned ok = 0u;
-          const int per = na - 1;
-          for (int t = 0; t < p.k2; ++t)
+          double3 x[kMaxAtoms];
+          orientedMolecule(p, cc, sh.first, move, kKindOrient, tid, x);
+          for (int i = 0; i < na; ++i)
           {
-            double e = 0.0;
-            bool o = false;
+            sh.cpos[tid][i] = x[i];
+            sh.cq[tid][i] = cc.charges[i];
+          }
+          sh.cn[tid] = na;
+          storeOrientation(p, sh, atomGrid, cc, x, tid * (na - 1));
+        }
+        __syncthreads();
+        if (!phase(p, sh, -1, atomGrid)) break;
+        if (tid < 32)
+        {
+          const int per = na - 1, t = tid;
+          double e = 0.0;
+          bool o = false;
+          if (t < p.k2)
             for (int i = 0; i < per; ++i)
             {
               e += sh.tot[t * per + i];
               o |= ovlOf(sh, t * per + i);
             }
-            lw[t] = -p.beta * e;
-            if (!o) ok |= 1u << t;
-          }
           double W2;
-          const int sel = selectTrial(lw, ok, p.k2, urand(p, move, slot(kKindMove, 2, 0)).x, &W2);
-          if (sel >= 0 && sh.W * W2 >= 1e-150)
+          const int sel = warpSelect(-p.beta * e, t < p.k2 && !o, p.k2, urand(p, move, slot(kKindMove, 2, 0)).x, &W2);
+          if (tid == 0 && sel >= 0 && sh.W * W2 >= 1e-150)
           {
             const double dEw = p.use_charge ? sh.tot[sh.nta + sel] + cc.self_excl : 0.0;
             const double W = sh.W * W2;
@@ -847,65 +916,48 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
         sh.preCl = __ldcg(p.comp_of + last);
         sh.preSl = __ldcg(p.slot + last);
         for (int i = 0; i < na; ++i) sh.preLast[i] = loadPos(p, last * na + i);
-        const double3 first = loadPos(p, m * na + sb);
-        int a = p.k1;
-        for (int t = 0; t < p.k2; ++t)
-        {
-          double3 x[kMaxAtoms];
-          if (t == 0)
-            for (int i = 0; i < na; ++i) x[i] = loadPos(p, m * na + i);
-          else
-            orientedMolecule(p, cc, first, move, kKindOrient, t, x);
-          for (int i = 0; i < na; ++i)
-          {
-            if (i == sb) continue;
-            sh.ta[a] = x[i];
-            sh.tf[a] = toFixed(p, x[i], cc.types[i]);
-            atomGrid[a] = cc.vdw_grid[i];
-            ++a;
-          }
-        }
         for (int i = 0; i < na; ++i)
         {
           sh.cpos[0][i] = loadPos(p, m * na + i);
           sh.cq[0][i] = -cc.charges[i];
         }
         sh.cn[0] = na;
-        sh.nta = a;
+        sh.nta = p.k1 + p.k2 * (na - 1);
         sh.ncand = p.use_charge ? 1 : 0;
+      }
+      // retrace orientations about the old first bead, one per thread (trial 0: the molecule itself)
+      if (tid < p.k2)
+      {
+        double3 x[kMaxAtoms];
+        if (tid == 0)
+          for (int i = 0; i < na; ++i) x[i] = loadPos(p, m * na + i);
+        else
+          orientedMolecule(p, cc, loadPos(p, m * na + sb), move, kKindOrient, tid, x);
+        storeOrientation(p, sh, atomGrid, cc, x, p.k1 + tid * (na - 1));
       }
       __syncthreads();
       if (!phase(p, sh, m, atomGrid)) break;
-      if (tid == 0)
+      if (tid < 32)
       {
-        double lw[kMaxTrials];
-        unsigned ok = 0u;
-        for (int t = 0; t < p.k1; ++t)
-        {
-          lw[t] = -p.beta * sh.tot[t] - sh.logq[t];
-          if (!ovlOf(sh, t)) ok |= 1u << t;
-        }
+        // Rosenbluth weights of the retrace: first beads (trial 0 = the old bead) and orientations (trial 0 = the
+        // molecule itself); lane t holds trial t of each
+        const int t = tid, per = na - 1;
+        const bool ok1 = t < p.k1 && !ovlOf(sh, t);
         double W1, W2;
-        selectTrial(lw, ok, p.k1, 0.0, &W1);
-        unsigned ok2 = 0u;
-        double lw2[kMaxTrials], e0 = 0.0;
-        const int per = na - 1;
-        for (int t = 0; t < p.k2; ++t)
-        {
-          double e = 0.0;
-          bool o = false;
+        warpSelect(t < p.k1 ? -p.beta * sh.tot[t] - sh.logq[t] : 0.0, ok1, p.k1, 0.0, &W1);
+        double e = 0.0;
+        bool o = false;
+        if (t < p.k2)
           for (int i = 0; i < per; ++i)
           {
             e += sh.tot[p.k1 + t * per + i];
             o |= ovlOf(sh, p.k1 + t * per + i);
           }
-          if (t == 0) e0 = e;
-          lw2[t] = -p.beta * e;
-          if (!o) ok2 |= 1u << t;
-        }
-        selectTrial(lw2, ok2, p.k2, 0.0, &W2);
-        if ((ok & 1u) && (ok2 & 1u))
+        warpSelect(-p.beta * e, t < p.k2 && !o, p.k2, 0.0, &W2);
+        const bool ok2 = !o;
+        if (tid == 0 && ok1 && ok2)
         {
+          const double e0 = e;
           const double dEw = p.use_charge ? sh.tot[sh.nta] - cc.self_excl : 0.0;
           const double W = W1 * W2;
           const double pacc = exp(-p.beta * dEw) * static_cast<double>(sh.count[c]) /
@@ -975,75 +1027,58 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
         const int m = sh.m, oldC = sh.c, newC = sh.c2;
         const Comp& co = p.comp[oldC];
         const Comp& cn = p.comp[newC];
+        // trial atoms: new first bead (on the old starting bead), new orientations, old first bead, old retrace; the
+        // orientations are built one per thread (new: threads [0, k2), old: threads [k2, 2 k2))
+        const int base2 = 1 + p.k2 * (na - 1);  // slot of the old first bead
+        const double3 first = loadPos(p, m * na + co.starting_bead);
         if (tid == 0)
         {
           sh.preSlot = __ldcg(p.slot + m);
           sh.preLastC = __ldcg(p.list + oldC * p.capacity + sh.count[oldC] - 1);
-          // trial atoms: new first bead (on the old starting bead), new orientations, old first bead, old retrace
-          const double3 first = loadPos(p, m * na + co.starting_bead);
-          int a = 0;
-          sh.ta[a] = first;
-          sh.tf[a] = toFixed(p, first, cn.types[cn.starting_bead]);
-          atomGrid[a] = cn.vdw_grid[cn.starting_bead];
-          ++a;
-          for (int t = 0; t < p.k2; ++t)
-          {
-            double3 x[kMaxAtoms];
-            orientedMolecule(p, cn, first, move, kKindNewOrient, t, x);
-            for (int i = 0; i < na; ++i)
-            {
-              sh.cpos[t][i] = x[i];
-              sh.cq[t][i] = cn.charges[i];
-              if (i == cn.starting_bead) continue;
-              sh.ta[a] = x[i];
-              sh.tf[a] = toFixed(p, x[i], cn.types[i]);
-              atomGrid[a] = cn.vdw_grid[i];
-              ++a;
-            }
-            for (int i = 0; i < na; ++i)
-            {
-              sh.cpos[t][na + i] = loadPos(p, m * na + i);
-              sh.cq[t][na + i] = -co.charges[i];
-            }
-            sh.cn[t] = 2 * na;
-          }
-          sh.ta[a] = first;
-          sh.tf[a] = toFixed(p, first, co.types[co.starting_bead]);
-          atomGrid[a] = co.vdw_grid[co.starting_bead];
-          ++a;
-          const double3 firstOld = first;
-          for (int t = 0; t < p.k2; ++t)
-          {
-            double3 x[kMaxAtoms];
-            if (t == 0)
-              for (int i = 0; i < na; ++i) x[i] = loadPos(p, m * na + i);
-            else
-              orientedMolecule(p, co, firstOld, move, kKindOldOrient, t, x);
-            for (int i = 0; i < na; ++i)
-            {
-              if (i == co.starting_bead) continue;
-              sh.ta[a] = x[i];
-              sh.tf[a] = toFixed(p, x[i], co.types[i]);
-              atomGrid[a] = co.vdw_grid[i];
-              ++a;
-            }
-          }
-          sh.nta = a;
+          sh.ta[0] = first;
+          sh.tf[0] = toFixed(p, first, cn.types[cn.starting_bead]);
+          atomGrid[0] = cn.vdw_grid[cn.starting_bead];
+          sh.ta[base2] = first;
+          sh.tf[base2] = toFixed(p, first, co.types[co.starting_bead]);
+          atomGrid[base2] = co.vdw_grid[co.starting_bead];
+          sh.nta = 2 * base2;
           sh.ncand = p.use_charge ? p.k2 : 0;
+        }
+        if (tid < p.k2)
+        {
+          const int t = tid;
+          double3 x[kMaxAtoms];
+          orientedMolecule(p, cn, first, move, kKindNewOrient, t, x);
+          for (int i = 0; i < na; ++i)
+          {
+            sh.cpos[t][i] = x[i];
+            sh.cq[t][i] = cn.charges[i];
+            sh.cpos[t][na + i] = loadPos(p, m * na + i);
+            sh.cq[t][na + i] = -co.charges[i];
+          }
+          sh.cn[t] = 2 * na;
+          storeOrientation(p, sh, atomGrid, cn, x, 1 + t * (na - 1));
+        }
+        else if (tid < 2 * p.k2)
+        {
+          const int t = tid - p.k2;
+          double3 x[kMaxAtoms];
+          if (t == 0)
+            for (int i = 0; i < na; ++i) x[i] = loadPos(p, m * na + i);
+          else
+            orientedMolecule(p, co, first, move, kKindOldOrient, t, x);
+          storeOrientation(p, sh, atomGrid, co, x, base2 + 1 + t * (na - 1));
         }
         __syncthreads();
         if (!phase(p, sh, m, atomGrid)) break;
-        if (tid == 0)
+        if (tid < 32)
         {
           const int per = na - 1;
-          const int base2 = 1 + p.k2 * per;  // index of the old first bead
-          double lw[kMaxTrials], lw2[kMaxTrials];
-          unsigned ok = 0u, ok2 = 0u;
-          double e0 = 0.0;
-          for (int t = 0; t < p.k2; ++t)
-          {
-            double e = 0.0, eo = 0.0;
-            bool o = false, oo = false;
+          // lane t: new orientation t and old retrace orientation t (trial 0 = the molecule itself)
+          const int t = tid;
+          double e = 0.0, eo = 0.0;
+          bool o = false, oo = false;
+          if (t < p.k2)
             for (int i = 0; i < per; ++i)
             {
               e += sh.tot[1 + t * per + i];
@@ -1051,18 +1086,14 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
               eo += sh.tot[base2 + 1 + t * per + i];
               oo |= ovlOf(sh, base2 + 1 + t * per + i);
             }
-            lw[t] = -p.beta * e;
-            lw2[t] = -p.beta * eo;
-            if (!o) ok |= 1u << t;
-            if (!oo) ok2 |= 1u << t;
-            if (t == 0) e0 = eo;
-          }
           double Wn2, Wo2;
-          const int sel = selectTrial(lw, ok, p.k2, urand(p, move, slot(kKindMove, 3, 0)).x, &Wn2);
-          selectTrial(lw2, ok2, p.k2, 0.0, &Wo2);
-          const bool newFirstOk = !ovlOf(sh, 0), oldOk = !ovlOf(sh, base2) && (ok2 & 1u);
+          const int sel = warpSelect(-p.beta * e, t < p.k2 && !o, p.k2, urand(p, move, slot(kKindMove, 3, 0)).x, &Wn2);
+          warpSelect(-p.beta * eo, t < p.k2 && !oo, p.k2, 0.0, &Wo2);
+          const double eSel = __shfl_sync(0xffffffffu, e, sel >= 0 ? sel : 0);
+          const double e0 = eo;  // lane 0: the old molecule's own orientation
+          const bool newFirstOk = !ovlOf(sh, 0), oldOk = !ovlOf(sh, base2) && !oo;
           const double Wn = exp(-p.beta * sh.tot[0]) * Wn2, Wo = exp(-p.beta * sh.tot[base2]) * Wo2;
-          if (newFirstOk && sel >= 0 && oldOk && Wn >= 1e-150)
+          if (tid == 0 && newFirstOk && sel >= 0 && oldOk && Wn >= 1e-150)
           {
             const double dEw = p.use_charge ? sh.tot[sh.nta + sel] + cn.self_excl - co.self_excl : 0.0;
             const double pacc = exp(-p.beta * dEw) * (Wn / cn.w_ig) * cn.fugacity *
@@ -1070,8 +1101,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
                                 ((Wo / co.w_ig) * co.fugacity * static_cast<double>(sh.count[newC] + 1));
             if (sh.u[6] < pacc)
             {
-              double en = sh.tot[0];
-              for (int i = 0; i < per; ++i) en += sh.tot[1 + sel * per + i];
+              const double en = sh.tot[0] + eSel;
               sh.accept = 1;
               sh.energy += (en - (sh.tot[base2] + e0)) + dEw;
               sh.selOrient = sel;
@@ -1138,6 +1168,7 @@ struct rg_mixture
   Params p{};
   int blocks = 0;
   int n_comp = 0;
+  size_t smem = 0;  // dynamic shared memory of a launch: the Ewald phasor tables
   std::vector<void*> allocs;
 };
 
@@ -1350,17 +1381,23 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
     p.kvec = kv;
     p.temp = temp;
     p.nk = static_cast<int>(nk);
+    for (int d = 0; d < 3; ++d) p.km[d] = kmax[d];
   }
+  p.tabK = 1 + std::max({p.km[0], p.km[1], p.km[2]});
+  x->smem = sizeof(double2) * kMaxCand * kMaxCandAtoms * 3 * static_cast<size_t>(p.tabK);
   // launch geometry: one CTA per SM, co-resident
   int sms = 0, perSM = 0;
   cudaError_t err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, mixtureKernel, kThreads, 0);
+  if (err == cudaSuccess)
+    err = cudaFuncSetAttribute(mixtureKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(x->smem));
+  if (err == cudaSuccess)
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, mixtureKernel, kThreads, x->smem);
   if (err != cudaSuccess || perSM < 1)
   {
     delete x;
     return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: kernel does not fit on an SM");
   }
-  x->blocks = params->n_blocks > 0 ? std::min(params->n_blocks, sms * perSM) : sms;
+  x->blocks = std::min(kMaxBlocks, params->n_blocks > 0 ? std::min(params->n_blocks, sms * perSM) : sms);
   if (p.use_charge && (p.nk + x->blocks - 1) / x->blocks > kMaxKPerCta)
   {
     delete x;
@@ -1387,7 +1424,7 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   alloc(reinterpret_cast<void**>(&p.stats), sizeof(double) * kStats);
   alloc(reinterpret_cast<void**>(&p.sk), sizeof(double2) * std::max(1, p.nk));
   alloc(reinterpret_cast<void**>(&p.part), sizeof(double) * kRow * 2 * x->blocks);
-  alloc(reinterpret_cast<void**>(&p.bar), sizeof(unsigned) * 4);
+  alloc(reinterpret_cast<void**>(&p.bar), sizeof(unsigned long long) * 2);
   int4* dfwx = nullptr;
   float* dfwq = nullptr;
   alloc(reinterpret_cast<void**>(&dfwx), sizeof(int4) * hfw.size());
@@ -1465,7 +1502,7 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   if (err == cudaSuccess) err = cudaMemcpyAsync(p.move_base, &zl, sizeof(long long), cudaMemcpyHostToDevice, sm);
   if (err == cudaSuccess) err = cudaMemsetAsync(p.stats, 0, sizeof(double) * kStats, sm);
   if (err == cudaSuccess) err = cudaMemsetAsync(p.sk, 0, sizeof(double2) * std::max(1, p.nk), sm);
-  if (err == cudaSuccess) err = cudaMemsetAsync(p.bar, 0, sizeof(unsigned) * 4, sm);
+  if (err == cudaSuccess) err = cudaMemsetAsync(p.bar, 0, sizeof(unsigned long long) * 2, sm);
   if (err == cudaSuccess) err = cudaStreamSynchronize(sm);
   if (err != cudaSuccess)
   {
@@ -1513,8 +1550,10 @@ extern "C" rg_status rg_mixture_run(rg_mixture* x, int64_t moves, int record)
   {
     int m = static_cast<int>(std::min<int64_t>(per, moves - done));
     void* args[] = {&x->p, &m};
+    // the barrier's arrival counter starts at zero in every launch (the error flag beside it persists)
+    RG_CUDA(ctx, cudaMemsetAsync(x->p.bar, 0, sizeof(unsigned long long), ctx->stream));
     RG_CUDA(ctx, cudaLaunchCooperativeKernel(reinterpret_cast<void*>(mixtureKernel), dim3(x->blocks), dim3(kThreads),
-                                             args, 0, ctx->stream));
+                                             args, x->smem, ctx->stream));
   }
   return RG_OK;
 }
@@ -1526,7 +1565,7 @@ extern "C" rg_status rg_mixture_results(rg_mixture* x, rg_mixture_result* out)
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
   int ns[1 + kMaxComp];
   double e, st[kStats];
-  unsigned bar[4];
+  unsigned long long bar[2];
   RG_CUDA(ctx, cudaMemcpyAsync(ns, x->p.n_state, sizeof(ns), cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(ctx, cudaMemcpyAsync(&e, x->p.energy, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(ctx, cudaMemcpyAsync(st, x->p.stats, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1546,7 +1585,7 @@ extern "C" rg_status rg_mixture_results(rg_mixture* x, rg_mixture_result* out)
   }
   out->sum_energy = st[14];
   out->samples = static_cast<int64_t>(st[15]);
-  out->status = bar[2] ? RG_ERR_TIMEOUT : RG_OK;
+  out->status = bar[1] ? RG_ERR_TIMEOUT : RG_OK;
   return RG_OK;
 }
 

@@ -3,9 +3,10 @@
 The framework is the configuration-1/2 generator (96 T + 192 O per cell, T +2.05 e, O -1.025 e) on a cell 1.5 times
 the configuration-1/2 lengths (30.0 x 29.85 x 20.1 A), replicated 4 x 4 x 4: 18,432 atoms, holding 2,000 rigid CO2
 and 2,000 rigid 3-site N2 (N-N 1.10 A, N 36 K / 3.31 A / -0.482 e, massless centre +0.964 e); Ewald alpha = 0.265 per
-Angstrom with kmax 12 (integer sphere: 3,796 k-vectors). Framework energies come from the unit-cell grids (C_co2, O_co2,
-N_n2 and N_com Lennard-Jones -- every adsorbate type has one, N_com's being zero -- and the unit-charge real-space Ewald
-grid, 0.15 A spacing). The larger cell is what makes room for
+Angstrom and kmax 12 given explicitly, so every k of the half-box is used, as the reference does for explicit Ewald
+parameters (forcefield.cpp:388-418; 8,124 k-vectors; the integer sphere belongs to the automatic setting). Framework
+energies come from the unit-cell grids (C_co2, O_co2, N_n2 and N_com Lennard-Jones -- every adsorbate type has one,
+N_com's being zero -- and the unit-charge real-space Ewald grid, 0.15 A spacing). The larger cell is what makes room for
 4,000 molecules: in the 20.0 x 19.9 x 13.4 A cell with randomly placed atoms only 0.7 % of the volume is farther than
 2.6 A from an atom, too little for 62.5 molecules per cell; at 1.5 times the lengths it is 44 %.
 """
@@ -108,7 +109,7 @@ def config5(ctx, torch, reps=(4, 4, 4), counts=(2000, 2000), kmax: int = 12, see
     kept alive), System, Ewald, components and the starting configuration."""
     from . import native
 
-    ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=kmax)
+    ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=kmax, sphere=False)
     ucell, ufw = synthetic_framework(ff, lengths, n_t=96, seed=42)
     scell, sfw = replicate(ucell, ufw, reps)
     dims = dims or grid_points_for_spacing(ucell, spacing)

@@ -48,6 +48,8 @@ constexpr int kMaxKPerCta = 64;
 constexpr int kMaxTypes = 16;
 constexpr int kRow = kMaxItems + kMaxCand + 4;  // columns of partial sums per CTA (last 4: overlap-bit words)
 constexpr int kMaxBlocks = 256;                 // CTAs of the cooperative launch (lanes x 8 in the column sums)
+constexpr int kSlice = 512;                     // molecule sites of a CTA's slice staged in shared memory per phase
+constexpr int kFwSlice = 512;                   // framework atoms of a CTA's slice kept in shared memory
 constexpr long long kSpinLimit = 1ll << 22;
 constexpr int kStats = 24;
 constexpr double kPi = 3.141592653589793238462643383279502884;
@@ -141,6 +143,11 @@ struct Shared
   double2 dk[kMaxCand][kMaxKPerCta];  // structure-factor change of each candidate over this CTA's k-range
   double ek[kMaxCand][kMaxKPerCta];   // its energy change per k
   double fwE[kMaxItems];              // framework (grid) energy of the trial atoms this CTA owns
+  // this CTA's k-range for the whole launch: k-vectors, prefactors and its S(k) (only this CTA updates them; written
+  // back to global memory at the end of the launch)
+  char4 kv[kMaxKPerCta];
+  double kt[kMaxKPerCta];
+  double2 ks[kMaxKPerCta];
   double red[kThreads];
   unsigned ovl_bits[4];
   double tot[kMaxItems + kMaxCand];  // totals over the grid
@@ -160,6 +167,7 @@ struct Shared
   double3 first;
   double logq[kMaxTrials];
   double stats[kStats];
+  double3 rel[kMaxTrials][kMaxAtoms];  // insertion: orientation offsets from the starting bead, computed up front
 };
 
 __device__ __forceinline__ double2 urand(const Params& p, long long move, uint32_t sl)
@@ -254,6 +262,73 @@ __device__ bool gridBarrier(const Params& p, Shared& sh)
   return !sh.fail;
 }
 
+// Dynamic shared memory: the Ewald phasor tables (kMaxCand x kMaxCandAtoms x 3 axes x tabK), this CTA's molecule
+// sites staged per phase, and its framework atoms (explicit pairs of grid-less types) kept for the launch.
+struct Dyn
+{
+  double2* phasor;
+  int4* slice;  // [kSlice]
+  int4* fws;    // [kFwSlice]
+  float* fwq;   // [kFwSlice]
+};
+__host__ __device__ constexpr size_t phasorBytes(int tabK)
+{
+  return sizeof(double2) * kMaxCand * kMaxCandAtoms * 3 * static_cast<size_t>(tabK);
+}
+__host__ __device__ constexpr size_t dynBytes(int tabK)
+{
+  return phasorBytes(tabK) + sizeof(int4) * (kSlice + kFwSlice) + sizeof(float) * kFwSlice;
+}
+__device__ __forceinline__ Dyn dynOf(const Params& p)
+{
+  extern __shared__ __align__(16) unsigned char dynSmem[];
+  Dyn d;
+  d.phasor = reinterpret_cast<double2*>(dynSmem);
+  d.slice = reinterpret_cast<int4*>(dynSmem + phasorBytes(p.tabK));
+  d.fws = d.slice + kSlice;
+  d.fwq = reinterpret_cast<float*>(d.fws + kFwSlice);
+  return d;
+}
+
+// Lennard-Jones + real-space Ewald of trial atom B (type bt, charge qb) with partner P (fixed point, .w & 0xff = type;
+// charge qP), FP32 from the exact fixed-point displacement (the uint32 wrap is the minimum image), added to acc in FP64.
+__device__ __forceinline__ void pairTerm(const Params& p, const Shared& sh, int4 B, int bt, float qb, int4 P, float qP,
+                                         float rc2v, double& acc, bool& ov)
+{
+  const int pt = P.w & 0xff;
+  const float f0 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.x) - static_cast<uint32_t>(P.x))) * kFix;
+  const float f1 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.y) - static_cast<uint32_t>(P.y))) * kFix;
+  const float f2 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.z) - static_cast<uint32_t>(P.z))) * kFix;
+  const float rx = fmaf(p.hf[0][0], f0, fmaf(p.hf[1][0], f1, p.hf[2][0] * f2));
+  const float ry = fmaf(p.hf[0][1], f0, fmaf(p.hf[1][1], f1, p.hf[2][1] * f2));
+  const float rz = fmaf(p.hf[0][2], f0, fmaf(p.hf[1][2], f1, p.hf[2][2] * f2));
+  const float rr = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+  if (rr < rc2v)
+  {
+    const float4 q = sh.tab[bt * kMaxTypes + pt];
+    if (q.w != 0.0f)
+    {
+      const float t = q.y * rgd::rcpRn(rr);
+      const float t3 = t * t * t;
+      const float e = q.x * (t3 * (t3 - 1.0f)) - q.z;
+      if (e > p.overlap_f) ov = true;
+      acc += static_cast<double>(e);
+    }
+  }
+  if (p.use_charge && rr < p.rc2_c)
+  {
+    const float qq = qb * qP;
+    if (qq != 0.0f)
+    {
+      // potentialCoulomb<0>, Ewald branch at full scaling: C qA qB erfc(alpha r) / r
+      const float invr = rgd::rsqrtRn(rr);
+      const float r = rr * invr;
+      const float ex = expf(-p.alpha * p.alpha * rr);
+      acc += static_cast<double>(p.coul * qq * rgd::erfcFromExp(p.alpha * r, ex) * invr);
+    }
+  }
+}
+
 // One phase: energies of sh.nta trial atoms (framework + molecules other than `skip`) and the Ewald energy change of
 // sh.ncand candidates, each summed over the whole grid into sh.tot[0, nta) and sh.tot[nta, nta + ncand); overlap bits
 // per trial atom in sh.ovl. vdwOf/qOf: the framework grid and charge of each trial atom (set by the caller in
@@ -263,6 +338,10 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int G = gridDim.x, cta = blockIdx.x;
   const int nta = sh.nta, ncand = sh.ncand;
+  const int ns = sh.n * p.na;
+  const int chunk = (ns + G - 1) / G, s0 = min(ns, cta * chunk), s1 = min(ns, s0 + chunk);
+  const int nst = min(s1 - s0, kSlice);
+  const Dyn dy = dynOf(p);
   if (tid < 4)
   {
     sh.ovl_bits[tid] = 0u;
@@ -271,37 +350,41 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
   if (tid < nta) sh.fwE[tid] = 0.0;
   __syncthreads();
   // 0. framework grids of the trial atoms this CTA owns (b = cta, cta + G, ..), by 16 lanes of the last warp: lane l
-  //    takes corner l & 7 of the VDW grid (l < 8) or of the unit-charge Ewald grid (l >= 8). Started first, so its
-  //    grid loads overlap the pair loop of the other warps. The grid branch of interactions_framework_molecule.cpp:
-  //    only an atom whose type has a VDW grid takes it (its charge term then comes from the Ewald grid); any other
-  //    atom sees the framework atoms explicitly (below).
-  if (warp == kWarps - 1 && lane < 16)
-    for (int b = cta; b < nta; b += G)
-    {
-      const double* vdw = atomGrid[b];
-      const double q = static_cast<double>(sh.qt[sh.tf[b].w & 0xff]);
-      const bool charged = p.use_charge && p.ewald_grid != nullptr && q != 0.0;
-      double v = 0.0;
-      if (vdw != nullptr && (lane < 8 || charged))
+  //    takes corner l & 7 of the VDW grid (l < 8) or of the unit-charge Ewald grid (l >= 8). Meanwhile the other warps
+  //    stage this CTA's slice of molecule sites in shared memory. The grid branch of
+  //    interactions_framework_molecule.cpp: only an atom whose type has a VDW grid takes it (its charge term then
+  //    comes from the Ewald grid); any other atom sees the framework atoms explicitly (below).
+  if (warp == kWarps - 1)
+  {
+    if (lane < 16)
+      for (int b = cta; b < nta; b += G)
       {
-        rgd::Grid g = p.grid;
-        g.data = lane < 8 ? vdw : p.ewald_grid;
-        const double3 r = sh.ta[b];
-        v = rgd::interpolateCorner(g, rgd::gridCell(g, r.x, r.y, r.z), lane & 7);
+        const double* vdw = atomGrid[b];
+        const double q = static_cast<double>(sh.qt[sh.tf[b].w & 0xff]);
+        const bool charged = p.use_charge && p.ewald_grid != nullptr && q != 0.0;
+        double v = 0.0;
+        if (vdw != nullptr && (lane < 8 || charged))
+        {
+          rgd::Grid g = p.grid;
+          g.data = lane < 8 ? vdw : p.ewald_grid;
+          const double3 r = sh.ta[b];
+          v = rgd::interpolateCorner(g, rgd::gridCell(g, r.x, r.y, r.z), lane & 7);
+        }
+        v += __shfl_xor_sync(0x0000ffffu, v, 1);
+        v += __shfl_xor_sync(0x0000ffffu, v, 2);
+        v += __shfl_xor_sync(0x0000ffffu, v, 4);
+        const double ew = __shfl_sync(0x0000ffffu, v, 8);
+        if (lane == 0)
+        {
+          sh.fwE[b] = v + q * ew;
+          if (v > p.overlap) atomicOr(&sh.ovl_bits[b >> 5], 1u << (b & 31));
+        }
       }
-      v += __shfl_xor_sync(0x0000ffffu, v, 1);
-      v += __shfl_xor_sync(0x0000ffffu, v, 2);
-      v += __shfl_xor_sync(0x0000ffffu, v, 4);
-      const double ew = __shfl_sync(0x0000ffffu, v, 8);
-      if (lane == 0)
-      {
-        sh.fwE[b] = v + q * ew;
-        if (v > p.overlap) atomicOr(&sh.ovl_bits[b >> 5], 1u << (b & 31));
-      }
-    }
-  // 1. molecule-molecule pairs over this CTA's slice of sites
-  const int ns = sh.n * p.na;
-  const int chunk = (ns + G - 1) / G, s0 = cta * chunk, s1 = min(ns, s0 + chunk);
+  }
+  else
+    for (int i = tid; i < nst; i += (kWarps - 1) * 32) dy.slice[i] = __ldcg(p.fx + s0 + i);
+  __syncthreads();
+  // 1. molecule-molecule pairs over this CTA's slice of sites (staged part from shared memory, any rest from L2)
   double acc = 0.0;
   bool ov = false;
   const int streams = nta > 0 ? kThreads / nta : 0;
@@ -311,81 +394,21 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
     const int4 B = sh.tf[b];
     const int bt = B.w & 0xff;
     const float qb = sh.qt[bt];
-    for (int i = s0 + st; i < s1; i += streams)
+    for (int i = st; i < s1 - s0; i += streams)
     {
-      const int4 P = __ldcg(p.fx + i);
+      const int4 P = i < kSlice ? dy.slice[i] : __ldcg(p.fx + s0 + i);
       if ((P.w >> 8) == skip) continue;
-      const int pt = P.w & 0xff;
-      const float f0 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.x) - static_cast<uint32_t>(P.x))) * kFix;
-      const float f1 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.y) - static_cast<uint32_t>(P.y))) * kFix;
-      const float f2 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.z) - static_cast<uint32_t>(P.z))) * kFix;
-      const float rx = fmaf(p.hf[0][0], f0, fmaf(p.hf[1][0], f1, p.hf[2][0] * f2));
-      const float ry = fmaf(p.hf[0][1], f0, fmaf(p.hf[1][1], f1, p.hf[2][1] * f2));
-      const float rz = fmaf(p.hf[0][2], f0, fmaf(p.hf[1][2], f1, p.hf[2][2] * f2));
-      const float rr = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-      if (rr < p.rc2_mm)
-      {
-        const float4 q = sh.tab[bt * kMaxTypes + pt];
-        if (q.w != 0.0f)
-        {
-          const float t = q.y * rgd::rcpRn(rr);
-          const float t3 = t * t * t;
-          const float e = q.x * (t3 * (t3 - 1.0f)) - q.z;
-          if (e > p.overlap_f) ov = true;
-          acc += static_cast<double>(e);
-        }
-      }
-      if (p.use_charge && rr < p.rc2_c)
-      {
-        const float qq = qb * sh.qt[pt];
-        if (qq != 0.0f)
-        {
-          // potentialCoulomb<0>, Ewald branch at full scaling: C qA qB erfc(alpha r) / r
-          const float invr = rgd::rsqrtRn(rr);
-          const float r = rr * invr;
-          const float ex = expf(-p.alpha * p.alpha * rr);
-          acc += static_cast<double>(p.coul * qq * rgd::erfcFromExp(p.alpha * r, ex) * invr);
-        }
-      }
+      pairTerm(p, sh, B, bt, qb, P, sh.qt[P.w & 0xff], p.rc2_mm, acc, ov);
     }
     // trial atom without a VDW grid: explicit pairs with this CTA's slice of the framework atoms
     if (p.n_fw > 0 && atomGrid[b] == nullptr)
     {
-      const int fchunk = (p.n_fw + G - 1) / G, fa = cta * fchunk, fb = min(p.n_fw, fa + fchunk);
-      for (int i = fa + st; i < fb; i += streams)
+      const int fchunk = (p.n_fw + G - 1) / G, fa = min(p.n_fw, cta * fchunk), fb = min(p.n_fw, fa + fchunk);
+      for (int i = st; i < fb - fa; i += streams)
       {
-        const int4 P = __ldg(p.fwx + i);
-        const int pt = P.w;
-        const float f0 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.x) - static_cast<uint32_t>(P.x))) * kFix;
-        const float f1 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.y) - static_cast<uint32_t>(P.y))) * kFix;
-        const float f2 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.z) - static_cast<uint32_t>(P.z))) * kFix;
-        const float rx = fmaf(p.hf[0][0], f0, fmaf(p.hf[1][0], f1, p.hf[2][0] * f2));
-        const float ry = fmaf(p.hf[0][1], f0, fmaf(p.hf[1][1], f1, p.hf[2][1] * f2));
-        const float rz = fmaf(p.hf[0][2], f0, fmaf(p.hf[1][2], f1, p.hf[2][2] * f2));
-        const float rr = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-        if (rr < p.rc2_fw)
-        {
-          const float4 q = sh.tab[bt * kMaxTypes + pt];
-          if (q.w != 0.0f)
-          {
-            const float t = q.y * rgd::rcpRn(rr);
-            const float t3 = t * t * t;
-            const float e = q.x * (t3 * (t3 - 1.0f)) - q.z;
-            if (e > p.overlap_f) ov = true;
-            acc += static_cast<double>(e);
-          }
-        }
-        if (p.use_charge && rr < p.rc2_c)
-        {
-          const float qq = qb * __ldg(p.fwq + i);
-          if (qq != 0.0f)
-          {
-            const float invr = rgd::rsqrtRn(rr);
-            const float r = rr * invr;
-            const float ex = expf(-p.alpha * p.alpha * rr);
-            acc += static_cast<double>(p.coul * qq * rgd::erfcFromExp(p.alpha * r, ex) * invr);
-          }
-        }
+        const bool staged = i < kFwSlice;
+        pairTerm(p, sh, B, bt, qb, staged ? dy.fws[i] : __ldg(p.fwx + fa + i), staged ? dy.fwq[i] : __ldg(p.fwq + fa + i),
+                 p.rc2_fw, acc, ov);
       }
     }
   }
@@ -407,7 +430,7 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
   //    tab[j] = exp(2 pi i j s_d), j = 0..kmax_d (j < 0: the conjugate), built by powers of tab[1] (one thread per
   //    table); then per (candidate, k) the structure-factor change sum_a q_a tab_x[kx] tab_y[ky] tab_z[kz] and its
   //    energy change (ewald.cpp:1043-1244), one thread each; then per candidate the sum over k in a fixed order.
-  extern __shared__ double2 phasor[];
+  double2* phasor = dy.phasor;
   const int kchunk = (p.nk + G - 1) / G, k0 = cta * kchunk, nkr = max(0, min(p.nk, k0 + kchunk) - k0);
   if (ncand > 0)
   {
@@ -432,8 +455,8 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
     __syncthreads();
     for (int task = tid; task < ncand * nkr; task += kThreads)
     {
-      const int c = task / nkr, kk = task - c * nkr, k = k0 + kk;
-      const char4 kv = p.kvec[k];
+      const int c = task / nkr, kk = task - c * nkr;
+      const char4 kv = sh.kv[kk];
       double2 d = make_double2(0.0, 0.0);
       for (int a = 0; a < sh.cn[c]; ++a)
       {
@@ -447,8 +470,8 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
         d.x += q * (exy.x * ez.x - exy.y * ez.y);
         d.y += q * (exy.x * ez.y + exy.y * ez.x);
       }
-      const double2 sk = p.sk[k];
-      sh.ek[c][kk] = p.temp[k] * (2.0 * (sk.x * d.x + sk.y * d.y) + (d.x * d.x + d.y * d.y));
+      const double2 sk = sh.ks[kk];
+      sh.ek[c][kk] = sh.kt[kk] * (2.0 * (sk.x * d.x + sk.y * d.y) + (d.x * d.x + d.y * d.y));
       sh.dk[c][kk] = d;
     }
     __syncthreads();
@@ -464,34 +487,46 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
   if (!gridBarrier(p, sh)) return false;
   // 3. totals: columns spread over the warps, lanes over the CTAs; all loads of a column are issued before any sum.
   //    The order is fixed (lane partials over j, then a fixed shuffle tree), so every CTA gets identical totals.
-  const int nitems = nta + ncand, nwords = (nta + 31) >> 5;
-  for (int it = warp; it < nitems + nwords; it += kWarps)
+  const int nitems = nta + ncand, ncol = nitems + ((nta + 31) >> 5);
+  constexpr int kU = 4;  // columns per warp with their loads in flight together
+  for (int base = warp; base < ncol; base += kU * kWarps)
   {
-    const int col = it < nta ? it : it < nitems ? kMaxItems + (it - nta) : kMaxItems + kMaxCand + (it - nitems);
-    const double* src = cols + static_cast<long long>(col) * G;
-    double v[kMaxBlocks / 32];
+    double v[kU][kMaxBlocks / 32];
 #pragma unroll
-    for (int j = 0; j < kMaxBlocks / 32; ++j)
+    for (int u = 0; u < kU; ++u)
     {
-      const int q = lane + 32 * j;
-      v[j] = q < G ? __ldcg(src + q) : 0.0;
+      const int it = base + u * kWarps;
+      const int col = min(kRow - 1, it < nta ? it : it < nitems ? kMaxItems + (it - nta) : kMaxItems + kMaxCand + (it - nitems));
+      const double* src = cols + static_cast<long long>(col) * G;
+#pragma unroll
+      for (int j = 0; j < kMaxBlocks / 32; ++j)
+      {
+        const int q = lane + 32 * j;
+        v[u][j] = (it < ncol && q < G) ? __ldcg(src + q) : 0.0;
+      }
     }
-    if (it < nitems)
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
     {
-      double s = 0.0;
+      const int it = base + u * kWarps;
+      if (it >= ncol) continue;
+      if (it < nitems)
+      {
+        double sum = 0.0;
 #pragma unroll
-      for (int j = 0; j < kMaxBlocks / 32; ++j) s += v[j];
+        for (int j = 0; j < kMaxBlocks / 32; ++j) sum += v[u][j];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) sh.tot[it] = s;
-    }
-    else
-    {
-      unsigned o = 0u;
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) sh.tot[it] = sum;
+      }
+      else
+      {
+        unsigned o = 0u;
 #pragma unroll
-      for (int j = 0; j < kMaxBlocks / 32; ++j) o |= static_cast<unsigned>(v[j]);
-      o = __reduce_or_sync(0xffffffffu, o);
-      if (lane == 0) sh.ovl[it - nitems] = o;
+        for (int j = 0; j < kMaxBlocks / 32; ++j) o |= static_cast<unsigned>(v[u][j]);
+        o = __reduce_or_sync(0xffffffffu, o);
+        if (lane == 0) sh.ovl[it - nitems] = o;
+      }
     }
   }
   if (tid == 0) sh.phases += 1;
@@ -550,6 +585,26 @@ __device__ double3 firstBeadPosition(const Params& p, const Comp& c, long long m
   return make_double3(cell[0][0] * sf[0] + cell[1][0] * sf[1] + cell[2][0] * sf[2],
                       cell[0][1] * sf[0] + cell[1][1] * sf[1] + cell[2][1] * sf[2],
                       cell[0][2] * sf[0] + cell[1][2] * sf[1] + cell[2][2] * sf[2]);
+}
+
+// orientation (kind, t) of component c as offsets from its starting bead: rel[i] = R o_i - R o_sb
+__device__ void orientationOffsets(const Params& p, const Comp& c, long long move, uint32_t kind, int t, double3* rel)
+{
+  const double2 a = urand(p, move, slot(kind, t, 0));
+  const double2 b = urand(p, move, slot(kind, t, 1));
+  double R[3][3];
+  rotationFromUniforms(a.x, a.y, b.x, R);
+  const double* o0 = c.offsets[c.starting_bead];
+  const double rc[3] = {R[0][0] * o0[0] + R[0][1] * o0[1] + R[0][2] * o0[2],
+                        R[1][0] * o0[0] + R[1][1] * o0[1] + R[1][2] * o0[2],
+                        R[2][0] * o0[0] + R[2][1] * o0[1] + R[2][2] * o0[2]};
+  for (int i = 0; i < c.n_atoms; ++i)
+  {
+    const double* o = c.offsets[i];
+    rel[i] = make_double3(R[0][0] * o[0] + R[0][1] * o[1] + R[0][2] * o[2] - rc[0],
+                          R[1][0] * o[0] + R[1][1] * o[1] + R[1][2] * o[2] - rc[1],
+                          R[2][0] * o[0] + R[2][1] * o[1] + R[2][2] * o[2] - rc[2]);
+  }
 }
 
 // the atoms of component c with its starting bead at `first`, orientation from (kind, t)
@@ -658,6 +713,24 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
   const int kchunk = (p.nk + G - 1) / G, k0 = blockIdx.x * kchunk, k1 = min(p.nk, k0 + kchunk);
   const long long move0 = *p.move_base;
   __shared__ const double* atomGrid[kMaxItems];
+  // this CTA's k-range and framework slice, kept in shared memory for the whole launch
+  for (int kk = tid; kk < k1 - k0; kk += kThreads)
+  {
+    sh.kv[kk] = p.kvec[k0 + kk];
+    sh.kt[kk] = p.temp[k0 + kk];
+    sh.ks[kk] = p.sk[k0 + kk];
+  }
+  if (p.n_fw > 0)
+  {
+    const int fchunk = (p.n_fw + G - 1) / G, fa = min(p.n_fw, static_cast<int>(blockIdx.x) * fchunk);
+    const int nf = min(min(p.n_fw, fa + fchunk) - fa, kFwSlice);
+    const Dyn dy = dynOf(p);
+    for (int i = tid; i < nf; i += kThreads)
+    {
+      dy.fws[i] = p.fwx[fa + i];
+      dy.fwq[i] = p.fwq[fa + i];
+    }
+  }
   __syncthreads();
   if (sh.fail) return;
   for (int mv = 0; mv < moves; ++mv)
@@ -775,8 +848,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
           for (int kk = tid; kk < k1 - k0; kk += kThreads)
           {
             const double2 d = sh.dk[0][kk];
-            p.sk[k0 + kk].x += d.x;
-            p.sk[k0 + kk].y += d.y;
+            sh.ks[kk].x += d.x;
+            sh.ks[kk].y += d.y;
           }
       }
       ran = true;
@@ -799,6 +872,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
         sh.nta = p.k1;
         sh.ncand = 0;
       }
+      // the orientations depend only on the move: their offsets are computed now, by threads of another warp
+      if (tid >= 32 && tid < 32 + p.k2) orientationOffsets(p, cc, move, kKindOrient, tid - 32, sh.rel[tid - 32]);
       __syncthreads();
       if (!phase(p, sh, -1, atomGrid)) break;
       if (tid < 32)
@@ -827,9 +902,11 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
         if (tid < p.k2)
         {
           double3 x[kMaxAtoms];
-          orientedMolecule(p, cc, sh.first, move, kKindOrient, tid, x);
+          const double3 f = sh.first;
           for (int i = 0; i < na; ++i)
           {
+            const double3 r = sh.rel[tid][i];
+            x[i] = make_double3(f.x + r.x, f.y + r.y, f.z + r.z);
             sh.cpos[tid][i] = x[i];
             sh.cq[tid][i] = cc.charges[i];
           }
@@ -885,8 +962,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
             for (int kk = tid; kk < k1 - k0; kk += kThreads)
             {
               const double2 d = sh.dk[sh.selOrient][kk];
-              p.sk[k0 + kk].x += d.x;
-              p.sk[k0 + kk].y += d.y;
+              sh.ks[kk].x += d.x;
+              sh.ks[kk].y += d.y;
             }
         }
       }
@@ -908,22 +985,29 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
         atomGrid[tid] = cc.vdw_grid[sb];
         sh.logq[tid] = cc.prop_cdf ? log(proposalDensity(p, cc, r)) : 0.0;
       }
-      if (tid == 0)
+      // list state and positions the update needs, read by threads of an idle warp in parallel
       {
-        const int last = sh.n - 1;
-        sh.preSlot = __ldcg(p.slot + m);
-        sh.preLastC = __ldcg(p.list + c * p.capacity + sh.count[c] - 1);
-        sh.preCl = __ldcg(p.comp_of + last);
-        sh.preSl = __ldcg(p.slot + last);
-        for (int i = 0; i < na; ++i) sh.preLast[i] = loadPos(p, last * na + i);
-        for (int i = 0; i < na; ++i)
+        const int last = sh.n - 1, q = tid - 128;
+        if (q == 0)
         {
-          sh.cpos[0][i] = loadPos(p, m * na + i);
-          sh.cq[0][i] = -cc.charges[i];
+          sh.preSlot = __ldcg(p.slot + m);
+          sh.cn[0] = na;
+          sh.nta = p.k1 + p.k2 * (na - 1);
+          sh.ncand = p.use_charge ? 1 : 0;
         }
-        sh.cn[0] = na;
-        sh.nta = p.k1 + p.k2 * (na - 1);
-        sh.ncand = p.use_charge ? 1 : 0;
+        else if (q == 1)
+          sh.preLastC = __ldcg(p.list + c * p.capacity + sh.count[c] - 1);
+        else if (q == 2)
+          sh.preCl = __ldcg(p.comp_of + last);
+        else if (q == 3)
+          sh.preSl = __ldcg(p.slot + last);
+        else if (q >= 4 && q < 4 + na)
+          sh.preLast[q - 4] = loadPos(p, last * na + (q - 4));
+        else if (q >= 8 && q < 8 + na)
+        {
+          sh.cpos[0][q - 8] = loadPos(p, m * na + (q - 8));
+          sh.cq[0][q - 8] = -cc.charges[q - 8];
+        }
       }
       // retrace orientations about the old first bead, one per thread (trial 0: the molecule itself)
       if (tid < p.k2)
@@ -996,8 +1080,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
           for (int kk = tid; kk < k1 - k0; kk += kThreads)
           {
             const double2 d = sh.dk[0][kk];
-            p.sk[k0 + kk].x += d.x;
-            p.sk[k0 + kk].y += d.y;
+            sh.ks[kk].x += d.x;
+            sh.ks[kk].y += d.y;
           }
       }
       ran = true;
@@ -1129,8 +1213,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
             for (int kk = tid; kk < k1 - k0; kk += kThreads)
             {
               const double2 d = sh.dk[sh.selOrient][kk];
-              p.sk[k0 + kk].x += d.x;
-              p.sk[k0 + kk].y += d.y;
+              sh.ks[kk].x += d.x;
+              sh.ks[kk].y += d.y;
             }
         }
         c = oldC;
@@ -1149,6 +1233,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
     }
     __syncthreads();
   }
+  for (int kk = tid; kk < k1 - k0; kk += kThreads) p.sk[k0 + kk] = sh.ks[kk];
   if (blockIdx.x == 0 && tid == 0 && !sh.fail)
   {
     p.n_state[0] = sh.n;
@@ -1384,7 +1469,7 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
     for (int d = 0; d < 3; ++d) p.km[d] = kmax[d];
   }
   p.tabK = 1 + std::max({p.km[0], p.km[1], p.km[2]});
-  x->smem = sizeof(double2) * kMaxCand * kMaxCandAtoms * 3 * static_cast<size_t>(p.tabK);
+  x->smem = dynBytes(p.tabK);
   // launch geometry: one CTA per SM, co-resident
   int sms = 0, perSM = 0;
   cudaError_t err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);

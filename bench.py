@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-vs-uniform proposal section")
     ap.add_argument("--no-alkane", action="store_true", help="skip the batched flexible-chain CBMC section")
     ap.add_argument("--no-mixture", action="store_true", help="skip the large two-component system section")
+    ap.add_argument("--no-paths", action="store_true", help="skip the trial-energy and Ewald C-ABI section")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the cpu_baseline sample")
     return ap.parse_args()
 
@@ -516,6 +517,196 @@ def run_learned(args, ctx, world, rank, dist, torch):
     return out
 
 
+PATH_INSERTIONS = 200   # CBMC insertions whose trial sets go through rg_cbmc_external_energies, per precision
+PATH_DELTAS = 1000      # Ewald Fourier differences through rg_ewald_delta, per box
+PATH_FULL = 20          # full structure-factor recomputes through rg_ewald_full
+EWALD_FLOPS_PER_TERM = 16  # one (atom, k) term of the full recompute: two complex products + a complex multiply-add
+
+
+def run_paths(args, ctx, world, rank, dist, torch):
+    """Paths (b) and (c) on their own, through their C-ABI entry points with host buffers, on the configuration-5
+    system (18,432 framework atoms, 2,000 CO2 + 2,000 N2, Ewald kmax 12: 8,124 k-vectors):
+    (b) the trial sets of one CBMC insertion of CO2 (10 first-bead C positions, then 10 orientations whose two O atoms
+        are the trial atoms), each trial atom against the grids and the 12,000 adsorbate sites, in FP64 and FP32C;
+    (c) the Ewald Fourier difference of a CO2 translation (3 new + 3 old atoms) at the configuration-5 box and at the
+        configuration-2 box (1,152 k-vectors), and the full recompute of the configuration-5 structure factors."""
+    from raspa3_b200 import native
+    from raspa3_b200.forcefield import make_atoms
+    from raspa3_b200.mixture import config5, molecules_as_atoms
+    from raspa3_b200.synthetic import (CO2_NAMES, CO2_OFFSETS, random_molecules, random_rotation, replicate,
+                                       rigid_molecule, synthetic_forcefield, synthetic_framework)
+
+    d = config5(ctx, torch)
+    ff, comps, sysg, ew = d["ff"], d["components"], d["system"], d["ewald"]
+    atoms = molecules_as_atoms(ff, comps, d["xyz"], d["comp"])
+    n_mol = len(d["comp"])
+    sysg.set_molecules(atoms)
+    rng = np.random.default_rng(17)
+    q_c = float(ff.pseudo_atoms[ff.index("C_co2")].charge)
+    inserts = []
+    for _ in range(PATH_INSERTIONS):
+        first = make_atoms(rng.random((10, 3)) @ d["cell"], ff.index("C_co2"), q_c, molecule_ids=np.full(10, n_mol))
+        centre = first[int(rng.integers(10))]
+        c = np.array([centre["x"], centre["y"], centre["z"]])
+        orient = np.concatenate([rigid_molecule(ff, CO2_NAMES, CO2_OFFSETS, c, random_rotation(rng), n_mol)
+                                 for _ in range(10)])
+        inserts.append((first, orient))
+    trial_atoms = 10 + 10 * 2
+    stream = torch.cuda.current_stream()
+    out = {"workload": "configuration 5: 18,432 framework atoms, 12,000 adsorbate sites, grids for every adsorbate "
+                       "type, Ewald alpha 0.265 kmax 12 (8,124 k)"}
+
+    def time_trials():
+        for first, orient in inserts[:3]:
+            sysg.external_energies(first, 1)
+            sysg.external_energies(orient, 3, skip=1)
+        dev = 0.0
+        t0 = time.perf_counter()
+        for first, orient in inserts:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sysg.external_energies(first, 1)
+            sysg.external_energies(orient, 3, skip=1)
+            e1.record(stream)
+            e1.synchronize()
+            dev += e0.elapsed_time(e1) / 1e3
+        return time.perf_counter() - t0, dev
+
+    trials = {}
+    for name, prec in (("fp64", native.PRECISION_FP64), ("fp32c", native.PRECISION_FP32C)):
+        sysg.set_precision(prec)
+        wall, dev = time_trials()
+        tests = PATH_INSERTIONS * trial_atoms * len(atoms)
+        trials[name] = {"insertions_per_s": PATH_INSERTIONS / wall, "pair_tests_per_s": tests / wall,
+                        "device_pair_tests_per_s": tests / dev, "ms_per_insertion": 1e3 * wall / PATH_INSERTIONS}
+    sysg.set_precision(native.PRECISION_FP64)
+    out["trial_energies"] = {
+        "metric": "CBMC trial-atom x partner pair tests/s through rg_cbmc_external_energies", "unit": "pair tests/s",
+        "value": trials["fp32c"]["pair_tests_per_s"], "per_precision": trials,
+        "per_insertion": "10 first-bead sets of 1 atom + 10 orientation sets of 2 atoms, 12,000 partners each, two "
+                         "calls with host buffers",
+        "e2e": {"value": trials["fp32c"]["pair_tests_per_s"], "unit": "pair tests/s",
+                "h2d_bytes_per_step": trial_atoms * 64 + 20 * 64, "d2h_bytes_per_step": 20 * 104}}
+
+    # (c) Fourier differences: configuration 5 and configuration 2
+    ew.full(atoms, np.full(n_mol, 3, dtype=np.int32))
+    ff2 = synthetic_forcefield(charges=True, alpha=0.265, kmax=8)
+    ucell2, ufw2 = synthetic_framework(ff2, seed=42)
+    cell2, fw2 = replicate(ucell2, ufw2, (2, 2, 3))
+    ew2 = native.Ewald(ctx, ff2, cell2)
+    ew2.set_framework(fw2)
+    ads2 = random_molecules(ff2, cell2, 30, seed=8)
+    ew2.full(ads2, np.full(30, 3, dtype=np.int32))
+
+    def moves(a, n, count):
+        mv = []
+        for _ in range(count):
+            m = int(rng.integers(n))
+            old = a[3 * m:3 * m + 3].copy()
+            new = old.copy()
+            step = (rng.random(3) - 0.5) * 2.0
+            new["x"] += step[0]
+            new["y"] += step[1]
+            new["z"] += step[2]
+            mv.append((new, old))
+        return mv
+
+    deltas = {}
+    for name, e_, a_, n_ in (("config5", ew, atoms, n_mol), ("config2", ew2, ads2, 30)):
+        mv = moves(a_, n_, PATH_DELTAS)
+        for new, old in mv[:10]:
+            e_.delta(new, old)
+        t0 = time.perf_counter()
+        for new, old in mv:
+            e_.delta(new, old)
+        wall = time.perf_counter() - t0
+        nk = e_.n_kvectors
+        deltas[name] = {"n_kvectors": nk, "deltas_per_s": PATH_DELTAS / wall, "us_per_delta": 1e6 * wall / PATH_DELTAS,
+                        "algorithmic_bytes_per_delta": 40 * nk,
+                        "achieved_gbs": 40 * nk * PATH_DELTAS / wall / 1e9}
+    # full recompute of configuration 5 (adsorbates on top of the rigid framework structure factor)
+    sizes = np.full(n_mol, 3, dtype=np.int32)
+    for _ in range(2):
+        ew.full(atoms, sizes)
+    t0 = time.perf_counter()
+    for _ in range(PATH_FULL):
+        ew.full(atoms, sizes)
+    full_s = (time.perf_counter() - t0) / PATH_FULL
+    terms = len(atoms) * ew.n_kvectors
+    peak64 = ctx.probe_fma_peak(native.PRECISION_FP64)
+    full_tf = terms * EWALD_FLOPS_PER_TERM / full_s / 1e12
+    out["ewald"] = {
+        "metric": "Ewald Fourier differences/s through rg_ewald_delta", "unit": "differences/s",
+        "value": deltas["config5"]["deltas_per_s"], "per_box": deltas,
+        "full_recompute": {"atoms": len(atoms), "n_kvectors": ew.n_kvectors, "ms": 1e3 * full_s,
+                           "terms_per_s": terms / full_s, "tflops": full_tf, "fp64_peak_tflops": peak64,
+                           "frac_of_fp64_peak": full_tf / peak64 if peak64 else None,
+                           "flops_per_term": EWALD_FLOPS_PER_TERM,
+                           "includes": "host packing of the atoms, their upload, both kernels and the host self / "
+                                       "exclusion sums"},
+        "note": "one difference reads S(k) and temp(k) and writes the trial S(k): 40 B per k, L2-resident at both "
+                "sizes (130 KB at 8,124 k), so a single difference is latency-bound and its GB/s is far below HBM"}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        from concurrent.futures import ThreadPoolExecutor
+
+        threads = os.cpu_count() or 1
+        host_grids = [None] * (ff.n_types + 1)
+        ctx.synchronize()
+        for idx, buf in zip(d["grid_types"], d["grids"]):
+            host_grids[idx] = buf.cpu().numpy()
+
+        def cpu_insertion(k):
+            first, orient = inserts[k % len(inserts)]
+            for t in range(10):
+                oracle.cbmc_framework_molecule(ff, d["cell"], np.zeros(0, dtype=atoms.dtype), first[t:t + 1],
+                                               ff.cutoff_framework_vdw, ff.cutoff_coulomb, grids=host_grids,
+                                               grid_dims=d["dims"], grid_cell=d["unit_cell"])
+                oracle.cbmc_intermolecular(ff, d["cell"], atoms, first[t:t + 1], ff.cutoff_molecule_vdw,
+                                           ff.cutoff_coulomb)
+            for t in range(10):
+                s3 = orient[3 * t:3 * t + 3]
+                oracle.cbmc_framework_molecule(ff, d["cell"], np.zeros(0, dtype=atoms.dtype), s3,
+                                               ff.cutoff_framework_vdw, ff.cutoff_coulomb, grids=host_grids,
+                                               grid_dims=d["dims"], grid_cell=d["unit_cell"], skip=1)
+                oracle.cbmc_intermolecular(ff, d["cell"], atoms, s3, ff.cutoff_molecule_vdw, ff.cutoff_coulomb,
+                                           skip=1)
+
+        t0 = time.perf_counter()
+        cpu_insertion(0)
+        one = time.perf_counter() - t0
+        per_thread = max(1, int(args.cpu_seconds / 2 / max(one, 1e-3)))
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as pool:
+            list(pool.map(cpu_insertion, range(threads * per_thread)))
+        secs = time.perf_counter() - t0
+        tests = threads * per_thread * trial_atoms * len(atoms)
+        out["trial_energies"]["cpu_baseline"] = {
+            "value": tests / secs, "unit": "pair tests/s", "cores": threads, "kind": "port",
+            "sample": f"{threads * per_thread} insertions' trial sets in {secs:.1f} s (FP64 oracle of "
+                      f"computeFrameworkMoleculeEnergy + computeInterMolecularEnergy, one insertion per thread)"}
+        # the oracle's Fourier difference, one core (a single system's move is serial in the reference)
+        cpu_d = {}
+        for name, ff_, cell_, a_, n_, fw_ in (("config5", ff, d["cell"], atoms, n_mol, d["framework"]),
+                                              ("config2", ff2, cell2, ads2, 30, fw2)):
+            s_rig = oracle.ewald_rigid(ff_, cell_, fw_)
+            _, stored = oracle.ewald_fourier_energy(ff_, cell_, a_, np.full(n_, 3, dtype=np.int32), s_rigid=s_rig)
+            mv = moves(a_, n_, 1000)
+            count = 0
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < args.cpu_seconds / 4:
+                new, old = mv[count % len(mv)]
+                oracle.ewald_delta(ff_, cell_, stored, new, old)
+                count += 1
+            cpu_d[name] = count / (time.perf_counter() - t0)
+        out["ewald"]["cpu_baseline"] = {
+            "value": cpu_d["config5"], "unit": "differences/s", "cores": 1, "kind": "port",
+            "per_box": cpu_d, "sample": "FP64 oracle of energyDifferenceEwaldFourier on one core, same moves"}
+    ew2.close()
+    return out
+
+
 def cpu_gcmc_rate(ff, cell, scell, sfw, dims, grids, outs, target_seconds):
     """The oracle GCMC (the reference's moves restated) on all host cores, one chain per core, same grids."""
     import oracle
@@ -718,6 +909,9 @@ def run_ours(args):
     # ---- one large two-component system on the whole GPU (configuration 5) ----
     if not args.no_mixture:
         line["mixture"] = run_mixture(args, ctx, world, rank, dist, torch)
+    # ---- paths (b) and (c) on their own through the C-ABI (configuration 5, and configuration 2 for the Ewald) ----
+    if not args.no_paths:
+        line["paths"] = run_paths(args, ctx, world, rank, dist, torch)
     # ---- learned vs uniform first-bead proposal at equal loading error (configuration 4) ----
     if not args.no_learned:
         del flush

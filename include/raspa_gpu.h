@@ -180,6 +180,10 @@ rg_status rg_system_set_grid(rg_system* system, int index, const rg_box* unit_ce
                              const double* data, int data_on_device);
 /* Uploads the adsorbate atoms (System::spanOfMoleculeAtoms, the moleculeAtoms of CBMC::GrowContext). */
 rg_status rg_system_set_molecules(rg_system* system, const rg_atom* atoms, int n_atoms);
+/* Arithmetic of rg_cbmc_external_energies for this system: RG_PRECISION_FP64 (the default) or RG_PRECISION_FP32C
+ * (FP32 pair terms from the FP64 minimum-image displacement, TwoSum-compensated FP32 sums per thread, FP64 totals;
+ * the grid branch stays FP64). */
+rg_status rg_system_set_precision(rg_system* system, int precision);
 /* Replaces CBMC::computeExternalNonOverlappingEnergies (src/raspakit/cbmc/interactions.cpp:54-179) and its callees
  * CBMC::computeFrameworkMoleculeEnergy (cbmc/interactions_framework_molecule.cpp:31-104) and
  * CBMC::computeInterMolecularEnergy (cbmc/interactions_intermolecular.cpp:22-95); called from the first-bead schemes

@@ -11,19 +11,24 @@
 // atoms from other molecules), and the per-trial totals are reduced in a fixed order by the last CTA of the trial.
 // Trial atoms with a grid (and not fractional) take the grid branch: one tricubic interpolation of their VDW grid and,
 // with charges, q times the unit-charge Ewald grid. A trial is flagged as overlapping if any VDW pair energy or
-// interpolated VDW energy exceeds the overlap criterion, which is the reference's std::nullopt. Arithmetic is FP64:
-// these launches are latency-bound and FP64 keeps them exact against the FP64 path.
+// interpolated VDW energy exceeds the overlap criterion, which is the reference's std::nullopt. Arithmetic: FP64 by
+// default; with RG_PRECISION_FP32C (rg_system_set_precision) the pair terms are FP32 from the FP64 minimum-image
+// displacement and each thread sums them in TwoSum-compensated FP32 pairs, folded into the FP64 totals. The grid
+// branch stays FP64.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "common.cuh"
 #include "energy.cuh"
+#include "fastmath.cuh"
 
 namespace
 {
 constexpr int kThreads = 256;
-constexpr int kChunk = 2048;           // partner atoms per CTA
+constexpr int kMinChunk = 256;         // partner atoms per CTA at least (a call fills the GPU with smaller chunks)
+constexpr int kMaxChunk = 4096;         // and at most
 constexpr int kMaxTrialAtoms = 64;     // atoms of one trial set
 constexpr int kNumOut = 12;            // fmVDW, fmCharge, mmVDW, mmCharge, dudl VDW[4], dudl charge[4]
 }  // namespace
@@ -56,7 +61,10 @@ struct rg_system
   rg_trial_energy* out = nullptr;
   int out_cap = 0;
   rg_atom* trials_host = nullptr;     // pinned
-  rg_trial_energy* out_host = nullptr;  // pinned
+  rg_trial_energy* out_host = nullptr;    // mapped pinned: the last CTA of each trial writes its result here directly
+  rg_trial_energy* out_mapped = nullptr;  // device view of out_host
+  int precision = RG_PRECISION_FP64;      // of rg_cbmc_external_energies
+  int sms = 148;
 };
 
 namespace
@@ -79,12 +87,64 @@ struct TrialArgs
   int gnx, gny, gnz;
   double gic[3][3];
   int n_chunks;
+  int chunk;               // partner atoms per CTA
   int fw_partners;         // framework atoms scanned (0 if every trial atom has a grid)
   double* partial;         // [trial][chunk][kNumOut + 1]
   unsigned int* counters;  // per trial
   rg_trial_energy* out;
 };
 
+// FP32 forms of rgd::pairVDW / rgd::pairCoulomb: the same soft-core formulas (pair_vdw.ixx:85-101,
+// pair_coulomb.ixx:51-77) with the table entries rounded to FP32; erfc from the shared exp(-x^2).
+__device__ __forceinline__ float2 pairVDWf(const rgd::FF& ff, float sA, float sB, float rr, int tA, int tB)
+{
+  const int idx = tA * ff.n + tB;
+  if (!ff.lj[idx]) return make_float2(0.0f, 0.0f);
+  const float scaling = sA * sB;
+  const float arg1 = static_cast<float>(ff.eps4[idx]);
+  const float arg2 = static_cast<float>(ff.sig2[idx]);
+  const float arg3 = static_cast<float>(ff.shift[idx]);
+  const float temp = rr * rgd::rcpRn(arg2);
+  const float temp3 = temp * temp * temp;
+  const float inv_scaling = 1.0f - scaling;
+  const float rri3 = rgd::rcpRn(temp3 + 0.5f * inv_scaling * inv_scaling);
+  const float rri6 = rri3 * rri3;
+  const float term = arg1 * (rri3 * (rri3 - 1.0f)) - arg3;
+  const float dlambda_term = arg1 * scaling * inv_scaling * (2.0f * rri6 * rri3 - rri6);
+  return make_float2(scaling * term, term + dlambda_term);
+}
+
+__device__ __forceinline__ float2 pairCoulombf(const rgd::FF& ff, float sA, float sB, float r, double qA, double qB)
+{
+  const float scaling = sA * sB;
+  const float alpha = static_cast<float>(ff.alpha);
+  const float prefactor = static_cast<float>(ff.coul * qA * qB);
+  const float s = r + 0.01f * (1.0f - scaling);
+  const float inverseS = rgd::rcpRn(s);
+  const float inverseSS = inverseS * inverseS;
+  const float ex = expf(-alpha * alpha * s * s);
+  const float erfcTerm = rgd::erfcFromExp(alpha * s, ex);
+  const float gaussian = ex * 0.564189583547756f;
+  const float phi = erfcTerm * inverseS;
+  const float phiPrime = -(erfcTerm * inverseSS + 2.0f * alpha * gaussian * inverseS);
+  return make_float2(scaling * prefactor * phi, prefactor * (phi - scaling * 0.01f * phiPrime));
+}
+
+// FP32 sum with its rounding error carried exactly (Knuth TwoSum) in a second FP32 word
+struct Sum32
+{
+  float hi = 0.0f, lo = 0.0f;
+  __device__ __forceinline__ void add(float x)
+  {
+    const float t = hi + x;
+    const float z = t - hi;
+    lo += (hi - (t - z)) + (x - z);
+    hi = t;
+  }
+  __device__ __forceinline__ double value() const { return static_cast<double>(hi) + static_cast<double>(lo); }
+};
+
+template <bool F32>
 __global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a)
 {
   const int trial = blockIdx.x;
@@ -105,6 +165,7 @@ __global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a)
   double acc[kNumOut];
 #pragma unroll
   for (int c = 0; c < kNumOut; ++c) acc[c] = 0.0;
+  Sum32 acc32[F32 ? kNumOut : 1];
   double overlap = 0.0;
 
   // grid branch: one thread per trial atom, in chunk 0 only
@@ -129,8 +190,8 @@ __global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a)
   }
 
   const long long total = static_cast<long long>(a.fw_partners) + a.n_mol;
-  const long long begin = static_cast<long long>(chunk) * kChunk;
-  const long long end = begin + kChunk < total ? begin + kChunk : total;
+  const long long begin = static_cast<long long>(chunk) * a.chunk;
+  const long long end = begin + a.chunk < total ? begin + a.chunk : total;
   for (long long p = begin + threadIdx.x; p < end; p += blockDim.x)
   {
     const bool isFw = p < a.fw_partners;
@@ -150,26 +211,55 @@ __global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a)
       const double rr = dx * dx + dy * dy + dz * dz;
       const double rcv2 = isFw ? a.rcv_fw2 : a.rcv_mol2;
       const int gA = rgd::groupOf(A);
-      if (rr < rcv2)
+      if constexpr (F32)
       {
-        const double2 f = rgd::pairVDW(a.ff, B.scaling_vdw, A.scaling_vdw, rr, B.type, A.type);
-        if (f.x > a.ff.overlap) overlap = 1.0;
-        acc[isFw ? 0 : 2] += f.x;
-        // addDudlambdaVDW(groupIdA(partner), groupIdB(trial), ...) (running_energy.ixx:258-263)
-        if (gB != 0) acc[4 + gB - 1] += A.scaling_vdw * f.y;
-        if (gA != 0) acc[4 + gA - 1] += B.scaling_vdw * f.y;
+        const float rrf = static_cast<float>(rr);
+        if (rr < rcv2)
+        {
+          const float2 f = pairVDWf(a.ff, static_cast<float>(B.scaling_vdw), static_cast<float>(A.scaling_vdw), rrf,
+                                    B.type, A.type);
+          if (static_cast<double>(f.x) > a.ff.overlap) overlap = 1.0;
+          acc32[isFw ? 0 : 2].add(f.x);
+          if (gB != 0) acc32[4 + gB - 1].add(static_cast<float>(A.scaling_vdw) * f.y);
+          if (gA != 0) acc32[4 + gA - 1].add(static_cast<float>(B.scaling_vdw) * f.y);
+        }
+        if (a.ff.use_charge && rr < a.rcc2)
+        {
+          const float2 f = pairCoulombf(a.ff, static_cast<float>(B.scaling_coulomb), static_cast<float>(A.scaling_coulomb),
+                                        sqrtf(rrf), B.charge, A.charge);
+          acc32[isFw ? 1 : 3].add(f.x);
+          if (gB != 0) acc32[8 + gB - 1].add(static_cast<float>(A.scaling_coulomb) * f.y);
+          if (gA != 0) acc32[8 + gA - 1].add(static_cast<float>(B.scaling_coulomb) * f.y);
+        }
       }
-      if (a.ff.use_charge && rr < a.rcc2)
+      else
       {
-        const double r = sqrt(rr);
-        const double2 f = rgd::pairCoulomb(a.ff, B.scaling_coulomb, A.scaling_coulomb, r, B.charge, A.charge);
-        acc[isFw ? 1 : 3] += f.x;
-        if (gB != 0) acc[8 + gB - 1] += A.scaling_coulomb * f.y;
-        if (gA != 0) acc[8 + gA - 1] += B.scaling_coulomb * f.y;
+        if (rr < rcv2)
+        {
+          const double2 f = rgd::pairVDW(a.ff, B.scaling_vdw, A.scaling_vdw, rr, B.type, A.type);
+          if (f.x > a.ff.overlap) overlap = 1.0;
+          acc[isFw ? 0 : 2] += f.x;
+          // addDudlambdaVDW(groupIdA(partner), groupIdB(trial), ...) (running_energy.ixx:258-263)
+          if (gB != 0) acc[4 + gB - 1] += A.scaling_vdw * f.y;
+          if (gA != 0) acc[4 + gA - 1] += B.scaling_vdw * f.y;
+        }
+        if (a.ff.use_charge && rr < a.rcc2)
+        {
+          const double r = sqrt(rr);
+          const double2 f = rgd::pairCoulomb(a.ff, B.scaling_coulomb, A.scaling_coulomb, r, B.charge, A.charge);
+          acc[isFw ? 1 : 3] += f.x;
+          if (gB != 0) acc[8 + gB - 1] += A.scaling_coulomb * f.y;
+          if (gA != 0) acc[8 + gA - 1] += B.scaling_coulomb * f.y;
+        }
       }
     }
   }
 
+  if constexpr (F32)
+  {
+#pragma unroll
+    for (int c = 0; c < kNumOut; ++c) acc[c] += acc32[c].value();
+  }
   // block reduction (fixed order), then the last CTA of this trial sums the chunks in order
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -275,7 +365,10 @@ rg_status rg_system_create(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* b
   }
   if (!err) err = cudaStreamSynchronize(ctx->stream);
   if (!err) err = cudaMallocHost(reinterpret_cast<void**>(&s->trials_host), sizeof(rg_atom) * 4096);
-  if (!err) err = cudaMallocHost(reinterpret_cast<void**>(&s->out_host), sizeof(rg_trial_energy) * 4096);
+  if (!err)
+    err = cudaHostAlloc(reinterpret_cast<void**>(&s->out_host), sizeof(rg_trial_energy) * 4096, cudaHostAllocMapped);
+  if (!err) err = cudaHostGetDevicePointer(reinterpret_cast<void**>(&s->out_mapped), s->out_host, 0);
+  if (!err) err = cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, ctx->device);
   if (err)
   {
     rg_status st = rg::cudaFail(ctx, err, "rg_system_create");
@@ -377,6 +470,13 @@ rg_status rg_system_set_molecules(rg_system* s, const rg_atom* atoms, int n)
   return RG_OK;
 }
 
+rg_status rg_system_set_precision(rg_system* s, int precision)
+{
+  if (!s || (precision != RG_PRECISION_FP64 && precision != RG_PRECISION_FP32C)) return RG_ERR_INVALID_ARGUMENT;
+  s->precision = precision;
+  return RG_OK;
+}
+
 rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_trials, int atoms_per_trial, int skip,
                                     int64_t skip_background_molecule, double cutoff_framework_vdw,
                                     double cutoff_molecule_vdw, double cutoff_coulomb, rg_trial_energy* out)
@@ -401,7 +501,11 @@ rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_t
   }
   const int fw_partners = needFw ? s->n_fw : 0;
   const long long total = static_cast<long long>(fw_partners) + s->n_mol;
-  const int n_chunks = static_cast<int>(total > 0 ? (total + kChunk - 1) / kChunk : 1);
+  // chunks of partners: enough CTAs for about two per SM, each with at least kMinChunk partners
+  const long long want = (2LL * s->sms + n_trials - 1) / n_trials;
+  long long chunk = total > 0 ? (total + want - 1) / want : 1;
+  chunk = std::min<long long>(kMaxChunk, std::max<long long>(kMinChunk, chunk));
+  const int n_chunks = static_cast<int>(total > 0 ? (total + chunk - 1) / chunk : 1);
   rg_status st = growDevice(ctx, &s->trials, &s->trial_cap, nt_atoms);
   if (!st) st = growDevice(ctx, &s->partial, &s->partial_cap, n_trials * n_chunks * (kNumOut + 1));
   if (!st && s->counter_cap < n_trials)
@@ -409,7 +513,6 @@ rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_t
     st = growDevice(ctx, &s->counters, &s->counter_cap, n_trials);
     if (!st) RG_CUDA(ctx, cudaMemsetAsync(s->counters, 0, sizeof(unsigned int) * s->counter_cap, ctx->stream));
   }
-  if (!st) st = growDevice(ctx, &s->out, &s->out_cap, n_trials);
   if (st) return st;
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // pinned staging of the previous call is free again
   std::memcpy(s->trials_host, trials, sizeof(rg_atom) * nt_atoms);
@@ -437,15 +540,18 @@ rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_t
   for (int c = 0; c < 3; ++c)
     for (int r = 0; r < 3; ++r) a.gic[c][r] = s->gic[c][r];
   a.n_chunks = n_chunks;
+  a.chunk = static_cast<int>(chunk);
   a.fw_partners = fw_partners;
   a.partial = s->partial;
   a.counters = s->counters;
-  a.out = s->out;
+  a.out = s->out_mapped;
   dim3 grid(n_trials, n_chunks);
-  trialEnergyKernel<<<grid, kThreads, 0, ctx->stream>>>(a);
+  if (s->precision == RG_PRECISION_FP32C)
+    trialEnergyKernel<true><<<grid, kThreads, 0, ctx->stream>>>(a);
+  else
+    trialEnergyKernel<false><<<grid, kThreads, 0, ctx->stream>>>(a);
   RG_CUDA(ctx, cudaGetLastError());
-  RG_CUDA(ctx, cudaMemcpyAsync(s->out_host, s->out, sizeof(rg_trial_energy) * n_trials, cudaMemcpyDeviceToHost,
-                               ctx->stream));
+  // the last CTA of each trial wrote its result into mapped pinned memory: completion makes it visible here
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   std::memcpy(out, s->out_host, sizeof(rg_trial_energy) * n_trials);
   return RG_OK;

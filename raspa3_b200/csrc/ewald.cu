@@ -11,7 +11,11 @@
 // writes trial = stored + Delta rho; accepting swaps the two pointers instead of the reference's full vector copy.
 // The Fourier energy change per k is computed as temp*(2 Re(conj(S) dRho) + |dRho|^2), algebraically the reference's
 // temp*(|S + dRho|^2 - |S|^2) without the cancellation. Block partial sums are reduced in a fixed order by the last
-// block to finish (deterministic). Self, exclusion and net-charge terms are few-atom FP64 host sums.
+// block to finish (deterministic), which writes the totals straight into mapped pinned host memory. A move of up to 16
+// atoms travels in the launch's parameter block, so one difference costs one launch and one synchronisation. The full
+// recompute splits the atoms into chunks along a second grid dimension and sums the chunks' partial structure factors
+// in chunk order. Self, exclusion and net-charge terms are few-atom FP64 host sums.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -39,11 +43,14 @@ struct rg_ewald
   double2* trial = nullptr;    // nk*(1+G)
   double* partial = nullptr;   // per-block partial sums
   unsigned int* counter = nullptr;
-  double* result = nullptr;    // 1 + G doubles (+ spare)
+  double* result = nullptr;    // 1 + G doubles (+ spare): device view of result_host (mapped pinned memory)
+  double2* scratch = nullptr;  // full recompute: partial structure factors per atom chunk
+  size_t scratch_bytes = 0;
+  int sms = 148;
   void* moved = nullptr;       // moved-atom staging (device)
   size_t moved_bytes = 0;
   void* moved_host = nullptr;  // pinned staging
-  double* result_host = nullptr;
+  double* result_host = nullptr;  // mapped pinned: the kernels' last block writes the totals here directly
 };
 
 namespace
@@ -51,6 +58,7 @@ namespace
 constexpr int kThreads = 256;
 constexpr int kMaxGroups = 4;
 constexpr int kMaxMoved = 512;  // old + new atoms of one move (staged in shared memory)
+constexpr int kParamMoved = 16; // moves of up to this many atoms travel in the launch's parameter block
 
 struct MovedAtom
 {
@@ -59,6 +67,12 @@ struct MovedAtom
   double wg;     // sign * charge (dU/dlambda group sums)
   int group;     // 0 = none, 1..4
   int pad;
+};
+
+// the moved atoms of a small move, passed by value in the launch parameters (no copy before the launch)
+struct MovedParam
+{
+  MovedAtom a[kParamMoved];
 };
 
 __device__ __forceinline__ double2 phase(const char4 k, const double* s)
@@ -120,11 +134,12 @@ __global__ void __launch_bounds__(kThreads) ewaldDeltaKernel(int64_t nk, const c
                                                              const double* __restrict__ temp,
                                                              const double2* __restrict__ stored,
                                                              double2* __restrict__ trial,
-                                                             const MovedAtom* __restrict__ moved, int n_moved,
-                                                             double* partial, unsigned int* counter, double* result)
+                                                             const MovedAtom* __restrict__ moved, MovedParam small,
+                                                             int n_moved, double* partial, unsigned int* counter,
+                                                             double* result)
 {
   extern __shared__ MovedAtom sm[];
-  for (int a = threadIdx.x; a < n_moved; a += blockDim.x) sm[a] = moved[a];
+  for (int a = threadIdx.x; a < n_moved; a += blockDim.x) sm[a] = moved ? moved[a] : small.a[a];
   __syncthreads();
   double v[1 + G];
 #pragma unroll
@@ -177,28 +192,28 @@ __global__ void __launch_bounds__(kThreads) ewaldDeltaKernel(int64_t nk, const c
 constexpr int kFullTile = 32;
 
 template <int G>
-__global__ void __launch_bounds__(kThreads) ewaldFullKernel(int64_t nk, const char4* __restrict__ kvec,
-                                                            const double* __restrict__ temp,
-                                                            const double2* __restrict__ s_rigid,
-                                                            double2* __restrict__ stored,
-                                                            const MovedAtom* __restrict__ atoms, int n_atoms, int kxm,
-                                                            int kym, int kzm, int omit_inter, double* partial,
-                                                            unsigned int* counter, double* result)
+__global__ void __launch_bounds__(kThreads) ewaldFullPartialKernel(int64_t nk, const char4* __restrict__ kvec,
+                                                                   const MovedAtom* __restrict__ atoms, int n_atoms,
+                                                                   int chunk_atoms, int kxm, int kym, int kzm,
+                                                                   double2* __restrict__ scratch)
 {
+  // blockIdx.y: a chunk of atoms; each thread owns one k-vector and sums the chunk's atoms with two complex products
+  // per atom, from per-atom phase tables e^{i 2 pi m s_d} (m = 0..kmax_d) built in shared memory per tile
   extern __shared__ double2 tab[];  // kFullTile * (kxm+1 + kym+1 + kzm+1)
   __shared__ double wq[kFullTile], wgq[kFullTile];
   __shared__ int grp[kFullTile];
   const int stride = (kxm + 1) + (kym + 1) + (kzm + 1);
   const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int a0 = blockIdx.y * chunk_atoms, a1 = min(n_atoms, a0 + chunk_atoms);
   char4 kv = make_char4(0, 0, 0, 0);
   if (k < nk) kv = kvec[k];
   double2 acc = make_double2(0.0, 0.0);
   double2 accg[G > 0 ? G : 1];
 #pragma unroll
   for (int g = 0; g < (G > 0 ? G : 1); ++g) accg[g] = make_double2(0.0, 0.0);
-  for (int base = 0; base < n_atoms; base += kFullTile)
+  for (int base = a0; base < a1; base += kFullTile)
   {
-    const int na = min(kFullTile, n_atoms - base);
+    const int na = min(kFullTile, a1 - base);
     __syncthreads();
     for (int idx = threadIdx.x; idx < na * stride; idx += blockDim.x)
     {
@@ -243,11 +258,48 @@ __global__ void __launch_bounds__(kThreads) ewaldFullKernel(int64_t nk, const ch
       }
     }
   }
+  if (k < nk)
+  {
+    double2* out = scratch + (static_cast<int64_t>(blockIdx.y) * nk + k) * (1 + G);
+    out[0] = acc;
+#pragma unroll
+    for (int g = 0; g < G; ++g) out[1 + g] = accg[g];
+  }
+}
+
+// The chunks' partial structure factors summed in chunk order, the framework's added, the Fourier energy and its
+// dU/dlambda group terms (ewald.cpp:458-468), reduced in a fixed order by the last block.
+template <int G>
+__global__ void __launch_bounds__(kThreads) ewaldFullFinishKernel(int64_t nk, int n_chunks,
+                                                                  const double2* __restrict__ scratch,
+                                                                  const double* __restrict__ temp,
+                                                                  const double2* __restrict__ s_rigid,
+                                                                  double2* __restrict__ stored, int omit_inter,
+                                                                  double* partial, unsigned int* counter,
+                                                                  double* result)
+{
+  const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   double v[1 + G];
 #pragma unroll
   for (int c = 0; c < 1 + G; ++c) v[c] = 0.0;
   if (k < nk)
   {
+    double2 acc = make_double2(0.0, 0.0);
+    double2 accg[G > 0 ? G : 1];
+#pragma unroll
+    for (int g = 0; g < (G > 0 ? G : 1); ++g) accg[g] = make_double2(0.0, 0.0);
+    for (int c = 0; c < n_chunks; ++c)
+    {
+      const double2* in = scratch + (static_cast<int64_t>(c) * nk + k) * (1 + G);
+      acc.x += in[0].x;
+      acc.y += in[0].y;
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+      {
+        accg[g].x += in[1 + g].x;
+        accg[g].y += in[1 + g].y;
+      }
+    }
     const double t = temp[k];
     const double2 R = s_rigid[k];
     const double2 T = make_double2(R.x + acc.x, R.y + acc.y);
@@ -350,6 +402,24 @@ void addDud(double* arr, int gA, int gB, double sA, double sB, double factor)
   if (gB != 0) arr[gB - 1] += sA * factor;
 }
 
+// fractional coordinates and signed weights of the old (sign old_sign) and new atoms of a move
+void packMoved(const rg_ewald* e, const rg_atom* old_atoms, int n_old, const rg_atom* new_atoms, int n_new,
+               double old_sign, MovedAtom* h)
+{
+  for (int i = 0; i < n_old + n_new; ++i)
+  {
+    const bool isOld = i < n_old;
+    const rg_atom& a = isOld ? old_atoms[i] : new_atoms[i - n_old];
+    const double sign = isOld ? old_sign : 1.0;
+    double r[3] = {a.x, a.y, a.z};
+    rg::matvec(e->box.ic, r, h[i].s);
+    h[i].w = sign * a.scaling_coulomb * a.charge;
+    h[i].wg = sign * a.charge;
+    h[i].group = groupOf(a);
+    h[i].pad = 0;
+  }
+}
+
 rg_status stageAtoms(rg_ewald* e, const rg_atom* old_atoms, int n_old, const rg_atom* new_atoms, int n_new,
                      double old_sign)
 {
@@ -371,51 +441,62 @@ rg_status stageAtoms(rg_ewald* e, const rg_atom* old_atoms, int n_old, const rg_
     RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // the staging buffer of the previous call is free again
   }
   MovedAtom* h = static_cast<MovedAtom*>(e->moved_host);
-  for (int i = 0; i < n; ++i)
-  {
-    const bool isOld = i < n_old;
-    const rg_atom& a = isOld ? old_atoms[i] : new_atoms[i - n_old];
-    const double sign = isOld ? old_sign : 1.0;
-    double r[3] = {a.x, a.y, a.z};
-    rg::matvec(e->box.ic, r, h[i].s);
-    h[i].w = sign * a.scaling_coulomb * a.charge;
-    h[i].wg = sign * a.charge;
-    h[i].group = groupOf(a);
-    h[i].pad = 0;
-  }
+  packMoved(e, old_atoms, n_old, new_atoms, n_new, old_sign, h);
   if (n > 0) RG_CUDA(ctx, cudaMemcpyAsync(e->moved, h, sizeof(MovedAtom) * n, cudaMemcpyHostToDevice, ctx->stream));
   return RG_OK;
 }
 
 template <int G>
-cudaError_t launchDelta(rg_ewald* e, int n_moved)
+cudaError_t launchDelta(rg_ewald* e, int n_moved, const MovedParam* small)
 {
   const int blocks = static_cast<int>((e->nk + kThreads - 1) / kThreads);
   ewaldDeltaKernel<G><<<blocks, kThreads, sizeof(MovedAtom) * (n_moved > 0 ? n_moved : 1), e->ctx->stream>>>(
-      e->nk, e->kvec, e->temp, e->stored, e->trial, static_cast<const MovedAtom*>(e->moved), n_moved, e->partial,
-      e->counter, e->result);
+      e->nk, e->kvec, e->temp, e->stored, e->trial, small ? nullptr : static_cast<const MovedAtom*>(e->moved),
+      small ? *small : MovedParam{}, n_moved, e->partial, e->counter, e->result);
   return cudaGetLastError();
 }
 
 template <int G>
 cudaError_t launchFull(rg_ewald* e, int n_atoms)
 {
+  // atoms split into chunks so that k-blocks x chunks fill the GPU (about four CTAs per SM), at least one tile each
   const int blocks = static_cast<int>((e->nk + kThreads - 1) / kThreads);
+  const int maxChunks = std::max(1, (n_atoms + kFullTile - 1) / kFullTile);
+  const int chunks = std::min(maxChunks, std::max(1, (4 * e->sms + blocks - 1) / blocks));
+  const int chunkAtoms = std::max(kFullTile, (((n_atoms + chunks - 1) / chunks + kFullTile - 1) / kFullTile) * kFullTile);
+  const int n_chunks = n_atoms > 0 ? (n_atoms + chunkAtoms - 1) / chunkAtoms : 1;
+  const size_t need = sizeof(double2) * static_cast<size_t>(n_chunks) * e->nk * (1 + G);
+  if (e->scratch_bytes < need)
+  {
+    cudaError_t err = cudaStreamSynchronize(e->ctx->stream);
+    if (err) return err;
+    if (e->scratch) cudaFree(e->scratch);
+    e->scratch = nullptr;
+    e->scratch_bytes = 0;
+    err = cudaMalloc(reinterpret_cast<void**>(&e->scratch), need);
+    if (err) return err;
+    e->scratch_bytes = need;
+  }
   const int stride = (e->ff.kmax_x + 1) + (e->ff.kmax_y + 1) + (e->ff.kmax_z + 1);
   size_t shmem = sizeof(double2) * kFullTile * stride;
-  auto kern = ewaldFullKernel<G>;
+  auto kern = ewaldFullPartialKernel<G>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shmem));
-  kern<<<blocks, kThreads, shmem, e->ctx->stream>>>(e->nk, e->kvec, e->temp, e->s_rigid, e->stored,
-                                                   static_cast<const MovedAtom*>(e->moved), n_atoms, e->ff.kmax_x,
-                                                   e->ff.kmax_y, e->ff.kmax_z, e->omit_inter ? 1 : 0, e->partial,
-                                                   e->counter, e->result);
+  if (n_atoms > 0)
+    kern<<<dim3(blocks, n_chunks), kThreads, shmem, e->ctx->stream>>>(
+        e->nk, e->kvec, static_cast<const MovedAtom*>(e->moved), n_atoms, chunkAtoms, e->ff.kmax_x, e->ff.kmax_y,
+        e->ff.kmax_z, e->scratch);
+  else
+    cudaMemsetAsync(e->scratch, 0, need, e->ctx->stream);
+  ewaldFullFinishKernel<G><<<blocks, kThreads, 0, e->ctx->stream>>>(e->nk, n_chunks, e->scratch, e->temp, e->s_rigid,
+                                                                    e->stored, e->omit_inter ? 1 : 0, e->partial,
+                                                                    e->counter, e->result);
   return cudaGetLastError();
 }
 
 rg_status readResult(rg_ewald* e, double* out, int n)
 {
+  // the last block wrote the totals into mapped pinned memory: the stream's completion makes them visible here
   rg_ctx* ctx = e->ctx;
-  RG_CUDA(ctx, cudaMemcpyAsync(e->result_host, e->result, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   std::memcpy(out, e->result_host, sizeof(double) * n);
   return RG_OK;
@@ -485,8 +566,9 @@ rg_status rg_ewald_create(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* bo
   if (!err) err = alloc(reinterpret_cast<void**>(&e->trial), sizeof(double2) * nk * (1 + n_groups));
   if (!err) err = alloc(reinterpret_cast<void**>(&e->partial), sizeof(double) * blocks * (1 + kMaxGroups));
   if (!err) err = alloc(reinterpret_cast<void**>(&e->counter), sizeof(unsigned int) * 4);
-  if (!err) err = alloc(reinterpret_cast<void**>(&e->result), sizeof(double) * 8);
-  if (!err) err = cudaMallocHost(reinterpret_cast<void**>(&e->result_host), sizeof(double) * 8);
+  if (!err) err = cudaHostAlloc(reinterpret_cast<void**>(&e->result_host), sizeof(double) * 8, cudaHostAllocMapped);
+  if (!err) err = cudaHostGetDevicePointer(reinterpret_cast<void**>(&e->result), e->result_host, 0);
+  if (!err) err = cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, ctx->device);
   if (!err && e->nk > 0)
     err = cudaMemcpyAsync(e->kvec, kv.data(), sizeof(char4) * e->nk, cudaMemcpyHostToDevice, ctx->stream);
   if (!err && e->nk > 0)
@@ -516,7 +598,7 @@ rg_status rg_ewald_destroy(rg_ewald* e)
   cudaFree(e->trial);
   cudaFree(e->partial);
   cudaFree(e->counter);
-  cudaFree(e->result);
+  if (e->scratch) cudaFree(e->scratch);
   if (e->moved) cudaFree(e->moved);
   if (e->moved_host) cudaFreeHost(e->moved_host);
   if (e->result_host) cudaFreeHost(e->result_host);
@@ -659,19 +741,27 @@ rg_status rg_ewald_delta(rg_ewald* e, const rg_atom* new_atoms, int n_new, const
   double res[1 + kMaxGroups] = {0, 0, 0, 0, 0};
   if (e->nk > 0)
   {
-    rg_status st = stageAtoms(e, old_atoms, n_old, new_atoms, n_new, -1.0);
-    if (st) return st;
+    MovedParam small{};
+    const bool inParams = n <= kParamMoved;
+    if (inParams)
+      packMoved(e, old_atoms, n_old, new_atoms, n_new, -1.0, small.a);
+    else
+    {
+      rg_status st = stageAtoms(e, old_atoms, n_old, new_atoms, n_new, -1.0);
+      if (st) return st;
+    }
+    const MovedParam* sp = inParams ? &small : nullptr;
     cudaError_t err;
     switch (G)
     {
-      case 0: err = launchDelta<0>(e, n); break;
-      case 1: err = launchDelta<1>(e, n); break;
-      case 2: err = launchDelta<2>(e, n); break;
-      case 3: err = launchDelta<3>(e, n); break;
-      default: err = launchDelta<4>(e, n); break;
+      case 0: err = launchDelta<0>(e, n, sp); break;
+      case 1: err = launchDelta<1>(e, n, sp); break;
+      case 2: err = launchDelta<2>(e, n, sp); break;
+      case 3: err = launchDelta<3>(e, n, sp); break;
+      default: err = launchDelta<4>(e, n, sp); break;
     }
     if (err) return rg::cudaFail(ctx, err, "ewaldDeltaKernel");
-    st = readResult(e, res, 1 + G);
+    rg_status st = readResult(e, res, 1 + G);
     if (st) return st;
   }
   out->ewald_fourier = res[0];

@@ -140,6 +140,7 @@ def lib():
         L.rg_system_destroy.argtypes = [vp]
         L.rg_system_set_grid.argtypes = [vp, i32, P(RgBox), i32, i32, i32, vp, i32]
         L.rg_system_set_molecules.argtypes = [vp, vp, i32]
+        L.rg_system_set_precision.argtypes = [vp, i32]
         L.rg_cbmc_external_energies.argtypes = [vp, vp, i32, i32, i32, i64, d, d, d, vp]
         L.rg_gcmc_create.argtypes = [vp, vp, P(GcmcComponent), P(GcmcParams), i32, P(vp)]
         L.rg_gcmc_destroy.argtypes = [vp]
@@ -408,6 +409,10 @@ class System:
     def set_molecules(self, atoms):
         a, p = _atoms_ptr(atoms)
         check(self.ctx.handle, lib().rg_system_set_molecules(self.handle, p, len(a)), "rg_system_set_molecules")
+
+    def set_precision(self, precision: int):
+        """Arithmetic of external_energies: PRECISION_FP64 (default) or PRECISION_FP32C."""
+        check(self.ctx.handle, lib().rg_system_set_precision(self.handle, precision), "rg_system_set_precision")
 
     def external_energies(self, trials, atoms_per_trial: int, skip: int = -1, skip_background: int = -1,
                           cutoff_framework_vdw: float | None = None, cutoff_molecule_vdw: float | None = None,

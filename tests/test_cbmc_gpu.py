@@ -139,3 +139,40 @@ def test_skip_background_molecule(config2, oracle):
     got = c["sys"].external_energies(trial, 3, skip_background=2)
     ok, ref = oracle_trial(oracle, c, trial, skip_background=2)
     check(got[0], ok, ref)
+
+
+def test_fp32c_trial_energies(config2, oracle):
+    """RG_PRECISION_FP32C: FP32 pair terms from the FP64 minimum-image displacement, TwoSum-compensated FP32 sums.
+    Bound: a trial's energy (the sum of its framework / molecule, VDW / charge parts) agrees with the FP64 oracle within
+    1e-6 of the sum of the parts' magnitudes, and each VDW part within 1e-5 of itself. A charge part alone can be
+    further off relative to itself where +2.05 / -1.025 e terms cancel (measured up to 6e-4 for the framework charge of
+    a fractional molecule, whose pair loop runs over the charged framework atoms)."""
+    c = config2
+    ff = c["ff"]
+    rng = np.random.default_rng(23)
+    first = make_atoms(rng.random((20, 3)) @ c["scell"], ff.index("C_co2"), 0.70, molecule_ids=np.full(20, 30))
+    orient = [rigid_molecule(ff, CO2_NAMES, CO2_OFFSETS, rng.random(3) @ c["scell"], random_rotation(rng), 30)
+              for _ in range(10)]
+    frac = [rigid_molecule(ff, CO2_NAMES, CO2_OFFSETS, rng.random(3) @ c["scell"], random_rotation(rng), 31, lam=0.6,
+                           group=1, fractional=True) for _ in range(6)]
+    c["sys"].set_precision(native.PRECISION_FP32C)
+    try:
+        cases = [(c["sys"].external_energies(first, 1), [first[t:t + 1] for t in range(20)], -1),
+                 (c["sys"].external_energies(np.concatenate(orient), 3, skip=1), orient, 1),
+                 (c["sys"].external_energies(np.concatenate(frac), 3), frac, -1)]
+    finally:
+        c["sys"].set_precision(native.PRECISION_FP64)
+    n_ok = 0
+    for got, sets, skip in cases:
+        for g, s in zip(got, sets):
+            ok, ref = oracle_trial(oracle, c, s, skip=skip)
+            assert bool(g.overlap) == (not ok)
+            if not ok:
+                continue
+            n_ok += 1
+            scale = sum(abs(ref[k]) for k in FIELDS)
+            total = sum(getattr(g, k) for k in FIELDS)
+            assert abs(total - sum(ref[k] for k in FIELDS)) <= 1e-6 * max(1.0, scale), (total, ref)
+            for k in ("framework_vdw", "molecule_vdw"):
+                assert abs(getattr(g, k) - ref[k]) <= 1e-5 * max(1.0, abs(ref[k])), (k, getattr(g, k), ref[k])
+    assert n_ok >= 10

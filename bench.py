@@ -517,6 +517,52 @@ def run_learned(args, ctx, world, rank, dist, torch):
     return out
 
 
+VALIDATION_POINTS = 100000  # the reference's default NumberOfGridTestPoints (forcefield.ixx:172)
+
+
+def run_grid_validation(args, ctx, ff, cell, atoms, dims, outs, rank, world, native):
+    """The grid test that System::createFrameworkInterpolationGrids runs after each build, on the device: the C_co2
+    grid just built (FP32C) and its charge term (+0.70 e x the unit-charge Ewald grid) at 100,000 points of the 2x2x3
+    box, weighted as at 300 K. CPU baseline: the oracle of the same test on a sample of points, one core (the reference's
+    test is serial)."""
+    import torch
+
+    scell, _ = gcmc_setup(ff, cell, atoms)
+    probe = ff.index("C_co2")
+    kw = dict(probe_charge=0.70, weight_beta=1.0 / 300.0, n_points=VALIDATION_POINTS)
+    ctx.grid_validate(ff, cell, atoms, scell, probe, dims, outs[0].data_ptr(), outs[2].data_ptr(), seed=1, **kw)
+    reps = 5
+    t0 = time.perf_counter()
+    for r in range(reps):
+        res = ctx.grid_validate(ff, cell, atoms, scell, probe, dims, outs[0].data_ptr(), outs[2].data_ptr(), seed=2 + r,
+                                **kw)
+    secs = (time.perf_counter() - t0) / reps
+    out = {"metric": "grid test points/s through rg_grid_validate", "value": VALIDATION_POINTS / secs,
+           "unit": "points/s", "ms": 1e3 * secs, "points": VALIDATION_POINTS,
+           "energy_relative_error": res["energy_relative_error"],
+           "charge_energy_relative_error": res["charge_energy_relative_error"],
+           "gradient_relative_error": res["gradient_relative_error"],
+           "workload": "C_co2 FP32C grid of configuration 2 with its charge term, 2x2x3 box, weights at 300 K"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        torch.cuda.synchronize()
+        ctx.synchronize()
+        host = [outs[0].cpu().numpy(), outs[2].cpu().numpy()]
+        pts = np.random.default_rng(5).random((200, 3))
+        t0 = time.perf_counter()
+        oracle.grid_validate(ff, cell, atoms, scell, probe, dims, host[0], host[1], 0.70, 1.0 / 300.0, pts[:20])
+        one = (time.perf_counter() - t0) / 20
+        n = int(max(20, min(20000, args.cpu_seconds / 2 / max(one, 1e-6))))
+        pts = np.random.default_rng(5).random((n, 3))
+        t0 = time.perf_counter()
+        oracle.grid_validate(ff, cell, atoms, scell, probe, dims, host[0], host[1], 0.70, 1.0 / 300.0, pts)
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n / t, "unit": "points/s", "cores": 1, "kind": "port",
+                               "sample": f"{n} points in {t:.1f} s (FP64 oracle of the reference's grid test, one core)"}
+    return out
+
+
 PATH_INSERTIONS = 200   # CBMC insertions whose trial sets go through rg_cbmc_external_energies, per precision
 PATH_DELTAS = 1000      # Ewald Fourier differences through rg_ewald_delta, per box
 PATH_FULL = 20          # full structure-factor recomputes through rg_ewald_full
@@ -866,6 +912,9 @@ def run_ours(args):
         e2e_s = float(t.item())
     e2e_value = world * len(grids) * npts * e2e_steps / e2e_s
 
+    # the reference's grid test after the build (rg_grid_validate): 100,000 points on the C_co2 grid and its charge term
+    validation = run_grid_validation(args, ctx, ff, cell, atoms, dims, outs, rank, world, native)
+
     # roofline of the dominant kernel: algorithmic FLOPs = in-cutoff pairs x FLOPs per pair, per grid built
     mean_ms = [statistics.mean(k) for k in kern_ms]
     call_flops = [sum(stats[g]["pair_count"] * FLOPS_PER_PAIR["ewald" if grids[g][1] == 1 else "lj"] for g in idx)
@@ -899,6 +948,7 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps, "path": "rg_grid_build_set with pinned host outputs"},
         "gpu_launches": len(calls) * args.steps,
+        "grid_validation": validation,
     }
     # ---- GCMC steps/s on the same workload: CO2 in the 2x2x3 simulation box, the FP32C grids just built ----
     if not args.no_gcmc:

@@ -141,6 +141,36 @@ rg_status rg_grid_build_set(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* 
                             const int* grid_types, const int* probe_types, double* const* out_device,
                             double* const* out_host, rg_grid_stats* stats);
 
+/* Result of rg_grid_validate. sums[0..16]: the VDW term, sums[17..33]: the charge term (probe charge x unit-charge
+ * Ewald grid), each as: sum w, sum w E_table, sum w E_full, sum w (E_full - E_table)^2, sum w E_full^2, then per axis
+ * x, y, z: sum w G_table, sum w G_full, sum w (G_full - G_table)^2, sum w G_full^2 (energies in K, Cartesian gradients
+ * in K/Angstrom, w = exp(-weight_beta * E_full,vdw)). The derived fields are the Boltzmann averages and the relative
+ * errors sqrt(sum w diff^2 / sum w full^2) that the reference prints (NaN where a sum is zero). */
+typedef struct rg_grid_validation
+{
+  int64_t n_points;        /* points tested */
+  int64_t n_points_charge; /* points whose analytical VDW energy is below the overlap criterion (charge term) */
+  double sums[34];
+  double energy_table, energy_full, energy_relative_error;
+  double gradient_table[3], gradient_full[3], gradient_relative_error[3];
+  double charge_energy_table, charge_energy_full, charge_energy_relative_error;
+  double charge_gradient_table[3], charge_gradient_full[3], charge_gradient_relative_error[3];
+} rg_grid_validation;
+
+/* The grid test of System::createFrameworkInterpolationGrids (src/raspakit/system_interpolation_grids.cpp:240-651,
+ * tricubic scheme), which the reference runs serially after each grid build: at n_points points of the simulation
+ * box, the interpolated energy and gradient of the VDW grid of probe_type (a device buffer laid out as rg_grid_build
+ * writes it) against the analytical Lennard-Jones sum, and, with ewald_grid_device and a nonzero probe_charge, the
+ * charge term against the analytical real-space Ewald sum where the VDW energy is below ff->overlap_criteria. The
+ * points are `points` (3 fractions of the simulation box each, host memory) or, if NULL, drawn from `seed`.
+ * weight_beta multiplies the energy in K in the Boltzmann weight: the reference uses System::beta (1/(kB T) in
+ * inverse internal energy units) there; 1/T weights at temperature T. */
+rg_status rg_grid_validate(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* unit_cell, const rg_atom* unit_atoms,
+                           int n_unit_atoms, const rg_box* simulation_box, int probe_type, int nx, int ny, int nz,
+                           const double* vdw_grid_device, const double* ewald_grid_device, double probe_charge,
+                           double weight_beta, int64_t n_points, uint64_t seed, const double* points,
+                           rg_grid_validation* out);
+
 /* Grid build that allocates nothing, for callers that cannot allocate device memory: applications whose device memory
  * is owned by another allocator (a host framework that reserves the whole device up front, or a memory pool with a hard
  * budget) where any cudaMalloc by a library would fail or break the budget. No counterpart in the reference.

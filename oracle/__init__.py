@@ -86,6 +86,8 @@ def lib():
         L.oracle_tricubic_matrix.argtypes = [vp]
         L.oracle_grid_interpolate.argtypes = [vp, i32, i32, i32, P(OBox), vp]
         L.oracle_grid_interpolate.restype = d
+        L.oracle_grid_validate.argtypes = [P(OFF), P(OBox), vp, i32, P(OBox), i32, i32, i32, i32, vp, vp, d, d, vp,
+                                           ctypes.c_int64, vp]
         L.oracle_pair_vdw.argtypes = [P(OFF), d, d, d, i32, i32, vp]
         L.oracle_pair_coulomb.argtypes = [P(OFF), d, d, d, d, d, vp]
         L.oracle_cbmc_framework_molecule.argtypes = [P(OFF), P(OBox), vp, i32, i32, i32, P(OBox), vp, i32, d, d, vp,
@@ -182,6 +184,23 @@ def tricubic_matrix() -> np.ndarray:
     m = np.empty(64 * 64)
     lib().oracle_tricubic_matrix(_ptr(m))
     return m.reshape(64, 64)
+
+
+def grid_validate(ff, unit_cell, unit_atoms, simulation_cell, probe_type, dims, vdw_grid, ewald_grid, probe_charge,
+                  weight_beta, points):
+    """The grid test of System::createFrameworkInterpolationGrids (tricubic) at the given points (n x 3 fractions of
+    the simulation box): 36 values, the Boltzmann-weighted sums of the VDW (0..16) and charge (17..33) terms and the
+    two point counts."""
+    nx, ny, nz = dims
+    atoms = np.ascontiguousarray(unit_atoms)
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    vg = np.ascontiguousarray(vdw_grid, dtype=np.float64)
+    eg = None if ewald_grid is None else np.ascontiguousarray(ewald_grid, dtype=np.float64)
+    out = np.zeros(36)
+    lib().oracle_grid_validate(off(ff), obox(unit_cell), _ptr(atoms), len(atoms), obox(simulation_cell), probe_type,
+                               nx, ny, nz, _ptr(vg), _ptr(eg), probe_charge, weight_beta, _ptr(pts), len(pts),
+                               _ptr(out))
+    return out
 
 
 def interpolate(grid, dims, cell, pos) -> float:

@@ -444,10 +444,13 @@ const TricubicMatrix& tricubicMatrix()
   return tm;
 }
 
-double interpolateTricubic(const double* data, int nx, int ny, int nz, const Box& unit, const double* pos)
+// The 64 monomial coefficients of the cell holding pos and the local coordinates in it (InterpolationEnergyGrid::
+// interpolate, tricubic branch, interpolation_energy_grid.cpp:3980-4118; the same steps as interpolateHessian,
+// :4518-4571).
+void tricubicCoefficients(const double* data, int nx, int ny, int nz, const Box& unit, const double* pos, double a[64],
+                          double s[3])
 {
-  // InterpolationEnergyGrid::interpolate, tricubic branch (interpolation_energy_grid.cpp:3980-4118)
-  double sraw[3], s[3];
+  double sraw[3];
   matvec(unit.ic, pos, sraw);
   for (int d = 0; d < 3; ++d) s[d] = fract1(sraw[d]);
   const int ncx = nx - 1, ncy = ny - 1, ncz = nz - 1;
@@ -459,7 +462,7 @@ double interpolateTricubic(const double* data, int nx, int ny, int nz, const Box
   s[1] = (s[1] * static_cast<double>(ncy)) - static_cast<double>(y0);
   s[2] = (s[2] * static_cast<double>(ncz)) - static_cast<double>(z0);
   auto at = [&](int l, int64_t i, int64_t j, int64_t k) { return data[l + 8 * (i + nx * (j + ny * k))]; };
-  double X[64], a[64];
+  double X[64];
   for (int l = 0; l != 8; ++l)
   {
     X[8 * l + 0] = at(l, x0, y0, z0);
@@ -478,11 +481,41 @@ double interpolateTricubic(const double* data, int nx, int ny, int nz, const Box
     for (int q = T.start[r]; q < T.start[r + 1]; ++q) acc += T.nzv[q] * X[T.nzc[q]];
     a[r] = acc;
   }
+}
+
+double interpolateTricubic(const double* data, int nx, int ny, int nz, const Box& unit, const double* pos)
+{
+  double a[64], s[3];
+  tricubicCoefficients(data, nx, ny, nz, unit, pos, a, s);
   double value = 0.0;
   for (int k = 0; k != 4; ++k)
     for (int j = 0; j != 4; ++j)
       for (int i = 0; i != 4; ++i)
         value += a[i + 4 * j + 16 * k] * std::pow(s[0], i) * std::pow(s[1], j) * std::pow(s[2], k);
+  return value;
+}
+
+// Value and Cartesian gradient (InterpolationEnergyGrid::interpolateHessian, tricubic branch,
+// interpolation_energy_grid.cpp:4572-4590)
+double interpolateTricubicGradient(const double* data, int nx, int ny, int nz, const Box& unit, const double* pos,
+                                   double grad[3])
+{
+  double a[64], s[3];
+  tricubicCoefficients(data, nx, ny, nz, unit, pos, a, s);
+  const double nc[3] = {static_cast<double>(nx - 1), static_cast<double>(ny - 1), static_cast<double>(nz - 1)};
+  double value = 0.0, g[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k != 4; ++k)
+    for (int j = 0; j != 4; ++j)
+      for (int i = 0; i != 4; ++i)
+      {
+        const double c = a[i + 4 * j + 16 * k];
+        value += c * std::pow(s[0], i) * std::pow(s[1], j) * std::pow(s[2], k);
+        if (i > 0) g[0] += nc[0] * i * c * std::pow(s[0], i - 1) * std::pow(s[1], j) * std::pow(s[2], k);
+        if (j > 0) g[1] += nc[1] * j * c * std::pow(s[0], i) * std::pow(s[1], j - 1) * std::pow(s[2], k);
+        if (k > 0) g[2] += nc[2] * k * c * std::pow(s[0], i) * std::pow(s[1], j) * std::pow(s[2], k - 1);
+      }
+  // inverseCell^T * g: with M = inverseCell stored column-major (ic[col][row]), (M^T g)_a = sum_b ic[a][b] g_b
+  for (int a2 = 0; a2 < 3; ++a2) grad[a2] = unit.ic[a2][0] * g[0] + unit.ic[a2][1] * g[1] + unit.ic[a2][2] * g[2];
   return value;
 }
 
@@ -715,6 +748,64 @@ double oracle_grid_interpolate(const double* data, int nx, int ny, int nz, const
 {
   Box ub = makeBox(unit_box);
   return interpolateTricubic(data, nx, ny, nz, ub, pos);
+}
+
+void oracle_grid_validate(const off* ff, const obox* unit_box, const oatom* unit_atoms, int n_unit,
+                          const obox* simulation_box, int probe_type, int nx, int ny, int nz, const double* vdw_grid,
+                          const double* ewald_grid, double probe_charge, double weight_beta, const double* points,
+                          int64_t n_points, double* out)
+{
+  // System::createFrameworkInterpolationGrids, grid test of the tricubic scheme (system_interpolation_grids.cpp:272-651):
+  // at each point (fractions of the simulation box) the interpolated and the analytical energy and Cartesian gradient
+  // in K, Boltzmann weight exp(-weight_beta * E_vdw[K]); the charge term (probe charge x unit-charge Ewald grid) only
+  // where the analytical VDW energy is below the overlap criterion. out: the 34 weighted sums and the two counts.
+  const GridSetup gs = gridSetup(unit_box, unit_atoms, n_unit, ff->cutoff_framework_vdw, nx, ny, nz);
+  const Box sim = makeBox(simulation_box);
+  const double toK = energyConversionFactor() * kAvogadroConstant / kMolarGasConstant;
+  for (int i = 0; i < 36; ++i) out[i] = 0.0;
+  auto accumulate = [&](double* o, double w, double ei, double ef, const double* gi, const double* gf)
+  {
+    o[0] += w;
+    o[1] += ei * w;
+    o[2] += ef * w;
+    o[3] += (ef - ei) * (ef - ei) * w;
+    o[4] += ef * ef * w;
+    for (int a = 0; a < 3; ++a)
+    {
+      o[5 + a] += gi[a] * w;
+      o[8 + a] += gf[a] * w;
+      o[11 + a] += (gf[a] - gi[a]) * (gf[a] - gi[a]) * w;
+      o[14 + a] += gf[a] * gf[a] * w;
+    }
+  };
+  for (int64_t p = 0; p < n_points; ++p)
+  {
+    double pos[3];
+    matvec(sim.c, points + 3 * p, pos);
+    double gi[3], gf[3], d8[8];
+    double ei = interpolateTricubicGradient(vdw_grid, nx, ny, nz, gs.unit, pos, gi) * toK;
+    for (int a = 0; a < 3; ++a) gi[a] *= toK;
+    tricubicFractional(0, ff, gs.super, pos, probe_type, gs.unit, gs.atoms.data(), static_cast<int>(gs.atoms.size()),
+                       d8);
+    const double ef = d8[0] * toK;
+    for (int a = 0; a < 3; ++a)
+      gf[a] = (gs.unit.ic[a][0] * d8[1] + gs.unit.ic[a][1] * d8[2] + gs.unit.ic[a][2] * d8[3]) * toK;
+    const double w = std::exp(-weight_beta * ef);
+    accumulate(out, w, ei, ef, gi, gf);
+    out[34] += 1.0;
+    if (ewald_grid && probe_charge != 0.0 && ef < ff->overlap_criteria)
+    {
+      double ci[3], cf[3];
+      const double eci = interpolateTricubicGradient(ewald_grid, nx, ny, nz, gs.unit, pos, ci) * probe_charge * toK;
+      for (int a = 0; a < 3; ++a) ci[a] *= probe_charge * toK;
+      tricubicFractional(1, ff, gs.super, pos, 0, gs.unit, gs.atoms.data(), static_cast<int>(gs.atoms.size()), d8);
+      const double ecf = d8[0] * probe_charge * toK;
+      for (int a = 0; a < 3; ++a)
+        cf[a] = (gs.unit.ic[a][0] * d8[1] + gs.unit.ic[a][1] * d8[2] + gs.unit.ic[a][2] * d8[3]) * probe_charge * toK;
+      accumulate(out + 17, w, eci, ecf, ci, cf);
+      out[35] += 1.0;
+    }
+  }
 }
 
 void oracle_pair_vdw(const off* ff, double scaling_a, double scaling_b, double rr, int type_a, int type_b,

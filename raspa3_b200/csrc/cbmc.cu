@@ -275,29 +275,39 @@ __global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a)
     if (lane == 0) red[warp][c] = x;
   }
   __syncthreads();
+  // one thread per channel: the CTA's partial over the warps, then (last CTA) the trial's total over the chunks
+  const int c = threadIdx.x;
+  if (c <= kNumOut)
+  {
+    double x = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) x = (c < kNumOut) ? x + red[w][c] : fmax(x, red[w][c]);
+    a.partial[(static_cast<long long>(trial) * a.n_chunks + chunk) * (kNumOut + 1) + c] = x;
+    __threadfence();
+  }
+  __syncthreads();
   if (threadIdx.x == 0)
   {
-    double* dst = a.partial + (static_cast<long long>(trial) * a.n_chunks + chunk) * (kNumOut + 1);
-    for (int c = 0; c <= kNumOut; ++c)
-    {
-      double x = 0.0;
-      for (int w = 0; w < kThreads / 32; ++w) x = (c < kNumOut) ? x + red[w][c] : fmax(x, red[w][c]);
-      dst[c] = x;
-    }
-    __threadfence();
     const unsigned int done = atomicAdd(a.counters + trial, 1u);
     last = (done == static_cast<unsigned int>(a.n_chunks - 1));
   }
   __syncthreads();
-  if (last && threadIdx.x == 0)
+  if (!last) return;
+  __threadfence();
+  __shared__ double tot[kNumOut + 1];
+  if (c <= kNumOut)
   {
-    __threadfence();
-    double tot[kNumOut + 1];
-    for (int c = 0; c <= kNumOut; ++c) tot[c] = 0.0;
-    const volatile double* src = a.partial + static_cast<long long>(trial) * a.n_chunks * (kNumOut + 1);
+    const double* src = a.partial + static_cast<long long>(trial) * a.n_chunks * (kNumOut + 1);
+    double x = 0.0;
     for (int ch = 0; ch < a.n_chunks; ++ch)
-      for (int c = 0; c <= kNumOut; ++c)
-        tot[c] = (c < kNumOut) ? tot[c] + src[ch * (kNumOut + 1) + c] : fmax(tot[c], src[ch * (kNumOut + 1) + c]);
+    {
+      const double y = __ldcg(src + ch * (kNumOut + 1) + c);
+      x = (c < kNumOut) ? x + y : fmax(x, y);
+    }
+    tot[c] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
     rg_trial_energy o;
     o.framework_vdw = tot[0];
     o.framework_charge = tot[1];
@@ -514,7 +524,7 @@ rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_t
     if (!st) RG_CUDA(ctx, cudaMemsetAsync(s->counters, 0, sizeof(unsigned int) * s->counter_cap, ctx->stream));
   }
   if (st) return st;
-  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // pinned staging of the previous call is free again
+  // the pinned staging buffer is free: every call ends by synchronising the stream
   std::memcpy(s->trials_host, trials, sizeof(rg_atom) * nt_atoms);
   RG_CUDA(ctx, cudaMemcpyAsync(s->trials, s->trials_host, sizeof(rg_atom) * nt_atoms, cudaMemcpyHostToDevice,
                                ctx->stream));

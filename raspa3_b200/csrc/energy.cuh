@@ -172,6 +172,54 @@ __device__ __forceinline__ double interpolateCorner(const Grid& g, const GridCel
   return value;
 }
 
+// Value and Cartesian gradient of the interpolant (InterpolationEnergyGrid::interpolateHessian, tricubic branch,
+// interpolation_energy_grid.cpp:4518-4590): the same tensor-product Hermite form, differentiated along each local cell
+// coordinate t = s * (n - 1) - i0, then dE/ds = (n - 1) dE/dt and dE/dr_a = sum_b dE/ds_b * ic[a][b].
+__device__ __forceinline__ double interpolateGradient(const Grid& g, double px, double py, double pz, double grad[3])
+{
+  const GridCell cl = gridCell(g, px, py, pz);
+  double s[3];
+  s[0] = fract1(g.ic[0][0] * px + g.ic[1][0] * py + g.ic[2][0] * pz);
+  s[1] = fract1(g.ic[0][1] * px + g.ic[1][1] * py + g.ic[2][1] * pz);
+  s[2] = fract1(g.ic[0][2] * px + g.ic[1][2] * py + g.ic[2][2] * pz);
+  const int nc[3] = {g.nx - 1, g.ny - 1, g.nz - 1};
+  double dh[3][2][2];  // d/dt of the bases
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    const double t = s[d] * static_cast<double>(nc[d]) - static_cast<double>(cl.i0[d]), t2 = t * t;
+    dh[d][0][0] = 6.0 * t2 - 6.0 * t;
+    dh[d][1][0] = -6.0 * t2 + 6.0 * t;
+    dh[d][0][1] = 3.0 * t2 - 4.0 * t + 1.0;
+    dh[d][1][1] = 3.0 * t2 - 2.0 * t;
+  }
+  const int ox[8] = {0, 1, 0, 0, 1, 1, 0, 1};
+  const int oy[8] = {0, 0, 1, 0, 1, 0, 1, 1};
+  const int oz[8] = {0, 0, 0, 1, 0, 1, 1, 1};
+  double value = 0.0, dt[3] = {0.0, 0.0, 0.0};
+  for (int corner = 0; corner < 8; ++corner)
+  {
+    const int cx = corner & 1, cy = (corner >> 1) & 1, cz = (corner >> 2) & 1;
+    const double* p = g.data + 8 * (static_cast<long long>(cl.i0[0] + cx) +
+                                    static_cast<long long>(g.nx) * (static_cast<long long>(cl.i0[1] + cy) +
+                                                                   static_cast<long long>(g.ny) * (cl.i0[2] + cz)));
+#pragma unroll
+    for (int l = 0; l < 8; ++l)
+    {
+      const double v = p[l];
+      const double hx = cl.h[0][cx][ox[l]], hy = cl.h[1][cy][oy[l]], hz = cl.h[2][cz][oz[l]];
+      value += v * hx * hy * hz;
+      dt[0] += v * dh[0][cx][ox[l]] * hy * hz;
+      dt[1] += v * hx * dh[1][cy][oy[l]] * hz;
+      dt[2] += v * hx * hy * dh[2][cz][oz[l]];
+    }
+  }
+  const double ds[3] = {dt[0] * nc[0], dt[1] * nc[1], dt[2] * nc[2]};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) grad[a] = g.ic[a][0] * ds[0] + g.ic[a][1] * ds[1] + g.ic[a][2] * ds[2];
+  return value;
+}
+
 __device__ __forceinline__ double interpolate(const Grid& g, double px, double py, double pz)
 {
   const GridCell cl = gridCell(g, px, py, pz);

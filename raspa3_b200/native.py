@@ -112,6 +112,23 @@ class GridStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class GridValidation(ctypes.Structure):
+    _fields_ = [("n_points", ctypes.c_int64), ("n_points_charge", ctypes.c_int64), ("sums", ctypes.c_double * 34),
+                ("energy_table", ctypes.c_double), ("energy_full", ctypes.c_double),
+                ("energy_relative_error", ctypes.c_double), ("gradient_table", ctypes.c_double * 3),
+                ("gradient_full", ctypes.c_double * 3), ("gradient_relative_error", ctypes.c_double * 3),
+                ("charge_energy_table", ctypes.c_double), ("charge_energy_full", ctypes.c_double),
+                ("charge_energy_relative_error", ctypes.c_double), ("charge_gradient_table", ctypes.c_double * 3),
+                ("charge_gradient_full", ctypes.c_double * 3), ("charge_gradient_relative_error", ctypes.c_double * 3)]
+
+    def as_dict(self):
+        out = {}
+        for f, _ in self._fields_:
+            v = getattr(self, f)
+            out[f] = list(v) if isinstance(v, ctypes.Array) else v
+        return out
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -134,6 +151,8 @@ def lib():
         L.rg_probe_fma_peak.argtypes = [vp, i32, P(d), P(d)]
         L.rg_grid_build_set.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, d, i32, i32, i32, i32, i32, vp, vp, vp,
                                         vp, vp]
+        L.rg_grid_validate.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, P(RgBox), i32, i32, i32, i32, vp, vp, d,
+                                       d, i64, ctypes.c_uint64, vp, P(GridValidation)]
         L.rg_grid_build_noalloc.argtypes = [i32, vp, i32, P(RgForceField), P(RgBox), vp, i32, i32, d, i32, i32, i32,
                                             i32, vp, P(GridStats)]
         L.rg_system_create.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, P(vp)]
@@ -260,6 +279,28 @@ class Context:
                                  ctypes.byref(stats) if count_pairs else None)
         check(self.handle, st, "rg_grid_build")
         return out, (stats.as_dict() if count_pairs else None)
+
+    def grid_validate(self, ff: ForceField, unit_cell, unit_atoms: np.ndarray, simulation_cell, probe_type: int, dims,
+                      vdw_grid_device: int, ewald_grid_device: int | None = None, probe_charge: float = 0.0,
+                      weight_beta: float = 1.0 / 300.0, n_points: int = 100000, seed: int = 1, points=None) -> dict:
+        """The reference's grid test on the device (rg_grid_validate): Boltzmann-weighted sums, averages and relative
+        errors of the interpolated vs analytical energy and gradient. points: (n, 3) fractions of the simulation box,
+        or None for n_points Philox points from seed."""
+        nx, ny, nz = (int(v) for v in dims)
+        atoms = np.ascontiguousarray(unit_atoms, dtype=ATOM_DTYPE)
+        pts = None if points is None else np.ascontiguousarray(points, dtype=np.float64)
+        n = n_points if pts is None else len(pts)
+        out = GridValidation()
+        ffs, ubox, sbox = ff_struct(ff), box_struct(unit_cell), box_struct(simulation_cell)
+        st = lib().rg_grid_validate(self.handle, ctypes.byref(ffs), ctypes.byref(ubox),
+                                    ctypes.c_void_p(atoms.ctypes.data), len(atoms), ctypes.byref(sbox), probe_type,
+                                    nx, ny, nz,
+                                    ctypes.c_void_p(vdw_grid_device),
+                                    ctypes.c_void_p(ewald_grid_device) if ewald_grid_device else None, probe_charge,
+                                    weight_beta, n, seed, ctypes.c_void_p(pts.ctypes.data) if pts is not None else None,
+                                    ctypes.byref(out))
+        check(self.handle, st, "rg_grid_validate")
+        return out.as_dict()
 
     def grid_build_set(self, ff: ForceField, cell, unit_atoms: np.ndarray, cutoff: float, dims, precision: int,
                        grid_types, probe_types, out_device_ptrs, count_pairs: bool = False, out_host=None):

@@ -173,3 +173,59 @@ def test_grid_build_set_matches_single_builds(ctx, precision):
         np.testing.assert_array_equal(outs[g].cpu().numpy(), ref)
         np.testing.assert_array_equal(hosts[g], ref)
         assert stats[g]["pair_count"] == rs["pair_count"]
+
+
+def _close(d, o, scale, rel=1e-9):
+    return abs(d - o) <= rel * max(abs(o), scale, 1e-300)
+
+
+def test_grid_validation_matches_oracle(ctx, oracle):
+    """rg_grid_validate (the reference's grid test, system_interpolation_grids.cpp:240-651) on the device against the
+    oracle at the same 2,000 points: every Boltzmann-weighted sum of the C_co2 VDW grid and of its charge term (0.70 e
+    x the unit-charge Ewald grid), FP64 grids of the configuration-2 framework on a 0.5 A mesh in the 2x2x3 box.
+    Tolerance 1e-9 of each sum's scale (for a sum of w x, sqrt(sum w x^2 sum w))."""
+    torch = pytest.importorskip("torch")
+    from raspa3_b200.synthetic import replicate
+
+    ff = synthetic_forcefield(charges=True)
+    ucell, ufw = synthetic_framework(ff, seed=42)
+    scell, _ = replicate(ucell, ufw, (2, 2, 3))
+    dims = (41, 41, 28)
+    probe = ff.index("C_co2")
+    bufs = []
+    for gt, pr in ((0, probe), (1, 0)):
+        host, _ = ctx.grid_build(gt, ff, ucell, ufw, pr, 12.0, dims, native.PRECISION_FP64)
+        bufs.append((host, torch.from_numpy(host).cuda()))
+    pts = np.random.default_rng(7).random((2000, 3))
+    beta = 1.0 / 300.0
+    got = ctx.grid_validate(ff, ucell, ufw, scell, probe, dims, bufs[0][1].data_ptr(), bufs[1][1].data_ptr(), 0.70,
+                            beta, points=pts)
+    ref = oracle.grid_validate(ff, ucell, ufw, scell, probe, dims, bufs[0][0], bufs[1][0], 0.70, beta, pts)
+    assert got["n_points"] == ref[34] == 2000
+    assert got["n_points_charge"] == ref[35] > 100
+    s = got["sums"]
+    for base in (0, 17):
+        o = ref[base:base + 17]
+        assert _close(s[base], o[0], 0.0) and _close(s[base + 4], o[4], 0.0)
+        for i in (1, 2):
+            assert _close(s[base + i], o[i], np.sqrt(o[4] * o[0])), (base, i, s[base + i], o[i])
+        assert _close(s[base + 3], o[3], o[4]), (base, s[base + 3], o[3])
+        for a in range(3):
+            g2 = o[14 + a]
+            for i in (5 + a, 8 + a):
+                assert _close(s[base + i], o[i], np.sqrt(g2 * o[0])), (base, i, s[base + i], o[i])
+            assert _close(s[base + 11 + a], o[11 + a], g2), (base, a)
+            assert _close(s[base + 14 + a], o[14 + a], 0.0), (base, a)
+    # derived figures as the reference prints them
+    assert abs(got["energy_relative_error"] - np.sqrt(ref[3] / ref[4])) <= 1e-9 * np.sqrt(ref[3] / ref[4])
+    assert abs(got["charge_energy_table"] - ref[18] / ref[17]) <= 1e-9 * abs(ref[18] / ref[17])
+    # Philox points: the same seed gives the same result, another seed another sample
+    a = ctx.grid_validate(ff, ucell, ufw, scell, probe, dims, bufs[0][1].data_ptr(), bufs[1][1].data_ptr(), 0.70,
+                          beta, n_points=50000, seed=3)
+    b = ctx.grid_validate(ff, ucell, ufw, scell, probe, dims, bufs[0][1].data_ptr(), bufs[1][1].data_ptr(), 0.70,
+                          beta, n_points=50000, seed=3)
+    c = ctx.grid_validate(ff, ucell, ufw, scell, probe, dims, bufs[0][1].data_ptr(), bufs[1][1].data_ptr(), 0.70,
+                          beta, n_points=50000, seed=4)
+    assert a["sums"] == b["sums"] and a["n_points"] == 50000
+    assert a["sums"] != c["sums"]
+    assert abs(a["energy_relative_error"] - c["energy_relative_error"]) < 0.5 * a["energy_relative_error"]

@@ -1,0 +1,45 @@
+"""The oracle of the grid test (System::createFrameworkInterpolationGrids, system_interpolation_grids.cpp:240-651):
+both gradients it compares, the interpolant's (interpolateHessian) and the analytical one
+(calculateTricubicFractionalAtPosition mapped to Cartesian), agree with central finite differences of their energies.
+"""
+
+import numpy as np
+
+from raspa3_b200.forcefield import ENERGY_TO_KELVIN
+from raspa3_b200.synthetic import replicate, synthetic_forcefield, synthetic_framework
+
+
+def test_oracle_gradients_match_finite_differences(oracle):
+    ff = synthetic_forcefield(charges=True)
+    ucell, ufw = synthetic_framework(ff, seed=42)
+    scell, _ = replicate(ucell, ufw, (2, 2, 3))
+    dims = (21, 21, 14)
+    probe = ff.index("CH4")
+    grid = oracle.make_grid(0, ff, ucell, ufw, probe, 12.0, dims)
+    inv = np.linalg.inv(scell)
+    rng = np.random.default_rng(11)
+    h = 1e-5
+    checked = 0
+    for _ in range(400):
+        if checked == 4:
+            break
+        pos = rng.random(3) @ scell
+        one = oracle.grid_validate(ff, ucell, ufw, scell, probe, dims, grid, None, 0.0, 0.0, [pos @ inv])
+        if one[2] > 1e4:  # inside the framework (most of this dense cell for methane): skip steep overlap regions
+            continue
+        checked += 1
+        fd_table, fd_full = [], []
+        for a in range(3):
+            d = np.zeros(3)
+            d[a] = h
+            e_up = oracle.interpolate(grid, dims, ucell, pos + d)
+            e_dn = oracle.interpolate(grid, dims, ucell, pos - d)
+            fd_table.append((e_up - e_dn) / (2 * h) * ENERGY_TO_KELVIN)
+            up = oracle.grid_validate(ff, ucell, ufw, scell, probe, dims, grid, None, 0.0, 0.0, [(pos + d) @ inv])
+            dn = oracle.grid_validate(ff, ucell, ufw, scell, probe, dims, grid, None, 0.0, 0.0, [(pos - d) @ inv])
+            fd_full.append((up[2] - dn[2]) / (2 * h))
+        scale_t = max(1.0, np.abs(one[5:8]).max())
+        scale_f = max(1.0, np.abs(one[8:11]).max())
+        np.testing.assert_allclose(one[5:8], fd_table, rtol=0, atol=1e-5 * scale_t)
+        np.testing.assert_allclose(one[8:11], fd_full, rtol=0, atol=1e-5 * scale_f)
+    assert checked == 4

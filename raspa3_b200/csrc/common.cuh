@@ -25,6 +25,10 @@ struct rg_ctx
   std::vector<Slot> scratch;
   // Pinned host staging slots.
   std::vector<Slot> pinned;
+  // Second stream for device-to-host copies that overlap the work of `stream`, and events to order the two (created
+  // on first use).
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> events;
 };
 
 namespace rg
@@ -45,6 +49,11 @@ rg_status cudaFail(rg_ctx* ctx, cudaError_t err, const char* what);
 rg_status scratch(rg_ctx* ctx, int slot, size_t bytes, void** out);
 // Pinned host slot `slot` of at least `bytes`.
 rg_status pinnedScratch(rg_ctx* ctx, int slot, size_t bytes, void** out);
+// The context's copy stream and its event `i` (created on first use).
+rg_status copyStream(rg_ctx* ctx, cudaStream_t* out);
+rg_status event(rg_ctx* ctx, int i, cudaEvent_t* out);
+// Makes the context stream wait for everything queued on the copy stream so far.
+rg_status joinCopies(rg_ctx* ctx);
 
 struct HostBox
 {

@@ -19,6 +19,36 @@ rg_status cudaFail(rg_ctx* ctx, cudaError_t err, const char* what)
   return fail(ctx, err == cudaErrorMemoryAllocation ? RG_ERR_OUT_OF_MEMORY : RG_ERR_CUDA, msg);
 }
 
+rg_status copyStream(rg_ctx* ctx, cudaStream_t* out)
+{
+  if (!ctx->copy_stream) RG_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  *out = ctx->copy_stream;
+  return RG_OK;
+}
+
+rg_status event(rg_ctx* ctx, int i, cudaEvent_t* out)
+{
+  while (static_cast<int>(ctx->events.size()) <= i)
+  {
+    cudaEvent_t e = nullptr;
+    RG_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ctx->events.push_back(e);
+  }
+  *out = ctx->events[i];
+  return RG_OK;
+}
+
+rg_status joinCopies(rg_ctx* ctx)
+{
+  if (!ctx->copy_stream) return RG_OK;
+  cudaEvent_t e = nullptr;
+  rg_status st = event(ctx, 0, &e);
+  if (st) return st;
+  RG_CUDA(ctx, cudaEventRecord(e, ctx->copy_stream));
+  RG_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, e, 0));
+  return RG_OK;
+}
+
 rg_status scratch(rg_ctx* ctx, int slot, size_t bytes, void** out)
 {
   if (static_cast<int>(ctx->scratch.size()) <= slot) ctx->scratch.resize(slot + 1);
@@ -136,6 +166,12 @@ rg_status rg_ctx_destroy(rg_ctx* ctx)
     if (s.ptr) cudaFree(s.ptr);
   for (auto& s : ctx->pinned)
     if (s.ptr) cudaFreeHost(s.ptr);
+  if (ctx->copy_stream)
+  {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
+  for (cudaEvent_t e : ctx->events) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return RG_OK;

@@ -17,6 +17,7 @@
 // Precisions: FP64 throughout; or FP32C — coordinates relative to the brick centre kept as double-float (hi, lo) FP32
 // pairs so that each displacement is rounded to FP32 once, FP32 pair terms, FP32 partial sums per staged chunk folded into a compensated (TwoSum) hi/lo FP32 pair, and an
 // FP64 epilogue.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -46,6 +47,7 @@ struct GridParams
   double overlap;
   unsigned long long* pair_count;
   double* out[2];  // one output grid per Lennard-Jones probe sharing the candidate set (out[0] otherwise)
+  int zb0, zb1;    // bricks along z launched: [zb0, zb1) (zb1 == 0: all)
 };
 
 __device__ __forceinline__ double rcpRn(double x) { return __drcp_rn(x); }
@@ -250,7 +252,8 @@ __global__ void __launch_bounds__(256, (NP == 2 && sizeof(Real) == 4) ? 3 : 1) g
 
   const int tid = threadIdx.x;
   const int lx = tid % bx, ly = (tid / bx) % by, lz = tid / (bx * by);
-  const int i = blockIdx.x * bx + lx, j = blockIdx.y * by + ly, k = blockIdx.z * bz + lz;
+  const int kb = static_cast<int>(blockIdx.z) + p.zb0;  // brick index along z
+  const int i = blockIdx.x * bx + lx, j = blockIdx.y * by + ly, k = kb * bz + lz;
   const bool valid = (i < p.nx) && (j < p.ny) && (k < p.nz) && (lz < bz);
 
   // grid point (interpolation_energy_grid.cpp:3827-3829): s = (i,j,k)*delta, pos = cell * s
@@ -261,7 +264,7 @@ __global__ void __launch_bounds__(256, (NP == 2 && sizeof(Real) == 4) ? 3 : 1) g
   for (int r = 0; r < 3; ++r) pos[r] = p.cell[0][r] * s[0] + p.cell[1][r] * s[1] + p.cell[2][r] * s[2];
   // brick centre
   double sc[3] = {(blockIdx.x * bx + 0.5 * (bx - 1)) * p.delta[0], (blockIdx.y * by + 0.5 * (by - 1)) * p.delta[1],
-                  (blockIdx.z * bz + 0.5 * (bz - 1)) * p.delta[2]};
+                  (kb * bz + 0.5 * (bz - 1)) * p.delta[2]};
   double ctr[3];
 #pragma unroll
   for (int r = 0; r < 3; ++r) ctr[r] = p.cell[0][r] * sc[0] + p.cell[1][r] * sc[1] + p.cell[2][r] * sc[2];
@@ -496,7 +499,8 @@ template <typename Real, int TYPE, bool TRI, int NP = 1>
 cudaError_t launchTyped(const GridParams& p, const double4* ipos, const double4* ipar, int bx, int by, int bz,
                         bool count, cudaStream_t stream)
 {
-  dim3 grid((p.nx + bx - 1) / bx, (p.ny + by - 1) / by, (p.nz + bz - 1) / bz);
+  const int zbricks = p.zb1 > p.zb0 ? p.zb1 - p.zb0 : (p.nz + bz - 1) / bz;
+  dim3 grid((p.nx + bx - 1) / bx, (p.ny + by - 1) / by, zbricks);
   int nt = bx * by * bz;
   size_t shmem = ((1 + NP) * sizeof(typename Vec4<Real>::T) + (sizeof(Real) == 4 ? sizeof(float4) : 0)) *
                  static_cast<size_t>(nt) * kPer;
@@ -530,6 +534,49 @@ cudaError_t launchPrec(int type, const GridParams& p, const double4* ipos, const
     default:
       return launchTyped<Real, RG_GRID_LENNARD_JONES_ATTRACTION, TRI>(p, ipos, ipar, bx, by, bz, count, stream);
   }
+}
+
+constexpr int kSlabs = 8;  // z-slabs of a grid whose host copy overlaps the build
+
+// Launches the grid kernel in z-slabs of bricks when host copies are wanted: after each slab, that slab of every
+// output grid (a contiguous range of the layout data[l + 8*(i + nx*(j + ny*k))]) is copied to its host buffer on the
+// context's copy stream, so the copies run while the later slabs (and the next grids of a set) are computed. Without
+// host outputs it is one launch. The caller joins the copy stream before synchronising.
+template <typename Launch>
+rg_status launchSlabbed(rg_ctx* ctx, GridParams& gp, int bz, double* const* dev, double* const* host, int n_out,
+                        Launch launch)
+{
+  bool any = false;
+  for (int q = 0; q < n_out; ++q) any = any || (host && host[q]);
+  const int zb = (gp.nz + bz - 1) / bz;
+  const int n_slabs = any ? std::min(zb, kSlabs) : 1;
+  cudaStream_t cs = nullptr;
+  if (any)
+  {
+    rg_status st = rg::copyStream(ctx, &cs);
+    if (st) return st;
+  }
+  const size_t plane = 8 * static_cast<size_t>(gp.nx) * gp.ny;  // doubles per z-plane
+  for (int sl = 0; sl < n_slabs; ++sl)
+  {
+    gp.zb0 = any ? sl * zb / n_slabs : 0;
+    gp.zb1 = any ? (sl + 1) * zb / n_slabs : 0;
+    cudaError_t err = launch(gp);
+    if (err != cudaSuccess) return rg::cudaFail(ctx, err, "gridKernel launch");
+    if (!any) continue;
+    cudaEvent_t ev = nullptr;
+    rg_status st = rg::event(ctx, 1 + sl, &ev);
+    if (st) return st;
+    RG_CUDA(ctx, cudaEventRecord(ev, ctx->stream));
+    RG_CUDA(ctx, cudaStreamWaitEvent(cs, ev, 0));
+    const size_t k0 = static_cast<size_t>(gp.zb0) * bz, k1 = std::min<size_t>(gp.nz, static_cast<size_t>(gp.zb1) * bz);
+    for (int q = 0; q < n_out; ++q)
+      if (host && host[q] && k1 > k0)
+        RG_CUDA(ctx, cudaMemcpyAsync(host[q] + plane * k0, dev[q] + plane * k0, sizeof(double) * plane * (k1 - k0),
+                                     cudaMemcpyDeviceToHost, cs));
+  }
+  gp.zb0 = gp.zb1 = 0;
+  return RG_OK;
 }
 
 }  // namespace
@@ -587,10 +634,12 @@ int buildGridImages(int grid_type, const rg_forcefield* ff, const HostBox& box, 
 }
 }  // namespace rg
 
-extern "C" rg_status rg_grid_build(rg_ctx* ctx, int grid_type, const rg_forcefield* ff, const rg_box* unit_cell,
-                                   const rg_atom* unit_atoms, int n_unit_atoms, int probe_type, double cutoff, int nx,
-                                   int ny, int nz, int precision, double* out_device, double* out_host,
-                                   rg_grid_stats* stats)
+namespace
+{
+// One grid; the host copy (if any) is queued on the copy stream slab by slab. sync_out: join the copies and wait.
+rg_status buildOne(rg_ctx* ctx, int grid_type, const rg_forcefield* ff, const rg_box* unit_cell,
+                   const rg_atom* unit_atoms, int n_unit_atoms, int probe_type, double cutoff, int nx, int ny, int nz,
+                   int precision, double* out_device, double* out_host, rg_grid_stats* stats, bool sync_out)
 {
   if (!ctx) return RG_ERR_INVALID_ARGUMENT;
   if (!ff || !unit_cell || (n_unit_atoms > 0 && !unit_atoms) || n_unit_atoms < 0)
@@ -677,17 +726,17 @@ extern "C" rg_status rg_grid_build(rg_ctx* ctx, int grid_type, const rg_forcefie
   gp.out[0] = dout;
   gp.out[1] = nullptr;
 
-  cudaError_t err;
   const bool count = stats != nullptr;
-  if (precision == RG_PRECISION_FP64)
-    err = box.triclinic ? launchPrec<double, true>(grid_type, gp, dpos, dpar, bx, by, bz, count, ctx->stream)
-                        : launchPrec<double, false>(grid_type, gp, dpos, dpar, bx, by, bz, count, ctx->stream);
-  else
-    err = box.triclinic ? launchPrec<float, true>(grid_type, gp, dpos, dpar, bx, by, bz, count, ctx->stream)
-                        : launchPrec<float, false>(grid_type, gp, dpos, dpar, bx, by, bz, count, ctx->stream);
-  if (err != cudaSuccess) return rg::cudaFail(ctx, err, "gridKernel launch");
-
-  if (out_host) RG_CUDA(ctx, cudaMemcpyAsync(out_host, dout, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  double* devs[1] = {dout};
+  double* hosts[1] = {out_host};
+  rg_status lst = launchSlabbed(ctx, gp, bz, devs, hosts, 1, [&](const GridParams& g) {
+    if (precision == RG_PRECISION_FP64)
+      return box.triclinic ? launchPrec<double, true>(grid_type, g, dpos, dpar, bx, by, bz, count, ctx->stream)
+                           : launchPrec<double, false>(grid_type, g, dpos, dpar, bx, by, bz, count, ctx->stream);
+    return box.triclinic ? launchPrec<float, true>(grid_type, g, dpos, dpar, bx, by, bz, count, ctx->stream)
+                         : launchPrec<float, false>(grid_type, g, dpos, dpar, bx, by, bz, count, ctx->stream);
+  });
+  if (lst) return lst;
   if (stats)
   {
     unsigned long long c = 0;
@@ -698,11 +747,23 @@ extern "C" rg_status rg_grid_build(rg_ctx* ctx, int grid_type, const rg_forcefie
     stats->h2d_bytes = static_cast<int64_t>(2 * sizeof(double4)) * n_images;
     stats->d2h_bytes = out_host ? static_cast<int64_t>(out_bytes) : 0;
   }
-  else if (out_host)
+  if (out_host && sync_out)
   {
+    rg_status st2 = rg::joinCopies(ctx);
+    if (st2) return st2;
     RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   return RG_OK;
+}
+}  // namespace
+
+extern "C" rg_status rg_grid_build(rg_ctx* ctx, int grid_type, const rg_forcefield* ff, const rg_box* unit_cell,
+                                   const rg_atom* unit_atoms, int n_unit_atoms, int probe_type, double cutoff, int nx,
+                                   int ny, int nz, int precision, double* out_device, double* out_host,
+                                   rg_grid_stats* stats)
+{
+  return buildOne(ctx, grid_type, ff, unit_cell, unit_atoms, n_unit_atoms, probe_type, cutoff, nx, ny, nz, precision,
+                  out_device, out_host, stats, true);
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -929,13 +990,6 @@ extern "C" rg_status rg_grid_build_set(rg_ctx* ctx, const rg_forcefield* ff, con
   };
   std::vector<int> done(n_grids, 0);
   const size_t grid_bytes = sizeof(double) * 8 * static_cast<size_t>(nx) * ny * nz;
-  auto download = [&](int q) -> rg_status
-  {
-    if (out_host && out_host[q])
-      RG_CUDA(ctx, cudaMemcpyAsync(out_host[q], out_device[q], grid_bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    if (stats && out_host && out_host[q]) stats[q].d2h_bytes = static_cast<int64_t>(grid_bytes);
-    return RG_OK;
-  };
   for (int g = 0; g < n_grids; ++g)
   {
     if (done[g]) continue;
@@ -948,9 +1002,9 @@ extern "C" rg_status rg_grid_build_set(rg_ctx* ctx, const rg_forcefield* ff, con
     }
     if (partner < 0)
     {
-      rg_status st = rg_grid_build(ctx, grid_types[g], ff, unit_cell, unit_atoms, n_unit_atoms, probe_types[g], cutoff,
-                                   nx, ny, nz, precision, out_device[g], nullptr, stats ? &stats[g] : nullptr);
-      if (!st) st = download(g);
+      rg_status st = buildOne(ctx, grid_types[g], ff, unit_cell, unit_atoms, n_unit_atoms, probe_types[g], cutoff, nx,
+                              ny, nz, precision, out_device[g], out_host ? out_host[g] : nullptr,
+                              stats ? &stats[g] : nullptr, false);
       if (st) return st;
       done[g] = 1;
       continue;
@@ -1016,16 +1070,18 @@ extern "C" rg_status rg_grid_build_set(rg_ctx* ctx, const rg_forcefield* ff, con
     gp.out[0] = out_device[g];
     gp.out[1] = out_device[partner];
     const bool count = stats != nullptr;
-    cudaError_t err;
-    if (precision == RG_PRECISION_FP64)
-      err = box.triclinic
-                ? launchTyped<double, RG_GRID_LENNARD_JONES, true, 2>(gp, dpos, dpar, bx, by, bz, count, ctx->stream)
-                : launchTyped<double, RG_GRID_LENNARD_JONES, false, 2>(gp, dpos, dpar, bx, by, bz, count, ctx->stream);
-    else
-      err = box.triclinic
-                ? launchTyped<float, RG_GRID_LENNARD_JONES, true, 2>(gp, dpos, dpar, bx, by, bz, count, ctx->stream)
-                : launchTyped<float, RG_GRID_LENNARD_JONES, false, 2>(gp, dpos, dpar, bx, by, bz, count, ctx->stream);
-    if (err != cudaSuccess) return rg::cudaFail(ctx, err, "gridKernel (two probes) launch");
+    double* devs[2] = {out_device[g], out_device[partner]};
+    double* hosts[2] = {out_host ? out_host[g] : nullptr, out_host ? out_host[partner] : nullptr};
+    st = launchSlabbed(ctx, gp, bz, devs, hosts, 2, [&](const GridParams& q) {
+      if (precision == RG_PRECISION_FP64)
+        return box.triclinic
+                   ? launchTyped<double, RG_GRID_LENNARD_JONES, true, 2>(q, dpos, dpar, bx, by, bz, count, ctx->stream)
+                   : launchTyped<double, RG_GRID_LENNARD_JONES, false, 2>(q, dpos, dpar, bx, by, bz, count, ctx->stream);
+      return box.triclinic
+                 ? launchTyped<float, RG_GRID_LENNARD_JONES, true, 2>(q, dpos, dpar, bx, by, bz, count, ctx->stream)
+                 : launchTyped<float, RG_GRID_LENNARD_JONES, false, 2>(q, dpos, dpar, bx, by, bz, count, ctx->stream);
+    });
+    if (st) return st;
     if (stats)
     {
       unsigned long long c = 0;
@@ -1036,14 +1092,16 @@ extern "C" rg_status rg_grid_build_set(rg_ctx* ctx, const rg_forcefield* ff, con
         stats[q].pair_count = static_cast<int64_t>(c);
         stats[q].n_images = n_images;
         stats[q].h2d_bytes = static_cast<int64_t>(3 * sizeof(double4)) * n_images / 2;
-        stats[q].d2h_bytes = 0;
+        stats[q].d2h_bytes = (out_host && out_host[q]) ? static_cast<int64_t>(grid_bytes) : 0;
       }
     }
-    rg_status dst = download(g);
-    if (!dst) dst = download(partner);
-    if (dst) return dst;
     done[g] = done[partner] = 1;
   }
-  if (out_host) RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (out_host)
+  {
+    rg_status st = rg::joinCopies(ctx);
+    if (st) return st;
+    RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   return RG_OK;
 }

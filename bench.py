@@ -115,6 +115,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def max_over_ranks(seconds: float, world: int, dist, device: str = "cuda") -> float:
+    """The slowest rank's time of a timed region (every rank makes this call at the same point, so the collective
+    sequence is the same on all ranks); the time itself with one rank."""
+    if world <= 1:
+        return seconds
+    import torch
+
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, world: int, seconds: float) -> float:
+    """Units per second of the whole job: every rank processed units_per_rank in at most `seconds` (weak scaling)."""
+    return world * units_per_rank / seconds
+
+
 def cpu_oracle_rate(ff, cell, atoms, dims, grids, target_seconds, threads=0, seed=5):
     """FP64 oracle on a random sample of grid points of every grid; returns (points/s, points, seconds, threads)."""
     import oracle
@@ -177,10 +194,7 @@ def run_gcmc(args, ctx, ff, cell, atoms, dims, grids, outs, world, rank, dist, t
     e1.record(stream)
     torch.cuda.synchronize()
     secs = e0.elapsed_time(e1) / 1e3
-    if world > 1:
-        t = torch.tensor([secs], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        secs = float(t.item())
+    secs = max_over_ranks(secs, world, dist)
     # e2e: the same run call plus the read-back of every chain's statistics through the C-ABI
     t0 = time.perf_counter()
     g.run(GCMC_MOVES, record=True)
@@ -245,10 +259,7 @@ def run_alkane(args, ctx, peak_fp32, world, rank, dist, torch):
     secs = e0.elapsed_time(e1) / 1e3
     pairs = a.pair_count() - pairs0
     launches = a.launch_count() - launches0
-    if world > 1:
-        t = torch.tensor([secs], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        secs = float(t.item())
+    secs = max_over_ranks(secs, world, dist)
     res = a.results()
     # e2e: the run call plus the read-back of every system's statistics through the C-ABI
     t0 = time.perf_counter()
@@ -336,10 +347,7 @@ def run_mixture(args, ctx, world, rank, dist, torch):
     e1_.record(stream)
     torch.cuda.synchronize()
     secs = e0_.elapsed_time(e1_) / 1e3
-    if world > 1:
-        t = torch.tensor([secs], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        secs = float(t.item())
+    secs = max_over_ranks(secs, world, dist)
     r = mx.results()
     # e2e: the run call plus the read-back of the statistics
     t1 = time.perf_counter()
@@ -881,11 +889,8 @@ def run_ours(args):
     step_ms = [ev[s][0].elapsed_time(ev[s][-1]) for s in range(args.steps)]
     kern_ms = [[ev[s][c].elapsed_time(ev[s][c + 1]) for s in range(args.steps)] for c in range(len(calls))]
     total_s = sum(step_ms) / 1e3
-    if world > 1:
-        t = torch.tensor([total_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_s = float(t.item())
-    value = world * len(grids) * npts * args.steps / total_s
+    total_s = max_over_ranks(total_s, world, dist)
+    value = whole_job_rate(len(grids) * npts * args.steps, world, total_s)
 
     # e2e through the C-ABI with pinned host output buffers (framework upload + grid download inside the region)
     e2e_steps = max(1, min(args.steps, 5))
@@ -906,10 +911,7 @@ def run_ours(args):
             d2h = sum(x["d2h_bytes"] for x in st)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, world, dist)
     e2e_value = world * len(grids) * npts * e2e_steps / e2e_s
 
     # the reference's grid test after the build (rg_grid_validate): 100,000 points on the C_co2 grid and its charge term

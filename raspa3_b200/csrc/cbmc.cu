@@ -6,11 +6,12 @@
 //
 // A system (rg_system) keeps on the device: the pair table, the simulation box, the framework atoms, the tricubic
 // grids (one per pseudo-atom type plus the unit-charge Ewald grid) and the adsorbate atoms. One launch evaluates all
-// trials of a growth step: the grid is (trial, partner chunk); each CTA stages the trial's atoms in shared memory,
-// the threads stride over their chunk of partners (framework atoms for trial atoms without a grid, then adsorbate
-// atoms from other molecules), and the per-trial totals are reduced in a fixed order by the last CTA of the trial.
-// Trial atoms with a grid (and not fractional) take the grid branch: one tricubic interpolation of their VDW grid and,
-// with charges, q times the unit-charge Ewald grid. A trial is flagged as overlapping if any VDW pair energy or
+// trials of a growth step: the grid is (trial, chunk), sized to one wave of resident CTAs; each CTA stages the trial's
+// atoms in shared memory (a call of up to 32 trial atoms brings them in the launch parameters, so it costs one launch
+// and one synchronisation), the threads of chunks 1.. stride over their chunk of partners (framework atoms for trial
+// atoms without a grid, then adsorbate atoms from other molecules), and the per-trial totals are reduced in a fixed
+// order by the last CTA of the trial. Trial atoms with a grid (and not fractional) take the grid branch in chunk 0:
+// one tricubic interpolation of their VDW grid and, with charges, q times the unit-charge Ewald grid. A trial is flagged as overlapping if any VDW pair energy or
 // interpolated VDW energy exceeds the overlap criterion, which is the reference's std::nullopt. Arithmetic: FP64 by
 // default; with RG_PRECISION_FP32C (rg_system_set_precision) the pair terms are FP32 from the FP64 minimum-image
 // displacement and each thread sums them in TwoSum-compensated FP32 pairs, folded into the FP64 totals. The grid
@@ -31,6 +32,7 @@ constexpr int kMinChunk = 256;         // partner atoms per CTA at least (a call
 constexpr int kMaxChunk = 4096;         // and at most
 constexpr int kMaxTrialAtoms = 64;     // atoms of one trial set
 constexpr int kNumOut = 12;            // fmVDW, fmCharge, mmVDW, mmCharge, dudl VDW[4], dudl charge[4]
+constexpr int kParamTrialAtoms = 32;   // trial sets of up to this many atoms in total travel in the launch parameters
 }  // namespace
 
 struct rg_system
@@ -65,6 +67,7 @@ struct rg_system
   rg_trial_energy* out_mapped = nullptr;  // device view of out_host
   int precision = RG_PRECISION_FP64;      // of rg_cbmc_external_energies
   int sms = 148;
+  int resident[2] = {0, 0};               // CTAs per SM of trialEnergyKernel<false>, <true> (0 = not yet queried)
 };
 
 namespace
@@ -86,12 +89,18 @@ struct TrialArgs
   const double* ewald_grid;
   int gnx, gny, gnz;
   double gic[3][3];
-  int n_chunks;
+  int n_chunks;            // chunk 0: the grid branch; chunks 1..: partner atoms
   int chunk;               // partner atoms per CTA
   int fw_partners;         // framework atoms scanned (0 if every trial atom has a grid)
   double* partial;         // [trial][chunk][kNumOut + 1]
   unsigned int* counters;  // per trial
   rg_trial_energy* out;
+};
+
+// the trial atoms of a small call, passed by value in the launch parameters (no copy before the launch)
+struct TrialParam
+{
+  rg_atom a[kParamTrialAtoms];
 };
 
 // FP32 forms of rgd::pairVDW / rgd::pairCoulomb: the same soft-core formulas (pair_vdw.ixx:85-101,
@@ -144,8 +153,23 @@ struct Sum32
   __device__ __forceinline__ double value() const { return static_cast<double>(hi) + static_cast<double>(lo); }
 };
 
+// acc[g - 1] += x for a dU/dlambda group g in 1..4, with constant indices so that the accumulators stay in registers
+template <typename T, typename V>
+__device__ __forceinline__ void addToGroup(T* acc, int g, V x)
+{
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (g == k + 1) acc[k] += x;
+}
+
+__device__ __forceinline__ Sum32& operator+=(Sum32& s, float x)
+{
+  s.add(x);
+  return s;
+}
+
 template <bool F32>
-__global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a)
+__global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a, TrialParam small)
 {
   const int trial = blockIdx.x;
   const int chunk = blockIdx.y;
@@ -156,7 +180,7 @@ __global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a)
   const int nA = a.atoms_per_trial;
   for (int i = threadIdx.x; i < nA; i += blockDim.x)
   {
-    sT[i] = a.trials[static_cast<long long>(trial) * nA + i];
+    sT[i] = a.trials ? a.trials[static_cast<long long>(trial) * nA + i] : small.a[trial * nA + i];
     const int t = sT[i].type;
     sGridBranch[i] = (t < 64 && a.grid[t] != nullptr && !rgd::fractionalOf(sT[i])) ? 1 : 0;
   }
@@ -168,29 +192,32 @@ __global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a)
   Sum32 acc32[F32 ? kNumOut : 1];
   double overlap = 0.0;
 
-  // grid branch: one thread per trial atom, in chunk 0 only
+  // chunk 0 is the grid branch alone: one thread per (trial atom, grid), the VDW grid on even threads and q times the
+  // unit-charge Ewald grid on odd ones, so that no partner chunk waits for an interpolation
   if (chunk == 0)
   {
-    for (int i = threadIdx.x; i < nA; i += blockDim.x)
+    for (int j = threadIdx.x; j < 2 * nA; j += blockDim.x)
     {
+      const int i = j >> 1;
       if (i == a.skip || !sGridBranch[i]) continue;
-      rgd::Grid g{a.grid[sT[i].type], a.gnx, a.gny, a.gnz, {}};
+      const bool ewald = (j & 1) != 0;
+      if (ewald && !(a.ff.use_charge && a.ewald_grid)) continue;
+      rgd::Grid g{ewald ? a.ewald_grid : a.grid[sT[i].type], a.gnx, a.gny, a.gnz, {}};
       for (int r = 0; r < 3; ++r)
         for (int c = 0; c < 3; ++c) g.ic[r][c] = a.gic[r][c];
       const double e = rgd::interpolate(g, sT[i].x, sT[i].y, sT[i].z);
-      if (e > a.ff.overlap) overlap = 1.0;
-      acc[0] += e;
-      if (a.ff.use_charge && a.ewald_grid)
+      if (ewald)
+        acc[1] += sT[i].charge * e;
+      else
       {
-        rgd::Grid ge = g;
-        ge.data = a.ewald_grid;
-        acc[1] += sT[i].charge * rgd::interpolate(ge, sT[i].x, sT[i].y, sT[i].z);
+        if (e > a.ff.overlap) overlap = 1.0;
+        acc[0] += e;
       }
     }
   }
 
   const long long total = static_cast<long long>(a.fw_partners) + a.n_mol;
-  const long long begin = static_cast<long long>(chunk) * a.chunk;
+  const long long begin = chunk == 0 ? total : static_cast<long long>(chunk - 1) * a.chunk;
   const long long end = begin + a.chunk < total ? begin + a.chunk : total;
   for (long long p = begin + threadIdx.x; p < end; p += blockDim.x)
   {
@@ -219,17 +246,23 @@ __global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a)
           const float2 f = pairVDWf(a.ff, static_cast<float>(B.scaling_vdw), static_cast<float>(A.scaling_vdw), rrf,
                                     B.type, A.type);
           if (static_cast<double>(f.x) > a.ff.overlap) overlap = 1.0;
-          acc32[isFw ? 0 : 2].add(f.x);
-          if (gB != 0) acc32[4 + gB - 1].add(static_cast<float>(A.scaling_vdw) * f.y);
-          if (gA != 0) acc32[4 + gA - 1].add(static_cast<float>(B.scaling_vdw) * f.y);
+          if (isFw)
+            acc32[0].add(f.x);
+          else
+            acc32[2].add(f.x);
+          addToGroup(acc32 + 4, gB, static_cast<float>(A.scaling_vdw) * f.y);
+          addToGroup(acc32 + 4, gA, static_cast<float>(B.scaling_vdw) * f.y);
         }
         if (a.ff.use_charge && rr < a.rcc2)
         {
           const float2 f = pairCoulombf(a.ff, static_cast<float>(B.scaling_coulomb), static_cast<float>(A.scaling_coulomb),
                                         sqrtf(rrf), B.charge, A.charge);
-          acc32[isFw ? 1 : 3].add(f.x);
-          if (gB != 0) acc32[8 + gB - 1].add(static_cast<float>(A.scaling_coulomb) * f.y);
-          if (gA != 0) acc32[8 + gA - 1].add(static_cast<float>(B.scaling_coulomb) * f.y);
+          if (isFw)
+            acc32[1].add(f.x);
+          else
+            acc32[3].add(f.x);
+          addToGroup(acc32 + 8, gB, static_cast<float>(A.scaling_coulomb) * f.y);
+          addToGroup(acc32 + 8, gA, static_cast<float>(B.scaling_coulomb) * f.y);
         }
       }
       else
@@ -238,18 +271,24 @@ __global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a)
         {
           const double2 f = rgd::pairVDW(a.ff, B.scaling_vdw, A.scaling_vdw, rr, B.type, A.type);
           if (f.x > a.ff.overlap) overlap = 1.0;
-          acc[isFw ? 0 : 2] += f.x;
+          if (isFw)
+            acc[0] += f.x;
+          else
+            acc[2] += f.x;
           // addDudlambdaVDW(groupIdA(partner), groupIdB(trial), ...) (running_energy.ixx:258-263)
-          if (gB != 0) acc[4 + gB - 1] += A.scaling_vdw * f.y;
-          if (gA != 0) acc[4 + gA - 1] += B.scaling_vdw * f.y;
+          addToGroup(acc + 4, gB, A.scaling_vdw * f.y);
+          addToGroup(acc + 4, gA, B.scaling_vdw * f.y);
         }
         if (a.ff.use_charge && rr < a.rcc2)
         {
           const double r = sqrt(rr);
           const double2 f = rgd::pairCoulomb(a.ff, B.scaling_coulomb, A.scaling_coulomb, r, B.charge, A.charge);
-          acc[isFw ? 1 : 3] += f.x;
-          if (gB != 0) acc[8 + gB - 1] += A.scaling_coulomb * f.y;
-          if (gA != 0) acc[8 + gA - 1] += B.scaling_coulomb * f.y;
+          if (isFw)
+            acc[1] += f.x;
+          else
+            acc[3] += f.x;
+          addToGroup(acc + 8, gB, A.scaling_coulomb * f.y);
+          addToGroup(acc + 8, gA, B.scaling_coulomb * f.y);
         }
       }
     }
@@ -293,16 +332,29 @@ __global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a)
   __syncthreads();
   if (!last) return;
   __threadfence();
+  // the trial's total over its chunks: 16 threads per channel sum the chunks j, j + 16, ... (their loads in flight
+  // together), then each channel's 16 sub-sums in order
+  static_assert(kThreads == 16 * 16 && kNumOut + 1 <= 16, "16 threads for each of at most 16 channels");
+  __shared__ double sub[kNumOut + 1][16];
   __shared__ double tot[kNumOut + 1];
+  const int cc = threadIdx.x >> 4, j0 = threadIdx.x & 15;
+  if (cc <= kNumOut)
+  {
+    const double* src = a.partial + static_cast<long long>(trial) * a.n_chunks * (kNumOut + 1) + cc;
+    double x = 0.0;
+#pragma unroll 4
+    for (int ch = j0; ch < a.n_chunks; ch += 16)
+    {
+      const double y = __ldcg(src + static_cast<long long>(ch) * (kNumOut + 1));
+      x = (cc < kNumOut) ? x + y : fmax(x, y);
+    }
+    sub[cc][j0] = x;
+  }
+  __syncthreads();
   if (c <= kNumOut)
   {
-    const double* src = a.partial + static_cast<long long>(trial) * a.n_chunks * (kNumOut + 1);
     double x = 0.0;
-    for (int ch = 0; ch < a.n_chunks; ++ch)
-    {
-      const double y = __ldcg(src + ch * (kNumOut + 1) + c);
-      x = (c < kNumOut) ? x + y : fmax(x, y);
-    }
+    for (int j = 0; j < 16; ++j) x = (c < kNumOut) ? x + sub[c][j] : fmax(x, sub[c][j]);
     tot[c] = x;
   }
   __syncthreads();
@@ -511,12 +563,24 @@ rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_t
   }
   const int fw_partners = needFw ? s->n_fw : 0;
   const long long total = static_cast<long long>(fw_partners) + s->n_mol;
-  // chunks of partners: enough CTAs for about two per SM, each with at least kMinChunk partners
-  const long long want = (2LL * s->sms + n_trials - 1) / n_trials;
+  const bool f32 = s->precision == RG_PRECISION_FP32C;
+  int& resident = s->resident[f32 ? 1 : 0];
+  if (resident == 0)
+  {
+    cudaError_t err = f32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, trialEnergyKernel<true>, kThreads, 0)
+                          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, trialEnergyKernel<false>, kThreads, 0);
+    if (err) return rg::cudaFail(ctx, err, "rg_cbmc_external_energies: occupancy");
+    resident = std::max(1, resident);
+  }
+  // chunks of partners: as many CTAs as are resident at once (one wave, the grid-branch chunk included), each with
+  // at least kMinChunk and at most kMaxChunk partners
+  const long long want = std::max<long long>(1, static_cast<long long>(resident) * s->sms / n_trials - 1);
   long long chunk = total > 0 ? (total + want - 1) / want : 1;
   chunk = std::min<long long>(kMaxChunk, std::max<long long>(kMinChunk, chunk));
-  const int n_chunks = static_cast<int>(total > 0 ? (total + chunk - 1) / chunk : 1);
-  rg_status st = growDevice(ctx, &s->trials, &s->trial_cap, nt_atoms);
+  const int n_chunks = 1 + static_cast<int>(total > 0 ? (total + chunk - 1) / chunk : 0);
+  rg_status st = RG_OK;
+  const bool inParams = nt_atoms <= kParamTrialAtoms;
+  if (!inParams) st = growDevice(ctx, &s->trials, &s->trial_cap, nt_atoms);
   if (!st) st = growDevice(ctx, &s->partial, &s->partial_cap, n_trials * n_chunks * (kNumOut + 1));
   if (!st && s->counter_cap < n_trials)
   {
@@ -524,10 +588,16 @@ rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_t
     if (!st) RG_CUDA(ctx, cudaMemsetAsync(s->counters, 0, sizeof(unsigned int) * s->counter_cap, ctx->stream));
   }
   if (st) return st;
-  // the pinned staging buffer is free: every call ends by synchronising the stream
-  std::memcpy(s->trials_host, trials, sizeof(rg_atom) * nt_atoms);
-  RG_CUDA(ctx, cudaMemcpyAsync(s->trials, s->trials_host, sizeof(rg_atom) * nt_atoms, cudaMemcpyHostToDevice,
-                               ctx->stream));
+  TrialParam small{};
+  if (inParams)
+    std::memcpy(small.a, trials, sizeof(rg_atom) * nt_atoms);
+  else
+  {
+    // the pinned staging buffer is free: every call ends by synchronising the stream
+    std::memcpy(s->trials_host, trials, sizeof(rg_atom) * nt_atoms);
+    RG_CUDA(ctx, cudaMemcpyAsync(s->trials, s->trials_host, sizeof(rg_atom) * nt_atoms, cudaMemcpyHostToDevice,
+                                 ctx->stream));
+  }
   TrialArgs a{};
   a.ff = s->ff;
   a.box = s->box;
@@ -535,7 +605,7 @@ rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_t
   a.n_fw = s->n_fw;
   a.mol = s->mol;
   a.n_mol = s->n_mol;
-  a.trials = s->trials;
+  a.trials = inParams ? nullptr : s->trials;
   a.atoms_per_trial = atoms_per_trial;
   a.skip = skip;
   a.skip_background = skip_background_molecule;
@@ -556,10 +626,10 @@ rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_t
   a.counters = s->counters;
   a.out = s->out_mapped;
   dim3 grid(n_trials, n_chunks);
-  if (s->precision == RG_PRECISION_FP32C)
-    trialEnergyKernel<true><<<grid, kThreads, 0, ctx->stream>>>(a);
+  if (f32)
+    trialEnergyKernel<true><<<grid, kThreads, 0, ctx->stream>>>(a, small);
   else
-    trialEnergyKernel<false><<<grid, kThreads, 0, ctx->stream>>>(a);
+    trialEnergyKernel<false><<<grid, kThreads, 0, ctx->stream>>>(a, small);
   RG_CUDA(ctx, cudaGetLastError());
   // the last CTA of each trial wrote its result into mapped pinned memory: completion makes it visible here
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

@@ -114,13 +114,33 @@ __device__ __forceinline__ void blockReduceAndFinish(double (&v)[1 + G], double*
     last = (done == gridDim.x - 1);
   }
   __syncthreads();
-  if (last && threadIdx.x == 0)
+  if (!last) return;
+  __threadfence();
+  // the last block: each thread sums the partials of blocks threadIdx.x, threadIdx.x + blockDim.x, ... (all its loads
+  // in flight together), then the same fixed-order warp and block reduction
+  double y[1 + G];
+#pragma unroll
+  for (int c = 0; c < 1 + G; ++c) y[c] = 0.0;
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
   {
-    __threadfence();
+#pragma unroll
+    for (int c = 0; c < 1 + G; ++c) y[c] += __ldcg(partial + b * (1 + kMaxGroups) + c);
+  }
+#pragma unroll
+  for (int c = 0; c < 1 + G; ++c)
+  {
+    double x = y[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[warp][c] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
     for (int c = 0; c < 1 + G; ++c)
     {
       double x = 0.0;
-      for (unsigned b = 0; b < gridDim.x; ++b) x += static_cast<volatile double*>(partial)[b * (1 + kMaxGroups) + c];
+      for (int w = 0; w < kThreads / 32; ++w) x += red[w][c];
       result[c] = x;
     }
     *counter = 0u;  // ready for the next launch on this system

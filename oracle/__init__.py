@@ -84,6 +84,16 @@ def lib():
         L.oracle_grid_pair_count.restype = i64
         L.oracle_tricubic_fractional_at_position.argtypes = [i32, P(OFF), P(OBox), vp, i32, P(OBox), vp, i32, vp]
         L.oracle_tricubic_matrix.argtypes = [vp]
+        L.oracle_triquintic_fractional_at_position.argtypes = [i32, P(OFF), P(OBox), vp, i32, P(OBox), vp, i32, i32,
+                                                               vp]
+        L.oracle_make_triquintic_grid.argtypes = [i32, P(OFF), P(OBox), vp, i32, i32, d, i32, i32, i32, i32, vp, i64,
+                                                  i32, vp]
+        L.oracle_make_triquintic_grid.restype = i32
+        L.oracle_triquintic_interpolate.argtypes = [vp, i32, i32, i32, P(OBox), vp, vp]
+        L.oracle_triquintic_interpolate.restype = d
+        L.oracle_interpolant_from_corners.argtypes = [i32, vp, vp, vp]
+        L.oracle_interpolant_from_corners.restype = d
+        L.oracle_triquintic_matrix.argtypes = [vp]
         L.oracle_grid_interpolate.argtypes = [vp, i32, i32, i32, P(OBox), vp]
         L.oracle_grid_interpolate.restype = d
         L.oracle_grid_validate.argtypes = [P(OFF), P(OBox), vp, i32, P(OBox), i32, i32, i32, i32, vp, vp, d, d, vp,
@@ -184,6 +194,60 @@ def tricubic_matrix() -> np.ndarray:
     m = np.empty(64 * 64)
     lib().oracle_tricubic_matrix(_ptr(m))
     return m.reshape(64, 64)
+
+
+def make_grid_triquintic(grid_type, ff, cell, atoms, probe_type, cutoff, dims, points=None, threads=0,
+                         reference_rectangular=False):
+    """Triquintic grid (27 values per point, flat reference layout) or the 27 values at the listed flat indices."""
+    nx, ny, nz = dims
+    o, b = off(ff), obox(cell)
+    atoms = np.ascontiguousarray(atoms)
+    rr = 1 if reference_rectangular else 0
+    if points is None:
+        out = np.empty(27 * nx * ny * nz)
+        lib().oracle_make_triquintic_grid(grid_type, o, b, _ptr(atoms), len(atoms), probe_type, cutoff, nx, ny, nz, rr,
+                                          None, 0, threads, _ptr(out))
+        return out
+    pts = np.ascontiguousarray(points, dtype=np.int64)
+    out = np.empty((len(pts), 27))
+    lib().oracle_make_triquintic_grid(grid_type, o, b, _ptr(atoms), len(atoms), probe_type, cutoff, nx, ny, nz, rr,
+                                      _ptr(pts), len(pts), threads, _ptr(out))
+    return out
+
+
+def triquintic_fractional(grid_type, ff, super_cell, pos, type_a, unit_cell, super_atoms, reference_rectangular=False,
+                          triclinic=None):
+    out = np.empty(27)
+    p = np.ascontiguousarray(pos, dtype=np.float64)
+    sa = np.ascontiguousarray(super_atoms)
+    lib().oracle_triquintic_fractional_at_position(grid_type, off(ff), obox(super_cell, triclinic), _ptr(p), type_a,
+                                                   obox(unit_cell, triclinic), _ptr(sa), len(sa),
+                                                   1 if reference_rectangular else 0, _ptr(out))
+    return out
+
+
+def interpolate_triquintic(grid, dims, cell, pos):
+    """(value, Cartesian gradient) of a triquintic grid at pos."""
+    g = np.ascontiguousarray(grid, dtype=np.float64)
+    p = np.ascontiguousarray(pos, dtype=np.float64)
+    grad = np.empty(3)
+    v = lib().oracle_triquintic_interpolate(_ptr(g), dims[0], dims[1], dims[2], obox(cell), _ptr(p), _ptr(grad))
+    return v, grad
+
+
+def interpolant_from_corners(scheme, X, s):
+    """(value, d/ds) of one cell's interpolating polynomial from its corner data (scheme 8 or 27)."""
+    x = np.ascontiguousarray(X, dtype=np.float64)
+    sv = np.ascontiguousarray(s, dtype=np.float64)
+    ds = np.empty(3)
+    v = lib().oracle_interpolant_from_corners(scheme, _ptr(x), _ptr(sv), _ptr(ds))
+    return v, ds
+
+
+def triquintic_matrix() -> np.ndarray:
+    m = np.empty(216 * 216)
+    lib().oracle_triquintic_matrix(_ptr(m))
+    return m.reshape(216, 216)
 
 
 def grid_validate(ff, unit_cell, unit_atoms, simulation_cell, probe_type, dims, vdw_grid, ewald_grid, probe_charge,

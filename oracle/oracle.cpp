@@ -519,6 +519,358 @@ double interpolateTricubicGradient(const double* data, int nx, int ny, int nz, c
   return value;
 }
 
+// ---- triquintic scheme (27 values per grid point) ----
+//
+// Channel l of a triquintic grid point holds the mixed derivative of the energy of orders kQuinticOrder[l] along the
+// three lattice directions; the order list follows the divisors of makeFrameworkInterpolationGrid's triquintic branch
+// (interpolation_energy_grid.cpp:3882-3945).
+constexpr int kQuinticOrder[27][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0}, {1, 1, 0}, {1, 0, 1},
+                                      {0, 2, 0}, {0, 1, 1}, {0, 0, 2}, {2, 1, 0}, {2, 0, 1}, {1, 2, 0}, {1, 1, 1},
+                                      {0, 2, 1}, {1, 0, 2}, {0, 1, 2}, {2, 2, 0}, {2, 0, 2}, {0, 2, 2}, {2, 1, 1},
+                                      {1, 2, 1}, {1, 1, 2}, {2, 2, 1}, {2, 1, 2}, {1, 2, 2}, {2, 2, 2}};
+
+// F[k] = (1/r d/dr)^k U(r), k = 0..6
+struct Factor6
+{
+  double f[7];
+};
+
+// potentialLennardJonesTriquinticDerivative (potentials/interpolation/triquintic_derivative_lj.ixx:33-51). The
+// reference's triquintic branch uses it for the repulsion and attraction grid types too
+// (interactions/framework_molecule_grid.cpp:584-592).
+inline Factor6 ljTriquintic(double eps, double sigma, double shift, double r2)
+{
+  const double arg1 = 4.0 * eps;
+  const double arg2 = sigma * sigma;
+  const double temp3 = (arg2 / r2) * (arg2 / r2) * (arg2 / r2);
+  const double r4 = r2 * r2, r6 = r4 * r2, r8 = r6 * r2, r10 = r8 * r2, r12 = r10 * r2;
+  const double t6 = temp3 * temp3;
+  return {{arg1 * (t6 - temp3) - shift, -6.0 * arg1 * (2.0 * t6 - temp3) / r2, 24.0 * arg1 * (7.0 * t6 - 2.0 * temp3) / r4,
+           -96.0 * arg1 * (28.0 * t6 - 5.0 * temp3) / r6, 1152.0 * arg1 * (42.0 * t6 - 5.0 * temp3) / r8,
+           -80640.0 * arg1 * (12.0 * t6 - temp3) / r10, 645120.0 * arg1 * (33.0 * t6 - 2.0 * temp3) / r12}};
+}
+
+// potentialRealEwaldTriquinticDerivative (potentials/interpolation/triquintic_derivative_real_ewald.ixx:32-78)
+inline Factor6 ewaldTriquintic(double alpha, double rr, double r, double qa, double qb)
+{
+  const double Cq = coulombFactor() * qa * qb;
+  const double ec = std::erfc(alpha * r);
+  const double et = 2.0 * alpha * r * std::exp(-alpha * alpha * rr) * kInvSqrtPi;
+  const double a2 = (alpha * r) * (alpha * r), a4 = a2 * a2, a6 = a4 * a2, a8 = a6 * a2, a10 = a8 * a2;
+  const double r3 = rr * r, r5 = r3 * rr, r7 = r5 * rr, r9 = r7 * rr, r11 = r9 * rr, r13 = r11 * rr;
+  return {{Cq * ec / r, -Cq * ((et + ec) / r3), Cq * ((et * (2.0 * a2 + 3.0) + 3.0 * ec) / r5),
+           -Cq * ((et * (4.0 * a4 + 10.0 * a2 + 15.0) + 15.0 * ec) / r7),
+           Cq * ((et * (8.0 * a6 + 28.0 * a4 + 70.0 * a2 + 105.0) + 105.0 * ec) / r9),
+           -Cq * ((et * (16.0 * a8 + 72.0 * a6 + 252.0 * a4 + 630.0 * a2 + 945.0) + 945.0 * ec) / r11),
+           Cq * ((et * (32.0 * a10 + 176.0 * a8 + 792.0 * a6 + 2772.0 * a4 + 6930.0 * a2 + 10395.0) + 10395.0 * ec) /
+                 r13)}};
+}
+
+inline Factor6 quinticFactor(int grid_type, const off* ff, double rr, int typeA, const oatom& b)
+{
+  if (grid_type == 1) return ewaldTriquintic(ff->ewald_alpha, rr, std::sqrt(rr), 1.0, b.charge);
+  const int idx = typeA * ff->n_types + b.type;
+  return ljTriquintic(ff->epsilon[idx], ff->sigma[idx], ff->shift[idx], rr);
+}
+
+// d^n/dx^n of a radial function along one Cartesian axis, as a polynomial in x and the factors F:
+// sum over m pairs of n!/(m! 2^m (n-2m)!) x^(n-2m) F[n-m]. The mixed Cartesian derivative of orders (i, j, k) is the
+// product of the three axis polynomials with the F indices added up (every derivative of a radial function is a sum
+// over partial pairings of its directions: each pair gives a Kronecker delta, each unpaired direction a component of
+// dr, and F takes the index directions - pairs).
+double cartesianDerivative(int i, int j, int k, const double dr[3], const double F[7])
+{
+  auto terms = [](int n, double x, double* c, int* fk, int& cnt)
+  {
+    cnt = 0;
+    for (int m = 0; 2 * m <= n; ++m)
+    {
+      double coef = 1.0;
+      for (int q = 0; q < n; ++q) coef *= static_cast<double>(q + 1);  // n!
+      double den = 1.0;
+      for (int q = 0; q < m; ++q) den *= static_cast<double>(q + 1) * 2.0;  // m! 2^m
+      for (int q = 0; q < n - 2 * m; ++q) den *= static_cast<double>(q + 1);  // (n-2m)!
+      c[cnt] = coef / den * std::pow(x, n - 2 * m);
+      fk[cnt] = n - m;
+      ++cnt;
+    }
+  };
+  double cx[4], cy[4], cz[4];
+  int kx[4], ky[4], kz[4], nx, ny, nz;
+  terms(i, dr[0], cx, kx, nx);
+  terms(j, dr[1], cy, ky, ny);
+  terms(k, dr[2], cz, kz, nz);
+  double v = 0.0;
+  for (int a = 0; a < nx; ++a)
+    for (int b = 0; b < ny; ++b)
+      for (int c = 0; c < nz; ++c) v += cx[a] * cy[b] * cz[c] * F[kx[a] + ky[b] + kz[c]];
+  return v;
+}
+
+// Interactions::calculateTriquinticFractionalAtPosition (interactions/framework_molecule_grid.cpp:549-813).
+// Rectangular cells (:568-683): the 27 Cartesian mixed derivatives summed over the supercell atoms, scaled by the cell
+// diagonal. With reference_rectangular the two deviations of that branch are kept: the first derivatives along y and
+// z are scaled by cell[0][0] (:648-650), and the (2,2,2) channel lacks its F3 term (:671-676). Without it the branch
+// gives the exact derivatives, the values of the triclinic branch for the same cell.
+// Triclinic cells (:684-812, with calculateTriquinticDerivativeAtPosition :284-503): the full Cartesian derivative
+// tensors summed over the atoms, then contracted with the cell vectors.
+void triquinticFractional(int grid_type, const off* ff, const Box& superBox, const double* posA, int typeA,
+                          const Box& unitBox, const oatom* atoms, int n, bool reference_rectangular, double out[27])
+{
+  const double rc2 = ff->cutoff_framework_vdw * ff->cutoff_framework_vdw;
+  // Cartesian derivative sums by multiset (i x's, j y's, k z's), i + j + k <= 6
+  double T[7][7][7];
+  std::memset(T, 0, sizeof(T));
+  double sumF3 = 0.0;
+  for (int a = 0; a < n; ++a)
+  {
+    double dr[3] = {posA[0] - atoms[a].x, posA[1] - atoms[a].y, posA[2] - atoms[a].z};
+    pbc(superBox, dr);
+    const double rr = std::max(0.1, dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+    if (rr >= rc2) continue;
+    const Factor6 v = quinticFactor(grid_type, ff, rr, typeA, atoms[a]);
+    sumF3 += v.f[3];
+    for (int i = 0; i <= 6; ++i)
+      for (int j = 0; i + j <= 6; ++j)
+        for (int k = 0; i + j + k <= 6; ++k) T[i][j][k] += cartesianDerivative(i, j, k, dr, v.f);
+  }
+  const auto& C = unitBox.c;  // C[a][p]: component p of lattice vector a
+  if (!unitBox.triclinic)
+  {
+    for (int l = 0; l < 27; ++l)
+    {
+      const int* o = kQuinticOrder[l];
+      out[l] = T[o[0]][o[1]][o[2]] * std::pow(C[0][0], o[0]) * std::pow(C[1][1], o[1]) * std::pow(C[2][2], o[2]);
+    }
+    if (reference_rectangular)
+    {
+      out[2] = T[0][1][0] * C[0][0];
+      out[3] = T[0][0][1] * C[0][0];
+      out[26] -= sumF3 * C[0][0] * C[0][0] * C[1][1] * C[1][1] * C[2][2] * C[2][2];
+    }
+    return;
+  }
+  // contraction: sum over Cartesian index tuples p_1..p_n of prod_t C[d_t][p_t] * T[multiset(p)]
+  for (int l = 0; l < 27; ++l)
+  {
+    const int* o = kQuinticOrder[l];
+    int dirs[6], nd = 0;
+    for (int ax = 0; ax < 3; ++ax)
+      for (int q = 0; q < o[ax]; ++q) dirs[nd++] = ax;
+    int total = 1;
+    for (int q = 0; q < nd; ++q) total *= 3;
+    double acc = 0.0;
+    for (int code = 0; code < total; ++code)
+    {
+      int cnt[3] = {0, 0, 0}, c = code;
+      double w = 1.0;
+      for (int q = 0; q < nd; ++q)
+      {
+        const int p = c % 3;
+        c /= 3;
+        ++cnt[p];
+        w *= C[dirs[q]][p];
+      }
+      acc += w * T[cnt[0]][cnt[1]][cnt[2]];
+    }
+    out[l] = acc;
+  }
+}
+
+// One grid point of makeFrameworkInterpolationGrid, triquintic branch (interpolation_energy_grid.cpp:3882-3962).
+void gridPointQuintic(int grid_type, const off* ff, const GridSetup& s, int probe_type, int64_t i, int64_t j, int64_t k,
+                      bool reference_rectangular, double* dst)
+{
+  const double delta[3] = {1.0 / static_cast<double>(s.ncx), 1.0 / static_cast<double>(s.ncy),
+                           1.0 / static_cast<double>(s.ncz)};
+  const double frac[3] = {static_cast<double>(i) * delta[0], static_cast<double>(j) * delta[1],
+                          static_cast<double>(k) * delta[2]};
+  double pos[3];
+  matvec(s.unit.c, frac, pos);
+  double values[27];
+  triquinticFractional(grid_type, ff, s.super, pos, probe_type, s.unit, s.atoms.data(),
+                       static_cast<int>(s.atoms.size()), reference_rectangular, values);
+  const double nc[3] = {static_cast<double>(s.ncx), static_cast<double>(s.ncy), static_cast<double>(s.ncz)};
+  for (int l = 1; l < 27; ++l)
+  {
+    const int* o = kQuinticOrder[l];
+    values[l] /= std::pow(nc[0], o[0]) * std::pow(nc[1], o[1]) * std::pow(nc[2], o[2]);
+  }
+  const double oc = ff->overlap_criteria;
+  if (values[0] > oc)
+  {
+    dst[0] = 2.0 * oc;
+    dst[1] = std::clamp(values[1], -oc, oc);
+    dst[2] = std::clamp(values[2], -oc, oc);
+    dst[3] = std::clamp(values[3], -oc, oc);
+    for (int l = 4; l < 27; ++l) dst[l] = 0.0;
+  }
+  else
+  {
+    for (int l = 0; l < 27; ++l) dst[l] = values[l];
+  }
+}
+
+// Triquintic coefficient map: inverse of the map from the 216 monomial coefficients a[i + 6j + 36k] to the corner data
+// X[8*l + corner] (channel l of kQuinticOrder, corner bit 0 = x, bit 1 = y, bit 2 = z), regenerated by Gauss-Jordan
+// elimination. 8 times each entry is an integer (the reference stores those integers and scales by 0.125,
+// interpolation_energy_grid.cpp:360, 4160-4164); the oracle rounds to them.
+struct TriquinticMatrix
+{
+  std::vector<double> m;  // 216 x 216
+  std::vector<int> start, nzc;
+  std::vector<double> nzv;
+  TriquinticMatrix() : m(216 * 216), start(217)
+  {
+    auto dmono = [](int p, int d, int x) -> double
+    {
+      if (d > p) return 0.0;
+      double c = 1.0;
+      for (int q = 0; q < d; ++q) c *= static_cast<double>(p - q);
+      if (x == 0) return (p == d) ? c : 0.0;
+      return c;
+    };
+    const int N = 216;
+    std::vector<double> B(static_cast<size_t>(N) * 2 * N, 0.0);
+    auto b = [&](int r, int c) -> double& { return B[static_cast<size_t>(r) * 2 * N + c]; };
+    for (int l = 0; l < 27; ++l)
+      for (int corner = 0; corner < 8; ++corner)
+      {
+        const int row = 8 * l + corner;
+        const int x = corner & 1, y = (corner >> 1) & 1, z = (corner >> 2) & 1;
+        for (int k = 0; k < 6; ++k)
+          for (int j = 0; j < 6; ++j)
+            for (int i = 0; i < 6; ++i)
+              b(row, i + 6 * j + 36 * k) = dmono(i, kQuinticOrder[l][0], x) * dmono(j, kQuinticOrder[l][1], y) *
+                                           dmono(k, kQuinticOrder[l][2], z);
+        b(row, N + row) = 1.0;
+      }
+    for (int col = 0; col < N; ++col)
+    {
+      int piv = col;
+      for (int r = col + 1; r < N; ++r)
+        if (std::fabs(b(r, col)) > std::fabs(b(piv, col))) piv = r;
+      if (piv != col)
+        for (int c = 0; c < 2 * N; ++c) std::swap(b(piv, c), b(col, c));
+      const double p = b(col, col);
+      for (int c = 0; c < 2 * N; ++c) b(col, c) /= p;
+      for (int r = 0; r < N; ++r)
+      {
+        if (r == col) continue;
+        const double f = b(r, col);
+        if (f == 0.0) continue;
+        for (int c = 0; c < 2 * N; ++c) b(r, c) -= f * b(col, c);
+      }
+    }
+    for (int r = 0; r < N; ++r)
+    {
+      start[r] = static_cast<int>(nzc.size());
+      for (int c = 0; c < N; ++c)
+      {
+        const double v = 0.125 * std::rint(8.0 * b(r, N + c));
+        m[static_cast<size_t>(r) * N + c] = v;
+        if (v != 0.0)
+        {
+          nzc.push_back(c);
+          nzv.push_back(v);
+        }
+      }
+    }
+    start[N] = static_cast<int>(nzc.size());
+  }
+};
+
+const TriquinticMatrix& triquinticMatrix()
+{
+  static const TriquinticMatrix tm;
+  return tm;
+}
+
+// Value and d/ds of sum_ijk a[i + 6j + 36k] s_x^i s_y^j s_z^k (the triquintic branch of interpolate and
+// interpolateGradient, interpolation_energy_grid.cpp:4119-4178, 4348-4410) from the corner data X.
+double quinticFromCorners(const double X[216], const double s[3], double ds[3])
+{
+  const TriquinticMatrix& T = triquinticMatrix();
+  double a[216];
+  for (int r = 0; r < 216; ++r)
+  {
+    double acc = 0.0;
+    for (int q = T.start[r]; q < T.start[r + 1]; ++q) acc += T.nzv[q] * X[T.nzc[q]];
+    a[r] = acc;
+  }
+  double value = 0.0;
+  ds[0] = ds[1] = ds[2] = 0.0;
+  for (int i = 0; i != 6; ++i)
+    for (int j = 0; j != 6; ++j)
+      for (int k = 0; k != 6; ++k)
+      {
+        const double c = a[i + 6 * j + 36 * k];
+        value += c * std::pow(s[0], i) * std::pow(s[1], j) * std::pow(s[2], k);
+        if (i > 0) ds[0] += i * c * std::pow(s[0], i - 1) * std::pow(s[1], j) * std::pow(s[2], k);
+        if (j > 0) ds[1] += j * c * std::pow(s[0], i) * std::pow(s[1], j - 1) * std::pow(s[2], k);
+        if (k > 0) ds[2] += k * c * std::pow(s[0], i) * std::pow(s[1], j) * std::pow(s[2], k - 1);
+      }
+  return value;
+}
+
+// The same for the tricubic map (a[i + 4j + 16k], X[8*v + corner])
+double cubicFromCorners(const double X[64], const double s[3], double ds[3])
+{
+  const TricubicMatrix& T = tricubicMatrix();
+  double a[64];
+  for (int r = 0; r < 64; ++r)
+  {
+    double acc = 0.0;
+    for (int q = T.start[r]; q < T.start[r + 1]; ++q) acc += T.nzv[q] * X[T.nzc[q]];
+    a[r] = acc;
+  }
+  double value = 0.0;
+  ds[0] = ds[1] = ds[2] = 0.0;
+  for (int k = 0; k != 4; ++k)
+    for (int j = 0; j != 4; ++j)
+      for (int i = 0; i != 4; ++i)
+      {
+        const double c = a[i + 4 * j + 16 * k];
+        value += c * std::pow(s[0], i) * std::pow(s[1], j) * std::pow(s[2], k);
+        if (i > 0) ds[0] += i * c * std::pow(s[0], i - 1) * std::pow(s[1], j) * std::pow(s[2], k);
+        if (j > 0) ds[1] += j * c * std::pow(s[0], i) * std::pow(s[1], j - 1) * std::pow(s[2], k);
+        if (k > 0) ds[2] += k * c * std::pow(s[0], i) * std::pow(s[1], j) * std::pow(s[2], k - 1);
+      }
+  return value;
+}
+
+// InterpolationEnergyGrid::interpolate / interpolateGradient, triquintic branch: the cell of pos, its 216 corner
+// values, the polynomial; the gradient mapped to Cartesian with the inverse cell (interpolation_energy_grid.cpp:4410).
+double interpolateTriquintic(const double* data, int nx, int ny, int nz, const Box& unit, const double* pos,
+                             double grad[3])
+{
+  double sraw[3], s[3];
+  matvec(unit.ic, pos, sraw);
+  for (int d = 0; d < 3; ++d) s[d] = fract1(sraw[d]);
+  const int nc[3] = {nx - 1, ny - 1, nz - 1};
+  int64_t i0[3];
+  for (int d = 0; d < 3; ++d)
+  {
+    i0[d] = std::min(static_cast<int64_t>(s[d] * static_cast<double>(nc[d])), static_cast<int64_t>(nc[d] - 1));
+    s[d] = s[d] * static_cast<double>(nc[d]) - static_cast<double>(i0[d]);
+  }
+  double X[216];
+  for (int l = 0; l < 27; ++l)
+    for (int corner = 0; corner < 8; ++corner)
+    {
+      const int64_t x = i0[0] + (corner & 1), y = i0[1] + ((corner >> 1) & 1), z = i0[2] + ((corner >> 2) & 1);
+      X[8 * l + corner] = data[l + 27 * (x + nx * (y + ny * z))];
+    }
+  double ds[3];
+  const double value = quinticFromCorners(X, s, ds);
+  if (grad)
+  {
+    const double g[3] = {ds[0] * nc[0], ds[1] * nc[1], ds[2] * nc[2]};
+    for (int a = 0; a < 3; ++a) grad[a] = unit.ic[a][0] * g[0] + unit.ic[a][1] * g[1] + unit.ic[a][2] * g[2];
+  }
+  return value;
+}
+
 inline int groupOf(const oatom& a) { return a.group_fractional & 0x0f; }
 inline bool fractionalOf(const oatom& a) { return (a.group_fractional >> 4) != 0; }
 
@@ -1269,5 +1621,56 @@ int oracle_select_trial(const double* log_boltzmann, int n, double uniform)
   double ws = uniform * sum;
   while (selected + 1 < n && cumw < ws) cumw += shifted[++selected];
   return selected;
+}
+void oracle_triquintic_fractional_at_position(int grid_type, const off* ff, const obox* super_box, const double* pos,
+                                              int type_a, const obox* unit_box, const oatom* super_atoms, int n,
+                                              int reference_rectangular, double out[27])
+{
+  Box sb = makeBox(super_box), ub = makeBox(unit_box);
+  triquinticFractional(grid_type, ff, sb, pos, type_a, ub, super_atoms, n, reference_rectangular != 0, out);
+}
+
+int oracle_make_triquintic_grid(int grid_type, const off* ff, const obox* unit_box, const oatom* unit_atoms,
+                                int n_unit, int probe_type, double cutoff, int nx, int ny, int nz,
+                                int reference_rectangular, const int64_t* points, int64_t n_points, int threads,
+                                double* out)
+{
+  GridSetup s = gridSetup(unit_box, unit_atoms, n_unit, cutoff, nx, ny, nz);
+  const int64_t total = points ? n_points : static_cast<int64_t>(nx) * ny * nz;
+#ifdef _OPENMP
+  if (threads < 1) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threads)
+#endif
+  for (int64_t p = 0; p < total; ++p)
+  {
+    const int64_t flat = points ? points[p] : p;
+    const int64_t i = flat % nx, j = (flat / nx) % ny, k = flat / (static_cast<int64_t>(nx) * ny);
+    double* dst = points ? out + 27 * p : out + 27 * flat;
+    gridPointQuintic(grid_type, ff, s, probe_type, i, j, k, reference_rectangular != 0, dst);
+  }
+  (void)threads;
+  return static_cast<int>(s.atoms.size());
+}
+
+double oracle_triquintic_interpolate(const double* data, int nx, int ny, int nz, const obox* unit_box,
+                                     const double* pos, double* grad)
+{
+  Box ub = makeBox(unit_box);
+  return interpolateTriquintic(data, nx, ny, nz, ub, pos, grad);
+}
+
+double oracle_interpolant_from_corners(int scheme, const double* X, const double* s, double* ds)
+{
+  double d[3];
+  const double v = scheme == 27 ? quinticFromCorners(X, s, d) : cubicFromCorners(X, s, d);
+  if (ds)
+    for (int a = 0; a < 3; ++a) ds[a] = d[a];
+  return v;
+}
+
+void oracle_triquintic_matrix(double* m)
+{
+  const auto& M = triquinticMatrix().m;
+  std::memcpy(m, M.data(), sizeof(double) * M.size());
 }
 }

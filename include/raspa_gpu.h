@@ -171,6 +171,46 @@ rg_status rg_grid_validate(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* u
                            double weight_beta, int64_t n_points, uint64_t seed, const double* points,
                            rg_grid_validation* out);
 
+/* Interpolation schemes (ForceField::InterpolationScheme, src/raspakit/forcefield/forcefield.ixx:79-84): the values
+ * stored per grid point. */
+enum
+{
+  RG_SCHEME_TRICUBIC = 8,    /* energy and its mixed first derivatives per cell axis (rg_grid_build) */
+  RG_SCHEME_TRIQUINTIC = 27  /* all mixed derivatives up to second order per cell axis (rg_grid_build_triquintic) */
+};
+/* rg_grid_build_triquintic flags */
+enum
+{
+  RG_TRIQUINTIC_REFERENCE_RECTANGULAR = 1 /* rectangular cells: keep the reference's two deviations (see below) */
+};
+
+/* Replaces the triquintic branch of InterpolationEnergyGrid::makeFrameworkInterpolationGrid
+ * (src/raspakit/interpolation_energy_grid.cpp:3882-3962) with the per-point sums of
+ * Interactions::calculateTriquinticFractionalAtPosition (src/raspakit/interactions/framework_molecule_grid.cpp:549-813).
+ * Same arguments as rg_grid_build; FP64; grid_type RG_GRID_LENNARD_JONES or RG_GRID_EWALD_REAL (the reference's
+ * triquintic branch evaluates the full Lennard-Jones factor for the repulsion and attraction types, which are
+ * rejected with RG_ERR_UNSUPPORTED). The result, 27 doubles per point in the reference layout
+ * data[l + 27*(i + nx*(j + ny*k))], channel l the mixed derivative of orders (ox, oy, oz) along the cell axes in the
+ * reference order (0,0,0), (1,0,0), (0,1,0), (0,0,1), (2,0,0), (1,1,0), (1,0,1), (0,2,0), (0,1,1), (0,0,2), (2,1,0),
+ * (2,0,1), (1,2,0), (1,1,1), (0,2,1), (1,0,2), (0,1,2), (2,2,0), (2,0,2), (0,2,2), (2,1,1), (1,2,1), (1,1,2), (2,2,1),
+ * (2,1,2), (1,2,2), (2,2,2), goes to out_device (27*nx*ny*nz doubles) and/or out_host. The values are the exact
+ * derivatives (those of the reference's triclinic branch for any cell). With RG_TRIQUINTIC_REFERENCE_RECTANGULAR a
+ * rectangular cell gets the reference's rectangular branch instead, whose (0,1,0) and (0,0,1) channels are scaled by
+ * cell[0][0] in place of cell[1][1] and cell[2][2] (framework_molecule_grid.cpp:648-650) and whose (2,2,2) channel
+ * lacks its F3 term (:671-676). */
+rg_status rg_grid_build_triquintic(rg_ctx* ctx, int grid_type, const rg_forcefield* ff, const rg_box* unit_cell,
+                                   const rg_atom* unit_atoms, int n_unit_atoms, int probe_type, double cutoff, int nx,
+                                   int ny, int nz, int flags, double* out_device, double* out_host,
+                                   rg_grid_stats* stats);
+
+/* InterpolationEnergyGrid::interpolate and interpolateGradient (interpolation_energy_grid.cpp:3980-4178, 4211-4410,
+ * tricubic and triquintic branches) on the device: the value and, if gradients is non-NULL, the Cartesian gradient
+ * of a grid (a device buffer as rg_grid_build / rg_grid_build_triquintic write it, scheme RG_SCHEME_TRICUBIC or
+ * RG_SCHEME_TRIQUINTIC) at n Cartesian positions (host, 3 doubles each). energies: n doubles; gradients: 3n. */
+rg_status rg_grid_interpolate(rg_ctx* ctx, int scheme, const double* grid_device, int nx, int ny, int nz,
+                              const rg_box* unit_cell, const double* positions, int n, double* energies,
+                              double* gradients);
+
 /* Grid build that allocates nothing, for callers that cannot allocate device memory: applications whose device memory
  * is owned by another allocator (a host framework that reserves the whole device up front, or a memory pool with a hard
  * budget) where any cudaMalloc by a library would fail or break the budget. No counterpart in the reference.
@@ -214,6 +254,13 @@ rg_status rg_system_set_molecules(rg_system* system, const rg_atom* atoms, int n
  * (FP32 pair terms from the FP64 minimum-image displacement, TwoSum-compensated FP32 sums per thread, FP64 totals;
  * the grid branch stays FP64). */
 rg_status rg_system_set_precision(rg_system* system, int precision);
+
+/* Interpolation scheme of this system's grids (ForceField::interpolationScheme): RG_SCHEME_TRICUBIC (the default,
+ * 8 values per point) or RG_SCHEME_TRIQUINTIC (27, from rg_grid_build_triquintic). Set it before the first
+ * rg_system_set_grid. rg_cbmc_external_energies then interpolates with that scheme
+ * (InterpolationEnergyGrid::interpolate, interpolation_energy_grid.cpp:4119-4178); the device-resident Monte Carlo
+ * drivers (rg_gcmc, rg_mixture, rg_proposal) take tricubic systems only. */
+rg_status rg_system_set_interpolation_scheme(rg_system* system, int scheme);
 /* Replaces CBMC::computeExternalNonOverlappingEnergies (src/raspakit/cbmc/interactions.cpp:54-179) and its callees
  * CBMC::computeFrameworkMoleculeEnergy (cbmc/interactions_framework_molecule.cpp:31-104) and
  * CBMC::computeInterMolecularEnergy (cbmc/interactions_intermolecular.cpp:22-95); called from the first-bead schemes

@@ -67,7 +67,8 @@ struct rg_system
   rg_trial_energy* out_mapped = nullptr;  // device view of out_host
   int precision = RG_PRECISION_FP64;      // of rg_cbmc_external_energies
   int sms = 148;
-  int resident[2] = {0, 0};               // CTAs per SM of trialEnergyKernel<false>, <true> (0 = not yet queried)
+  int resident[4] = {0, 0, 0, 0};         // CTAs per SM of trialEnergyKernel<F32, QUINTIC> (0 = not yet queried)
+  int scheme = RG_SCHEME_TRICUBIC;        // values per grid point: 8 (tricubic) or 27 (triquintic)
 };
 
 namespace
@@ -168,7 +169,7 @@ __device__ __forceinline__ Sum32& operator+=(Sum32& s, float x)
   return s;
 }
 
-template <bool F32>
+template <bool F32, bool QUINTIC>
 __global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a, TrialParam small)
 {
   const int trial = blockIdx.x;
@@ -205,7 +206,8 @@ __global__ void __launch_bounds__(kThreads) trialEnergyKernel(TrialArgs a, Trial
       rgd::Grid g{ewald ? a.ewald_grid : a.grid[sT[i].type], a.gnx, a.gny, a.gnz, {}};
       for (int r = 0; r < 3; ++r)
         for (int c = 0; c < 3; ++c) g.ic[r][c] = a.gic[r][c];
-      const double e = rgd::interpolate(g, sT[i].x, sT[i].y, sT[i].z);
+      const double e = QUINTIC ? rgd::interpolateQuintic(g, sT[i].x, sT[i].y, sT[i].z, nullptr)
+                               : rgd::interpolate(g, sT[i].x, sT[i].y, sT[i].z);
       if (ewald)
         acc[1] += sT[i].charge * e;
       else
@@ -495,7 +497,7 @@ rg_status rg_system_set_grid(rg_system* s, int index, const rg_box* unit_cell, i
   if (!first && (nx != s->gnx || ny != s->gny || nz != s->gnz))
     return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_system_set_grid: all grids of a system share one shape");
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
-  const size_t bytes = sizeof(double) * 8 * static_cast<size_t>(nx) * ny * nz;
+  const size_t bytes = sizeof(double) * s->scheme * static_cast<size_t>(nx) * ny * nz;
   if (s->grid_owned[index]) RG_CUDA(ctx, cudaFree(s->grids[index]));
   s->grids[index] = nullptr;
   s->grid_owned[index] = 0;
@@ -539,6 +541,20 @@ rg_status rg_system_set_precision(rg_system* s, int precision)
   return RG_OK;
 }
 
+rg_status rg_system_set_interpolation_scheme(rg_system* s, int scheme)
+{
+  if (!s) return RG_ERR_INVALID_ARGUMENT;
+  if (scheme != RG_SCHEME_TRICUBIC && scheme != RG_SCHEME_TRIQUINTIC)
+    return rg::fail(s->ctx, RG_ERR_INVALID_ARGUMENT, "rg_system_set_interpolation_scheme: RG_SCHEME_TRICUBIC or "
+                                                     "RG_SCHEME_TRIQUINTIC");
+  for (int i = 0; i <= s->n_types; ++i)
+    if (s->grids[i] && scheme != s->scheme)
+      return rg::fail(s->ctx, RG_ERR_INVALID_ARGUMENT,
+                      "rg_system_set_interpolation_scheme: set the scheme before the first grid");
+  s->scheme = scheme;
+  return RG_OK;
+}
+
 rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_trials, int atoms_per_trial, int skip,
                                     int64_t skip_background_molecule, double cutoff_framework_vdw,
                                     double cutoff_molecule_vdw, double cutoff_coulomb, rg_trial_energy* out)
@@ -564,11 +580,13 @@ rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_t
   const int fw_partners = needFw ? s->n_fw : 0;
   const long long total = static_cast<long long>(fw_partners) + s->n_mol;
   const bool f32 = s->precision == RG_PRECISION_FP32C;
-  int& resident = s->resident[f32 ? 1 : 0];
+  const bool quintic = s->scheme == RG_SCHEME_TRIQUINTIC;
+  const auto kernel = f32 ? (quintic ? trialEnergyKernel<true, true> : trialEnergyKernel<true, false>)
+                          : (quintic ? trialEnergyKernel<false, true> : trialEnergyKernel<false, false>);
+  int& resident = s->resident[(f32 ? 1 : 0) + (quintic ? 2 : 0)];
   if (resident == 0)
   {
-    cudaError_t err = f32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, trialEnergyKernel<true>, kThreads, 0)
-                          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, trialEnergyKernel<false>, kThreads, 0);
+    cudaError_t err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, kThreads, 0);
     if (err) return rg::cudaFail(ctx, err, "rg_cbmc_external_energies: occupancy");
     resident = std::max(1, resident);
   }
@@ -626,10 +644,7 @@ rg_status rg_cbmc_external_energies(rg_system* s, const rg_atom* trials, int n_t
   a.counters = s->counters;
   a.out = s->out_mapped;
   dim3 grid(n_trials, n_chunks);
-  if (f32)
-    trialEnergyKernel<true><<<grid, kThreads, 0, ctx->stream>>>(a, small);
-  else
-    trialEnergyKernel<false><<<grid, kThreads, 0, ctx->stream>>>(a, small);
+  kernel<<<grid, kThreads, 0, ctx->stream>>>(a, small);
   RG_CUDA(ctx, cudaGetLastError());
   // the last CTA of each trial wrote its result into mapped pinned memory: completion makes it visible here
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -657,6 +672,8 @@ rg_status systemExport(rg_system* s, FF* ff, Box* box, const double** type_grids
   *ctx = s->ctx;
   return RG_OK;
 }
+
+int systemScheme(const rg_system* s) { return s ? s->scheme : RG_SCHEME_TRICUBIC; }
 
 rg_status systemFramework(rg_system* s, const rg_atom** fw, int* n_fw)
 {

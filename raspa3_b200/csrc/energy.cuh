@@ -229,11 +229,108 @@ __device__ __forceinline__ double interpolate(const Grid& g, double px, double p
   return value;
 }
 
+// Triquintic scheme (27 values per point, data[l + 27*(i + nx*(j + ny*k))]): channel l holds the mixed derivative of
+// orders quinticOrder(l, axis) along the three cell axes, in units of the grid cell (makeFrameworkInterpolationGrid,
+// interpolation_energy_grid.cpp:3882-3962). The reference maps the 216 corner values through a 216x216 matrix to the
+// monomial coefficients of a polynomial of degree 5 per axis (computeCoefficients, :2116-3500); that polynomial is
+// the tensor product of the 1D quintic Hermite bases (value, first and second derivative at both ends), evaluated
+// here directly as 27 x 8 products.
+__host__ __device__ constexpr int quinticOrder(int l, int axis)
+{
+  // orders (x, y, z) packed one per hex digit, x lowest
+  constexpr int packed[27] = {0x000, 0x001, 0x010, 0x100, 0x002, 0x011, 0x101, 0x020, 0x110,
+                              0x200, 0x012, 0x102, 0x021, 0x111, 0x120, 0x201, 0x210, 0x022,
+                              0x202, 0x220, 0x112, 0x121, 0x211, 0x122, 0x212, 0x221, 0x222};
+  return (packed[l] >> (4 * axis)) & 0xf;
+}
+
+// quintic Hermite bases of the corner at t = 0 (value, first, second derivative) and their derivatives; the corner at
+// t = 1 uses u = 1 - t with the first-derivative basis negated
+__device__ __forceinline__ void quinticBases(double t, double b[3], double db[3])
+{
+  const double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
+  b[0] = 1.0 - 10.0 * t3 + 15.0 * t4 - 6.0 * t5;
+  b[1] = t - 6.0 * t3 + 8.0 * t4 - 3.0 * t5;
+  b[2] = 0.5 * t2 - 1.5 * t3 + 1.5 * t4 - 0.5 * t5;
+  db[0] = -30.0 * t2 + 60.0 * t3 - 30.0 * t4;
+  db[1] = 1.0 - 18.0 * t2 + 32.0 * t3 - 15.0 * t4;
+  db[2] = t - 4.5 * t2 + 6.0 * t3 - 2.5 * t4;
+}
+
+// Value of the triquintic interpolant at a Cartesian position (InterpolationEnergyGrid::interpolate, triquintic
+// branch, interpolation_energy_grid.cpp:4119-4178) and, if grad != nullptr, its Cartesian gradient
+// (interpolateGradient, :4348-4410): dE/dt along each cell axis, times (n - 1), mapped with the inverse cell.
+__device__ __forceinline__ double interpolateQuintic(const Grid& g, double px, double py, double pz, double* grad)
+{
+  double s[3];
+  s[0] = fract1(g.ic[0][0] * px + g.ic[1][0] * py + g.ic[2][0] * pz);
+  s[1] = fract1(g.ic[0][1] * px + g.ic[1][1] * py + g.ic[2][1] * pz);
+  s[2] = fract1(g.ic[0][2] * px + g.ic[1][2] * py + g.ic[2][2] * pz);
+  const int nc[3] = {g.nx - 1, g.ny - 1, g.nz - 1};
+  int i0[3];
+  // h[d][corner][order], dh = d/dt
+  double h[3][2][3], dh[3][2][3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    const long long c = static_cast<long long>(s[d] * static_cast<double>(nc[d]));
+    i0[d] = static_cast<int>(c < nc[d] - 1 ? c : nc[d] - 1);
+    const double t = s[d] * static_cast<double>(nc[d]) - static_cast<double>(i0[d]);
+    double b[3], db[3];
+    quinticBases(t, b, db);
+#pragma unroll
+    for (int o = 0; o < 3; ++o)
+    {
+      h[d][0][o] = b[o];
+      dh[d][0][o] = db[o];
+    }
+    quinticBases(1.0 - t, b, db);
+    h[d][1][0] = b[0];
+    h[d][1][1] = -b[1];
+    h[d][1][2] = b[2];
+    dh[d][1][0] = -db[0];
+    dh[d][1][1] = db[1];
+    dh[d][1][2] = -db[2];
+  }
+  double value = 0.0, dt[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int corner = 0; corner < 8; ++corner)
+  {
+    const int cx = corner & 1, cy = (corner >> 1) & 1, cz = (corner >> 2) & 1;
+    const double* p = g.data + 27 * (static_cast<long long>(i0[0] + cx) +
+                                     static_cast<long long>(g.nx) * (static_cast<long long>(i0[1] + cy) +
+                                                                    static_cast<long long>(g.ny) * (i0[2] + cz)));
+#pragma unroll
+    for (int l = 0; l < 27; ++l)
+    {
+      const double v = __ldg(p + l);
+      const int ox = quinticOrder(l, 0), oy = quinticOrder(l, 1), oz = quinticOrder(l, 2);
+      const double hx = h[0][cx][ox], hy = h[1][cy][oy], hz = h[2][cz][oz];
+      value += v * hx * hy * hz;
+      if (grad)
+      {
+        dt[0] += v * dh[0][cx][ox] * hy * hz;
+        dt[1] += v * hx * dh[1][cy][oy] * hz;
+        dt[2] += v * hx * hy * dh[2][cz][oz];
+      }
+    }
+  }
+  if (grad)
+  {
+    const double ds[3] = {dt[0] * nc[0], dt[1] * nc[1], dt[2] * nc[2]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) grad[a] = g.ic[a][0] * ds[0] + g.ic[a][1] * ds[1] + g.ic[a][2] * ds[2];
+  }
+  return value;
+}
+
 // Internal accessors between translation units: the device data of a system and of an Ewald state.
 rg_status systemExport(rg_system* s, FF* ff, Box* box, const double** type_grids /*[64]*/, const double** ewald_grid,
                        int* n_types, int gdims[3], double gic[3][3], rg_ctx** ctx);
 // the framework atoms of a system (device rg_atom array, count)
 rg_status systemFramework(rg_system* s, const rg_atom** fw, int* n_fw);
+// the interpolation scheme of a system's grids (RG_SCHEME_TRICUBIC or RG_SCHEME_TRIQUINTIC)
+int systemScheme(const rg_system* s);
 rg_status proposalExport(rg_proposal* p, const double** cdf, const double** density, int* G, double* eps);
 rg_status ewaldExport(rg_ewald* e, const char4** kvec, const double** temp, const double2** s_rigid, int64_t* nk,
                       int kmax[3], double* alpha, double* single_ion_sum);

@@ -665,6 +665,8 @@ rg_status rg_gcmc_create(rg_system* system, rg_ewald* ewald, const rg_gcmc_compo
   rg_ctx* ctx;
   rg_status st = rgd::systemExport(system, &ff, &box, grids, &ewald_grid, &n_types, gdims, gic, &ctx);
   if (st) return st;
+  if (rgd::systemScheme(system) != RG_SCHEME_TRICUBIC)
+    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_gcmc: tricubic grids only (triquintic grids serve rg_cbmc_external_energies)");
   for (int i = 0; i < comp->n_atoms; ++i)
     if (comp->types[i] < 0 || comp->types[i] >= n_types) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_gcmc: type");
   RG_CUDA(ctx, cudaSetDevice(ctx->device));

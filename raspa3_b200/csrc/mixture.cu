@@ -1283,6 +1283,8 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   rg_ctx* ctx = nullptr;
   rg_status st = rgd::systemExport(system, &ff, &box, tg, &eg, &nt, gd, gic, &ctx);
   if (st) return st;
+  if (rgd::systemScheme(system) != RG_SCHEME_TRICUBIC)
+    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: tricubic grids only (triquintic grids serve rg_cbmc_external_energies)");
   if (nt > kMaxTypes) return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: at most 16 pseudo-atom types");
   const int na = comps[0].n_atoms;
   if (na < 2 || na > kMaxAtoms) return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: molecules of 2-4 atoms");

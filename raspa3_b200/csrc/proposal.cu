@@ -549,6 +549,8 @@ rg_status rg_proposal_sample_targets(rg_system* system, int pseudo_atom, double 
   rg_ctx* ctx;
   rg_status st = rgd::systemExport(system, &ff, &box, grids, &ewald_grid, &n_types, gd, gic, &ctx);
   if (st) return st;
+  if (rgd::systemScheme(system) != RG_SCHEME_TRICUBIC)
+    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_proposal: tricubic grids only (triquintic grids serve rg_cbmc_external_energies)");
   if (pseudo_atom < 0 || pseudo_atom >= 64 || pseudo_atom >= n_types || !grids[pseudo_atom])
     return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_proposal_sample_targets: no grid for this pseudo-atom");
   rgd::Grid g{grids[pseudo_atom], gd[0], gd[1], gd[2], {}};

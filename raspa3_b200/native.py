@@ -24,6 +24,9 @@ GRID_LENNARD_JONES_REPULSION = 2
 GRID_LENNARD_JONES_ATTRACTION = 3
 PRECISION_FP64 = 0
 PRECISION_FP32C = 1
+SCHEME_TRICUBIC = 8
+SCHEME_TRIQUINTIC = 27
+TRIQUINTIC_REFERENCE_RECTANGULAR = 1
 
 _lib = None
 
@@ -149,6 +152,9 @@ def lib():
         L.rg_grid_build.argtypes = [vp, i32, P(RgForceField), P(RgBox), vp, i32, i32, d, i32, i32, i32, i32, vp, vp,
                                     P(GridStats)]
         L.rg_probe_fma_peak.argtypes = [vp, i32, P(d), P(d)]
+        L.rg_grid_build_triquintic.argtypes = [vp, i32, P(RgForceField), P(RgBox), vp, i32, i32, d, i32, i32, i32, i32,
+                                               vp, vp, P(GridStats)]
+        L.rg_grid_interpolate.argtypes = [vp, i32, vp, i32, i32, i32, P(RgBox), vp, i32, vp, vp]
         L.rg_grid_build_set.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, d, i32, i32, i32, i32, i32, vp, vp, vp,
                                         vp, vp]
         L.rg_grid_validate.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, P(RgBox), i32, i32, i32, i32, vp, vp, d,
@@ -158,6 +164,7 @@ def lib():
         L.rg_system_create.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, P(vp)]
         L.rg_system_destroy.argtypes = [vp]
         L.rg_system_set_grid.argtypes = [vp, i32, P(RgBox), i32, i32, i32, vp, i32]
+        L.rg_system_set_interpolation_scheme.argtypes = [vp, i32]
         L.rg_system_set_molecules.argtypes = [vp, vp, i32]
         L.rg_system_set_precision.argtypes = [vp, i32]
         L.rg_cbmc_external_energies.argtypes = [vp, vp, i32, i32, i32, i64, d, d, d, vp]
@@ -279,6 +286,40 @@ class Context:
                                  ctypes.byref(stats) if count_pairs else None)
         check(self.handle, st, "rg_grid_build")
         return out, (stats.as_dict() if count_pairs else None)
+
+    def grid_build_triquintic(self, grid_type: int, ff: ForceField, cell, unit_atoms: np.ndarray, probe_type: int,
+                              cutoff: float, dims, reference_rectangular: bool = False, out_device: int | None = None,
+                              host: bool = True, count_pairs: bool = False):
+        """Triquintic grid (27 doubles per point, rg_grid_build_triquintic). Returns (host array or None, stats or
+        None); out_device: device pointer of 27*nx*ny*nz doubles."""
+        nx, ny, nz = (int(v) for v in dims)
+        atoms = np.ascontiguousarray(unit_atoms, dtype=ATOM_DTYPE)
+        ffs, box = ff_struct(ff), box_struct(cell)
+        out = np.empty(27 * nx * ny * nz) if host else None
+        stats = GridStats()
+        flags = TRIQUINTIC_REFERENCE_RECTANGULAR if reference_rectangular else 0
+        st = lib().rg_grid_build_triquintic(self.handle, grid_type, ctypes.byref(ffs), ctypes.byref(box),
+                                            ctypes.c_void_p(atoms.ctypes.data), len(atoms), probe_type, cutoff, nx, ny,
+                                            nz, flags, out_device,
+                                            None if out is None else ctypes.c_void_p(out.ctypes.data),
+                                            ctypes.byref(stats) if count_pairs else None)
+        check(self.handle, st, "rg_grid_build_triquintic")
+        return out, (stats.as_dict() if count_pairs else None)
+
+    def grid_interpolate(self, scheme: int, grid_device: int, dims, cell, positions, gradients: bool = True):
+        """Values (and Cartesian gradients) of a device grid at Cartesian positions (rg_grid_interpolate)."""
+        nx, ny, nz = (int(v) for v in dims)
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        n = len(pos)
+        e = np.empty(n)
+        g = np.empty((n, 3)) if gradients else None
+        box = box_struct(cell)
+        st = lib().rg_grid_interpolate(self.handle, scheme, ctypes.c_void_p(grid_device), nx, ny, nz,
+                                       ctypes.byref(box), ctypes.c_void_p(pos.ctypes.data), n,
+                                       ctypes.c_void_p(e.ctypes.data),
+                                       None if g is None else ctypes.c_void_p(g.ctypes.data))
+        check(self.handle, st, "rg_grid_interpolate")
+        return e, g
 
     def grid_validate(self, ff: ForceField, unit_cell, unit_atoms: np.ndarray, simulation_cell, probe_type: int, dims,
                       vdw_grid_device: int, ewald_grid_device: int | None = None, probe_charge: float = 0.0,
@@ -450,6 +491,10 @@ class System:
     def set_molecules(self, atoms):
         a, p = _atoms_ptr(atoms)
         check(self.ctx.handle, lib().rg_system_set_molecules(self.handle, p, len(a)), "rg_system_set_molecules")
+
+    def set_interpolation_scheme(self, scheme: int):
+        check(self.ctx.handle, lib().rg_system_set_interpolation_scheme(self.handle, scheme),
+              "rg_system_set_interpolation_scheme")
 
     def set_precision(self, precision: int):
         """Arithmetic of external_energies: PRECISION_FP64 (default) or PRECISION_FP32C."""

@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-alkane", action="store_true", help="skip the batched flexible-chain CBMC section")
     ap.add_argument("--no-mixture", action="store_true", help="skip the large two-component system section")
     ap.add_argument("--no-paths", action="store_true", help="skip the trial-energy and Ewald C-ABI section")
+    ap.add_argument("--no-triquintic", action="store_true", help="skip the triquintic grid section")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the cpu_baseline sample")
     return ap.parse_args()
 
@@ -571,6 +572,81 @@ def run_grid_validation(args, ctx, ff, cell, atoms, dims, outs, rank, world, nat
     return out
 
 
+TRIQUINTIC_STEPS = 5
+# FP64 FLOPs per in-cutoff pair of the rectangular Lennard-Jones triquintic formula as evaluated (add/mul = 1,
+# FMA = 2, reciprocal = 1): distance 8, radial factors F0..F6 45, axis powers 6, the 20 non-trivial monomials 20,
+# factor-monomial products 50, and 64 channel terms as FMAs 128
+TRIQUINTIC_FLOPS_PER_PAIR = 257
+
+
+def run_triquintic(args, ctx, ff, cell, atoms, dims, world, rank, dist, torch):
+    """Triquintic grid (27 values per point, FP64) of the C_co2 Lennard-Jones probe on the configuration-2 framework and
+    grid (133 x 133 x 89 points, 340 MB): grid points/s with the output on the device (CUDA events; each output is
+    larger than L2), end to end with a pinned host output, and the FP64 roofline of the kernel. CPU baseline: the
+    oracle of the reference's triquintic branch on a sample of points, all host cores."""
+    from raspa3_b200 import native
+
+    probe = ff.index("C_co2")
+    npts = dims[0] * dims[1] * dims[2]
+    out = torch.empty(27 * npts, dtype=torch.float64, device="cuda")
+    _, st = ctx.grid_build_triquintic(native.GRID_LENNARD_JONES, ff, cell, atoms, probe, 12.0, dims,
+                                      out_device=out.data_ptr(), host=False, count_pairs=True)
+    stream = torch.cuda.current_stream()
+    for _ in range(2):
+        ctx.grid_build_triquintic(native.GRID_LENNARD_JONES, ff, cell, atoms, probe, 12.0, dims,
+                                  out_device=out.data_ptr(), host=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(TRIQUINTIC_STEPS):
+        ctx.grid_build_triquintic(native.GRID_LENNARD_JONES, ff, cell, atoms, probe, 12.0, dims,
+                                  out_device=out.data_ptr(), host=False)
+    e1.record(stream)
+    e1.synchronize()
+    secs = max_over_ranks(e0.elapsed_time(e1) / 1e3 / TRIQUINTIC_STEPS, world, dist)
+    host = torch.empty(27 * npts, dtype=torch.float64, pin_memory=True).numpy()
+    # untimed warm-up of the end-to-end call (first copies into freshly pinned pages)
+    ctx.grid_build_triquintic(native.GRID_LENNARD_JONES, ff, cell, atoms, probe, 12.0, dims,
+                              out_device=out.data_ptr(), out_host=host)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(2):
+        ctx.grid_build_triquintic(native.GRID_LENNARD_JONES, ff, cell, atoms, probe, 12.0, dims,
+                                  out_device=out.data_ptr(), out_host=host)
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / 2, world, dist)
+    peak64 = ctx.probe_fma_peak(native.PRECISION_FP64)
+    tflops = st["pair_count"] * TRIQUINTIC_FLOPS_PER_PAIR / secs / 1e12
+    res = {"metric": "triquintic grid pts/s through rg_grid_build_triquintic", "unit": "grid points/s",
+           "value": whole_job_rate(npts, world, secs), "ms": 1e3 * secs,
+           "workload": "C_co2 Lennard-Jones triquintic grid (27 channels, FP64) of configuration 2, 133 x 133 x 89 "
+                       "points, 340 MB",
+           "pairs": st["pair_count"], "pairs_per_s": st["pair_count"] / secs,
+           "roofline": {"bound": "fp64", "achieved": tflops, "peak": peak64, "unit": "TFLOP/s",
+                        "frac": tflops / peak64 if peak64 else None, "flops_per_pair": TRIQUINTIC_FLOPS_PER_PAIR,
+                        "peak_source": "rg_probe_fma_peak FP64, measured in this run"},
+           "e2e": {"value": whole_job_rate(npts, world, e2e_s), "unit": "grid points/s",
+                   "h2d_bytes_per_step": st["h2d_bytes"], "d2h_bytes_per_step": 27 * 8 * npts}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        threads = os.cpu_count() or 1
+        rng = np.random.default_rng(6)
+        n = 16 * threads
+        pts = np.sort(rng.choice(npts, size=n, replace=False)).astype(np.int64)
+        t0 = time.perf_counter()
+        oracle.make_grid_triquintic(0, ff, cell, atoms, probe, 12.0, dims, points=pts, threads=threads)
+        t = time.perf_counter() - t0
+        n = int(min(npts, n * max(1.0, args.cpu_seconds / 2 / max(t, 1e-3))))
+        pts = np.sort(rng.choice(npts, size=n, replace=False)).astype(np.int64)
+        t0 = time.perf_counter()
+        oracle.make_grid_triquintic(0, ff, cell, atoms, probe, 12.0, dims, points=pts, threads=threads)
+        t = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": n / t, "unit": "grid points/s", "cores": threads, "kind": "port",
+                               "sample": f"{n} random grid points in {t:.1f} s (FP64 oracle of the triquintic branch "
+                                         f"of makeFrameworkInterpolationGrid, OpenMP over points)"}
+    return res
+
+
 PATH_INSERTIONS = 200   # CBMC insertions whose trial sets go through rg_cbmc_external_energies, per precision
 PATH_DELTAS = 1000      # Ewald Fourier differences through rg_ewald_delta, per box
 PATH_FULL = 20          # full structure-factor recomputes through rg_ewald_full
@@ -966,6 +1042,9 @@ def run_ours(args):
     # ---- one large two-component system on the whole GPU (configuration 5) ----
     if not args.no_mixture:
         line["mixture"] = run_mixture(args, ctx, world, rank, dist, torch)
+    # ---- triquintic grid of configuration 2 (27 channels, FP64) ----
+    if not args.no_triquintic:
+        line["triquintic"] = run_triquintic(args, ctx, ff, cell, atoms, dims, world, rank, dist, torch)
     # ---- paths (b) and (c) on their own through the C-ABI (configuration 5, and configuration 2 for the Ewald) ----
     if not args.no_paths:
         line["paths"] = run_paths(args, ctx, world, rank, dist, torch)

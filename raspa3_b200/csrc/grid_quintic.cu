@@ -40,6 +40,7 @@ constexpr int kBX = 8, kBY = 4, kBZ = 4;  // grid points per brick (one per thre
 constexpr int kThreads = kBX * kBY * kBZ;
 constexpr int kPer = 2;                   // images tested per thread per staging chunk
 constexpr int kChunk = kThreads * kPer;
+constexpr int kSlabs = 8;                 // z-slabs of a build whose host copy overlaps the computation
 
 struct QuinticTable
 {
@@ -56,6 +57,7 @@ struct QuinticParams
   double rc2, filter2, alpha, overlap;
   unsigned long long* pair_count;
   double* out;
+  int zb0;  // first brick along z of this launch
 };
 
 // F_k = (1/r d/dr)^k of 4 eps ((sigma^2/r^2)^6 - (sigma^2/r^2)^3) - shift, k = 0..6: the reference's factors written
@@ -118,13 +120,14 @@ __global__ void __launch_bounds__(kThreads) quinticKernel(QuinticParams p, Quint
   __shared__ int warp_sums[33];
   const int tid = threadIdx.x;
   const int lx = tid % kBX, ly = (tid / kBX) % kBY, lz = tid / (kBX * kBY);
-  const int i = blockIdx.x * kBX + lx, j = blockIdx.y * kBY + ly, k = blockIdx.z * kBZ + lz;
+  const int kb = static_cast<int>(blockIdx.z) + p.zb0;
+  const int i = blockIdx.x * kBX + lx, j = blockIdx.y * kBY + ly, k = kb * kBZ + lz;
   const bool valid = i < p.nx && j < p.ny && k < p.nz;
 
   // grid point (interpolation_energy_grid.cpp:3827-3829) and brick centre, both from fractions of the unit cell
   const double s[3] = {i * p.delta[0], j * p.delta[1], k * p.delta[2]};
   const double sc[3] = {(blockIdx.x * kBX + 0.5 * (kBX - 1)) * p.delta[0], (blockIdx.y * kBY + 0.5 * (kBY - 1)) * p.delta[1],
-                        (blockIdx.z * kBZ + 0.5 * (kBZ - 1)) * p.delta[2]};
+                        (kb * kBZ + 0.5 * (kBZ - 1)) * p.delta[2]};
   double pr[3], ctr[3];
 #pragma unroll
   for (int r = 0; r < 3; ++r)
@@ -302,11 +305,12 @@ QuinticTable makeTable(const rg::HostBox& box, bool reference_rectangular)
   return t;
 }
 
+// bricks [p.zb0, zb1) along z
 template <int TYPE, bool TRI>
-cudaError_t launchQuintic(const QuinticParams& p, const QuinticTable& t, const double4* ipos, const double4* ipar,
-                          bool count, cudaStream_t stream)
+cudaError_t launchQuintic(const QuinticParams& p, int zb1, const QuinticTable& t, const double4* ipos,
+                          const double4* ipar, bool count, cudaStream_t stream)
 {
-  dim3 grid((p.nx + kBX - 1) / kBX, (p.ny + kBY - 1) / kBY, (p.nz + kBZ - 1) / kBZ);
+  dim3 grid((p.nx + kBX - 1) / kBX, (p.ny + kBY - 1) / kBY, zb1 - p.zb0);
   if (count)
     quinticKernel<TYPE, TRI, true><<<grid, kThreads, 0, stream>>>(p, t, ipos, ipar);
   else
@@ -427,15 +431,40 @@ extern "C" rg_status rg_grid_build_triquintic(rg_ctx* ctx, int grid_type, const 
   qp.out = dout;
   const QuinticTable table = makeTable(box, (flags & RG_TRIQUINTIC_REFERENCE_RECTANGULAR) != 0);
   const bool count = stats != nullptr;
-  cudaError_t err;
-  if (grid_type == RG_GRID_EWALD_REAL)
-    err = box.triclinic ? launchQuintic<RG_GRID_EWALD_REAL, true>(qp, table, dpos, dpar, count, ctx->stream)
-                        : launchQuintic<RG_GRID_EWALD_REAL, false>(qp, table, dpos, dpar, count, ctx->stream);
-  else
-    err = box.triclinic ? launchQuintic<RG_GRID_LENNARD_JONES, true>(qp, table, dpos, dpar, count, ctx->stream)
-                        : launchQuintic<RG_GRID_LENNARD_JONES, false>(qp, table, dpos, dpar, count, ctx->stream);
-  if (err != cudaSuccess) return rg::cudaFail(ctx, err, "quinticKernel launch");
-  if (out_host) RG_CUDA(ctx, cudaMemcpyAsync(out_host, dout, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  // with a host output the grid is built in z-slabs and each slab's rows (contiguous in the layout) are copied on the
+  // context's copy stream while the next slabs are computed
+  const int zb = (nz + kBZ - 1) / kBZ;
+  const int n_slabs = out_host ? std::min(zb, kSlabs) : 1;
+  cudaStream_t cs = nullptr;
+  if (out_host)
+  {
+    st = rg::copyStream(ctx, &cs);
+    if (st) return st;
+  }
+  const size_t plane = 27 * static_cast<size_t>(nx) * ny;  // doubles per z-plane
+  for (int sl = 0; sl < n_slabs; ++sl)
+  {
+    qp.zb0 = sl * zb / n_slabs;
+    const int zb1 = (sl + 1) * zb / n_slabs;
+    cudaError_t err;
+    if (grid_type == RG_GRID_EWALD_REAL)
+      err = box.triclinic ? launchQuintic<RG_GRID_EWALD_REAL, true>(qp, zb1, table, dpos, dpar, count, ctx->stream)
+                          : launchQuintic<RG_GRID_EWALD_REAL, false>(qp, zb1, table, dpos, dpar, count, ctx->stream);
+    else
+      err = box.triclinic ? launchQuintic<RG_GRID_LENNARD_JONES, true>(qp, zb1, table, dpos, dpar, count, ctx->stream)
+                          : launchQuintic<RG_GRID_LENNARD_JONES, false>(qp, zb1, table, dpos, dpar, count, ctx->stream);
+    if (err != cudaSuccess) return rg::cudaFail(ctx, err, "quinticKernel launch");
+    if (!out_host) continue;
+    cudaEvent_t ev = nullptr;
+    st = rg::event(ctx, 1 + sl, &ev);
+    if (st) return st;
+    RG_CUDA(ctx, cudaEventRecord(ev, ctx->stream));
+    RG_CUDA(ctx, cudaStreamWaitEvent(cs, ev, 0));
+    const size_t k0 = static_cast<size_t>(qp.zb0) * kBZ, k1 = std::min<size_t>(nz, static_cast<size_t>(zb1) * kBZ);
+    if (k1 > k0)
+      RG_CUDA(ctx, cudaMemcpyAsync(out_host + plane * k0, dout + plane * k0, sizeof(double) * plane * (k1 - k0),
+                                   cudaMemcpyDeviceToHost, cs));
+  }
   if (stats)
   {
     unsigned long long c = 0;
@@ -446,7 +475,12 @@ extern "C" rg_status rg_grid_build_triquintic(rg_ctx* ctx, int grid_type, const 
     stats->h2d_bytes = static_cast<int64_t>(2 * sizeof(double4)) * n_images;
     stats->d2h_bytes = out_host ? static_cast<int64_t>(out_bytes) : 0;
   }
-  if (out_host) RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (out_host)
+  {
+    st = rg::joinCopies(ctx);
+    if (st) return st;
+    RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   return RG_OK;
 }
 

@@ -289,13 +289,14 @@ class Context:
 
     def grid_build_triquintic(self, grid_type: int, ff: ForceField, cell, unit_atoms: np.ndarray, probe_type: int,
                               cutoff: float, dims, reference_rectangular: bool = False, out_device: int | None = None,
-                              host: bool = True, count_pairs: bool = False):
+                              host: bool = True, count_pairs: bool = False, out_host: np.ndarray | None = None):
         """Triquintic grid (27 doubles per point, rg_grid_build_triquintic). Returns (host array or None, stats or
-        None); out_device: device pointer of 27*nx*ny*nz doubles."""
+        None); out_device: device pointer of 27*nx*ny*nz doubles; out_host: a caller-provided host float64 array
+        (e.g. pinned) used instead of a fresh one."""
         nx, ny, nz = (int(v) for v in dims)
         atoms = np.ascontiguousarray(unit_atoms, dtype=ATOM_DTYPE)
         ffs, box = ff_struct(ff), box_struct(cell)
-        out = np.empty(27 * nx * ny * nz) if host else None
+        out = (out_host if out_host is not None else np.empty(27 * nx * ny * nz)) if host else None
         stats = GridStats()
         flags = TRIQUINTIC_REFERENCE_RECTANGULAR if reference_rectangular else 0
         st = lib().rg_grid_build_triquintic(self.handle, grid_type, ctypes.byref(ffs), ctypes.byref(box),

@@ -29,7 +29,9 @@ enum
   RG_ERR_TIMEOUT = 3,
   RG_ERR_UNSUPPORTED = 4,
   RG_ERR_OUT_OF_MEMORY = 5,
-  RG_ERR_NO_DEVICE = 6
+  RG_ERR_NO_DEVICE = 6,
+  RG_ERR_IO = 7,         /* a file could not be written or read */
+  RG_ERR_CACHE_MISS = 8  /* rg_grid_load: no file, or one for other inputs, shape or a damaged one */
 };
 
 /* Byte-for-byte the reference Atom (src/raspakit/atom.ixx:28-39, 64 bytes): a std::span<const Atom> can be passed
@@ -210,6 +212,32 @@ rg_status rg_grid_build_triquintic(rg_ctx* ctx, int grid_type, const rg_forcefie
 rg_status rg_grid_interpolate(rg_ctx* ctx, int scheme, const double* grid_device, int nx, int ny, int nz,
                               const rg_box* unit_cell, const double* positions, int n, double* energies,
                               double* gradients);
+
+/* ---- grids on disk (host code; no device work) ----
+ * The reference rebuilds every grid at start and restart: grids are not in its archive (system.cpp:1558-1562). These
+ * calls keep a grid in a binary file keyed by a fingerprint of its inputs, so a restart can load it instead. */
+
+/* 64-bit FNV-1a fingerprint of everything that determines a grid: grid type, scheme, flags, shape, unit cell, the
+ * pair-table row of the probe (Lennard-Jones grids), cutoff, Ewald alpha, overlap criterion and the unit-cell atoms'
+ * positions, charges and types. */
+uint64_t rg_grid_fingerprint(int grid_type, int scheme, int flags, const rg_forcefield* ff, const rg_box* unit_cell,
+                             const rg_atom* unit_atoms, int n_unit_atoms, int probe_type, int nx, int ny, int nz);
+
+/* Writes scheme*nx*ny*nz doubles (host memory, the layout rg_grid_build / rg_grid_build_triquintic write) with a header
+ * (fingerprint, scheme, shape, cell, checksum of the values) to path, through a temporary file renamed into place. */
+rg_status rg_grid_save(const char* path, uint64_t fingerprint, int scheme, const rg_box* unit_cell, int nx, int ny,
+                       int nz, const double* data);
+
+/* Reads a grid written by rg_grid_save into data (scheme*nx*ny*nz doubles) if the file exists and its fingerprint,
+ * scheme, shape and checksum all match; RG_ERR_CACHE_MISS otherwise (data may then hold partial values). */
+rg_status rg_grid_load(const char* path, uint64_t fingerprint, int scheme, int nx, int ny, int nz, double* data);
+
+/* InterpolationEnergyGrid::writeOutput (interpolation_energy_grid.cpp:4760-4789): a cube file of the energy channel in
+ * K, values in memory order (x fastest), one per line. The point counts are written as the negative numbers the
+ * reference's cube reader expects (parseExternalFieldGridDimensions, :3516-3568); the reference's writer negates an
+ * unsigned count there. origin: 3 doubles or NULL for (0, 0, 0). */
+rg_status rg_grid_write_cube(const char* path, int scheme, const double* data, int nx, int ny, int nz,
+                             const rg_box* unit_cell, const double* origin);
 
 /* Grid build that allocates nothing, for callers that cannot allocate device memory: applications whose device memory
  * is owned by another allocator (a host framework that reserves the whole device up front, or a memory pool with a hard

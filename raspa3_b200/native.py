@@ -18,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libraspagpu.so")
 
 RG_OK = 0
+RG_ERR_CACHE_MISS = 8
 GRID_LENNARD_JONES = 0
 GRID_EWALD_REAL = 1
 GRID_LENNARD_JONES_REPULSION = 2
@@ -155,6 +156,11 @@ def lib():
         L.rg_grid_build_triquintic.argtypes = [vp, i32, P(RgForceField), P(RgBox), vp, i32, i32, d, i32, i32, i32, i32,
                                                vp, vp, P(GridStats)]
         L.rg_grid_interpolate.argtypes = [vp, i32, vp, i32, i32, i32, P(RgBox), vp, i32, vp, vp]
+        L.rg_grid_fingerprint.argtypes = [i32, i32, i32, P(RgForceField), P(RgBox), vp, i32, i32, i32, i32, i32]
+        L.rg_grid_fingerprint.restype = ctypes.c_uint64
+        L.rg_grid_save.argtypes = [ctypes.c_char_p, ctypes.c_uint64, i32, P(RgBox), i32, i32, i32, vp]
+        L.rg_grid_load.argtypes = [ctypes.c_char_p, ctypes.c_uint64, i32, i32, i32, i32, vp]
+        L.rg_grid_write_cube.argtypes = [ctypes.c_char_p, i32, vp, i32, i32, i32, P(RgBox), vp]
         L.rg_grid_build_set.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, d, i32, i32, i32, i32, i32, vp, vp, vp,
                                         vp, vp]
         L.rg_grid_validate.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, P(RgBox), i32, i32, i32, i32, vp, vp, d,
@@ -227,6 +233,40 @@ def check(ctx_handle, status: int, what: str):
     if status != RG_OK:
         msg = lib().rg_ctx_last_error(ctx_handle).decode() if ctx_handle else ""
         raise RaspaGpuError(f"{what} failed with status {status}: {msg}")
+
+
+def grid_fingerprint(grid_type: int, scheme: int, ff: ForceField, cell, unit_atoms, probe_type: int, dims,
+                     flags: int = 0) -> int:
+    """rg_grid_fingerprint: 64-bit key of every input that determines a grid."""
+    atoms = np.ascontiguousarray(unit_atoms, dtype=ATOM_DTYPE)
+    ffs, box = ff_struct(ff), box_struct(cell)
+    return int(lib().rg_grid_fingerprint(grid_type, scheme, flags, ctypes.byref(ffs), ctypes.byref(box),
+                                         ctypes.c_void_p(atoms.ctypes.data), len(atoms), probe_type, *dims))
+
+
+def grid_save(path: str, fingerprint: int, scheme: int, cell, dims, data: np.ndarray):
+    d = np.ascontiguousarray(data, dtype=np.float64)
+    st = lib().rg_grid_save(path.encode(), fingerprint, scheme, ctypes.byref(box_struct(cell)), *dims,
+                            ctypes.c_void_p(d.ctypes.data))
+    check(None, st, "rg_grid_save")
+
+
+def grid_load(path: str, fingerprint: int, scheme: int, dims):
+    """The cached grid, or None on a cache miss (no file, other inputs or shape, damaged file)."""
+    out = np.empty(scheme * int(np.prod(dims)))
+    st = lib().rg_grid_load(path.encode(), fingerprint, scheme, *dims, ctypes.c_void_p(out.ctypes.data))
+    if st == RG_ERR_CACHE_MISS:
+        return None
+    check(None, st, "rg_grid_load")
+    return out
+
+
+def grid_write_cube(path: str, scheme: int, data: np.ndarray, dims, cell, origin=None):
+    d = np.ascontiguousarray(data, dtype=np.float64)
+    o = None if origin is None else np.ascontiguousarray(origin, dtype=np.float64)
+    st = lib().rg_grid_write_cube(path.encode(), scheme, ctypes.c_void_p(d.ctypes.data), *dims,
+                                  ctypes.byref(box_struct(cell)), None if o is None else ctypes.c_void_p(o.ctypes.data))
+    check(None, st, "rg_grid_write_cube")
 
 
 class Context:

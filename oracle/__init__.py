@@ -110,6 +110,8 @@ def lib():
         L.oracle_ewald_rigid.argtypes = [P(OFF), P(OBox), vp, i32, vp]
         L.oracle_ewald_fourier_energy.argtypes = [P(OFF), P(OBox), vp, vp, i32, vp, i32, d, vp, P(OEnergy)]
         L.oracle_ewald_delta.argtypes = [P(OFF), P(OBox), vp, vp, i32, vp, i32, d, vp, vp, P(OEnergy)]
+        L.oracle_ewald_delta_parallel.argtypes = [P(OFF), P(OBox), vp, vp, i64, vp, vp, i32, vp, i32, vp, i32]
+        L.oracle_ewald_delta_parallel.restype = d
         L.oracle_ewald_single_ion.argtypes = [P(OFF), P(OBox), vp, d]
         L.oracle_ewald_single_ion.restype = d
         L.oracle_select_trial.argtypes = [vp, i32, d]
@@ -358,6 +360,23 @@ def ewald_delta(ff, cell, stored, new_atoms, old_atoms, net_charge=0.0, net_char
     lib().oracle_ewald_delta(off(ff), obox(cell), _ptr(st), _ptr(na), len(na), _ptr(oa), len(oa), net_charge,
                              _ptr(nd), _ptr(trial), ctypes.byref(e))
     return e.as_dict(), trial
+
+
+class EwaldDeltaParallel:
+    """The k loop of energyDifferenceEwaldFourier on all host cores (OpenMP over a precomputed k table): the
+    "restated reference loop, parallelised by us" CPU baseline of one Fourier difference."""
+
+    def __init__(self, ff, cell, threads=0):
+        self.off, self.box = off(ff), obox(cell)
+        self.kvec, self.temp, _ = ewald_kvectors(ff, cell)
+        self.threads = threads
+
+    def __call__(self, stored, new_atoms, old_atoms, trial=None):
+        st = np.ascontiguousarray(stored, dtype=np.float64)
+        na, oa = np.ascontiguousarray(new_atoms), np.ascontiguousarray(old_atoms)
+        return lib().oracle_ewald_delta_parallel(self.off, self.box, _ptr(self.kvec), _ptr(self.temp), len(self.temp),
+                                                 _ptr(st), _ptr(na), len(na), _ptr(oa), len(oa), _ptr(trial),
+                                                 self.threads)
 
 
 def ewald_single_ion(ff, cell, pos, charge) -> float:

@@ -1293,6 +1293,52 @@ int64_t oracle_ewald_kvectors(const off* ff, const obox* box, int32_t* kvec, dou
   return n;
 }
 
+double oracle_ewald_delta_parallel(const off* ff, const obox* box, const int32_t* kvec, const double* temp, int64_t nk,
+                                   const double* stored, const oatom* new_atoms, int n_new, const oatom* old_atoms,
+                                   int n_old, double* trial, int threads)
+{
+  // The k loop of energyDifferenceEwaldFourier (ewald.cpp:1098-1162) without dU/dlambda groups, over a precomputed
+  // k table (oracle_ewald_kvectors), parallelised over k with OpenMP: the CPU baseline on all host cores. Returns the
+  // Fourier energy change; trial (10 doubles per k, groups zero) receives the trial structure factors.
+  Box b = makeBox(box);
+  const int n = n_new + n_old;
+  std::vector<const oatom*> ptr(n);
+  for (int i = 0; i < n_old; ++i) ptr[i] = &old_atoms[i];
+  for (int i = 0; i < n_new; ++i) ptr[n_old + i] = &new_atoms[i];
+  EikTables eik(b, ptr, ff->kmax_x, ff->kmax_y, ff->kmax_z);
+  std::vector<double> w(n);
+  for (int i = 0; i < n; ++i) w[i] = (i < n_old ? -1.0 : 1.0) * ptr[i]->scaling_coulomb * ptr[i]->charge;
+  double energy = 0.0;
+#ifdef _OPENMP
+  if (threads < 1) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(static) reduction(+ : energy) num_threads(threads)
+#endif
+  for (int64_t k = 0; k < nk; ++k)
+  {
+    const int kx = kvec[3 * k], ky = kvec[3 * k + 1], kz = kvec[3 * k + 2];
+    Cplx d{0.0, 0.0};
+    for (int i = 0; i < n; ++i)
+    {
+      const Cplx ei = cmul(eik.xy(i, kx, ky), eik.zf(i, kz));
+      d.re += w[i] * ei.re;
+      d.im += w[i] * ei.im;
+    }
+    const double* s = stored + 10 * k;
+    const Cplx S{s[0], s[1]};
+    const Cplx T{S.re + d.re, S.im + d.im};
+    energy += temp[k] * (norm2(T) - norm2(S));
+    if (trial)
+    {
+      double* t = trial + 10 * k;
+      t[0] = T.re;
+      t[1] = T.im;
+      for (int g = 2; g < 10; ++g) t[g] = 0.0;
+    }
+  }
+  (void)threads;
+  return energy;
+}
+
 void oracle_ewald_rigid(const off* ff, const obox* box, const oatom* fw, int n_fw, double* s_rigid)
 {
   // precomputeEwaldFourierRigid, ewald.cpp:276-348

@@ -236,7 +236,7 @@ __device__ __forceinline__ int sym2(int i, int j)
 // NP Lennard-Jones probes (1 or 2) share one candidate set: the distances, the reciprocal and the staging are computed
 // once per pair and each probe adds its own factors (ipar holds NP parameter sets per image).
 template <typename Real, int TYPE, bool TRICLINIC, bool COUNT, int NP>
-__global__ void __launch_bounds__(256, (NP == 2 && sizeof(Real) == 4) ? 3 : 1) gridKernel(GridParams p, const double4* __restrict__ ipos,
+__global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1) gridKernel(GridParams p, const double4* __restrict__ ipos,
                                                   const double4* __restrict__ ipar, int bx, int by, int bz)
 {
   using V4 = typename Vec4<Real>::T;

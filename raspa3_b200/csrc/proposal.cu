@@ -31,7 +31,7 @@ constexpr int kIn = 96, kH = 64;
 constexpr int kParams = kH * kIn + kH + kH * kH + kH + kH + 1;  // 10433
 constexpr int kOffW1 = 0, kOffB1 = kH * kIn, kOffW2 = kOffB1 + kH, kOffB2 = kOffW2 + kH * kH, kOffW3 = kOffB2 + kH,
               kOffB3 = kOffW3 + kH;
-constexpr int kTile = 64;
+constexpr int kTile = 32;  // samples per CTA: a batch of 4,096 spreads over 128 CTAs (one per SM)
 constexpr int kThreads = 256;
 constexpr int kLdIn = kIn + 1, kLdH = kH + 1;  // padded leading dimensions (no shared-memory bank conflicts)
 
@@ -581,11 +581,14 @@ rg_status rg_proposal_create(rg_mlp* m, int32_t cells_per_axis, double eps_unifo
     s[3 * c + 1] = static_cast<float>((j + 0.5) / G);
     s[3 * c + 2] = static_cast<float>((k + 0.5) / G);
   }
-  float *ds = nullptr, *df = nullptr;
-  RG_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&ds), sizeof(float) * 3 * nc));
-  RG_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&df), sizeof(float) * nc));
+  // cell centres and MLP outputs in the context's scratch slot 6 (no allocation or free per table)
+  void* scr = nullptr;
+  rg_status st = rg::scratch(ctx, 6, sizeof(float) * 4 * static_cast<size_t>(nc), &scr);
+  if (st) return st;
+  float* ds = static_cast<float*>(scr);
+  float* df = ds + 3 * nc;
   cudaError_t err = cudaMemcpyAsync(ds, s.data(), sizeof(float) * 3 * nc, cudaMemcpyHostToDevice, ctx->stream);
-  rg_status st = err ? rg::cudaFail(ctx, err, "rg_proposal_create") : rg_mlp_evaluate(m, ds, nc, df);
+  st = err ? rg::cudaFail(ctx, err, "rg_proposal_create") : rg_mlp_evaluate(m, ds, nc, df);
   std::vector<float> f(nc);
   if (!st)
   {
@@ -593,8 +596,6 @@ rg_status rg_proposal_create(rg_mlp* m, int32_t cells_per_axis, double eps_unifo
     if (!err) err = cudaStreamSynchronize(ctx->stream);
     if (err) st = rg::cudaFail(ctx, err, "rg_proposal_create");
   }
-  cudaFree(ds);
-  cudaFree(df);
   if (st) return st;
   // p_c ~ exp(f_c - max f), cumulative in FP64
   double fmax = -1e300;

@@ -239,6 +239,28 @@ rg_status rg_grid_load(const char* path, uint64_t fingerprint, int scheme, int n
 rg_status rg_grid_write_cube(const char* path, int scheme, const double* data, int nx, int ny, int nz,
                              const rg_box* unit_cell, const double* origin);
 
+/* Hessian part of the triquintic grid test. sums[0..23]: the VDW term, sums[24..47]: the charge term; per term four
+ * Boltzmann-weighted groups of six components (xx, xy, xz, yy, yz, zz): interpolated, analytical, squared difference,
+ * squared analytical. The averages and relative errors follow from them as for the energy. */
+typedef struct rg_grid_validation_hessian
+{
+  double sums[48];
+  double hessian_table[6], hessian_full[6], hessian_relative_error[6];
+  double charge_hessian_table[6], charge_hessian_full[6], charge_hessian_relative_error[6];
+} rg_grid_validation_hessian;
+
+/* The grid test of the triquintic scheme (system_interpolation_grids.cpp:240-760, triquintic branches): as
+ * rg_grid_validate, with grids written by rg_grid_build_triquintic, the triquintic interpolant
+ * (InterpolationEnergyGrid::interpolateHessian) and, in addition, the Hessians of both terms. The analytical side is
+ * the exact derivative of the pair sums: for a rectangular non-cubic cell the reference's own rectangular branch
+ * would report y and z gradients scaled by cell[0][0] (see rg_grid_build_triquintic). */
+rg_status rg_grid_validate_triquintic(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* unit_cell,
+                                      const rg_atom* unit_atoms, int n_unit_atoms, const rg_box* simulation_box,
+                                      int probe_type, int nx, int ny, int nz, const double* vdw_grid_device,
+                                      const double* ewald_grid_device, double probe_charge, double weight_beta,
+                                      int64_t n_points, uint64_t seed, const double* points, rg_grid_validation* out,
+                                      rg_grid_validation_hessian* hessian);
+
 /* Grid build that allocates nothing, for callers that cannot allocate device memory: applications whose device memory
  * is owned by another allocator (a host framework that reserves the whole device up front, or a memory pool with a hard
  * budget) where any cudaMalloc by a library would fail or break the budget. No counterpart in the reference.

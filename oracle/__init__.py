@@ -94,6 +94,8 @@ def lib():
         L.oracle_interpolant_from_corners.argtypes = [i32, vp, vp, vp]
         L.oracle_interpolant_from_corners.restype = d
         L.oracle_triquintic_matrix.argtypes = [vp]
+        L.oracle_grid_validate_triquintic.argtypes = [P(OFF), P(OBox), vp, i32, P(OBox), i32, i32, i32, i32, vp, vp, d, d,
+                                                      vp, i64, vp]
         L.oracle_grid_interpolate.argtypes = [vp, i32, i32, i32, P(OBox), vp]
         L.oracle_grid_interpolate.restype = d
         L.oracle_grid_validate.argtypes = [P(OFF), P(OBox), vp, i32, P(OBox), i32, i32, i32, i32, vp, vp, d, d, vp,
@@ -266,6 +268,22 @@ def grid_validate(ff, unit_cell, unit_atoms, simulation_cell, probe_type, dims, 
     lib().oracle_grid_validate(off(ff), obox(unit_cell), _ptr(atoms), len(atoms), obox(simulation_cell), probe_type,
                                nx, ny, nz, _ptr(vg), _ptr(eg), probe_charge, weight_beta, _ptr(pts), len(pts),
                                _ptr(out))
+    return out
+
+
+def grid_validate_triquintic(ff, unit_cell, unit_atoms, simulation_cell, probe_type, dims, vdw_grid, ewald_grid,
+                             probe_charge, weight_beta, points):
+    """The grid test of the triquintic scheme at the given points: 84 values (the 36 of grid_validate, then 24 VDW and
+    24 charge Hessian sums)."""
+    nx, ny, nz = dims
+    atoms = np.ascontiguousarray(unit_atoms)
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    vg = np.ascontiguousarray(vdw_grid, dtype=np.float64)
+    eg = None if ewald_grid is None else np.ascontiguousarray(ewald_grid, dtype=np.float64)
+    out = np.zeros(84)
+    lib().oracle_grid_validate_triquintic(off(ff), obox(unit_cell), _ptr(atoms), len(atoms), obox(simulation_cell),
+                                          probe_type, nx, ny, nz, _ptr(vg), _ptr(eg), probe_charge, weight_beta,
+                                          _ptr(pts), len(pts), _ptr(out))
     return out
 
 

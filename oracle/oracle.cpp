@@ -813,6 +813,97 @@ double quinticFromCorners(const double X[216], const double s[3], double ds[3])
   return value;
 }
 
+// Value, d/ds and d2/(ds_a ds_b) (h[0..5]: xx, xy, xz, yy, yz, zz) of the triquintic cell polynomial from the corner
+// data X (the triquintic branch of interpolateHessian, interpolation_energy_grid.cpp:4602-4745)
+double quinticFromCornersHessian(const double X[216], const double s[3], double ds[3], double h[6])
+{
+  const TriquinticMatrix& T = triquinticMatrix();
+  double a[216];
+  for (int r = 0; r < 216; ++r)
+  {
+    double acc = 0.0;
+    for (int q = T.start[r]; q < T.start[r + 1]; ++q) acc += T.nzv[q] * X[T.nzc[q]];
+    a[r] = acc;
+  }
+  // powers and their first and second derivatives per axis
+  double pw[3][6], d1[3][6], d2[3][6];
+  for (int ax = 0; ax < 3; ++ax)
+    for (int e = 0; e < 6; ++e)
+    {
+      pw[ax][e] = std::pow(s[ax], e);
+      d1[ax][e] = e > 0 ? e * std::pow(s[ax], e - 1) : 0.0;
+      d2[ax][e] = e > 1 ? e * (e - 1) * std::pow(s[ax], e - 2) : 0.0;
+    }
+  double value = 0.0;
+  for (int q = 0; q < 3; ++q) ds[q] = 0.0;
+  for (int q = 0; q < 6; ++q) h[q] = 0.0;
+  for (int i = 0; i != 6; ++i)
+    for (int j = 0; j != 6; ++j)
+      for (int k = 0; k != 6; ++k)
+      {
+        const double c = a[i + 6 * j + 36 * k];
+        value += c * pw[0][i] * pw[1][j] * pw[2][k];
+        ds[0] += c * d1[0][i] * pw[1][j] * pw[2][k];
+        ds[1] += c * pw[0][i] * d1[1][j] * pw[2][k];
+        ds[2] += c * pw[0][i] * pw[1][j] * d1[2][k];
+        h[0] += c * d2[0][i] * pw[1][j] * pw[2][k];
+        h[1] += c * d1[0][i] * d1[1][j] * pw[2][k];
+        h[2] += c * d1[0][i] * pw[1][j] * d1[2][k];
+        h[3] += c * pw[0][i] * d2[1][j] * pw[2][k];
+        h[4] += c * pw[0][i] * d1[1][j] * d1[2][k];
+        h[5] += c * pw[0][i] * pw[1][j] * d2[2][k];
+      }
+  return value;
+}
+
+// Cartesian gradient and Hessian from derivatives along the cell axes: grad = M^T g, H = M^T Hs M with M the inverse
+// cell (interpolation_energy_grid.cpp:4745-4748, system_interpolation_grids.cpp:336-350)
+void toCartesian(const Box& unit, const double g[3], const double hs[6], double grad[3], double hc[6])
+{
+  const double Hs[3][3] = {{hs[0], hs[1], hs[2]}, {hs[1], hs[3], hs[4]}, {hs[2], hs[4], hs[5]}};
+  for (int i = 0; i < 3; ++i) grad[i] = unit.ic[i][0] * g[0] + unit.ic[i][1] * g[1] + unit.ic[i][2] * g[2];
+  const int pairs[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  for (int q = 0; q < 6; ++q)
+  {
+    const int i = pairs[q][0], j = pairs[q][1];
+    double acc = 0.0;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) acc += unit.ic[i][a] * unit.ic[j][b] * Hs[a][b];
+    hc[q] = acc;
+  }
+}
+
+// interpolateHessian, triquintic branch: value, Cartesian gradient and Hessian
+double interpolateTriquinticHessian(const double* data, int nx, int ny, int nz, const Box& unit, const double* pos,
+                                    double grad[3], double hess[6])
+{
+  double sraw[3], s[3];
+  matvec(unit.ic, pos, sraw);
+  for (int d = 0; d < 3; ++d) s[d] = fract1(sraw[d]);
+  const int nc[3] = {nx - 1, ny - 1, nz - 1};
+  int64_t i0[3];
+  for (int d = 0; d < 3; ++d)
+  {
+    i0[d] = std::min(static_cast<int64_t>(s[d] * static_cast<double>(nc[d])), static_cast<int64_t>(nc[d] - 1));
+    s[d] = s[d] * static_cast<double>(nc[d]) - static_cast<double>(i0[d]);
+  }
+  double X[216];
+  for (int l = 0; l < 27; ++l)
+    for (int corner = 0; corner < 8; ++corner)
+    {
+      const int64_t x = i0[0] + (corner & 1), y = i0[1] + ((corner >> 1) & 1), z = i0[2] + ((corner >> 2) & 1);
+      X[8 * l + corner] = data[l + 27 * (x + nx * (y + ny * z))];
+    }
+  double ds[3], hs[6];
+  const double value = quinticFromCornersHessian(X, s, ds, hs);
+  const double g[3] = {ds[0] * nc[0], ds[1] * nc[1], ds[2] * nc[2]};
+  const int pairs[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  double h[6];
+  for (int q = 0; q < 6; ++q) h[q] = hs[q] * nc[pairs[q][0]] * nc[pairs[q][1]];
+  toCartesian(unit, g, h, grad, hess);
+  return value;
+}
+
 // The same for the tricubic map (a[i + 4j + 16k], X[8*v + corner])
 double cubicFromCorners(const double X[64], const double s[3], double ds[3])
 {
@@ -1155,6 +1246,83 @@ void oracle_grid_validate(const off* ff, const obox* unit_box, const oatom* unit
       for (int a = 0; a < 3; ++a)
         cf[a] = (gs.unit.ic[a][0] * d8[1] + gs.unit.ic[a][1] * d8[2] + gs.unit.ic[a][2] * d8[3]) * probe_charge * toK;
       accumulate(out + 17, w, eci, ecf, ci, cf);
+      out[35] += 1.0;
+    }
+  }
+}
+
+void oracle_grid_validate_triquintic(const off* ff, const obox* unit_box, const oatom* unit_atoms, int n_unit,
+                                     const obox* simulation_box, int probe_type, int nx, int ny, int nz,
+                                     const double* vdw_grid, const double* ewald_grid, double probe_charge,
+                                     double weight_beta, const double* points, int64_t n_points, double* out)
+{
+  // The grid test of the triquintic scheme (system_interpolation_grids.cpp:272-651): energy, gradient and Hessian,
+  // interpolated (interpolateHessian) and analytical (calculateTriquinticFractionalAtPosition, the gradient from its
+  // channels 1-3 and the Hessian from channels 4-9 mapped with the inverse cell), in K, Boltzmann-weighted. The
+  // analytical channels are the exact ones (for a rectangular cell the reference's own branch scales its y and z first
+  // derivatives by cell[0][0]). out: the 36 values of oracle_grid_validate, then 24 VDW and 24 charge Hessian sums
+  // (interpolated, full, squared difference, squared full; components xx, xy, xz, yy, yz, zz).
+  const GridSetup gs = gridSetup(unit_box, unit_atoms, n_unit, ff->cutoff_framework_vdw, nx, ny, nz);
+  const Box sim = makeBox(simulation_box);
+  const double toK = energyConversionFactor() * kAvogadroConstant / kMolarGasConstant;
+  for (int i = 0; i < 84; ++i) out[i] = 0.0;
+  auto accumulate = [&](double* o, double* oh, double w, double ei, double ef, const double* gi, const double* gf,
+                        const double* hi, const double* hf)
+  {
+    o[0] += w;
+    o[1] += ei * w;
+    o[2] += ef * w;
+    o[3] += (ef - ei) * (ef - ei) * w;
+    o[4] += ef * ef * w;
+    for (int a = 0; a < 3; ++a)
+    {
+      o[5 + a] += gi[a] * w;
+      o[8 + a] += gf[a] * w;
+      o[11 + a] += (gf[a] - gi[a]) * (gf[a] - gi[a]) * w;
+      o[14 + a] += gf[a] * gf[a] * w;
+    }
+    for (int q = 0; q < 6; ++q)
+    {
+      oh[q] += hi[q] * w;
+      oh[6 + q] += hf[q] * w;
+      oh[12 + q] += (hf[q] - hi[q]) * (hf[q] - hi[q]) * w;
+      oh[18 + q] += hf[q] * hf[q] * w;
+    }
+  };
+  // analytical energy, gradient and Hessian from the 27 fractional channels
+  auto analytical = [&](int grid_type, int type, const double* pos, double scale, double& e, double* g, double* h)
+  {
+    double d[27];
+    triquinticFractional(grid_type, ff, gs.super, pos, type, gs.unit, gs.atoms.data(),
+                         static_cast<int>(gs.atoms.size()), false, d);
+    const double gfrac[3] = {d[1], d[2], d[3]};
+    const double hfrac[6] = {d[4], d[5], d[6], d[7], d[8], d[9]};
+    toCartesian(gs.unit, gfrac, hfrac, g, h);
+    e = d[0] * scale;
+    for (int a = 0; a < 3; ++a) g[a] *= scale;
+    for (int q = 0; q < 6; ++q) h[q] *= scale;
+  };
+  for (int64_t p = 0; p < n_points; ++p)
+  {
+    double pos[3];
+    matvec(sim.c, points + 3 * p, pos);
+    double gi[3], hi[6], ef, gf[3], hf[6];
+    const double ei = interpolateTriquinticHessian(vdw_grid, nx, ny, nz, gs.unit, pos, gi, hi) * toK;
+    for (int a = 0; a < 3; ++a) gi[a] *= toK;
+    for (int q = 0; q < 6; ++q) hi[q] *= toK;
+    analytical(0, probe_type, pos, toK, ef, gf, hf);
+    const double w = std::exp(-weight_beta * ef);
+    accumulate(out, out + 36, w, ei, ef, gi, gf, hi, hf);
+    out[34] += 1.0;
+    if (ewald_grid && probe_charge != 0.0 && ef < ff->overlap_criteria)
+    {
+      const double sc = probe_charge * toK;
+      double ci[3], chi[6], ecf, cf[3], chf[6];
+      const double eci = interpolateTriquinticHessian(ewald_grid, nx, ny, nz, gs.unit, pos, ci, chi) * sc;
+      for (int a = 0; a < 3; ++a) ci[a] *= sc;
+      for (int q = 0; q < 6; ++q) chi[q] *= sc;
+      analytical(1, 0, pos, sc, ecf, cf, chf);
+      accumulate(out + 17, out + 60, w, eci, ecf, ci, cf, chi, chf);
       out[35] += 1.0;
     }
   }

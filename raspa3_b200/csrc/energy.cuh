@@ -324,6 +324,104 @@ __device__ __forceinline__ double interpolateQuintic(const Grid& g, double px, d
   return value;
 }
 
+// second derivatives of the quintic Hermite bases of the corner at t = 0
+__device__ __forceinline__ void quinticBases2(double t, double d2[3])
+{
+  const double t2 = t * t, t3 = t2 * t;
+  d2[0] = -60.0 * t + 180.0 * t2 - 120.0 * t3;
+  d2[1] = -36.0 * t + 96.0 * t2 - 60.0 * t3;
+  d2[2] = 1.0 - 9.0 * t + 18.0 * t2 - 10.0 * t3;
+}
+
+// Value, Cartesian gradient and Hessian (xx, xy, xz, yy, yz, zz) of the triquintic interpolant
+// (InterpolationEnergyGrid::interpolateHessian, triquintic branch, interpolation_energy_grid.cpp:4602-4748): the
+// derivatives along the cell axes of the tensor-product Hermite form, times (n - 1) per axis, mapped with the inverse
+// cell (grad = M^T g, H = M^T Hs M).
+__device__ __forceinline__ double interpolateQuinticHessian(const Grid& g, double px, double py, double pz,
+                                                            double grad[3], double hess[6])
+{
+  double s[3];
+  s[0] = fract1(g.ic[0][0] * px + g.ic[1][0] * py + g.ic[2][0] * pz);
+  s[1] = fract1(g.ic[0][1] * px + g.ic[1][1] * py + g.ic[2][1] * pz);
+  s[2] = fract1(g.ic[0][2] * px + g.ic[1][2] * py + g.ic[2][2] * pz);
+  const int nc[3] = {g.nx - 1, g.ny - 1, g.nz - 1};
+  int i0[3];
+  double h[3][2][3], dh[3][2][3], d2h[3][2][3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+  {
+    const long long c = static_cast<long long>(s[d] * static_cast<double>(nc[d]));
+    i0[d] = static_cast<int>(c < nc[d] - 1 ? c : nc[d] - 1);
+    const double t = s[d] * static_cast<double>(nc[d]) - static_cast<double>(i0[d]);
+    double b[3], db[3], b2[3];
+    quinticBases(t, b, db);
+    quinticBases2(t, b2);
+#pragma unroll
+    for (int o = 0; o < 3; ++o)
+    {
+      h[d][0][o] = b[o];
+      dh[d][0][o] = db[o];
+      d2h[d][0][o] = b2[o];
+    }
+    quinticBases(1.0 - t, b, db);
+    quinticBases2(1.0 - t, b2);
+    h[d][1][0] = b[0];
+    h[d][1][1] = -b[1];
+    h[d][1][2] = b[2];
+    dh[d][1][0] = -db[0];
+    dh[d][1][1] = db[1];
+    dh[d][1][2] = -db[2];
+    d2h[d][1][0] = b2[0];
+    d2h[d][1][1] = -b2[1];
+    d2h[d][1][2] = b2[2];
+  }
+  double value = 0.0, dt[3] = {0.0, 0.0, 0.0}, ht[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int corner = 0; corner < 8; ++corner)
+  {
+    const int cx = corner & 1, cy = (corner >> 1) & 1, cz = (corner >> 2) & 1;
+    const double* p = g.data + 27 * (static_cast<long long>(i0[0] + cx) +
+                                     static_cast<long long>(g.nx) * (static_cast<long long>(i0[1] + cy) +
+                                                                    static_cast<long long>(g.ny) * (i0[2] + cz)));
+#pragma unroll
+    for (int l = 0; l < 27; ++l)
+    {
+      const double v = __ldg(p + l);
+      const int ox = quinticOrder(l, 0), oy = quinticOrder(l, 1), oz = quinticOrder(l, 2);
+      const double hx = h[0][cx][ox], hy = h[1][cy][oy], hz = h[2][cz][oz];
+      const double gx = dh[0][cx][ox], gy = dh[1][cy][oy], gz = dh[2][cz][oz];
+      value += v * hx * hy * hz;
+      dt[0] += v * gx * hy * hz;
+      dt[1] += v * hx * gy * hz;
+      dt[2] += v * hx * hy * gz;
+      ht[0] += v * d2h[0][cx][ox] * hy * hz;
+      ht[1] += v * gx * gy * hz;
+      ht[2] += v * gx * hy * gz;
+      ht[3] += v * hx * d2h[1][cy][oy] * hz;
+      ht[4] += v * hx * gy * gz;
+      ht[5] += v * hx * hy * d2h[2][cz][oz];
+    }
+  }
+  const double gs[3] = {dt[0] * nc[0], dt[1] * nc[1], dt[2] * nc[2]};
+  const double Hs[3][3] = {{ht[0] * nc[0] * nc[0], ht[1] * nc[0] * nc[1], ht[2] * nc[0] * nc[2]},
+                           {ht[1] * nc[0] * nc[1], ht[3] * nc[1] * nc[1], ht[4] * nc[1] * nc[2]},
+                           {ht[2] * nc[0] * nc[2], ht[4] * nc[1] * nc[2], ht[5] * nc[2] * nc[2]}};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) grad[a] = g.ic[a][0] * gs[0] + g.ic[a][1] * gs[1] + g.ic[a][2] * gs[2];
+  constexpr int pi[6] = {0, 0, 0, 1, 1, 2}, pj[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+  {
+    double acc = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) acc += g.ic[pi[q]][a] * g.ic[pj[q]][b] * Hs[a][b];
+    hess[q] = acc;
+  }
+  return value;
+}
+
 // Internal accessors between translation units: the device data of a system and of an Ewald state.
 rg_status systemExport(rg_system* s, FF* ff, Box* box, const double** type_grids /*[64]*/, const double** ewald_grid,
                        int* n_types, int gdims[3], double gic[3][3], rg_ctx** ctx);

@@ -31,6 +31,9 @@ namespace
 constexpr int kThreads = 256;
 constexpr int kTile = 128;  // images staged per tile
 constexpr int kSums = 36;   // 17 VDW sums, 17 charge sums, two counts (the layout of rg_grid_validation.sums)
+constexpr int kHessSums = 48;  // triquintic scheme: 24 VDW and 24 charge Hessian sums (rg_grid_validation_hessian.sums)
+template <int SCHEME>
+constexpr int sumsOf() { return SCHEME == RG_SCHEME_TRIQUINTIC ? kSums + kHessSums : kSums; }
 
 struct ValidateParams
 {
@@ -65,10 +68,37 @@ __device__ __forceinline__ void accumulate(double* o, double w, double ei, doubl
   }
 }
 
+// Hessian sums of one term: interpolated, full, squared difference, squared full, for xx, xy, xz, yy, yz, zz
+__device__ __forceinline__ void accumulateHessian(double* o, double w, const double* hi, const double* hf)
+{
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+  {
+    o[q] += hi[q] * w;
+    o[6 + q] += hf[q] * w;
+    o[12 + q] += (hf[q] - hi[q]) * (hf[q] - hi[q]) * w;
+    o[18 + q] += hf[q] * hf[q] * w;
+  }
+}
+
+// H_ij += F2 dr_i dr_j + F1 delta_ij (xx, xy, xz, yy, yz, zz)
+__device__ __forceinline__ void addHessian(double* h, double f1, double f2, double dx, double dy, double dz)
+{
+  h[0] += f2 * dx * dx + f1;
+  h[1] += f2 * dx * dy;
+  h[2] += f2 * dx * dz;
+  h[3] += f2 * dy * dy + f1;
+  h[4] += f2 * dy * dz;
+  h[5] += f2 * dz * dz + f1;
+}
+
+template <int SCHEME>
 __global__ void __launch_bounds__(kThreads) gridValidateKernel(ValidateParams p)
 {
+  constexpr bool Q = SCHEME == RG_SCHEME_TRIQUINTIC;
+  constexpr int NS = sumsOf<SCHEME>();
   __shared__ double4 tpos[kTile], tpar[kTile];
-  __shared__ double red[kThreads / 32][kSums];
+  __shared__ double red[kThreads / 32][NS];
   const long long i = static_cast<long long>(blockIdx.x) * kThreads + threadIdx.x;
   const bool active = i < p.n_points;
   double u[3] = {0.5, 0.5, 0.5};
@@ -101,7 +131,7 @@ __global__ void __launch_bounds__(kThreads) gridValidateKernel(ValidateParams p)
   }
   // analytical Lennard-Jones energy and gradient (potentialLennardJonesTricubicDerivative: U = B - A - shift,
   // F1 = (6A - 12B)/r^2 with A = 4 eps t^3, B = A t^3; gradient = F1 * (r - r_image))
-  double ev = 0.0, gv[3] = {0.0, 0.0, 0.0};
+  double ev = 0.0, gv[3] = {0.0, 0.0, 0.0}, hv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   for (int base = 0; base < p.n_vdw; base += kTile)
   {
     const int n = min(kTile, p.n_vdw - base);
@@ -129,17 +159,23 @@ __global__ void __launch_bounds__(kThreads) gridValidateKernel(ValidateParams p)
           gv[0] += f1 * dx;
           gv[1] += f1 * dy;
           gv[2] += f1 * dz;
+          // F2 = (168 B - 48 A) / r^4 (potentialLennardJonesTriquinticDerivative)
+          if constexpr (Q) addHessian(hv, f1, (168.0 * B - 48.0 * A) * inv * inv, dx, dy, dz);
         }
       }
   }
-  double sums[kSums];
+  double sums[NS];
 #pragma unroll
-  for (int c = 0; c < kSums; ++c) sums[c] = 0.0;
+  for (int c = 0; c < NS; ++c) sums[c] = 0.0;
   double evK = 0.0, w = 0.0;
   if (active)
   {
-    double gi[3], gf[3];
-    const double ei = rgd::interpolateGradient(p.vdw, r[0], r[1], r[2], gi) * p.to_kelvin;
+    double gi[3], gf[3], hi[6], hf[6];
+    double ei;
+    if constexpr (Q)
+      ei = rgd::interpolateQuinticHessian(p.vdw, r[0], r[1], r[2], gi, hi) * p.to_kelvin;
+    else
+      ei = rgd::interpolateGradient(p.vdw, r[0], r[1], r[2], gi) * p.to_kelvin;
 #pragma unroll
     for (int a = 0; a < 3; ++a)
     {
@@ -150,12 +186,22 @@ __global__ void __launch_bounds__(kThreads) gridValidateKernel(ValidateParams p)
     w = exp(-p.beta * evK);
     accumulate(sums, w, ei, evK, gi, gf);
     sums[34] = 1.0;
+    if constexpr (Q)
+    {
+#pragma unroll
+      for (int q = 0; q < 6; ++q)
+      {
+        hi[q] *= p.to_kelvin;
+        hf[q] = hv[q] * p.to_kelvin;
+      }
+      accumulateHessian(sums + kSums, w, hi, hf);
+    }
   }
   // charge term: the unit-charge Ewald sum (potentialRealEwaldTricubicDerivative with qA = 1) times the probe charge
   if (p.ewald.data && p.charge != 0.0)
   {
     const bool take = active && evK < p.overlap;
-    double ee = 0.0, ge[3] = {0.0, 0.0, 0.0};
+    double ee = 0.0, ge[3] = {0.0, 0.0, 0.0}, he[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     for (int base = 0; base < p.n_ewald; base += kTile)
     {
       const int n = min(kTile, p.n_ewald - base);
@@ -178,27 +224,46 @@ __global__ void __launch_bounds__(kThreads) gridValidateKernel(ValidateParams p)
             ge[0] += f1 * dx;
             ge[1] += f1 * dy;
             ge[2] += f1 * dz;
+            // F2 = C q (e (2 a^2 r^2 + 3) + 3 erfc) / r^5 (potentialRealEwaldTriquinticDerivative)
+            if constexpr (Q)
+              addHessian(he, f1,
+                         cq * (etr * (2.0 * p.alpha * p.alpha * rr + 3.0) + 3.0 * ec) / (rr * rr * rd), dx, dy, dz);
           }
         }
     }
     if (take)
     {
-      double ci[3], cf[3];
-      const double eci = rgd::interpolateGradient(p.ewald, r[0], r[1], r[2], ci) * p.charge * p.to_kelvin;
+      const double sc = p.charge * p.to_kelvin;
+      double ci[3], cf[3], chi[6], chf[6];
+      double eci;
+      if constexpr (Q)
+        eci = rgd::interpolateQuinticHessian(p.ewald, r[0], r[1], r[2], ci, chi) * sc;
+      else
+        eci = rgd::interpolateGradient(p.ewald, r[0], r[1], r[2], ci) * sc;
 #pragma unroll
       for (int a = 0; a < 3; ++a)
       {
-        ci[a] *= p.charge * p.to_kelvin;
-        cf[a] = ge[a] * p.charge * p.to_kelvin;
+        ci[a] *= sc;
+        cf[a] = ge[a] * sc;
       }
-      accumulate(sums + 17, w, eci, ee * p.charge * p.to_kelvin, ci, cf);
+      accumulate(sums + 17, w, eci, ee * sc, ci, cf);
       sums[35] = 1.0;
+      if constexpr (Q)
+      {
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+        {
+          chi[q] *= sc;
+          chf[q] = he[q] * sc;
+        }
+        accumulateHessian(sums + kSums + 24, w, chi, chf);
+      }
     }
   }
   // fixed-order block reduction: warps by shuffles, then one thread per sum over the warps
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int c = 0; c < kSums; ++c)
+  for (int c = 0; c < NS; ++c)
   {
     double x = sums[c];
 #pragma unroll
@@ -206,11 +271,11 @@ __global__ void __launch_bounds__(kThreads) gridValidateKernel(ValidateParams p)
     if (lane == 0) red[warp][c] = x;
   }
   __syncthreads();
-  if (threadIdx.x < kSums)
+  if (threadIdx.x < NS)
   {
     double x = 0.0;
     for (int wi = 0; wi < kThreads / 32; ++wi) x += red[wi][threadIdx.x];
-    p.partial[static_cast<long long>(blockIdx.x) * kSums + threadIdx.x] = x;
+    p.partial[static_cast<long long>(blockIdx.x) * NS + threadIdx.x] = x;
   }
 }
 
@@ -239,23 +304,24 @@ void derive(const double* s, double* e_table, double* e_full, double* e_rel, dou
     g_rel[a] = s[14 + a] > 0.0 ? std::sqrt(s[11 + a] / s[14 + a]) : nan;
   }
 }
-}  // namespace
-
-extern "C" rg_status rg_grid_validate(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* unit_cell,
-                                      const rg_atom* unit_atoms, int n_unit_atoms, const rg_box* simulation_box,
-                                      int probe_type, int nx, int ny, int nz, const double* vdw_grid_device,
-                                      const double* ewald_grid_device, double probe_charge, double weight_beta,
-                                      int64_t n_points, uint64_t seed, const double* points, rg_grid_validation* out)
+// Checks, image staging, the launch and the block-ordered sum of the partials: sumsOf<SCHEME>() values in s
+template <int SCHEME>
+rg_status runValidate(rg_ctx* ctx, const char* name, const rg_forcefield* ff, const rg_box* unit_cell,
+                      const rg_atom* unit_atoms, int n_unit_atoms, const rg_box* simulation_box, int probe_type, int nx,
+                      int ny, int nz, const double* vdw_grid_device, const double* ewald_grid_device,
+                      double probe_charge, double weight_beta, int64_t n_points, uint64_t seed, const double* points,
+                      std::vector<double>& s)
 {
+  constexpr int NS = sumsOf<SCHEME>();
+  s.assign(NS, 0.0);
   if (!ctx) return RG_ERR_INVALID_ARGUMENT;
-  if (!ff || !unit_cell || !simulation_box || !vdw_grid_device || !out || n_unit_atoms < 0 ||
+  if (!ff || !unit_cell || !simulation_box || !vdw_grid_device || n_unit_atoms < 0 ||
       (n_unit_atoms > 0 && !unit_atoms) || n_points < 0)
-    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_validate: null or negative argument");
-  if (nx < 2 || ny < 2 || nz < 2) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_validate: grid shape");
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, std::string(name) + ": null or negative argument");
+  if (nx < 2 || ny < 2 || nz < 2) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, std::string(name) + ": grid shape");
   if (probe_type < 0 || probe_type >= ff->n_types)
-    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_validate: probe_type out of range");
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, std::string(name) + ": probe_type out of range");
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
-  std::memset(out, 0, sizeof(*out));
   if (n_points == 0) return RG_OK;
 
   const rg::HostBox ub = rg::makeHostBox(unit_cell), sb = rg::makeHostBox(simulation_box);
@@ -271,7 +337,7 @@ extern "C" rg_status rg_grid_validate(rg_ctx* ctx, const rg_forcefield* ff, cons
   void *dimg = nullptr, *dpts = nullptr, *dpart = nullptr, *stage = nullptr;
   rg_status st = rg::scratch(ctx, 2, img_bytes, &dimg);
   if (!st && points) st = rg::scratch(ctx, 3, pts_bytes, &dpts);
-  if (!st) st = rg::scratch(ctx, 4, sizeof(double) * kSums * static_cast<size_t>(blocks), &dpart);
+  if (!st) st = rg::scratch(ctx, 4, sizeof(double) * NS * static_cast<size_t>(blocks), &dpart);
   if (st) return st;
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // the pinned staging slot is free
   st = rg::pinnedScratch(ctx, 1, img_bytes + pts_bytes, &stage);
@@ -312,21 +378,83 @@ extern "C" rg_status rg_grid_validate(rg_ctx* ctx, const rg_forcefield* ff, cons
   p.points = static_cast<const double*>(dpts);
   p.seed = seed;
   p.partial = static_cast<double*>(dpart);
-  gridValidateKernel<<<static_cast<unsigned>(blocks), kThreads, 0, ctx->stream>>>(p);
+  gridValidateKernel<SCHEME><<<static_cast<unsigned>(blocks), kThreads, 0, ctx->stream>>>(p);
   RG_CUDA(ctx, cudaGetLastError());
 
-  std::vector<double> part(static_cast<size_t>(blocks) * kSums);
+  std::vector<double> part(static_cast<size_t>(blocks) * NS);
   RG_CUDA(ctx, cudaMemcpyAsync(part.data(), dpart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  double s[kSums] = {};
   for (long long b = 0; b < blocks; ++b)
-    for (int c = 0; c < kSums; ++c) s[c] += part[static_cast<size_t>(b) * kSums + c];
+    for (int c = 0; c < NS; ++c) s[c] += part[static_cast<size_t>(b) * NS + c];
+  return RG_OK;
+}
+
+void fillValidation(const std::vector<double>& s, rg_grid_validation* out)
+{
   for (int c = 0; c < 34; ++c) out->sums[c] = s[c];
   out->n_points = static_cast<int64_t>(s[34]);
   out->n_points_charge = static_cast<int64_t>(s[35]);
-  derive(s, &out->energy_table, &out->energy_full, &out->energy_relative_error, out->gradient_table,
+  derive(s.data(), &out->energy_table, &out->energy_full, &out->energy_relative_error, out->gradient_table,
          out->gradient_full, out->gradient_relative_error);
-  derive(s + 17, &out->charge_energy_table, &out->charge_energy_full, &out->charge_energy_relative_error,
+  derive(s.data() + 17, &out->charge_energy_table, &out->charge_energy_full, &out->charge_energy_relative_error,
          out->charge_gradient_table, out->charge_gradient_full, out->charge_gradient_relative_error);
+}
+
+// Boltzmann averages and relative errors of one term's 24 Hessian sums (system_interpolation_grids.cpp:700-760)
+void deriveHessian(const double* hs, double weight, double* table, double* full, double* rel)
+{
+  const double nan = std::nan("");
+  for (int q = 0; q < 6; ++q)
+  {
+    table[q] = weight > 0.0 ? hs[q] / weight : nan;
+    full[q] = weight > 0.0 ? hs[6 + q] / weight : nan;
+    rel[q] = hs[18 + q] > 0.0 ? std::sqrt(hs[12 + q] / hs[18 + q]) : nan;
+  }
+}
+}  // namespace
+
+extern "C" rg_status rg_grid_validate(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* unit_cell,
+                                      const rg_atom* unit_atoms, int n_unit_atoms, const rg_box* simulation_box,
+                                      int probe_type, int nx, int ny, int nz, const double* vdw_grid_device,
+                                      const double* ewald_grid_device, double probe_charge, double weight_beta,
+                                      int64_t n_points, uint64_t seed, const double* points, rg_grid_validation* out)
+{
+  if (ctx && !out) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_validate: null or negative argument");
+  std::vector<double> s;
+  rg_status st = runValidate<RG_SCHEME_TRICUBIC>(ctx, "rg_grid_validate", ff, unit_cell, unit_atoms, n_unit_atoms,
+                                                 simulation_box, probe_type, nx, ny, nz, vdw_grid_device,
+                                                 ewald_grid_device, probe_charge, weight_beta, n_points, seed, points,
+                                                 s);
+  if (st) return st;
+  std::memset(out, 0, sizeof(*out));
+  if (n_points > 0) fillValidation(s, out);
+  return RG_OK;
+}
+
+extern "C" rg_status rg_grid_validate_triquintic(rg_ctx* ctx, const rg_forcefield* ff, const rg_box* unit_cell,
+                                                 const rg_atom* unit_atoms, int n_unit_atoms,
+                                                 const rg_box* simulation_box, int probe_type, int nx, int ny, int nz,
+                                                 const double* vdw_grid_device, const double* ewald_grid_device,
+                                                 double probe_charge, double weight_beta, int64_t n_points,
+                                                 uint64_t seed, const double* points, rg_grid_validation* out,
+                                                 rg_grid_validation_hessian* hessian)
+{
+  if (ctx && (!out || !hessian))
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_validate_triquintic: null or negative argument");
+  std::vector<double> s;
+  rg_status st = runValidate<RG_SCHEME_TRIQUINTIC>(ctx, "rg_grid_validate_triquintic", ff, unit_cell, unit_atoms,
+                                                   n_unit_atoms, simulation_box, probe_type, nx, ny, nz,
+                                                   vdw_grid_device, ewald_grid_device, probe_charge, weight_beta,
+                                                   n_points, seed, points, s);
+  if (st) return st;
+  std::memset(out, 0, sizeof(*out));
+  std::memset(hessian, 0, sizeof(*hessian));
+  if (n_points == 0) return RG_OK;
+  fillValidation(s, out);
+  for (int c = 0; c < kHessSums; ++c) hessian->sums[c] = s[kSums + c];
+  deriveHessian(s.data() + kSums, s[0], hessian->hessian_table, hessian->hessian_full,
+                hessian->hessian_relative_error);
+  deriveHessian(s.data() + kSums + 24, s[17], hessian->charge_hessian_table, hessian->charge_hessian_full,
+                hessian->charge_hessian_relative_error);
   return RG_OK;
 }

@@ -52,7 +52,6 @@ constexpr int kSlice = 512;                     // molecule sites of a CTA's sli
 constexpr int kFwSlice = 512;                   // framework atoms of a CTA's slice kept in shared memory
 constexpr long long kSpinLimit = 1ll << 22;
 constexpr int kStats = 24;
-constexpr double kPi = 3.141592653589793238462643383279502884;
 constexpr float kFix = 2.3283064365386963e-10f;  // 2^-32
 
 struct Comp
@@ -758,7 +757,6 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
     __syncthreads();
     const int kind = sh.kind;
     int c = sh.c;
-    bool ran = false;
     if ((kind == 0 || kind == 1) && sh.count[c] > 0)
     {
       // translation (one Cartesian direction) or rotation (one Cartesian axis about the centre of mass)
@@ -852,7 +850,6 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
             sh.ks[kk].y += d.y;
           }
       }
-      ran = true;
     }
     else if (kind == 2 && sh.n < p.capacity)
     {
@@ -967,7 +964,6 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
             }
         }
       }
-      ran = true;
     }
     else if (kind == 3 && sh.count[c] > 0)
     {
@@ -1084,7 +1080,6 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
             sh.ks[kk].y += d.y;
           }
       }
-      ran = true;
     }
     else if (kind == 4 && p.n_comp > 1)
     {
@@ -1219,9 +1214,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
         }
         c = oldC;
       }
-      ran = true;
     }
-    (void)ran;
     __syncthreads();
     if (tid == 0 && p.record)
     {

@@ -133,6 +133,16 @@ class GridValidation(ctypes.Structure):
         return out
 
 
+class GridValidationHessian(ctypes.Structure):
+    _fields_ = [("sums", ctypes.c_double * 48), ("hessian_table", ctypes.c_double * 6),
+                ("hessian_full", ctypes.c_double * 6), ("hessian_relative_error", ctypes.c_double * 6),
+                ("charge_hessian_table", ctypes.c_double * 6), ("charge_hessian_full", ctypes.c_double * 6),
+                ("charge_hessian_relative_error", ctypes.c_double * 6)]
+
+    def as_dict(self):
+        return {f: list(getattr(self, f)) for f, _ in self._fields_}
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -165,6 +175,9 @@ def lib():
                                         vp, vp]
         L.rg_grid_validate.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, P(RgBox), i32, i32, i32, i32, vp, vp, d,
                                        d, i64, ctypes.c_uint64, vp, P(GridValidation)]
+        L.rg_grid_validate_triquintic.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, P(RgBox), i32, i32, i32, i32,
+                                                  vp, vp, d, d, i64, ctypes.c_uint64, vp, P(GridValidation),
+                                                  P(GridValidationHessian)]
         L.rg_grid_build_noalloc.argtypes = [i32, vp, i32, P(RgForceField), P(RgBox), vp, i32, i32, d, i32, i32, i32,
                                             i32, vp, P(GridStats)]
         L.rg_system_create.argtypes = [vp, P(RgForceField), P(RgBox), vp, i32, P(vp)]
@@ -383,6 +396,27 @@ class Context:
                                     ctypes.byref(out))
         check(self.handle, st, "rg_grid_validate")
         return out.as_dict()
+
+    def grid_validate_triquintic(self, ff: ForceField, unit_cell, unit_atoms: np.ndarray, simulation_cell,
+                                 probe_type: int, dims, vdw_grid_device: int, ewald_grid_device: int | None = None,
+                                 probe_charge: float = 0.0, weight_beta: float = 1.0 / 300.0, n_points: int = 100000,
+                                 seed: int = 1, points=None):
+        """The triquintic grid test (rg_grid_validate_triquintic): the dict of grid_validate plus a "hessian" dict."""
+        nx, ny, nz = (int(v) for v in dims)
+        atoms = np.ascontiguousarray(unit_atoms, dtype=ATOM_DTYPE)
+        pts = None if points is None else np.ascontiguousarray(points, dtype=np.float64)
+        n = n_points if pts is None else len(pts)
+        out, hess = GridValidation(), GridValidationHessian()
+        ffs, ubox, sbox = ff_struct(ff), box_struct(unit_cell), box_struct(simulation_cell)
+        st = lib().rg_grid_validate_triquintic(
+            self.handle, ctypes.byref(ffs), ctypes.byref(ubox), ctypes.c_void_p(atoms.ctypes.data), len(atoms),
+            ctypes.byref(sbox), probe_type, nx, ny, nz, ctypes.c_void_p(vdw_grid_device),
+            ctypes.c_void_p(ewald_grid_device) if ewald_grid_device else None, probe_charge, weight_beta, n, seed,
+            ctypes.c_void_p(pts.ctypes.data) if pts is not None else None, ctypes.byref(out), ctypes.byref(hess))
+        check(self.handle, st, "rg_grid_validate_triquintic")
+        d = out.as_dict()
+        d["hessian"] = hess.as_dict()
+        return d
 
     def grid_build_set(self, ff: ForceField, cell, unit_atoms: np.ndarray, cutoff: float, dims, precision: int,
                        grid_types, probe_types, out_device_ptrs, count_pairs: bool = False, out_host=None):

@@ -203,3 +203,57 @@ def test_trial_energies_with_triquintic_grids(ctx, oracle):
             assert r.framework_vdw == pytest.approx(e_vdw, rel=1e-10, abs=1e-8)
             assert r.framework_charge == pytest.approx(q * e_q, rel=1e-10, abs=1e-8)
     sysg.close()
+
+
+def _close(a, b, scale):
+    return abs(a - b) <= 1e-9 * max(abs(b), scale, 1e-300)
+
+
+def test_triquintic_grid_test_matches_oracle(ctx, oracle, torch):
+    """rg_grid_validate_triquintic (the reference's grid test with the triquintic scheme, Hessians included) against
+    the oracle at the same 600 points: every Boltzmann-weighted sum of the C_co2 VDW grid and of its charge term
+    (0.70 e x the unit-charge Ewald grid), configuration-2 framework on a 0.5 A mesh, 2x2x3 box. Tolerance 1e-9 of each
+    sum's scale (for a sum of w x, sqrt(sum w x^2 sum w))."""
+    ff = synthetic_forcefield(charges=True)
+    ucell, ufw = synthetic_framework(ff, seed=42)
+    scell, _ = replicate(ucell, ufw, (2, 2, 3))
+    dims = (41, 41, 28)
+    probe = ff.index("C_co2")
+    bufs = []
+    for gt, pr in ((native.GRID_LENNARD_JONES, probe), (native.GRID_EWALD_REAL, 0)):
+        host, _ = ctx.grid_build_triquintic(gt, ff, ucell, ufw, pr, 12.0, dims)
+        bufs.append((host, torch.from_numpy(host).cuda()))
+    pts = np.random.default_rng(7).random((600, 3))
+    beta = 1.0 / 300.0
+    got = ctx.grid_validate_triquintic(ff, ucell, ufw, scell, probe, dims, bufs[0][1].data_ptr(),
+                                       bufs[1][1].data_ptr(), 0.70, beta, points=pts)
+    ref = oracle.grid_validate_triquintic(ff, ucell, ufw, scell, probe, dims, bufs[0][0], bufs[1][0], 0.70, beta, pts)
+    assert got["n_points"] == ref[34] == 600
+    assert got["n_points_charge"] == ref[35] > 30
+    s, hs = got["sums"], got["hessian"]["sums"]
+    for base, hbase in ((0, 0), (17, 24)):
+        o, oh = ref[base:base + 17], ref[36 + hbase:36 + hbase + 24]
+        w = o[0]
+        assert _close(s[base], w, 0.0) and _close(s[base + 4], o[4], 0.0)
+        for i in (1, 2):
+            assert _close(s[base + i], o[i], np.sqrt(o[4] * w)), (base, i, s[base + i], o[i])
+        assert _close(s[base + 3], o[3], o[4])
+        for a in range(3):
+            g2 = o[14 + a]
+            for i in (5 + a, 8 + a):
+                assert _close(s[base + i], o[i], np.sqrt(g2 * w)), (base, i, s[base + i], o[i])
+            assert _close(s[base + 11 + a], o[11 + a], g2)
+            assert _close(s[base + 14 + a], o[14 + a], 0.0)
+        for q in range(6):
+            h2 = oh[18 + q]
+            for i in (q, 6 + q):
+                assert _close(hs[hbase + i], oh[i], np.sqrt(h2 * w)), (base, q, i, hs[hbase + i], oh[i])
+            assert _close(hs[hbase + 12 + q], oh[12 + q], h2), (base, q)
+            assert _close(hs[hbase + 18 + q], oh[18 + q], 0.0), (base, q)
+    h = got["hessian"]
+    assert abs(h["hessian_relative_error"][0] - np.sqrt(ref[36 + 12] / ref[36 + 18])) <= \
+        1e-9 * np.sqrt(ref[36 + 12] / ref[36 + 18])
+    # the triquintic grid's VDW energy error is well below the tricubic grid's on the same mesh
+    c = torch.from_numpy(ctx.grid_build(0, ff, ucell, ufw, probe, 12.0, dims, native.PRECISION_FP64)[0]).cuda()
+    tri = ctx.grid_validate(ff, ucell, ufw, scell, probe, dims, c.data_ptr(), None, 0.0, beta, points=pts)
+    assert got["energy_relative_error"] < tri["energy_relative_error"]

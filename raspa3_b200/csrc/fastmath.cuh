@@ -20,6 +20,14 @@ __device__ __forceinline__ float rsqrtRn(float a)
   const float h = 0.5f * a * r;
   return r * fmaf(-h, r, 1.5f);
 }
+// exp(x) as 2^(x log2 e) from the hardware base-2 exponential (ex2.approx, a few ulp): the Gaussian factor of the FP32
+// Ewald grid terms, whose FP32 rounding of the large cancelling pair terms already dominates the grid error
+__device__ __forceinline__ float expApprox(float x)
+{
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x * 1.4426950408889634f));
+  return r;
+}
 // erfc(x) = exp(-x^2) R(x) for 0 <= x <= 4, with R(x) = exp(x^2) erfc(x) fitted (weighted least squares in Chebyshev
 // form, relative error 4e-8 in FP64, ~2 ulp in FP32) as a degree-9 polynomial in t = 1 / (1 + x/2); the caller passes
 // exp(-x^2), which the derivative factors need anyway.

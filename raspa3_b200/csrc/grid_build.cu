@@ -14,9 +14,9 @@
 // and accumulate energy and the seven derivative channels. Edge semantics kept from the reference: rr = max(0.1, rr),
 // the strict rr < rc^2 test, fractional scaling by the cell and division by the cell counts, and the overlap clamp.
 //
-// Precisions: FP64 throughout; or FP32C — coordinates relative to the brick centre kept as double-float (hi, lo) FP32
-// pairs so that each displacement is rounded to FP32 once, FP32 pair terms, FP32 partial sums per staged chunk folded into a compensated (TwoSum) hi/lo FP32 pair, and an
-// FP64 epilogue.
+// Precisions: FP64 throughout; or FP32C — the point and the staged images relative to the brick centre, computed in
+// FP64 and rounded to FP32 once (|offset| <= rc + R, so a displacement is off by at most ~1e-6 A), FP32 pair terms,
+// FP32 partial sums per staged chunk folded into a compensated (TwoSum) hi/lo FP32 pair, and an FP64 epilogue.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -112,7 +112,7 @@ __device__ __forceinline__ Factor<float> ewaldFactor<float>(float rr, float cq, 
 {
   const float invr = rsqrtRn(rr);
   const float r = rr * invr;
-  const float ex = expf(-alpha * alpha * rr);
+  const float ex = rgd::expApprox(-alpha * alpha * rr);
   const float ec = erfcFromExp(alpha * r, ex);
   const float etr = 2.0f * alpha * r * ex * 0.564189583547756286948079451560772586f;
   const float ar2 = alpha * alpha * rr;
@@ -247,7 +247,6 @@ __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1
   const int chunk = nt * kPer;
   V4* cpos = reinterpret_cast<V4*>(smem_raw);
   V4* cpar = cpos + chunk;                                     // NP * chunk parameter sets
-  float4* clo = reinterpret_cast<float4*>(cpar + NP * chunk);  // FP32C only: low parts of the candidate coordinates
   __shared__ int warp_sums[33];
 
   const int tid = threadIdx.x;
@@ -268,15 +267,10 @@ __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1
   double ctr[3];
 #pragma unroll
   for (int r = 0; r < 3; ++r) ctr[r] = p.cell[0][r] * sc[0] + p.cell[1][r] * sc[1] + p.cell[2][r] * sc[2];
-  // the point relative to the brick centre, in the working precision; in FP32C as a double-float hi + lo pair so that
-  // the point-atom displacement keeps ~FP64 accuracy before its final rounding to FP32
-  const double prx = pos[0] - ctr[0], pry = pos[1] - ctr[1], prz = pos[2] - ctr[2];
-  const Real px = static_cast<Real>(prx);
-  const Real py = static_cast<Real>(pry);
-  const Real pz = static_cast<Real>(prz);
-  const float pxl = static_cast<float>(prx - static_cast<double>(px));
-  const float pyl = static_cast<float>(pry - static_cast<double>(py));
-  const float pzl = static_cast<float>(prz - static_cast<double>(pz));
+  // the point relative to the brick centre, computed in FP64, then in the working precision
+  const Real px = static_cast<Real>(pos[0] - ctr[0]);
+  const Real py = static_cast<Real>(pos[1] - ctr[1]);
+  const Real pz = static_cast<Real>(pos[2] - ctr[2]);
   const Real rc2 = static_cast<Real>(p.rc2);
   const Real alpha = static_cast<Real>(p.alpha);
 
@@ -319,10 +313,6 @@ __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1
         c.z = static_cast<Real>(rz);
         c.w = static_cast<Real>(ip[r].w);
         cpos[off] = c;
-        if constexpr (sizeof(Real) == 4)
-          clo[off] = make_float4(static_cast<float>(rx - static_cast<double>(c.x)),
-                                 static_cast<float>(ry - static_cast<double>(c.y)),
-                                 static_cast<float>(rz - static_cast<double>(c.z)), 0.0f);
         if (!EWALD)
         {
 #pragma unroll
@@ -345,20 +335,7 @@ __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1
     for (int c = 0; c < total; ++c)
     {
       V4 a = cpos[c];
-      Real dx, dy, dz;
-      if constexpr (sizeof(Real) == 4)
-      {
-        const float4 l = clo[c];
-        dx = (px - a.x) + (pxl - l.x);
-        dy = (py - a.y) + (pyl - l.y);
-        dz = (pz - a.z) + (pzl - l.z);
-      }
-      else
-      {
-        dx = px - a.x;
-        dy = py - a.y;
-        dz = pz - a.z;
-      }
+      const Real dx = px - a.x, dy = py - a.y, dz = pz - a.z;
       Real rr = dx * dx + dy * dy + dz * dz;
       rr = rr > Real(0.1) ? rr : Real(0.1);
       if (rr < rc2)
@@ -502,8 +479,7 @@ cudaError_t launchTyped(const GridParams& p, const double4* ipos, const double4*
   const int zbricks = p.zb1 > p.zb0 ? p.zb1 - p.zb0 : (p.nz + bz - 1) / bz;
   dim3 grid((p.nx + bx - 1) / bx, (p.ny + by - 1) / by, zbricks);
   int nt = bx * by * bz;
-  size_t shmem = ((1 + NP) * sizeof(typename Vec4<Real>::T) + (sizeof(Real) == 4 ? sizeof(float4) : 0)) *
-                 static_cast<size_t>(nt) * kPer;
+  size_t shmem = (1 + NP) * sizeof(typename Vec4<Real>::T) * static_cast<size_t>(nt) * kPer;
   if (count)
   {
     auto kern = gridKernel<Real, TYPE, TRI, true, NP>;

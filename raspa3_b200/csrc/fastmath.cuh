@@ -28,12 +28,27 @@ __device__ __forceinline__ float expApprox(float x)
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x * 1.4426950408889634f));
   return r;
 }
+// the hardware reciprocal and reciprocal square root unrefined (a few ulp): the FP32 grid kernels, whose error is
+// dominated by the FP32 rounding of the large cancelling pair terms
+__device__ __forceinline__ float rcpApprox(float a)
+{
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  return r;
+}
+__device__ __forceinline__ float rsqrtApprox(float a)
+{
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  return r;
+}
 // erfc(x) = exp(-x^2) R(x) for 0 <= x <= 4, with R(x) = exp(x^2) erfc(x) fitted (weighted least squares in Chebyshev
 // form, relative error 4e-8 in FP64, ~2 ulp in FP32) as a degree-9 polynomial in t = 1 / (1 + x/2); the caller passes
-// exp(-x^2), which the derivative factors need anyway.
+// exp(-x^2), which the derivative factors need anyway. REFINED = false takes t from the unrefined reciprocal.
+template <bool REFINED = true>
 __device__ __forceinline__ float erfcFromExp(float x, float expmx2)
 {
-  const float t = rcpRn(fmaf(0.5f, x, 1.0f));
+  const float t = REFINED ? rcpRn(fmaf(0.5f, x, 1.0f)) : rcpApprox(fmaf(0.5f, x, 1.0f));
   float r = -0.02496027760207653f;
   r = fmaf(r, t, 0.09420006722211838f);
   r = fmaf(r, t, -0.024484887719154358f);

@@ -28,9 +28,6 @@
 
 namespace
 {
-using rgd::erfcFromExp;
-using rgd::rcpRn;
-using rgd::rsqrtRn;
 constexpr int kPer = 2;  // images tested per thread per chunk
 
 struct GridParams
@@ -50,7 +47,9 @@ struct GridParams
   int zb0, zb1;    // bricks along z launched: [zb0, zb1) (zb1 == 0: all)
 };
 
-__device__ __forceinline__ double rcpRn(double x) { return __drcp_rn(x); }
+// FP32: the hardware approximations unrefined; FP64: correctly rounded
+__device__ __forceinline__ float rcpT(float x) { return rgd::rcpApprox(x); }
+__device__ __forceinline__ double rcpT(double x) { return __drcp_rn(x); }
 __device__ __forceinline__ double sqrtT(double x) { return sqrt(x); }
 __device__ __forceinline__ double erfcT(double x) { return erfc(x); }
 __device__ __forceinline__ double expT(double x) { return exp(x); }
@@ -66,7 +65,7 @@ struct Factor
 template <int TYPE, typename Real>
 __device__ __forceinline__ Factor<Real> ljFactor(Real rr, Real a1, Real s2, Real shift)
 {
-  Real inv = rcpRn(rr);
+  Real inv = rcpT(rr);
   Real q = s2 * inv;
   Real t3 = q * q * q;
   Real t6 = t3 * t3;
@@ -110,10 +109,10 @@ __device__ __forceinline__ Factor<Real> ewaldFactor(Real rr, Real cq, Real alpha
 template <>
 __device__ __forceinline__ Factor<float> ewaldFactor<float>(float rr, float cq, float alpha)
 {
-  const float invr = rsqrtRn(rr);
+  const float invr = rgd::rsqrtApprox(rr);
   const float r = rr * invr;
   const float ex = rgd::expApprox(-alpha * alpha * rr);
-  const float ec = erfcFromExp(alpha * r, ex);
+  const float ec = rgd::erfcFromExp<false>(alpha * r, ex);
   const float etr = 2.0f * alpha * r * ex * 0.564189583547756286948079451560772586f;
   const float ar2 = alpha * alpha * rr;
   const float invrr = invr * invr;
@@ -137,7 +136,7 @@ __device__ __forceinline__ Factor<double> ewaldFactor<double>(double rr, double 
   Real ex = expT(-alpha * alpha * rr);
   Real etr = Real(2) * alpha * r * ex * Real(0.564189583547756286948079451560772586);
   Real ar2 = alpha * alpha * rr;
-  Real invr = rcpRn(r);
+  Real invr = rcpT(r);
   Real invrr = invr * invr;
   Real i3 = invr * invrr;
   Real i5 = i3 * invrr;

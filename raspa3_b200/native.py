@@ -450,8 +450,19 @@ class Context:
 
 
 def _atoms_ptr(a):
-    a = np.ascontiguousarray(a, dtype=ATOM_DTYPE)
-    return a, (ctypes.c_void_p(a.ctypes.data) if len(a) else None)
+    if not (isinstance(a, np.ndarray) and a.dtype == ATOM_DTYPE and a.flags.c_contiguous):
+        a = np.ascontiguousarray(a, dtype=ATOM_DTYPE)
+    return a, (a.ctypes.data if len(a) else None)
+
+
+def _ewald_delta(*args):
+    global _ewald_delta_fn
+    if _ewald_delta_fn is None:
+        _ewald_delta_fn = lib().rg_ewald_delta
+    return _ewald_delta_fn(*args)
+
+
+_ewald_delta_fn = None
 
 
 class Ewald:
@@ -503,9 +514,10 @@ class Ewald:
         if net_charge_derivative_ext is not None:
             nd = np.ascontiguousarray(net_charge_derivative_ext, dtype=np.float64)
         e = EwaldEnergy()
-        check(self.ctx.handle, lib().rg_ewald_delta(self.handle, pn, len(na), po, len(oa), net_charge,
-                                                    None if nd is None else ctypes.c_void_p(nd.ctypes.data),
-                                                    ctypes.byref(e)), "rg_ewald_delta")
+        st = _ewald_delta(self.handle, pn, len(na), po, len(oa), net_charge, None if nd is None else nd.ctypes.data,
+                          ctypes.byref(e))
+        if st:
+            check(self.ctx.handle, st, "rg_ewald_delta")
         return e.as_dict()
 
     def accept(self):

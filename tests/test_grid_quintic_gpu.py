@@ -257,3 +257,23 @@ def test_triquintic_grid_test_matches_oracle(ctx, oracle, torch):
     c = torch.from_numpy(ctx.grid_build(0, ff, ucell, ufw, probe, 12.0, dims, native.PRECISION_FP64)[0]).cuda()
     tri = ctx.grid_validate(ff, ucell, ufw, scell, probe, dims, c.data_ptr(), None, 0.0, beta, points=pts)
     assert got["energy_relative_error"] < tri["energy_relative_error"]
+
+
+def test_triquintic_edge_cases(ctx, oracle, torch):
+    """An empty framework gives an all-zero grid, the smallest grid (2 x 2 x 2 points) matches the oracle, and the
+    triquintic grid test of no points returns zero counts."""
+    ff = synthetic_forcefield(charges=True)
+    cell = np.diag([10.0, 11.0, 12.0])
+    empty = make_atoms(np.zeros((0, 3)), np.zeros(0, dtype=np.uint16), np.zeros(0))
+    for gt in (native.GRID_LENNARD_JONES, native.GRID_EWALD_REAL):
+        out, _ = ctx.grid_build_triquintic(gt, ff, cell, empty, ff.index("CH4"), 12.0, (3, 3, 2))
+        assert out.shape == (27 * 18,) and np.all(out == 0.0)
+    cell2, atoms = triclinic_system(ff, n=12, seed=5)
+    out, _ = ctx.grid_build_triquintic(native.GRID_LENNARD_JONES, ff, cell2, atoms, ff.index("CH4"), 12.0, (2, 2, 2))
+    ref = oracle.make_grid_triquintic(0, ff, cell2, atoms, ff.index("CH4"), 12.0, (2, 2, 2))
+    err, _ = channel_errors(out, ref)
+    assert np.all(err < 1e-9)
+    buf = torch.from_numpy(out).cuda()
+    r = ctx.grid_validate_triquintic(ff, cell2, atoms, cell2, ff.index("CH4"), (2, 2, 2), buf.data_ptr(),
+                                     points=np.zeros((0, 3)))
+    assert r["n_points"] == 0 and r["n_points_charge"] == 0

@@ -613,6 +613,18 @@ def run_triquintic(args, ctx, ff, cell, atoms, dims, world, rank, dist, torch):
     e1.record(stream)
     e1.synchronize()
     secs = max_over_ranks(e0.elapsed_time(e1) / 1e3 / TRIQUINTIC_STEPS, world, dist)
+    # the same grid with FP32 pair terms and compensated sums (RG_TRIQUINTIC_FP32C)
+    for _ in range(2):
+        ctx.grid_build_triquintic(native.GRID_LENNARD_JONES, ff, cell, atoms, probe, 12.0, dims,
+                                  out_device=out.data_ptr(), host=False, fp32c=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(TRIQUINTIC_STEPS):
+        ctx.grid_build_triquintic(native.GRID_LENNARD_JONES, ff, cell, atoms, probe, 12.0, dims,
+                                  out_device=out.data_ptr(), host=False, fp32c=True)
+    e1.record(stream)
+    e1.synchronize()
+    secs32 = max_over_ranks(e0.elapsed_time(e1) / 1e3 / TRIQUINTIC_STEPS, world, dist)
     host = torch.empty(27 * npts, dtype=torch.float64, pin_memory=True).numpy()
     # untimed warm-up of the end-to-end call (first copies into freshly pinned pages)
     ctx.grid_build_triquintic(native.GRID_LENNARD_JONES, ff, cell, atoms, probe, 12.0, dims,
@@ -633,6 +645,8 @@ def run_triquintic(args, ctx, ff, cell, atoms, dims, world, rank, dist, torch):
            "roofline": {"bound": "fp64", "achieved": tflops, "peak": peak64, "unit": "TFLOP/s",
                         "frac": tflops / peak64 if peak64 else None, "flops_per_pair": TRIQUINTIC_FLOPS_PER_PAIR,
                         "peak_source": "rg_probe_fma_peak FP64, measured in this run"},
+           "fp32c": {"value": whole_job_rate(npts, world, secs32), "ms": 1e3 * secs32,
+                     "note": "RG_TRIQUINTIC_FP32C: FP32 pair terms, compensated FP32 sums, FP64 epilogue"},
            "e2e": {"value": whole_job_rate(npts, world, e2e_s), "unit": "grid points/s",
                    "h2d_bytes_per_step": st["h2d_bytes"], "d2h_bytes_per_step": 27 * 8 * npts}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

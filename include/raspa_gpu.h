@@ -183,7 +183,8 @@ enum
 /* rg_grid_build_triquintic flags */
 enum
 {
-  RG_TRIQUINTIC_REFERENCE_RECTANGULAR = 1 /* rectangular cells: keep the reference's two deviations (see below) */
+  RG_TRIQUINTIC_REFERENCE_RECTANGULAR = 1, /* rectangular cells: keep the reference's two deviations (see below) */
+  RG_TRIQUINTIC_FP32C = 2                  /* FP32 pair terms, compensated FP32 sums, FP64 epilogue (default FP64) */
 };
 
 /* Replaces the triquintic branch of InterpolationEnergyGrid::makeFrameworkInterpolationGrid

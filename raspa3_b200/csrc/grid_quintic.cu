@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -42,9 +43,10 @@ constexpr int kPer = 2;                   // images tested per thread per stagin
 constexpr int kChunk = kThreads * kPer;
 constexpr int kSlabs = 8;                 // z-slabs of a build whose host copy overlaps the computation
 
+template <typename Real>
 struct QuinticTable
 {
-  double c[27][27];  // c[channel][u_x + 3 u_y + 9 u_z]
+  Real c[27][27];  // c[channel][u_x + 3 u_y + 9 u_z]
 };
 
 struct QuinticParams
@@ -62,16 +64,17 @@ struct QuinticParams
 
 // F_k = (1/r d/dr)^k of 4 eps ((sigma^2/r^2)^6 - (sigma^2/r^2)^3) - shift, k = 0..6: the reference's factors written
 // as A (c12_k t^2 - c6_k t) / r^(2k) with t = (sigma^2 / r^2)^3
-__device__ __forceinline__ void ljFactors(double rr, double a1, double s2, double shift, double F[7])
+template <typename Real>
+__device__ __forceinline__ void ljFactors(Real rr, Real a1, Real s2, Real shift, Real F[7])
 {
-  const double inv = 1.0 / rr;
-  const double q = s2 * inv;
-  const double t = q * q * q;
-  const double t2 = t * t;
-  constexpr double c12[7] = {1.0, -12.0, 168.0, -2688.0, 48384.0, -967680.0, 21288960.0};
-  constexpr double c6[7] = {1.0, -6.0, 48.0, -480.0, 5760.0, -80640.0, 1290240.0};
+  const Real inv = Real(1) / rr;
+  const Real q = s2 * inv;
+  const Real t = q * q * q;
+  const Real t2 = t * t;
+  constexpr Real c12[7] = {1, -12, 168, -2688, 48384, -967680, 21288960};
+  constexpr Real c6[7] = {1, -6, 48, -480, 5760, -80640, 1290240};
   F[0] = a1 * (t2 - t) - shift;
-  double ip = 1.0;
+  Real ip = 1;
 #pragma unroll
   for (int k = 1; k < 7; ++k)
   {
@@ -82,41 +85,47 @@ __device__ __forceinline__ void ljFactors(double rr, double a1, double s2, doubl
 
 // the reference's closed forms: F_k = (-1)^k Cq (e P_k(a) + (2k-1)!! erfc(alpha r)) / r^(2k+1), a = alpha^2 r^2,
 // e = 2 alpha r exp(-alpha^2 r^2) / sqrt(pi)
-__device__ __forceinline__ void ewaldFactors(double rr, double cq, double alpha, double F[7])
+template <typename Real>
+__device__ __forceinline__ void ewaldFactors(Real rr, Real cq, Real alpha, Real F[7])
 {
-  const double r = sqrt(rr);
-  const double ec = erfc(alpha * r);
-  const double et = 2.0 * alpha * r * exp(-alpha * alpha * rr) * 0.564189583547756286948079451560772586;
-  const double a = alpha * alpha * rr;
-  const double inv = 1.0 / rr;
-  const double ir = 1.0 / r;
-  const double P[7] = {0.0,
-                       1.0,
-                       2.0 * a + 3.0,
-                       (4.0 * a + 10.0) * a + 15.0,
-                       ((8.0 * a + 28.0) * a + 70.0) * a + 105.0,
-                       (((16.0 * a + 72.0) * a + 252.0) * a + 630.0) * a + 945.0,
-                       ((((32.0 * a + 176.0) * a + 792.0) * a + 2772.0) * a + 6930.0) * a + 10395.0};
-  constexpr double dfact[7] = {1.0, 1.0, 3.0, 15.0, 105.0, 945.0, 10395.0};
+  const Real r = sqrt(rr);
+  const Real ec = erfc(alpha * r);
+  const Real et = Real(2) * alpha * r * exp(-alpha * alpha * rr) * Real(0.564189583547756286948079451560772586);
+  const Real a = alpha * alpha * rr;
+  const Real inv = Real(1) / rr;
+  const Real ir = Real(1) / r;
+  const Real P[7] = {0,
+                     1,
+                     Real(2) * a + Real(3),
+                     (Real(4) * a + Real(10)) * a + Real(15),
+                     ((Real(8) * a + Real(28)) * a + Real(70)) * a + Real(105),
+                     (((Real(16) * a + Real(72)) * a + Real(252)) * a + Real(630)) * a + Real(945),
+                     ((((Real(32) * a + Real(176)) * a + Real(792)) * a + Real(2772)) * a + Real(6930)) * a +
+                         Real(10395)};
+  constexpr Real dfact[7] = {1, 1, 3, 15, 105, 945, 10395};
   F[0] = cq * ec * ir;
-  double ip = ir;
+  Real ip = ir;
 #pragma unroll
   for (int k = 1; k < 7; ++k)
   {
     ip *= inv;
-    const double v = cq * (et * P[k] + dfact[k] * ec) * ip;
+    const Real v = cq * (et * P[k] + dfact[k] * ec) * ip;
     F[k] = (k & 1) ? -v : v;
   }
 }
 
-template <int TYPE, bool TRI, bool COUNT>
-__global__ void __launch_bounds__(kThreads) quinticKernel(QuinticParams p, QuinticTable tab,
+// Real = double: FP64 throughout. Real = float (FP32C): offsets from the brick centre rounded to FP32 once, FP32 pair
+// terms, FP32 partial sums per staged chunk folded into TwoSum-compensated hi/lo pairs, FP64 epilogue.
+template <typename Real, int TYPE, bool TRI, bool COUNT>
+__global__ void __launch_bounds__(kThreads) quinticKernel(QuinticParams p, QuinticTable<Real> tab,
                                                           const double4* __restrict__ ipos,
                                                           const double4* __restrict__ ipar)
 {
+  using V4 = std::conditional_t<std::is_same_v<Real, float>, float4, double4>;
+  constexpr bool F32 = std::is_same_v<Real, float>;
   constexpr bool EWALD = TYPE == RG_GRID_EWALD_REAL;
-  __shared__ double4 cpos[kChunk];
-  __shared__ double4 cpar[EWALD ? 1 : kChunk];
+  __shared__ V4 cpos[kChunk];
+  __shared__ V4 cpar[EWALD ? 1 : kChunk];
   __shared__ int warp_sums[33];
   const int tid = threadIdx.x;
   const int lx = tid % kBX, ly = (tid / kBX) % kBY, lz = tid / (kBX * kBY);
@@ -128,18 +137,26 @@ __global__ void __launch_bounds__(kThreads) quinticKernel(QuinticParams p, Quint
   const double s[3] = {i * p.delta[0], j * p.delta[1], k * p.delta[2]};
   const double sc[3] = {(blockIdx.x * kBX + 0.5 * (kBX - 1)) * p.delta[0], (blockIdx.y * kBY + 0.5 * (kBY - 1)) * p.delta[1],
                         (kb * kBZ + 0.5 * (kBZ - 1)) * p.delta[2]};
-  double pr[3], ctr[3];
+  double ctr[3];
+  Real pr[3], cellR[3][3];
 #pragma unroll
   for (int r = 0; r < 3; ++r)
   {
     const double pos = p.cell[0][r] * s[0] + p.cell[1][r] * s[1] + p.cell[2][r] * s[2];
     ctr[r] = p.cell[0][r] * sc[0] + p.cell[1][r] * sc[1] + p.cell[2][r] * sc[2];
-    pr[r] = pos - ctr[r];
-  }
-
-  double acc[27];
+    pr[r] = static_cast<Real>(pos - ctr[r]);
 #pragma unroll
-  for (int l = 0; l < 27; ++l) acc[l] = 0.0;
+    for (int c = 0; c < 3; ++c) cellR[c][r] = static_cast<Real>(p.cell[c][r]);
+  }
+  const Real rc2 = static_cast<Real>(p.rc2);
+  const Real alpha = static_cast<Real>(p.alpha);
+
+  Real acc[27];                             // FP64: the sums; FP32C: the partial sums of the current chunk
+  float hi[F32 ? 27 : 1], lo[F32 ? 27 : 1];  // FP32C: compensated running sums
+#pragma unroll
+  for (int l = 0; l < 27; ++l) acc[l] = 0;
+#pragma unroll
+  for (int l = 0; l < (F32 ? 27 : 1); ++l) hi[l] = lo[l] = 0.0f;
   unsigned long long npairs = 0;
 
   for (int base = 0; base < p.n_images; base += kChunk)
@@ -167,34 +184,48 @@ __global__ void __launch_bounds__(kThreads) quinticKernel(QuinticParams p, Quint
       if (ok[q])
       {
         // image relative to the brick centre, in image order (deterministic sums)
-        cpos[off] = make_double4(ip[q].x - ctr[0], ip[q].y - ctr[1], ip[q].z - ctr[2], ip[q].w);
-        if (!EWALD) cpar[off] = ipar[base + tid * kPer + q];
+        V4 c;
+        c.x = static_cast<Real>(ip[q].x - ctr[0]);
+        c.y = static_cast<Real>(ip[q].y - ctr[1]);
+        c.z = static_cast<Real>(ip[q].z - ctr[2]);
+        c.w = static_cast<Real>(ip[q].w);
+        cpos[off] = c;
+        if (!EWALD)
+        {
+          const double4 pq = ipar[base + tid * kPer + q];
+          V4 pr4;
+          pr4.x = static_cast<Real>(pq.x);
+          pr4.y = static_cast<Real>(pq.y);
+          pr4.z = static_cast<Real>(pq.z);
+          pr4.w = 0;
+          cpar[off] = pr4;
+        }
         ++off;
       }
     __syncthreads();
     for (int c = 0; c < total; ++c)
     {
-      const double4 a = cpos[c];
+      const V4 a = cpos[c];
       // dr = posA - posB (framework_molecule_grid.cpp:575-576)
-      const double d[3] = {pr[0] - a.x, pr[1] - a.y, pr[2] - a.z};
-      const double rr = fmax(0.1, d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-      if (rr >= p.rc2) continue;
+      const Real d[3] = {pr[0] - a.x, pr[1] - a.y, pr[2] - a.z};
+      const Real rr = fmax(Real(0.1), d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      if (rr >= rc2) continue;
       if (COUNT && valid) ++npairs;
-      double F[7];
+      Real F[7];
       if constexpr (EWALD)
-        ewaldFactors(rr, a.w, p.alpha, F);
+        ewaldFactors<Real>(rr, a.w, alpha, F);
       else
       {
-        const double4 pq = cpar[c];
-        ljFactors(rr, pq.x, pq.y, pq.z, F);
+        const V4 pq = cpar[c];
+        ljFactors<Real>(rr, pq.x, pq.y, pq.z, F);
       }
       // x_a = u_a . dr and its powers
-      double xp[3][3];
+      Real xp[3][3];
 #pragma unroll
       for (int ax = 0; ax < 3; ++ax)
       {
-        const double x = TRI ? p.cell[ax][0] * d[0] + p.cell[ax][1] * d[1] + p.cell[ax][2] * d[2] : p.cell[ax][ax] * d[ax];
-        xp[ax][0] = 1.0;
+        const Real x = TRI ? cellR[ax][0] * d[0] + cellR[ax][1] * d[1] + cellR[ax][2] * d[2] : cellR[ax][ax] * d[ax];
+        xp[ax][0] = 1;
         xp[ax][1] = x;
         xp[ax][2] = x * x;
       }
@@ -218,6 +249,19 @@ __global__ void __launch_bounds__(kThreads) quinticKernel(QuinticParams p, Quint
             }
       }
     }
+    if constexpr (F32)
+    {
+      // fold the chunk's partial sums into the compensated sums (Knuth TwoSum; the error term is exact)
+#pragma unroll
+      for (int l = 0; l < 27; ++l)
+      {
+        const float t = __fadd_rn(hi[l], acc[l]);
+        const float z = __fsub_rn(t, hi[l]);
+        lo[l] = __fadd_rn(lo[l], __fadd_rn(__fsub_rn(hi[l], __fsub_rn(t, z)), __fsub_rn(acc[l], z)));
+        hi[l] = t;
+        acc[l] = 0.0f;
+      }
+    }
     __syncthreads();
   }
 
@@ -237,7 +281,9 @@ __global__ void __launch_bounds__(kThreads) quinticKernel(QuinticParams p, Quint
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax)
       for (int q = 0; q < quinticOrder(l, ax); ++q) den *= p.nc[ax];
-    v[l] = l == 0 ? acc[0] : acc[l] / den;
+    const double sum = F32 ? static_cast<double>(hi[F32 ? l : 0]) + static_cast<double>(lo[F32 ? l : 0])
+                           : static_cast<double>(acc[l]);
+    v[l] = l == 0 ? sum : sum / den;
   }
   double* dst = p.out + 27 * (static_cast<long long>(i) + static_cast<long long>(p.nx) * (j + static_cast<long long>(p.ny) * k));
   const double oc = p.overlap;
@@ -277,7 +323,8 @@ double pairings(int r0, int r1, int r2, const double d[3][3])
   return sum;
 }
 
-QuinticTable makeTable(const rg::HostBox& box, bool reference_rectangular)
+template <typename Real>
+QuinticTable<Real> makeTable(const rg::HostBox& box, bool reference_rectangular)
 {
   double d[3][3];
   for (int a = 0; a < 3; ++a)
@@ -285,7 +332,7 @@ QuinticTable makeTable(const rg::HostBox& box, bool reference_rectangular)
       d[a][b] = box.triclinic ? box.c[a][0] * box.c[b][0] + box.c[a][1] * box.c[b][1] + box.c[a][2] * box.c[b][2]
                               : (a == b ? box.c[a][a] * box.c[a][a] : 0.0);
   auto binom = [](int n, int k) { return (k == 0 || k == n) ? 1.0 : static_cast<double>(n); };  // n <= 2
-  QuinticTable t{};
+  QuinticTable<double> t{};
   for (int l = 0; l < 27; ++l)
     for (int u2 = 0; u2 < 3; ++u2)
       for (int u1 = 0; u1 < 3; ++u1)
@@ -302,20 +349,35 @@ QuinticTable makeTable(const rg::HostBox& box, bool reference_rectangular)
     t.c[3][9] *= box.c[0][0] / box.c[2][2];  // (0,0,1) channel, monomial x_z
     t.c[26][0] = 0.0;                        // (2,2,2) channel without its F3 term
   }
-  return t;
+  QuinticTable<Real> out{};
+  for (int l = 0; l < 27; ++l)
+    for (int u = 0; u < 27; ++u) out.c[l][u] = static_cast<Real>(t.c[l][u]);
+  return out;
 }
 
 // bricks [p.zb0, zb1) along z
-template <int TYPE, bool TRI>
-cudaError_t launchQuintic(const QuinticParams& p, int zb1, const QuinticTable& t, const double4* ipos,
+template <typename Real, int TYPE, bool TRI>
+cudaError_t launchQuintic(const QuinticParams& p, int zb1, const QuinticTable<Real>& t, const double4* ipos,
                           const double4* ipar, bool count, cudaStream_t stream)
 {
   dim3 grid((p.nx + kBX - 1) / kBX, (p.ny + kBY - 1) / kBY, zb1 - p.zb0);
   if (count)
-    quinticKernel<TYPE, TRI, true><<<grid, kThreads, 0, stream>>>(p, t, ipos, ipar);
+    quinticKernel<Real, TYPE, TRI, true><<<grid, kThreads, 0, stream>>>(p, t, ipos, ipar);
   else
-    quinticKernel<TYPE, TRI, false><<<grid, kThreads, 0, stream>>>(p, t, ipos, ipar);
+    quinticKernel<Real, TYPE, TRI, false><<<grid, kThreads, 0, stream>>>(p, t, ipos, ipar);
   return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launchQuinticTyped(int grid_type, bool triclinic, const QuinticParams& p, int zb1,
+                               const QuinticTable<Real>& t, const double4* ipos, const double4* ipar, bool count,
+                               cudaStream_t stream)
+{
+  if (grid_type == RG_GRID_EWALD_REAL)
+    return triclinic ? launchQuintic<Real, RG_GRID_EWALD_REAL, true>(p, zb1, t, ipos, ipar, count, stream)
+                     : launchQuintic<Real, RG_GRID_EWALD_REAL, false>(p, zb1, t, ipos, ipar, count, stream);
+  return triclinic ? launchQuintic<Real, RG_GRID_LENNARD_JONES, true>(p, zb1, t, ipos, ipar, count, stream)
+                   : launchQuintic<Real, RG_GRID_LENNARD_JONES, false>(p, zb1, t, ipos, ipar, count, stream);
 }
 
 // One thread per position: value (and gradient) of a tricubic or triquintic grid
@@ -356,7 +418,7 @@ extern "C" rg_status rg_grid_build_triquintic(rg_ctx* ctx, int grid_type, const 
                     "branch evaluates the full Lennard-Jones factor for the repulsion and attraction types)");
   if (grid_type != RG_GRID_LENNARD_JONES && grid_type != RG_GRID_EWALD_REAL)
     return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_triquintic: bad grid_type");
-  if ((flags & ~RG_TRIQUINTIC_REFERENCE_RECTANGULAR) != 0)
+  if ((flags & ~(RG_TRIQUINTIC_REFERENCE_RECTANGULAR | RG_TRIQUINTIC_FP32C)) != 0)
     return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_triquintic: unknown flags");
   if (nx < 2 || ny < 2 || nz < 2)
     return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_triquintic: need >= 2 points per axis");
@@ -429,7 +491,10 @@ extern "C" rg_status rg_grid_build_triquintic(rg_ctx* ctx, int grid_type, const 
   qp.overlap = ff->overlap_criteria;
   qp.pair_count = dcount;
   qp.out = dout;
-  const QuinticTable table = makeTable(box, (flags & RG_TRIQUINTIC_REFERENCE_RECTANGULAR) != 0);
+  const bool refRect = (flags & RG_TRIQUINTIC_REFERENCE_RECTANGULAR) != 0;
+  const bool fp32c = (flags & RG_TRIQUINTIC_FP32C) != 0;
+  const QuinticTable<double> table64 = makeTable<double>(box, refRect);
+  const QuinticTable<float> table32 = makeTable<float>(box, refRect);
   const bool count = stats != nullptr;
   // with a host output the grid is built in z-slabs and each slab's rows (contiguous in the layout) are copied on the
   // context's copy stream while the next slabs are computed
@@ -446,13 +511,9 @@ extern "C" rg_status rg_grid_build_triquintic(rg_ctx* ctx, int grid_type, const 
   {
     qp.zb0 = sl * zb / n_slabs;
     const int zb1 = (sl + 1) * zb / n_slabs;
-    cudaError_t err;
-    if (grid_type == RG_GRID_EWALD_REAL)
-      err = box.triclinic ? launchQuintic<RG_GRID_EWALD_REAL, true>(qp, zb1, table, dpos, dpar, count, ctx->stream)
-                          : launchQuintic<RG_GRID_EWALD_REAL, false>(qp, zb1, table, dpos, dpar, count, ctx->stream);
-    else
-      err = box.triclinic ? launchQuintic<RG_GRID_LENNARD_JONES, true>(qp, zb1, table, dpos, dpar, count, ctx->stream)
-                          : launchQuintic<RG_GRID_LENNARD_JONES, false>(qp, zb1, table, dpos, dpar, count, ctx->stream);
+    const cudaError_t err =
+        fp32c ? launchQuinticTyped<float>(grid_type, box.triclinic, qp, zb1, table32, dpos, dpar, count, ctx->stream)
+              : launchQuinticTyped<double>(grid_type, box.triclinic, qp, zb1, table64, dpos, dpar, count, ctx->stream);
     if (err != cudaSuccess) return rg::cudaFail(ctx, err, "quinticKernel launch");
     if (!out_host) continue;
     cudaEvent_t ev = nullptr;

@@ -28,6 +28,7 @@ PRECISION_FP32C = 1
 SCHEME_TRICUBIC = 8
 SCHEME_TRIQUINTIC = 27
 TRIQUINTIC_REFERENCE_RECTANGULAR = 1
+TRIQUINTIC_FP32C = 2
 
 _lib = None
 
@@ -342,7 +343,8 @@ class Context:
 
     def grid_build_triquintic(self, grid_type: int, ff: ForceField, cell, unit_atoms: np.ndarray, probe_type: int,
                               cutoff: float, dims, reference_rectangular: bool = False, out_device: int | None = None,
-                              host: bool = True, count_pairs: bool = False, out_host: np.ndarray | None = None):
+                              host: bool = True, count_pairs: bool = False, out_host: np.ndarray | None = None,
+                              fp32c: bool = False):
         """Triquintic grid (27 doubles per point, rg_grid_build_triquintic). Returns (host array or None, stats or
         None); out_device: device pointer of 27*nx*ny*nz doubles; out_host: a caller-provided host float64 array
         (e.g. pinned) used instead of a fresh one."""
@@ -351,7 +353,7 @@ class Context:
         ffs, box = ff_struct(ff), box_struct(cell)
         out = (out_host if out_host is not None else np.empty(27 * nx * ny * nz)) if host else None
         stats = GridStats()
-        flags = TRIQUINTIC_REFERENCE_RECTANGULAR if reference_rectangular else 0
+        flags = (TRIQUINTIC_REFERENCE_RECTANGULAR if reference_rectangular else 0) | (TRIQUINTIC_FP32C if fp32c else 0)
         st = lib().rg_grid_build_triquintic(self.handle, grid_type, ctypes.byref(ffs), ctypes.byref(box),
                                             ctypes.c_void_p(atoms.ctypes.data), len(atoms), probe_type, cutoff, nx, ny,
                                             nz, flags, out_device,

@@ -121,23 +121,49 @@ enum class InterpolationGridType : int
   LennardJonesAttraction = RG_GRID_LENNARD_JONES_ATTRACTION
 };
 
-// InterpolationEnergyGrid (src/raspakit/interpolation_energy_grid.ixx), tricubic scheme: 8 doubles per point.
+// ForceField::InterpolationScheme values this layer builds (forcefield/forcefield.ixx:79-84)
+enum class InterpolationScheme : int
+{
+  Tricubic = RG_SCHEME_TRICUBIC,
+  Triquintic = RG_SCHEME_TRIQUINTIC
+};
+
+// InterpolationEnergyGrid (src/raspakit/interpolation_energy_grid.ixx): `order` doubles per point (8 tricubic, 27
+// triquintic) in the reference layout.
 class InterpolationEnergyGrid
 {
  public:
-  InterpolationEnergyGrid(const rg_box& unitCellBox, std::array<int, 3> numberOfGridPoints)
+  InterpolationEnergyGrid(const rg_box& unitCellBox, std::array<int, 3> numberOfGridPoints,
+                          InterpolationScheme order = InterpolationScheme::Tricubic)
       : unitCellBox(unitCellBox),
         numberOfGridPoints(numberOfGridPoints),
-        data(8 * static_cast<size_t>(numberOfGridPoints[0]) * numberOfGridPoints[1] * numberOfGridPoints[2])
+        order(order),
+        data(static_cast<size_t>(order) * static_cast<size_t>(numberOfGridPoints[0]) * numberOfGridPoints[1] *
+             numberOfGridPoints[2])
   {
   }
 
+  // precision: RG_PRECISION_FP64 or RG_PRECISION_FP32C (tricubic); the triquintic build takes
+  // RG_TRIQUINTIC_FP32C for FP32C and keeps the exact derivatives unless referenceRectangular is set
   void makeFrameworkInterpolationGrid(Context& ctx, InterpolationGridType interpolationGridType,
                                       const ForceField& forceField, std::span<const rg_atom> frameworkUnitCellAtoms,
                                       double cutOff, std::size_t pseudo_atom_index,
-                                      int precision = RG_PRECISION_FP64)
+                                      int precision = RG_PRECISION_FP64, bool referenceRectangular = false)
   {
     const rg_forcefield f = forceField.abi();
+    if (order == InterpolationScheme::Triquintic)
+    {
+      const int flags = (referenceRectangular ? RG_TRIQUINTIC_REFERENCE_RECTANGULAR : 0) |
+                        (precision == RG_PRECISION_FP32C ? RG_TRIQUINTIC_FP32C : 0);
+      check(ctx.get(),
+            rg_grid_build_triquintic(ctx.get(), static_cast<int>(interpolationGridType), &f, &unitCellBox,
+                                     frameworkUnitCellAtoms.data(), static_cast<int>(frameworkUnitCellAtoms.size()),
+                                     static_cast<int>(pseudo_atom_index), cutOff, numberOfGridPoints[0],
+                                     numberOfGridPoints[1], numberOfGridPoints[2], flags, nullptr, data.data(),
+                                     nullptr),
+            "makeFrameworkInterpolationGrid");
+      return;
+    }
     check(ctx.get(),
           rg_grid_build(ctx.get(), static_cast<int>(interpolationGridType), &f, &unitCellBox,
                         frameworkUnitCellAtoms.data(), static_cast<int>(frameworkUnitCellAtoms.size()),
@@ -146,8 +172,18 @@ class InterpolationEnergyGrid
           "makeFrameworkInterpolationGrid");
   }
 
+  // InterpolationEnergyGrid::writeOutput (interpolation_energy_grid.cpp:4760-4789): the energy channel as a cube file
+  void writeOutput(const std::string& path, std::array<double, 3> origin = {0.0, 0.0, 0.0}) const
+  {
+    check(nullptr,
+          rg_grid_write_cube(path.c_str(), static_cast<int>(order), data.data(), numberOfGridPoints[0],
+                             numberOfGridPoints[1], numberOfGridPoints[2], &unitCellBox, origin.data()),
+          "writeOutput");
+  }
+
   rg_box unitCellBox;
   std::array<int, 3> numberOfGridPoints;
+  InterpolationScheme order;
   std::vector<double> data;
 };
 

@@ -249,6 +249,26 @@ int main()
                   1e-3 * std::fabs(ex[0].energy.frameworkMoleculeVDW));
   }
 
+  {  // the triquintic scheme through the same class: at the grid points its energy channel is the same pair sum as
+     // the tricubic grid's, and its first-derivative channels equal the tricubic ones
+    ForceField ff = zeoliteForceField(12.0, false);
+    const std::vector<rg_atom> fw = itq29(1);
+    const double a = 11.8671;
+    InterpolationEnergyGrid cubicGrid(cubic(a), {12, 12, 12});
+    InterpolationEnergyGrid quinticGrid(cubic(a), {12, 12, 12}, InterpolationScheme::Triquintic);
+    cubicGrid.makeFrameworkInterpolationGrid(ctx, InterpolationGridType::LennardJones, ff, fw, 12.0, CH4);
+    quinticGrid.makeFrameworkInterpolationGrid(ctx, InterpolationGridType::LennardJones, ff, fw, 12.0, CH4);
+    EXPECT_NEAR(static_cast<double>(quinticGrid.data.size()), 27.0 * 12 * 12 * 12, 0.0);
+    double worst = 0.0;
+    for (std::size_t pt = 0; pt < 12 * 12 * 12; ++pt)
+      for (int l = 0; l < 4; ++l)
+      {
+        const double c = cubicGrid.data[8 * pt + l], q = quinticGrid.data[27 * pt + l];
+        worst = std::fmax(worst, std::fabs(c - q) / std::fmax(1.0, std::fabs(c)));
+      }
+    EXPECT_NEAR(worst, 0.0, 1e-12);
+  }
+
   std::printf("%s (%d failures)\n", failures ? "FAILED" : "PASSED", failures);
   return failures ? 1 : 0;
 }

@@ -579,14 +579,20 @@ typedef struct rg_mixture_result
 rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const rg_gcmc_component* components, int n_components,
                             const rg_mixture_params* params, const double* xyz, const int32_t* comp_of_molecule,
                             int n_molecules, rg_mixture** out);
+/* Frees the mixture's device state (destroy it before its system, Ewald state and context). */
 rg_status rg_mixture_destroy(rg_mixture* mixture);
 /* energy: total energy of the configuration; sk: its structure factors (framework included), 2 doubles per k-vector
  * in the rg_ewald order (NULL: leave them). */
 rg_status rg_mixture_set_state(rg_mixture* mixture, double energy, const double* sk, int64_t n_doubles);
+/* Advances the system by `moves` move attempts (the mix of mc_moves/mc_moves.cpp's component moves); record != 0
+ * accumulates the loading and energy averages. Results, positions and structure factors are read afterwards. */
 rg_status rg_mixture_run(rg_mixture* mixture, int64_t moves, int record);
 rg_status rg_mixture_results(rg_mixture* mixture, rg_mixture_result* out);
+/* The current molecules, made whole (n_atoms * 3 doubles each) with their components, for output or a restart;
+ * capacity_molecules bounds what xyz and comp can hold, *n_molecules receives the count. */
 rg_status rg_mixture_get_positions(rg_mixture* mixture, double* xyz, int32_t* comp, int capacity_molecules,
                                    int* n_molecules);
+/* The current structure factors (framework included), 2 doubles per k-vector in the rg_ewald order: storedEik. */
 rg_status rg_mixture_get_structure_factors(rg_mixture* mixture, double* host, int64_t n_doubles);
 /* Learned first-bead proposal of one component (NULL: uniform). */
 rg_status rg_mixture_set_proposal(rg_mixture* mixture, int component, rg_proposal* proposal, const rg_box* unit_cell);

@@ -28,7 +28,7 @@ int buildGridImages(int grid_type, const rg_forcefield* ff, const HostBox& box, 
 
 namespace
 {
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;
 constexpr int kTile = 128;  // images staged per tile
 constexpr int kSums = 36;   // 17 VDW sums, 17 charge sums, two counts (the layout of rg_grid_validation.sums)
 constexpr int kHessSums = 48;  // triquintic scheme: 24 VDW and 24 charge Hessian sums (rg_grid_validation_hessian.sums)

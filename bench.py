@@ -156,6 +156,78 @@ def cpu_oracle_rate(ff, cell, atoms, dims, grids, target_seconds, threads=0, see
     return pts1 / t1, pts1, t1, threads
 
 
+def run_config1(args, ctx, world, rank, dist, torch):
+    """Configuration 1 (plain method, small, FP64): the methane Lennard-Jones tricubic grid of the uncharged synthetic
+    framework, 133 x 133 x 89 points, FP64 pair terms and sums: grid points/s, the FP64-pipe roofline, end to end
+    through rg_grid_build with a pinned host output, and the FP64 oracle on the host cores."""
+    from raspa3_b200 import native
+    from raspa3_b200.synthetic import config1_grid_dims, synthetic_forcefield, synthetic_framework
+
+    ff = synthetic_forcefield(charges=False)
+    cell, atoms = synthetic_framework(ff, seed=42)
+    dims = config1_grid_dims(cell)
+    npts = dims[0] * dims[1] * dims[2]
+    probe = ff.index("CH4")
+    stream = torch.cuda.current_stream()
+    out = torch.empty(8 * npts, dtype=torch.float64, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    _, st = ctx.grid_build(0, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP64, out_device=out.data_ptr(),
+                           host=False, count_pairs=True)
+    peak64 = ctx.probe_fma_peak(native.PRECISION_FP64)
+    for _ in range(args.warmup):
+        ctx.grid_build(0, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP64, out_device=out.data_ptr(),
+                       host=False)
+    steps = max(1, min(args.steps, 40))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(stream)
+        ctx.grid_build(0, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP64, out_device=out.data_ptr(),
+                       host=False)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    total_s = max_over_ranks(sum(ms) / 1e3, world, dist)
+    value = whole_job_rate(npts * steps, world, total_s)
+    achieved = st["pair_count"] * FLOPS_PER_PAIR["lj"] / (statistics.mean(ms) * 1e-3) / 1e12
+    # end to end: rg_grid_build with a pinned host output (upload of the images and the 100.75 MB download inside)
+    host = torch.empty(8 * npts, dtype=torch.float64, pin_memory=True).numpy()
+    ctx.grid_build(0, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP64, out_host=host)
+    torch.cuda.synchronize()
+    e2e_steps = 5
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.grid_build(0, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP64, out_host=host)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, dist)
+    res = {"workload": "config1: CH4 Lennard-Jones tricubic grid of the uncharged synthetic framework (96 T + 192 O, "
+                       "20.0 x 19.9 x 13.4 A), 133 x 133 x 89 points, rc 12 A, FP64",
+           "value": value, "unit": UNIT, "ms_per_step": 1e3 * total_s / steps, "steps": steps, "dtype": "f64",
+           "pairs": st["pair_count"], "images": st["n_images"],
+           "roofline": {"kernel": "gridKernel<double> (Lennard-Jones)", "bound": "fp64", "achieved": achieved,
+                        "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
+                        "flops_per_pair": FLOPS_PER_PAIR["lj"],
+                        "peak_source": "rg_probe_fma_peak(FP64): FP64 FMA chains on all SMs, measured in this run"},
+           "e2e": {"value": whole_job_rate(npts * e2e_steps, world, e2e_s), "unit": UNIT,
+                   "h2d_bytes_per_step": st["h2d_bytes"], "d2h_bytes_per_step": 8 * 8 * npts,
+                   "path": "rg_grid_build with a pinned host output"},
+           "clocks": clocks, "l2": "256 MiB flush between timed steps"}
+    del flush
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, pts, secs, threads = cpu_oracle_rate(ff, cell, atoms, dims, [("CH4-LJ", 0, probe)],
+                                                   min(args.cpu_seconds, 8.0))
+        res["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"{pts} random grid points in {secs:.1f} s (FP64 oracle of "
+                                         f"makeFrameworkInterpolationGrid, release flags, OpenMP over points)"}
+    return res
+
+
 GCMC_CHAINS_PER_SM = 8
 GCMC_MOVES = 2000
 GCMC_EQUIL = 500
@@ -894,7 +966,8 @@ def run_reference(args):
         return
     import oracle
 
-    oracle.lib()
+    # the reference's release flags (-O3 -ffast-math) and -march=native, compiled here for this host's CPU
+    oracle.use_release_build()
     ff, cell, atoms, dims, grids = workload()
     threads = os.cpu_count() or 1
     # size one step so that W + K steps take a few minutes at most
@@ -923,7 +996,8 @@ def run_reference(args):
                    "parallelism": "cpu"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{n_pts} random grid points x 3 grids per step (FP64 oracle restating "
-                                   f"makeFrameworkInterpolationGrid, OpenMP over points)"},
+                                   f"makeFrameworkInterpolationGrid, release flags -O3 -ffast-math -march=native, "
+                                   f"OpenMP over points)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -944,6 +1018,12 @@ def run_ours(args):
 
     from raspa3_b200 import native
 
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # every CPU baseline below runs the oracle built with the reference's release flags (-O3 -ffast-math) and
+        # -march=native for this host; the strict build stays the parity oracle of the tests
+        import oracle
+
+        oracle.use_release_build()
     ff, cell, atoms, dims, grids = workload()
     npts = dims[0] * dims[1] * dims[2]
     ctx = native.Context(local)
@@ -1034,10 +1114,9 @@ def run_ours(args):
                   for idx in calls]
     dom = int(np.argmax(mean_ms))
     achieved = call_flops[dom] / (mean_ms[dom] * 1e-3) / 1e12
+    # DRAM traffic is not measured in this run: the 100.75 MB a grid kernel writes is still in the 126 MB L2 when
+    # the kernel ends, so the kernel's own DRAM counters miss the write-back (the ncu capture is in profiles/)
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "grid_build_config2_traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(call_names[dom])
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -1056,13 +1135,17 @@ def run_ours(args):
         "roofline": {"kernel": f"gridKernel<float> ({call_names[dom]})", "bound": "fp32", "achieved": achieved,
                      "peak": peak_fp32, "unit": "TFLOP/s", "frac": achieved / peak_fp32, "traffic": traffic,
                      "peak_source": "rg_probe_fma_peak: FP32 FMA chains on all SMs, measured in this run",
-                     "flops_per_pair": FLOPS_PER_PAIR},
+                     "flops_per_pair": FLOPS_PER_PAIR,
+                     "traffic_note": "null: the kernel's output (100.75 MB per grid) is still in L2 when it ends, so "
+                                     "its DRAM counters miss the write-back"},
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps, "step_ms": e2e_step_ms, "path": "rg_grid_build_set with pinned host outputs"},
         "gpu_launches": len(calls) * args.steps,
         "grid_validation": validation,
     }
+    # ---- configuration 1: the methane grid in FP64 (FP64-pipe roofline) ----
+    line["config1_fp64"] = run_config1(args, ctx, world, rank, dist, torch)
     # ---- GCMC steps/s on the same workload: CO2 in the 2x2x3 simulation box, the FP32C grids just built ----
     if not args.no_gcmc:
         line["gcmc"] = run_gcmc(args, ctx, ff, cell, atoms, dims, grids, outs, world, rank, dist, torch)
@@ -1087,7 +1170,7 @@ def run_ours(args):
         rate, pts, secs, threads = cpu_oracle_rate(ff, cell, atoms, dims, grids, args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{pts // len(grids)} random grid points x {len(grids)} grids in {secs:.1f} s "
-                                          f"(FP64 oracle of makeFrameworkInterpolationGrid, OpenMP over points)"}
+                                          f"(FP64 oracle of makeFrameworkInterpolationGrid, release flags, OpenMP over points)"}
     if rank == 0:
         print(json.dumps(line))
     ctx.close()

@@ -31,7 +31,9 @@ enum
   RG_ERR_OUT_OF_MEMORY = 5,
   RG_ERR_NO_DEVICE = 6,
   RG_ERR_IO = 7,         /* a file could not be written or read */
-  RG_ERR_CACHE_MISS = 8  /* rg_grid_load: no file, or one for other inputs, shape or a damaged one */
+  RG_ERR_CACHE_MISS = 8, /* rg_grid_load: no file, or one for other inputs, shape or a damaged one */
+  RG_ERR_NONFINITE = 9   /* an input position, charge, scaling factor or cell entry is NaN or infinite: nothing is
+                            launched (the reference has no such check; its sums would turn NaN) */
 };
 
 /* Byte-for-byte the reference Atom (src/raspakit/atom.ixx:28-39, 64 bytes): a std::span<const Atom> can be passed
@@ -286,7 +288,9 @@ typedef struct rg_trial_energy
   double molecule_charge;
   double dudlambda_vdw[4];
   double dudlambda_charge[4];
-  int32_t overlap; /* 1: the trial overlaps (the reference drops it: std::nullopt) */
+  double external_field_vdw; /* RunningEnergy::externalFieldVDW of CBMC::computeExternalFieldEnergy */
+  int32_t overlap; /* nonzero: the reference drops the trial (std::nullopt): 1 an overlap or a confining external
+                      field's outside, 2 inside a blocked pocket */
   int32_t pad;
 } rg_trial_energy;
 
@@ -301,9 +305,11 @@ rg_status rg_system_set_grid(rg_system* system, int index, const rg_box* unit_ce
                              const double* data, int data_on_device);
 /* Uploads the adsorbate atoms (System::spanOfMoleculeAtoms, the moleculeAtoms of CBMC::GrowContext). */
 rg_status rg_system_set_molecules(rg_system* system, const rg_atom* atoms, int n_atoms);
-/* Arithmetic of rg_cbmc_external_energies for this system: RG_PRECISION_FP64 (the default) or RG_PRECISION_FP32C
- * (FP32 pair terms from the FP64 minimum-image displacement, TwoSum-compensated FP32 sums per thread, FP64 totals;
- * the grid branch stays FP64). */
+/* Arithmetic of the trial energies and differences of this system: RG_PRECISION_FP64 (the default) or
+ * RG_PRECISION_FP32C (Lennard-Jones pair terms in FP32 from the FP64 minimum-image displacement, TwoSum-compensated
+ * FP32 sums per thread, FP64 totals; the real-space Coulomb pairs and the grid branch stay FP64, because charged
+ * framework terms cancel by orders of magnitude and FP32 rounding of them would exceed 1e-6 of a trial's energy).
+ * Both modes meet 1e-6 relative to each trial's energy. */
 rg_status rg_system_set_precision(rg_system* system, int precision);
 
 /* Interpolation scheme of this system's grids (ForceField::interpolationScheme): RG_SCHEME_TRICUBIC (the default,
@@ -313,15 +319,92 @@ rg_status rg_system_set_precision(rg_system* system, int precision);
  * drivers (rg_gcmc, rg_mixture, rg_proposal) take tricubic systems only. */
 rg_status rg_system_set_interpolation_scheme(rg_system* system, int scheme);
 /* Replaces CBMC::computeExternalNonOverlappingEnergies (src/raspakit/cbmc/interactions.cpp:54-179) and its callees
+ * CBMC::insideBlockedPockets (:25-52), CBMC::computeExternalFieldEnergy (cbmc/interactions_external_field.cpp:22-200),
  * CBMC::computeFrameworkMoleculeEnergy (cbmc/interactions_framework_molecule.cpp:31-104) and
  * CBMC::computeInterMolecularEnergy (cbmc/interactions_intermolecular.cpp:22-95); called from the first-bead schemes
  * (cbmc/multiple_first_bead.cpp) and the chain growth (cbmc/flexible_molecules/insertion.cpp:63-64).
  * trials: n_trials consecutive sets of atoms_per_trial atoms (<= 64 per set, <= 4096 in total); skip: index within a
  * set to leave out (-1: none); skip_background_molecule: moleculeId of adsorbate atoms to leave out (-1: none).
- * out[t] gets trial t's energies; overlapping trials are flagged, not removed. */
+ * out[t] gets trial t's energies; trials the reference drops are flagged (overlap != 0), not removed: an overlap, a
+ * blocked pocket (rg_system_set_blocked_pockets) or an atom outside a confining external field
+ * (rg_system_set_external_field). */
 rg_status rg_cbmc_external_energies(rg_system* system, const rg_atom* trials, int n_trials, int atoms_per_trial,
                                     int skip, int64_t skip_background_molecule, double cutoff_framework_vdw,
                                     double cutoff_molecule_vdw, double cutoff_coulomb, rg_trial_energy* out);
+
+/* CBMC::computeDualCutOffCorrection (src/raspakit/cbmc/interactions.cpp:214-251) with
+ * computeExternalNonOverlappingEnergyDualCutOff (:181-212): the trial set's external energy with the force field's
+ * cutoffs minus the same with dual_cutoff for all three, in one launch; out->overlap is nonzero where either is
+ * dropped (the reference's std::nullopt). n_atoms <= 64. */
+rg_status rg_cbmc_dual_cutoff_correction(rg_system* system, const rg_atom* trial_set, int n_atoms,
+                                         int64_t skip_background_molecule, double dual_cutoff, rg_trial_energy* out);
+
+/* ForceField::ChargeMethod (src/raspakit/forcefield/forcefield.ixx:31-39). This library implements the Ewald
+ * real-space pair; the other methods are accepted where no charge term is evaluated (ff->use_charge == 0). */
+enum
+{
+  RG_CHARGE_METHOD_EWALD = 0,
+  RG_CHARGE_METHOD_COULOMB = 1,
+  RG_CHARGE_METHOD_WOLF = 2,
+  RG_CHARGE_METHOD_DAMPED_SHIFTED_FORCE = 3,
+  RG_CHARGE_METHOD_MODIFIED_SHIFTED_FORCE = 4,
+  RG_CHARGE_METHOD_ZERO_DIPOLE = 5
+};
+
+/* Replaces Interactions::computeFrameworkMoleculeEnergyDifference (src/raspakit/interactions/framework_molecule.cpp:
+ * 117-252), called by the translation, rotation and CFCMC moves (mc_moves/component/translation.cpp:30-200,
+ * rotation.cpp:30-190, swap_cfcmc.cpp): E(new atoms) - E(old atoms) against the framework of `system`. An atom takes
+ * the grid branch only if it has a grid, is not fractional and charge_method is RG_CHARGE_METHOD_EWALD
+ * (framework_molecule.cpp:145-146); otherwise the pair loop with the force field's cutoffs. out->overlap = 1 when a
+ * new atom overlaps (the reference returns std::nullopt; old atoms are not tested). n_new, n_old <= 64. Other charge
+ * methods with ff->use_charge set return RG_ERR_UNSUPPORTED. */
+rg_status rg_framework_molecule_energy_difference(rg_system* system, int charge_method, const rg_atom* new_atoms,
+                                                  int n_new, const rg_atom* old_atoms, int n_old, rg_trial_energy* out);
+
+/* Replaces Interactions::computeInterMolecularEnergyDifference (src/raspakit/interactions/intermolecular.cpp:198-290),
+ * called by the same moves: every adsorbate atom stored in `system` (rg_system_set_molecules) of another molecule
+ * (moleculeId differs) against the new atoms minus against the old atoms, force-field cutoffs; zero when
+ * ff->omit_inter is set. out->overlap = 1 when a new atom overlaps. n_new, n_old <= 64. */
+rg_status rg_intermolecular_energy_difference(rg_system* system, const rg_atom* new_atoms, int n_new,
+                                              const rg_atom* old_atoms, int n_old, rg_trial_energy* out);
+
+/* Overwrites n_atoms stored adsorbate atoms from index first_atom on (the moved molecule's span after an accepted
+ * move, as the reference copies the trial positions into System::spanOfMoleculeAtoms). */
+rg_status rg_system_update_molecules(rg_system* system, int first_atom, const rg_atom* atoms, int n_atoms);
+
+/* Component::blockingPockets for CBMC::insideBlockedPockets (src/raspakit/cbmc/interactions.cpp:25-52): 4 doubles per
+ * pocket (centre as fractions of the framework unit cell, radius in Angstrom). A trial set with an atom closer than
+ * radius * sqrt(scalingVDW) to a pocket centre (minimum image in the unit cell) is flagged 2 by
+ * rg_cbmc_external_energies and rg_cbmc_dual_cutoff_correction. n_pockets = 0 clears the list. */
+rg_status rg_system_set_blocked_pockets(rg_system* system, const rg_box* unit_cell, const double* pockets,
+                                        int n_pockets);
+
+/* ForceField::PotentialEnergySurfaceType (src/raspakit/forcefield/forcefield.ixx:50-68), the external field of
+ * CBMC::computeExternalFieldEnergy. RG_SURFACE_OFF: no external field (System::hasExternalField false). */
+enum
+{
+  RG_SURFACE_OFF = -1,
+  RG_SURFACE_NONE = 0,
+  RG_SURFACE_GRID_FILE = 1,
+  RG_SURFACE_THIRD_ORDER_POLYNOMIAL = 3,
+  RG_SURFACE_MULLER_BROWN = 8,
+  RG_SURFACE_CYLINDER_X = 11,
+  RG_SURFACE_CYLINDER_Y = 12,
+  RG_SURFACE_CYLINDER_Z = 13,
+  RG_SURFACE_RECTANGLE_X = 14,
+  RG_SURFACE_RECTANGLE_Y = 15,
+  RG_SURFACE_RECTANGLE_Z = 16
+};
+/* The external field of rg_cbmc_external_energies (cbmc/interactions_external_field.cpp:22-200). With `grid` (the
+ * system's interpolation scheme, nx*ny*nz points over grid_box, the simulation box of
+ * System::createExternalFieldInterpolationGrid; device memory the caller keeps alive if grid_on_device, else copied)
+ * each atom adds scalingVDW times the interpolated value. Without a grid: the Muller-Brown surface, the x y z test
+ * function, or a cylinder (radius geometry[0]) or rectangle (half-widths geometry[0], geometry[1]) along a cell axis
+ * through the box centre whose outside drops the trial; the other surface types (0-16) add nothing, as in the
+ * reference's switch. geometry: ForceField::externalFieldGeometryParameters (4 doubles, may be NULL). */
+rg_status rg_system_set_external_field(rg_system* system, int surface_type, const double* geometry,
+                                       const rg_box* grid_box, int nx, int ny, int nz, const double* grid,
+                                       int grid_on_device);
 
 /* ---- device-resident GCMC of a rigid component (many independent chains) ---- */
 typedef struct rg_gcmc rg_gcmc;
@@ -588,6 +671,12 @@ rg_status rg_mixture_set_state(rg_mixture* mixture, double energy, const double*
  * accumulates the loading and energy averages. Results, positions and structure factors are read afterwards. */
 rg_status rg_mixture_run(rg_mixture* mixture, int64_t moves, int record);
 rg_status rg_mixture_results(rg_mixture* mixture, rg_mixture_result* out);
+/* Test of the bounded grid-barrier wait (no counterpart in the reference, whose moves run on one CPU thread): in the
+ * next launch CTA absent_cta does not arrive at the first barrier, so every CTA's wait gives up after spin_limit polls
+ * (at most the production limit), the launch raises its error flag and leaves, rg_mixture_results reports
+ * RG_ERR_TIMEOUT, and later launches return without doing anything; the mixture must then be destroyed. absent_cta
+ * = -1 arrives normally. Nothing faults or hangs: the wait ends by itself. */
+rg_status rg_mixture_set_wait_test(rg_mixture* mixture, int absent_cta, int64_t spin_limit);
 /* The current molecules, made whole (n_atoms * 3 doubles each) with their components, for output or a restart;
  * capacity_molecules bounds what xyz and comp can hold, *n_molecules receives the count. */
 rg_status rg_mixture_get_positions(rg_mixture* mixture, double* xyz, int32_t* comp, int capacity_molecules,

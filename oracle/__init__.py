@@ -67,6 +67,29 @@ class OEnergy(ctypes.Structure):
         return d
 
 
+def use_release_build(quiet: bool = True) -> str:
+    """Switches this module to the oracle built with the reference's release flags (-O3 -ffast-math, plus
+    -march=native), compiled on this machine: the timed CPU baseline. The strict build stays the parity oracle of the
+    tests; call this only from a process that times the baseline."""
+    global _lib, _LIB_PATH
+    import hashlib
+
+    cpu = ""
+    if os.path.exists("/proc/cpuinfo"):
+        for line in open("/proc/cpuinfo"):
+            if line.startswith(("model name", "flags")):
+                cpu += line
+            if cpu.count("\n") >= 2:
+                break
+    tag = hashlib.sha1(cpu.encode()).hexdigest()[:12]
+    rel = os.path.join("_build", "release_" + tag)
+    subprocess.run(["make", "-C", _HERE, "-j4", "release", f"RELEASE_DIR={rel}"], check=True, capture_output=quiet)
+    _LIB_PATH = os.path.join(_HERE, rel, "liboracle_release.so")
+    _lib = None
+    lib()
+    return _LIB_PATH
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -107,6 +130,16 @@ def lib():
         L.oracle_cbmc_framework_molecule.restype = i32
         L.oracle_cbmc_intermolecular.argtypes = [P(OFF), P(OBox), vp, i32, d, d, vp, i32, i32, i64, P(OEnergy)]
         L.oracle_cbmc_intermolecular.restype = i32
+        L.oracle_framework_molecule_energy_difference.argtypes = [P(OFF), P(OBox), vp, i32, i32, i32, P(OBox), vp, i32,
+                                                                  i32, vp, i32, vp, i32, P(OEnergy)]
+        L.oracle_framework_molecule_energy_difference.restype = i32
+        L.oracle_intermolecular_energy_difference.argtypes = [P(OFF), P(OBox), vp, i32, vp, i32, vp, i32, P(OEnergy)]
+        L.oracle_intermolecular_energy_difference.restype = i32
+        L.oracle_inside_blocked_pockets.argtypes = [P(OBox), vp, i32, vp, i32]
+        L.oracle_inside_blocked_pockets.restype = i32
+        L.oracle_external_field_energy.argtypes = [i32, vp, P(OBox), vp, i32, i32, i32, P(OBox), vp, i32, i32,
+                                                   P(ctypes.c_double)]
+        L.oracle_external_field_energy.restype = i32
         L.oracle_ewald_kvectors.argtypes = [P(OFF), P(OBox), vp, vp, vp]
         L.oracle_ewald_kvectors.restype = i64
         L.oracle_ewald_rigid.argtypes = [P(OFF), P(OBox), vp, i32, vp]
@@ -324,6 +357,61 @@ def cbmc_intermolecular(ff, cell, molecule_atoms, atoms, cutoff_vdw, cutoff_coul
     ok = lib().oracle_cbmc_intermolecular(off(ff), obox(cell), _ptr(ma), len(ma), cutoff_vdw, cutoff_coulomb,
                                           _ptr(at), len(at), skip, skip_background, ctypes.byref(e))
     return bool(ok), e.as_dict()
+
+
+def _grid_table(grids):
+    """(pointer to an array of grid pointers, arrays kept alive) for a list of flat grids or None entries."""
+    if grids is None:
+        return None, None
+    arr = (ctypes.c_void_p * len(grids))()
+    keep = [None if g is None else np.ascontiguousarray(g, dtype=np.float64) for g in grids]
+    for i, g in enumerate(keep):
+        arr[i] = None if g is None else g.ctypes.data
+    return ctypes.cast(arr, ctypes.c_void_p), (arr, keep)
+
+
+def framework_molecule_energy_difference(ff, cell, fw_atoms, new_atoms, old_atoms, grids=None, grid_dims=None,
+                                         grid_cell=None, charge_method_ewald=True):
+    """Interactions::computeFrameworkMoleculeEnergyDifference: (ok, energy dict of E(new) - E(old))."""
+    e = OEnergy()
+    fw, na, oa = (np.ascontiguousarray(x) for x in (fw_atoms, new_atoms, old_atoms))
+    gptr, keep = _grid_table(grids)
+    gnx, gny, gnz = grid_dims if grid_dims is not None else (0, 0, 0)
+    gbox = obox(grid_cell if grid_cell is not None else cell) if grids is not None else None
+    ok = lib().oracle_framework_molecule_energy_difference(off(ff), obox(cell), gptr, gnx, gny, gnz, gbox, _ptr(fw),
+                                                           len(fw), 1 if charge_method_ewald else 0, _ptr(na), len(na),
+                                                           _ptr(oa), len(oa), ctypes.byref(e))
+    del keep
+    return bool(ok), e.as_dict()
+
+
+def intermolecular_energy_difference(ff, cell, molecule_atoms, new_atoms, old_atoms):
+    """Interactions::computeInterMolecularEnergyDifference: (ok, energy dict of E(new) - E(old))."""
+    e = OEnergy()
+    ma, na, oa = (np.ascontiguousarray(x) for x in (molecule_atoms, new_atoms, old_atoms))
+    ok = lib().oracle_intermolecular_energy_difference(off(ff), obox(cell), _ptr(ma), len(ma), _ptr(na), len(na),
+                                                       _ptr(oa), len(oa), ctypes.byref(e))
+    return bool(ok), e.as_dict()
+
+
+def inside_blocked_pockets(unit_cell, pockets, atoms) -> bool:
+    """CBMC::insideBlockedPockets; pockets: (n, 4) fractional centre and radius."""
+    pk = np.ascontiguousarray(pockets, dtype=np.float64).reshape(-1, 4)
+    at = np.ascontiguousarray(atoms)
+    return bool(lib().oracle_inside_blocked_pockets(obox(unit_cell), _ptr(pk), len(pk), _ptr(at), len(at)))
+
+
+def external_field_energy(surface_type, geometry, cell, atoms, grid=None, grid_dims=None, grid_cell=None, skip=-1):
+    """CBMC::computeExternalFieldEnergy: (ok, energy); ok False where a confinement surface returns nullopt."""
+    g = np.asarray(geometry, dtype=np.float64).reshape(4)
+    at = np.ascontiguousarray(atoms)
+    gd = None if grid is None else np.ascontiguousarray(grid, dtype=np.float64)
+    gnx, gny, gnz = grid_dims if grid_dims is not None else (0, 0, 0)
+    e = ctypes.c_double()
+    ok = lib().oracle_external_field_energy(int(surface_type), _ptr(g), obox(cell), _ptr(gd), gnx, gny, gnz,
+                                            obox(grid_cell if grid_cell is not None else cell), _ptr(at), len(at),
+                                            skip, ctypes.byref(e))
+    return bool(ok), e.value
 
 
 def pair_vdw(ff, sa, sb, rr, ta, tb):

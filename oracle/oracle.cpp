@@ -1437,6 +1437,199 @@ int oracle_cbmc_intermolecular(const off* ff, const obox* box, const oatom* mole
   return 1;
 }
 
+int oracle_framework_molecule_energy_difference(const off* ff, const obox* box, const double* const* grids, int gnx,
+                                                int gny, int gnz, const obox* grid_box, const oatom* fw, int n_fw,
+                                                int charge_method_ewald, const oatom* new_atoms, int n_new,
+                                                const oatom* old_atoms, int n_old, oenergy* e)
+{
+  // Interactions::computeFrameworkMoleculeEnergyDifference (interactions/framework_molecule.cpp:117-252): the grid
+  // branch only for non-fractional atoms with a grid under the Ewald charge method; overlap (nullopt, return 0) checked
+  // for the new atoms only; the result is E(new) - E(old).
+  std::memset(e, 0, sizeof(oenergy));
+  Box b = makeBox(box);
+  Box gb = grid_box ? makeBox(grid_box) : b;
+  const bool useCharge = ff->use_charge != 0;
+  const double overlap = ff->overlap_criteria;
+  const double rcv2 = ff->cutoff_framework_vdw * ff->cutoff_framework_vdw;
+  const double rcc2 = ff->cutoff_coulomb * ff->cutoff_coulomb;
+  for (int pass = 0; pass < 2; ++pass)
+  {
+    const oatom* atoms = pass == 0 ? new_atoms : old_atoms;
+    const int n = pass == 0 ? n_new : n_old;
+    const double sign = pass == 0 ? 1.0 : -1.0;
+    for (int index = 0; index < n; ++index)
+    {
+      const oatom& B = atoms[index];
+      double posB[3] = {B.x, B.y, B.z};
+      if (grids && grids[B.type] && !fractionalOf(B) && charge_method_ewald)
+      {
+        double energy = interpolateTricubic(grids[B.type], gnx, gny, gnz, gb, posB);
+        if (pass == 0 && energy > overlap) return 0;
+        e->framework_molecule_vdw += sign * energy;
+        if (useCharge && grids[ff->n_types])
+          e->framework_molecule_charge +=
+              sign * B.charge * interpolateTricubic(grids[ff->n_types], gnx, gny, gnz, gb, posB);
+        continue;
+      }
+      for (int a = 0; a < n_fw; ++a)
+      {
+        const oatom& A = fw[a];
+        double dr[3] = {A.x - B.x, A.y - B.y, A.z - B.z};
+        pbc(b, dr);
+        double rr = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+        if (rr < rcv2)
+        {
+          double f[2];
+          pairVDW(ff, A.scaling_vdw, B.scaling_vdw, rr, A.type, B.type, f);
+          if (pass == 0 && f[0] > overlap) return 0;
+          e->framework_molecule_vdw += sign * f[0];
+          addDud(e->dudlambda_vdw, groupOf(A), groupOf(B), A.scaling_vdw, B.scaling_vdw, sign * f[1]);
+        }
+        if (useCharge && rr < rcc2)
+        {
+          double r = std::sqrt(rr);
+          double f[2];
+          pairCoulomb(ff, A.scaling_coulomb, B.scaling_coulomb, r, A.charge, B.charge, f);
+          e->framework_molecule_charge += sign * f[0];
+          addDud(e->dudlambda_charge, groupOf(A), groupOf(B), A.scaling_coulomb, B.scaling_coulomb, sign * f[1]);
+        }
+      }
+    }
+  }
+  return 1;
+}
+
+int oracle_intermolecular_energy_difference(const off* ff, const obox* box, const oatom* molecule_atoms, int n_mol,
+                                            const oatom* new_atoms, int n_new, const oatom* old_atoms, int n_old,
+                                            oenergy* e)
+{
+  // Interactions::computeInterMolecularEnergyDifference (interactions/intermolecular.cpp:198-290): every stored
+  // adsorbate atom of another molecule against the new atoms (overlap checked) and the old atoms (subtracted).
+  std::memset(e, 0, sizeof(oenergy));
+  if (ff->omit_inter) return 1;
+  Box b = makeBox(box);
+  const bool useCharge = ff->use_charge != 0;
+  const double overlap = ff->overlap_criteria;
+  const double rcv2 = ff->cutoff_molecule_vdw * ff->cutoff_molecule_vdw;
+  const double rcc2 = ff->cutoff_coulomb * ff->cutoff_coulomb;
+  for (int m = 0; m < n_mol; ++m)
+  {
+    const oatom& A = molecule_atoms[m];
+    for (int pass = 0; pass < 2; ++pass)
+    {
+      const oatom* atoms = pass == 0 ? new_atoms : old_atoms;
+      const int n = pass == 0 ? n_new : n_old;
+      const double sign = pass == 0 ? 1.0 : -1.0;
+      for (int index = 0; index < n; ++index)
+      {
+        const oatom& B = atoms[index];
+        if (A.molecule_id == B.molecule_id) continue;
+        double dr[3] = {A.x - B.x, A.y - B.y, A.z - B.z};
+        pbc(b, dr);
+        double rr = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+        if (rr < rcv2)
+        {
+          double f[2];
+          pairVDW(ff, A.scaling_vdw, B.scaling_vdw, rr, A.type, B.type, f);
+          if (pass == 0 && f[0] > overlap) return 0;
+          e->molecule_molecule_vdw += sign * f[0];
+          addDud(e->dudlambda_vdw, groupOf(A), groupOf(B), A.scaling_vdw, B.scaling_vdw, sign * f[1]);
+        }
+        if (useCharge && rr < rcc2)
+        {
+          double r = std::sqrt(rr);
+          double f[2];
+          pairCoulomb(ff, A.scaling_coulomb, B.scaling_coulomb, r, A.charge, B.charge, f);
+          e->molecule_molecule_charge += sign * f[0];
+          addDud(e->dudlambda_charge, groupOf(A), groupOf(B), A.scaling_coulomb, B.scaling_coulomb, sign * f[1]);
+        }
+      }
+    }
+  }
+  return 1;
+}
+
+int oracle_inside_blocked_pockets(const obox* unit_box, const double* pockets, int n_pockets, const oatom* atoms,
+                                  int n_atoms)
+{
+  // CBMC::insideBlockedPockets (cbmc/interactions.cpp:25-52): pocket centres are fractions of the framework's unit
+  // cell, the minimum image is taken in that unit cell, and the radius is scaled by the atom's VDW scaling.
+  Box b = makeBox(unit_box);
+  for (int i = 0; i < n_pockets; ++i)
+  {
+    const double radius_squared = pockets[4 * i + 3] * pockets[4 * i + 3];
+    const double f[3] = {pockets[4 * i], pockets[4 * i + 1], pockets[4 * i + 2]};
+    double pos[3];
+    matvec(b.c, f, pos);
+    for (int a = 0; a < n_atoms; ++a)
+    {
+      double dr[3] = {atoms[a].x - pos[0], atoms[a].y - pos[1], atoms[a].z - pos[2]};
+      pbc(b, dr);
+      if (dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2] < atoms[a].scaling_vdw * radius_squared) return 1;
+    }
+  }
+  return 0;
+}
+
+int oracle_external_field_energy(int surface_type, const double* geometry, const obox* box, const double* grid,
+                                 int gnx, int gny, int gnz, const obox* grid_box, const oatom* atoms, int n_atoms,
+                                 int skip, double* energy)
+{
+  // CBMC::computeExternalFieldEnergy (cbmc/interactions_external_field.cpp:22-200): a grid (scaled by the atom's VDW
+  // scaling) takes precedence; otherwise the analytic surfaces of the switch, the confinements returning nullopt
+  // (here 0) outside; every other surface type adds nothing.
+  *energy = 0.0;
+  Box b = makeBox(box);
+  Box gb = grid_box ? makeBox(grid_box) : b;
+  for (int index = 0; index < n_atoms; ++index)
+  {
+    if (index == skip) continue;
+    const oatom& A = atoms[index];
+    const double pos[3] = {A.x, A.y, A.z};
+    double e = 0.0;
+    if (grid)
+      e = A.scaling_vdw * interpolateTricubic(grid, gnx, gny, gnz, gb, pos);
+    else if (surface_type == 8)  // MullerBrown
+    {
+      const double Ak[4] = {-200.0, -100.0, -170.0, -15.0}, ak[4] = {-1.0, -1.0, -6.5, -0.7},
+                   x0[4] = {1.0, 0.0, -0.5, -1.0}, bk[4] = {0.0, 0.0, 11.0, 0.6}, y0[4] = {0.0, 0.5, 1.5, 1.0},
+                   ck[4] = {-10.0, -10.0, -6.5, 0.7};
+      for (int i = 0; i < 4; ++i)
+        e += Ak[i] * std::exp(ak[i] * (pos[0] - x0[i]) * (pos[0] - x0[i]) +
+                              bk[i] * (pos[0] - x0[i]) * (pos[1] - y0[i]) + ck[i] * (pos[1] - y0[i]) * (pos[1] - y0[i]));
+    }
+    else if (surface_type == 3)  // ThirdOrderPolynomialTestFunction
+      e = pos[0] * pos[1] * pos[2];
+    else if (surface_type >= 11 && surface_type <= 16)  // CylinderX/Y/Z, RectangleX/Y/Z
+    {
+      const int axis = (surface_type - 11) % 3;
+      double fb[3] = {0.5, 0.5, 0.5}, fe[3] = {0.5, 0.5, 0.5};
+      fb[axis] = 0.0;
+      fe[axis] = 1.0;
+      double cb[3], ce[3];
+      matvec(b.c, fb, cb);
+      matvec(b.c, fe, ce);
+      double v[3] = {ce[0] - cb[0], ce[1] - cb[1], ce[2] - cb[2]};
+      const double len = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      for (double& x : v) x /= len;
+      const double d[3] = {pos[0] - cb[0], pos[1] - cb[1], pos[2] - cb[2]};
+      const double w[3] = {d[1] * v[2] - d[2] * v[1], d[2] * v[0] - d[0] * v[2], d[0] * v[1] - d[1] * v[0]};
+      bool inside;
+      if (surface_type <= 13)
+        inside = w[0] * w[0] + w[1] * w[1] + w[2] * w[2] < geometry[0] * geometry[0];
+      else if (surface_type == 14)
+        inside = std::fabs(w[1]) < geometry[0] && std::fabs(w[2]) < geometry[1];
+      else if (surface_type == 15)
+        inside = std::fabs(w[2]) < geometry[0] && std::fabs(w[0]) < geometry[1];
+      else
+        inside = std::fabs(w[1]) < geometry[0] && std::fabs(w[0]) < geometry[1];
+      if (!inside) return 0;
+    }
+    *energy += e;
+  }
+  return 1;
+}
+
 int64_t oracle_ewald_kvectors(const off* ff, const obox* box, int32_t* kvec, double* temp, double* single_ion_sum)
 {
   Box b = makeBox(box);

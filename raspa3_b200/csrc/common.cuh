@@ -55,6 +55,11 @@ rg_status event(rg_ctx* ctx, int i, cudaEvent_t* out);
 // Makes the context stream wait for everything queued on the copy stream so far.
 rg_status joinCopies(rg_ctx* ctx);
 
+// RG_ERR_NONFINITE (with a message naming `what`) if any position, charge or scaling factor of the atoms is NaN or
+// infinite, RG_OK otherwise. Host inputs are checked before anything is launched.
+rg_status checkFinite(rg_ctx* ctx, const rg_atom* atoms, long long n, const char* what);
+rg_status checkFiniteBox(rg_ctx* ctx, const rg_box* box, const char* what);
+
 struct HostBox
 {
   double c[3][3];   // c[col][row]
@@ -64,6 +69,11 @@ struct HostBox
 };
 HostBox makeHostBox(const rg_box* b);
 void perpendicularWidths(const HostBox& b, double w[3]);
+// The supercell that `cutoff` sizes in the reference's grid builds (ceil(2 cutoff / width) unit cells per axis,
+// SimulationBox::smallestNumberOfUnitCellsForMinimumImagesConvention, simulationbox.cpp:150-156): half its lengths
+// (h, rectangular) and its inverse as ic[d][k] (fraction d from Cartesian k). Returns whether its minimum image can
+// drop pairs within the pair cutoff `rc`, i.e. whether it is narrower than 2 rc along some axis.
+bool supercellClip(const HostBox& b, double rc, double cutoff, double h[3], double ic[3][3]);
 inline void matvec(const double m[3][3], const double v[3], double out[3])
 {
   for (int r = 0; r < 3; ++r) out[r] = m[0][r] * v[0] + m[1][r] * v[1] + m[2][r] * v[2];

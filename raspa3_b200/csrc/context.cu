@@ -12,6 +12,41 @@ rg_status fail(rg_ctx* ctx, rg_status code, const std::string& msg)
   return code;
 }
 
+rg_status checkFinite(rg_ctx* ctx, const rg_atom* atoms, long long n, const char* what)
+{
+  for (long long i = 0; i < n; ++i)
+  {
+    const rg_atom& a = atoms[i];
+    if (!(std::isfinite(a.x) && std::isfinite(a.y) && std::isfinite(a.z) && std::isfinite(a.charge) &&
+          std::isfinite(a.scaling_vdw) && std::isfinite(a.scaling_coulomb)))
+      return fail(ctx, RG_ERR_NONFINITE,
+                  std::string(what) + ": atom " + std::to_string(i) + " has a NaN or infinite position, charge or scaling");
+  }
+  return RG_OK;
+}
+
+rg_status checkFiniteBox(rg_ctx* ctx, const rg_box* box, const char* what)
+{
+  for (int i = 0; i < 9; ++i)
+    if (!std::isfinite(box->cell[i])) return fail(ctx, RG_ERR_NONFINITE, std::string(what) + ": NaN or infinite cell");
+  return RG_OK;
+}
+
+bool supercellClip(const HostBox& b, double rc, double cutoff, double h[3], double ic[3][3])
+{
+  double w[3];
+  perpendicularWidths(b, w);
+  bool clip = false;
+  for (int d = 0; d < 3; ++d)
+  {
+    const double n = std::ceil(2.0 * cutoff / w[d]);
+    if (n * w[d] < 2.0 * rc) clip = true;
+    h[d] = 0.5 * n * b.c[d][d];
+    for (int e = 0; e < 3; ++e) ic[d][e] = b.ic[e][d] / n;
+  }
+  return clip;
+}
+
 rg_status cudaFail(rg_ctx* ctx, cudaError_t err, const char* what)
 {
   std::string msg = std::string("CUDA error in ") + what + ": " + cudaGetErrorName(err) + " (" +

@@ -433,6 +433,27 @@ rg_status proposalExport(rg_proposal* p, const double** cdf, const double** dens
 rg_status ewaldExport(rg_ewald* e, const char4** kvec, const double** temp, const double2** s_rigid, int64_t* nk,
                       int kmax[3], double* alpha, double* single_ion_sum);
 
+// The supercell's minimum image keeps a displacement iff it lies in (-1/2, 1/2] of the supercell along every axis
+// (SimulationBox::applyPeriodicBoundaryConditions, simulationbox.ixx:131-161, in the supercell of
+// makeFrameworkInterpolationGrid, interpolation_energy_grid.cpp:3812-3815).
+template <bool TRICLINIC, typename R>
+__device__ __forceinline__ bool insideSupercell(const R (&h)[3], const R (&ic)[9], R dx, R dy, R dz)
+{
+  if constexpr (!TRICLINIC)
+    return dx > -h[0] && dx <= h[0] && dy > -h[1] && dy <= h[1] && dz > -h[2] && dz <= h[2];
+  else
+  {
+    bool in = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+      const R sd = ic[3 * d] * dx + ic[3 * d + 1] * dy + ic[3 * d + 2] * dz;
+      in = in && sd > R(-0.5) && sd <= R(0.5);
+    }
+    return in;
+  }
+}
+
 __device__ __forceinline__ int groupOf(const rg_atom& a) { return a.group_fractional & 0x0f; }
 __device__ __forceinline__ bool fractionalOf(const rg_atom& a) { return (a.group_fractional >> 4) != 0; }
 }  // namespace rgd

@@ -753,6 +753,8 @@ rg_status rg_ewald_delta(rg_ewald* e, const rg_atom* new_atoms, int n_new, const
     return RG_ERR_INVALID_ARGUMENT;
   rg_ctx* ctx = e->ctx;
   std::memset(out, 0, sizeof(rg_ewald_energy));
+  if (rg_status fs = rg::checkFinite(ctx, new_atoms, n_new, "rg_ewald_delta")) return fs;
+  if (rg_status fs = rg::checkFinite(ctx, old_atoms, n_old, "rg_ewald_delta")) return fs;
   if (!e->use_charge) return RG_OK;
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
   const int G = e->n_groups;

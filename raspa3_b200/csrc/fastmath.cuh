@@ -61,4 +61,28 @@ __device__ __forceinline__ float erfcFromExp(float x, float expmx2)
   r = fmaf(r, t, -0.00021772264153696597f);
   return expmx2 * r;
 }
+// erf(x)/x as a polynomial in u = x^2 for 0 <= x <= 2 (FP64): a Chebyshev least-squares fit of erf(sqrt(u))/sqrt(u) on
+// u in [0, 4] against a 40-digit reference, in monomial form, relative error 2e-15. erf(x)/x is entire, so the
+// complement erfc(x)/x = 1/x - erf(x)/x needs no exponential and no branch (relative error 4e-13 for x <= 2).
+constexpr double kErfOverXMax = 2.0;
+__device__ __forceinline__ double erfOverX(double u)
+{
+  double r = 1.805761181299233e-16;
+  r = fma(r, u, -1.0300117447682573e-14);
+  r = fma(r, u, 2.927836726213971e-13);
+  r = fma(r, u, -5.731081299066304e-12);
+  r = fma(r, u, 8.96014012256378e-11);
+  r = fma(r, u, -1.2127292658512346e-09);
+  r = fma(r, u, 1.4763819202890526e-08);
+  r = fma(r, u, -1.635716222383698e-07);
+  r = fma(r, u, 1.6460811429838825e-06);
+  r = fma(r, u, -1.4925505494318574e-05);
+  r = fma(r, u, 0.00012055321281183126);
+  r = fma(r, u, -0.000854832635719831);
+  r = fma(r, u, 0.005223977599866574);
+  r = fma(r, u, -0.026866170638949895);
+  r = fma(r, u, 0.11283791670871149);
+  r = fma(r, u, -0.37612638903178647);
+  return fma(r, u, 1.1283791670955123);
+}
 }  // namespace rgd

@@ -17,6 +17,14 @@
 // Precisions: FP64 throughout; or FP32C — the point and the staged images relative to the brick centre, computed in
 // FP64 and rounded to FP32 once (|offset| <= rc + R, so a displacement is off by at most ~1e-6 A), FP32 pair terms,
 // FP32 partial sums per staged chunk folded into a compensated (TwoSum) hi/lo FP32 pair, and an FP64 epilogue.
+// The FP32C unit-charge Ewald grid stages the images within kNearRadius + R of the brick centre in a second list and
+// evaluates them in FP64: their terms (up to ~5e5 K for +2.05 e at 2.5 A) cancel to totals of a few 1e3 K, and FP32
+// rounding of those few terms is what limits the energy channel otherwise.
+//
+// Supercell. The reference sizes its supercell with the `cutoff` argument (cutOffCoulomb for the Ewald grid,
+// system_interpolation_grids.cpp:211) and tests pairs against cutOffFrameworkVDW. When that supercell is narrower
+// than 2 cutOffFrameworkVDW, its minimum image drops images that lie within the pair cutoff; the CLIP kernels then
+// keep a pair only if its displacement lies inside the half-open supercell box, (-1/2, 1/2] in supercell fractions.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -24,6 +32,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "energy.cuh"
 #include "fastmath.cuh"
 
 namespace
@@ -45,7 +54,16 @@ struct GridParams
   unsigned long long* pair_count;
   double* out[2];  // one output grid per Lennard-Jones probe sharing the candidate set (out[0] otherwise)
   int zb0, zb1;    // bricks along z launched: [zb0, zb1) (zb1 == 0: all)
+  double near2;    // FP32C Ewald grid: images within sqrt(near2) of the brick centre are evaluated in FP64
+  double clip_h[3];      // CLIP, rectangular: half the supercell lengths
+  double clip_ic[3][3];  // CLIP, triclinic: supercell fractions s[d] = sum_k clip_ic[d][k] dr[k]
 };
+
+// Radius around a brick within which the FP32C Ewald grid evaluates its pair terms in FP64 (Angstrom).
+#ifndef RG_GRID_NEAR_RADIUS
+#define RG_GRID_NEAR_RADIUS 5.0
+#endif
+constexpr double kNearRadius = RG_GRID_NEAR_RADIUS;
 
 // FP32: the hardware approximations unrefined; FP64: correctly rounded
 __device__ __forceinline__ float rcpT(float x) { return rgd::rcpApprox(x); }
@@ -188,6 +206,17 @@ struct AccF32C
       p[i] = 0.0f;
     }
   }
+  // adds an FP64 value: its FP32 head by TwoSum into hi, its FP32 tail and the TwoSum error into lo
+  __device__ __forceinline__ void fold(int i, double v)
+  {
+    const float vh = __double2float_rn(v);
+    const float vl = __double2float_rn(v - static_cast<double>(vh));
+    float s = __fadd_rn(hi[i], vh);
+    float bp = __fsub_rn(s, hi[i]);
+    float err = __fadd_rn(__fsub_rn(hi[i], __fsub_rn(s, bp)), __fsub_rn(vh, bp));
+    hi[i] = s;
+    lo[i] = __fadd_rn(lo[i], __fadd_rn(err, vl));
+  }
   __device__ __forceinline__ double get(int i) const { return static_cast<double>(hi[i]) + static_cast<double>(lo[i]); }
 };
 
@@ -232,20 +261,60 @@ __device__ __forceinline__ int sym2(int i, int j)
   return table[a * 3 + b];
 }
 
+// Adds one pair's factors to the channels: rectangular cells need E, the gradient, the three mixed second derivatives
+// and the mixed third derivative; triclinic cells the full Cartesian tensors (framework_molecule_grid.cpp:76-144) in
+// symmetric storage, contracted with the cell in the epilogue.
+template <bool TRICLINIC, typename Acc, typename R>
+__device__ __forceinline__ void addPair(Acc& acc, const Factor<R>& f, R dx, R dy, R dz)
+{
+  acc.add(0, f.e);
+  if constexpr (!TRICLINIC)
+  {
+    acc.add(1, dx * f.f1);
+    acc.add(2, dy * f.f1);
+    acc.add(3, dz * f.f1);
+    acc.add(4, f.f2 * dx * dy);
+    acc.add(5, f.f2 * dx * dz);
+    acc.add(6, f.f2 * dy * dz);
+    acc.add(7, f.f3 * dx * dy * dz);
+  }
+  else
+  {
+    const R d[3] = {dx, dy, dz};
+    acc.add(1, dx * f.f1);
+    acc.add(2, dy * f.f1);
+    acc.add(3, dz * f.f1);
+#pragma unroll
+    for (int u = 0; u < 3; ++u)
+#pragma unroll
+      for (int v = u; v < 3; ++v) acc.add(4 + sym2(u, v), f.f2 * d[u] * d[v] + (u == v ? f.f1 : R(0)));
+#pragma unroll
+    for (int u = 0; u < 3; ++u)
+#pragma unroll
+      for (int v = u; v < 3; ++v)
+#pragma unroll
+        for (int w = v; w < 3; ++w)
+          acc.add(10 + sym3(u, v, w), f.f3 * d[u] * d[v] * d[w] + (v == w ? f.f2 * d[u] : R(0)) +
+                                          (u == w ? f.f2 * d[v] : R(0)) + (u == v ? f.f2 * d[w] : R(0)));
+  }
+}
+
 // NP Lennard-Jones probes (1 or 2) share one candidate set: the distances, the reciprocal and the staging are computed
 // once per pair and each probe adds its own factors (ipar holds NP parameter sets per image).
-template <typename Real, int TYPE, bool TRICLINIC, bool COUNT, int NP>
+template <typename Real, int TYPE, bool TRICLINIC, bool COUNT, int NP, bool CLIP>
 __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1) gridKernel(GridParams p, const double4* __restrict__ ipos,
                                                   const double4* __restrict__ ipar, int bx, int by, int bz)
 {
   using V4 = typename Vec4<Real>::T;
   constexpr bool EWALD = (TYPE == RG_GRID_EWALD_REAL);
+  constexpr bool NEAR64 = EWALD && sizeof(Real) == 4;  // FP32C Ewald: FP64 list of the images near the brick
   constexpr int NCH = TRICLINIC ? 20 : 8;
   extern __shared__ unsigned char smem_raw[];
   const int nt = blockDim.x;
   const int chunk = nt * kPer;
   V4* cpos = reinterpret_cast<V4*>(smem_raw);
-  V4* cpar = cpos + chunk;                                     // NP * chunk parameter sets
+  V4* cpar = cpos + chunk;                                     // NP * chunk parameter sets (Lennard-Jones)
+  double4* npos = reinterpret_cast<double4*>(cpos + chunk);   // near list (FP32C Ewald)
   __shared__ int warp_sums[33];
 
   const int tid = threadIdx.x;
@@ -272,6 +341,23 @@ __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1
   const Real pz = static_cast<Real>(pos[2] - ctr[2]);
   const Real rc2 = static_cast<Real>(p.rc2);
   const Real alpha = static_cast<Real>(p.alpha);
+  Real ch[3], cic[9];
+  double chd[3], cicd[9];
+  if constexpr (CLIP)
+  {
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+      chd[d] = p.clip_h[d];
+      ch[d] = static_cast<Real>(chd[d]);
+#pragma unroll
+      for (int e = 0; e < 3; ++e)
+      {
+        cicd[3 * d + e] = p.clip_ic[d][e];
+        cic[3 * d + e] = static_cast<Real>(cicd[3 * d + e]);
+      }
+    }
+  }
 
   typename AccOf<Real, NCH>::T accs[NP];
 #pragma unroll
@@ -280,33 +366,42 @@ __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1
 
   for (int base = 0; base < p.n_images; base += chunk)
   {
-    // stage: each thread tests kPer consecutive images; a block scan keeps image order (deterministic sums)
+    // stage: each thread tests kPer consecutive images; a block scan keeps image order (deterministic sums). The far
+    // and near counts travel packed in one scan (each block total is at most `chunk` < 2^16).
     double4 ip[kPer];
-    bool ok[kPer];
+    bool ok[kPer], nr[kPer];
     int cnt = 0;
 #pragma unroll
     for (int r = 0; r < kPer; ++r)
     {
       int idx = base + tid * kPer + r;
-      ok[r] = false;
+      ok[r] = nr[r] = false;
       if (idx < p.n_images)
       {
         ip[r] = ipos[idx];
         double dx = ip[r].x - ctr[0], dy = ip[r].y - ctr[1], dz = ip[r].z - ctr[2];
-        ok[r] = (dx * dx + dy * dy + dz * dz) < p.filter2;
-        cnt += ok[r] ? 1 : 0;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        const bool in = d2 < p.filter2;
+        nr[r] = NEAR64 && in && d2 < p.near2;
+        ok[r] = in && !nr[r];
+        cnt += ok[r] ? 1 : (nr[r] ? (1 << 16) : 0);
       }
     }
     int total;
     int off = blockExclusiveScan(cnt, warp_sums, &total);
+    int offn = off >> 16;
+    off &= 0xffff;
+    const int total_near = total >> 16;
+    total &= 0xffff;
 #pragma unroll
     for (int r = 0; r < kPer; ++r)
     {
+      const double rx = ip[r].x - ctr[0], ry = ip[r].y - ctr[1], rz = ip[r].z - ctr[2];
+      if (NEAR64 && nr[r]) npos[offn++] = make_double4(rx, ry, rz, ip[r].w);
       if (ok[r])
       {
         int idx = base + tid * kPer + r;
         V4 c;
-        const double rx = ip[r].x - ctr[0], ry = ip[r].y - ctr[1], rz = ip[r].z - ctr[2];
         c.x = static_cast<Real>(rx);
         c.y = static_cast<Real>(ry);
         c.z = static_cast<Real>(rz);
@@ -337,7 +432,9 @@ __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1
       const Real dx = px - a.x, dy = py - a.y, dz = pz - a.z;
       Real rr = dx * dx + dy * dy + dz * dz;
       rr = rr > Real(0.1) ? rr : Real(0.1);
-      if (rr < rc2)
+      bool in = rr < rc2;
+      if constexpr (CLIP) in = in && rgd::insideSupercell<TRICLINIC>(ch, cic, dx, dy, dz);
+      if (in)
       {
         if (COUNT && valid) ++npairs;
 #pragma unroll
@@ -351,43 +448,64 @@ __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1
             V4 pq = cpar[q * chunk + c];
             f = ljFactor<TYPE, Real>(rr, pq.x, pq.y, pq.z);
           }
-          auto& acc = accs[q];
-          acc.add(0, f.e);
-          if constexpr (!TRICLINIC)
-          {
-            acc.add(1, dx * f.f1);
-            acc.add(2, dy * f.f1);
-            acc.add(3, dz * f.f1);
-            acc.add(4, f.f2 * dx * dy);
-            acc.add(5, f.f2 * dx * dz);
-            acc.add(6, f.f2 * dy * dz);
-            acc.add(7, f.f3 * dx * dy * dz);
-          }
-          else
-          {
-            // full Cartesian tensors (framework_molecule_grid.cpp:76-144), symmetric storage
-            const Real d[3] = {dx, dy, dz};
-            acc.add(1, dx * f.f1);
-            acc.add(2, dy * f.f1);
-            acc.add(3, dz * f.f1);
-#pragma unroll
-            for (int u = 0; u < 3; ++u)
-#pragma unroll
-              for (int v = u; v < 3; ++v) acc.add(4 + sym2(u, v), f.f2 * d[u] * d[v] + (u == v ? f.f1 : Real(0)));
-#pragma unroll
-            for (int u = 0; u < 3; ++u)
-#pragma unroll
-              for (int v = u; v < 3; ++v)
-#pragma unroll
-                for (int w = v; w < 3; ++w)
-                  acc.add(10 + sym3(u, v, w), f.f3 * d[u] * d[v] * d[w] + (v == w ? f.f2 * d[u] : Real(0)) +
-                                                  (u == w ? f.f2 * d[v] : Real(0)) + (u == v ? f.f2 * d[w] : Real(0)));
-          }
+          addPair<TRICLINIC>(accs[q], f, dx, dy, dz);
         }
       }
     }
+    if constexpr (NEAR64)
+    {
+      // the near images: the energy in FP64 from FP64 offsets as C q (1/r - alpha erf(x)/x), x = alpha r (no erfc, no
+      // exponential), folded into the compensated sums after the chunk; the derivative channels in FP32 from the
+      // displacement rounded once
+      double near_energy = 0.0;
+      // the point's FP64 offset from the brick centre, recomputed here rather than kept live through the far loop
+      double ppx, ppy, ppz;
+      {
+        const double si[3] = {static_cast<double>(i) * p.delta[0], static_cast<double>(j) * p.delta[1],
+                              static_cast<double>(k) * p.delta[2]};
+        const double sb[3] = {(blockIdx.x * bx + 0.5 * (bx - 1)) * p.delta[0],
+                              (blockIdx.y * by + 0.5 * (by - 1)) * p.delta[1], (kb * bz + 0.5 * (bz - 1)) * p.delta[2]};
+        double q[3];
 #pragma unroll
-    for (int q = 0; q < NP; ++q) accs[q].flush();
+        for (int r = 0; r < 3; ++r)
+          q[r] = (p.cell[0][r] * si[0] + p.cell[1][r] * si[1] + p.cell[2][r] * si[2]) -
+                 (p.cell[0][r] * sb[0] + p.cell[1][r] * sb[1] + p.cell[2][r] * sb[2]);
+        ppx = q[0];
+        ppy = q[1];
+        ppz = q[2];
+      }
+      for (int c = 0; c < total_near; ++c)
+      {
+        const double4 a = npos[c];
+        const double dx = ppx - a.x, dy = ppy - a.y, dz = ppz - a.z;
+        double rr = dx * dx + dy * dy + dz * dz;
+        rr = rr > 0.1 ? rr : 0.1;
+        bool in = rr < p.rc2;
+        if constexpr (CLIP) in = in && rgd::insideSupercell<TRICLINIC>(chd, cicd, dx, dy, dz);
+        if (in)
+        {
+          if (COUNT && valid) ++npairs;
+          const double u = p.alpha * p.alpha * rr;
+          if (u <= rgd::kErfOverXMax * rgd::kErfOverXMax)
+            near_energy += a.w * (rsqrt(rr) - p.alpha * rgd::erfOverX(u));
+          else  // coarse grids (large bricks) only: beyond the polynomial's range
+          {
+            const double r = sqrt(rr);
+            near_energy += a.w * erfc(p.alpha * r) / r;
+          }
+          Factor<Real> f = ewaldFactor<Real>(static_cast<Real>(rr), static_cast<Real>(a.w), alpha);
+          f.e = Real(0);
+          addPair<TRICLINIC>(accs[0], f, static_cast<Real>(dx), static_cast<Real>(dy), static_cast<Real>(dz));
+        }
+      }
+      accs[0].flush();
+      accs[0].fold(0, near_energy);
+    }
+    else
+    {
+#pragma unroll
+      for (int q = 0; q < NP; ++q) accs[q].flush();
+    }
     __syncthreads();
   }
 
@@ -471,44 +589,97 @@ __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1
   }
 }
 
-template <typename Real, int TYPE, bool TRI, int NP = 1>
-cudaError_t launchTyped(const GridParams& p, const double4* ipos, const double4* ipar, int bx, int by, int bz,
-                        bool count, cudaStream_t stream)
+// Dynamic shared memory of a launch: the FP32/FP64 candidate list, NP parameter lists for Lennard-Jones grids, and the
+// FP64 near list of the FP32C Ewald grid.
+template <typename Real, int TYPE, int NP>
+size_t gridSharedBytes(int nt)
+{
+  const size_t chunk = static_cast<size_t>(nt) * kPer;
+  size_t b = sizeof(typename Vec4<Real>::T) * chunk;
+  if (TYPE != RG_GRID_EWALD_REAL) b += NP * sizeof(typename Vec4<Real>::T) * chunk;
+  if (TYPE == RG_GRID_EWALD_REAL && sizeof(Real) == 4) b += sizeof(double4) * chunk;
+  return b;
+}
+
+template <typename Real, int TYPE, bool TRI, int NP, bool COUNT, bool CLIP>
+cudaError_t launchKernel(const GridParams& p, const double4* ipos, const double4* ipar, int bx, int by, int bz,
+                         cudaStream_t stream)
 {
   const int zbricks = p.zb1 > p.zb0 ? p.zb1 - p.zb0 : (p.nz + bz - 1) / bz;
   dim3 grid((p.nx + bx - 1) / bx, (p.ny + by - 1) / by, zbricks);
-  int nt = bx * by * bz;
-  size_t shmem = (1 + NP) * sizeof(typename Vec4<Real>::T) * static_cast<size_t>(nt) * kPer;
-  if (count)
-  {
-    auto kern = gridKernel<Real, TYPE, TRI, true, NP>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shmem));
-    kern<<<grid, nt, shmem, stream>>>(p, ipos, ipar, bx, by, bz);
-  }
-  else
-  {
-    auto kern = gridKernel<Real, TYPE, TRI, false, NP>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shmem));
-    kern<<<grid, nt, shmem, stream>>>(p, ipos, ipar, bx, by, bz);
-  }
+  const int nt = bx * by * bz;
+  const size_t shmem = gridSharedBytes<Real, TYPE, NP>(nt);
+  auto kern = gridKernel<Real, TYPE, TRI, COUNT, NP, CLIP>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shmem));
+  kern<<<grid, nt, shmem, stream>>>(p, ipos, ipar, bx, by, bz);
   return cudaGetLastError();
+}
+
+template <typename Real, int TYPE, bool TRI, int NP = 1>
+cudaError_t launchTyped(const GridParams& p, const double4* ipos, const double4* ipar, int bx, int by, int bz,
+                        bool count, bool clip, cudaStream_t stream)
+{
+  if (clip)
+    return count ? launchKernel<Real, TYPE, TRI, NP, true, true>(p, ipos, ipar, bx, by, bz, stream)
+                 : launchKernel<Real, TYPE, TRI, NP, false, true>(p, ipos, ipar, bx, by, bz, stream);
+  return count ? launchKernel<Real, TYPE, TRI, NP, true, false>(p, ipos, ipar, bx, by, bz, stream)
+               : launchKernel<Real, TYPE, TRI, NP, false, false>(p, ipos, ipar, bx, by, bz, stream);
 }
 
 template <typename Real, bool TRI>
 cudaError_t launchPrec(int type, const GridParams& p, const double4* ipos, const double4* ipar, int bx, int by, int bz,
-                       bool count, cudaStream_t stream)
+                       bool count, bool clip, cudaStream_t stream)
 {
   switch (type)
   {
     case RG_GRID_LENNARD_JONES:
-      return launchTyped<Real, RG_GRID_LENNARD_JONES, TRI>(p, ipos, ipar, bx, by, bz, count, stream);
+      return launchTyped<Real, RG_GRID_LENNARD_JONES, TRI>(p, ipos, ipar, bx, by, bz, count, clip, stream);
     case RG_GRID_EWALD_REAL:
-      return launchTyped<Real, RG_GRID_EWALD_REAL, TRI>(p, ipos, ipar, bx, by, bz, count, stream);
+      return launchTyped<Real, RG_GRID_EWALD_REAL, TRI>(p, ipos, ipar, bx, by, bz, count, clip, stream);
     case RG_GRID_LENNARD_JONES_REPULSION:
-      return launchTyped<Real, RG_GRID_LENNARD_JONES_REPULSION, TRI>(p, ipos, ipar, bx, by, bz, count, stream);
+      return launchTyped<Real, RG_GRID_LENNARD_JONES_REPULSION, TRI>(p, ipos, ipar, bx, by, bz, count, clip, stream);
     default:
-      return launchTyped<Real, RG_GRID_LENNARD_JONES_ATTRACTION, TRI>(p, ipos, ipar, bx, by, bz, count, stream);
+      return launchTyped<Real, RG_GRID_LENNARD_JONES_ATTRACTION, TRI>(p, ipos, ipar, bx, by, bz, count, clip, stream);
   }
+}
+
+// Launch geometry shared by every entry point: cell, spacing, pair cutoff, the brick's staging radii and the supercell
+// clip. Returns whether the CLIP kernels are needed (the supercell that `cutoff` sizes is narrower than twice the pair
+// cutoff along some axis).
+bool setupGridParams(GridParams& gp, const rg::HostBox& box, const rg_forcefield* ff, double cutoff, int nx, int ny,
+                     int nz, int bx, int by, int bz)
+{
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) gp.cell[c][r] = box.c[c][r];
+  gp.ncells[0] = static_cast<double>(nx - 1);
+  gp.ncells[1] = static_cast<double>(ny - 1);
+  gp.ncells[2] = static_cast<double>(nz - 1);
+  for (int d = 0; d < 3; ++d) gp.delta[d] = 1.0 / gp.ncells[d];
+  gp.nx = nx;
+  gp.ny = ny;
+  gp.nz = nz;
+  const double rc = ff->cutoff_framework_vdw;
+  gp.rc2 = rc * rc;
+  double R = 0.0;  // brick half-diagonal
+  for (int sx = -1; sx <= 1; sx += 2)
+    for (int sy = -1; sy <= 1; sy += 2)
+      for (int sz = -1; sz <= 1; sz += 2)
+      {
+        double f[3] = {sx * 0.5 * (bx - 1) * gp.delta[0], sy * 0.5 * (by - 1) * gp.delta[1],
+                       sz * 0.5 * (bz - 1) * gp.delta[2]},
+               d[3];
+        rg::matvec(box.c, f, d);
+        R = std::fmax(R, std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
+      }
+  const double rf = rc + R + 1e-6;
+  gp.filter2 = rf * rf;
+  // near images: within kNearRadius + R of the brick centre, so that every pair closer than kNearRadius is among them
+  const double rn = kNearRadius + R;
+  gp.near2 = rn * rn;
+  gp.alpha = ff->ewald_alpha;
+  gp.coul = rg::coulombFactor();
+  gp.overlap = ff->overlap_criteria;
+  return rg::supercellClip(box, rc, cutoff, gp.clip_h, gp.clip_ic);
 }
 
 constexpr int kSlabs = 8;  // z-slabs of a grid whose host copy overlaps the build
@@ -626,7 +797,9 @@ rg_status buildOne(rg_ctx* ctx, int grid_type, const rg_forcefield* ff, const rg
   if (grid_type != RG_GRID_EWALD_REAL && (probe_type < 0 || probe_type >= ff->n_types))
     return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build: probe_type out of range");
   if (!out_device && !out_host) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build: no output");
-  (void)cutoff;  // the supercell size only selects which images the reference visits; all images within rc are used
+  if (!(cutoff > 0.0)) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build: cutoff must be positive");
+  if (rg_status fs = rg::checkFinite(ctx, unit_atoms, n_unit_atoms, "rg_grid_build")) return fs;
+  if (rg_status fs = rg::checkFiniteBox(ctx, unit_cell, "rg_grid_build")) return fs;
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
 
   rg::HostBox box = rg::makeHostBox(unit_cell);
@@ -665,38 +838,11 @@ rg_status buildOne(rg_ctx* ctx, int grid_type, const rg_forcefield* ff, const rg
   }
   RG_CUDA(ctx, cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), ctx->stream));
 
-  // brick shape and its half-diagonal
+  // brick shape, staging radii and supercell
   const int bx = 8, by = 8, bz = 4;
   GridParams gp{};
-  for (int c = 0; c < 3; ++c)
-    for (int r = 0; r < 3; ++r) gp.cell[c][r] = box.c[c][r];
-  gp.ncells[0] = static_cast<double>(nx - 1);
-  gp.ncells[1] = static_cast<double>(ny - 1);
-  gp.ncells[2] = static_cast<double>(nz - 1);
-  gp.delta[0] = 1.0 / gp.ncells[0];
-  gp.delta[1] = 1.0 / gp.ncells[1];
-  gp.delta[2] = 1.0 / gp.ncells[2];
-  gp.nx = nx;
-  gp.ny = ny;
-  gp.nz = nz;
+  const bool clip = setupGridParams(gp, box, ff, cutoff, nx, ny, nz, bx, by, bz);
   gp.n_images = n_images;
-  gp.rc2 = ff->cutoff_framework_vdw * ff->cutoff_framework_vdw;
-  double R = 0.0;
-  for (int sx = -1; sx <= 1; sx += 2)
-    for (int sy = -1; sy <= 1; sy += 2)
-      for (int sz = -1; sz <= 1; sz += 2)
-      {
-        double f[3] = {sx * 0.5 * (bx - 1) * gp.delta[0], sy * 0.5 * (by - 1) * gp.delta[1],
-                       sz * 0.5 * (bz - 1) * gp.delta[2]},
-               d[3];
-        rg::matvec(box.c, f, d);
-        R = std::fmax(R, std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
-      }
-  double rf = ff->cutoff_framework_vdw + R + 1e-6;
-  gp.filter2 = rf * rf;
-  gp.alpha = ff->ewald_alpha;
-  gp.coul = rg::coulombFactor();
-  gp.overlap = ff->overlap_criteria;
   gp.pair_count = dcount;
   gp.out[0] = dout;
   gp.out[1] = nullptr;
@@ -706,10 +852,10 @@ rg_status buildOne(rg_ctx* ctx, int grid_type, const rg_forcefield* ff, const rg
   double* hosts[1] = {out_host};
   rg_status lst = launchSlabbed(ctx, gp, bz, devs, hosts, 1, [&](const GridParams& g) {
     if (precision == RG_PRECISION_FP64)
-      return box.triclinic ? launchPrec<double, true>(grid_type, g, dpos, dpar, bx, by, bz, count, ctx->stream)
-                           : launchPrec<double, false>(grid_type, g, dpos, dpar, bx, by, bz, count, ctx->stream);
-    return box.triclinic ? launchPrec<float, true>(grid_type, g, dpos, dpar, bx, by, bz, count, ctx->stream)
-                         : launchPrec<float, false>(grid_type, g, dpos, dpar, bx, by, bz, count, ctx->stream);
+      return box.triclinic ? launchPrec<double, true>(grid_type, g, dpos, dpar, bx, by, bz, count, clip, ctx->stream)
+                           : launchPrec<double, false>(grid_type, g, dpos, dpar, bx, by, bz, count, clip, ctx->stream);
+    return box.triclinic ? launchPrec<float, true>(grid_type, g, dpos, dpar, bx, by, bz, count, clip, ctx->stream)
+                         : launchPrec<float, false>(grid_type, g, dpos, dpar, bx, by, bz, count, clip, ctx->stream);
   });
   if (lst) return lst;
   if (stats)
@@ -778,21 +924,13 @@ cudaError_t noallocScratchAddress(int device, void** out)
 }
 }  // namespace
 
-extern "C" rg_status rg_grid_build_noalloc(int device, void* stream, int grid_type, const rg_forcefield* ff,
-                                           const rg_box* unit_cell, const rg_atom* unit_atoms, int n_unit_atoms,
-                                           int probe_type, double cutoff, int nx, int ny, int nz, int precision,
-                                           double* out_device, rg_grid_stats* stats)
+namespace
 {
-  (void)cutoff;
-  if (!ff || !unit_cell || (n_unit_atoms > 0 && !unit_atoms) || n_unit_atoms < 0 || !out_device)
-    return RG_ERR_INVALID_ARGUMENT;
-  if (grid_type < 0 || grid_type > 3 || (precision != RG_PRECISION_FP64 && precision != RG_PRECISION_FP32C))
-    return RG_ERR_INVALID_ARGUMENT;
-  if (nx < 2 || ny < 2 || nz < 2) return RG_ERR_INVALID_ARGUMENT;
-  if (grid_type != RG_GRID_EWALD_REAL && (probe_type < 0 || probe_type >= ff->n_types)) return RG_ERR_INVALID_ARGUMENT;
-  if (device < 0 || device >= kMaxDevices) return RG_ERR_INVALID_ARGUMENT;
-  if (cudaSetDevice(device) != cudaSuccess) return RG_ERR_CUDA;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
+// The body of rg_grid_build_noalloc, with `device` current.
+rg_status gridBuildNoalloc(int device, cudaStream_t st, int grid_type, const rg_forcefield* ff, const rg_box* unit_cell,
+                           const rg_atom* unit_atoms, int n_unit_atoms, int probe_type, double cutoff, int nx, int ny,
+                           int nz, int precision, double* out_device, rg_grid_stats* stats)
+{
   void* base = nullptr;
   if (noallocScratchAddress(device, &base) != cudaSuccess) return RG_ERR_CUDA;
   double4* dpos = static_cast<double4*>(base);
@@ -873,46 +1011,19 @@ extern "C" rg_status rg_grid_build_noalloc(int device, void* stream, int grid_ty
 
   const int bx = 8, by = 8, bz = 4;
   GridParams gp{};
-  for (int c = 0; c < 3; ++c)
-    for (int r = 0; r < 3; ++r) gp.cell[c][r] = box.c[c][r];
-  gp.ncells[0] = static_cast<double>(nx - 1);
-  gp.ncells[1] = static_cast<double>(ny - 1);
-  gp.ncells[2] = static_cast<double>(nz - 1);
-  gp.delta[0] = 1.0 / gp.ncells[0];
-  gp.delta[1] = 1.0 / gp.ncells[1];
-  gp.delta[2] = 1.0 / gp.ncells[2];
-  gp.nx = nx;
-  gp.ny = ny;
-  gp.nz = nz;
+  const bool clip = setupGridParams(gp, box, ff, cutoff, nx, ny, nz, bx, by, bz);
   gp.n_images = n_images;
-  gp.rc2 = rc * rc;
-  double R = 0.0;
-  for (int sx = -1; sx <= 1; sx += 2)
-    for (int sy = -1; sy <= 1; sy += 2)
-      for (int sz = -1; sz <= 1; sz += 2)
-      {
-        double f[3] = {sx * 0.5 * (bx - 1) * gp.delta[0], sy * 0.5 * (by - 1) * gp.delta[1],
-                       sz * 0.5 * (bz - 1) * gp.delta[2]},
-               d[3];
-        rg::matvec(box.c, f, d);
-        R = std::fmax(R, std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
-      }
-  const double rf = rc + R + 1e-6;
-  gp.filter2 = rf * rf;
-  gp.alpha = ff->ewald_alpha;
-  gp.coul = C;
-  gp.overlap = ff->overlap_criteria;
   gp.pair_count = dcount;
   gp.out[0] = out_device;
   gp.out[1] = nullptr;
   const bool count = stats != nullptr;
   cudaError_t err;
   if (precision == RG_PRECISION_FP64)
-    err = box.triclinic ? launchPrec<double, true>(grid_type, gp, dpos, dpar, bx, by, bz, count, st)
-                        : launchPrec<double, false>(grid_type, gp, dpos, dpar, bx, by, bz, count, st);
+    err = box.triclinic ? launchPrec<double, true>(grid_type, gp, dpos, dpar, bx, by, bz, count, clip, st)
+                        : launchPrec<double, false>(grid_type, gp, dpos, dpar, bx, by, bz, count, clip, st);
   else
-    err = box.triclinic ? launchPrec<float, true>(grid_type, gp, dpos, dpar, bx, by, bz, count, st)
-                        : launchPrec<float, false>(grid_type, gp, dpos, dpar, bx, by, bz, count, st);
+    err = box.triclinic ? launchPrec<float, true>(grid_type, gp, dpos, dpar, bx, by, bz, count, clip, st)
+                        : launchPrec<float, false>(grid_type, gp, dpos, dpar, bx, by, bz, count, clip, st);
   if (err != cudaSuccess) return RG_ERR_CUDA;
   if (stats)
   {
@@ -925,6 +1036,32 @@ extern "C" rg_status rg_grid_build_noalloc(int device, void* stream, int grid_ty
     stats->d2h_bytes = 0;
   }
   return RG_OK;
+}
+}  // namespace
+
+extern "C" rg_status rg_grid_build_noalloc(int device, void* stream, int grid_type, const rg_forcefield* ff,
+                                           const rg_box* unit_cell, const rg_atom* unit_atoms, int n_unit_atoms,
+                                           int probe_type, double cutoff, int nx, int ny, int nz, int precision,
+                                           double* out_device, rg_grid_stats* stats)
+{
+  if (!ff || !unit_cell || (n_unit_atoms > 0 && !unit_atoms) || n_unit_atoms < 0 || !out_device)
+    return RG_ERR_INVALID_ARGUMENT;
+  if (grid_type < 0 || grid_type > 3 || (precision != RG_PRECISION_FP64 && precision != RG_PRECISION_FP32C))
+    return RG_ERR_INVALID_ARGUMENT;
+  if (nx < 2 || ny < 2 || nz < 2 || !(cutoff > 0.0)) return RG_ERR_INVALID_ARGUMENT;
+  if (rg_status fs = rg::checkFinite(nullptr, unit_atoms, n_unit_atoms, "rg_grid_build_noalloc")) return fs;
+  if (rg_status fs = rg::checkFiniteBox(nullptr, unit_cell, "rg_grid_build_noalloc")) return fs;
+  if (grid_type != RG_GRID_EWALD_REAL && (probe_type < 0 || probe_type >= ff->n_types)) return RG_ERR_INVALID_ARGUMENT;
+  if (device < 0 || device >= kMaxDevices) return RG_ERR_INVALID_ARGUMENT;
+  // the work runs with `device` current; the caller's current device is restored on every return
+  int previous = -1;
+  if (cudaGetDevice(&previous) != cudaSuccess) return RG_ERR_CUDA;
+  if (previous != device && cudaSetDevice(device) != cudaSuccess) return RG_ERR_CUDA;
+  const rg_status status = gridBuildNoalloc(device, static_cast<cudaStream_t>(stream), grid_type, ff, unit_cell,
+                                            unit_atoms, n_unit_atoms, probe_type, cutoff, nx, ny, nz, precision,
+                                            out_device, stats);
+  if (previous != device && cudaSetDevice(previous) != cudaSuccess) return RG_ERR_CUDA;
+  return status;
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -953,7 +1090,15 @@ extern "C" rg_status rg_grid_build_set(rg_ctx* ctx, const rg_forcefield* ff, con
     if (grid_types[g] != RG_GRID_EWALD_REAL && (probe_types[g] < 0 || probe_types[g] >= ff->n_types))
       return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_set: probe_type out of range");
   }
-  (void)cutoff;
+  // the cutoff that sizes each grid's supercell: the caller's, or the reference's per type (cutOffCoulomb for the Ewald
+  // grid, cutOffFrameworkVDW for the VDW grids; system_interpolation_grids.cpp:211, 236)
+  auto gridCutoff = [&](int type)
+  { return cutoff > 0.0 ? cutoff : (type == RG_GRID_EWALD_REAL ? ff->cutoff_coulomb : ff->cutoff_framework_vdw); };
+  for (int g = 0; g < n_grids; ++g)
+    if (!(gridCutoff(grid_types[g]) > 0.0))
+      return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_set: cutoff must be positive");
+  if (rg_status fs = rg::checkFinite(ctx, unit_atoms, n_unit_atoms, "rg_grid_build_set")) return fs;
+  if (rg_status fs = rg::checkFiniteBox(ctx, unit_cell, "rg_grid_build_set")) return fs;
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
   const rg::HostBox box = rg::makeHostBox(unit_cell);
   // which framework atoms a Lennard-Jones probe sees
@@ -977,8 +1122,9 @@ extern "C" rg_status rg_grid_build_set(rg_ctx* ctx, const rg_forcefield* ff, con
     }
     if (partner < 0)
     {
-      rg_status st = buildOne(ctx, grid_types[g], ff, unit_cell, unit_atoms, n_unit_atoms, probe_types[g], cutoff, nx,
-                              ny, nz, precision, out_device[g], out_host ? out_host[g] : nullptr,
+      rg_status st = buildOne(ctx, grid_types[g], ff, unit_cell, unit_atoms, n_unit_atoms, probe_types[g],
+                              gridCutoff(grid_types[g]), nx, ny, nz, precision, out_device[g],
+                              out_host ? out_host[g] : nullptr,
                               stats ? &stats[g] : nullptr, false);
       if (st) return st;
       done[g] = 1;
@@ -1014,33 +1160,8 @@ extern "C" rg_status rg_grid_build_set(rg_ctx* ctx, const rg_forcefield* ff, con
     RG_CUDA(ctx, cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), ctx->stream));
     const int bx = 8, by = 8, bz = 4;
     GridParams gp{};
-    for (int c = 0; c < 3; ++c)
-      for (int r = 0; r < 3; ++r) gp.cell[c][r] = box.c[c][r];
-    gp.ncells[0] = static_cast<double>(nx - 1);
-    gp.ncells[1] = static_cast<double>(ny - 1);
-    gp.ncells[2] = static_cast<double>(nz - 1);
-    for (int d = 0; d < 3; ++d) gp.delta[d] = 1.0 / gp.ncells[d];
-    gp.nx = nx;
-    gp.ny = ny;
-    gp.nz = nz;
+    const bool clip = setupGridParams(gp, box, ff, gridCutoff(RG_GRID_LENNARD_JONES), nx, ny, nz, bx, by, bz);
     gp.n_images = n_images;
-    gp.rc2 = ff->cutoff_framework_vdw * ff->cutoff_framework_vdw;
-    double R = 0.0;
-    for (int sx = -1; sx <= 1; sx += 2)
-      for (int sy = -1; sy <= 1; sy += 2)
-        for (int sz = -1; sz <= 1; sz += 2)
-        {
-          double f[3] = {sx * 0.5 * (bx - 1) * gp.delta[0], sy * 0.5 * (by - 1) * gp.delta[1],
-                         sz * 0.5 * (bz - 1) * gp.delta[2]},
-                 d[3];
-          rg::matvec(box.c, f, d);
-          R = std::fmax(R, std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]));
-        }
-    const double rf = ff->cutoff_framework_vdw + R + 1e-6;
-    gp.filter2 = rf * rf;
-    gp.alpha = ff->ewald_alpha;
-    gp.coul = rg::coulombFactor();
-    gp.overlap = ff->overlap_criteria;
     gp.pair_count = dcount;
     gp.out[0] = out_device[g];
     gp.out[1] = out_device[partner];
@@ -1049,12 +1170,14 @@ extern "C" rg_status rg_grid_build_set(rg_ctx* ctx, const rg_forcefield* ff, con
     double* hosts[2] = {out_host ? out_host[g] : nullptr, out_host ? out_host[partner] : nullptr};
     st = launchSlabbed(ctx, gp, bz, devs, hosts, 2, [&](const GridParams& q) {
       if (precision == RG_PRECISION_FP64)
-        return box.triclinic
-                   ? launchTyped<double, RG_GRID_LENNARD_JONES, true, 2>(q, dpos, dpar, bx, by, bz, count, ctx->stream)
-                   : launchTyped<double, RG_GRID_LENNARD_JONES, false, 2>(q, dpos, dpar, bx, by, bz, count, ctx->stream);
-      return box.triclinic
-                 ? launchTyped<float, RG_GRID_LENNARD_JONES, true, 2>(q, dpos, dpar, bx, by, bz, count, ctx->stream)
-                 : launchTyped<float, RG_GRID_LENNARD_JONES, false, 2>(q, dpos, dpar, bx, by, bz, count, ctx->stream);
+        return box.triclinic ? launchTyped<double, RG_GRID_LENNARD_JONES, true, 2>(q, dpos, dpar, bx, by, bz, count,
+                                                                                   clip, ctx->stream)
+                             : launchTyped<double, RG_GRID_LENNARD_JONES, false, 2>(q, dpos, dpar, bx, by, bz, count,
+                                                                                    clip, ctx->stream);
+      return box.triclinic ? launchTyped<float, RG_GRID_LENNARD_JONES, true, 2>(q, dpos, dpar, bx, by, bz, count, clip,
+                                                                                ctx->stream)
+                           : launchTyped<float, RG_GRID_LENNARD_JONES, false, 2>(q, dpos, dpar, bx, by, bz, count, clip,
+                                                                                 ctx->stream);
     });
     if (st) return st;
     if (stats)

@@ -57,6 +57,7 @@ struct QuinticParams
   int nx, ny, nz;
   int n_images;
   double rc2, filter2, alpha, overlap;
+  double clip_h[3], clip_ic[3][3];  // CLIP: the supercell that the cutoff argument sizes (see grid_build.cu)
   unsigned long long* pair_count;
   double* out;
   int zb0;  // first brick along z of this launch
@@ -116,7 +117,7 @@ __device__ __forceinline__ void ewaldFactors(Real rr, Real cq, Real alpha, Real 
 
 // Real = double: FP64 throughout. Real = float (FP32C): offsets from the brick centre rounded to FP32 once, FP32 pair
 // terms, FP32 partial sums per staged chunk folded into TwoSum-compensated hi/lo pairs, FP64 epilogue.
-template <typename Real, int TYPE, bool TRI, bool COUNT>
+template <typename Real, int TYPE, bool TRI, bool COUNT, bool CLIP>
 __global__ void __launch_bounds__(kThreads) quinticKernel(QuinticParams p, QuinticTable<Real> tab,
                                                           const double4* __restrict__ ipos,
                                                           const double4* __restrict__ ipar)
@@ -150,6 +151,17 @@ __global__ void __launch_bounds__(kThreads) quinticKernel(QuinticParams p, Quint
   }
   const Real rc2 = static_cast<Real>(p.rc2);
   const Real alpha = static_cast<Real>(p.alpha);
+  Real ch[3], cic[9];
+  if constexpr (CLIP)
+  {
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+      ch[d] = static_cast<Real>(p.clip_h[d]);
+#pragma unroll
+      for (int e = 0; e < 3; ++e) cic[3 * d + e] = static_cast<Real>(p.clip_ic[d][e]);
+    }
+  }
 
   Real acc[27];                             // FP64: the sums; FP32C: the partial sums of the current chunk
   float hi[F32 ? 27 : 1], lo[F32 ? 27 : 1];  // FP32C: compensated running sums
@@ -210,6 +222,8 @@ __global__ void __launch_bounds__(kThreads) quinticKernel(QuinticParams p, Quint
       const Real d[3] = {pr[0] - a.x, pr[1] - a.y, pr[2] - a.z};
       const Real rr = fmax(Real(0.1), d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
       if (rr >= rc2) continue;
+      if constexpr (CLIP)
+        if (!rgd::insideSupercell<TRI>(ch, cic, d[0], d[1], d[2])) continue;
       if (COUNT && valid) ++npairs;
       Real F[7];
       if constexpr (EWALD)
@@ -358,26 +372,33 @@ QuinticTable<Real> makeTable(const rg::HostBox& box, bool reference_rectangular)
 // bricks [p.zb0, zb1) along z
 template <typename Real, int TYPE, bool TRI>
 cudaError_t launchQuintic(const QuinticParams& p, int zb1, const QuinticTable<Real>& t, const double4* ipos,
-                          const double4* ipar, bool count, cudaStream_t stream)
+                          const double4* ipar, bool count, bool clip, cudaStream_t stream)
 {
   dim3 grid((p.nx + kBX - 1) / kBX, (p.ny + kBY - 1) / kBY, zb1 - p.zb0);
-  if (count)
-    quinticKernel<Real, TYPE, TRI, true><<<grid, kThreads, 0, stream>>>(p, t, ipos, ipar);
+  if (clip)
+  {
+    if (count)
+      quinticKernel<Real, TYPE, TRI, true, true><<<grid, kThreads, 0, stream>>>(p, t, ipos, ipar);
+    else
+      quinticKernel<Real, TYPE, TRI, false, true><<<grid, kThreads, 0, stream>>>(p, t, ipos, ipar);
+  }
+  else if (count)
+    quinticKernel<Real, TYPE, TRI, true, false><<<grid, kThreads, 0, stream>>>(p, t, ipos, ipar);
   else
-    quinticKernel<Real, TYPE, TRI, false><<<grid, kThreads, 0, stream>>>(p, t, ipos, ipar);
+    quinticKernel<Real, TYPE, TRI, false, false><<<grid, kThreads, 0, stream>>>(p, t, ipos, ipar);
   return cudaGetLastError();
 }
 
 template <typename Real>
 cudaError_t launchQuinticTyped(int grid_type, bool triclinic, const QuinticParams& p, int zb1,
                                const QuinticTable<Real>& t, const double4* ipos, const double4* ipar, bool count,
-                               cudaStream_t stream)
+                               bool clip, cudaStream_t stream)
 {
   if (grid_type == RG_GRID_EWALD_REAL)
-    return triclinic ? launchQuintic<Real, RG_GRID_EWALD_REAL, true>(p, zb1, t, ipos, ipar, count, stream)
-                     : launchQuintic<Real, RG_GRID_EWALD_REAL, false>(p, zb1, t, ipos, ipar, count, stream);
-  return triclinic ? launchQuintic<Real, RG_GRID_LENNARD_JONES, true>(p, zb1, t, ipos, ipar, count, stream)
-                   : launchQuintic<Real, RG_GRID_LENNARD_JONES, false>(p, zb1, t, ipos, ipar, count, stream);
+    return triclinic ? launchQuintic<Real, RG_GRID_EWALD_REAL, true>(p, zb1, t, ipos, ipar, count, clip, stream)
+                     : launchQuintic<Real, RG_GRID_EWALD_REAL, false>(p, zb1, t, ipos, ipar, count, clip, stream);
+  return triclinic ? launchQuintic<Real, RG_GRID_LENNARD_JONES, true>(p, zb1, t, ipos, ipar, count, clip, stream)
+                   : launchQuintic<Real, RG_GRID_LENNARD_JONES, false>(p, zb1, t, ipos, ipar, count, clip, stream);
 }
 
 // One thread per position: value (and gradient) of a tricubic or triquintic grid
@@ -425,7 +446,9 @@ extern "C" rg_status rg_grid_build_triquintic(rg_ctx* ctx, int grid_type, const 
   if (grid_type == RG_GRID_LENNARD_JONES && (probe_type < 0 || probe_type >= ff->n_types))
     return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_triquintic: probe_type out of range");
   if (!out_device && !out_host) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_triquintic: no output");
-  (void)cutoff;  // as in the tricubic build: every periodic image within rc is summed
+  if (!(cutoff > 0.0)) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_grid_build_triquintic: cutoff must be positive");
+  if (rg_status fs = rg::checkFinite(ctx, unit_atoms, n_unit_atoms, "rg_grid_build_triquintic")) return fs;
+  if (rg_status fs = rg::checkFiniteBox(ctx, unit_cell, "rg_grid_build_triquintic")) return fs;
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
 
   const rg::HostBox box = rg::makeHostBox(unit_cell);
@@ -489,6 +512,7 @@ extern "C" rg_status rg_grid_build_triquintic(rg_ctx* ctx, int grid_type, const 
   qp.filter2 = rf * rf;
   qp.alpha = ff->ewald_alpha;
   qp.overlap = ff->overlap_criteria;
+  const bool clip = rg::supercellClip(box, ff->cutoff_framework_vdw, cutoff, qp.clip_h, qp.clip_ic);
   qp.pair_count = dcount;
   qp.out = dout;
   const bool refRect = (flags & RG_TRIQUINTIC_REFERENCE_RECTANGULAR) != 0;
@@ -512,8 +536,8 @@ extern "C" rg_status rg_grid_build_triquintic(rg_ctx* ctx, int grid_type, const 
     qp.zb0 = sl * zb / n_slabs;
     const int zb1 = (sl + 1) * zb / n_slabs;
     const cudaError_t err =
-        fp32c ? launchQuinticTyped<float>(grid_type, box.triclinic, qp, zb1, table32, dpos, dpar, count, ctx->stream)
-              : launchQuinticTyped<double>(grid_type, box.triclinic, qp, zb1, table64, dpos, dpar, count, ctx->stream);
+        fp32c ? launchQuinticTyped<float>(grid_type, box.triclinic, qp, zb1, table32, dpos, dpar, count, clip, ctx->stream)
+              : launchQuinticTyped<double>(grid_type, box.triclinic, qp, zb1, table64, dpos, dpar, count, clip, ctx->stream);
     if (err != cudaSuccess) return rg::cudaFail(ctx, err, "quinticKernel launch");
     if (!out_host) continue;
     cudaEvent_t ev = nullptr;

@@ -113,6 +113,8 @@ struct Params
   double* part;    // [2][kRow][gridDim]: partial sums, column-major, two buffers alternating by phase
   unsigned long long* bar;  // [0] barrier arrivals in this launch (zeroed before each launch), [1] error flag
   int record;
+  long long spin_limit;     // polls before a barrier wait gives up (kSpinLimit; shorter only in the wait test)
+  int absent_cta;           // wait test: this CTA does not arrive at the first barrier of a launch (-1: none)
 };
 
 enum : uint32_t
@@ -237,11 +239,13 @@ __device__ bool gridBarrier(const Params& p, Shared& sh)
   if (threadIdx.x == 0)
   {
     const unsigned long long target = static_cast<unsigned long long>(sh.gen + 1) * gridDim.x;
-    unsigned long long v = addRelease(&p.bar[0], 1ull) + 1ull;
+    // the wait test leaves one arrival out of the first barrier, so that every CTA's bounded wait runs out
+    const bool absent = static_cast<int>(blockIdx.x) == p.absent_cta && sh.gen == 0;
+    unsigned long long v = absent ? loadAcquire(&p.bar[0]) : addRelease(&p.bar[0], 1ull) + 1ull;
     long long spins = 0;
     while (v < target)
     {
-      if (++spins > kSpinLimit)
+      if (++spins > p.spin_limit)
       {
         atomicExch(&p.bar[1], 1ull);
         sh.fail = 1;
@@ -1583,6 +1587,8 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   if (err == cudaSuccess) err = cudaMemsetAsync(p.stats, 0, sizeof(double) * kStats, sm);
   if (err == cudaSuccess) err = cudaMemsetAsync(p.sk, 0, sizeof(double2) * std::max(1, p.nk), sm);
   if (err == cudaSuccess) err = cudaMemsetAsync(p.bar, 0, sizeof(unsigned long long) * 2, sm);
+  p.spin_limit = kSpinLimit;
+  p.absent_cta = -1;
   if (err == cudaSuccess) err = cudaStreamSynchronize(sm);
   if (err != cudaSuccess)
   {
@@ -1635,6 +1641,14 @@ extern "C" rg_status rg_mixture_run(rg_mixture* x, int64_t moves, int record)
     RG_CUDA(ctx, cudaLaunchCooperativeKernel(reinterpret_cast<void*>(mixtureKernel), dim3(x->blocks), dim3(kThreads),
                                              args, x->smem, ctx->stream));
   }
+  return RG_OK;
+}
+
+extern "C" rg_status rg_mixture_set_wait_test(rg_mixture* x, int absent_cta, int64_t spin_limit)
+{
+  if (!x || absent_cta < -1 || absent_cta >= x->blocks || spin_limit < 1) return RG_ERR_INVALID_ARGUMENT;
+  x->p.absent_cta = absent_cta;
+  x->p.spin_limit = std::min<long long>(spin_limit, kSpinLimit);  // never longer than the production limit
   return RG_OK;
 }
 

@@ -15,6 +15,7 @@
 #include <array>
 #include <cmath>
 #include <cstdint>
+#include <optional>
 #include <span>
 #include <stdexcept>
 #include <string>
@@ -57,6 +58,7 @@ struct ForceField
   uint64_t reciprocalIntegerCutOffSquared = UINT64_MAX;
   double reciprocalCutOffSquared = 1.7976931348623157e308;
   double energyOverlapCriteria = 1e6;
+  int chargeMethod = RG_CHARGE_METHOD_EWALD;  // ForceField::chargeMethod
   bool useCharge = true;
   bool omitInterInteractions = false;
 
@@ -102,14 +104,15 @@ inline rg_box makeBox(const std::array<std::array<double, 3>, 3>& columns)
 // RunningEnergy fields these paths produce (internal units).
 struct RunningEnergy
 {
+  double externalFieldVDW = 0;
   double frameworkMoleculeVDW = 0, frameworkMoleculeCharge = 0, moleculeMoleculeVDW = 0, moleculeMoleculeCharge = 0;
   double ewald_fourier = 0, ewald_self = 0, ewald_exclusion = 0;
   std::array<double, 4> dudlambdaVDW{}, dudlambdaCharge{}, dudlambdaEwald{};
   double ewaldFourier() const { return ewald_fourier + ewald_self + ewald_exclusion; }
   double potentialEnergy() const
   {
-    return frameworkMoleculeVDW + frameworkMoleculeCharge + moleculeMoleculeVDW + moleculeMoleculeCharge +
-           ewald_fourier + ewald_self + ewald_exclusion;
+    return externalFieldVDW + frameworkMoleculeVDW + frameworkMoleculeCharge + moleculeMoleculeVDW +
+           moleculeMoleculeCharge + ewald_fourier + ewald_self + ewald_exclusion;
   }
 };
 
@@ -293,6 +296,33 @@ class GrowContext
     check(ctx_->get(), rg_system_set_molecules(s_, moleculeAtoms.data(), static_cast<int>(moleculeAtoms.size())),
           "rg_system_set_molecules");
   }
+  // an accepted move: the molecule's atoms from index `first` on, as the reference copies them into
+  // System::spanOfMoleculeAtoms
+  void updateMoleculeAtoms(std::size_t first, std::span<const rg_atom> atoms)
+  {
+    check(ctx_->get(),
+          rg_system_update_molecules(s_, static_cast<int>(first), atoms.data(), static_cast<int>(atoms.size())),
+          "rg_system_update_molecules");
+  }
+  // Component::blockingPockets: {fractional x, y, z, radius} in the framework's unit cell
+  void setBlockedPockets(const rg_box& frameworkUnitCell, const std::vector<std::array<double, 4>>& pockets)
+  {
+    check(ctx_->get(),
+          rg_system_set_blocked_pockets(s_, &frameworkUnitCell, pockets.empty() ? nullptr : pockets.front().data(),
+                                        static_cast<int>(pockets.size())),
+          "rg_system_set_blocked_pockets");
+  }
+  // System::hasExternalField with ForceField::potentialEnergySurfaceType / externalFieldGeometryParameters, or the
+  // external-field grid over the simulation box (RG_SURFACE_OFF switches it off)
+  void setExternalField(int surfaceType, const std::array<double, 4>& geometry,
+                        const InterpolationEnergyGrid* grid = nullptr)
+  {
+    check(ctx_->get(),
+          rg_system_set_external_field(s_, surfaceType, geometry.data(), grid ? &grid->unitCellBox : nullptr,
+                                       grid ? grid->numberOfGridPoints[0] : 0, grid ? grid->numberOfGridPoints[1] : 0,
+                                       grid ? grid->numberOfGridPoints[2] : 0, grid ? grid->data.data() : nullptr, 0),
+          "rg_system_set_external_field");
+  }
   rg_system* get() const { return s_; }
   rg_ctx* ctx() const { return ctx_->get(); }
   const ForceField& forceField() const { return forceField_; }
@@ -318,6 +348,7 @@ struct ChainTrial
 inline RunningEnergy fromTrial(const rg_trial_energy& t)
 {
   RunningEnergy r;
+  r.externalFieldVDW = t.external_field_vdw;
   r.frameworkMoleculeVDW = t.framework_vdw;
   r.frameworkMoleculeCharge = t.framework_charge;
   r.moleculeMoleculeVDW = t.molecule_vdw;
@@ -373,5 +404,55 @@ inline std::vector<ChainTrial> computeExternalNonOverlappingEnergies(const GrowC
     if (!out[i].overlap) energies.push_back({sets[i], fromTrial(out[i])});
   return energies;
 }
+
+// computeDualCutOffCorrection (cbmc/interactions.cpp:214-251): the set with the force field's cutoffs minus with
+// the dual cutoff; std::nullopt where either is dropped
+inline std::optional<RunningEnergy> computeDualCutOffCorrection(const GrowContext& context,
+                                                                std::span<const rg_atom> trialPositionSet,
+                                                                double dualCutOff, int64_t skipBackgroundMolecule = -1)
+{
+  rg_trial_energy out{};
+  check(context.ctx(),
+        rg_cbmc_dual_cutoff_correction(context.get(), trialPositionSet.data(),
+                                       static_cast<int>(trialPositionSet.size()), skipBackgroundMolecule, dualCutOff,
+                                       &out),
+        "computeDualCutOffCorrection");
+  if (out.overlap) return std::nullopt;
+  return fromTrial(out);
+}
 }  // namespace CBMC
+
+namespace Interactions
+{
+// computeFrameworkMoleculeEnergyDifference (interactions/framework_molecule.cpp:117-252) on the framework, grids and
+// force field of `context`; std::nullopt when a new atom overlaps
+inline std::optional<RunningEnergy> computeFrameworkMoleculeEnergyDifference(const CBMC::GrowContext& context,
+                                                                             std::span<const rg_atom> newatoms,
+                                                                             std::span<const rg_atom> oldatoms)
+{
+  rg_trial_energy out{};
+  check(context.ctx(),
+        rg_framework_molecule_energy_difference(context.get(), context.forceField().chargeMethod, newatoms.data(),
+                                                static_cast<int>(newatoms.size()), oldatoms.data(),
+                                                static_cast<int>(oldatoms.size()), &out),
+        "computeFrameworkMoleculeEnergyDifference");
+  if (out.overlap) return std::nullopt;
+  return CBMC::fromTrial(out);
+}
+
+// computeInterMolecularEnergyDifference (interactions/intermolecular.cpp:198-290) against the adsorbate atoms stored
+// in `context`; std::nullopt when a new atom overlaps
+inline std::optional<RunningEnergy> computeInterMolecularEnergyDifference(const CBMC::GrowContext& context,
+                                                                          std::span<const rg_atom> newatoms,
+                                                                          std::span<const rg_atom> oldatoms)
+{
+  rg_trial_energy out{};
+  check(context.ctx(),
+        rg_intermolecular_energy_difference(context.get(), newatoms.data(), static_cast<int>(newatoms.size()),
+                                            oldatoms.data(), static_cast<int>(oldatoms.size()), &out),
+        "computeInterMolecularEnergyDifference");
+  if (out.overlap) return std::nullopt;
+  return CBMC::fromTrial(out);
+}
+}  // namespace Interactions
 }  // namespace raspa_b200

@@ -25,6 +25,19 @@ GRID_LENNARD_JONES_REPULSION = 2
 GRID_LENNARD_JONES_ATTRACTION = 3
 PRECISION_FP64 = 0
 PRECISION_FP32C = 1
+CHARGE_METHOD_EWALD = 0
+CHARGE_METHOD_COULOMB = 1
+SURFACE_OFF = -1
+SURFACE_NONE = 0
+SURFACE_GRID_FILE = 1
+SURFACE_THIRD_ORDER_POLYNOMIAL = 3
+SURFACE_MULLER_BROWN = 8
+SURFACE_CYLINDER_X = 11
+SURFACE_CYLINDER_Y = 12
+SURFACE_CYLINDER_Z = 13
+SURFACE_RECTANGLE_X = 14
+SURFACE_RECTANGLE_Y = 15
+SURFACE_RECTANGLE_Z = 16
 SCHEME_TRICUBIC = 8
 SCHEME_TRIQUINTIC = 27
 TRIQUINTIC_REFERENCE_RECTANGULAR = 1
@@ -50,7 +63,7 @@ class TrialEnergy(ctypes.Structure):
     _fields_ = [("framework_vdw", ctypes.c_double), ("framework_charge", ctypes.c_double),
                 ("molecule_vdw", ctypes.c_double), ("molecule_charge", ctypes.c_double),
                 ("dudlambda_vdw", ctypes.c_double * 4), ("dudlambda_charge", ctypes.c_double * 4),
-                ("overlap", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("external_field_vdw", ctypes.c_double), ("overlap", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
 class GcmcComponent(ctypes.Structure):
@@ -188,6 +201,12 @@ def lib():
         L.rg_system_set_molecules.argtypes = [vp, vp, i32]
         L.rg_system_set_precision.argtypes = [vp, i32]
         L.rg_cbmc_external_energies.argtypes = [vp, vp, i32, i32, i32, i64, d, d, d, vp]
+        L.rg_cbmc_dual_cutoff_correction.argtypes = [vp, vp, i32, i64, d, vp]
+        L.rg_framework_molecule_energy_difference.argtypes = [vp, i32, vp, i32, vp, i32, vp]
+        L.rg_intermolecular_energy_difference.argtypes = [vp, vp, i32, vp, i32, vp]
+        L.rg_system_update_molecules.argtypes = [vp, i32, vp, i32]
+        L.rg_system_set_blocked_pockets.argtypes = [vp, P(RgBox), vp, i32]
+        L.rg_system_set_external_field.argtypes = [vp, i32, vp, P(RgBox), i32, i32, i32, vp, i32]
         L.rg_gcmc_create.argtypes = [vp, vp, P(GcmcComponent), P(GcmcParams), i32, P(vp)]
         L.rg_gcmc_destroy.argtypes = [vp]
         L.rg_gcmc_run.argtypes = [vp, i64, i32]
@@ -220,6 +239,7 @@ def lib():
         L.rg_mixture_set_state.argtypes = [vp, d, vp, i64]
         L.rg_mixture_run.argtypes = [vp, i64, i32]
         L.rg_mixture_results.argtypes = [vp, P(MixtureResult)]
+        L.rg_mixture_set_wait_test.argtypes = [vp, i32, i64]
         L.rg_mixture_get_positions.argtypes = [vp, vp, vp, i32, P(i32)]
         L.rg_mixture_get_structure_factors.argtypes = [vp, vp, i64]
         L.rg_mixture_set_proposal.argtypes = [vp, i32, vp, P(RgBox)]
@@ -604,6 +624,66 @@ class System:
             "rg_cbmc_external_energies")
         return [out[i] for i in range(n)]
 
+    def dual_cutoff_correction(self, trial_set, dual_cutoff: float, skip_background: int = -1) -> TrialEnergy:
+        """CBMC::computeDualCutOffCorrection of one trial set (rg_cbmc_dual_cutoff_correction)."""
+        t, p = _atoms_ptr(trial_set)
+        out = TrialEnergy()
+        check(self.ctx.handle, lib().rg_cbmc_dual_cutoff_correction(self.handle, p, len(t), skip_background,
+                                                                     dual_cutoff, ctypes.byref(out)),
+              "rg_cbmc_dual_cutoff_correction")
+        return out
+
+    def framework_energy_difference(self, new_atoms, old_atoms, charge_method: int = CHARGE_METHOD_EWALD):
+        """Interactions::computeFrameworkMoleculeEnergyDifference (rg_framework_molecule_energy_difference)."""
+        n, pn = _atoms_ptr(new_atoms)
+        o, po = _atoms_ptr(old_atoms)
+        out = TrialEnergy()
+        check(self.ctx.handle, lib().rg_framework_molecule_energy_difference(self.handle, charge_method, pn, len(n), po,
+                                                                              len(o), ctypes.byref(out)),
+              "rg_framework_molecule_energy_difference")
+        return out
+
+    def intermolecular_energy_difference(self, new_atoms, old_atoms):
+        """Interactions::computeInterMolecularEnergyDifference (rg_intermolecular_energy_difference)."""
+        n, pn = _atoms_ptr(new_atoms)
+        o, po = _atoms_ptr(old_atoms)
+        out = TrialEnergy()
+        check(self.ctx.handle, lib().rg_intermolecular_energy_difference(self.handle, pn, len(n), po, len(o),
+                                                                          ctypes.byref(out)),
+              "rg_intermolecular_energy_difference")
+        return out
+
+    def update_molecules(self, first_atom: int, atoms):
+        a, p = _atoms_ptr(atoms)
+        check(self.ctx.handle, lib().rg_system_update_molecules(self.handle, first_atom, p, len(a)),
+              "rg_system_update_molecules")
+
+    def set_blocked_pockets(self, unit_cell, pockets):
+        """pockets: (n, 4) centre as fractions of the framework unit cell and radius (Angstrom)."""
+        pk = np.ascontiguousarray(pockets, dtype=np.float64).reshape(-1, 4)
+        box = box_struct(unit_cell)
+        check(self.ctx.handle, lib().rg_system_set_blocked_pockets(self.handle, ctypes.byref(box),
+                                                                    ctypes.c_void_p(pk.ctypes.data), len(pk)),
+              "rg_system_set_blocked_pockets")
+
+    def set_external_field(self, surface_type: int, geometry=(5.0, 5.0, 0.0, 0.0), grid=None, grid_cell=None,
+                           grid_dims=(0, 0, 0), grid_on_device: bool = False):
+        """External field of the trial energies (rg_system_set_external_field); grid: host array or device pointer."""
+        g = np.ascontiguousarray(geometry, dtype=np.float64).reshape(4)
+        self._ext_geometry = g
+        box = box_struct(grid_cell) if grid_cell is not None else None
+        if grid is None:
+            gptr = None
+        elif grid_on_device:
+            gptr = ctypes.c_void_p(int(grid))
+        else:
+            self._ext_grid = np.ascontiguousarray(grid, dtype=np.float64)
+            gptr = ctypes.c_void_p(self._ext_grid.ctypes.data)
+        check(self.ctx.handle, lib().rg_system_set_external_field(
+            self.handle, surface_type, ctypes.c_void_p(g.ctypes.data), None if box is None else ctypes.byref(box),
+            int(grid_dims[0]), int(grid_dims[1]), int(grid_dims[2]), gptr, 1 if grid_on_device else 0),
+            "rg_system_set_external_field")
+
 
 class Gcmc:
     """Independent device-resident GCMC chains of one rigid component (rg_gcmc)."""
@@ -975,6 +1055,11 @@ class Mixture:
         r = MixtureResult()
         check(self.ctx.handle, lib().rg_mixture_results(self.handle, ctypes.byref(r)), "rg_mixture_results")
         return r.as_dict()
+
+    def set_wait_test(self, absent_cta: int, spin_limit: int):
+        """Test of the bounded barrier wait (rg_mixture_set_wait_test): the next launch's waits give up by design."""
+        check(self.ctx.handle, lib().rg_mixture_set_wait_test(self.handle, absent_cta, spin_limit),
+              "rg_mixture_set_wait_test")
 
     def positions(self):
         xyz = np.empty(3 * self.max_molecules * self.na)

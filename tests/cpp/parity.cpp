@@ -72,6 +72,15 @@ static ForceField zeoliteForceField(double rc, bool useCharge)
   return ff;
 }
 
+// the automatic Ewald alpha that System's constructor sets (ForceField::initializeEwaldParameters,
+// src/raspakit/forcefield/forcefield.cpp:1415-1424), precision 1e-6
+static double automaticEwaldAlpha(double cutOffCoulomb)
+{
+  const double eps = 1e-6;
+  const double tol = std::sqrt(std::fabs(std::log(eps * cutOffCoulomb)));
+  return std::sqrt(std::fabs(std::log(eps * cutOffCoulomb * tol))) / cutOffCoulomb;
+}
+
 static rg_atom atom(double x, double y, double z, double q, int type, uint32_t mol)
 {
   rg_atom a{};
@@ -224,6 +233,71 @@ int main()
       EXPECT_NEAR(e2[0].energy.moleculeMoleculeVDW * EnergyToKelvin, 2352.42793591, 1e-6);
       EXPECT_NEAR(e2[1].energy.moleculeMoleculeVDW * EnergyToKelvin, 2352.42793591, 1e-6);
     }
+  }
+
+  {  // static_energy.Test_2_CO2_in_ITQ_29_1x1x1 (tests/raspakit-tests/static_energy.cpp:21-46): the real-space Ewald
+     // Coulomb pair and the Lennard-Jones pair, framework-molecule and molecule-molecule, charged framework
+    ForceField ff = zeoliteForceField(12.0, true);
+    ff.EwaldAlpha = automaticEwaldAlpha(12.0);
+    const std::vector<rg_atom> fw = itq29(1);
+    CBMC::GrowContext context(ctx, ff, cubic(11.8671), fw);
+    std::vector<rg_atom> atoms = co2(5.93355, 7.93355, 5.93355, 0);
+    std::vector<rg_atom> second = co2(5.93355, 3.93355, 5.93355, 1);
+    atoms.insert(atoms.end(), second.begin(), second.end());
+    context.setMoleculeAtoms(atoms);
+    auto e = CBMC::computeExternalNonOverlappingEnergies(context, atoms);  // one trial per atom
+    EXPECT_NEAR(e.size(), 6.0, 0.0);
+    if (e.size() == 6)
+    {
+      double fwVDW = 0.0, fwCharge = 0.0, mmVDW = 0.0, mmCharge = 0.0;
+      for (std::size_t i = 0; i < 6; ++i)
+      {
+        fwVDW += e[i].energy.frameworkMoleculeVDW;
+        fwCharge += e[i].energy.frameworkMoleculeCharge;
+      }
+      for (std::size_t i = 0; i < 3; ++i)  // the first CO2 against the second: every intermolecular pair once
+      {
+        mmVDW += e[i].energy.moleculeMoleculeVDW;
+        mmCharge += e[i].energy.moleculeMoleculeCharge;
+      }
+      EXPECT_NEAR(fwVDW * EnergyToKelvin, -1545.62921755, 1e-6);
+      EXPECT_NEAR(fwCharge * EnergyToKelvin, -592.13188606, 1e-6);
+      EXPECT_NEAR(mmVDW * EnergyToKelvin, -242.42459776, 1e-6);
+      EXPECT_NEAR(mmCharge * EnergyToKelvin, 154.11883595, 1e-6);
+    }
+
+    // a translation of the second CO2 through the difference shims (the translation move's calls,
+    // mc_moves/component/translation.cpp:30-200) equals the change of the energies above
+    std::vector<rg_atom> moved = co2(5.93355 + 0.41, 3.93355 - 0.27, 5.93355 + 0.33, 1);
+    std::span<const rg_atom> old(atoms.data() + 3, 3);
+    auto dFramework = Interactions::computeFrameworkMoleculeEnergyDifference(context, moved, old);
+    auto dMolecule = Interactions::computeInterMolecularEnergyDifference(context, moved, old);
+    EXPECT_NEAR(dFramework.has_value() && dMolecule.has_value() ? 1.0 : 0.0, 1.0, 0.0);
+    std::vector<rg_atom> after(atoms.begin(), atoms.begin() + 3);
+    after.insert(after.end(), moved.begin(), moved.end());
+    auto eNew = CBMC::computeExternalNonOverlappingEnergies(context, moved);
+    auto eOld = CBMC::computeExternalNonOverlappingEnergies(context, std::vector<rg_atom>(old.begin(), old.end()));
+    if (dFramework && dMolecule && eNew.size() == 3 && eOld.size() == 3)
+    {
+      double fv = 0.0, fq = 0.0, mv = 0.0, mq = 0.0;
+      for (int i = 0; i < 3; ++i)
+      {
+        fv += eNew[i].energy.frameworkMoleculeVDW - eOld[i].energy.frameworkMoleculeVDW;
+        fq += eNew[i].energy.frameworkMoleculeCharge - eOld[i].energy.frameworkMoleculeCharge;
+        mv += eNew[i].energy.moleculeMoleculeVDW - eOld[i].energy.moleculeMoleculeVDW;
+        mq += eNew[i].energy.moleculeMoleculeCharge - eOld[i].energy.moleculeMoleculeCharge;
+      }
+      EXPECT_NEAR(dFramework->frameworkMoleculeVDW, fv, 1e-9 * std::fabs(fv) + 1e-12);
+      EXPECT_NEAR(dFramework->frameworkMoleculeCharge, fq, 1e-9 * std::fabs(fq) + 1e-12);
+      EXPECT_NEAR(dMolecule->moleculeMoleculeVDW, mv, 1e-9 * std::fabs(mv) + 1e-12);
+      EXPECT_NEAR(dMolecule->moleculeMoleculeCharge, mq, 1e-9 * std::fabs(mq) + 1e-12);
+    }
+    // accepted: the stored atoms follow, and moving back gives the opposite difference
+    context.updateMoleculeAtoms(3, moved);
+    auto back = Interactions::computeInterMolecularEnergyDifference(context, old, moved);
+    if (back && dMolecule)
+      EXPECT_NEAR(back->moleculeMoleculeCharge, -dMolecule->moleculeMoleculeCharge,
+                  1e-9 * std::fabs(dMolecule->moleculeMoleculeCharge) + 1e-12);
   }
 
   {  // grid build through InterpolationEnergyGrid, then the grid branch of the trial energies

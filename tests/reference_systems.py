@@ -13,6 +13,7 @@
 from __future__ import annotations
 
 import itertools
+import math
 
 import numpy as np
 
@@ -37,6 +38,15 @@ _ZEOLITE = [
     ("probe-CH4", False, 0.0, 158.5, 3.72),
     ("probe-N2", False, 0.0, 91.5, 3.681),
 ]
+
+
+def auto_ewald_alpha(cutoff_coulomb: float, precision: float = 1e-6) -> float:
+    """The automatic Ewald alpha that System's constructor sets (ForceField::initializeEwaldParameters,
+    src/raspakit/forcefield/forcefield.cpp:1415-1424): 0.26505830360350674 for a 12 Angstrom cutoff, where the
+    force field's default is the rounded 0.265058."""
+    eps = min(abs(precision), 0.5)
+    tol = math.sqrt(abs(math.log(eps * cutoff_coulomb)))
+    return math.sqrt(abs(math.log(eps * cutoff_coulomb * tol))) / cutoff_coulomb
 
 
 def zeolite_forcefield(rc: float = 12.0, shifted: bool = True, use_charge: bool = True) -> ForceField:

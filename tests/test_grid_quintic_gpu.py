@@ -302,3 +302,20 @@ def test_triquintic_fp32c_vs_oracle(ctx, oracle, grid_type, triclinic):
     print("triquintic fp32c", grid_type, triclinic, "max channel error", err.max(), "points", n)
     assert n >= 30
     assert np.all(err < TQ_FP32C_TOL[grid_type]), err
+
+
+@pytest.mark.parametrize("triclinic", [False, True])
+def test_triquintic_cutoff_sizes_the_supercell(ctx, oracle, triclinic):
+    """As for the tricubic build: the cutoff argument sizes the reference's supercell, whose minimum image drops pairs
+    within the pair cutoff when it is narrower than twice that cutoff."""
+    ff = synthetic_forcefield(charges=True)
+    cell, atoms = triclinic_system(ff) if triclinic else synthetic_framework(ff)
+    cutoff = 5.0 if triclinic else 9.0
+    dims = (9, 8, 8)
+    for grid_type, probe in ((native.GRID_EWALD_REAL, 0), (native.GRID_LENNARD_JONES, ff.index("CH4"))):
+        out, stats = ctx.grid_build_triquintic(grid_type, ff, cell, atoms, probe, cutoff, dims, count_pairs=True)
+        ref = oracle.make_grid_triquintic(grid_type, ff, cell, atoms, probe, cutoff, dims)
+        err, n = channel_errors(out, ref)
+        assert n >= 20 and np.all(err < 1e-9), err
+        assert stats["pair_count"] == oracle.grid_pair_count(grid_type, ff, cell, atoms, probe, cutoff, dims)
+        assert stats["pair_count"] < oracle.grid_pair_count(grid_type, ff, cell, atoms, probe, 12.0, dims)

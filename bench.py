@@ -459,6 +459,38 @@ def run_mixture(args, ctx, world, rank, dist, torch):
                                                "by its grid barriers, not by memory"},
            "e2e": {"value": world * (MIXTURE_MOVES // 4) / e2e_secs, "unit": "MC move attempts/s",
                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 176}}
+    # several independent copies of the system at once: one cooperative launch, each copy on its own quarter of the
+    # SMs (rg_mixture_run_many), the way the GPU is used for a batch of systems rather than a single chain
+    n_sys, sms = 4, torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    many = []
+    for s in range(n_sys):
+        m = native.Mixture(d["system"], d["ewald"], comps, beta, [fugacity_of(1e5), fugacity_of(1e5)], d["xyz"],
+                           d["comp"], max_molecules=6000, seed=100 + 10 * rank + s, n_blocks=sms // n_sys)
+        m.set_state(e0, sk0)
+        for c, pr in enumerate(props):
+            m.set_proposal(c, pr, d["unit_cell"])
+        many.append(m)
+    native.Mixture.run_many(many, MIXTURE_EQUIL, record=False)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e2_, e3_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2_.record(stream)
+    native.Mixture.run_many(many, MIXTURE_MOVES, record=True)
+    e3_.record(stream)
+    torch.cuda.synchronize()
+    secs_many = max_over_ranks(e2_.elapsed_time(e3_) / 1e3, world, dist)
+    rm = [m.results() for m in many]
+    xyz_m, comp_m = many[0].positions()
+    e_many = total_energy(d["system"], d["ewald"], ff, comps, xyz_m, comp_m)
+    out["several_systems"] = {
+        "systems": n_sys, "blocks_per_system": sms // n_sys, "moves_per_system": MIXTURE_MOVES,
+        "value": world * n_sys * MIXTURE_MOVES / secs_many, "unit": "MC move attempts/s (all systems)",
+        "ms": secs_many * 1e3, "status": [r_["status"] for r_ in rm],
+        "drift_relative_first_system": abs(rm[0]["energy"] - e_many) / max(1.0, abs(e_many)),
+        "path": "rg_mixture_run_many: one cooperative launch, CTAs [s B, (s + 1) B) run system s"}
+    for m in many:
+        m.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
         from concurrent.futures import ThreadPoolExecutor
@@ -746,6 +778,112 @@ PATH_INSERTIONS = 200   # CBMC insertions whose trial sets go through rg_cbmc_ex
 PATH_DELTAS = 1000      # Ewald Fourier differences through rg_ewald_delta, per box
 PATH_FULL = 20          # full structure-factor recomputes through rg_ewald_full
 EWALD_FLOPS_PER_TERM = 16  # one (atom, k) term of the full recompute: two complex products + a complex multiply-add
+
+
+EWALD_BATCH_SYSTEMS = 1184
+EWALD_BATCH_STEPS = 20
+
+
+def run_ewald_batch(args, ctx, world, rank, dist, torch):
+    """Path (c) batched: the Fourier energy difference of one CO2 translation in each of 1,184 systems that share the
+    configuration-5 box and k-vectors (kmax 12, the full half-box, 8,124 k-vectors), one rg_ewald_batch_delta call per
+    step: every system's S(k) read and its trial S(k) written (32 bytes per k-vector and system), the HBM roofline of
+    the structure-factor update."""
+    from raspa3_b200 import native
+    from raspa3_b200.mixture import CONFIG5_CELL
+    from raspa3_b200.synthetic import random_molecules, synthetic_forcefield
+
+    ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=12, sphere=False)
+    cell = np.diag([4 * CONFIG5_CELL[0], 4 * CONFIG5_CELL[1], 4 * CONFIG5_CELL[2]])
+    ew = native.Ewald(ctx, ff, cell)
+    nk = ew.n_kvectors
+    n_sys = EWALD_BATCH_SYSTEMS
+    batch = native.EwaldBatch(ew, n_sys)
+    mols = random_molecules(ff, cell, 200, seed=5)
+    ew.full(mols, [3] * 200)
+    for sy in range(n_sys):
+        batch.set(sy)
+    rng = np.random.default_rng(8)
+
+    def moves():
+        out = []
+        for sy in range(n_sys):
+            m = int(rng.integers(200))
+            old = mols[3 * m:3 * m + 3]
+            new = old.copy()
+            d = rng.normal(size=3) * 0.5
+            for i, k in enumerate("xyz"):
+                new[k] += d[i]
+            out.append(np.concatenate([new, old]))
+        return np.concatenate(out)
+
+    steps_atoms = [moves() for _ in range(4)]
+    previous = ctx.stream
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    for w in range(max(3, args.warmup)):
+        batch.delta(steps_atoms[w % 4], 6, [3] * n_sys, [3] * n_sys)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(EWALD_BATCH_STEPS)]
+    t0 = time.perf_counter()
+    for i, (a, b) in enumerate(ev):
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            batch.delta(steps_atoms[i % 4], 6, [3] * n_sys, [3] * n_sys)
+            b.record(stream)
+    torch.cuda.synchronize()
+    host_s = time.perf_counter() - t0
+    dev_ms = statistics.mean(x.elapsed_time(y) for x, y in ev)
+    ctx.set_stream(previous or None)
+    host_s = max_over_ranks(host_s, world, dist)
+    sk_bytes = n_sys * nk * 32
+    atom_bytes = n_sys * 6 * 48
+    hbm = None
+    try:
+        hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs")
+    except (OSError, ValueError):
+        hbm = None
+    gbs = sk_bytes / (dev_ms * 1e-3) / 1e9
+    out = {"workload": f"{n_sys} systems x one CO2 translation, {nk} k-vectors (kmax 12, the full half-box), "
+                       "config-5 box, one rg_ewald_batch_delta call per step",
+           "value": world * n_sys / (dev_ms * 1e-3), "unit": "Fourier differences/s",
+           "ms_per_step": dev_ms, "steps": EWALD_BATCH_STEPS,
+           "roofline": {"kernel": "ewaldBatchDeltaKernel", "bound": "hbm", "achieved": gbs, "peak": hbm,
+                        "unit": "GB/s", "frac": (gbs / hbm) if hbm else None,
+                        "bytes_per_step": sk_bytes, "bytes_note": "32 B per k-vector and system: read S(k), write the "
+                        "trial S(k); the step's device time also holds the 0.34 MB upload of the moved atoms",
+                        "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+           "e2e": {"value": world * n_sys * EWALD_BATCH_STEPS / host_s, "unit": "Fourier differences/s",
+                   "h2d_bytes_per_step": atom_bytes, "d2h_bytes_per_step": 8 * n_sys,
+                   "path": "rg_ewald_batch_delta with host atoms and host results"}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        from concurrent.futures import ThreadPoolExecutor
+
+        _, stored = oracle.ewald_fourier_energy(ff, cell, mols, [3] * 200)
+        threads = os.cpu_count() or 1
+        atoms = steps_atoms[0]
+        per = max(1, int(8 * args.cpu_seconds / 12.0))
+
+        def one(t):
+            for j in range(per):
+                sy = (t * per + j) % n_sys
+                a = atoms[6 * sy:6 * sy + 6]
+                oracle.ewald_delta(ff, cell, stored, a[:3], a[3:])
+
+        one(0)
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as pool:
+            list(pool.map(one, range(threads)))
+        secs = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": threads * per / secs, "unit": "Fourier differences/s", "cores": threads,
+                               "kind": "port", "sample": f"{threads * per} differences, one system per thread "
+                                                         f"(FP64 oracle of energyDifferenceEwaldFourier) in {secs:.1f} s"}
+    batch.close()
+    ew.close()
+    return out
 
 
 def run_paths(args, ctx, world, rank, dist, torch):
@@ -1161,6 +1299,7 @@ def run_ours(args):
     # ---- paths (b) and (c) on their own through the C-ABI (configuration 5, and configuration 2 for the Ewald) ----
     if not args.no_paths:
         line["paths"] = run_paths(args, ctx, world, rank, dist, torch)
+        line["paths"]["ewald_batch"] = run_ewald_batch(args, ctx, world, rank, dist, torch)
     # ---- learned vs uniform first-bead proposal at equal loading error (configuration 4) ----
     if not args.no_learned:
         del flush

@@ -238,7 +238,11 @@ rg_status rg_grid_load(const char* path, uint64_t fingerprint, int scheme, int n
 /* InterpolationEnergyGrid::writeOutput (interpolation_energy_grid.cpp:4760-4789): a cube file of the energy channel in
  * K, values in memory order (x fastest), one per line. The point counts are written as the negative numbers the
  * reference's cube reader expects (parseExternalFieldGridDimensions, :3516-3568); the reference's writer negates an
- * unsigned count there. origin: 3 doubles or NULL for (0, 0, 0). */
+ * unsigned count there. origin: 3 doubles or NULL for (0, 0, 0).
+ * unit_cell is the grid's own box (the framework unit cell the grid was built over), not the simulation box: the
+ * header's voxel vectors are its cell vectors divided by the point counts. Only channel 0 (the energy) of a tricubic
+ * or triquintic grid is written; a caller migrating from writeOutput(systemId, simulationBox, forceField) passes the
+ * framework's unit cell. */
 rg_status rg_grid_write_cube(const char* path, int scheme, const double* data, int nx, int ny, int nz,
                              const rg_box* unit_cell, const double* origin);
 
@@ -529,6 +533,30 @@ rg_status rg_ewald_delta(rg_ewald* ewald, const rg_atom* new_atoms, int n_new, c
 /* Replaces Interactions::acceptEwaldMove (ewald.cpp:1565-1574): the trial structure factors become the stored ones
  * (a pointer swap, no copy). */
 rg_status rg_ewald_accept(rg_ewald* ewald);
+
+/* ---- the structure-factor update of many systems at once ----
+ * n_systems systems that share the box, force field and k-vectors of `ewald` (created without dU/dlambda groups),
+ * each with its own stored and trial structure factors on the device: the Fourier part of
+ * Interactions::energyDifferenceEwaldFourier (src/raspakit/interactions/ewald.cpp:1098-1162) for one move in every
+ * system in one launch, and acceptEwaldMove (:1565-1574) per system as a buffer flip. It serves the drivers that
+ * advance many independent systems (replicas, chains of a screening run); a system's self, exclusion and net-charge
+ * terms need no structure factors and come from rg_ewald_delta's host terms (zero for translations and rotations).
+ * Traffic per system and move: 32 bytes per k-vector (read S(k), write the trial S(k)). */
+typedef struct rg_ewald_batch rg_ewald_batch;
+rg_status rg_ewald_batch_create(rg_ewald* ewald, int n_systems, rg_ewald_batch** out);
+rg_status rg_ewald_batch_destroy(rg_ewald_batch* batch);
+/* Stored S(k) of one system: 2 nk doubles (re, im per k) from host memory, or, with sk == NULL, ewald's stored
+ * structure factor (as rg_ewald_full or rg_ewald_set_structure_factors left it). */
+rg_status rg_ewald_batch_set(rg_ewald_batch* batch, int system, const double* sk);
+/* which = 0: the stored S(k) of a system, 1: its trial S(k) from the last rg_ewald_batch_delta (2 nk doubles). */
+rg_status rg_ewald_batch_get(rg_ewald_batch* batch, int system, int which, double* sk);
+/* One move per system: atoms[s * max_atoms ...] holds system s's n_new[s] new atoms followed by its n_old[s] old atoms
+ * (at most 16 together). delta_fourier[s] receives the Fourier energy change (internal units, the ewald_fourier term
+ * of rg_ewald_delta) and the system's trial S(k) is written. */
+rg_status rg_ewald_batch_delta(rg_ewald_batch* batch, const rg_atom* atoms, int max_atoms, const int32_t* n_new,
+                               const int32_t* n_old, double* delta_fourier);
+/* accept[s] != 0: system s's trial S(k) becomes its stored S(k). */
+rg_status rg_ewald_batch_accept(rg_ewald_batch* batch, const uint8_t* accept);
 /* Copies structure factors to the host, 2*(1+n_groups) doubles per k-vector in the reference's storedEik order
  * (total, then group sums; re, im). which: 0 = stored, 1 = trial, 2 = framework (2 doubles per k). */
 rg_status rg_ewald_get_structure_factors(rg_ewald* ewald, int which, double* host, int64_t n_doubles);
@@ -670,6 +698,11 @@ rg_status rg_mixture_set_state(rg_mixture* mixture, double energy, const double*
 /* Advances the system by `moves` move attempts (the mix of mc_moves/mc_moves.cpp's component moves); record != 0
  * accumulates the loading and energy averages. Results, positions and structure factors are read afterwards. */
 rg_status rg_mixture_run(rg_mixture* mixture, int64_t moves, int record);
+/* Several independent mixtures advanced by one cooperative launch: system s runs on CTAs [s B, (s + 1) B), B the
+ * CTA count every one of them was created with (rg_mixture_params.n_blocks, the same for all), so n small systems
+ * share the GPU instead of each leaving most SMs idle. All on one rg_ctx; n <= 8 and n B CTAs must fit on the GPU
+ * at once (one CTA per SM). No counterpart in the reference, whose systems run on separate threads. */
+rg_status rg_mixture_run_many(rg_mixture* const* mixtures, int n, int64_t moves, int record);
 rg_status rg_mixture_results(rg_mixture* mixture, rg_mixture_result* out);
 /* Test of the bounded grid-barrier wait (no counterpart in the reference, whose moves run on one CPU thread): in the
  * next launch CTA absent_cta does not arrive at the first barrier, so every CTA's wait gives up after spin_limit polls

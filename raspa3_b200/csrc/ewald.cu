@@ -902,3 +902,273 @@ rg_status ewaldExport(rg_ewald* e, const char4** kvec, const double** temp, cons
   return RG_OK;
 }
 }  // namespace rgd
+
+// ---------------------------------------------------------------------------------------------------------------------
+// The structure-factor update of many systems in one launch (the Fourier part of energyDifferenceEwaldFourier,
+// ewald.cpp:1098-1162, for one move in each of n systems that share the box, the force field and the k-vectors).
+//
+// Each system keeps two structure-factor buffers, stored and trial, and a flag says which is which; an accepted move
+// flips its system's flag (acceptEwaldMove, ewald.cpp:1565-1574, without a copy). The launch is (k-tile, system): a
+// block loads its system's moved atoms, builds their phase tables e^{i 2 pi m s_d} (m = 0..kmax_d) in shared memory,
+// and every thread forms Delta rho(k) of its k-vectors from two complex products per atom, reads S(k), writes
+// S(k) + Delta rho(k) and sums temp(k) (2 Re(conj(S) Delta rho) + |Delta rho|^2). Block partials are reduced per system
+// in block order by the system's last block, which writes the total into mapped pinned host memory. The traffic per
+// system and move is 32 bytes per k-vector (read S, write the trial S); k-vectors and prefactors are shared by all
+// systems and stay in L2.
+// ---------------------------------------------------------------------------------------------------------------------
+struct rg_ewald_batch
+{
+  rg_ewald* ewald = nullptr;
+  int n = 0;
+  int max_atoms = 0;
+  double2* sk = nullptr;           // [2][n][nk]
+  unsigned char* cur = nullptr;    // [n]: which buffer holds the stored S(k) of system s
+  std::vector<unsigned char> cur_host;
+  MovedAtom* atoms = nullptr;      // [n][kBatchAtoms] device
+  MovedAtom* atoms_host = nullptr; // pinned
+  int* counts = nullptr;           // [n] moved atoms per system (device)
+  int* counts_host = nullptr;      // pinned
+  double* partial = nullptr;       // [n][blocks]
+  unsigned int* counter = nullptr; // [n]
+  double* result = nullptr;        // device view of result_host
+  double* result_host = nullptr;   // [n] mapped pinned
+  int blocks = 0;                  // k-tiles per system
+};
+
+namespace
+{
+constexpr int kBatchAtoms = 16;   // old + new atoms of one system's move
+constexpr int kBatchKPerThread = 2;
+
+__global__ void __launch_bounds__(kThreads) ewaldBatchDeltaKernel(
+    int64_t nk, int n_systems, const char4* __restrict__ kvec, const double* __restrict__ temp, double2* sk,
+    const unsigned char* __restrict__ cur, const MovedAtom* __restrict__ atoms, int atom_stride,
+    const int* __restrict__ counts, int kxm, int kym, int kzm, double* partial, unsigned int* counter, double* result)
+{
+  extern __shared__ double2 tab[];  // [kBatchAtoms][(kxm+1) + (kym+1) + (kzm+1)]
+  __shared__ double wq[kBatchAtoms];
+  __shared__ double red[kThreads / 32];
+  __shared__ bool last;
+  const int sys = blockIdx.y;
+  const int na = counts[sys];
+  const int stride = (kxm + 1) + (kym + 1) + (kzm + 1);
+  const MovedAtom* ma = atoms + static_cast<long long>(sys) * atom_stride;
+  for (int idx = threadIdx.x; idx < na * stride; idx += blockDim.x)
+  {
+    const int a = idx / stride, m = idx - a * stride;
+    const int d = (m <= kxm) ? 0 : ((m <= kxm + 1 + kym) ? 1 : 2);
+    const int mm = (d == 0) ? m : ((d == 1) ? m - (kxm + 1) : m - (kxm + 1) - (kym + 1));
+    double sn, cs;
+    sincospi(2.0 * static_cast<double>(mm) * ma[a].s[d], &sn, &cs);
+    tab[a * stride + m] = make_double2(cs, sn);
+  }
+  for (int a = threadIdx.x; a < na; a += blockDim.x) wq[a] = ma[a].w;
+  __syncthreads();
+  const double2* S = sk + (static_cast<long long>(cur[sys]) * n_systems + sys) * nk;
+  double2* T = sk + (static_cast<long long>(1 - cur[sys]) * n_systems + sys) * nk;
+  double e = 0.0;
+#pragma unroll
+  for (int r = 0; r < kBatchKPerThread; ++r)
+  {
+    const int64_t k = (static_cast<int64_t>(blockIdx.x) * kBatchKPerThread + r) * blockDim.x + threadIdx.x;
+    if (k >= nk) continue;
+    const char4 kv = kvec[k];
+    const int ay = abs(kv.y), az = abs(kv.z);
+    const double sy = kv.y < 0 ? -1.0 : 1.0, sz = kv.z < 0 ? -1.0 : 1.0;
+    double2 d = make_double2(0.0, 0.0);
+    for (int a = 0; a < na; ++a)
+    {
+      const double2* t = tab + a * stride;
+      const double2 ex = t[kv.x], ey0 = t[kxm + 1 + ay], ez0 = t[kxm + 1 + kym + 1 + az];
+      const double2 ey = make_double2(ey0.x, sy * ey0.y), ez = make_double2(ez0.x, sz * ez0.y);
+      const double2 exy = make_double2(ex.x * ey.x - ex.y * ey.y, ex.x * ey.y + ex.y * ey.x);
+      const double w = wq[a];
+      d.x += w * (exy.x * ez.x - exy.y * ez.y);
+      d.y += w * (exy.x * ez.y + exy.y * ez.x);
+    }
+    const double2 s = __ldcs(S + k);
+    e += temp[k] * (2.0 * (s.x * d.x + s.y * d.y) + (d.x * d.x + d.y * d.y));
+    __stcs(T + k, make_double2(s.x + d.x, s.y + d.y));
+  }
+  // fixed-order reduction: warps, then the block, then (the system's last block) the blocks in order
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+  if (lane == 0) red[warp] = e;
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    double x = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) x += red[w];
+    partial[static_cast<long long>(sys) * gridDim.x + blockIdx.x] = x;
+    __threadfence();
+    last = atomicAdd(counter + sys, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double y = 0.0;
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) y += __ldcg(partial + static_cast<long long>(sys) * gridDim.x + b);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) y += __shfl_down_sync(0xffffffffu, y, o);
+  if (lane == 0) red[warp] = y;
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    double x = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) x += red[w];
+    result[sys] = x;
+    counter[sys] = 0u;  // ready for the next launch
+  }
+}
+}  // namespace
+
+extern "C"
+{
+rg_status rg_ewald_batch_create(rg_ewald* e, int n_systems, rg_ewald_batch** out)
+{
+  if (!e || !out || n_systems < 1 || n_systems > 65535) return RG_ERR_INVALID_ARGUMENT;
+  rg_ctx* ctx = e->ctx;
+  if (e->n_groups != 0)
+    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_ewald_batch_create: the batch carries no dU/dlambda groups");
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  rg_ewald_batch* b = new rg_ewald_batch();
+  b->ewald = e;
+  b->n = n_systems;
+  const int64_t nk = std::max<int64_t>(1, e->nk);
+  b->blocks = static_cast<int>((nk + kThreads * kBatchKPerThread - 1) / (kThreads * kBatchKPerThread));
+  cudaError_t err = cudaMalloc(reinterpret_cast<void**>(&b->sk), sizeof(double2) * 2 * n_systems * nk);
+  if (!err) err = cudaMemsetAsync(b->sk, 0, sizeof(double2) * 2 * n_systems * nk, ctx->stream);
+  if (!err) err = cudaMalloc(reinterpret_cast<void**>(&b->cur), n_systems);
+  if (!err) err = cudaMemsetAsync(b->cur, 0, n_systems, ctx->stream);
+  if (!err) err = cudaMalloc(reinterpret_cast<void**>(&b->atoms), sizeof(MovedAtom) * kBatchAtoms * n_systems);
+  if (!err) err = cudaMallocHost(reinterpret_cast<void**>(&b->atoms_host), sizeof(MovedAtom) * kBatchAtoms * n_systems);
+  if (!err) err = cudaMalloc(reinterpret_cast<void**>(&b->counts), sizeof(int) * n_systems);
+  if (!err) err = cudaMallocHost(reinterpret_cast<void**>(&b->counts_host), sizeof(int) * n_systems);
+  if (!err) err = cudaMalloc(reinterpret_cast<void**>(&b->partial), sizeof(double) * n_systems * b->blocks);
+  if (!err) err = cudaMalloc(reinterpret_cast<void**>(&b->counter), sizeof(unsigned int) * n_systems);
+  if (!err) err = cudaMemsetAsync(b->counter, 0, sizeof(unsigned int) * n_systems, ctx->stream);
+  if (!err) err = cudaHostAlloc(reinterpret_cast<void**>(&b->result_host), sizeof(double) * n_systems, cudaHostAllocMapped);
+  if (!err) err = cudaHostGetDevicePointer(reinterpret_cast<void**>(&b->result), b->result_host, 0);
+  if (!err) err = cudaStreamSynchronize(ctx->stream);
+  if (err)
+  {
+    rg_status st = rg::cudaFail(ctx, err, "rg_ewald_batch_create");
+    rg_ewald_batch_destroy(b);
+    return st;
+  }
+  b->cur_host.assign(n_systems, 0);
+  *out = b;
+  return RG_OK;
+}
+
+rg_status rg_ewald_batch_destroy(rg_ewald_batch* b)
+{
+  if (!b) return RG_OK;
+  if (b->ewald && b->ewald->ctx) cudaStreamSynchronize(b->ewald->ctx->stream);
+  cudaFree(b->sk);
+  cudaFree(b->cur);
+  cudaFree(b->atoms);
+  cudaFree(b->counts);
+  cudaFree(b->partial);
+  cudaFree(b->counter);
+  if (b->atoms_host) cudaFreeHost(b->atoms_host);
+  if (b->counts_host) cudaFreeHost(b->counts_host);
+  if (b->result_host) cudaFreeHost(b->result_host);
+  delete b;
+  return RG_OK;
+}
+
+rg_status rg_ewald_batch_set(rg_ewald_batch* b, int system, const double* sk)
+{
+  if (!b || system < 0 || system >= b->n) return RG_ERR_INVALID_ARGUMENT;
+  rg_ewald* e = b->ewald;
+  rg_ctx* ctx = e->ctx;
+  if (e->nk == 0) return RG_OK;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  double2* dst = b->sk + (static_cast<long long>(b->cur_host[system]) * b->n + system) * e->nk;
+  if (sk)
+  {
+    for (int64_t i = 0; i < 2 * e->nk; ++i)
+      if (!std::isfinite(sk[i])) return rg::fail(ctx, RG_ERR_NONFINITE, "rg_ewald_batch_set: NaN or infinite S(k)");
+    RG_CUDA(ctx, cudaMemcpyAsync(dst, sk, sizeof(double2) * e->nk, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  else  // the Ewald state's stored total structure factor (entry 0 of each k)
+    RG_CUDA(ctx, cudaMemcpy2DAsync(dst, sizeof(double2), e->stored, sizeof(double2) * (1 + e->n_groups),
+                                   sizeof(double2), e->nk, cudaMemcpyDeviceToDevice, ctx->stream));
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
+}
+
+rg_status rg_ewald_batch_get(rg_ewald_batch* b, int system, int which, double* sk)
+{
+  if (!b || !sk || system < 0 || system >= b->n || (which != 0 && which != 1)) return RG_ERR_INVALID_ARGUMENT;
+  rg_ewald* e = b->ewald;
+  rg_ctx* ctx = e->ctx;
+  if (e->nk == 0) return RG_OK;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int buf = which == 0 ? b->cur_host[system] : 1 - b->cur_host[system];
+  RG_CUDA(ctx, cudaMemcpyAsync(sk, b->sk + (static_cast<long long>(buf) * b->n + system) * e->nk,
+                               sizeof(double2) * e->nk, cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
+}
+
+rg_status rg_ewald_batch_delta(rg_ewald_batch* b, const rg_atom* atoms, int max_atoms, const int32_t* n_new,
+                               const int32_t* n_old, double* delta_fourier)
+{
+  if (!b || !atoms || !n_new || !n_old || !delta_fourier || max_atoms < 1) return RG_ERR_INVALID_ARGUMENT;
+  rg_ewald* e = b->ewald;
+  rg_ctx* ctx = e->ctx;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  // the staging buffers are free: every call ends by synchronising the stream; system s's atoms are packed at
+  // s * stride (stride = max_atoms, at most kBatchAtoms)
+  const int stride = std::min(max_atoms, kBatchAtoms);
+  for (int s = 0; s < b->n; ++s)
+  {
+    if (n_new[s] < 0 || n_old[s] < 0 || n_new[s] + n_old[s] > std::min(max_atoms, kBatchAtoms))
+      return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_ewald_batch_delta: at most 16 old + new atoms per system");
+    const rg_atom* a = atoms + static_cast<long long>(s) * max_atoms;
+    if (rg_status fs = rg::checkFinite(ctx, a, n_new[s] + n_old[s], "rg_ewald_batch_delta")) return fs;
+    // new atoms with +q, then old atoms with -q (packMoved takes the old ones first)
+    packMoved(e, a + n_new[s], n_old[s], a, n_new[s], -1.0, b->atoms_host + static_cast<long long>(s) * stride);
+    b->counts_host[s] = e->use_charge ? n_new[s] + n_old[s] : 0;
+  }
+  if (e->nk == 0 || !e->use_charge)
+  {
+    for (int s = 0; s < b->n; ++s) delta_fourier[s] = 0.0;
+    return RG_OK;
+  }
+  RG_CUDA(ctx, cudaMemcpyAsync(b->atoms, b->atoms_host, sizeof(MovedAtom) * stride * b->n, cudaMemcpyHostToDevice,
+                               ctx->stream));
+  RG_CUDA(ctx, cudaMemcpyAsync(b->counts, b->counts_host, sizeof(int) * b->n, cudaMemcpyHostToDevice, ctx->stream));
+  const int kxm = e->ff.kmax_x, kym = e->ff.kmax_y, kzm = e->ff.kmax_z;
+  const size_t shmem = sizeof(double2) * kBatchAtoms * ((kxm + 1) + (kym + 1) + (kzm + 1));
+  dim3 grid(b->blocks, b->n);
+  ewaldBatchDeltaKernel<<<grid, kThreads, shmem, ctx->stream>>>(e->nk, b->n, e->kvec, e->temp, b->sk, b->cur, b->atoms,
+                                                               stride, b->counts, kxm, kym, kzm, b->partial,
+                                                               b->counter, b->result);
+  RG_CUDA(ctx, cudaGetLastError());
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  std::memcpy(delta_fourier, b->result_host, sizeof(double) * b->n);
+  return RG_OK;
+}
+
+rg_status rg_ewald_batch_accept(rg_ewald_batch* b, const uint8_t* accept)
+{
+  if (!b || !accept) return RG_ERR_INVALID_ARGUMENT;
+  rg_ctx* ctx = b->ewald->ctx;
+  bool any = false;
+  for (int s = 0; s < b->n; ++s)
+    if (accept[s])
+    {
+      b->cur_host[s] ^= 1;
+      any = true;
+    }
+  if (!any) return RG_OK;
+  RG_CUDA(ctx, cudaSetDevice(ctx->device));
+  RG_CUDA(ctx, cudaMemcpyAsync(b->cur, b->cur_host.data(), b->n, cudaMemcpyHostToDevice, ctx->stream));
+  RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return RG_OK;
+}
+}  // extern "C"

@@ -589,6 +589,364 @@ __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1
   }
 }
 
+// ---------------------------------------------------------------------------------------------------------------------
+// FP32C rectangular grids with packed FP32 arithmetic (sm_100a f32x2 FMA / multiply / add).
+//
+// Each thread owns two grid points of its brick column, four planes apart along z: (i, j, k) and (i, j, k + 2) in a
+// brick of 8 x 8 x 4 points (128 threads). The two points share dx and dy to every staged image, and every operation
+// after dz is one packed instruction for both pairs; the reciprocal, reciprocal square root and base-2 exponential
+// stay scalar. A lane whose pair is outside the cutoff is masked by zeroing its parameters (its factors are then 0).
+// FP32 partial sums per staged chunk are added into FP64 sums kept in shared memory. The unit-charge Ewald grid keeps
+// the near-image list of gridKernel: images within kNearRadius + R of the brick centre, energy in FP64.
+// ---------------------------------------------------------------------------------------------------------------------
+constexpr int kPackThreads = 128;
+constexpr int kPackPer = 4;
+constexpr int kPackChunk = kPackThreads * kPackPer;
+
+__device__ __forceinline__ float2 bc(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+struct Factor2
+{
+  float2 e, f1, f2, f3;
+};
+
+// ewaldFactor<float> for two pairs; cq is zero on a masked lane
+__device__ __forceinline__ Factor2 ewaldFactor2(float2 rr, float2 cq, float alpha)
+{
+  const float2 invr = make_float2(rgd::rsqrtApprox(rr.x), rgd::rsqrtApprox(rr.y));
+  const float2 r = mul2(rr, invr);
+  const float2 ar2 = mul2(rr, bc(alpha * alpha));
+  const float2 g = mul2(ar2, bc(-1.4426950408889634f));
+  float2 ex;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(ex.x) : "f"(g.x));
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(ex.y) : "f"(g.y));
+  const float2 x = mul2(r, bc(alpha));
+  const float2 tden = fma2(x, bc(0.5f), bc(1.0f));
+  const float2 t = make_float2(rgd::rcpApprox(tden.x), rgd::rcpApprox(tden.y));
+  // rgd::erfcFromExp's polynomial in t, packed
+  float2 R = bc(-0.02496027760207653f);
+  R = fma2(R, t, bc(0.09420006722211838f));
+  R = fma2(R, t, bc(-0.024484887719154358f));
+  R = fma2(R, t, bc(-0.36430737376213074f));
+  R = fma2(R, t, bc(0.534475564956665f));
+  R = fma2(R, t, bc(-0.11705945432186127f));
+  R = fma2(R, t, bc(0.3620023727416992f));
+  R = fma2(R, t, bc(0.25453805923461914f));
+  R = fma2(R, t, bc(0.2858136296272278f));
+  R = fma2(R, t, bc(-0.00021772264153696597f));
+  const float2 ec = mul2(ex, R);
+  const float2 etr = mul2(mul2(x, ex), bc(1.1283791670955126f));  // 2 alpha r exp(-alpha^2 r^2) / sqrt(pi)
+  const float2 invrr = mul2(invr, invr);
+  const float2 i3 = mul2(invr, invrr);
+  const float2 i5 = mul2(i3, invrr);
+  const float2 i7 = mul2(i5, invrr);
+  const float2 ncq = mul2(cq, bc(-1.0f));
+  Factor2 f;
+  f.e = mul2(mul2(cq, ec), invr);
+  f.f1 = mul2(mul2(ncq, add2(etr, ec)), i3);
+  f.f2 = mul2(mul2(cq, fma2(etr, fma2(ar2, bc(2.0f), bc(3.0f)), mul2(ec, bc(3.0f)))), i5);
+  f.f3 = mul2(mul2(ncq, fma2(etr, fma2(fma2(ar2, bc(4.0f), bc(10.0f)), ar2, bc(15.0f)), mul2(ec, bc(15.0f)))), i7);
+  return f;
+}
+
+// ljFactor for two pairs from the shared reciprocals; a1 and shift are zero on a masked lane
+template <int TYPE>
+__device__ __forceinline__ Factor2 ljFactor2(float2 inv, float2 inv2, float2 inv3, float2 a1, float s2, float2 shift)
+{
+  const float2 q = mul2(inv, bc(s2));
+  const float2 t3 = mul2(mul2(q, q), q);
+  Factor2 f;
+  if constexpr (TYPE == RG_GRID_LENNARD_JONES_REPULSION)
+  {
+    const float2 B = mul2(mul2(a1, t3), t3);
+    f.e = B;
+    f.f1 = mul2(mul2(B, bc(-12.0f)), inv);
+    f.f2 = mul2(mul2(B, bc(168.0f)), inv2);
+    f.f3 = mul2(mul2(B, bc(-2688.0f)), inv3);
+  }
+  else if constexpr (TYPE == RG_GRID_LENNARD_JONES_ATTRACTION)
+  {
+    const float2 A = mul2(a1, t3);
+    f.e = A;
+    f.f1 = mul2(mul2(A, bc(-6.0f)), inv);
+    f.f2 = mul2(mul2(A, bc(48.0f)), inv2);
+    f.f3 = mul2(mul2(A, bc(-480.0f)), inv3);
+  }
+  else
+  {
+    const float2 A = mul2(a1, t3);
+    const float2 B = mul2(A, t3);
+    f.e = add2(fma2(A, bc(-1.0f), B), mul2(shift, bc(-1.0f)));
+    f.f1 = mul2(fma2(A, bc(6.0f), mul2(B, bc(-12.0f))), inv);
+    f.f2 = mul2(fma2(B, bc(168.0f), mul2(A, bc(-48.0f))), inv2);
+    f.f3 = mul2(fma2(A, bc(480.0f), mul2(B, bc(-2688.0f))), inv3);
+  }
+  return f;
+}
+
+// the 8 rectangular channels of both points: E, dx f1, dy f1, dz f1, f2 dx dy, f2 dx dz, f2 dy dz, f3 dx dy dz
+template <bool ENERGY>
+__device__ __forceinline__ void addPair2(float2 (&P)[8], const Factor2& f, float dx, float dy, float2 dz)
+{
+  if constexpr (ENERGY) P[0] = add2(P[0], f.e);
+  P[1] = fma2(bc(dx), f.f1, P[1]);
+  P[2] = fma2(bc(dy), f.f1, P[2]);
+  P[3] = fma2(dz, f.f1, P[3]);
+  const float dxy = dx * dy;
+  P[4] = fma2(bc(dxy), f.f2, P[4]);
+  P[5] = fma2(mul2(bc(dx), dz), f.f2, P[5]);
+  P[6] = fma2(mul2(bc(dy), dz), f.f2, P[6]);
+  P[7] = fma2(mul2(bc(dxy), dz), f.f3, P[7]);
+}
+
+// FP64 energy of a near image: C q erfc(alpha r) / r as C q (1/r - alpha erf(x)/x), x = alpha r, or erfc directly
+// beyond the polynomial's range (coarse grids only)
+__device__ __forceinline__ double nearEwaldEnergy(double rr, double cq, double alpha)
+{
+  const double u = alpha * alpha * rr;
+  if (u <= rgd::kErfOverXMax * rgd::kErfOverXMax) return cq * (rsqrt(rr) - alpha * rgd::erfOverX(u));
+  const double r = sqrt(rr);
+  return cq * erfc(alpha * r) / r;
+}
+
+template <int TYPE, int NP, bool COUNT>
+__global__ void __launch_bounds__(kPackThreads, 4) gridKernelPacked(GridParams p, const double4* __restrict__ ipos,
+                                                                   const double4* __restrict__ ipar)
+{
+  constexpr bool EWALD = (TYPE == RG_GRID_EWALD_REAL);
+  constexpr int kSlots = NP * 8 * 2;  // FP64 sums: [probe][channel][point]
+  extern __shared__ unsigned char smem_raw[];
+  float4* cpos = reinterpret_cast<float4*>(smem_raw);
+  float4* cpar = cpos + kPackChunk;                              // Lennard-Jones: NP parameter lists
+  double4* npos = reinterpret_cast<double4*>(cpos + kPackChunk);  // Ewald: near list
+  double* sums = reinterpret_cast<double*>(smem_raw + sizeof(float4) * kPackChunk *
+                                                         (EWALD ? 3 : 1 + NP));  // [slot][thread]
+  __shared__ int warp_sums[33];
+
+  const int tid = threadIdx.x;
+  const int lx = tid & 7, ly = (tid >> 3) & 7, lz = tid >> 6;
+  const int kb = static_cast<int>(blockIdx.z) + p.zb0;
+  const int i = blockIdx.x * 8 + lx, j = blockIdx.y * 8 + ly;
+  const int k0 = kb * 4 + lz, k1 = k0 + 2;
+  const bool valid0 = i < p.nx && j < p.ny && k0 < p.nz;
+  const bool valid1 = i < p.nx && j < p.ny && k1 < p.nz;
+
+  // the points and the brick centre (rectangular: the cell diagonal), relative offsets computed in FP64
+  const double cx = p.cell[0][0], cy = p.cell[1][1], cz = p.cell[2][2];
+  const double ctr[3] = {(blockIdx.x * 8 + 3.5) * p.delta[0] * cx, (blockIdx.y * 8 + 3.5) * p.delta[1] * cy,
+                         (kb * 4 + 1.5) * p.delta[2] * cz};
+  const double qx = i * p.delta[0] * cx - ctr[0], qy = j * p.delta[1] * cy - ctr[1];
+  const double qz0 = k0 * p.delta[2] * cz - ctr[2], qz1 = k1 * p.delta[2] * cz - ctr[2];
+  const float px = static_cast<float>(qx), py = static_cast<float>(qy);
+  const float2 pz = make_float2(static_cast<float>(qz0), static_cast<float>(qz1));
+  const float rc2 = static_cast<float>(p.rc2);
+  const float alpha = static_cast<float>(p.alpha);
+
+#pragma unroll
+  for (int s = 0; s < kSlots; ++s) sums[s * kPackThreads + tid] = 0.0;
+  unsigned long long npairs = 0;
+
+  for (int base = 0; base < p.n_images; base += kPackChunk)
+  {
+    double4 ip[kPackPer];
+    bool ok[kPackPer], nr[kPackPer];
+    int cnt = 0;
+#pragma unroll
+    for (int r = 0; r < kPackPer; ++r)
+    {
+      const int idx = base + tid * kPackPer + r;
+      ok[r] = nr[r] = false;
+      if (idx < p.n_images)
+      {
+        ip[r] = ipos[idx];
+        const double dx = ip[r].x - ctr[0], dy = ip[r].y - ctr[1], dz = ip[r].z - ctr[2];
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        const bool in = d2 < p.filter2;
+        nr[r] = EWALD && in && d2 < p.near2;
+        ok[r] = in && !nr[r];
+        cnt += ok[r] ? 1 : (nr[r] ? (1 << 16) : 0);
+      }
+    }
+    int total;
+    int off = blockExclusiveScan(cnt, warp_sums, &total);
+    int offn = off >> 16;
+    off &= 0xffff;
+    const int total_near = total >> 16;
+    total &= 0xffff;
+#pragma unroll
+    for (int r = 0; r < kPackPer; ++r)
+    {
+      const double rx = ip[r].x - ctr[0], ry = ip[r].y - ctr[1], rz = ip[r].z - ctr[2];
+      if (EWALD && nr[r]) npos[offn++] = make_double4(rx, ry, rz, ip[r].w);
+      if (ok[r])
+      {
+        cpos[off] = make_float4(static_cast<float>(rx), static_cast<float>(ry), static_cast<float>(rz),
+                                static_cast<float>(ip[r].w));
+        if constexpr (!EWALD)
+        {
+          const long long idx = base + tid * kPackPer + r;
+#pragma unroll
+          for (int q = 0; q < NP; ++q)
+          {
+            const double4 pq = ipar[idx * NP + q];
+            cpar[q * kPackChunk + off] =
+                make_float4(static_cast<float>(pq.x), static_cast<float>(pq.y), static_cast<float>(pq.z), 0.0f);
+          }
+        }
+        ++off;
+      }
+    }
+    __syncthreads();
+
+    float2 P[NP][8];
+#pragma unroll
+    for (int q = 0; q < NP; ++q)
+#pragma unroll
+      for (int ch = 0; ch < 8; ++ch) P[q][ch] = bc(0.0f);
+#pragma unroll 2
+    for (int c = 0; c < total; ++c)
+    {
+      const float4 a = cpos[c];
+      const float dx = px - a.x, dy = py - a.y;
+      const float2 dz = add2(pz, bc(-a.z));
+      float2 rr = fma2(dz, dz, bc(fmaf(dx, dx, dy * dy)));
+      rr.x = fmaxf(rr.x, 0.1f);
+      rr.y = fmaxf(rr.y, 0.1f);
+      const bool in0 = rr.x < rc2, in1 = rr.y < rc2;
+      if (in0 || in1)
+      {
+        if (COUNT) npairs += (in0 && valid0 ? 1 : 0) + (in1 && valid1 ? 1 : 0);
+        if constexpr (EWALD)
+        {
+          const Factor2 f = ewaldFactor2(rr, make_float2(in0 ? a.w : 0.0f, in1 ? a.w : 0.0f), alpha);
+          addPair2<true>(P[0], f, dx, dy, dz);
+        }
+        else
+        {
+          const float2 inv = make_float2(rgd::rcpApprox(rr.x), rgd::rcpApprox(rr.y));
+          const float2 inv2 = mul2(inv, inv);
+          const float2 inv3 = mul2(inv2, inv);
+#pragma unroll
+          for (int q = 0; q < NP; ++q)
+          {
+            const float4 pq = cpar[q * kPackChunk + c];
+            const Factor2 f = ljFactor2<TYPE>(inv, inv2, inv3, make_float2(in0 ? pq.x : 0.0f, in1 ? pq.x : 0.0f),
+                                              pq.y, make_float2(in0 ? pq.z : 0.0f, in1 ? pq.z : 0.0f));
+            addPair2<true>(P[q], f, dx, dy, dz);
+          }
+        }
+      }
+    }
+    double ne0 = 0.0, ne1 = 0.0;
+    if constexpr (EWALD)
+    {
+      // near images: energy in FP64 from FP64 offsets, derivative channels packed in FP32 from the exact
+      // displacement rounded once
+      for (int c = 0; c < total_near; ++c)
+      {
+        const double4 a = npos[c];
+        const double dx = qx - a.x, dy = qy - a.y, dz0 = qz0 - a.z, dz1 = qz1 - a.z;
+        const double dxy = dx * dx + dy * dy;
+        const double rr0 = fmax(dxy + dz0 * dz0, 0.1), rr1 = fmax(dxy + dz1 * dz1, 0.1);
+        const bool in0 = rr0 < p.rc2, in1 = rr1 < p.rc2;
+        if (in0 || in1)
+        {
+          if (COUNT) npairs += (in0 && valid0 ? 1 : 0) + (in1 && valid1 ? 1 : 0);
+          if (in0) ne0 += nearEwaldEnergy(rr0, a.w, p.alpha);
+          if (in1) ne1 += nearEwaldEnergy(rr1, a.w, p.alpha);
+          const float cq = static_cast<float>(a.w);
+          const Factor2 f = ewaldFactor2(make_float2(static_cast<float>(rr0), static_cast<float>(rr1)),
+                                         make_float2(in0 ? cq : 0.0f, in1 ? cq : 0.0f), alpha);
+          addPair2<false>(P[0], f, static_cast<float>(dx), static_cast<float>(dy),
+                          make_float2(static_cast<float>(dz0), static_cast<float>(dz1)));
+        }
+      }
+    }
+    // the chunk's FP32 partial sums into the FP64 sums
+#pragma unroll
+    for (int q = 0; q < NP; ++q)
+#pragma unroll
+      for (int ch = 0; ch < 8; ++ch)
+      {
+        const int s = (q * 8 + ch) * 2;
+        double e0 = static_cast<double>(P[q][ch].x), e1 = static_cast<double>(P[q][ch].y);
+        if (EWALD && ch == 0)
+        {
+          e0 += ne0;
+          e1 += ne1;
+        }
+        sums[s * kPackThreads + tid] += e0;
+        sums[(s + 1) * kPackThreads + tid] += e1;
+      }
+    __syncthreads();
+  }
+
+  if (COUNT)
+  {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) npairs += __shfl_down_sync(0xffffffffu, npairs, o);
+    if ((tid & 31) == 0 && npairs) atomicAdd(p.pair_count, npairs);
+  }
+#pragma unroll
+  for (int q = 0; q < NP; ++q)
+#pragma unroll
+    for (int pt = 0; pt < 2; ++pt)
+    {
+      if (!(pt == 0 ? valid0 : valid1)) continue;
+      const int k = pt == 0 ? k0 : k1;
+      double v[8];
+#pragma unroll
+      for (int ch = 0; ch < 8; ++ch) v[ch] = sums[((q * 8 + ch) * 2 + pt) * kPackThreads + tid];
+      // rectangular scaling by the cell diagonal and division by the cell counts (framework_molecule_grid.cpp:236-243,
+      // interpolation_energy_grid.cpp:3847-3856), then the overlap clamp (:3858-3874)
+      v[1] *= cx / p.ncells[0];
+      v[2] *= cy / p.ncells[1];
+      v[3] *= cz / p.ncells[2];
+      v[4] *= cx * cy / (p.ncells[0] * p.ncells[1]);
+      v[5] *= cx * cz / (p.ncells[0] * p.ncells[2]);
+      v[6] *= cy * cz / (p.ncells[1] * p.ncells[2]);
+      v[7] *= cx * cy * cz / (p.ncells[0] * p.ncells[1] * p.ncells[2]);
+      const double oc = p.overlap;
+      if (v[0] > oc)
+      {
+        v[0] = 2.0 * oc;
+        v[1] = fmin(fmax(v[1], -oc), oc);
+        v[2] = fmin(fmax(v[2], -oc), oc);
+        v[3] = fmin(fmax(v[3], -oc), oc);
+        v[4] = v[5] = v[6] = v[7] = 0.0;
+      }
+      double2* dst = reinterpret_cast<double2*>(
+          p.out[q] + 8 * (static_cast<long long>(i) +
+                          static_cast<long long>(p.nx) * (static_cast<long long>(j) + static_cast<long long>(p.ny) * k)));
+      dst[0] = make_double2(v[0], v[1]);
+      dst[1] = make_double2(v[2], v[3]);
+      dst[2] = make_double2(v[4], v[5]);
+      dst[3] = make_double2(v[6], v[7]);
+    }
+}
+
+template <int TYPE, int NP>
+size_t packedSharedBytes()
+{
+  constexpr bool EWALD = TYPE == RG_GRID_EWALD_REAL;
+  return sizeof(float4) * kPackChunk * (EWALD ? 3 : 1 + NP) + sizeof(double) * NP * 16 * kPackThreads;
+}
+
+template <int TYPE, int NP, bool COUNT>
+cudaError_t launchPacked(const GridParams& p, const double4* ipos, const double4* ipar, cudaStream_t stream)
+{
+  const int zbricks = p.zb1 > p.zb0 ? p.zb1 - p.zb0 : (p.nz + 3) / 4;
+  dim3 grid((p.nx + 7) / 8, (p.ny + 7) / 8, zbricks);
+  const size_t shmem = packedSharedBytes<TYPE, NP>();
+  auto kern = gridKernelPacked<TYPE, NP, COUNT>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(shmem));
+  kern<<<grid, kPackThreads, shmem, stream>>>(p, ipos, ipar);
+  return cudaGetLastError();
+}
+
 // Dynamic shared memory of a launch: the FP32/FP64 candidate list, NP parameter lists for Lennard-Jones grids, and the
 // FP64 near list of the FP32C Ewald grid.
 template <typename Real, int TYPE, int NP>
@@ -619,6 +977,13 @@ template <typename Real, int TYPE, bool TRI, int NP = 1>
 cudaError_t launchTyped(const GridParams& p, const double4* ipos, const double4* ipar, int bx, int by, int bz,
                         bool count, bool clip, cudaStream_t stream)
 {
+  // FP32C rectangular grids (cell diagonal only) without a supercell clip: the packed two-point kernel (bricks of
+  // 8 x 8 x 4 points)
+  if constexpr (sizeof(Real) == 4 && !TRI)
+    if (!clip && bx == 8 && by == 8 && bz == 4 && p.cell[0][1] == 0.0 && p.cell[0][2] == 0.0 && p.cell[1][0] == 0.0 &&
+        p.cell[1][2] == 0.0 && p.cell[2][0] == 0.0 && p.cell[2][1] == 0.0)
+      return count ? launchPacked<TYPE, NP, true>(p, ipos, ipar, stream)
+                   : launchPacked<TYPE, NP, false>(p, ipos, ipar, stream);
   if (clip)
     return count ? launchKernel<Real, TYPE, TRI, NP, true, true>(p, ipos, ipar, bx, by, bz, stream)
                  : launchKernel<Real, TYPE, TRI, NP, false, true>(p, ipos, ipar, bx, by, bz, stream);

@@ -44,7 +44,8 @@ constexpr int kMaxTrials = 12;
 constexpr int kMaxItems = 96;          // trial atoms of one phase
 constexpr int kMaxCand = kMaxTrials;   // Ewald candidates of one phase
 constexpr int kMaxCandAtoms = 2 * kMaxAtoms;
-constexpr int kMaxKPerCta = 64;
+constexpr int kMaxKPerCta = 384;  // k-vectors of one CTA's range (in dynamic shared memory)
+constexpr int kMaxSystems = 8;    // independent systems of one launch (rg_mixture_run_many)
 constexpr int kMaxTypes = 16;
 constexpr int kRow = kMaxItems + kMaxCand + 4;  // columns of partial sums per CTA (last 4: overlap-bit words)
 constexpr int kMaxBlocks = 256;                 // CTAs of the cooperative launch (lanes x 8 in the column sums)
@@ -110,9 +111,11 @@ struct Params
   double2* sk;     // [nk]
   int km[3];       // kmax per axis: the phasor tables hold exp(2 pi i j s) for j = 0..km[d]
   int tabK;        // table stride: max(km) + 1
-  double* part;    // [2][kRow][gridDim]: partial sums, column-major, two buffers alternating by phase
+  double* part;    // [2][kRow][group]: partial sums, column-major, two buffers alternating by phase
   unsigned long long* bar;  // [0] barrier arrivals in this launch (zeroed before each launch), [1] error flag
   int record;
+  int group;                // CTAs of this system in the launch; the system's CTA index is blockIdx.x % group
+  int kpc;                  // k-vectors per CTA (the stride of the per-CTA k arrays in dynamic shared memory)
   long long spin_limit;     // polls before a barrier wait gives up (kSpinLimit; shorter only in the wait test)
   int absent_cta;           // wait test: this CTA does not arrive at the first barrier of a launch (-1: none)
 };
@@ -141,14 +144,7 @@ struct Shared
   double cq[kMaxCand][kMaxCandAtoms];
   int cn[kMaxCand];
   int ncand;
-  double2 dk[kMaxCand][kMaxKPerCta];  // structure-factor change of each candidate over this CTA's k-range
-  double ek[kMaxCand][kMaxKPerCta];   // its energy change per k
   double fwE[kMaxItems];              // framework (grid) energy of the trial atoms this CTA owns
-  // this CTA's k-range for the whole launch: k-vectors, prefactors and its S(k) (only this CTA updates them; written
-  // back to global memory at the end of the launch)
-  char4 kv[kMaxKPerCta];
-  double kt[kMaxKPerCta];
-  double2 ks[kMaxKPerCta];
   double red[kThreads];
   unsigned ovl_bits[4];
   double tot[kMaxItems + kMaxCand];  // totals over the grid
@@ -229,7 +225,7 @@ __device__ __forceinline__ unsigned long long addRelease(unsigned long long* a, 
 }
 
 // Grid barrier over all CTAs of the cooperative launch: a monotonic arrival counter (zeroed before each launch); the
-// n-th barrier of the launch is passed once the counter reaches n x gridDim. One release add per CTA, then acquire
+// n-th barrier of the launch is passed once the counter reaches n x group (the system's CTAs). One release add per CTA, then acquire
 // polls: no reset, no second round trip. Spin-waits are bounded: on timeout the error flag is raised and false
 // returned, and every CTA leaves the kernel; a CTA waiting on a barrier that a failed CTA will never reach sees the
 // flag (polled every 64 spins) and leaves too.
@@ -238,9 +234,9 @@ __device__ bool gridBarrier(const Params& p, Shared& sh)
   __syncthreads();
   if (threadIdx.x == 0)
   {
-    const unsigned long long target = static_cast<unsigned long long>(sh.gen + 1) * gridDim.x;
+    const unsigned long long target = static_cast<unsigned long long>(sh.gen + 1) * p.group;
     // the wait test leaves one arrival out of the first barrier, so that every CTA's bounded wait runs out
-    const bool absent = static_cast<int>(blockIdx.x) == p.absent_cta && sh.gen == 0;
+    const bool absent = static_cast<int>(blockIdx.x) % p.group == p.absent_cta && sh.gen == 0;
     unsigned long long v = absent ? loadAcquire(&p.bar[0]) : addRelease(&p.bar[0], 1ull) + 1ull;
     long long spins = 0;
     while (v < target)
@@ -273,14 +269,25 @@ struct Dyn
   int4* slice;  // [kSlice]
   int4* fws;    // [kFwSlice]
   float* fwq;   // [kFwSlice]
+  // this CTA's k-range for the whole launch: S(k) (only this CTA updates it; written back at the end of the launch),
+  // the structure-factor change and energy change of each candidate, the k-vectors and prefactors
+  double2* ks;  // [kpc]
+  double2* dk;  // [kMaxCand][kpc]
+  double* ek;   // [kMaxCand][kpc]
+  double* kt;   // [kpc]
+  char4* kv;    // [kpc]
 };
 __host__ __device__ constexpr size_t phasorBytes(int tabK)
 {
   return sizeof(double2) * kMaxCand * kMaxCandAtoms * 3 * static_cast<size_t>(tabK);
 }
-__host__ __device__ constexpr size_t dynBytes(int tabK)
+__host__ __device__ constexpr size_t kRangeBytes(int kpc)
 {
-  return phasorBytes(tabK) + sizeof(int4) * (kSlice + kFwSlice) + sizeof(float) * kFwSlice;
+  return static_cast<size_t>(kpc) * (sizeof(double2) * (1 + kMaxCand) + sizeof(double) * (1 + kMaxCand) + sizeof(char4));
+}
+__host__ __device__ constexpr size_t dynBytes(int tabK, int kpc)
+{
+  return phasorBytes(tabK) + sizeof(int4) * (kSlice + kFwSlice) + sizeof(float) * kFwSlice + kRangeBytes(kpc);
 }
 __device__ __forceinline__ Dyn dynOf(const Params& p)
 {
@@ -290,6 +297,11 @@ __device__ __forceinline__ Dyn dynOf(const Params& p)
   d.slice = reinterpret_cast<int4*>(dynSmem + phasorBytes(p.tabK));
   d.fws = d.slice + kSlice;
   d.fwq = reinterpret_cast<float*>(d.fws + kFwSlice);
+  d.ks = reinterpret_cast<double2*>(d.fwq + kFwSlice);
+  d.dk = d.ks + p.kpc;
+  d.ek = reinterpret_cast<double*>(d.dk + kMaxCand * p.kpc);
+  d.kt = d.ek + kMaxCand * p.kpc;
+  d.kv = reinterpret_cast<char4*>(d.kt + p.kpc);
   return d;
 }
 
@@ -339,7 +351,7 @@ __device__ __forceinline__ void pairTerm(const Params& p, const Shared& sh, int4
 __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const* atomGrid)
 {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int G = gridDim.x, cta = blockIdx.x;
+  const int G = p.group, cta = static_cast<int>(blockIdx.x) % p.group;
   const int nta = sh.nta, ncand = sh.ncand;
   const int ns = sh.n * p.na;
   const int chunk = (ns + G - 1) / G, s0 = min(ns, cta * chunk), s1 = min(ns, s0 + chunk);
@@ -459,7 +471,7 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
     for (int task = tid; task < ncand * nkr; task += kThreads)
     {
       const int c = task / nkr, kk = task - c * nkr;
-      const char4 kv = sh.kv[kk];
+      const char4 kv = dy.kv[kk];
       double2 d = make_double2(0.0, 0.0);
       for (int a = 0; a < sh.cn[c]; ++a)
       {
@@ -473,15 +485,15 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
         d.x += q * (exy.x * ez.x - exy.y * ez.y);
         d.y += q * (exy.x * ez.y + exy.y * ez.x);
       }
-      const double2 sk = sh.ks[kk];
-      sh.ek[c][kk] = sh.kt[kk] * (2.0 * (sk.x * d.x + sk.y * d.y) + (d.x * d.x + d.y * d.y));
-      sh.dk[c][kk] = d;
+      const double2 sk = dy.ks[kk];
+      dy.ek[c * p.kpc + kk] = dy.kt[kk] * (2.0 * (sk.x * d.x + sk.y * d.y) + (d.x * d.x + d.y * d.y));
+      dy.dk[c * p.kpc + kk] = d;
     }
     __syncthreads();
     for (int c = warp; c < ncand; c += kWarps)
     {
       double e = 0.0;
-      for (int kk = lane; kk < nkr; kk += 32) e += sh.ek[c][kk];
+      for (int kk = lane; kk < nkr; kk += 32) e += dy.ek[c * p.kpc + kk];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
       if (lane == 0) cols[static_cast<long long>(kMaxItems + c) * G + cta] = e;
@@ -694,8 +706,17 @@ __device__ void storeOrientation(const Params& p, Shared& sh, const double** ato
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves)
+// The parameters of the systems of one launch: CTAs [s * group, (s + 1) * group) run system s.
+struct Launch
 {
+  Params p[kMaxSystems];
+};
+static_assert(sizeof(Launch) <= 32000, "kernel parameter space");
+
+__global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_constant__ Launch L, int moves)
+{
+  const Params& p = L.p[blockIdx.x / L.p[0].group];
+  const int cta = static_cast<int>(blockIdx.x) % p.group;
   __shared__ Shared sh;
   const int tid = threadIdx.x;
   const int na = p.na;
@@ -712,20 +733,21 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
     for (int k = 0; k < kStats; ++k) sh.stats[k] = p.stats[k];
   }
   // this CTA's k-range
-  const int G = gridDim.x;
-  const int kchunk = (p.nk + G - 1) / G, k0 = blockIdx.x * kchunk, k1 = min(p.nk, k0 + kchunk);
+  const int G = p.group;
+  const int kchunk = (p.nk + G - 1) / G, k0 = cta * kchunk, k1 = min(p.nk, k0 + kchunk);
   const long long move0 = *p.move_base;
   __shared__ const double* atomGrid[kMaxItems];
+  const Dyn dyk = dynOf(p);
   // this CTA's k-range and framework slice, kept in shared memory for the whole launch
   for (int kk = tid; kk < k1 - k0; kk += kThreads)
   {
-    sh.kv[kk] = p.kvec[k0 + kk];
-    sh.kt[kk] = p.temp[k0 + kk];
-    sh.ks[kk] = p.sk[k0 + kk];
+    dyk.kv[kk] = p.kvec[k0 + kk];
+    dyk.kt[kk] = p.temp[k0 + kk];
+    dyk.ks[kk] = p.sk[k0 + kk];
   }
   if (p.n_fw > 0)
   {
-    const int fchunk = (p.n_fw + G - 1) / G, fa = min(p.n_fw, static_cast<int>(blockIdx.x) * fchunk);
+    const int fchunk = (p.n_fw + G - 1) / G, fa = min(p.n_fw, cta * fchunk);
     const int nf = min(min(p.n_fw, fa + fchunk) - fa, kFwSlice);
     const Dyn dy = dynOf(p);
     for (int i = tid; i < nf; i += kThreads)
@@ -849,9 +871,9 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
         if (p.use_charge)
           for (int kk = tid; kk < k1 - k0; kk += kThreads)
           {
-            const double2 d = sh.dk[0][kk];
-            sh.ks[kk].x += d.x;
-            sh.ks[kk].y += d.y;
+            const double2 d = dyk.dk[kk];
+            dyk.ks[kk].x += d.x;
+            dyk.ks[kk].y += d.y;
           }
       }
     }
@@ -962,9 +984,9 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
           if (p.use_charge)
             for (int kk = tid; kk < k1 - k0; kk += kThreads)
             {
-              const double2 d = sh.dk[sh.selOrient][kk];
-              sh.ks[kk].x += d.x;
-              sh.ks[kk].y += d.y;
+              const double2 d = dyk.dk[sh.selOrient * p.kpc + kk];
+              dyk.ks[kk].x += d.x;
+              dyk.ks[kk].y += d.y;
             }
         }
       }
@@ -1079,9 +1101,9 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
         if (p.use_charge)
           for (int kk = tid; kk < k1 - k0; kk += kThreads)
           {
-            const double2 d = sh.dk[0][kk];
-            sh.ks[kk].x += d.x;
-            sh.ks[kk].y += d.y;
+            const double2 d = dyk.dk[kk];
+            dyk.ks[kk].x += d.x;
+            dyk.ks[kk].y += d.y;
           }
       }
     }
@@ -1211,9 +1233,9 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
           if (p.use_charge)
             for (int kk = tid; kk < k1 - k0; kk += kThreads)
             {
-              const double2 d = sh.dk[sh.selOrient][kk];
-              sh.ks[kk].x += d.x;
-              sh.ks[kk].y += d.y;
+              const double2 d = dyk.dk[sh.selOrient * p.kpc + kk];
+              dyk.ks[kk].x += d.x;
+              dyk.ks[kk].y += d.y;
             }
         }
         c = oldC;
@@ -1230,8 +1252,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(Params p, int moves
     }
     __syncthreads();
   }
-  for (int kk = tid; kk < k1 - k0; kk += kThreads) p.sk[k0 + kk] = sh.ks[kk];
-  if (blockIdx.x == 0 && tid == 0 && !sh.fail)
+  for (int kk = tid; kk < k1 - k0; kk += kThreads) p.sk[k0 + kk] = dyk.ks[kk];
+  if (cta == 0 && tid == 0 && !sh.fail)
   {
     p.n_state[0] = sh.n;
     for (int c = 0; c < kMaxComp; ++c) p.n_state[1 + c] = sh.count[c];
@@ -1468,24 +1490,29 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
     for (int d = 0; d < 3; ++d) p.km[d] = kmax[d];
   }
   p.tabK = 1 + std::max({p.km[0], p.km[1], p.km[2]});
-  x->smem = dynBytes(p.tabK);
-  // launch geometry: one CTA per SM, co-resident
+  // launch geometry: one CTA per SM, co-resident; this system's CTAs split its k-vectors into ranges of kpc
   int sms = 0, perSM = 0;
   cudaError_t err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  if (err == cudaSuccess)
-    err = cudaFuncSetAttribute(mixtureKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(x->smem));
-  if (err == cudaSuccess)
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, mixtureKernel, kThreads, x->smem);
+  if (err != cudaSuccess)
+  {
+    delete x;
+    return rg::cudaFail(ctx, err, "rg_mixture_create");
+  }
+  x->blocks = std::min(kMaxBlocks, params->n_blocks > 0 ? std::min(params->n_blocks, sms) : sms);
+  p.group = x->blocks;
+  p.kpc = std::max(1, (p.nk + x->blocks - 1) / x->blocks);
+  if (p.use_charge && p.kpc > kMaxKPerCta)
+  {
+    delete x;
+    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: more than 384 k-vectors per CTA (use more CTAs)");
+  }
+  x->smem = dynBytes(p.tabK, p.kpc);
+  err = cudaFuncSetAttribute(mixtureKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(x->smem));
+  if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, mixtureKernel, kThreads, x->smem);
   if (err != cudaSuccess || perSM < 1)
   {
     delete x;
     return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: kernel does not fit on an SM");
-  }
-  x->blocks = std::min(kMaxBlocks, params->n_blocks > 0 ? std::min(params->n_blocks, sms * perSM) : sms);
-  if (p.use_charge && (p.nk + x->blocks - 1) / x->blocks > kMaxKPerCta)
-  {
-    delete x;
-    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: more than 64 k-vectors per CTA");
   }
   // device state
   const int cap = p.capacity;
@@ -1625,23 +1652,56 @@ extern "C" rg_status rg_mixture_set_state(rg_mixture* x, double energy, const do
   return RG_OK;
 }
 
-extern "C" rg_status rg_mixture_run(rg_mixture* x, int64_t moves, int record)
+extern "C" rg_status rg_mixture_run_many(rg_mixture* const* mixtures, int n, int64_t moves, int record)
 {
-  if (!x || moves < 0) return RG_ERR_INVALID_ARGUMENT;
-  rg_ctx* ctx = x->ctx;
+  if (!mixtures || n < 1 || moves < 0) return RG_ERR_INVALID_ARGUMENT;
+  for (int s = 0; s < n; ++s)
+    if (!mixtures[s]) return RG_ERR_INVALID_ARGUMENT;
+  rg_mixture* x0 = mixtures[0];
+  rg_ctx* ctx = x0->ctx;
+  if (n > kMaxSystems) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_run_many: at most 8 systems");
+  size_t smem = 0;
+  for (int s = 0; s < n; ++s)
+  {
+    if (mixtures[s]->ctx != ctx || mixtures[s]->blocks != x0->blocks)
+      return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_run_many: one context and one CTA count for all");
+    for (int t = 0; t < s; ++t)
+      if (mixtures[t] == mixtures[s])
+        return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_run_many: a system listed twice");
+    smem = std::max(smem, mixtures[s]->smem);
+  }
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
-  x->p.record = record ? 1 : 0;
+  // every system's CTAs must be resident together with the others' (one cooperative launch)
+  int sms = 0, perSM = 0;
+  RG_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  RG_CUDA(ctx, cudaFuncSetAttribute(mixtureKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  RG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, mixtureKernel, kThreads, smem));
+  if (static_cast<long long>(n) * x0->blocks > static_cast<long long>(sms) * perSM)
+    return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_run_many: the systems' CTAs do not fit on the GPU at once");
+  Launch L{};
+  for (int s = 0; s < n; ++s)
+  {
+    mixtures[s]->p.record = record ? 1 : 0;
+    L.p[s] = mixtures[s]->p;
+  }
   const int64_t per = 8192;
   for (int64_t done = 0; done < moves; done += per)
   {
     int m = static_cast<int>(std::min<int64_t>(per, moves - done));
-    void* args[] = {&x->p, &m};
-    // the barrier's arrival counter starts at zero in every launch (the error flag beside it persists)
-    RG_CUDA(ctx, cudaMemsetAsync(x->p.bar, 0, sizeof(unsigned long long), ctx->stream));
-    RG_CUDA(ctx, cudaLaunchCooperativeKernel(reinterpret_cast<void*>(mixtureKernel), dim3(x->blocks), dim3(kThreads),
-                                             args, x->smem, ctx->stream));
+    void* args[] = {&L, &m};
+    // every barrier's arrival counter starts at zero in every launch (the error flags beside them persist)
+    for (int s = 0; s < n; ++s)
+      RG_CUDA(ctx, cudaMemsetAsync(mixtures[s]->p.bar, 0, sizeof(unsigned long long), ctx->stream));
+    RG_CUDA(ctx, cudaLaunchCooperativeKernel(reinterpret_cast<void*>(mixtureKernel), dim3(n * x0->blocks),
+                                             dim3(kThreads), args, smem, ctx->stream));
   }
   return RG_OK;
+}
+
+extern "C" rg_status rg_mixture_run(rg_mixture* x, int64_t moves, int record)
+{
+  if (!x) return RG_ERR_INVALID_ARGUMENT;
+  return rg_mixture_run_many(&x, 1, moves, record);
 }
 
 extern "C" rg_status rg_mixture_set_wait_test(rg_mixture* x, int absent_cta, int64_t spin_limit)

@@ -240,6 +240,13 @@ def lib():
         L.rg_mixture_run.argtypes = [vp, i64, i32]
         L.rg_mixture_results.argtypes = [vp, P(MixtureResult)]
         L.rg_mixture_set_wait_test.argtypes = [vp, i32, i64]
+        L.rg_mixture_run_many.argtypes = [vp, i32, i64, i32]
+        L.rg_ewald_batch_create.argtypes = [vp, i32, P(vp)]
+        L.rg_ewald_batch_destroy.argtypes = [vp]
+        L.rg_ewald_batch_set.argtypes = [vp, i32, vp]
+        L.rg_ewald_batch_get.argtypes = [vp, i32, i32, vp]
+        L.rg_ewald_batch_delta.argtypes = [vp, vp, i32, vp, vp, vp]
+        L.rg_ewald_batch_accept.argtypes = [vp, vp]
         L.rg_mixture_get_positions.argtypes = [vp, vp, vp, i32, P(i32)]
         L.rg_mixture_get_structure_factors.argtypes = [vp, vp, i64]
         L.rg_mixture_set_proposal.argtypes = [vp, i32, vp, P(RgBox)]
@@ -685,6 +692,52 @@ class System:
             "rg_system_set_external_field")
 
 
+class EwaldBatch:
+    """Structure factors of many systems sharing one Ewald state's k-vectors (rg_ewald_batch)."""
+
+    def __init__(self, ewald: "Ewald", n_systems: int):
+        self.ctx = ewald.ctx
+        self.n = n_systems
+        self.nk = ewald.n_kvectors
+        h = ctypes.c_void_p()
+        check(self.ctx.handle, lib().rg_ewald_batch_create(ewald.handle, n_systems, ctypes.byref(h)),
+              "rg_ewald_batch_create")
+        self.handle = h
+        self.ctx.adopt(self)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().rg_ewald_batch_destroy(self.handle)
+            self.handle = None
+
+    def set(self, system: int, sk=None):
+        s = None if sk is None else np.ascontiguousarray(sk, dtype=np.float64)
+        check(self.ctx.handle, lib().rg_ewald_batch_set(self.handle, system,
+                                                        None if s is None else ctypes.c_void_p(s.ctypes.data)),
+              "rg_ewald_batch_set")
+
+    def get(self, system: int, which: int = 0) -> np.ndarray:
+        out = np.empty(2 * self.nk)
+        check(self.ctx.handle, lib().rg_ewald_batch_get(self.handle, system, which, ctypes.c_void_p(out.ctypes.data)),
+              "rg_ewald_batch_get")
+        return out
+
+    def delta(self, atoms, max_atoms: int, n_new, n_old) -> np.ndarray:
+        a, p = _atoms_ptr(atoms)
+        nn = np.ascontiguousarray(n_new, dtype=np.int32)
+        no = np.ascontiguousarray(n_old, dtype=np.int32)
+        out = np.empty(self.n)
+        check(self.ctx.handle, lib().rg_ewald_batch_delta(self.handle, p, max_atoms, ctypes.c_void_p(nn.ctypes.data),
+                                                          ctypes.c_void_p(no.ctypes.data),
+                                                          ctypes.c_void_p(out.ctypes.data)), "rg_ewald_batch_delta")
+        return out
+
+    def accept(self, mask):
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        check(self.ctx.handle, lib().rg_ewald_batch_accept(self.handle, ctypes.c_void_p(m.ctypes.data)),
+              "rg_ewald_batch_accept")
+
+
 class Gcmc:
     """Independent device-resident GCMC chains of one rigid component (rg_gcmc)."""
 
@@ -1055,6 +1108,13 @@ class Mixture:
         r = MixtureResult()
         check(self.ctx.handle, lib().rg_mixture_results(self.handle, ctypes.byref(r)), "rg_mixture_results")
         return r.as_dict()
+
+    @staticmethod
+    def run_many(mixtures, moves: int, record: bool = True):
+        """Several mixtures (one context, one CTA count) advanced by one cooperative launch (rg_mixture_run_many)."""
+        arr = (ctypes.c_void_p * len(mixtures))(*[m.handle.value for m in mixtures])
+        check(mixtures[0].ctx.handle, lib().rg_mixture_run_many(ctypes.cast(arr, ctypes.c_void_p), len(mixtures),
+                                                                moves, 1 if record else 0), "rg_mixture_run_many")
 
     def set_wait_test(self, absent_cta: int, spin_limit: int):
         """Test of the bounded barrier wait (rg_mixture_set_wait_test): the next launch's waits give up by design."""

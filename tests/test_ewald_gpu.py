@@ -171,3 +171,51 @@ def test_running_energy_drift_over_many_moves(ctx, oracle):
     e_ref, stored = oracle.ewald_fourier_energy(ff, cell, ads, sizes, s_rigid=s_rigid)
     assert abs(recomputed - total(e_ref)) < 1e-8 * max(1.0, abs(total(e_ref)))
     np.testing.assert_allclose(s_gpu[0::2], stored[0::10], rtol=0, atol=1e-8)
+
+
+def test_batched_structure_factor_update(ctx, oracle):
+    """rg_ewald_batch: one CO2 move in each of 40 systems that share the configuration-5 k-vectors (kmax 12, the full
+    half-box), in one launch. Each system's Fourier energy change and trial S(k) equal the oracle's
+    energyDifferenceEwaldFourier on that system's own S(k) (1e-9), and accepting flips only the accepted systems."""
+    from raspa3_b200.synthetic import random_molecules
+
+    ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=12, sphere=False)
+    cell = np.diag([40.0, 39.8, 40.2])
+    ew = native.Ewald(ctx, ff, cell)
+    nk = ew.n_kvectors
+    n_sys = 40
+    batch = native.EwaldBatch(ew, n_sys)
+    rng = np.random.default_rng(12)
+    oracle_stored, moves = [], []
+    for s in range(n_sys):
+        mols = random_molecules(ff, cell, 20, seed=100 + s)
+        ew.full(mols, [3] * 20)  # this system's structure factor into the Ewald state, then into the batch
+        batch.set(s)
+        _, so = oracle.ewald_fourier_energy(ff, cell, mols, [3] * 20)
+        oracle_stored.append(so)
+        np.testing.assert_allclose(batch.get(s, 0)[0::2], so[0::10][:nk], rtol=0, atol=1e-9)
+        old = mols[3 * (s % 20):3 * (s % 20) + 3]
+        new = old.copy()
+        for k in "xyz":
+            new[k] += rng.normal() * 0.6
+        moves.append((new, old))
+    packed = np.concatenate([np.concatenate([n, o]) for n, o in moves])
+    d = batch.delta(packed, 6, [3] * n_sys, [3] * n_sys)
+    trials = []
+    for s in range(n_sys):
+        new, old = moves[s]
+        ref, trial = oracle.ewald_delta(ff, cell, oracle_stored[s], new, old)
+        trials.append(trial)
+        assert abs(d[s] - ref["ewald_fourier"]) <= 1e-9 * max(1.0, abs(ref["ewald_fourier"])), (s, d[s], ref)
+        got_trial = batch.get(s, 1)
+        np.testing.assert_allclose(got_trial[0::2], trial[0::10][:nk], rtol=0, atol=1e-9)
+        np.testing.assert_allclose(got_trial[1::2], trial[1::10][:nk], rtol=0, atol=1e-9)
+    mask = np.arange(n_sys) % 3 == 0
+    batch.accept(mask)
+    for s in range(6):
+        now = batch.get(s, 0)
+        ref = trials[s] if mask[s] else oracle_stored[s]
+        np.testing.assert_allclose(now[0::2], ref[0::10][:nk], rtol=0, atol=1e-9)
+        np.testing.assert_allclose(now[1::2], ref[1::10][:nk], rtol=0, atol=1e-9)
+    batch.close()
+    ew.close()

@@ -112,6 +112,55 @@ def itq29(ff: ForceField, replicate=(1, 1, 1)):
     return cell, make_atoms(np.concatenate(pos), np.concatenate(tt), np.concatenate(qq))
 
 
+# P n m a (space group 62, Hall "-P 2ac 2n", Hall number 292): the eight general positions of the standard setting
+# (International Tables for Crystallography A, No. 62), as (rotation diagonal, translation).
+_PNMA = [((1, 1, 1), (0.0, 0.0, 0.0)), ((-1, -1, 1), (0.5, 0.0, 0.5)), ((-1, 1, -1), (0.0, 0.5, 0.0)),
+         ((1, -1, -1), (0.5, 0.5, 0.5)), ((-1, -1, -1), (0.0, 0.0, 0.0)), ((1, 1, -1), (0.5, 0.0, 0.5)),
+         ((1, -1, 1), (0.0, 0.5, 0.0)), ((-1, 1, 1), (0.5, 0.5, 0.5))]
+
+
+def mfi(ff: ForceField, replicate=(1, 1, 1)):
+    """MFI (Framework::makeMFI, src/raspakit/framework.cpp:1591-1660): the asymmetric unit of tests/golden/
+    mfi_framework.json (generated from that source by tests/golden/make_mfi_fixture.py) expanded with P n m a,
+    reduced to [0, 1) and de-duplicated within 0.1 Angstrom as CIFReader::expandDefinedAtomsToUnitCell does
+    (cif_reader.cpp:589-631). Returns (cell rows, unit-cell or replicated atoms in Cartesian)."""
+    import json
+    import os
+
+    d = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mfi_framework.json")))
+    assert d["hall_number"] == 292
+    L = np.asarray(d["cell_lengths"])
+    expanded = []
+    for x, y, z, q, name in d["asymmetric_atoms"]:
+        p = np.array([x, y, z])
+        for rot, tr in _PNMA:
+            expanded.append((_fract(np.asarray(rot) * p + np.asarray(tr)), ff.index(name), q))
+    keep = []
+    for i, (fi, ti, qi) in enumerate(expanded):
+        dup = False
+        for j in range(i + 1, len(expanded)):
+            dd = (fi - expanded[j][0]) * L
+            dd = dd - np.rint(dd / L) * L
+            if float(dd @ dd) < 0.1 * 0.1:
+                dup = True
+                break
+        if not dup:
+            keep.append((fi, ti, qi))
+    frac = np.array([k[0] for k in keep])
+    types = np.array([k[1] for k in keep], dtype=np.uint16)
+    charges = np.array([k[2] for k in keep])
+    nx, ny, nz = replicate
+    pos, tt, qq = [], [], []
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz):
+                pos.append((frac + np.array([i, j, k])) * L)
+                tt.append(types)
+                qq.append(charges)
+    cell = np.diag(L * np.array(replicate, dtype=np.float64))
+    return cell, make_atoms(np.concatenate(pos), np.concatenate(tt), np.concatenate(qq))
+
+
 def co2_atoms(ff: ForceField, centers, molecule_ids, bond=1.149, axis=(0.0, 0.0, 1.0), charges=True):
     """Rigid CO2 (O, C, O order of Component::makeCO2) centred at each point along `axis`."""
     qO, qC = (-0.3256, 0.6512) if charges else (0.0, 0.0)

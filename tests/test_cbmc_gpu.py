@@ -8,7 +8,7 @@ from raspa3_b200.forcefield import ENERGY_TO_KELVIN, make_atoms
 from raspa3_b200.synthetic import (CO2_NAMES, CO2_OFFSETS, random_molecules, random_rotation, replicate,
                                    rigid_molecule, synthetic_forcefield, synthetic_framework)
 from reference_systems import ITQ29_A, itq29, methane_atoms, zeolite_forcefield
-from test_oracle_golden import STATIC_CO2_ITQ29, static_co2_itq29_system
+from test_oracle_golden import STATIC_CO2_ITQ29, STATIC_CO2_MFI, static_co2_itq29_system, static_co2_mfi_system
 
 pytestmark = pytest.mark.gpu
 
@@ -62,6 +62,19 @@ def test_golden_two_co2_itq29_charged(ctx, precision):
         np.testing.assert_allclose(got, ref, rtol=0, atol=1e-6)
     else:
         np.testing.assert_allclose(got, ref, rtol=1e-6, atol=0)
+    sysg.close()
+
+
+def test_golden_two_co2_mfi_charged(ctx):
+    """tests/raspakit-tests/static_energy.cpp:48-74 (2 CO2 in MFI 2x2x2, 2304 framework atoms) through
+    rg_cbmc_external_energies, to 1e-6 K."""
+    ff, cell, fw, atoms = static_co2_mfi_system()
+    sysg = native.System(ctx, ff, cell, fw)
+    sysg.set_molecules(atoms)
+    trials = sysg.external_energies(atoms, 1)
+    got = np.array([sum(t.framework_vdw for t in trials), sum(t.framework_charge for t in trials),
+                    sum(t.molecule_vdw for t in trials[:3]), sum(t.molecule_charge for t in trials[:3])])
+    np.testing.assert_allclose(got * ENERGY_TO_KELVIN, STATIC_CO2_MFI, rtol=0, atol=1e-6)
     sysg.close()
 
 

@@ -7,7 +7,7 @@ from raspa3_b200 import native
 from raspa3_b200.forcefield import ENERGY_TO_KELVIN
 from raspa3_b200.synthetic import (CO2_NAMES, CO2_OFFSETS, random_molecules, random_rotation, rigid_molecule,
                                    synthetic_forcefield, synthetic_framework)
-from reference_systems import co2_atoms, itq29, zeolite_forcefield
+from reference_systems import co2_atoms, itq29, mfi, zeolite_forcefield
 
 pytestmark = pytest.mark.gpu
 
@@ -55,6 +55,26 @@ def test_golden_itq29_with_framework(ctx, rep, single_ion, fourier):
     from raspa3_b200.forcefield import COULOMBIC_CONVERSION_FACTOR as C
     u = -(ew.single_ion_sum - C * ff.ewald_alpha / math.sqrt(math.pi))
     assert abs(u * ENERGY_TO_KELVIN - single_ion) < 1e-6
+
+
+@pytest.mark.parametrize("rep,single_ion,fourier", [((1, 1, 1), 12028.1731827280, -1191.77790165),
+                                                    ((2, 2, 2), 6309.7866899037, -1197.23909965)])
+def test_golden_mfi_with_framework(ctx, rep, single_ion, fourier):
+    """tests/raspakit-tests/ewald.cpp:212-278: 2 CO2 in MFI (Framework::makeMFI, P n m a) 1x1x1 and 2x2x2."""
+    import math
+    from raspa3_b200.forcefield import COULOMBIC_CONVERSION_FACTOR as C
+
+    ff = zeolite_forcefield(12.0, True, use_charge=True)
+    ff.ewald_alpha = 0.25
+    cell, fw = mfi(ff, rep)
+    ew = native.Ewald(ctx, ff, cell)
+    ew.set_framework(fw)
+    atoms = co2_atoms(ff, [(10.011, 4.97475 + 2.0, 0.0), (10.011, 4.97475 - 2.0, 0.0)], [0, 1])
+    e = ew.full(atoms, [3, 3])
+    assert abs(total(e) * ENERGY_TO_KELVIN - fourier) < 1e-6
+    u = -(ew.single_ion_sum - C * ff.ewald_alpha / math.sqrt(math.pi))
+    assert abs(u * ENERGY_TO_KELVIN - single_ion) < 1e-6
+    ew.close()
 
 
 def config2_system(n_mol=24, seed=3, sphere=True):

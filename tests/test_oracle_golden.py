@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 from raspa3_b200.forcefield import ENERGY_TO_KELVIN, COULOMBIC_CONVERSION_FACTOR, make_atoms
-from reference_systems import ITQ29_A, auto_ewald_alpha, co2_atoms, itq29, methane_atoms, zeolite_forcefield
+from reference_systems import ITQ29_A, auto_ewald_alpha, co2_atoms, itq29, methane_atoms, mfi, zeolite_forcefield
 
 
 def test_units_match_reference_constants(oracle):
@@ -182,3 +182,51 @@ def test_blocked_pockets_and_external_field_oracle(oracle):
     assert ok and e == 0.0  # 0.71 A from the z axis through the box centre (the position is not wrapped)
     ok, _ = oracle.external_field_energy(13, (2.0, 0, 0, 0), cell, make_atoms([(5.0, 9.0, 1.0)], 0, 0.0))
     assert not ok
+
+
+def test_mfi_expansion_counts():
+    """Framework::makeMFI: 12 Si + 26 O in the asymmetric unit, P n m a -> 96 Si + 192 O, neutral."""
+    ff = zeolite_forcefield()
+    cell, atoms = mfi(ff)
+    assert len(atoms) == 288 and int(np.sum(atoms["type"] == ff.index("Si"))) == 96
+    assert abs(float(np.sum(atoms["charge"]))) < 1e-9
+    np.testing.assert_allclose(np.diag(cell), (20.022, 19.899, 13.383))
+
+
+@pytest.mark.parametrize("rep,single_ion,fourier", [
+    ((1, 1, 1), 12028.1731827280, -1191.77790165),
+    ((2, 2, 2), 6309.7866899037, -1197.23909965),
+])
+def test_ewald_two_co2_in_mfi(oracle, rep, single_ion, fourier):
+    """tests/raspakit-tests/ewald.cpp:212-278."""
+    ff = zeolite_forcefield(12.0, True, use_charge=True)
+    ff.ewald_alpha = 0.25
+    ff.kmax = (8, 8, 8)
+    cell, fw = mfi(ff, rep)
+    atoms = co2_atoms(ff, [(10.011, 4.97475 + 2.0, 0.0), (10.011, 4.97475 - 2.0, 0.0)], [0, 1])
+    assert abs(oracle.ewald_single_ion(ff, cell, (0.0, 0.0, 0.0), 1.0) * ENERGY_TO_KELVIN - single_ion) < 1e-6
+    e, _ = oracle.ewald_fourier_energy(ff, cell, atoms, [3, 3], s_rigid=oracle.ewald_rigid(ff, cell, fw))
+    assert abs((e["ewald_fourier"] + e["ewald_self"] + e["ewald_exclusion"]) * ENERGY_TO_KELVIN - fourier) < 1e-6
+
+
+# tests/raspakit-tests/static_energy.cpp:48-74: 2 CO2 in MFI 2x2x2, shifted
+STATIC_CO2_MFI = (-2525.36580663, 2167.45591472, -242.42459776, 154.11883595)
+
+
+def static_co2_mfi_system():
+    ff = zeolite_forcefield(12.0, True, use_charge=True)
+    ff.ewald_alpha = auto_ewald_alpha(12.0)
+    cell, fw = mfi(ff, (2, 2, 2))
+    atoms = co2_atoms(ff, [(10.011, 4.97475 + 2.0, 0.0), (10.011, 4.97475 - 2.0, 0.0)], [0, 1])
+    return ff, cell, fw, atoms
+
+
+def test_static_energy_two_co2_in_mfi(oracle):
+    ff, cell, fw, atoms = static_co2_mfi_system()
+    ok, e = oracle.cbmc_framework_molecule(ff, cell, fw, atoms, 12.0, 12.0)
+    ok2, e2 = oracle.cbmc_intermolecular(ff, cell, atoms, atoms[:3], 12.0, 12.0)
+    assert ok and ok2
+    got = (e["framework_molecule_vdw"], e["framework_molecule_charge"], e2["molecule_molecule_vdw"],
+           e2["molecule_molecule_charge"])
+    for g, ref in zip(got, STATIC_CO2_MFI):
+        assert abs(g * ENERGY_TO_KELVIN - ref) < 1e-6, (g * ENERGY_TO_KELVIN, ref)

@@ -938,7 +938,7 @@ struct rg_ewald_batch
 namespace
 {
 constexpr int kBatchAtoms = 16;   // old + new atoms of one system's move
-constexpr int kBatchKPerThread = 2;
+constexpr int kBatchKPerThread = 8;
 
 __global__ void __launch_bounds__(kThreads) ewaldBatchDeltaKernel(
     int64_t nk, int n_systems, const char4* __restrict__ kvec, const double* __restrict__ temp, double2* sk,

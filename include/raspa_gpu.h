@@ -274,9 +274,9 @@ rg_status rg_grid_validate_triquintic(rg_ctx* ctx, const rg_forcefield* ff, cons
  * Same arguments and result as rg_grid_build, minus the context: the caller passes the device, a stream (NULL = the
  * legacy default stream) and the device output buffer; there is no host output. The working memory is one fixed
  * file-scope device array that every GPU loading the library holds until exit; it holds at most 32768 periodic images
- * of the unit-cell atoms (RG_ERR_INVALID_ARGUMENT beyond that). The first call on a device looks up the array's device
- * address, so make that first call before any stream capture. All calls share the array: calls whose work overlaps on
- * the GPU (from several threads or streams) race; serialise them. */
+ * of the unit-cell atoms (RG_ERR_INVALID_ARGUMENT beyond that). The work runs with `device` current and the caller's
+ * current device is restored before the call returns. All calls share the array: calls whose work overlaps on the GPU
+ * (from several threads or streams) race; serialise them. */
 rg_status rg_grid_build_noalloc(int device, void* stream, int grid_type, const rg_forcefield* ff,
                                 const rg_box* unit_cell, const rg_atom* unit_atoms, int n_unit_atoms, int probe_type,
                                 double cutoff, int nx, int ny, int nz, int precision, double* out_device,
@@ -520,8 +520,10 @@ rg_status rg_ewald_info(rg_ewald* ewald, int64_t* n_kvectors, double* single_ion
 rg_status rg_ewald_set_framework(rg_ewald* ewald, const rg_atom* framework_atoms, int n_framework_atoms);
 /* Replaces Interactions::computeEwaldFourierEnergy (ewald.cpp:352-563): full recompute of the adsorbate structure
  * factors (stored), Fourier energy minus the framework-framework part, self, exclusion and net-charge terms.
- * molecule_sizes: atom counts of the consecutive molecules in atoms (for the intramolecular exclusion). Called at
- * initialisation, for drift checks and for volume moves. */
+ * molecule_sizes: atom counts of the consecutive molecules in atoms (for the intramolecular exclusion; counts that
+ * are negative or add up to more than n_atoms give RG_ERR_INVALID_ARGUMENT). The host self, exclusion and net-charge
+ * sums run while the structure-factor kernels are in flight. Called at initialisation, for drift checks and for volume
+ * moves. */
 rg_status rg_ewald_full(rg_ewald* ewald, const rg_atom* atoms, int n_atoms, const int32_t* molecule_sizes,
                         int n_molecules, double net_charge_framework, rg_ewald_energy* out);
 /* Replaces Interactions::energyDifferenceEwaldFourier (ewald.cpp:1043-1244), called from every charged move

@@ -665,7 +665,18 @@ rg_status rg_ewald_full(rg_ewald* e, const rg_atom* atoms, int n_atoms, const in
     return RG_ERR_INVALID_ARGUMENT;
   rg_ctx* ctx = e->ctx;
   std::memset(out, 0, sizeof(rg_ewald_energy));
+  if (rg_status fs = rg::checkFinite(ctx, atoms, n_atoms, "rg_ewald_full")) return fs;
   if (!e->use_charge) return RG_OK;
+  if (!e->omit_inter)
+  {
+    int64_t total = 0;
+    for (int m = 0; m < n_molecules; ++m)
+    {
+      if (molecule_sizes[m] < 0) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_ewald_full: molecule sizes");
+      total += molecule_sizes[m];
+    }
+    if (total > n_atoms) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_ewald_full: molecule sizes");
+  }
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
   const int G = e->n_groups;
   double res[1 + kMaxGroups] = {0, 0, 0, 0, 0};
@@ -683,11 +694,8 @@ rg_status rg_ewald_full(rg_ewald* e, const rg_atom* atoms, int n_atoms, const in
       default: err = launchFull<4>(e, n_atoms); break;
     }
     if (err) return rg::cudaFail(ctx, err, "ewaldFullKernel");
-    st = readResult(e, res, 1 + G);
-    if (st) return st;
   }
-  out->ewald_fourier = res[0];
-  for (int g = 0; g < G; ++g) out->dudlambda_ewald[g] = res[1 + g];
+  // the host terms below run while the kernels are in flight; the reciprocal-space sum is read afterwards
   const double C = rg::coulombFactor();
   const double alpha = e->alpha;
   if (!e->omit_inter)
@@ -705,7 +713,6 @@ rg_status rg_ewald_full(rg_ewald* e, const rg_atom* atoms, int n_atoms, const in
     for (int m = 0; m < n_molecules; ++m)
     {
       const int size = molecule_sizes[m];
-      if (index + size > n_atoms) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_ewald_full: molecule sizes");
       const rg_atom* span = atoms + index;
       for (int i = 0; i + 1 < size; ++i)
         for (int j = i + 1; j < size; ++j)
@@ -732,17 +739,26 @@ rg_status rg_ewald_full(rg_ewald* e, const rg_atom* atoms, int n_atoms, const in
     if (g != 0) netChargeDerivative[g - 1] += atoms[i].charge;
   }
   const double uIon = -(e->single_ion_sum - C * alpha / std::sqrt(rg::kPi));
+  double netFourier = 0.0, netDudl[4] = {0, 0, 0, 0};
   if (e->omit_inter)
   {
-    out->ewald_fourier += 2.0 * uIon * net_charge_framework * netChargeAdsorbates;
-    for (int g = 0; g < 4; ++g) out->dudlambda_ewald[g] += 2.0 * uIon * net_charge_framework * netChargeDerivative[g];
+    netFourier = 2.0 * uIon * net_charge_framework * netChargeAdsorbates;
+    for (int g = 0; g < 4; ++g) netDudl[g] = 2.0 * uIon * net_charge_framework * netChargeDerivative[g];
   }
   else
   {
-    out->ewald_fourier += uIon * (2.0 * net_charge_framework + netChargeAdsorbates) * netChargeAdsorbates;
+    netFourier = uIon * (2.0 * net_charge_framework + netChargeAdsorbates) * netChargeAdsorbates;
     for (int g = 0; g < 4; ++g)
-      out->dudlambda_ewald[g] += 2.0 * uIon * (net_charge_framework + netChargeAdsorbates) * netChargeDerivative[g];
+      netDudl[g] = 2.0 * uIon * (net_charge_framework + netChargeAdsorbates) * netChargeDerivative[g];
   }
+  if (e->nk > 0)
+  {
+    rg_status st = readResult(e, res, 1 + G);
+    if (st) return st;
+  }
+  out->ewald_fourier = res[0] + netFourier;
+  for (int g = 0; g < G; ++g) out->dudlambda_ewald[g] += res[1 + g];
+  for (int g = 0; g < 4; ++g) out->dudlambda_ewald[g] += netDudl[g];
   return RG_OK;
 }
 

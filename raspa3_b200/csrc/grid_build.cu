@@ -28,7 +28,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -1268,25 +1267,10 @@ constexpr int kNoAllocMaxImages = 32768;
 constexpr size_t kNoAllocBytes = 2 * sizeof(double4) * kNoAllocMaxImages + 256;
 __device__ __align__(256) unsigned char g_grid_noalloc_scratch[kNoAllocBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-void* g_noalloc_address[kMaxDevices] = {};
-
-// The device address of g_grid_noalloc_scratch on `device` (looked up once per device with that device current; in
-// host code the symbol itself is only a host-side stand-in and must never be passed to a kernel).
-cudaError_t noallocScratchAddress(int device, void** out)
-{
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_address[device])
-  {
-    void* p = nullptr;
-    cudaError_t err = cudaGetSymbolAddress(&p, g_grid_noalloc_scratch);
-    if (err != cudaSuccess) return err;
-    g_noalloc_address[device] = p;
-  }
-  *out = g_noalloc_address[device];
-  return cudaSuccess;
-}
+// The device address of g_grid_noalloc_scratch on `device`, which must be current. Looked up on every call (a host-side
+// query, no allocation) so that no address outlives the context it belongs to; in host code the symbol itself is only a
+// host-side stand-in and must never be passed to a kernel.
+cudaError_t noallocScratchAddress(void** out) { return cudaGetSymbolAddress(out, g_grid_noalloc_scratch); }
 }  // namespace
 
 namespace
@@ -1297,7 +1281,7 @@ rg_status gridBuildNoalloc(int device, cudaStream_t st, int grid_type, const rg_
                            int nz, int precision, double* out_device, rg_grid_stats* stats)
 {
   void* base = nullptr;
-  if (noallocScratchAddress(device, &base) != cudaSuccess) return RG_ERR_CUDA;
+  if (noallocScratchAddress(&base) != cudaSuccess) return RG_ERR_CUDA;
   double4* dpos = static_cast<double4*>(base);
   double4* dpar = dpos + kNoAllocMaxImages;
   unsigned long long* dcount = reinterpret_cast<unsigned long long*>(dpar + kNoAllocMaxImages);
@@ -1417,7 +1401,9 @@ extern "C" rg_status rg_grid_build_noalloc(int device, void* stream, int grid_ty
   if (rg_status fs = rg::checkFinite(nullptr, unit_atoms, n_unit_atoms, "rg_grid_build_noalloc")) return fs;
   if (rg_status fs = rg::checkFiniteBox(nullptr, unit_cell, "rg_grid_build_noalloc")) return fs;
   if (grid_type != RG_GRID_EWALD_REAL && (probe_type < 0 || probe_type >= ff->n_types)) return RG_ERR_INVALID_ARGUMENT;
-  if (device < 0 || device >= kMaxDevices) return RG_ERR_INVALID_ARGUMENT;
+  int n_devices = 0;
+  if (cudaGetDeviceCount(&n_devices) != cudaSuccess) return RG_ERR_CUDA;
+  if (device < 0 || device >= n_devices) return RG_ERR_INVALID_ARGUMENT;
   // the work runs with `device` current; the caller's current device is restored on every return
   int previous = -1;
   if (cudaGetDevice(&previous) != cudaSuccess) return RG_ERR_CUDA;

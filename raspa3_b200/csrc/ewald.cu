@@ -948,37 +948,77 @@ struct rg_ewald_batch
   unsigned int* counter = nullptr; // [n]
   double* result = nullptr;        // device view of result_host
   double* result_host = nullptr;   // [n] mapped pinned
-  int blocks = 0;                  // k-tiles per system
+  int blocks = 0;                  // k-ranges per system
+  int4* desc = nullptr;            // [blocks]: first k, end k, first (kx, ky) pair, pairs
+  int* kinfo = nullptr;            // [nk]: pair * 256 + (kz + 128)
+  char2* pairs = nullptr;          // [pairs]: (kx, ky)
 };
 
 namespace
 {
-constexpr int kBatchAtoms = 16;   // old + new atoms of one system's move
-constexpr int kBatchKPerThread = 8;
+constexpr int kBatchAtoms = 16;       // old + new atoms of one system's move
+constexpr int kBatchKPerThread = 8;   // k-vectors per thread: a block covers at most kThreads * 8 of them
+constexpr int kBatchPairs = 128;      // (kx, ky) pairs of one block's k-range
 
-__global__ void __launch_bounds__(kThreads) ewaldBatchDeltaKernel(
-    int64_t nk, int n_systems, const char4* __restrict__ kvec, const double* __restrict__ temp, double2* sk,
-    const unsigned char* __restrict__ cur, const MovedAtom* __restrict__ atoms, int atom_stride,
-    const int* __restrict__ counts, int kxm, int kym, int kzm, double* partial, unsigned int* counter, double* result)
+// Shared memory of a block: the phasor tables exp(2 pi i m s_d) of its system's moved atoms (x: m = 0..kmax_x; y and z:
+// m = -kmax..kmax, the negative m as conjugates) and the weighted xy products of its (kx, ky) pairs.
+__host__ __device__ inline size_t batchSharedBytes(int stride, int kxm, int kym, int kzm)
 {
-  extern __shared__ double2 tab[];  // [kBatchAtoms][(kxm+1) + (kym+1) + (kzm+1)]
-  __shared__ double wq[kBatchAtoms];
+  return sizeof(double2) * static_cast<size_t>(stride) * ((kxm + 1) + (2 * kym + 1) + (2 * kzm + 1) + kBatchPairs);
+}
+
+// One block per (k-range, system). The k-vectors come in the reference's order (kx outer, then ky, then kz), so a
+// k-range spans few (kx, ky) pairs: the block forms w_a exp(2 pi i (kx s_a,x + ky s_a,y)) once per pair and atom, and
+// each k then costs one complex multiply-add per atom with its z phasor. desc[b] = {first k, end k, first pair,
+// pairs}; kinfo[k] = pair * 256 + (kz + 128); pairs[p] = (kx, ky).
+__global__ void __launch_bounds__(kThreads) ewaldBatchDeltaKernel(
+    const int4* __restrict__ desc, const int* __restrict__ kinfo, const char2* __restrict__ pairs, int64_t nk,
+    int n_systems, const double* __restrict__ temp, double2* sk, const unsigned char* __restrict__ cur,
+    const MovedAtom* __restrict__ atoms, int atom_stride, const int* __restrict__ counts, int kxm, int kym, int kzm,
+    double* partial, unsigned int* counter, double* result)
+{
+  extern __shared__ double2 tab[];
   __shared__ double red[kThreads / 32];
   __shared__ bool last;
   const int sys = blockIdx.y;
+  const int4 d = desc[blockIdx.x];
   const int na = counts[sys];
-  const int stride = (kxm + 1) + (kym + 1) + (kzm + 1);
+  const int nx = kxm + 1, ny = 2 * kym + 1, nz = 2 * kzm + 1;
+  double2* ex = tab;
+  double2* ey = ex + atom_stride * nx;
+  double2* ez = ey + atom_stride * ny;
+  double2* wxy = ez + atom_stride * nz;  // [pair][atom]
   const MovedAtom* ma = atoms + static_cast<long long>(sys) * atom_stride;
-  for (int idx = threadIdx.x; idx < na * stride; idx += blockDim.x)
+  const int per = nx + (kym + 1) + (kzm + 1);
+  for (int idx = threadIdx.x; idx < na * per; idx += blockDim.x)
   {
-    const int a = idx / stride, m = idx - a * stride;
-    const int d = (m <= kxm) ? 0 : ((m <= kxm + 1 + kym) ? 1 : 2);
-    const int mm = (d == 0) ? m : ((d == 1) ? m - (kxm + 1) : m - (kxm + 1) - (kym + 1));
+    const int a = idx / per, m = idx - a * per;
+    const int dim = m < nx ? 0 : (m < nx + kym + 1 ? 1 : 2);
+    const int mm = dim == 0 ? m : (dim == 1 ? m - nx : m - nx - (kym + 1));
     double sn, cs;
-    sincospi(2.0 * static_cast<double>(mm) * ma[a].s[d], &sn, &cs);
-    tab[a * stride + m] = make_double2(cs, sn);
+    sincospi(2.0 * static_cast<double>(mm) * ma[a].s[dim], &sn, &cs);
+    if (dim == 0)
+      ex[a * nx + mm] = make_double2(cs, sn);
+    else if (dim == 1)
+    {
+      ey[a * ny + kym + mm] = make_double2(cs, sn);
+      ey[a * ny + kym - mm] = make_double2(cs, -sn);
+    }
+    else
+    {
+      ez[a * nz + kzm + mm] = make_double2(cs, sn);
+      ez[a * nz + kzm - mm] = make_double2(cs, -sn);
+    }
   }
-  for (int a = threadIdx.x; a < na; a += blockDim.x) wq[a] = ma[a].w;
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < d.w * na; idx += blockDim.x)
+  {
+    const int j = idx / na, a = idx - j * na;
+    const char2 pq = pairs[d.z + j];
+    const double2 x = ex[a * nx + pq.x], y = ey[a * ny + kym + pq.y];
+    const double w = ma[a].w;
+    wxy[j * atom_stride + a] = make_double2(w * (x.x * y.x - x.y * y.y), w * (x.x * y.y + x.y * y.x));
+  }
   __syncthreads();
   const double2* S = sk + (static_cast<long long>(cur[sys]) * n_systems + sys) * nk;
   double2* T = sk + (static_cast<long long>(1 - cur[sys]) * n_systems + sys) * nk;
@@ -986,25 +1026,21 @@ __global__ void __launch_bounds__(kThreads) ewaldBatchDeltaKernel(
 #pragma unroll
   for (int r = 0; r < kBatchKPerThread; ++r)
   {
-    const int64_t k = (static_cast<int64_t>(blockIdx.x) * kBatchKPerThread + r) * blockDim.x + threadIdx.x;
-    if (k >= nk) continue;
-    const char4 kv = kvec[k];
-    const int ay = abs(kv.y), az = abs(kv.z);
-    const double sy = kv.y < 0 ? -1.0 : 1.0, sz = kv.z < 0 ? -1.0 : 1.0;
-    double2 d = make_double2(0.0, 0.0);
+    const int k = d.x + r * kThreads + static_cast<int>(threadIdx.x);
+    if (k >= d.y) continue;
+    const int info = kinfo[k];
+    const double2* w = wxy + ((info >> 8) - d.z) * atom_stride;
+    const double2* z = ez + (info & 0xff) - 128 + kzm;
+    double2 dr = make_double2(0.0, 0.0);
     for (int a = 0; a < na; ++a)
     {
-      const double2* t = tab + a * stride;
-      const double2 ex = t[kv.x], ey0 = t[kxm + 1 + ay], ez0 = t[kxm + 1 + kym + 1 + az];
-      const double2 ey = make_double2(ey0.x, sy * ey0.y), ez = make_double2(ez0.x, sz * ez0.y);
-      const double2 exy = make_double2(ex.x * ey.x - ex.y * ey.y, ex.x * ey.y + ex.y * ey.x);
-      const double w = wq[a];
-      d.x += w * (exy.x * ez.x - exy.y * ez.y);
-      d.y += w * (exy.x * ez.y + exy.y * ez.x);
+      const double2 wa = w[a], za = z[a * nz];
+      dr.x = fma(wa.x, za.x, fma(-wa.y, za.y, dr.x));
+      dr.y = fma(wa.x, za.y, fma(wa.y, za.x, dr.y));
     }
     const double2 s = __ldcs(S + k);
-    e += temp[k] * (2.0 * (s.x * d.x + s.y * d.y) + (d.x * d.x + d.y * d.y));
-    __stcs(T + k, make_double2(s.x + d.x, s.y + d.y));
+    e += temp[k] * (2.0 * (s.x * dr.x + s.y * dr.y) + (dr.x * dr.x + dr.y * dr.y));
+    __stcs(T + k, make_double2(s.x + dr.x, s.y + dr.y));
   }
   // fixed-order reduction: warps, then the block, then (the system's last block) the blocks in order
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1015,7 +1051,7 @@ __global__ void __launch_bounds__(kThreads) ewaldBatchDeltaKernel(
   if (threadIdx.x == 0)
   {
     double x = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) x += red[w];
+    for (int q = 0; q < kThreads / 32; ++q) x += red[q];
     partial[static_cast<long long>(sys) * gridDim.x + blockIdx.x] = x;
     __threadfence();
     last = atomicAdd(counter + sys, 1u) == gridDim.x - 1;
@@ -1024,7 +1060,8 @@ __global__ void __launch_bounds__(kThreads) ewaldBatchDeltaKernel(
   if (!last) return;
   __threadfence();
   double y = 0.0;
-  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) y += __ldcg(partial + static_cast<long long>(sys) * gridDim.x + b);
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+    y += __ldcg(partial + static_cast<long long>(sys) * gridDim.x + b);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) y += __shfl_down_sync(0xffffffffu, y, o);
   if (lane == 0) red[warp] = y;
@@ -1032,7 +1069,7 @@ __global__ void __launch_bounds__(kThreads) ewaldBatchDeltaKernel(
   if (threadIdx.x == 0)
   {
     double x = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) x += red[w];
+    for (int q = 0; q < kThreads / 32; ++q) x += red[q];
     result[sys] = x;
     counter[sys] = 0u;  // ready for the next launch
   }
@@ -1052,8 +1089,45 @@ rg_status rg_ewald_batch_create(rg_ewald* e, int n_systems, rg_ewald_batch** out
   b->ewald = e;
   b->n = n_systems;
   const int64_t nk = std::max<int64_t>(1, e->nk);
-  b->blocks = static_cast<int>((nk + kThreads * kBatchKPerThread - 1) / (kThreads * kBatchKPerThread));
-  cudaError_t err = cudaMalloc(reinterpret_cast<void**>(&b->sk), sizeof(double2) * 2 * n_systems * nk);
+  // k-ranges of at most kThreads * kBatchKPerThread k-vectors and kBatchPairs (kx, ky) pairs, from the k-vector list
+  std::vector<char4> kv(static_cast<size_t>(e->nk));
+  std::vector<int> kinfo(static_cast<size_t>(nk), 0);
+  std::vector<char2> pairs;
+  std::vector<int4> desc;
+  cudaError_t err = cudaSuccess;
+  if (e->nk > 0)
+  {
+    err = cudaMemcpyAsync(kv.data(), e->kvec, sizeof(char4) * e->nk, cudaMemcpyDeviceToHost, ctx->stream);
+    if (!err) err = cudaStreamSynchronize(ctx->stream);
+  }
+  if (err)
+  {
+    delete b;
+    return rg::cudaFail(ctx, err, "rg_ewald_batch_create");
+  }
+  for (int64_t k = 0; k < e->nk; ++k)
+  {
+    if (k == 0 || kv[k].x != kv[k - 1].x || kv[k].y != kv[k - 1].y) pairs.push_back(make_char2(kv[k].x, kv[k].y));
+    kinfo[k] = static_cast<int>(pairs.size() - 1) * 256 + (kv[k].z + 128);
+  }
+  for (int64_t k0 = 0; k0 < e->nk;)
+  {
+    const int p0 = kinfo[k0] >> 8;
+    int64_t k1 = k0;
+    while (k1 < e->nk && k1 - k0 < kThreads * kBatchKPerThread && (kinfo[k1] >> 8) - p0 < kBatchPairs) ++k1;
+    desc.push_back(make_int4(static_cast<int>(k0), static_cast<int>(k1), p0, (kinfo[k1 - 1] >> 8) - p0 + 1));
+    k0 = k1;
+  }
+  if (desc.empty()) desc.push_back(make_int4(0, 0, 0, 0));
+  if (pairs.empty()) pairs.push_back(make_char2(0, 0));
+  b->blocks = static_cast<int>(desc.size());
+  err = cudaMalloc(reinterpret_cast<void**>(&b->desc), sizeof(int4) * desc.size());
+  if (!err) err = cudaMemcpyAsync(b->desc, desc.data(), sizeof(int4) * desc.size(), cudaMemcpyHostToDevice, ctx->stream);
+  if (!err) err = cudaMalloc(reinterpret_cast<void**>(&b->kinfo), sizeof(int) * kinfo.size());
+  if (!err) err = cudaMemcpyAsync(b->kinfo, kinfo.data(), sizeof(int) * kinfo.size(), cudaMemcpyHostToDevice, ctx->stream);
+  if (!err) err = cudaMalloc(reinterpret_cast<void**>(&b->pairs), sizeof(char2) * pairs.size());
+  if (!err) err = cudaMemcpyAsync(b->pairs, pairs.data(), sizeof(char2) * pairs.size(), cudaMemcpyHostToDevice, ctx->stream);
+  if (!err) err = cudaMalloc(reinterpret_cast<void**>(&b->sk), sizeof(double2) * 2 * n_systems * nk);
   if (!err) err = cudaMemsetAsync(b->sk, 0, sizeof(double2) * 2 * n_systems * nk, ctx->stream);
   if (!err) err = cudaMalloc(reinterpret_cast<void**>(&b->cur), n_systems);
   if (!err) err = cudaMemsetAsync(b->cur, 0, n_systems, ctx->stream);
@@ -1088,6 +1162,9 @@ rg_status rg_ewald_batch_destroy(rg_ewald_batch* b)
   cudaFree(b->counts);
   cudaFree(b->partial);
   cudaFree(b->counter);
+  cudaFree(b->desc);
+  cudaFree(b->kinfo);
+  cudaFree(b->pairs);
   if (b->atoms_host) cudaFreeHost(b->atoms_host);
   if (b->counts_host) cudaFreeHost(b->counts_host);
   if (b->result_host) cudaFreeHost(b->result_host);
@@ -1159,11 +1236,15 @@ rg_status rg_ewald_batch_delta(rg_ewald_batch* b, const rg_atom* atoms, int max_
                                ctx->stream));
   RG_CUDA(ctx, cudaMemcpyAsync(b->counts, b->counts_host, sizeof(int) * b->n, cudaMemcpyHostToDevice, ctx->stream));
   const int kxm = e->ff.kmax_x, kym = e->ff.kmax_y, kzm = e->ff.kmax_z;
-  const size_t shmem = sizeof(double2) * kBatchAtoms * ((kxm + 1) + (kym + 1) + (kzm + 1));
+  const size_t shmem = batchSharedBytes(stride, kxm, kym, kzm);
+  if (shmem > 200 * 1024)
+    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_ewald_batch_delta: kmax too large for the shared-memory tables");
+  RG_CUDA(ctx, cudaFuncSetAttribute(ewaldBatchDeltaKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(shmem)));
   dim3 grid(b->blocks, b->n);
-  ewaldBatchDeltaKernel<<<grid, kThreads, shmem, ctx->stream>>>(e->nk, b->n, e->kvec, e->temp, b->sk, b->cur, b->atoms,
-                                                               stride, b->counts, kxm, kym, kzm, b->partial,
-                                                               b->counter, b->result);
+  ewaldBatchDeltaKernel<<<grid, kThreads, shmem, ctx->stream>>>(b->desc, b->kinfo, b->pairs, e->nk, b->n, e->temp,
+                                                               b->sk, b->cur, b->atoms, stride, b->counts, kxm, kym,
+                                                               kzm, b->partial, b->counter, b->result);
   RG_CUDA(ctx, cudaGetLastError());
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   std::memcpy(delta_fourier, b->result_host, sizeof(double) * b->n);

@@ -193,13 +193,16 @@ def test_running_energy_drift_over_many_moves(ctx, oracle):
     np.testing.assert_allclose(s_gpu[0::2], stored[0::10], rtol=0, atol=1e-8)
 
 
-def test_batched_structure_factor_update(ctx, oracle):
-    """rg_ewald_batch: one CO2 move in each of 40 systems that share the configuration-5 k-vectors (kmax 12, the full
-    half-box), in one launch. Each system's Fourier energy change and trial S(k) equal the oracle's
-    energyDifferenceEwaldFourier on that system's own S(k) (1e-9), and accepting flips only the accepted systems."""
+@pytest.mark.parametrize("kmax,sphere", [(12, False), (9, True)])
+def test_batched_structure_factor_update(ctx, oracle, kmax, sphere):
+    """rg_ewald_batch: one CO2 move in each of 40 systems that share one set of k-vectors, in one launch: the
+    configuration-5 set (kmax 12, the full half-box) with translations, and a spherical set (kmax 9, runs of kz of
+    every length) with insertions, deletions and translations. Each system's Fourier energy change and trial S(k)
+    equal the oracle's energyDifferenceEwaldFourier on that system's own S(k) (1e-9), and accepting flips only the
+    accepted systems."""
     from raspa3_b200.synthetic import random_molecules
 
-    ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=12, sphere=False)
+    ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=kmax, sphere=sphere)
     cell = np.diag([40.0, 39.8, 40.2])
     ew = native.Ewald(ctx, ff, cell)
     nk = ew.n_kvectors
@@ -218,9 +221,13 @@ def test_batched_structure_factor_update(ctx, oracle):
         new = old.copy()
         for k in "xyz":
             new[k] += rng.normal() * 0.6
-        moves.append((new, old))
-    packed = np.concatenate([np.concatenate([n, o]) for n, o in moves])
-    d = batch.delta(packed, 6, [3] * n_sys, [3] * n_sys)
+        kind = s % 3 if sphere else 2
+        moves.append((new if kind != 1 else new[:0], old if kind != 0 else old[:0]))
+    packed = np.zeros(6 * n_sys, dtype=moves[0][1].dtype if len(moves[0][1]) else moves[0][0].dtype)
+    for s, (new, old) in enumerate(moves):
+        packed[6 * s:6 * s + len(new)] = new
+        packed[6 * s + len(new):6 * s + len(new) + len(old)] = old
+    d = batch.delta(packed, 6, [len(m[0]) for m in moves], [len(m[1]) for m in moves])
     trials = []
     for s in range(n_sys):
         new, old = moves[s]

@@ -25,7 +25,7 @@ from raspa3_b200.synthetic import replicate, synthetic_forcefield, synthetic_fra
 
 pytestmark = pytest.mark.gpu
 BETA = beta_of(300.0)
-N_RUNS = 8  # independent runs per side in the loading comparison
+N_RUNS = 16  # independent runs per side in the loading comparison
 RECORDED = 50000  # recorded moves per run after 3000 discarded equilibration moves
 
 

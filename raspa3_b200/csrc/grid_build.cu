@@ -591,16 +591,21 @@ __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1
 // ---------------------------------------------------------------------------------------------------------------------
 // FP32C rectangular grids with packed FP32 arithmetic (sm_100a f32x2 FMA / multiply / add).
 //
-// Each thread owns two grid points of its brick column, four planes apart along z: (i, j, k) and (i, j, k + 2) in a
+// Each thread owns two grid points of its brick column, two planes apart along z: (i, j, k) and (i, j, k + 2) in a
 // brick of 8 x 8 x 4 points (128 threads). The two points share dx and dy to every staged image, and every operation
 // after dz is one packed instruction for both pairs; the reciprocal, reciprocal square root and base-2 exponential
-// stay scalar. A lane whose pair is outside the cutoff is masked by zeroing its parameters (its factors are then 0).
+// stay scalar. Each warp compacts the staged images within reach of its own 8 x 4 x 2 points into an index list and
+// runs over it without branches (independent iterations the compiler can interleave): a lane whose pair is outside
+// the cutoff is masked by zeroing its parameters, so its factors and terms are exactly 0.
 // FP32 partial sums per staged chunk are added into FP64 sums kept in shared memory. The unit-charge Ewald grid keeps
 // the near-image list of gridKernel: images within kNearRadius + R of the brick centre, energy in FP64.
 // ---------------------------------------------------------------------------------------------------------------------
 constexpr int kPackThreads = 128;
 constexpr int kPackPer = 4;
 constexpr int kPackChunk = kPackThreads * kPackPer;
+// candidate iterations unrolled in the packed kernels (measured on B200: 3 for the Ewald kernel, 4 for Lennard-Jones)
+constexpr int kPackUnrollEwald = 3;
+constexpr int kPackUnrollLJ = 4;
 
 __device__ __forceinline__ float2 bc(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
@@ -612,18 +617,34 @@ struct Factor2
   float2 e, f1, f2, f3;
 };
 
-// ewaldFactor<float> for two pairs; cq is zero on a masked lane
-__device__ __forceinline__ Factor2 ewaldFactor2(float2 rr, float2 cq, float alpha)
+// ewaldFactor<float> for two pairs; cq is zero on a masked lane. The first- and third-derivative factors come out with
+// their signs flipped (f1 = C q (etr + ec) / r^3 and f3 = C q (etr (4 a^2 + 10 a + 15) + 15 ec) / r^7, a = alpha^2 r^2,
+// both positive): the channels they feed are negated once when the chunk's sums are folded into FP64.
+struct EwaldConst
+{
+  float2 g, half_alpha, etr, two_a2, four_a4, ten_a2;
+};
+__device__ __forceinline__ EwaldConst ewaldConst(float alpha)
+{
+  const float a2 = alpha * alpha;
+  EwaldConst c;
+  c.g = bc(-a2 * 1.4426950408889634f);           // exp(-alpha^2 r^2) = 2^(g r^2)
+  c.half_alpha = bc(0.5f * alpha);
+  c.etr = bc(alpha * 1.1283791670955126f);       // 2 alpha / sqrt(pi)
+  c.two_a2 = bc(2.0f * a2);
+  c.four_a4 = bc(4.0f * a2 * a2);
+  c.ten_a2 = bc(10.0f * a2);
+  return c;
+}
+__device__ __forceinline__ Factor2 ewaldFactor2(float2 rr, float2 cq, const EwaldConst& k)
 {
   const float2 invr = make_float2(rgd::rsqrtApprox(rr.x), rgd::rsqrtApprox(rr.y));
   const float2 r = mul2(rr, invr);
-  const float2 ar2 = mul2(rr, bc(alpha * alpha));
-  const float2 g = mul2(ar2, bc(-1.4426950408889634f));
+  const float2 g = mul2(rr, k.g);
   float2 ex;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(ex.x) : "f"(g.x));
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(ex.y) : "f"(g.y));
-  const float2 x = mul2(r, bc(alpha));
-  const float2 tden = fma2(x, bc(0.5f), bc(1.0f));
+  const float2 tden = fma2(r, k.half_alpha, bc(1.0f));
   const float2 t = make_float2(rgd::rcpApprox(tden.x), rgd::rcpApprox(tden.y));
   // rgd::erfcFromExp's polynomial in t, packed
   float2 R = bc(-0.02496027760207653f);
@@ -636,18 +657,19 @@ __device__ __forceinline__ Factor2 ewaldFactor2(float2 rr, float2 cq, float alph
   R = fma2(R, t, bc(0.25453805923461914f));
   R = fma2(R, t, bc(0.2858136296272278f));
   R = fma2(R, t, bc(-0.00021772264153696597f));
-  const float2 ec = mul2(ex, R);
-  const float2 etr = mul2(mul2(x, ex), bc(1.1283791670955126f));  // 2 alpha r exp(-alpha^2 r^2) / sqrt(pi)
-  const float2 invrr = mul2(invr, invr);
-  const float2 i3 = mul2(invr, invrr);
-  const float2 i5 = mul2(i3, invrr);
-  const float2 i7 = mul2(i5, invrr);
-  const float2 ncq = mul2(cq, bc(-1.0f));
+  const float2 ec = mul2(ex, R);                 // erfc(alpha r)
+  const float2 etr = mul2(mul2(r, ex), k.etr);   // 2 alpha r exp(-alpha^2 r^2) / sqrt(pi)
+  const float2 q1 = mul2(cq, invr);              // C q / r
+  const float2 i2 = mul2(invr, invr);
+  const float2 s1 = mul2(q1, i2);
+  const float2 s2 = mul2(s1, i2);
+  const float2 s3 = mul2(s2, i2);
+  const float2 ec3 = mul2(ec, bc(3.0f));
   Factor2 f;
-  f.e = mul2(mul2(cq, ec), invr);
-  f.f1 = mul2(mul2(ncq, add2(etr, ec)), i3);
-  f.f2 = mul2(mul2(cq, fma2(etr, fma2(ar2, bc(2.0f), bc(3.0f)), mul2(ec, bc(3.0f)))), i5);
-  f.f3 = mul2(mul2(ncq, fma2(etr, fma2(fma2(ar2, bc(4.0f), bc(10.0f)), ar2, bc(15.0f)), mul2(ec, bc(15.0f)))), i7);
+  f.e = mul2(ec, q1);
+  f.f1 = mul2(add2(etr, ec), s1);
+  f.f2 = mul2(fma2(etr, fma2(rr, k.two_a2, bc(3.0f)), ec3), s2);
+  f.f3 = mul2(fma2(etr, fma2(fma2(rr, k.four_a4, k.ten_a2), rr, bc(15.0f)), mul2(ec3, bc(5.0f))), s3);
   return f;
 }
 
@@ -724,6 +746,7 @@ __global__ void __launch_bounds__(kPackThreads, 4) gridKernelPacked(GridParams p
   double* sums = reinterpret_cast<double*>(smem_raw + sizeof(float4) * kPackChunk *
                                                          (EWALD ? 3 : 1 + NP));  // [slot][thread]
   __shared__ int warp_sums[33];
+  __shared__ unsigned short wlists[(kPackThreads / 32) * kPackChunk];  // per warp: indices of its candidates
 
   const int tid = threadIdx.x;
   const int lx = tid & 7, ly = (tid >> 3) & 7, lz = tid >> 6;
@@ -742,7 +765,16 @@ __global__ void __launch_bounds__(kPackThreads, 4) gridKernelPacked(GridParams p
   const float px = static_cast<float>(qx), py = static_cast<float>(qy);
   const float2 pz = make_float2(static_cast<float>(qz0), static_cast<float>(qz1));
   const float rc2 = static_cast<float>(p.rc2);
-  const float alpha = static_cast<float>(p.alpha);
+  const EwaldConst ek = ewaldConst(static_cast<float>(p.alpha));
+  // the warp's points: x in [0, 7], y in [4 (warp & 1), + 3], z in {lz, lz + 2} (grid steps within the brick); its
+  // box centre relative to the brick centre and its half-diagonal R_w, plus a margin for FP32 rounding
+  const int warp = tid >> 5, lane = tid & 31;
+  const double hx = p.delta[0] * cx, hy = p.delta[1] * cy, hz = p.delta[2] * cz;
+  const float3 wc = make_float3(0.0f, static_cast<float>((4 * (warp & 1) - 2) * hy),
+                                static_cast<float>(((warp >> 1) - 0.5) * hz));
+  const double rw = sqrt(p.rc2) + sqrt(12.25 * hx * hx + 2.25 * hy * hy + hz * hz) + 1e-3;
+  const float rw2 = static_cast<float>(rw * rw);
+  unsigned short* wl = wlists + warp * kPackChunk;
 
 #pragma unroll
   for (int s = 0; s < kSlots; ++s) sums[s * kPackThreads + tid] = 0.0;
@@ -800,14 +832,37 @@ __global__ void __launch_bounds__(kPackThreads, 4) gridKernelPacked(GridParams p
     }
     __syncthreads();
 
+    // this warp's candidates: the staged images within rc + R_w of the warp's own point box (a superset of those within
+    // rc of any of its points), indices in staging order
+    int nw = 0;
+    for (int b0 = 0; b0 < total; b0 += 32)
+    {
+      const int c = b0 + lane;
+      bool in = false;
+      if (c < total)
+      {
+        const float4 a = cpos[c];
+        const float ex = a.x - wc.x, ey = a.y - wc.y, ez = a.z - wc.z;
+        in = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < rw2;
+      }
+      const unsigned ballot = __ballot_sync(0xffffffffu, in);
+      if (in) wl[nw + __popc(ballot & ((1u << lane) - 1u))] = static_cast<unsigned short>(c);
+      nw += __popc(ballot);
+    }
+    __syncwarp();
+
+    // every candidate of the list for both points of every lane, branch-free: a lane whose pair is outside the cutoff
+    // has its charge (Ewald) or its epsilon and shift (Lennard-Jones) zeroed, so its factors and terms are exactly 0
     float2 P[NP][8];
 #pragma unroll
     for (int q = 0; q < NP; ++q)
 #pragma unroll
       for (int ch = 0; ch < 8; ++ch) P[q][ch] = bc(0.0f);
-#pragma unroll 2
-    for (int c = 0; c < total; ++c)
+    constexpr int kUnroll = EWALD ? kPackUnrollEwald : kPackUnrollLJ;
+#pragma unroll kUnroll
+    for (int w = 0; w < nw; ++w)
     {
+      const int c = wl[w];
       const float4 a = cpos[c];
       const float dx = px - a.x, dy = py - a.y;
       const float2 dz = add2(pz, bc(-a.z));
@@ -815,27 +870,24 @@ __global__ void __launch_bounds__(kPackThreads, 4) gridKernelPacked(GridParams p
       rr.x = fmaxf(rr.x, 0.1f);
       rr.y = fmaxf(rr.y, 0.1f);
       const bool in0 = rr.x < rc2, in1 = rr.y < rc2;
-      if (in0 || in1)
+      if (COUNT) npairs += (in0 && valid0 ? 1 : 0) + (in1 && valid1 ? 1 : 0);
+      if constexpr (EWALD)
       {
-        if (COUNT) npairs += (in0 && valid0 ? 1 : 0) + (in1 && valid1 ? 1 : 0);
-        if constexpr (EWALD)
-        {
-          const Factor2 f = ewaldFactor2(rr, make_float2(in0 ? a.w : 0.0f, in1 ? a.w : 0.0f), alpha);
-          addPair2<true>(P[0], f, dx, dy, dz);
-        }
-        else
-        {
-          const float2 inv = make_float2(rgd::rcpApprox(rr.x), rgd::rcpApprox(rr.y));
-          const float2 inv2 = mul2(inv, inv);
-          const float2 inv3 = mul2(inv2, inv);
+        const Factor2 f = ewaldFactor2(rr, make_float2(in0 ? a.w : 0.0f, in1 ? a.w : 0.0f), ek);
+        addPair2<true>(P[0], f, dx, dy, dz);
+      }
+      else
+      {
+        const float2 inv = make_float2(rgd::rcpApprox(rr.x), rgd::rcpApprox(rr.y));
+        const float2 inv2 = mul2(inv, inv);
+        const float2 inv3 = mul2(inv2, inv);
 #pragma unroll
-          for (int q = 0; q < NP; ++q)
-          {
-            const float4 pq = cpar[q * kPackChunk + c];
-            const Factor2 f = ljFactor2<TYPE>(inv, inv2, inv3, make_float2(in0 ? pq.x : 0.0f, in1 ? pq.x : 0.0f),
-                                              pq.y, make_float2(in0 ? pq.z : 0.0f, in1 ? pq.z : 0.0f));
-            addPair2<true>(P[q], f, dx, dy, dz);
-          }
+        for (int q = 0; q < NP; ++q)
+        {
+          const float4 pq = cpar[q * kPackChunk + c];
+          const Factor2 f = ljFactor2<TYPE>(inv, inv2, inv3, make_float2(in0 ? pq.x : 0.0f, in1 ? pq.x : 0.0f),
+                                            pq.y, make_float2(in0 ? pq.z : 0.0f, in1 ? pq.z : 0.0f));
+          addPair2<true>(P[q], f, dx, dy, dz);
         }
       }
     }
@@ -858,7 +910,7 @@ __global__ void __launch_bounds__(kPackThreads, 4) gridKernelPacked(GridParams p
           if (in1) ne1 += nearEwaldEnergy(rr1, a.w, p.alpha);
           const float cq = static_cast<float>(a.w);
           const Factor2 f = ewaldFactor2(make_float2(static_cast<float>(rr0), static_cast<float>(rr1)),
-                                         make_float2(in0 ? cq : 0.0f, in1 ? cq : 0.0f), alpha);
+                                         make_float2(in0 ? cq : 0.0f, in1 ? cq : 0.0f), ek);
           addPair2<false>(P[0], f, static_cast<float>(dx), static_cast<float>(dy),
                           make_float2(static_cast<float>(dz0), static_cast<float>(dz1)));
         }
@@ -876,6 +928,11 @@ __global__ void __launch_bounds__(kPackThreads, 4) gridKernelPacked(GridParams p
         {
           e0 += ne0;
           e1 += ne1;
+        }
+        if (EWALD && (ch == 1 || ch == 2 || ch == 3 || ch == 7))
+        {
+          e0 = -e0;  // ewaldFactor2's sign-flipped f1 and f3
+          e1 = -e1;
         }
         sums[s * kPackThreads + tid] += e0;
         sums[(s + 1) * kPackThreads + tid] += e1;

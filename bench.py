@@ -373,6 +373,7 @@ def run_alkane(args, ctx, peak_fp32, world, rank, dist, torch):
 
 MIXTURE_EQUIL = 2000
 MIXTURE_MOVES = 20000
+MIXTURE_BLOCKS_PER_SYSTEM = 4  # CTAs per system in the many-systems run: 37 systems on 148 SMs
 
 
 def run_mixture(args, ctx, world, rank, dist, torch):
@@ -459,13 +460,14 @@ def run_mixture(args, ctx, world, rank, dist, torch):
                                                "by its grid barriers, not by memory"},
            "e2e": {"value": world * (MIXTURE_MOVES // 4) / e2e_secs, "unit": "MC move attempts/s",
                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 176}}
-    # several independent copies of the system at once: one cooperative launch, each copy on its own quarter of the
+    # many independent copies of the system at once: one cooperative launch, each copy on MIXTURE_BLOCKS_PER_SYSTEM
     # SMs (rg_mixture_run_many), the way the GPU is used for a batch of systems rather than a single chain
-    n_sys, sms = 4, torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    n_sys = sms // MIXTURE_BLOCKS_PER_SYSTEM
     many = []
     for s in range(n_sys):
         m = native.Mixture(d["system"], d["ewald"], comps, beta, [fugacity_of(1e5), fugacity_of(1e5)], d["xyz"],
-                           d["comp"], max_molecules=6000, seed=100 + 10 * rank + s, n_blocks=sms // n_sys)
+                           d["comp"], max_molecules=6000, seed=100 + 10 * rank + s, n_blocks=MIXTURE_BLOCKS_PER_SYSTEM)
         m.set_state(e0, sk0)
         for c, pr in enumerate(props):
             m.set_proposal(c, pr, d["unit_cell"])
@@ -484,7 +486,7 @@ def run_mixture(args, ctx, world, rank, dist, torch):
     xyz_m, comp_m = many[0].positions()
     e_many = total_energy(d["system"], d["ewald"], ff, comps, xyz_m, comp_m)
     out["several_systems"] = {
-        "systems": n_sys, "blocks_per_system": sms // n_sys, "moves_per_system": MIXTURE_MOVES,
+        "systems": n_sys, "blocks_per_system": MIXTURE_BLOCKS_PER_SYSTEM, "moves_per_system": MIXTURE_MOVES,
         "value": world * n_sys * MIXTURE_MOVES / secs_many, "unit": "MC move attempts/s (all systems)",
         "ms": secs_many * 1e3, "status": [r_["status"] for r_ in rm],
         "drift_relative_first_system": abs(rm[0]["energy"] - e_many) / max(1.0, abs(e_many)),

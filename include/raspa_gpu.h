@@ -701,9 +701,12 @@ rg_status rg_mixture_set_state(rg_mixture* mixture, double energy, const double*
  * accumulates the loading and energy averages. Results, positions and structure factors are read afterwards. */
 rg_status rg_mixture_run(rg_mixture* mixture, int64_t moves, int record);
 /* Several independent mixtures advanced by one cooperative launch: system s runs on CTAs [s B, (s + 1) B), B the
- * CTA count every one of them was created with (rg_mixture_params.n_blocks, the same for all), so n small systems
- * share the GPU instead of each leaving most SMs idle. All on one rg_ctx; n <= 8 and n B CTAs must fit on the GPU
- * at once (one CTA per SM). No counterpart in the reference, whose systems run on separate threads. */
+ * CTA count every one of them was created with (rg_mixture_params.n_blocks, the same for all), so n systems share the
+ * GPU instead of each leaving most SMs idle. All on one rg_ctx, created from the same system, Ewald state, components
+ * and parameters (they may differ in their molecules and seeds; RG_ERR_INVALID_ARGUMENT otherwise); n <= 148 and n B
+ * CTAs must fit on the GPU at once (one CTA per SM). Fewer CTAs per system give more aggregate moves per second as
+ * long as a system's k-vectors fit (at kmax 12, 2 CTAs). No counterpart in the reference, whose systems run on
+ * separate threads. */
 rg_status rg_mixture_run_many(rg_mixture* const* mixtures, int n, int64_t moves, int record);
 rg_status rg_mixture_results(rg_mixture* mixture, rg_mixture_result* out);
 /* Test of the bounded grid-barrier wait (no counterpart in the reference, whose moves run on one CPU thread): in the

@@ -44,12 +44,11 @@ constexpr int kMaxTrials = 12;
 constexpr int kMaxItems = 96;          // trial atoms of one phase
 constexpr int kMaxCand = kMaxTrials;   // Ewald candidates of one phase
 constexpr int kMaxCandAtoms = 2 * kMaxAtoms;
-constexpr int kMaxKPerCta = 384;  // k-vectors of one CTA's range (in dynamic shared memory)
-constexpr int kMaxSystems = 8;    // independent systems of one launch (rg_mixture_run_many)
+constexpr int kEwTile = 256;      // k-vectors per tile of the candidates' energy sums
+static_assert(kMaxCand <= 2 * kWarps, "two candidates per warp in the energy sums");
 constexpr int kMaxTypes = 16;
 constexpr int kRow = kMaxItems + kMaxCand + 4;  // columns of partial sums per CTA (last 4: overlap-bit words)
 constexpr int kMaxBlocks = 256;                 // CTAs of the cooperative launch (lanes x 8 in the column sums)
-constexpr int kSlice = 512;                     // molecule sites of a CTA's slice staged in shared memory per phase
 constexpr int kFwSlice = 512;                   // framework atoms of a CTA's slice kept in shared memory
 constexpr long long kSpinLimit = 1ll << 22;
 constexpr int kStats = 24;
@@ -90,15 +89,25 @@ struct Params
   const double* temp;
   double uc[3][3], uic[3][3];
   int rep[3];
+  // framework atoms, for trial atoms whose type has no VDW grid (explicit pairs; n_fw = 0 when every type has one)
+  int n_fw;
+  float rc2_fw;
+  int km[3];       // kmax per axis: the phasor tables hold exp(2 pi i j s) for j = 0..km[d]
+  int tabK;        // table stride: max(km) + 1
+  int group;                // CTAs of this system in the launch; the system's CTA index is blockIdx.x % group
+  int kpc;                  // k-vectors per CTA (the stride of the per-CTA k arrays in dynamic shared memory)
+  int nslice;               // molecule sites of a CTA's slice staged in shared memory per phase (any rest from L2)
+};
+
+// The state of one system: its molecules, running energy, statistics and structure factors, its launch flags and
+// its copies of the pair table and framework atoms. Everything else (Params) is shared by the systems of one launch.
+struct State
+{
   unsigned long long seed;
   const float4* ljf;  // [kMaxTypes^2]: 4 eps, sigma^2, shift, lj flag
   const float* qtype; // charge per type (the pseudo-atom charge)
-  // framework atoms, for trial atoms whose type has no VDW grid (explicit pairs; n_fw = 0 when every type has one)
   const int4* fwx;    // [n_fw] fixed point, .w = type
   const float* fwq;   // [n_fw] charges
-  int n_fw;
-  float rc2_fw;
-  // state
   double4* pos;    // [capacity * na] Cartesian
   int4* fx;        // [capacity * na] fixed point, .w = type | molecule << 8
   int* comp_of;    // [capacity]
@@ -109,16 +118,15 @@ struct Params
   long long* move_base;
   double* stats;   // attempted[5], accepted[5], sum_n[4], sum_energy, samples
   double2* sk;     // [nk]
-  int km[3];       // kmax per axis: the phasor tables hold exp(2 pi i j s) for j = 0..km[d]
-  int tabK;        // table stride: max(km) + 1
   double* part;    // [2][kRow][group]: partial sums, column-major, two buffers alternating by phase
   unsigned long long* bar;  // [0] barrier arrivals in this launch (zeroed before each launch), [1] error flag
   int record;
-  int group;                // CTAs of this system in the launch; the system's CTA index is blockIdx.x % group
-  int kpc;                  // k-vectors per CTA (the stride of the per-CTA k arrays in dynamic shared memory)
   long long spin_limit;     // polls before a barrier wait gives up (kSpinLimit; shorter only in the wait test)
   int absent_cta;           // wait test: this CTA does not arrive at the first barrier of a launch (-1: none)
 };
+
+// This CTA's system state, copied from global memory at the start of the launch (every device function reads it).
+__shared__ State gs;
 
 enum : uint32_t
 {
@@ -169,7 +177,7 @@ struct Shared
 
 __device__ __forceinline__ double2 urand(const Params& p, long long move, uint32_t sl)
 {
-  return rgd::uniform2(p.seed, 0, move, sl);
+  return rgd::uniform2(gs.seed, 0, move, sl);
 }
 
 __device__ __forceinline__ uint32_t fixOf(double s)
@@ -236,24 +244,24 @@ __device__ bool gridBarrier(const Params& p, Shared& sh)
   {
     const unsigned long long target = static_cast<unsigned long long>(sh.gen + 1) * p.group;
     // the wait test leaves one arrival out of the first barrier, so that every CTA's bounded wait runs out
-    const bool absent = static_cast<int>(blockIdx.x) % p.group == p.absent_cta && sh.gen == 0;
-    unsigned long long v = absent ? loadAcquire(&p.bar[0]) : addRelease(&p.bar[0], 1ull) + 1ull;
+    const bool absent = static_cast<int>(blockIdx.x) % p.group == gs.absent_cta && sh.gen == 0;
+    unsigned long long v = absent ? loadAcquire(&gs.bar[0]) : addRelease(&gs.bar[0], 1ull) + 1ull;
     long long spins = 0;
     while (v < target)
     {
-      if (++spins > p.spin_limit)
+      if (++spins > gs.spin_limit)
       {
-        atomicExch(&p.bar[1], 1ull);
+        atomicExch(&gs.bar[1], 1ull);
         sh.fail = 1;
         break;
       }
-      if ((spins & 63) == 0 && loadRelaxed(&p.bar[1]) != 0ull)
+      if ((spins & 63) == 0 && loadRelaxed(&gs.bar[1]) != 0ull)
       {
         sh.fail = 1;
         break;
       }
       __nanosleep(32);
-      v = loadAcquire(&p.bar[0]);
+      v = loadAcquire(&gs.bar[0]);
     }
     sh.gen += 1;
   }
@@ -262,18 +270,17 @@ __device__ bool gridBarrier(const Params& p, Shared& sh)
 }
 
 // Dynamic shared memory: the Ewald phasor tables (kMaxCand x kMaxCandAtoms x 3 axes x tabK), this CTA's molecule
-// sites staged per phase, and its framework atoms (explicit pairs of grid-less types) kept for the launch.
+// sites staged per phase, its framework atoms (explicit pairs of grid-less types) kept for the launch, and its k-range.
 struct Dyn
 {
   double2* phasor;
-  int4* slice;  // [kSlice]
+  int4* slice;  // [nslice]
   int4* fws;    // [kFwSlice]
   float* fwq;   // [kFwSlice]
+  double* ek;   // [kMaxCand][kEwTile]: the candidates' energy terms of one tile of k-vectors
   // this CTA's k-range for the whole launch: S(k) (only this CTA updates it; written back at the end of the launch),
-  // the structure-factor change and energy change of each candidate, the k-vectors and prefactors
+  // the prefactors and the k-vectors
   double2* ks;  // [kpc]
-  double2* dk;  // [kMaxCand][kpc]
-  double* ek;   // [kMaxCand][kpc]
   double* kt;   // [kpc]
   char4* kv;    // [kpc]
 };
@@ -283,11 +290,12 @@ __host__ __device__ constexpr size_t phasorBytes(int tabK)
 }
 __host__ __device__ constexpr size_t kRangeBytes(int kpc)
 {
-  return static_cast<size_t>(kpc) * (sizeof(double2) * (1 + kMaxCand) + sizeof(double) * (1 + kMaxCand) + sizeof(char4));
+  return static_cast<size_t>(kpc) * (sizeof(double2) + sizeof(double) + sizeof(char4));
 }
-__host__ __device__ constexpr size_t dynBytes(int tabK, int kpc)
+__host__ __device__ constexpr size_t dynBytes(int tabK, int kpc, int nslice)
 {
-  return phasorBytes(tabK) + sizeof(int4) * (kSlice + kFwSlice) + sizeof(float) * kFwSlice + kRangeBytes(kpc);
+  return phasorBytes(tabK) + sizeof(int4) * (static_cast<size_t>(nslice) + kFwSlice) + sizeof(float) * kFwSlice +
+         sizeof(double) * kMaxCand * kEwTile + kRangeBytes(kpc);
 }
 __device__ __forceinline__ Dyn dynOf(const Params& p)
 {
@@ -295,29 +303,67 @@ __device__ __forceinline__ Dyn dynOf(const Params& p)
   Dyn d;
   d.phasor = reinterpret_cast<double2*>(dynSmem);
   d.slice = reinterpret_cast<int4*>(dynSmem + phasorBytes(p.tabK));
-  d.fws = d.slice + kSlice;
+  d.fws = d.slice + p.nslice;
   d.fwq = reinterpret_cast<float*>(d.fws + kFwSlice);
-  d.ks = reinterpret_cast<double2*>(d.fwq + kFwSlice);
-  d.dk = d.ks + p.kpc;
-  d.ek = reinterpret_cast<double*>(d.dk + kMaxCand * p.kpc);
-  d.kt = d.ek + kMaxCand * p.kpc;
+  d.ek = reinterpret_cast<double*>(d.fwq + kFwSlice);
+  d.ks = reinterpret_cast<double2*>(d.ek + kMaxCand * kEwTile);
+  d.kt = reinterpret_cast<double*>(d.ks + p.kpc);
   d.kv = reinterpret_cast<char4*>(d.kt + p.kpc);
   return d;
 }
 
-// Lennard-Jones + real-space Ewald of trial atom B (type bt, charge qb) with partner P (fixed point, .w & 0xff = type;
-// charge qP), FP32 from the exact fixed-point displacement (the uint32 wrap is the minimum image), added to acc in FP64.
-__device__ __forceinline__ void pairTerm(const Params& p, const Shared& sh, int4 B, int bt, float qb, int4 P, float qP,
-                                         float rc2v, double& acc, bool& ov)
+// Structure-factor change of Ewald candidate c at k-vector kv: sum over its atoms of q exp(2 pi i k.s), from the
+// phasor tables of the current phase (ewald.cpp:1043-1244).
+__device__ __forceinline__ double2 candidateDelta(const Params& p, const Shared& sh, const double2* phasor, int c,
+                                                  char4 kv)
 {
-  const int pt = P.w & 0xff;
+  double2 d = make_double2(0.0, 0.0);
+  for (int a = 0; a < sh.cn[c]; ++a)
+  {
+    const double2* t = phasor + static_cast<long long>(c * kMaxCandAtoms + a) * 3 * p.tabK;
+    double2 ex = t[abs(kv.x)], ey = t[p.tabK + abs(kv.y)], ez = t[2 * p.tabK + abs(kv.z)];
+    if (kv.x < 0) ex.y = -ex.y;
+    if (kv.y < 0) ey.y = -ey.y;
+    if (kv.z < 0) ez.y = -ez.y;
+    const double2 exy = make_double2(ex.x * ey.x - ex.y * ey.y, ex.x * ey.y + ex.y * ey.x);
+    const double q = sh.cq[c][a];
+    d.x += q * (exy.x * ez.x - exy.y * ez.y);
+    d.y += q * (exy.x * ez.y + exy.y * ez.x);
+  }
+  return d;
+}
+
+// The accepted candidate's structure-factor change added to this CTA's S(k) range (the phasor tables of the phase
+// that evaluated it are still in shared memory).
+__device__ void addCandidate(const Params& p, const Shared& sh, const Dyn& dy, int c, int nkr)
+{
+  for (int kk = threadIdx.x; kk < nkr; kk += kThreads)
+  {
+    const double2 d = candidateDelta(p, sh, dy.phasor, c, dy.kv[kk]);
+    dy.ks[kk].x += d.x;
+    dy.ks[kk].y += d.y;
+  }
+}
+
+// Squared distance of trial atom B and partner P (fixed point) in FP32 from the exact fixed-point displacement (the
+// uint32 wrap is the minimum image).
+__device__ __forceinline__ float pairDistance2(const Params& p, int4 B, int4 P)
+{
   const float f0 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.x) - static_cast<uint32_t>(P.x))) * kFix;
   const float f1 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.y) - static_cast<uint32_t>(P.y))) * kFix;
   const float f2 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.z) - static_cast<uint32_t>(P.z))) * kFix;
   const float rx = fmaf(p.hf[0][0], f0, fmaf(p.hf[1][0], f1, p.hf[2][0] * f2));
   const float ry = fmaf(p.hf[0][1], f0, fmaf(p.hf[1][1], f1, p.hf[2][1] * f2));
   const float rz = fmaf(p.hf[0][2], f0, fmaf(p.hf[1][2], f1, p.hf[2][2] * f2));
-  const float rr = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+  return fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+}
+
+// Lennard-Jones + real-space Ewald of trial atom B (type bt, charge qb) with partner P at squared distance rr
+// (.w & 0xff = type; charge qP), FP32, added to acc in FP64.
+__device__ __forceinline__ void pairEnergy(const Params& p, const Shared& sh, int bt, float qb, int4 P, float qP,
+                                           float rr, float rc2v, double& acc, bool& ov)
+{
+  const int pt = P.w & 0xff;
   if (rr < rc2v)
   {
     const float4 q = sh.tab[bt * kMaxTypes + pt];
@@ -344,6 +390,12 @@ __device__ __forceinline__ void pairTerm(const Params& p, const Shared& sh, int4
   }
 }
 
+__device__ __forceinline__ void pairTerm(const Params& p, const Shared& sh, int4 B, int bt, float qb, int4 P, float qP,
+                                         float rc2v, double& acc, bool& ov)
+{
+  pairEnergy(p, sh, bt, qb, P, qP, pairDistance2(p, B, P), rc2v, acc, ov);
+}
+
 // One phase: energies of sh.nta trial atoms (framework + molecules other than `skip`) and the Ewald energy change of
 // sh.ncand candidates, each summed over the whole grid into sh.tot[0, nta) and sh.tot[nta, nta + ncand); overlap bits
 // per trial atom in sh.ovl. vdwOf/qOf: the framework grid and charge of each trial atom (set by the caller in
@@ -355,7 +407,7 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
   const int nta = sh.nta, ncand = sh.ncand;
   const int ns = sh.n * p.na;
   const int chunk = (ns + G - 1) / G, s0 = min(ns, cta * chunk), s1 = min(ns, s0 + chunk);
-  const int nst = min(s1 - s0, kSlice);
+  const int nst = min(s1 - s0, p.nslice);
   const Dyn dy = dynOf(p);
   if (tid < 4)
   {
@@ -366,9 +418,13 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
   __syncthreads();
   // 0. framework grids of the trial atoms this CTA owns (b = cta, cta + G, ..), by 16 lanes of the last warp: lane l
   //    takes corner l & 7 of the VDW grid (l < 8) or of the unit-charge Ewald grid (l >= 8). Meanwhile the other warps
-  //    stage this CTA's slice of molecule sites in shared memory. The grid branch of
-  //    interactions_framework_molecule.cpp: only an atom whose type has a VDW grid takes it (its charge term then
-  //    comes from the Ewald grid); any other atom sees the framework atoms explicitly (below).
+  //    stage this CTA's slice of molecule sites in shared memory and run the pairs (1.), so that the grid loads'
+  //    latency overlaps them. The grid branch of interactions_framework_molecule.cpp: only an atom whose type has a
+  //    VDW grid takes it (its charge term then comes from the Ewald grid); any other atom sees the framework atoms
+  //    explicitly (below).
+  double acc = 0.0;
+  bool ov = false;
+  int b = 0;
   if (warp == kWarps - 1)
   {
     if (lane < 16)
@@ -397,33 +453,59 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
       }
   }
   else
-    for (int i = tid; i < nst; i += (kWarps - 1) * 32) dy.slice[i] = __ldcg(p.fx + s0 + i);
-  __syncthreads();
-  // 1. molecule-molecule pairs over this CTA's slice of sites (staged part from shared memory, any rest from L2)
-  double acc = 0.0;
-  bool ov = false;
-  const int streams = nta > 0 ? kThreads / nta : 0;
-  const int b = nta > 0 ? tid % nta : 0, st = nta > 0 ? tid / nta : 0;
-  if (nta > 0 && st < streams)
   {
-    const int4 B = sh.tf[b];
-    const int bt = B.w & 0xff;
-    const float qb = sh.qt[bt];
-    for (int i = st; i < s1 - s0; i += streams)
+    constexpr int kPairThreads = (kWarps - 1) * 32;
+    for (int i = tid; i < nst; i += kPairThreads) dy.slice[i] = __ldcg(gs.fx + s0 + i);
+    asm volatile("bar.sync 1, %0;" ::"n"(kPairThreads) : "memory");  // the slice is staged (warps 0 .. kWarps - 2)
+    // 1. molecule-molecule pairs over this CTA's slice of sites (staged part from shared memory, any rest from L2),
+    //    four sites per iteration into four independent sums
+    const int streams = nta > 0 ? kPairThreads / nta : 0;
+    b = nta > 0 ? tid % nta : 0;
+    const int st = nta > 0 ? tid / nta : 0;
+    if (nta > 0 && st < streams)
     {
-      const int4 P = i < kSlice ? dy.slice[i] : __ldcg(p.fx + s0 + i);
-      if ((P.w >> 8) == skip) continue;
-      pairTerm(p, sh, B, bt, qb, P, sh.qt[P.w & 0xff], p.rc2_mm, acc, ov);
-    }
-    // trial atom without a VDW grid: explicit pairs with this CTA's slice of the framework atoms
-    if (p.n_fw > 0 && atomGrid[b] == nullptr)
-    {
-      const int fchunk = (p.n_fw + G - 1) / G, fa = min(p.n_fw, cta * fchunk), fb = min(p.n_fw, fa + fchunk);
-      for (int i = st; i < fb - fa; i += streams)
+      const int4 B = sh.tf[b];
+      const int bt = B.w & 0xff;
+      const float qb = sh.qt[bt];
+      const int n = s1 - s0, ns_staged = min(n, p.nslice);
+      const float rcut2 = p.use_charge ? fmaxf(p.rc2_mm, p.rc2_c) : p.rc2_mm;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      int i = st;
+      // staged sites, four per iteration: their distances without branches (the skipped molecule's at infinity),
+      // then the energies of the few within a cutoff
+      for (; i + 3 * streams < ns_staged; i += 4 * streams)
       {
-        const bool staged = i < kFwSlice;
-        pairTerm(p, sh, B, bt, qb, staged ? dy.fws[i] : __ldg(p.fwx + fa + i), staged ? dy.fwq[i] : __ldg(p.fwq + fa + i),
-                 p.rc2_fw, acc, ov);
+        const int4 P0 = dy.slice[i], P1 = dy.slice[i + streams], P2 = dy.slice[i + 2 * streams],
+                   P3 = dy.slice[i + 3 * streams];
+        const float r0 = (P0.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P0);
+        const float r1 = (P1.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P1);
+        const float r2 = (P2.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P2);
+        const float r3 = (P3.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P3);
+        if (fminf(fminf(r0, r1), fminf(r2, r3)) < rcut2)
+        {
+          if (r0 < rcut2) pairEnergy(p, sh, bt, qb, P0, sh.qt[P0.w & 0xff], r0, p.rc2_mm, a0, ov);
+          if (r1 < rcut2) pairEnergy(p, sh, bt, qb, P1, sh.qt[P1.w & 0xff], r1, p.rc2_mm, a1, ov);
+          if (r2 < rcut2) pairEnergy(p, sh, bt, qb, P2, sh.qt[P2.w & 0xff], r2, p.rc2_mm, a2, ov);
+          if (r3 < rcut2) pairEnergy(p, sh, bt, qb, P3, sh.qt[P3.w & 0xff], r3, p.rc2_mm, a3, ov);
+        }
+      }
+      // the rest: remaining staged sites, then any beyond the staged slice from L2
+      for (; i < n; i += streams)
+      {
+        const int4 P = i < p.nslice ? dy.slice[i] : __ldcg(gs.fx + s0 + i);
+        if ((P.w >> 8) != skip) pairTerm(p, sh, B, bt, qb, P, sh.qt[P.w & 0xff], p.rc2_mm, a0, ov);
+      }
+      acc = (a0 + a1) + (a2 + a3);
+      // trial atom without a VDW grid: explicit pairs with this CTA's slice of the framework atoms
+      if (p.n_fw > 0 && atomGrid[b] == nullptr)
+      {
+        const int fchunk = (p.n_fw + G - 1) / G, fa = min(p.n_fw, cta * fchunk), fb = min(p.n_fw, fa + fchunk);
+        for (int j = st; j < fb - fa; j += streams)
+        {
+          const bool staged = j < kFwSlice;
+          pairTerm(p, sh, B, bt, qb, staged ? dy.fws[j] : __ldg(gs.fwx + fa + j),
+                   staged ? dy.fwq[j] : __ldg(gs.fwq + fa + j), p.rc2_fw, acc, ov);
+        }
       }
     }
   }
@@ -433,9 +515,10 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
   // partial sums column-major ([column][CTA]), in two buffers alternating by phase: a CTA writes the next phase's
   // partials only after every CTA has passed this phase's barrier and read this phase's, which lie in the other buffer
   const int buf = sh.phases & 1;
-  double* cols = p.part + static_cast<long long>(buf) * kRow * G;
+  double* cols = gs.part + static_cast<long long>(buf) * kRow * G;
   if (tid < nta)
   {
+    const int streams = (kWarps - 1) * 32 / nta;
     double s = 0.0;
     for (int k = 0; k < streams; ++k) s += sh.red[tid + nta * k];
     cols[static_cast<long long>(tid) * G + cta] = s + sh.fwE[tid];
@@ -468,36 +551,34 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
       }
     }
     __syncthreads();
-    for (int task = tid; task < ncand * nkr; task += kThreads)
+    // energy change of each candidate over this CTA's k-range, in tiles of kEwTile k-vectors: one (candidate, k) task
+    // per thread, then warp w sums candidates w and w + kWarps, lane j over the tiles' k-vectors j, j + 32, ..
+    double esum0 = 0.0, esum1 = 0.0;
+    for (int t0 = 0; t0 < nkr; t0 += kEwTile)
     {
-      const int c = task / nkr, kk = task - c * nkr;
-      const char4 kv = dy.kv[kk];
-      double2 d = make_double2(0.0, 0.0);
-      for (int a = 0; a < sh.cn[c]; ++a)
+      const int nt = min(kEwTile, nkr - t0);
+      for (int task = tid; task < ncand * nt; task += kThreads)
       {
-        const double2* t = phasor + static_cast<long long>(c * kMaxCandAtoms + a) * 3 * p.tabK;
-        double2 ex = t[abs(kv.x)], ey = t[p.tabK + abs(kv.y)], ez = t[2 * p.tabK + abs(kv.z)];
-        if (kv.x < 0) ex.y = -ex.y;
-        if (kv.y < 0) ey.y = -ey.y;
-        if (kv.z < 0) ez.y = -ez.y;
-        const double2 exy = make_double2(ex.x * ey.x - ex.y * ey.y, ex.x * ey.y + ex.y * ey.x);
-        const double q = sh.cq[c][a];
-        d.x += q * (exy.x * ez.x - exy.y * ez.y);
-        d.y += q * (exy.x * ez.y + exy.y * ez.x);
+        const int c = task / nt, j = task - c * nt, kk = t0 + j;
+        const double2 d = candidateDelta(p, sh, phasor, c, dy.kv[kk]);
+        const double2 sk = dy.ks[kk];
+        dy.ek[c * kEwTile + j] = dy.kt[kk] * (2.0 * (sk.x * d.x + sk.y * d.y) + (d.x * d.x + d.y * d.y));
       }
-      const double2 sk = dy.ks[kk];
-      dy.ek[c * p.kpc + kk] = dy.kt[kk] * (2.0 * (sk.x * d.x + sk.y * d.y) + (d.x * d.x + d.y * d.y));
-      dy.dk[c * p.kpc + kk] = d;
+      __syncthreads();
+      if (warp < ncand)
+        for (int j = lane; j < nt; j += 32) esum0 += dy.ek[warp * kEwTile + j];
+      if (warp + kWarps < ncand)
+        for (int j = lane; j < nt; j += 32) esum1 += dy.ek[(warp + kWarps) * kEwTile + j];
+      __syncthreads();
     }
-    __syncthreads();
-    for (int c = warp; c < ncand; c += kWarps)
-    {
-      double e = 0.0;
-      for (int kk = lane; kk < nkr; kk += 32) e += dy.ek[c * p.kpc + kk];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
-      if (lane == 0) cols[static_cast<long long>(kMaxItems + c) * G + cta] = e;
+    for (int o = 16; o > 0; o >>= 1)
+    {
+      esum0 += __shfl_xor_sync(0xffffffffu, esum0, o);
+      esum1 += __shfl_xor_sync(0xffffffffu, esum1, o);
     }
+    if (lane == 0 && warp < ncand) cols[static_cast<long long>(kMaxItems + warp) * G + cta] = esum0;
+    if (lane == 0 && warp + kWarps < ncand) cols[static_cast<long long>(kMaxItems + warp + kWarps) * G + cta] = esum1;
   }
   if (!gridBarrier(p, sh)) return false;
   // 3. totals: columns spread over the warps, lanes over the CTAs; all loads of a column are issued before any sum.
@@ -675,7 +756,7 @@ __device__ int warpSelect(double lw, bool ok, int k, double u, double* W)
 
 __device__ __forceinline__ double3 loadPos(const Params& p, int site)
 {
-  const double2* q = reinterpret_cast<const double2*>(p.pos + site);
+  const double2* q = reinterpret_cast<const double2*>(gs.pos + site);
   const double2 a = __ldcg(q), b = __ldcg(q + 1);
   return make_double3(a.x, a.y, b.x);
 }
@@ -686,8 +767,8 @@ __device__ void storeMolecule(const Params& p, int m, int cidx, const double3* x
   const Comp& c = p.comp[cidx];
   for (int i = 0; i < p.na; ++i)
   {
-    p.pos[m * p.na + i] = make_double4(x[i].x, x[i].y, x[i].z, 0.0);
-    p.fx[m * p.na + i] = toFixed(p, x[i], c.types[i] | (m << 8));
+    gs.pos[m * p.na + i] = make_double4(x[i].x, x[i].y, x[i].z, 0.0);
+    gs.fx[m * p.na + i] = toFixed(p, x[i], c.types[i] | (m << 8));
   }
 }
 
@@ -706,36 +787,41 @@ __device__ void storeOrientation(const Params& p, Shared& sh, const double** ato
   }
 }
 
-// The parameters of the systems of one launch: CTAs [s * group, (s + 1) * group) run system s.
+// One launch: the parameters its systems share and each system's state (device copies); CTAs [s * group, (s + 1) *
+// group) run system s.
+constexpr int kMaxSystems = 148;  // independent systems of one launch (rg_mixture_run_many)
 struct Launch
 {
-  Params p[kMaxSystems];
+  Params p;
+  const State* st[kMaxSystems];
 };
 static_assert(sizeof(Launch) <= 32000, "kernel parameter space");
 
 __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_constant__ Launch L, int moves)
 {
-  const Params& p = L.p[blockIdx.x / L.p[0].group];
+  const Params& p = L.p;
   const int cta = static_cast<int>(blockIdx.x) % p.group;
+  if (threadIdx.x == 0) gs = *L.st[blockIdx.x / p.group];
+  __syncthreads();
   __shared__ Shared sh;
   const int tid = threadIdx.x;
   const int na = p.na;
-  for (int i = tid; i < kMaxTypes * kMaxTypes; i += kThreads) sh.tab[i] = p.ljf[i];
-  for (int i = tid; i < kMaxTypes; i += kThreads) sh.qt[i] = p.qtype[i];
+  for (int i = tid; i < kMaxTypes * kMaxTypes; i += kThreads) sh.tab[i] = gs.ljf[i];
+  for (int i = tid; i < kMaxTypes; i += kThreads) sh.qt[i] = gs.qtype[i];
   if (tid == 0)
   {
-    sh.n = p.n_state[0];
-    for (int c = 0; c < kMaxComp; ++c) sh.count[c] = p.n_state[1 + c];
-    sh.energy = *p.energy;
+    sh.n = gs.n_state[0];
+    for (int c = 0; c < kMaxComp; ++c) sh.count[c] = gs.n_state[1 + c];
+    sh.energy = *gs.energy;
     sh.gen = 0;
-    sh.fail = loadRelaxed(&p.bar[1]) != 0ull;  // a barrier of an earlier launch timed out: do nothing
+    sh.fail = loadRelaxed(&gs.bar[1]) != 0ull;  // a barrier of an earlier launch timed out: do nothing
     sh.phases = 0;
-    for (int k = 0; k < kStats; ++k) sh.stats[k] = p.stats[k];
+    for (int k = 0; k < kStats; ++k) sh.stats[k] = gs.stats[k];
   }
   // this CTA's k-range
   const int G = p.group;
   const int kchunk = (p.nk + G - 1) / G, k0 = cta * kchunk, k1 = min(p.nk, k0 + kchunk);
-  const long long move0 = *p.move_base;
+  const long long move0 = *gs.move_base;
   __shared__ const double* atomGrid[kMaxItems];
   const Dyn dyk = dynOf(p);
   // this CTA's k-range and framework slice, kept in shared memory for the whole launch
@@ -743,7 +829,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
   {
     dyk.kv[kk] = p.kvec[k0 + kk];
     dyk.kt[kk] = p.temp[k0 + kk];
-    dyk.ks[kk] = p.sk[k0 + kk];
+    dyk.ks[kk] = gs.sk[k0 + kk];
   }
   if (p.n_fw > 0)
   {
@@ -752,8 +838,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
     const Dyn dy = dynOf(p);
     for (int i = tid; i < nf; i += kThreads)
     {
-      dy.fws[i] = p.fwx[fa + i];
-      dy.fwq[i] = p.fwq[fa + i];
+      dy.fws[i] = gs.fwx[fa + i];
+      dy.fwq[i] = gs.fwq[fa + i];
     }
   }
   __syncthreads();
@@ -789,7 +875,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
       if (tid == 0)
       {
         const Comp& cc = p.comp[c];
-        const int m = __ldcg(p.list + c * p.capacity + min(sh.count[c] - 1, static_cast<int>(sh.u[3] * sh.count[c])));
+        const int m = __ldcg(gs.list + c * p.capacity + min(sh.count[c] - 1, static_cast<int>(sh.u[3] * sh.count[c])));
         sh.m = m;
         const int dir = min(2, static_cast<int>(3.0 * sh.u[4]));
         double3 old[kMaxAtoms], nw[kMaxAtoms];
@@ -868,13 +954,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
       if (sh.accept)
       {
         if (tid == 0) storeMolecule(p, sh.m, c, sh.mol);
-        if (p.use_charge)
-          for (int kk = tid; kk < k1 - k0; kk += kThreads)
-          {
-            const double2 d = dyk.dk[kk];
-            dyk.ks[kk].x += d.x;
-            dyk.ks[kk].y += d.y;
-          }
+        if (p.use_charge) addCandidate(p, sh, dyk, 0, k1 - k0);
       }
     }
     else if (kind == 2 && sh.n < p.capacity)
@@ -975,19 +1055,13 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
           {
             const int m = sh.n;
             storeMolecule(p, m, c, sh.mol);
-            p.comp_of[m] = c;
-            p.slot[m] = sh.count[c];
-            p.list[c * p.capacity + sh.count[c]] = m;
+            gs.comp_of[m] = c;
+            gs.slot[m] = sh.count[c];
+            gs.list[c * p.capacity + sh.count[c]] = m;
             sh.count[c] += 1;
             sh.n += 1;
           }
-          if (p.use_charge)
-            for (int kk = tid; kk < k1 - k0; kk += kThreads)
-            {
-              const double2 d = dyk.dk[sh.selOrient * p.kpc + kk];
-              dyk.ks[kk].x += d.x;
-              dyk.ks[kk].y += d.y;
-            }
+          if (p.use_charge) addCandidate(p, sh, dyk, sh.selOrient, k1 - k0);
         }
       }
     }
@@ -996,7 +1070,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
       // CBMC deletion: first-bead retrace (trial 0 = old bead) and orientation retrace about the old bead
       const Comp& cc = p.comp[c];
       const int sb = cc.starting_bead;
-      if (tid == 0) sh.m = __ldcg(p.list + c * p.capacity + min(sh.count[c] - 1, static_cast<int>(sh.u[3] * sh.count[c])));
+      if (tid == 0) sh.m = __ldcg(gs.list + c * p.capacity + min(sh.count[c] - 1, static_cast<int>(sh.u[3] * sh.count[c])));
       __syncthreads();
       const int m = sh.m;
       if (tid < p.k1)
@@ -1012,17 +1086,17 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
         const int last = sh.n - 1, q = tid - 128;
         if (q == 0)
         {
-          sh.preSlot = __ldcg(p.slot + m);
+          sh.preSlot = __ldcg(gs.slot + m);
           sh.cn[0] = na;
           sh.nta = p.k1 + p.k2 * (na - 1);
           sh.ncand = p.use_charge ? 1 : 0;
         }
         else if (q == 1)
-          sh.preLastC = __ldcg(p.list + c * p.capacity + sh.count[c] - 1);
+          sh.preLastC = __ldcg(gs.list + c * p.capacity + sh.count[c] - 1);
         else if (q == 2)
-          sh.preCl = __ldcg(p.comp_of + last);
+          sh.preCl = __ldcg(gs.comp_of + last);
         else if (q == 3)
-          sh.preSl = __ldcg(p.slot + last);
+          sh.preSl = __ldcg(gs.slot + last);
         else if (q >= 4 && q < 4 + na)
           sh.preLast[q - 4] = loadPos(p, last * na + (q - 4));
         else if (q >= 8 && q < 8 + na)
@@ -1083,8 +1157,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
           // remove m from its component list, then move the last molecule into slot m (from the values read before
           // the barrier)
           const int k = sh.preSlot, lastC = sh.preLastC;
-          p.list[c * p.capacity + k] = lastC;
-          p.slot[lastC] = k;
+          gs.list[c * p.capacity + k] = lastC;
+          gs.slot[lastC] = k;
           sh.count[c] -= 1;
           const int last = sh.n - 1;
           if (m != last)
@@ -1092,19 +1166,13 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
             const int cl = sh.preCl;
             const int sl = (lastC == last) ? k : sh.preSl;
             storeMolecule(p, m, cl, sh.preLast);
-            p.comp_of[m] = cl;
-            p.slot[m] = sl;
-            p.list[cl * p.capacity + sl] = m;
+            gs.comp_of[m] = cl;
+            gs.slot[m] = sl;
+            gs.list[cl * p.capacity + sl] = m;
           }
           sh.n -= 1;
         }
-        if (p.use_charge)
-          for (int kk = tid; kk < k1 - k0; kk += kThreads)
-          {
-            const double2 d = dyk.dk[kk];
-            dyk.ks[kk].x += d.x;
-            dyk.ks[kk].y += d.y;
-          }
+        if (p.use_charge) addCandidate(p, sh, dyk, 0, k1 - k0);
       }
     }
     else if (kind == 4 && p.n_comp > 1)
@@ -1122,7 +1190,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
         sh.c = oldC;
         sh.c2 = newC;
         sh.m = sh.count[oldC] > 0
-                   ? __ldcg(p.list + oldC * p.capacity +
+                   ? __ldcg(gs.list + oldC * p.capacity +
                             min(sh.count[oldC] - 1, static_cast<int>(sh.u[5] * sh.count[oldC])))
                    : -1;
       }
@@ -1138,8 +1206,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
         const double3 first = loadPos(p, m * na + co.starting_bead);
         if (tid == 0)
         {
-          sh.preSlot = __ldcg(p.slot + m);
-          sh.preLastC = __ldcg(p.list + oldC * p.capacity + sh.count[oldC] - 1);
+          sh.preSlot = __ldcg(gs.slot + m);
+          sh.preLastC = __ldcg(gs.list + oldC * p.capacity + sh.count[oldC] - 1);
           sh.ta[0] = first;
           sh.tf[0] = toFixed(p, first, cn.types[cn.starting_bead]);
           atomGrid[0] = cn.vdw_grid[cn.starting_bead];
@@ -1222,27 +1290,21 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
             storeMolecule(p, m, newC, sh.mol);
             // move m from the old component's list to the new one's (from the values read before the barrier)
             const int k = sh.preSlot, lastC = sh.preLastC;
-            p.list[oldC * p.capacity + k] = lastC;
-            p.slot[lastC] = k;
+            gs.list[oldC * p.capacity + k] = lastC;
+            gs.slot[lastC] = k;
             sh.count[oldC] -= 1;
-            p.comp_of[m] = newC;
-            p.slot[m] = sh.count[newC];
-            p.list[newC * p.capacity + sh.count[newC]] = m;
+            gs.comp_of[m] = newC;
+            gs.slot[m] = sh.count[newC];
+            gs.list[newC * p.capacity + sh.count[newC]] = m;
             sh.count[newC] += 1;
           }
-          if (p.use_charge)
-            for (int kk = tid; kk < k1 - k0; kk += kThreads)
-            {
-              const double2 d = dyk.dk[sh.selOrient * p.kpc + kk];
-              dyk.ks[kk].x += d.x;
-              dyk.ks[kk].y += d.y;
-            }
+          if (p.use_charge) addCandidate(p, sh, dyk, sh.selOrient, k1 - k0);
         }
         c = oldC;
       }
     }
     __syncthreads();
-    if (tid == 0 && p.record)
+    if (tid == 0 && gs.record)
     {
       sh.stats[kind] += 1.0;
       sh.stats[5 + kind] += sh.accept ? 1.0 : 0.0;
@@ -1252,14 +1314,14 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
     }
     __syncthreads();
   }
-  for (int kk = tid; kk < k1 - k0; kk += kThreads) p.sk[k0 + kk] = dyk.ks[kk];
+  for (int kk = tid; kk < k1 - k0; kk += kThreads) gs.sk[k0 + kk] = dyk.ks[kk];
   if (cta == 0 && tid == 0 && !sh.fail)
   {
-    p.n_state[0] = sh.n;
-    for (int c = 0; c < kMaxComp; ++c) p.n_state[1 + c] = sh.count[c];
-    *p.energy = sh.energy;
-    *p.move_base = move0 + moves;
-    for (int k = 0; k < kStats; ++k) p.stats[k] = sh.stats[k];
+    gs.n_state[0] = sh.n;
+    for (int c = 0; c < kMaxComp; ++c) gs.n_state[1 + c] = sh.count[c];
+    *gs.energy = sh.energy;
+    *gs.move_base = move0 + moves;
+    for (int k = 0; k < kStats; ++k) gs.stats[k] = sh.stats[k];
   }
 }
 }  // namespace
@@ -1270,6 +1332,8 @@ struct rg_mixture
   rg_system* system = nullptr;
   rg_ewald* ewald = nullptr;
   Params p{};
+  State st{};
+  State* d_st = nullptr;  // device copy of st, refreshed before each launch
   int blocks = 0;
   int n_comp = 0;
   size_t smem = 0;  // dynamic shared memory of a launch: the Ewald phasor tables
@@ -1352,7 +1416,7 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   p.capacity = params->max_molecules;
   p.na = na;
   p.n_comp = n_components;
-  p.seed = params->seed;
+  x->st.seed = params->seed;
   // pair table (FP32) and the charge of each type
   std::vector<float4> ljf(kMaxTypes * kMaxTypes, make_float4(0, 0, 0, 0));
   std::vector<float> qtype(kMaxTypes, 0.0f);
@@ -1501,12 +1565,27 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   x->blocks = std::min(kMaxBlocks, params->n_blocks > 0 ? std::min(params->n_blocks, sms) : sms);
   p.group = x->blocks;
   p.kpc = std::max(1, (p.nk + x->blocks - 1) / x->blocks);
-  if (p.use_charge && p.kpc > kMaxKPerCta)
+  // shared memory: the k-range must fit; the staged slice of molecule sites takes what is left, up to a CTA's share of
+  // a full system (sites beyond the slice are read from L2)
+  cudaFuncAttributes fa{};
+  int optin = 0;
+  err = cudaFuncGetAttributes(&fa, mixtureKernel);
+  if (err == cudaSuccess) err = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+  if (err != cudaSuccess)
   {
     delete x;
-    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: more than 384 k-vectors per CTA (use more CTAs)");
+    return rg::cudaFail(ctx, err, "rg_mixture_create");
   }
-  x->smem = dynBytes(p.tabK, p.kpc);
+  const long long budget = static_cast<long long>(optin) - static_cast<long long>(fa.sharedSizeBytes) - 1024;
+  const long long fixedBytes = static_cast<long long>(dynBytes(p.tabK, p.kpc, 0));
+  if (fixedBytes + 16 * 64 > budget)
+  {
+    delete x;
+    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: the CTA's k-range does not fit in shared memory (use more CTAs)");
+  }
+  const long long share = (static_cast<long long>(p.capacity) * na + x->blocks - 1) / x->blocks;
+  p.nslice = static_cast<int>(std::max<long long>(64, std::min(share, (budget - fixedBytes) / 16)));
+  x->smem = dynBytes(p.tabK, p.kpc, p.nslice);
   err = cudaFuncSetAttribute(mixtureKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(x->smem));
   if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, mixtureKernel, kThreads, x->smem);
   if (err != cudaSuccess || perSM < 1)
@@ -1524,26 +1603,27 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   float* dq = nullptr;
   alloc(reinterpret_cast<void**>(&dljf), sizeof(float4) * ljf.size());
   alloc(reinterpret_cast<void**>(&dq), sizeof(float) * qtype.size());
-  alloc(reinterpret_cast<void**>(&p.pos), sizeof(double4) * cap * na);
-  alloc(reinterpret_cast<void**>(&p.fx), sizeof(int4) * cap * na);
-  alloc(reinterpret_cast<void**>(&p.comp_of), sizeof(int) * cap);
-  alloc(reinterpret_cast<void**>(&p.list), sizeof(int) * cap * kMaxComp);
-  alloc(reinterpret_cast<void**>(&p.slot), sizeof(int) * cap);
-  alloc(reinterpret_cast<void**>(&p.n_state), sizeof(int) * (1 + kMaxComp));
-  alloc(reinterpret_cast<void**>(&p.energy), sizeof(double));
-  alloc(reinterpret_cast<void**>(&p.move_base), sizeof(long long));
-  alloc(reinterpret_cast<void**>(&p.stats), sizeof(double) * kStats);
-  alloc(reinterpret_cast<void**>(&p.sk), sizeof(double2) * std::max(1, p.nk));
-  alloc(reinterpret_cast<void**>(&p.part), sizeof(double) * kRow * 2 * x->blocks);
-  alloc(reinterpret_cast<void**>(&p.bar), sizeof(unsigned long long) * 2);
+  alloc(reinterpret_cast<void**>(&x->st.pos), sizeof(double4) * cap * na);
+  alloc(reinterpret_cast<void**>(&x->st.fx), sizeof(int4) * cap * na);
+  alloc(reinterpret_cast<void**>(&x->st.comp_of), sizeof(int) * cap);
+  alloc(reinterpret_cast<void**>(&x->st.list), sizeof(int) * cap * kMaxComp);
+  alloc(reinterpret_cast<void**>(&x->st.slot), sizeof(int) * cap);
+  alloc(reinterpret_cast<void**>(&x->st.n_state), sizeof(int) * (1 + kMaxComp));
+  alloc(reinterpret_cast<void**>(&x->st.energy), sizeof(double));
+  alloc(reinterpret_cast<void**>(&x->st.move_base), sizeof(long long));
+  alloc(reinterpret_cast<void**>(&x->st.stats), sizeof(double) * kStats);
+  alloc(reinterpret_cast<void**>(&x->st.sk), sizeof(double2) * std::max(1, p.nk));
+  alloc(reinterpret_cast<void**>(&x->st.part), sizeof(double) * kRow * 2 * x->blocks);
+  alloc(reinterpret_cast<void**>(&x->st.bar), sizeof(unsigned long long) * 2);
+  alloc(reinterpret_cast<void**>(&x->d_st), sizeof(State));
   int4* dfwx = nullptr;
   float* dfwq = nullptr;
   alloc(reinterpret_cast<void**>(&dfwx), sizeof(int4) * hfw.size());
   alloc(reinterpret_cast<void**>(&dfwq), sizeof(float) * hfq.size());
-  p.fwx = dfwx;
-  p.fwq = dfwq;
-  p.ljf = dljf;
-  p.qtype = dq;
+  x->st.fwx = dfwx;
+  x->st.fwq = dfwq;
+  x->st.ljf = dljf;
+  x->st.qtype = dq;
   // host copies of the starting configuration
   std::vector<double4> hpos(static_cast<size_t>(cap) * na);
   std::vector<int4> hfx(static_cast<size_t>(cap) * na);
@@ -1601,21 +1681,21 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   if (err == cudaSuccess && !hfq.empty())
     err = cudaMemcpyAsync(dfwq, hfq.data(), sizeof(float) * hfq.size(), cudaMemcpyHostToDevice, sm);
   if (err == cudaSuccess)
-    err = cudaMemcpyAsync(p.pos, hpos.data(), sizeof(double4) * hpos.size(), cudaMemcpyHostToDevice, sm);
-  if (err == cudaSuccess) err = cudaMemcpyAsync(p.fx, hfx.data(), sizeof(int4) * hfx.size(), cudaMemcpyHostToDevice, sm);
+    err = cudaMemcpyAsync(x->st.pos, hpos.data(), sizeof(double4) * hpos.size(), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(x->st.fx, hfx.data(), sizeof(int4) * hfx.size(), cudaMemcpyHostToDevice, sm);
   if (err == cudaSuccess)
-    err = cudaMemcpyAsync(p.comp_of, hcomp.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, sm);
+    err = cudaMemcpyAsync(x->st.comp_of, hcomp.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, sm);
   if (err == cudaSuccess)
-    err = cudaMemcpyAsync(p.list, hlist.data(), sizeof(int) * hlist.size(), cudaMemcpyHostToDevice, sm);
-  if (err == cudaSuccess) err = cudaMemcpyAsync(p.slot, hslot.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, sm);
-  if (err == cudaSuccess) err = cudaMemcpyAsync(p.n_state, nstate, sizeof(nstate), cudaMemcpyHostToDevice, sm);
-  if (err == cudaSuccess) err = cudaMemcpyAsync(p.energy, &zero, sizeof(double), cudaMemcpyHostToDevice, sm);
-  if (err == cudaSuccess) err = cudaMemcpyAsync(p.move_base, &zl, sizeof(long long), cudaMemcpyHostToDevice, sm);
-  if (err == cudaSuccess) err = cudaMemsetAsync(p.stats, 0, sizeof(double) * kStats, sm);
-  if (err == cudaSuccess) err = cudaMemsetAsync(p.sk, 0, sizeof(double2) * std::max(1, p.nk), sm);
-  if (err == cudaSuccess) err = cudaMemsetAsync(p.bar, 0, sizeof(unsigned long long) * 2, sm);
-  p.spin_limit = kSpinLimit;
-  p.absent_cta = -1;
+    err = cudaMemcpyAsync(x->st.list, hlist.data(), sizeof(int) * hlist.size(), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(x->st.slot, hslot.data(), sizeof(int) * cap, cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(x->st.n_state, nstate, sizeof(nstate), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(x->st.energy, &zero, sizeof(double), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(x->st.move_base, &zl, sizeof(long long), cudaMemcpyHostToDevice, sm);
+  if (err == cudaSuccess) err = cudaMemsetAsync(x->st.stats, 0, sizeof(double) * kStats, sm);
+  if (err == cudaSuccess) err = cudaMemsetAsync(x->st.sk, 0, sizeof(double2) * std::max(1, p.nk), sm);
+  if (err == cudaSuccess) err = cudaMemsetAsync(x->st.bar, 0, sizeof(unsigned long long) * 2, sm);
+  x->st.spin_limit = kSpinLimit;
+  x->st.absent_cta = -1;
   if (err == cudaSuccess) err = cudaStreamSynchronize(sm);
   if (err != cudaSuccess)
   {
@@ -1645,9 +1725,9 @@ extern "C" rg_status rg_mixture_set_state(rg_mixture* x, double energy, const do
   if (sk)
   {
     if (n_doubles != 2ll * x->p.nk) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_set_state: 2 nk doubles");
-    RG_CUDA(ctx, cudaMemcpyAsync(x->p.sk, sk, sizeof(double) * n_doubles, cudaMemcpyHostToDevice, ctx->stream));
+    RG_CUDA(ctx, cudaMemcpyAsync(x->st.sk, sk, sizeof(double) * n_doubles, cudaMemcpyHostToDevice, ctx->stream));
   }
-  RG_CUDA(ctx, cudaMemcpyAsync(x->p.energy, &energy, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  RG_CUDA(ctx, cudaMemcpyAsync(x->st.energy, &energy, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return RG_OK;
 }
@@ -1659,12 +1739,17 @@ extern "C" rg_status rg_mixture_run_many(rg_mixture* const* mixtures, int n, int
     if (!mixtures[s]) return RG_ERR_INVALID_ARGUMENT;
   rg_mixture* x0 = mixtures[0];
   rg_ctx* ctx = x0->ctx;
-  if (n > kMaxSystems) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_run_many: at most 8 systems");
+  if (n > kMaxSystems) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_run_many: at most 148 systems");
   size_t smem = 0;
   for (int s = 0; s < n; ++s)
   {
     if (mixtures[s]->ctx != ctx || mixtures[s]->blocks != x0->blocks)
       return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_run_many: one context and one CTA count for all");
+    // the systems of one launch share everything but their state: same system, Ewald state, components and
+    // parameters (their molecules, seeds and statistics may differ)
+    if (std::memcmp(&mixtures[s]->p, &x0->p, sizeof(Params)) != 0)
+      return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT,
+                      "rg_mixture_run_many: the systems differ in more than their state (system, components, parameters)");
     for (int t = 0; t < s; ++t)
       if (mixtures[t] == mixtures[s])
         return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_run_many: a system listed twice");
@@ -1679,10 +1764,13 @@ extern "C" rg_status rg_mixture_run_many(rg_mixture* const* mixtures, int n, int
   if (static_cast<long long>(n) * x0->blocks > static_cast<long long>(sms) * perSM)
     return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_run_many: the systems' CTAs do not fit on the GPU at once");
   Launch L{};
+  L.p = x0->p;
   for (int s = 0; s < n; ++s)
   {
-    mixtures[s]->p.record = record ? 1 : 0;
-    L.p[s] = mixtures[s]->p;
+    mixtures[s]->st.record = record ? 1 : 0;
+    RG_CUDA(ctx, cudaMemcpyAsync(mixtures[s]->d_st, &mixtures[s]->st, sizeof(State), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    L.st[s] = mixtures[s]->d_st;
   }
   const int64_t per = 8192;
   for (int64_t done = 0; done < moves; done += per)
@@ -1691,7 +1779,7 @@ extern "C" rg_status rg_mixture_run_many(rg_mixture* const* mixtures, int n, int
     void* args[] = {&L, &m};
     // every barrier's arrival counter starts at zero in every launch (the error flags beside them persist)
     for (int s = 0; s < n; ++s)
-      RG_CUDA(ctx, cudaMemsetAsync(mixtures[s]->p.bar, 0, sizeof(unsigned long long), ctx->stream));
+      RG_CUDA(ctx, cudaMemsetAsync(mixtures[s]->st.bar, 0, sizeof(unsigned long long), ctx->stream));
     RG_CUDA(ctx, cudaLaunchCooperativeKernel(reinterpret_cast<void*>(mixtureKernel), dim3(n * x0->blocks),
                                              dim3(kThreads), args, smem, ctx->stream));
   }
@@ -1707,8 +1795,8 @@ extern "C" rg_status rg_mixture_run(rg_mixture* x, int64_t moves, int record)
 extern "C" rg_status rg_mixture_set_wait_test(rg_mixture* x, int absent_cta, int64_t spin_limit)
 {
   if (!x || absent_cta < -1 || absent_cta >= x->blocks || spin_limit < 1) return RG_ERR_INVALID_ARGUMENT;
-  x->p.absent_cta = absent_cta;
-  x->p.spin_limit = std::min<long long>(spin_limit, kSpinLimit);  // never longer than the production limit
+  x->st.absent_cta = absent_cta;
+  x->st.spin_limit = std::min<long long>(spin_limit, kSpinLimit);  // never longer than the production limit
   return RG_OK;
 }
 
@@ -1720,10 +1808,10 @@ extern "C" rg_status rg_mixture_results(rg_mixture* x, rg_mixture_result* out)
   int ns[1 + kMaxComp];
   double e, st[kStats];
   unsigned long long bar[2];
-  RG_CUDA(ctx, cudaMemcpyAsync(ns, x->p.n_state, sizeof(ns), cudaMemcpyDeviceToHost, ctx->stream));
-  RG_CUDA(ctx, cudaMemcpyAsync(&e, x->p.energy, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  RG_CUDA(ctx, cudaMemcpyAsync(st, x->p.stats, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
-  RG_CUDA(ctx, cudaMemcpyAsync(bar, x->p.bar, sizeof(bar), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaMemcpyAsync(ns, x->st.n_state, sizeof(ns), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaMemcpyAsync(&e, x->st.energy, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaMemcpyAsync(st, x->st.stats, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaMemcpyAsync(bar, x->st.bar, sizeof(bar), cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   std::memset(out, 0, sizeof(*out));
   for (int c = 0; c < kMaxComp; ++c)
@@ -1750,15 +1838,15 @@ extern "C" rg_status rg_mixture_get_positions(rg_mixture* x, double* xyz, int32_
   rg_ctx* ctx = x->ctx;
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
   int n = 0;
-  RG_CUDA(ctx, cudaMemcpyAsync(&n, x->p.n_state, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaMemcpyAsync(&n, x->st.n_state, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (n > capacity_molecules) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_get_positions: capacity");
   std::vector<double4> pos(static_cast<size_t>(n) * x->p.na);
   if (n > 0)
   {
-    RG_CUDA(ctx, cudaMemcpyAsync(pos.data(), x->p.pos, sizeof(double4) * pos.size(), cudaMemcpyDeviceToHost,
+    RG_CUDA(ctx, cudaMemcpyAsync(pos.data(), x->st.pos, sizeof(double4) * pos.size(), cudaMemcpyDeviceToHost,
                                  ctx->stream));
-    RG_CUDA(ctx, cudaMemcpyAsync(comp, x->p.comp_of, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    RG_CUDA(ctx, cudaMemcpyAsync(comp, x->st.comp_of, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream));
   }
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   for (size_t i = 0; i < pos.size(); ++i)
@@ -1776,7 +1864,7 @@ extern "C" rg_status rg_mixture_get_structure_factors(rg_mixture* x, double* hos
   if (!x || !host || n_doubles != 2ll * x->p.nk) return RG_ERR_INVALID_ARGUMENT;
   rg_ctx* ctx = x->ctx;
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
-  RG_CUDA(ctx, cudaMemcpyAsync(host, x->p.sk, sizeof(double) * n_doubles, cudaMemcpyDeviceToHost, ctx->stream));
+  RG_CUDA(ctx, cudaMemcpyAsync(host, x->st.sk, sizeof(double) * n_doubles, cudaMemcpyDeviceToHost, ctx->stream));
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return RG_OK;
 }

@@ -183,6 +183,46 @@ def test_large_mixture_runs_without_drift(ctx, torch):
     mx.close()
 
 
+@pytest.mark.parametrize("blocks,n_systems", [(4, 3), (2, 2)])
+def test_large_mixtures_on_few_ctas_each(ctx, torch, blocks, n_systems):
+    """Configuration 5 with 2 or 4 CTAs per system (2,031 or 4,062 k-vectors per CTA: several tiles of the candidates'
+    energy sums; at 2 CTAs most of the 6,000 sites per CTA come from L2 beyond the staged slice), several systems per
+    launch: each system equals the same system run on its own, its running energy equals an FP64 recomputation of its
+    final configuration, and its structure factors equal a recomputation."""
+    d = config5(ctx, torch)
+    ff, comps = d["ff"], d["components"]
+    e0 = total_energy(d["system"], d["ewald"], ff, comps, d["xyz"], d["comp"])
+    sk0 = d["ewald"].structure_factors(0)
+
+    def make(s):
+        mx = native.Mixture(d["system"], d["ewald"], comps, BETA, [fugacity_of(1e5), fugacity_of(1e5)], d["xyz"],
+                            d["comp"], max_molecules=6000, seed=11 + s, n_blocks=blocks)
+        mx.set_state(e0, sk0)
+        return mx
+
+    batch = [make(s) for s in range(n_systems)]
+    native.Mixture.run_many(batch, 400)
+    alone = make(0)
+    alone.run(400)
+    assert batch[0].results() == alone.results()
+    np.testing.assert_array_equal(batch[0].structure_factors(), alone.structure_factors())
+    for mx in batch:
+        r = mx.results()
+        assert r["status"] == 0 and sum(r["accepted"]) > 0
+        xyz, comp = mx.positions()
+        e = total_energy(d["system"], d["ewald"], ff, comps, xyz, comp)  # leaves this configuration's S(k) behind
+        assert abs(r["energy"] - e) < 1e-6 * max(1.0, abs(e)) + 1e-3, (r["energy"], e)
+        ref = d["ewald"].structure_factors(0)
+        assert np.max(np.abs(mx.structure_factors() - ref)) < 1e-9 * max(1.0, np.max(np.abs(ref)))
+    # the systems of one launch must share everything but their state
+    other = native.Mixture(d["system"], d["ewald"], comps, BETA, [fugacity_of(2e5), fugacity_of(1e5)], d["xyz"],
+                           d["comp"], max_molecules=6000, seed=99, n_blocks=blocks)
+    with pytest.raises(native.RaspaGpuError):
+        native.Mixture.run_many([batch[0], other], 1)
+    for mx in batch + [alone, other]:
+        mx.close()
+
+
 def test_several_mixtures_in_one_launch_equal_separate_runs(ctx, torch):
     """rg_mixture_run_many: independent systems on disjoint CTA groups of one cooperative launch give exactly the
     results of the same systems run on their own (the same CTA count, seeds and moves), and each still matches an FP64

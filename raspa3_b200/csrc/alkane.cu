@@ -244,46 +244,76 @@ __device__ __forceinline__ int warpSelect(double lbf, bool ok, bool retrace, dou
   return hit ? __ffs(hit) - 1 : 31 - __clz(okMask);
 }
 
-// One bead against the partners partners[begin, n) with the given stride: FP32 pair terms from the fixed-point
-// displacement, accumulated in FP64. Bit b of ovl is set if a pair exceeds the overlap criterion.
+// Squared distance of bead B and partner P in FP32 from their exact fixed-point displacement (the uint32 wrap is the
+// minimum image).
+template <bool TRI>
+__device__ __forceinline__ float beadDistance2(const SysDev& S, int4 B, int4 P)
+{
+  const float f0 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.x) - static_cast<uint32_t>(P.x))) * kFix;
+  const float f1 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.y) - static_cast<uint32_t>(P.y))) * kFix;
+  const float f2 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.z) - static_cast<uint32_t>(P.z))) * kFix;
+  float rx, ry, rz;
+  if (TRI)
+  {
+    rx = fmaf(S.hf[0][0], f0, fmaf(S.hf[1][0], f1, S.hf[2][0] * f2));
+    ry = fmaf(S.hf[0][1], f0, fmaf(S.hf[1][1], f1, S.hf[2][1] * f2));
+    rz = fmaf(S.hf[0][2], f0, fmaf(S.hf[1][2], f1, S.hf[2][2] * f2));
+  }
+  else
+  {
+    rx = S.hf[0][0] * f0;
+    ry = S.hf[1][1] * f1;
+    rz = S.hf[2][2] * f2;
+  }
+  return fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+}
+
+__device__ __forceinline__ void beadPairEnergy(const Shared& sh, int bt, int4 P, float r2, float rc2, float ovlf,
+                                               double& acc, unsigned& ovl, unsigned& inside, int b)
+{
+  if (r2 < rc2)
+  {
+    const float4 q = sh.tab[bt + (P.w & 0xff)];
+    const float t = q.y * __frcp_rn(r2);
+    const float t3 = t * t * t;
+    const float e = q.x * (t3 * (t3 - 1.0f)) - q.z;
+    acc += static_cast<double>(e);
+    inside += 1u;
+    if (e > ovlf) ovl |= 1u << b;
+  }
+}
+
+// Lennard-Jones energy of bead B with partners[begin], partners[begin + stride], .. (fixed point), FP32 from the exact
+// displacement, accumulated in FP64 in partner order. Four partners per iteration: their distances without branches
+// (a skipped molecule's at infinity), then the energies of those within the cutoff. Bit b of ovl is set if a pair
+// exceeds the overlap criterion.
 template <bool TRI, bool SKIP>
 __device__ __forceinline__ void beadPartners(const Shared& sh, const SysDev& S, int4 B, const int4* partners,
                                              int begin, int n, int stride, int skip, float rc2, float ovlf,
                                              double& acc, unsigned& ovl, unsigned& inside, int b)
 {
   const int bt = (B.w & 0xff) * kMaxTypes;
-#pragma unroll 4
-  for (int i = begin; i < n; i += stride)
+  int i = begin;
+  for (; i + 3 * stride < n; i += 4 * stride)
+  {
+    const int4 P0 = partners[i], P1 = partners[i + stride], P2 = partners[i + 2 * stride], P3 = partners[i + 3 * stride];
+    const float r0 = SKIP && (P0.w >> 8) == skip ? INFINITY : beadDistance2<TRI>(S, B, P0);
+    const float r1 = SKIP && (P1.w >> 8) == skip ? INFINITY : beadDistance2<TRI>(S, B, P1);
+    const float r2 = SKIP && (P2.w >> 8) == skip ? INFINITY : beadDistance2<TRI>(S, B, P2);
+    const float r3 = SKIP && (P3.w >> 8) == skip ? INFINITY : beadDistance2<TRI>(S, B, P3);
+    if (fminf(fminf(r0, r1), fminf(r2, r3)) < rc2)
+    {
+      beadPairEnergy(sh, bt, P0, r0, rc2, ovlf, acc, ovl, inside, b);
+      beadPairEnergy(sh, bt, P1, r1, rc2, ovlf, acc, ovl, inside, b);
+      beadPairEnergy(sh, bt, P2, r2, rc2, ovlf, acc, ovl, inside, b);
+      beadPairEnergy(sh, bt, P3, r3, rc2, ovlf, acc, ovl, inside, b);
+    }
+  }
+  for (; i < n; i += stride)
   {
     const int4 P = partners[i];
     if (SKIP && (P.w >> 8) == skip) continue;
-    const float f0 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.x) - static_cast<uint32_t>(P.x))) * kFix;
-    const float f1 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.y) - static_cast<uint32_t>(P.y))) * kFix;
-    const float f2 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.z) - static_cast<uint32_t>(P.z))) * kFix;
-    float rx, ry, rz;
-    if (TRI)
-    {
-      rx = fmaf(S.hf[0][0], f0, fmaf(S.hf[1][0], f1, S.hf[2][0] * f2));
-      ry = fmaf(S.hf[0][1], f0, fmaf(S.hf[1][1], f1, S.hf[2][1] * f2));
-      rz = fmaf(S.hf[0][2], f0, fmaf(S.hf[1][2], f1, S.hf[2][2] * f2));
-    }
-    else
-    {
-      rx = S.hf[0][0] * f0;
-      ry = S.hf[1][1] * f1;
-      rz = S.hf[2][2] * f2;
-    }
-    const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-    if (r2 < rc2)
-    {
-      const float4 q = sh.tab[bt + (P.w & 0xff)];
-      const float t = q.y * __frcp_rn(r2);
-      const float t3 = t * t * t;
-      const float e = q.x * (t3 * (t3 - 1.0f)) - q.z;
-      acc += static_cast<double>(e);
-      inside += 1u;
-      if (e > ovlf) ovl |= 1u << b;
-    }
+    beadPairEnergy(sh, bt, P, beadDistance2<TRI>(S, B, P), rc2, ovlf, acc, ovl, inside, b);
   }
 }
 

@@ -601,8 +601,16 @@ __global__ void __launch_bounds__(256, (!TRICLINIC && sizeof(Real) == 4) ? 3 : 1
 // the near-image list of gridKernel: images within kNearRadius + R of the brick centre, energy in FP64.
 // ---------------------------------------------------------------------------------------------------------------------
 constexpr int kPackThreads = 128;
-constexpr int kPackPer = 4;
-constexpr int kPackChunk = kPackThreads * kPackPer;
+// images staged per thread and chunk: 4 for the Ewald kernel; for Lennard-Jones kernels RG_PACK_PER_LJ (their two
+// parameter lists and the sums of two probes would otherwise hold them to 3 CTAs per SM)
+#ifndef RG_PACK_PER_LJ
+#define RG_PACK_PER_LJ 2
+#endif
+template <int TYPE>
+constexpr int packPer()
+{
+  return TYPE == RG_GRID_EWALD_REAL ? 4 : RG_PACK_PER_LJ;
+}
 // candidate iterations unrolled in the packed kernels (measured on B200: 3 for the Ewald kernel, 4 for Lennard-Jones)
 constexpr int kPackUnrollEwald = 3;
 constexpr int kPackUnrollLJ = 4;
@@ -738,6 +746,8 @@ __global__ void __launch_bounds__(kPackThreads, 4) gridKernelPacked(GridParams p
                                                                    const double4* __restrict__ ipar)
 {
   constexpr bool EWALD = (TYPE == RG_GRID_EWALD_REAL);
+  constexpr int kPackPer = packPer<TYPE>();
+  constexpr int kPackChunk = kPackThreads * kPackPer;
   constexpr int kSlots = NP * 8 * 2;  // FP64 sums: [probe][channel][point]
   extern __shared__ unsigned char smem_raw[];
   float4* cpos = reinterpret_cast<float4*>(smem_raw);
@@ -988,7 +998,7 @@ template <int TYPE, int NP>
 size_t packedSharedBytes()
 {
   constexpr bool EWALD = TYPE == RG_GRID_EWALD_REAL;
-  return sizeof(float4) * kPackChunk * (EWALD ? 3 : 1 + NP) + sizeof(double) * NP * 16 * kPackThreads;
+  return sizeof(float4) * kPackThreads * packPer<TYPE>() * (EWALD ? 3 : 1 + NP) + sizeof(double) * NP * 16 * kPackThreads;
 }
 
 template <int TYPE, int NP, bool COUNT>

@@ -318,9 +318,9 @@ rg_status rg_system_set_precision(rg_system* system, int precision);
 
 /* Interpolation scheme of this system's grids (ForceField::interpolationScheme): RG_SCHEME_TRICUBIC (the default,
  * 8 values per point) or RG_SCHEME_TRIQUINTIC (27, from rg_grid_build_triquintic). Set it before the first
- * rg_system_set_grid. rg_cbmc_external_energies then interpolates with that scheme
- * (InterpolationEnergyGrid::interpolate, interpolation_energy_grid.cpp:4119-4178); the device-resident Monte Carlo
- * drivers (rg_gcmc, rg_mixture, rg_proposal) take tricubic systems only. */
+ * rg_system_set_grid. rg_cbmc_external_energies, the energy differences and the device-resident Monte Carlo drivers
+ * (rg_gcmc, rg_mixture, rg_proposal_sample_targets) then interpolate with that scheme (InterpolationEnergyGrid::
+ * interpolate, interpolation_energy_grid.cpp:3980-4178). */
 rg_status rg_system_set_interpolation_scheme(rg_system* system, int scheme);
 /* Replaces CBMC::computeExternalNonOverlappingEnergies (src/raspakit/cbmc/interactions.cpp:54-179) and its callees
  * CBMC::insideBlockedPockets (:25-52), CBMC::computeExternalFieldEnergy (cbmc/interactions_external_field.cpp:22-200),

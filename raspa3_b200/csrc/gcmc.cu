@@ -50,6 +50,7 @@ struct Params
   rgd::Grid grid;            // data unused; shape and inverse cell
   const double* vdw_grid[kMaxAtoms];  // grid of each component atom's type (NULL = no framework term)
   const double* ewald_grid;
+  int quintic;  // the grids hold the 27 triquintic values per point (RG_SCHEME_TRIQUINTIC) instead of 8
   double rcv_fw2, rcv_mol2, rcc2;
   Component comp;
   double beta, fugacity, volume;
@@ -145,13 +146,15 @@ __device__ double warpExternal(const Params& p, int chain, int n, const double (
     {
       rgd::Grid gg = p.grid;
       gg.data = g;
-      const double v = rgd::interpolate(gg, pos[lane][0], pos[lane][1], pos[lane][2]);
+      const double v = p.quintic ? rgd::interpolateQuintic(gg, pos[lane][0], pos[lane][1], pos[lane][2], nullptr)
+                                 : rgd::interpolate(gg, pos[lane][0], pos[lane][1], pos[lane][2]);
       if (v > p.ff.overlap) ov = 1;
       e += v;
       if (p.ff.use_charge && p.ewald_grid)
       {
         gg.data = p.ewald_grid;
-        e += c.charges[ai] * rgd::interpolate(gg, pos[lane][0], pos[lane][1], pos[lane][2]);
+        e += c.charges[ai] * (p.quintic ? rgd::interpolateQuintic(gg, pos[lane][0], pos[lane][1], pos[lane][2], nullptr)
+                                        : rgd::interpolate(gg, pos[lane][0], pos[lane][1], pos[lane][2]));
       }
     }
   }
@@ -665,8 +668,6 @@ rg_status rg_gcmc_create(rg_system* system, rg_ewald* ewald, const rg_gcmc_compo
   rg_ctx* ctx;
   rg_status st = rgd::systemExport(system, &ff, &box, grids, &ewald_grid, &n_types, gdims, gic, &ctx);
   if (st) return st;
-  if (rgd::systemScheme(system) != RG_SCHEME_TRICUBIC)
-    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_gcmc: tricubic grids only (triquintic grids serve rg_cbmc_external_energies)");
   for (int i = 0; i < comp->n_atoms; ++i)
     if (comp->types[i] < 0 || comp->types[i] >= n_types) return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_gcmc: type");
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -692,6 +693,7 @@ rg_status rg_gcmc_create(rg_system* system, rg_ewald* ewald, const rg_gcmc_compo
     p.vdw_grid[i] = comp->types[i] < 64 ? grids[comp->types[i]] : nullptr;
   }
   p.ewald_grid = ewald_grid;
+  p.quintic = rgd::systemScheme(system) == RG_SCHEME_TRIQUINTIC ? 1 : 0;
   p.rcv_fw2 = params->cutoff_framework_vdw * params->cutoff_framework_vdw;
   p.rcv_mol2 = params->cutoff_molecule_vdw * params->cutoff_molecule_vdw;
   p.rcc2 = params->cutoff_coulomb * params->cutoff_coulomb;

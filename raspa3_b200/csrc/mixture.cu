@@ -73,6 +73,7 @@ struct Params
   rgd::Box box;
   rgd::Grid grid;  // shape and inverse cell of the grids; data per atom in Comp::vdw_grid
   const double* ewald_grid;
+  int quintic;  // the grids hold the 27 triquintic values per point (RG_SCHEME_TRIQUINTIC) instead of 8
   double overlap;
   float overlap_f;
   int use_charge;
@@ -396,6 +397,12 @@ __device__ __forceinline__ void pairTerm(const Params& p, const Shared& sh, int4
   pairEnergy(p, sh, bt, qb, P, qP, pairDistance2(p, B, P), rc2v, acc, ov);
 }
 
+// The triquintic interpolant, out of line so that the tricubic path keeps its registers.
+__device__ __noinline__ double quinticValue(const rgd::Grid& g, double x, double y, double z)
+{
+  return rgd::interpolateQuintic(g, x, y, z, nullptr);
+}
+
 // One phase: energies of sh.nta trial atoms (framework + molecules other than `skip`) and the Ewald energy change of
 // sh.ncand candidates, each summed over the whole grid into sh.tot[0, nta) and sh.tot[nta, nta + ncand); overlap bits
 // per trial atom in sh.ovl. vdwOf/qOf: the framework grid and charge of each trial atom (set by the caller in
@@ -439,7 +446,10 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
           rgd::Grid g = p.grid;
           g.data = lane < 8 ? vdw : p.ewald_grid;
           const double3 r = sh.ta[b];
-          v = rgd::interpolateCorner(g, rgd::gridCell(g, r.x, r.y, r.z), lane & 7);
+          if (!p.quintic)
+            v = rgd::interpolateCorner(g, rgd::gridCell(g, r.x, r.y, r.z), lane & 7);
+          else if ((lane & 7) == 0)  // triquintic grids: lanes 0 and 8 take the whole interpolant
+            v = quinticValue(g, r.x, r.y, r.z);
         }
         v += __shfl_xor_sync(0x0000ffffu, v, 1);
         v += __shfl_xor_sync(0x0000ffffu, v, 2);
@@ -1366,8 +1376,6 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   rg_ctx* ctx = nullptr;
   rg_status st = rgd::systemExport(system, &ff, &box, tg, &eg, &nt, gd, gic, &ctx);
   if (st) return st;
-  if (rgd::systemScheme(system) != RG_SCHEME_TRICUBIC)
-    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: tricubic grids only (triquintic grids serve rg_cbmc_external_energies)");
   if (nt > kMaxTypes) return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: at most 16 pseudo-atom types");
   const int na = comps[0].n_atoms;
   if (na < 2 || na > kMaxAtoms) return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: molecules of 2-4 atoms");
@@ -1400,6 +1408,7 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
       p.hf[i][j] = static_cast<float>(box.c[i][j]);
     }
   p.ewald_grid = eg;
+  p.quintic = rgd::systemScheme(system) == RG_SCHEME_TRIQUINTIC ? 1 : 0;
   p.overlap = ff.overlap;
   p.overlap_f = static_cast<float>(ff.overlap);
   p.use_charge = (ff.use_charge && ewald) ? 1 : 0;

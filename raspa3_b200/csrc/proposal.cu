@@ -279,10 +279,10 @@ __global__ void __launch_bounds__(kThreads) mlpForwardKernel(const float* __rest
 
 // Grid-sampled Boltzmann targets of one bead: s uniform in the unit cell, t = max(-beta U(s), t_min) with
 // U = VDW grid + q * unit-charge Ewald grid (the grid branch of cbmc/interactions_framework_molecule.cpp:57-69).
-__global__ void sampleTargetsKernel(rgd::Grid vdw, const double* ewald_grid, double charge, double beta, double t_min,
-                                    double c00, double c01, double c02, double c10, double c11, double c12, double c20,
-                                    double c21, double c22, int64_t n, unsigned long long seed, float* s_out,
-                                    float* t_out)
+__global__ void sampleTargetsKernel(rgd::Grid vdw, const double* ewald_grid, int quintic, double charge, double beta,
+                                    double t_min, double c00, double c01, double c02, double c10, double c11, double c12,
+                                    double c20, double c21, double c22, int64_t n, unsigned long long seed,
+                                    float* s_out, float* t_out)
 {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -299,12 +299,13 @@ __global__ void sampleTargetsKernel(rgd::Grid vdw, const double* ewald_grid, dou
   const double x = c00 * u[0] + c10 * u[1] + c20 * u[2];
   const double y = c01 * u[0] + c11 * u[1] + c21 * u[2];
   const double z = c02 * u[0] + c12 * u[1] + c22 * u[2];
-  double e = rgd::interpolate(vdw, x, y, z);
+  // the scheme of the system's grids: tricubic (8 values per point) or triquintic (27)
+  double e = quintic ? rgd::interpolateQuintic(vdw, x, y, z, nullptr) : rgd::interpolate(vdw, x, y, z);
   if (ewald_grid)
   {
     rgd::Grid ge = vdw;
     ge.data = ewald_grid;
-    e += charge * rgd::interpolate(ge, x, y, z);
+    e += charge * (quintic ? rgd::interpolateQuintic(ge, x, y, z, nullptr) : rgd::interpolate(ge, x, y, z));
   }
   const double t = fmax(-beta * e, t_min);
   s_out[3 * i] = static_cast<float>(u[0]);
@@ -549,8 +550,6 @@ rg_status rg_proposal_sample_targets(rg_system* system, int pseudo_atom, double 
   rg_ctx* ctx;
   rg_status st = rgd::systemExport(system, &ff, &box, grids, &ewald_grid, &n_types, gd, gic, &ctx);
   if (st) return st;
-  if (rgd::systemScheme(system) != RG_SCHEME_TRICUBIC)
-    return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_proposal: tricubic grids only (triquintic grids serve rg_cbmc_external_energies)");
   if (pseudo_atom < 0 || pseudo_atom >= 64 || pseudo_atom >= n_types || !grids[pseudo_atom])
     return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_proposal_sample_targets: no grid for this pseudo-atom");
   rgd::Grid g{grids[pseudo_atom], gd[0], gd[1], gd[2], {}};
@@ -559,8 +558,8 @@ rg_status rg_proposal_sample_targets(rg_system* system, int pseudo_atom, double 
   const double* c = unit_cell->cell;
   RG_CUDA(ctx, cudaSetDevice(ctx->device));
   sampleTargetsKernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx->stream>>>(
-      g, ff.use_charge ? ewald_grid : nullptr, charge, beta, t_min, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7],
-      c[8], n, seed, s_device, t_device);
+      g, ff.use_charge ? ewald_grid : nullptr, rgd::systemScheme(system) == RG_SCHEME_TRIQUINTIC ? 1 : 0, charge, beta,
+      t_min, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8], n, seed, s_device, t_device);
   RG_CUDA(ctx, cudaGetLastError());
   return RG_OK;
 }

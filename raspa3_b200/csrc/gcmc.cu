@@ -130,6 +130,7 @@ struct Shared
 
 // External energy (framework grids + other molecules) of `count` atoms at pos[], component atom indices atomIdx[],
 // excluding molecule slot `skip`; evaluated by one warp. Returns the energy; *overlap set if the set overlaps.
+template <bool QUINTIC>  // the system's grids: triquintic (27 values per point) or tricubic (8)
 __device__ double warpExternal(const Params& p, int chain, int n, const double (*pos)[3], const int* atomIdx,
                                int count, int skip, int* overlap)
 {
@@ -146,15 +147,15 @@ __device__ double warpExternal(const Params& p, int chain, int n, const double (
     {
       rgd::Grid gg = p.grid;
       gg.data = g;
-      const double v = p.quintic ? rgd::interpolateQuintic(gg, pos[lane][0], pos[lane][1], pos[lane][2], nullptr)
-                                 : rgd::interpolate(gg, pos[lane][0], pos[lane][1], pos[lane][2]);
+      const double v = QUINTIC ? rgd::interpolateQuintic(gg, pos[lane][0], pos[lane][1], pos[lane][2], nullptr)
+                               : rgd::interpolate(gg, pos[lane][0], pos[lane][1], pos[lane][2]);
       if (v > p.ff.overlap) ov = 1;
       e += v;
       if (p.ff.use_charge && p.ewald_grid)
       {
         gg.data = p.ewald_grid;
-        e += c.charges[ai] * (p.quintic ? rgd::interpolateQuintic(gg, pos[lane][0], pos[lane][1], pos[lane][2], nullptr)
-                                        : rgd::interpolate(gg, pos[lane][0], pos[lane][1], pos[lane][2]));
+        e += c.charges[ai] * (QUINTIC ? rgd::interpolateQuintic(gg, pos[lane][0], pos[lane][1], pos[lane][2], nullptr)
+                                      : rgd::interpolate(gg, pos[lane][0], pos[lane][1], pos[lane][2]));
       }
     }
   }
@@ -328,6 +329,7 @@ __device__ __forceinline__ double proposalDensity(const Params& p, const double 
 
 extern __shared__ double2 gcmcDyn[];
 
+template <bool QUINTIC>
 __global__ void __launch_bounds__(kThreads) gcmcKernel(Params p, long long move0, int nmoves, int record,
                                                        long long block_len)
 {
@@ -402,7 +404,7 @@ __global__ void __launch_bounds__(kThreads) gcmcKernel(Params p, long long move0
       if (warp < 2)
       {
         int ov;
-        const double e = warpExternal(p, chain, n, warp == 0 ? sh.newPos : sh.oldPos, idx, na, m, &ov);
+        const double e = warpExternal<QUINTIC>(p, chain, n, warp == 0 ? sh.newPos : sh.oldPos, idx, na, m, &ov);
         if (lane == 0)
         {
           sh.setE[warp] = e;
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(kThreads) gcmcKernel(Params p, long long move0
         for (int t = warp; t < p.k1; t += kWarps)
         {
           int ov;
-          const double e = warpExternal(p, chain, n, sh.trial[t], one, 1, skip, &ov);
+          const double e = warpExternal<QUINTIC>(p, chain, n, sh.trial[t], one, 1, skip, &ov);
           if (lane == 0)
           {
             sh.setE[t] = e;
@@ -549,7 +551,7 @@ __global__ void __launch_bounds__(kThreads) gcmcKernel(Params p, long long move0
             for (int j = 0; j < no; ++j)
               for (int d = 0; d < 3; ++d) op[j][d] = sh.trial[t][others[j]][d];
             int ov = 0;
-            const double e = no > 0 ? warpExternal(p, chain, n, op, others, no, skip, &ov) : 0.0;
+            const double e = no > 0 ? warpExternal<QUINTIC>(p, chain, n, op, others, no, skip, &ov) : 0.0;
             if (lane == 0)
             {
               sh.setE[t] = e;
@@ -803,7 +805,12 @@ rg_status rg_gcmc_run(rg_gcmc* g, int64_t moves, int record)
   while (left > 0)
   {
     const int chunk = static_cast<int>(left < g->max_moves_per_launch ? left : g->max_moves_per_launch);
-    gcmcKernel<<<g->n_chains, kThreads, g->shmem, ctx->stream>>>(g->p, g->moves_done, chunk, record, g->block_len);
+    if (g->p.quintic)
+      gcmcKernel<true><<<g->n_chains, kThreads, g->shmem, ctx->stream>>>(g->p, g->moves_done, chunk, record,
+                                                                         g->block_len);
+    else
+      gcmcKernel<false><<<g->n_chains, kThreads, g->shmem, ctx->stream>>>(g->p, g->moves_done, chunk, record,
+                                                                          g->block_len);
     RG_CUDA(ctx, cudaGetLastError());
     g->moves_done += chunk;
     left -= chunk;

@@ -397,16 +397,11 @@ __device__ __forceinline__ void pairTerm(const Params& p, const Shared& sh, int4
   pairEnergy(p, sh, bt, qb, P, qP, pairDistance2(p, B, P), rc2v, acc, ov);
 }
 
-// The triquintic interpolant, out of line so that the tricubic path keeps its registers.
-__device__ __noinline__ double quinticValue(const rgd::Grid& g, double x, double y, double z)
-{
-  return rgd::interpolateQuintic(g, x, y, z, nullptr);
-}
-
 // One phase: energies of sh.nta trial atoms (framework + molecules other than `skip`) and the Ewald energy change of
 // sh.ncand candidates, each summed over the whole grid into sh.tot[0, nta) and sh.tot[nta, nta + ncand); overlap bits
 // per trial atom in sh.ovl. vdwOf/qOf: the framework grid and charge of each trial atom (set by the caller in
 // sh.tf[].w = type; the grids come from the type). Returns false if a barrier failed.
+template <bool QUINTIC>  // the system's grids: triquintic (27 values per point) or tricubic (8)
 __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const* atomGrid)
 {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -446,10 +441,10 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
           rgd::Grid g = p.grid;
           g.data = lane < 8 ? vdw : p.ewald_grid;
           const double3 r = sh.ta[b];
-          if (!p.quintic)
+          if (!QUINTIC)
             v = rgd::interpolateCorner(g, rgd::gridCell(g, r.x, r.y, r.z), lane & 7);
           else if ((lane & 7) == 0)  // triquintic grids: lanes 0 and 8 take the whole interpolant
-            v = quinticValue(g, r.x, r.y, r.z);
+            v = rgd::interpolateQuintic(g, r.x, r.y, r.z, nullptr);
         }
         v += __shfl_xor_sync(0x0000ffffu, v, 1);
         v += __shfl_xor_sync(0x0000ffffu, v, 2);
@@ -807,6 +802,7 @@ struct Launch
 };
 static_assert(sizeof(Launch) <= 32000, "kernel parameter space");
 
+template <bool QUINTIC>
 __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_constant__ Launch L, int moves)
 {
   const Params& p = L.p;
@@ -943,7 +939,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
         sh.ncand = p.use_charge ? 1 : 0;
       }
       __syncthreads();
-      if (!phase(p, sh, sh.m, atomGrid)) break;
+      if (!phase<QUINTIC>(p, sh, sh.m, atomGrid)) break;
       if (tid == 0)
       {
         bool ovn = false;
@@ -988,7 +984,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
       // the orientations depend only on the move: their offsets are computed now, by threads of another warp
       if (tid >= 32 && tid < 32 + p.k2) orientationOffsets(p, cc, move, kKindOrient, tid - 32, sh.rel[tid - 32]);
       __syncthreads();
-      if (!phase(p, sh, -1, atomGrid)) break;
+      if (!phase<QUINTIC>(p, sh, -1, atomGrid)) break;
       if (tid < 32)
       {
         const int t = tid;
@@ -1027,7 +1023,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
           storeOrientation(p, sh, atomGrid, cc, x, tid * (na - 1));
         }
         __syncthreads();
-        if (!phase(p, sh, -1, atomGrid)) break;
+        if (!phase<QUINTIC>(p, sh, -1, atomGrid)) break;
         if (tid < 32)
         {
           const int per = na - 1, t = tid;
@@ -1126,7 +1122,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
         storeOrientation(p, sh, atomGrid, cc, x, p.k1 + tid * (na - 1));
       }
       __syncthreads();
-      if (!phase(p, sh, m, atomGrid)) break;
+      if (!phase<QUINTIC>(p, sh, m, atomGrid)) break;
       if (tid < 32)
       {
         // Rosenbluth weights of the retrace: first beads (trial 0 = the old bead) and orientations (trial 0 = the
@@ -1253,7 +1249,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
           storeOrientation(p, sh, atomGrid, co, x, base2 + 1 + t * (na - 1));
         }
         __syncthreads();
-        if (!phase(p, sh, m, atomGrid)) break;
+        if (!phase<QUINTIC>(p, sh, m, atomGrid)) break;
         if (tid < 32)
         {
           const int per = na - 1;
@@ -1578,7 +1574,7 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   // a full system (sites beyond the slice are read from L2)
   cudaFuncAttributes fa{};
   int optin = 0;
-  err = cudaFuncGetAttributes(&fa, mixtureKernel);
+  err = cudaFuncGetAttributes(&fa, p.quintic ? mixtureKernel<true> : mixtureKernel<false>);
   if (err == cudaSuccess) err = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
   if (err != cudaSuccess)
   {
@@ -1595,8 +1591,11 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   const long long share = (static_cast<long long>(p.capacity) * na + x->blocks - 1) / x->blocks;
   p.nslice = static_cast<int>(std::max<long long>(64, std::min(share, (budget - fixedBytes) / 16)));
   x->smem = dynBytes(p.tabK, p.kpc, p.nslice);
-  err = cudaFuncSetAttribute(mixtureKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(x->smem));
-  if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, mixtureKernel, kThreads, x->smem);
+  err = cudaFuncSetAttribute(p.quintic ? mixtureKernel<true> : mixtureKernel<false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(x->smem));
+  if (err == cudaSuccess)
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, p.quintic ? mixtureKernel<true> : mixtureKernel<false>,
+                                                        kThreads, x->smem);
   if (err != cudaSuccess || perSM < 1)
   {
     delete x;
@@ -1768,8 +1767,9 @@ extern "C" rg_status rg_mixture_run_many(rg_mixture* const* mixtures, int n, int
   // every system's CTAs must be resident together with the others' (one cooperative launch)
   int sms = 0, perSM = 0;
   RG_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-  RG_CUDA(ctx, cudaFuncSetAttribute(mixtureKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  RG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, mixtureKernel, kThreads, smem));
+  auto kernel = x0->p.quintic ? mixtureKernel<true> : mixtureKernel<false>;
+  RG_CUDA(ctx, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  RG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, kThreads, smem));
   if (static_cast<long long>(n) * x0->blocks > static_cast<long long>(sms) * perSM)
     return rg::fail(ctx, RG_ERR_INVALID_ARGUMENT, "rg_mixture_run_many: the systems' CTAs do not fit on the GPU at once");
   Launch L{};
@@ -1789,7 +1789,7 @@ extern "C" rg_status rg_mixture_run_many(rg_mixture* const* mixtures, int n, int
     // every barrier's arrival counter starts at zero in every launch (the error flags beside them persist)
     for (int s = 0; s < n; ++s)
       RG_CUDA(ctx, cudaMemsetAsync(mixtures[s]->st.bar, 0, sizeof(unsigned long long), ctx->stream));
-    RG_CUDA(ctx, cudaLaunchCooperativeKernel(reinterpret_cast<void*>(mixtureKernel), dim3(n * x0->blocks),
+    RG_CUDA(ctx, cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kernel), dim3(n * x0->blocks),
                                              dim3(kThreads), args, smem, ctx->stream));
   }
   return RG_OK;

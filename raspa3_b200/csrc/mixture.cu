@@ -45,6 +45,8 @@ constexpr int kMaxItems = 96;          // trial atoms of one phase
 constexpr int kMaxCand = kMaxTrials;   // Ewald candidates of one phase
 constexpr int kMaxCandAtoms = 2 * kMaxAtoms;
 constexpr int kEwTile = 256;      // k-vectors per tile of the candidates' energy sums
+constexpr int kMaxCells = 1024;   // cells of the pair loop's binning of a CTA's slice
+constexpr int kPairWarps = kWarps - 1;  // warps of the pair loop (the last one interpolates the grids meanwhile)
 static_assert(kMaxCand <= 2 * kWarps, "two candidates per warp in the energy sums");
 constexpr int kMaxTypes = 16;
 constexpr int kRow = kMaxItems + kMaxCand + 4;  // columns of partial sums per CTA (last 4: overlap-bit words)
@@ -98,6 +100,10 @@ struct Params
   int group;                // CTAs of this system in the launch; the system's CTA index is blockIdx.x % group
   int kpc;                  // k-vectors per CTA (the stride of the per-CTA k arrays in dynamic shared memory)
   int nslice;               // molecule sites of a CTA's slice staged in shared memory per phase (any rest from L2)
+  int ncand_max;            // Ewald candidates of a phase at most (the orientation trials)
+  int cand_atoms;           // atoms of one candidate at most (old and new molecule: 2 x atoms per molecule)
+  int cells;                // 1: the pair loop walks the 27 cells around each trial atom (0: every site of the slice)
+  int nc[3];                // cells per axis, each at least the pair cutoff wide
 };
 
 // The state of one system: its molecules, running energy, statistics and structure factors, its launch flags and
@@ -174,6 +180,7 @@ struct Shared
   double logq[kMaxTrials];
   double stats[kStats];
   double3 rel[kMaxTrials][kMaxAtoms];  // insertion: orientation offsets from the starting bead, computed up front
+  int wsum[kWarps];                    // the pair warps' sums in the binning's prefix scan
 };
 
 __device__ __forceinline__ double2 urand(const Params& p, long long move, uint32_t sl)
@@ -270,7 +277,7 @@ __device__ bool gridBarrier(const Params& p, Shared& sh)
   return !sh.fail;
 }
 
-// Dynamic shared memory: the Ewald phasor tables (kMaxCand x kMaxCandAtoms x 3 axes x tabK), this CTA's molecule
+// Dynamic shared memory: the Ewald phasor tables (ncand_max x cand_atoms x 3 axes x tabK), this CTA's molecule
 // sites staged per phase, its framework atoms (explicit pairs of grid-less types) kept for the launch, and its k-range.
 struct Dyn
 {
@@ -278,38 +285,55 @@ struct Dyn
   int4* slice;  // [nslice]
   int4* fws;    // [kFwSlice]
   float* fwq;   // [kFwSlice]
-  double* ek;   // [kMaxCand][kEwTile]: the candidates' energy terms of one tile of k-vectors
+  double* ek;   // [ncand_max][kEwTile]: the candidates' energy terms of one tile of k-vectors
   // this CTA's k-range for the whole launch: S(k) (only this CTA updates it; written back at the end of the launch),
   // the prefactors and the k-vectors
   double2* ks;  // [kpc]
   double* kt;   // [kpc]
   char4* kv;    // [kpc]
+  // the staged slice binned into cells, rebuilt every phase: where each cell's run starts in `order` (and, last, the
+  // slice's length), per cell and pair warp the sites of the warp's part of the slice in that cell and then the
+  // warp's write cursor there, and the slice indices in (cell, index) order
+  int* cellStart;          // [ncell + 1]
+  int* cellWarp;           // [ncell][kPairWarps]
+  unsigned short* order;   // [nslice]
 };
-__host__ __device__ constexpr size_t phasorBytes(int tabK)
+__host__ __device__ constexpr size_t phasorBytes(int tabK, int ncand, int catoms)
 {
-  return sizeof(double2) * kMaxCand * kMaxCandAtoms * 3 * static_cast<size_t>(tabK);
+  return sizeof(double2) * static_cast<size_t>(ncand) * catoms * 3 * static_cast<size_t>(tabK);
 }
 __host__ __device__ constexpr size_t kRangeBytes(int kpc)
 {
   return static_cast<size_t>(kpc) * (sizeof(double2) + sizeof(double) + sizeof(char4));
 }
-__host__ __device__ constexpr size_t dynBytes(int tabK, int kpc, int nslice)
+__host__ __device__ constexpr size_t cellBytes(int ncell, int nslice)
 {
-  return phasorBytes(tabK) + sizeof(int4) * (static_cast<size_t>(nslice) + kFwSlice) + sizeof(float) * kFwSlice +
-         sizeof(double) * kMaxCand * kEwTile + kRangeBytes(kpc);
+  return ncell == 0 ? 0
+                    : sizeof(int) * ((kPairWarps + 1) * static_cast<size_t>(ncell) + 2) +
+                          ((sizeof(unsigned short) * static_cast<size_t>(nslice) + 15) & ~size_t(15));
+}
+__host__ __device__ constexpr size_t dynBytes(int tabK, int ncand, int catoms, int kpc, int nslice, int ncell)
+{
+  return phasorBytes(tabK, ncand, catoms) + sizeof(int4) * (static_cast<size_t>(nslice) + kFwSlice) +
+         sizeof(float) * kFwSlice + sizeof(double) * static_cast<size_t>(ncand) * kEwTile + kRangeBytes(kpc) +
+         cellBytes(ncell, nslice);
 }
 __device__ __forceinline__ Dyn dynOf(const Params& p)
 {
   extern __shared__ __align__(16) unsigned char dynSmem[];
   Dyn d;
   d.phasor = reinterpret_cast<double2*>(dynSmem);
-  d.slice = reinterpret_cast<int4*>(dynSmem + phasorBytes(p.tabK));
+  d.slice = reinterpret_cast<int4*>(dynSmem + phasorBytes(p.tabK, p.ncand_max, p.cand_atoms));
   d.fws = d.slice + p.nslice;
   d.fwq = reinterpret_cast<float*>(d.fws + kFwSlice);
   d.ek = reinterpret_cast<double*>(d.fwq + kFwSlice);
-  d.ks = reinterpret_cast<double2*>(d.ek + kMaxCand * kEwTile);
+  d.ks = reinterpret_cast<double2*>(d.ek + p.ncand_max * kEwTile);
   d.kt = reinterpret_cast<double*>(d.ks + p.kpc);
   d.kv = reinterpret_cast<char4*>(d.kt + p.kpc);
+  const int ncell = p.cells ? p.nc[0] * p.nc[1] * p.nc[2] : 0;
+  d.cellStart = reinterpret_cast<int*>(d.kv + p.kpc);
+  d.cellWarp = d.cellStart + (p.cells ? ncell + 2 : 0);
+  d.order = reinterpret_cast<unsigned short*>(d.cellWarp + kPairWarps * ncell);
   return d;
 }
 
@@ -321,7 +345,7 @@ __device__ __forceinline__ double2 candidateDelta(const Params& p, const Shared&
   double2 d = make_double2(0.0, 0.0);
   for (int a = 0; a < sh.cn[c]; ++a)
   {
-    const double2* t = phasor + static_cast<long long>(c * kMaxCandAtoms + a) * 3 * p.tabK;
+    const double2* t = phasor + static_cast<long long>(c * p.cand_atoms + a) * 3 * p.tabK;
     double2 ex = t[abs(kv.x)], ey = t[p.tabK + abs(kv.y)], ez = t[2 * p.tabK + abs(kv.z)];
     if (kv.x < 0) ex.y = -ex.y;
     if (kv.y < 0) ey.y = -ey.y;
@@ -344,6 +368,18 @@ __device__ void addCandidate(const Params& p, const Shared& sh, const Dyn& dy, i
     dy.ks[kk].x += d.x;
     dy.ks[kk].y += d.y;
   }
+}
+
+// Cell of a fixed-point fractional coordinate (uint32 x 2^-32) among nc cells along that axis, and the periodic wrap
+// of a neighbouring cell index.
+__device__ __forceinline__ int cellCoord(int f, int nc)
+{
+  return static_cast<int>((static_cast<unsigned long long>(static_cast<uint32_t>(f)) * static_cast<unsigned>(nc)) >> 32);
+}
+__device__ __forceinline__ int wrapCell(int c, int nc) { return c < 0 ? c + nc : (c >= nc ? c - nc : c); }
+__device__ __forceinline__ int siteCell(const Params& p, int4 P)
+{
+  return cellCoord(P.x, p.nc[0]) + p.nc[0] * (cellCoord(P.y, p.nc[1]) + p.nc[1] * cellCoord(P.z, p.nc[2]));
 }
 
 // Squared distance of trial atom B and partner P (fixed point) in FP32 from the exact fixed-point displacement (the
@@ -462,43 +498,125 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
     constexpr int kPairThreads = (kWarps - 1) * 32;
     for (int i = tid; i < nst; i += kPairThreads) dy.slice[i] = __ldcg(gs.fx + s0 + i);
     asm volatile("bar.sync 1, %0;" ::"n"(kPairThreads) : "memory");  // the slice is staged (warps 0 .. kWarps - 2)
-    // 1. molecule-molecule pairs over this CTA's slice of sites (staged part from shared memory, any rest from L2),
-    //    four sites per iteration into four independent sums
+    // 1. molecule-molecule pairs over this CTA's slice of sites (staged part from shared memory, any rest from L2)
     const int streams = nta > 0 ? kPairThreads / nta : 0;
     b = nta > 0 ? tid % nta : 0;
     const int st = nta > 0 ? tid / nta : 0;
+    const int n = s1 - s0;
+    // cells pay off when the slice holds at least about two sites per cell
+    const int ncell = p.nc[0] * p.nc[1] * p.nc[2];
+    const bool useCells = p.cells && n <= p.nslice && n >= 2 * ncell;
+    if (useCells)
+    {
+      // the staged slice binned into cells at least the cutoff wide, as a stable counting sort: pair warp w takes the
+      // w-th contiguous part of the slice and counts its sites per cell; a prefix scan over (cell, warp) in that order
+      // (each pair thread scans a run of cells) gives every warp its cursor in every cell; then each warp scatters its
+      // part in index order, so each cell lists its sites in slice order and the sums below are reproducible
+      const int part = (n + kPairWarps - 1) / kPairWarps, i0 = min(n, warp * part), i1 = min(n, i0 + part);
+      for (int c = tid; c < ncell * kPairWarps; c += kPairThreads) dy.cellWarp[c] = 0;
+      asm volatile("bar.sync 1, %0;" ::"n"(kPairThreads) : "memory");
+      for (int i = i0 + lane; i < i1; i += 32) atomicAdd(&dy.cellWarp[siteCell(p, dy.slice[i]) * kPairWarps + warp], 1);
+      asm volatile("bar.sync 1, %0;" ::"n"(kPairThreads) : "memory");
+      const int per = (ncell + kPairThreads - 1) / kPairThreads, c0 = min(ncell, tid * per), c1 = min(ncell, c0 + per);
+      int run = 0;
+      for (int c = c0 * kPairWarps; c < c1 * kPairWarps; ++c) run += dy.cellWarp[c];
+      int incl = run;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1)
+      {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane == 31) sh.wsum[warp] = incl;
+      asm volatile("bar.sync 1, %0;" ::"n"(kPairThreads) : "memory");
+      int at = incl - run;
+      for (int w = 0; w < warp; ++w) at += sh.wsum[w];
+      for (int c = c0; c < c1; ++c)
+      {
+        dy.cellStart[c] = at;
+        for (int w = 0; w < kPairWarps; ++w)
+        {
+          const int cnt = dy.cellWarp[c * kPairWarps + w];
+          dy.cellWarp[c * kPairWarps + w] = at;
+          at += cnt;
+        }
+      }
+      if (tid == 0) dy.cellStart[ncell] = n;
+      asm volatile("bar.sync 1, %0;" ::"n"(kPairThreads) : "memory");
+      for (int j0 = i0; j0 < i1; j0 += 32)
+      {
+        const int i = j0 + lane;
+        const bool act = i < i1;
+        const int c = act ? siteCell(p, dy.slice[i]) : -1 - lane;
+        const unsigned peers = __match_any_sync(0xffffffffu, c);
+        const int base = act ? dy.cellWarp[c * kPairWarps + warp] : 0;
+        __syncwarp();
+        if (act)
+        {
+          dy.order[base + __popc(peers & ((1u << lane) - 1u))] = static_cast<unsigned short>(i);
+          if (lane == 31 - __clz(peers)) dy.cellWarp[c * kPairWarps + warp] = base + __popc(peers);
+        }
+        __syncwarp();
+      }
+      asm volatile("bar.sync 1, %0;" ::"n"(kPairThreads) : "memory");
+    }
     if (nta > 0 && st < streams)
     {
       const int4 B = sh.tf[b];
       const int bt = B.w & 0xff;
       const float qb = sh.qt[bt];
-      const int n = s1 - s0, ns_staged = min(n, p.nslice);
+      const int ns_staged = min(n, p.nslice);
       const float rcut2 = p.use_charge ? fmaxf(p.rc2_mm, p.rc2_c) : p.rc2_mm;
       double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      int i = st;
-      // staged sites, four per iteration: their distances without branches (the skipped molecule's at infinity),
-      // then the energies of the few within a cutoff
-      for (; i + 3 * streams < ns_staged; i += 4 * streams)
+      if (useCells)
       {
-        const int4 P0 = dy.slice[i], P1 = dy.slice[i + streams], P2 = dy.slice[i + 2 * streams],
-                   P3 = dy.slice[i + 3 * streams];
-        const float r0 = (P0.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P0);
-        const float r1 = (P1.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P1);
-        const float r2 = (P2.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P2);
-        const float r3 = (P3.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P3);
-        if (fminf(fminf(r0, r1), fminf(r2, r3)) < rcut2)
+        // the 27 cells around the trial atom (distinct: at least 3 cells per axis) shared among the atom's streams: with
+        // fewer than 27 streams each walks every streams-th cell whole, with more each cell is split among
+        // streams / 27 of them
+        const int cstep = min(streams, 27), nsub = max(1, streams / 27);
+        if (st < cstep * nsub)
         {
-          if (r0 < rcut2) pairEnergy(p, sh, bt, qb, P0, sh.qt[P0.w & 0xff], r0, p.rc2_mm, a0, ov);
-          if (r1 < rcut2) pairEnergy(p, sh, bt, qb, P1, sh.qt[P1.w & 0xff], r1, p.rc2_mm, a1, ov);
-          if (r2 < rcut2) pairEnergy(p, sh, bt, qb, P2, sh.qt[P2.w & 0xff], r2, p.rc2_mm, a2, ov);
-          if (r3 < rcut2) pairEnergy(p, sh, bt, qb, P3, sh.qt[P3.w & 0xff], r3, p.rc2_mm, a3, ov);
+          const int cx = cellCoord(B.x, p.nc[0]), cy = cellCoord(B.y, p.nc[1]), cz = cellCoord(B.z, p.nc[2]);
+          for (int k = st % cstep; k < 27; k += cstep)
+          {
+            const int c = wrapCell(cx + k % 3 - 1, p.nc[0]) +
+                          p.nc[0] * (wrapCell(cy + (k / 3) % 3 - 1, p.nc[1]) + p.nc[1] * wrapCell(cz + k / 9 - 1, p.nc[2]));
+            const int e = dy.cellStart[c + 1];
+            for (int j = dy.cellStart[c] + st / cstep; j < e; j += nsub)
+            {
+              const int4 P = dy.slice[dy.order[j]];
+              if ((P.w >> 8) != skip) pairTerm(p, sh, B, bt, qb, P, sh.qt[P.w & 0xff], p.rc2_mm, a0, ov);
+            }
+          }
         }
       }
-      // the rest: remaining staged sites, then any beyond the staged slice from L2
-      for (; i < n; i += streams)
+      else
       {
-        const int4 P = i < p.nslice ? dy.slice[i] : __ldcg(gs.fx + s0 + i);
-        if ((P.w >> 8) != skip) pairTerm(p, sh, B, bt, qb, P, sh.qt[P.w & 0xff], p.rc2_mm, a0, ov);
+        int i = st;
+        // staged sites, four per iteration: their distances without branches (the skipped molecule's at infinity),
+        // then the energies of the few within a cutoff
+        for (; i + 3 * streams < ns_staged; i += 4 * streams)
+        {
+          const int4 P0 = dy.slice[i], P1 = dy.slice[i + streams], P2 = dy.slice[i + 2 * streams],
+                     P3 = dy.slice[i + 3 * streams];
+          const float r0 = (P0.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P0);
+          const float r1 = (P1.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P1);
+          const float r2 = (P2.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P2);
+          const float r3 = (P3.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P3);
+          if (fminf(fminf(r0, r1), fminf(r2, r3)) < rcut2)
+          {
+            if (r0 < rcut2) pairEnergy(p, sh, bt, qb, P0, sh.qt[P0.w & 0xff], r0, p.rc2_mm, a0, ov);
+            if (r1 < rcut2) pairEnergy(p, sh, bt, qb, P1, sh.qt[P1.w & 0xff], r1, p.rc2_mm, a1, ov);
+            if (r2 < rcut2) pairEnergy(p, sh, bt, qb, P2, sh.qt[P2.w & 0xff], r2, p.rc2_mm, a2, ov);
+            if (r3 < rcut2) pairEnergy(p, sh, bt, qb, P3, sh.qt[P3.w & 0xff], r3, p.rc2_mm, a3, ov);
+          }
+        }
+        // the rest: remaining staged sites, then any beyond the staged slice from L2
+        for (; i < n; i += streams)
+        {
+          const int4 P = i < p.nslice ? dy.slice[i] : __ldcg(gs.fx + s0 + i);
+          if ((P.w >> 8) != skip) pairTerm(p, sh, B, bt, qb, P, sh.qt[P.w & 0xff], p.rc2_mm, a0, ov);
+        }
       }
       acc = (a0 + a1) + (a2 + a3);
       // trial atom without a VDW grid: explicit pairs with this CTA's slice of the framework atoms
@@ -538,15 +656,15 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
   if (ncand > 0)
   {
     const rgd::Box& bx = p.box;
-    for (int task = tid; task < ncand * kMaxCandAtoms * 3; task += kThreads)
+    for (int task = tid; task < ncand * p.cand_atoms * 3; task += kThreads)
     {
-      const int c = task / (kMaxCandAtoms * 3), a = (task / 3) % kMaxCandAtoms, d = task % 3;
+      const int c = task / (p.cand_atoms * 3), a = (task / 3) % p.cand_atoms, d = task % 3;
       if (a >= sh.cn[c]) continue;
       const double3 r = sh.cpos[c][a];
       const double sd = bx.ic[0][d] * r.x + bx.ic[1][d] * r.y + bx.ic[2][d] * r.z;
       double sn, cs;
       sincospi(2.0 * sd, &sn, &cs);
-      double2* t = phasor + (static_cast<long long>(c * kMaxCandAtoms + a) * 3 + d) * p.tabK;
+      double2* t = phasor + (static_cast<long long>(c * p.cand_atoms + a) * 3 + d) * p.tabK;
       double2 w = make_double2(1.0, 0.0);
       t[0] = w;
       for (int j = 1; j <= p.km[d]; ++j)
@@ -1581,16 +1699,52 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
     delete x;
     return rg::cudaFail(ctx, err, "rg_mixture_create");
   }
+  // cells of the pair loop: at least the largest pair cutoff wide along each perpendicular width, at most kMaxCells in
+  // all (wider cells are still valid), and used only with at least 3 per axis (the 27 neighbours must be distinct)
+  {
+    const double rcut = std::sqrt(static_cast<double>(p.use_charge ? std::max(p.rc2_mm, p.rc2_c) : p.rc2_mm));
+    double w[3];
+    for (int a = 0; a < 3; ++a)
+    {
+      const int b1 = (a + 1) % 3, b2 = (a + 2) % 3;
+      const double cr[3] = {box.c[b1][1] * box.c[b2][2] - box.c[b1][2] * box.c[b2][1],
+                            box.c[b1][2] * box.c[b2][0] - box.c[b1][0] * box.c[b2][2],
+                            box.c[b1][0] * box.c[b2][1] - box.c[b1][1] * box.c[b2][0]};
+      w[a] = box.volume / std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+      const double n = rcut > 0.0 ? std::floor(w[a] / rcut) : 0.0;
+      p.nc[a] = static_cast<int>(std::min<double>(n, kMaxCells));
+    }
+    while (static_cast<long long>(p.nc[0]) * p.nc[1] * p.nc[2] > kMaxCells)
+    {
+      const int a = (p.nc[0] >= p.nc[1] && p.nc[0] >= p.nc[2]) ? 0 : (p.nc[1] >= p.nc[2] ? 1 : 2);
+      p.nc[a] -= 1;
+    }
+    p.cells = (p.nc[0] >= 3 && p.nc[1] >= 3 && p.nc[2] >= 3) ? 1 : 0;
+  }
+  // the Ewald candidates of a phase: up to k2 orientations (insertion, identity change) or one molecule, each of at
+  // most the old and the new molecule's atoms
+  p.ncand_max = std::max(1, p.k2);
+  p.cand_atoms = 2 * na;
   const long long budget = static_cast<long long>(optin) - static_cast<long long>(fa.sharedSizeBytes) - 1024;
-  const long long fixedBytes = static_cast<long long>(dynBytes(p.tabK, p.kpc, 0));
-  if (fixedBytes + 16 * 64 > budget)
+  auto fixedOf = [&](int cells) {
+    return static_cast<long long>(
+               dynBytes(p.tabK, p.ncand_max, p.cand_atoms, p.kpc, 0, cells ? p.nc[0] * p.nc[1] * p.nc[2] : 0)) +
+           16;
+  };
+  auto perSiteOf = [&](int cells) { return static_cast<long long>(sizeof(int4) + (cells ? sizeof(unsigned short) : 0)); };
+  // without room for the cells next to the k-range, the pair loop walks the slice as it is
+  if (p.cells && fixedOf(1) + perSiteOf(1) * 64 > budget) p.cells = 0;
+  const int ncell = p.cells ? p.nc[0] * p.nc[1] * p.nc[2] : 0;
+  const long long fixedBytes = fixedOf(p.cells);
+  const long long perSite = perSiteOf(p.cells);
+  if (fixedBytes + perSite * 64 > budget)
   {
     delete x;
     return rg::fail(ctx, RG_ERR_UNSUPPORTED, "rg_mixture: the CTA's k-range does not fit in shared memory (use more CTAs)");
   }
   const long long share = (static_cast<long long>(p.capacity) * na + x->blocks - 1) / x->blocks;
-  p.nslice = static_cast<int>(std::max<long long>(64, std::min(share, (budget - fixedBytes) / 16)));
-  x->smem = dynBytes(p.tabK, p.kpc, p.nslice);
+  p.nslice = static_cast<int>(std::max<long long>(64, std::min(std::min(share, (budget - fixedBytes) / perSite), 65535ll)));
+  x->smem = dynBytes(p.tabK, p.ncand_max, p.cand_atoms, p.kpc, p.nslice, ncell);
   err = cudaFuncSetAttribute(p.quintic ? mixtureKernel<true> : mixtureKernel<false>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(x->smem));
   if (err == cudaSuccess)

@@ -320,8 +320,8 @@ __device__ __forceinline__ void beadPartners(const Shared& sh, const SysDev& S, 
 // Framework + molecule energies of the nbd beads in sh.bead, summed over the cluster into sh.efw / sh.emm / sh.ovl.
 // Thread t works on bead t % nbd with partner stream t / nbd: the framework slice of this CTA is fwS[0, nfw), the
 // molecule beads molS[0, nmb) are interleaved over the cluster ranks. The per-thread sums are reduced per bead in a
-// fixed order, the CTAs' sums in rank order, so every CTA ends with identical totals. Called by every thread of every
-// CTA of the cluster.
+// fixed order (within a warp lanes l, l + nbd, .. by shuffles, then the warps in order), the CTAs' sums in rank
+// order, so every CTA ends with identical totals. Called by every thread of every CTA of the cluster.
 __device__ __noinline__ void evalBeads(Shared& sh, const Params& p, const SysDev& S, const int4* fwS, int nfw, const int4* molS,
                           int nmb, int nbd, int skip, Cl cl, int& eval)
 {
@@ -346,8 +346,23 @@ __device__ __noinline__ void evalBeads(Shared& sh, const Params& p, const SysDev
                                 amm, ovl, inside, b);
     }
   }
-  sh.red[0][tid] = afw;
-  sh.red[1][tid] = amm;
+  // lane l < nbd ends with its warp's sums of bead (32 warp + l) mod nbd (threads past the last stream add zeros)
+  const double ownf = afw, ownm = amm;
+  for (int o = nbd; nbd > 0 && o < 32; o += nbd)
+  {
+    const double yf = __shfl_down_sync(0xffffffffu, ownf, o), ym = __shfl_down_sync(0xffffffffu, ownm, o);
+    if (lane + o < 32)
+    {
+      afw += yf;
+      amm += ym;
+    }
+  }
+  if (lane < nbd)
+  {
+    const int bb = (32 * warp + lane) % nbd;
+    sh.red[0][warp * kMaxTrials + bb] = afw;
+    sh.red[1][warp * kMaxTrials + bb] = amm;
+  }
   inside = __reduce_add_sync(0xffffffffu, inside);
   if (lane == 0 && inside) atomicAdd(&sh.pairs, static_cast<unsigned long long>(inside));
   ovl = __reduce_or_sync(0xffffffffu, ovl);
@@ -355,23 +370,25 @@ __device__ __noinline__ void evalBeads(Shared& sh, const Params& p, const SysDev
   __syncthreads();
   const int buf = eval & 1;
   eval += 1;
-  if (tid < 2 * kMaxTrials)
-  {
-    // thread t < 16 sums the framework part of bead t, thread 16 + t its molecule part
-    const int which = tid >= kMaxTrials, bb = tid - which * kMaxTrials;
-    double sum = 0.0;
-    if (bb < nbd)
-      for (int k = 0; k < streams; ++k) sum += sh.red[which][bb + nbd * k];
-    sh.xch[buf][tid] = sum;
-  }
+  // thread t < 16 sums the framework part of bead t, thread 16 + t its molecule part, over the warps in order; a
+  // lone CTA writes its totals at once
+  double sum = 0.0;
+  const int which = tid >= kMaxTrials, bb = tid - which * kMaxTrials;
+  if (tid < 2 * kMaxTrials && bb < nbd)
+    for (int w = 0; w < nw; ++w) sum += sh.red[which][w * kMaxTrials + bb];
+  unsigned octa = 0;
   if (tid == 2 * kMaxTrials)
+    for (int w = 0; w < nw; ++w) octa |= sh.red_ovl[w];
+  if (C == 1)
   {
-    unsigned o = 0;
-    for (int w = 0; w < nw; ++w) o |= sh.red_ovl[w];
-    sh.xch_ovl[buf] = o;
+    if (tid < kMaxTrials) sh.efw[tid] = sum;
+    if (tid >= kMaxTrials && tid < 2 * kMaxTrials) sh.emm[tid - kMaxTrials] = sum;
+    if (tid == 2 * kMaxTrials) sh.ovl = octa;
   }
-  if (C > 1)
+  else
   {
+    if (tid < 2 * kMaxTrials) sh.xch[buf][tid] = sum;
+    if (tid == 2 * kMaxTrials) sh.xch_ovl[buf] = octa;
     // every CTA's sums are complete before any is read; sums are taken in rank order, identical in every CTA
     cg::cluster_group cluster = cg::this_cluster();
     cluster.sync();
@@ -390,13 +407,6 @@ __device__ __noinline__ void evalBeads(Shared& sh, const Params& p, const SysDev
       for (int q = 0; q < C; ++q) o |= cluster.map_shared_rank(&sh.xch_ovl[0], q)[buf];
       sh.ovl = o;
     }
-  }
-  else
-  {
-    __syncthreads();
-    if (tid < kMaxTrials) sh.efw[tid] = sh.xch[buf][tid];
-    if (tid >= kMaxTrials && tid < 2 * kMaxTrials) sh.emm[tid - kMaxTrials] = sh.xch[buf][tid];
-    if (tid == 2 * kMaxTrials) sh.ovl = sh.xch_ovl[buf];
   }
   __syncthreads();
 }

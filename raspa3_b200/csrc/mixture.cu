@@ -181,6 +181,8 @@ struct Shared
   double stats[kStats];
   double3 rel[kMaxTrials][kMaxAtoms];  // insertion: orientation offsets from the starting bead, computed up front
   int wsum[kWarps];                    // the pair warps' sums in the binning's prefix scan
+  int staged_ns;                       // sites of the system when the slice in shared memory was staged (-1: none)
+  int binned;                          // 1: the cells describe the staged slice as it is
 };
 
 __device__ __forceinline__ double2 urand(const Params& p, long long move, uint32_t sl)
@@ -496,8 +498,13 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
   else
   {
     constexpr int kPairThreads = (kWarps - 1) * 32;
-    for (int i = tid; i < nst; i += kPairThreads) dy.slice[i] = __ldcg(gs.fx + s0 + i);
+    // the slice stays in shared memory from phase to phase while the number of sites is unchanged (accepted moves
+    // update it in place), and so do its cells while no site of it moved
+    const bool fresh = sh.staged_ns == ns, binned = fresh && sh.binned;
+    if (!fresh)
+      for (int i = tid; i < nst; i += kPairThreads) dy.slice[i] = __ldcg(gs.fx + s0 + i);
     asm volatile("bar.sync 1, %0;" ::"n"(kPairThreads) : "memory");  // the slice is staged (warps 0 .. kWarps - 2)
+    if (tid == 0) sh.staged_ns = ns;
     // 1. molecule-molecule pairs over this CTA's slice of sites (staged part from shared memory, any rest from L2)
     const int streams = nta > 0 ? kPairThreads / nta : 0;
     b = nta > 0 ? tid % nta : 0;
@@ -506,7 +513,7 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
     // cells pay off when the slice holds at least about two sites per cell
     const int ncell = p.nc[0] * p.nc[1] * p.nc[2];
     const bool useCells = p.cells && n <= p.nslice && n >= 2 * ncell;
-    if (useCells)
+    if (useCells && !binned)
     {
       // the staged slice binned into cells at least the cutoff wide, as a stable counting sort: pair warp w takes the
       // w-th contiguous part of the slice and counts its sites per cell; a prefix scan over (cell, warp) in that order
@@ -559,6 +566,7 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
         __syncwarp();
       }
       asm volatile("bar.sync 1, %0;" ::"n"(kPairThreads) : "memory");
+      if (tid == 0) sh.binned = 1;
     }
     if (nta > 0 && st < streams)
     {
@@ -884,14 +892,27 @@ __device__ __forceinline__ double3 loadPos(const Params& p, int site)
   return make_double3(a.x, a.y, b.x);
 }
 
-// write the atoms of molecule m (every CTA writes the same values; each reads back only its own writes)
-__device__ void storeMolecule(const Params& p, int m, int cidx, const double3* x)
+// write the atoms of molecule m (every CTA writes the same values; each reads back only its own writes). Sites of
+// this CTA's staged slice are updated in shared memory as well, which then needs new cells; a change of the number of
+// molecules, made by the caller after this, moves every CTA's slice and so has it staged again.
+__device__ void storeMolecule(const Params& p, Shared& sh, int m, int cidx, const double3* x)
 {
   const Comp& c = p.comp[cidx];
+  const int G = p.group, cta = static_cast<int>(blockIdx.x) % p.group;
+  const int ns = sh.n * p.na, chunk = (ns + G - 1) / G, s0 = min(ns, cta * chunk), s1 = min(ns, s0 + chunk);
+  const int nst = min(s1 - s0, p.nslice);
+  int4* slice = dynOf(p).slice;
   for (int i = 0; i < p.na; ++i)
   {
+    const int4 f = toFixed(p, x[i], c.types[i] | (m << 8));
     gs.pos[m * p.na + i] = make_double4(x[i].x, x[i].y, x[i].z, 0.0);
-    gs.fx[m * p.na + i] = toFixed(p, x[i], c.types[i] | (m << 8));
+    gs.fx[m * p.na + i] = f;
+    const int at = m * p.na + i - s0;
+    if (sh.staged_ns == ns && at >= 0 && at < nst)
+    {
+      slice[at] = f;
+      sh.binned = 0;
+    }
   }
 }
 
@@ -935,6 +956,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
   if (tid == 0)
   {
     sh.n = gs.n_state[0];
+    sh.staged_ns = -1;
+    sh.binned = 0;
     for (int c = 0; c < kMaxComp; ++c) sh.count[c] = gs.n_state[1 + c];
     sh.energy = *gs.energy;
     sh.gen = 0;
@@ -1077,7 +1100,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
       __syncthreads();
       if (sh.accept)
       {
-        if (tid == 0) storeMolecule(p, sh.m, c, sh.mol);
+        if (tid == 0) storeMolecule(p, sh, sh.m, c, sh.mol);
         if (p.use_charge) addCandidate(p, sh, dyk, 0, k1 - k0);
       }
     }
@@ -1178,7 +1201,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
           if (tid == 0)
           {
             const int m = sh.n;
-            storeMolecule(p, m, c, sh.mol);
+            storeMolecule(p, sh, m, c, sh.mol);
             gs.comp_of[m] = c;
             gs.slot[m] = sh.count[c];
             gs.list[c * p.capacity + sh.count[c]] = m;
@@ -1289,7 +1312,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
           {
             const int cl = sh.preCl;
             const int sl = (lastC == last) ? k : sh.preSl;
-            storeMolecule(p, m, cl, sh.preLast);
+            storeMolecule(p, sh, m, cl, sh.preLast);
             gs.comp_of[m] = cl;
             gs.slot[m] = sl;
             gs.list[cl * p.capacity + sl] = m;
@@ -1411,7 +1434,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
         {
           if (tid == 0)
           {
-            storeMolecule(p, m, newC, sh.mol);
+            storeMolecule(p, sh, m, newC, sh.mol);
             // move m from the old component's list to the new one's (from the values read before the barrier)
             const int k = sh.preSlot, lastC = sh.preLastC;
             gs.list[oldC * p.capacity + k] = lastC;

@@ -21,6 +21,7 @@ Multi-GPU: the grid build is replicated (independent frameworks per rank, no col
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -985,10 +986,28 @@ def run_paths(args, ctx, world, rank, dist, torch):
         for new, old in mv:
             e_.delta(new, old)
         wall = time.perf_counter() - t0
+        # the C-ABI call alone, as a C++ caller makes it: its atom arrays and result struct exist before the loop, so
+        # the timed loop holds only rg_ewald_delta (atom packing, launch, kernel, synchronisation, host terms)
+        fn = native.lib().rg_ewald_delta
+        res = native.EwaldEnergy()
+        ref = ctypes.byref(res)
+        prepared = [(ctypes.c_void_p(n_.ctypes.data), len(n_), ctypes.c_void_p(o_.ctypes.data), len(o_))
+                    for n_, o_ in mv]
+        handle = e_.handle
+        for pn, nn, po, no in prepared[:10]:
+            fn(handle, pn, nn, po, no, 0.0, None, ref)
+        status = 0
+        t0 = time.perf_counter()
+        for pn, nn, po, no in prepared:
+            status |= fn(handle, pn, nn, po, no, 0.0, None, ref)
+        direct = time.perf_counter() - t0
+        if status:
+            raise RuntimeError("rg_ewald_delta failed in the timed loop")
         nk = e_.n_kvectors
-        deltas[name] = {"n_kvectors": nk, "deltas_per_s": PATH_DELTAS / wall, "us_per_delta": 1e6 * wall / PATH_DELTAS,
+        deltas[name] = {"n_kvectors": nk, "deltas_per_s": PATH_DELTAS / direct, "us_per_delta": 1e6 * direct / PATH_DELTAS,
+                        "python_wrapper_us_per_delta": 1e6 * wall / PATH_DELTAS,
                         "algorithmic_bytes_per_delta": 40 * nk,
-                        "achieved_gbs": 40 * nk * PATH_DELTAS / wall / 1e9}
+                        "achieved_gbs": 40 * nk * PATH_DELTAS / direct / 1e9}
     # full recompute of configuration 5 (adsorbates on top of the rigid framework structure factor)
     sizes = np.full(n_mol, 3, dtype=np.int32)
     for _ in range(2):

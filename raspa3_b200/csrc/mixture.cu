@@ -44,7 +44,7 @@ constexpr int kMaxTrials = 12;
 constexpr int kMaxItems = 96;          // trial atoms of one phase
 constexpr int kMaxCand = kMaxTrials;   // Ewald candidates of one phase
 constexpr int kMaxCandAtoms = 2 * kMaxAtoms;
-constexpr int kEwTile = 256;      // k-vectors per tile of the candidates' energy sums
+constexpr int kSegLen = 4;        // k-vectors per segment of the candidates' Ewald sums (one (kx, ky) per segment)
 constexpr int kMaxCells = 1024;   // cells of the pair loop's binning of a CTA's slice
 constexpr int kPairWarps = kWarps - 1;  // warps of the pair loop (the last one interpolates the grids meanwhile)
 static_assert(kMaxCand <= 2 * kWarps, "two candidates per warp in the energy sums");
@@ -100,6 +100,7 @@ struct Params
   int group;                // CTAs of this system in the launch; the system's CTA index is blockIdx.x % group
   int kpc;                  // k-vectors per CTA (the stride of the per-CTA k arrays in dynamic shared memory)
   int nslice;               // molecule sites of a CTA's slice staged in shared memory per phase (any rest from L2)
+  int nseg_max;             // segments of a CTA's k-range at most (runs of up to kSegLen k-vectors sharing kx and ky)
   int ncand_max;            // Ewald candidates of a phase at most (the orientation trials)
   int cand_atoms;           // atoms of one candidate at most (old and new molecule: 2 x atoms per molecule)
   int cells;                // 1: the pair loop walks the 27 cells around each trial atom (0: every site of the slice)
@@ -167,6 +168,7 @@ struct Shared
   // move state
   int kind, c, c2, m, axis, accept, fail, n, count[kMaxComp], gen;
   int phases;  // phases run by this CTA: its parity selects the buffer of partial-sum rows
+  int nseg;    // segments of this CTA's k-range
   // molecule-list state an accepted deletion / identity change rewrites, read before the phase's barrier (no CTA
   // writes it before every CTA has passed that barrier, so every CTA reads the same values and writes the same update)
   int preSlot, preLastC, preCl, preSl;
@@ -287,12 +289,13 @@ struct Dyn
   int4* slice;  // [nslice]
   int4* fws;    // [kFwSlice]
   float* fwq;   // [kFwSlice]
-  double* ek;   // [ncand_max][kEwTile]: the candidates' energy terms of one tile of k-vectors
+  double* eacc;  // [ncand_max][kThreads]: per thread its sum of each candidate's energy terms
   // this CTA's k-range for the whole launch: S(k) (only this CTA updates it; written back at the end of the launch),
   // the prefactors and the k-vectors
   double2* ks;  // [kpc]
   double* kt;   // [kpc]
   char4* kv;    // [kpc]
+  int* segStart;  // [nseg_max + 1]: where each segment of the k-range starts, and (last) the range's length
   // the staged slice binned into cells, rebuilt every phase: where each cell's run starts in `order` (and, last, the
   // slice's length), per cell and pair warp the sites of the warp's part of the slice in that cell and then the
   // warp's write cursor there, and the slice indices in (cell, index) order
@@ -314,11 +317,11 @@ __host__ __device__ constexpr size_t cellBytes(int ncell, int nslice)
                     : sizeof(int) * ((kPairWarps + 1) * static_cast<size_t>(ncell) + 2) +
                           ((sizeof(unsigned short) * static_cast<size_t>(nslice) + 15) & ~size_t(15));
 }
-__host__ __device__ constexpr size_t dynBytes(int tabK, int ncand, int catoms, int kpc, int nslice, int ncell)
+__host__ __device__ constexpr size_t dynBytes(int tabK, int ncand, int catoms, int kpc, int nseg, int nslice, int ncell)
 {
   return phasorBytes(tabK, ncand, catoms) + sizeof(int4) * (static_cast<size_t>(nslice) + kFwSlice) +
-         sizeof(float) * kFwSlice + sizeof(double) * static_cast<size_t>(ncand) * kEwTile + kRangeBytes(kpc) +
-         cellBytes(ncell, nslice);
+         sizeof(float) * kFwSlice + sizeof(double) * static_cast<size_t>(ncand) * kThreads + kRangeBytes(kpc) +
+         sizeof(int) * (static_cast<size_t>(nseg) + 2) + cellBytes(ncell, nslice);
 }
 __device__ __forceinline__ Dyn dynOf(const Params& p)
 {
@@ -328,47 +331,73 @@ __device__ __forceinline__ Dyn dynOf(const Params& p)
   d.slice = reinterpret_cast<int4*>(dynSmem + phasorBytes(p.tabK, p.ncand_max, p.cand_atoms));
   d.fws = d.slice + p.nslice;
   d.fwq = reinterpret_cast<float*>(d.fws + kFwSlice);
-  d.ek = reinterpret_cast<double*>(d.fwq + kFwSlice);
-  d.ks = reinterpret_cast<double2*>(d.ek + p.ncand_max * kEwTile);
+  d.eacc = reinterpret_cast<double*>(d.fwq + kFwSlice);
+  d.ks = reinterpret_cast<double2*>(d.eacc + p.ncand_max * kThreads);
   d.kt = reinterpret_cast<double*>(d.ks + p.kpc);
   d.kv = reinterpret_cast<char4*>(d.kt + p.kpc);
   const int ncell = p.cells ? p.nc[0] * p.nc[1] * p.nc[2] : 0;
-  d.cellStart = reinterpret_cast<int*>(d.kv + p.kpc);
+  d.segStart = reinterpret_cast<int*>(d.kv + p.kpc);
+  d.cellStart = d.segStart + p.nseg_max + 2;
   d.cellWarp = d.cellStart + (p.cells ? ncell + 2 : 0);
   d.order = reinterpret_cast<unsigned short*>(d.cellWarp + kPairWarps * ncell);
   return d;
 }
 
-// Structure-factor change of Ewald candidate c at k-vector kv: sum over its atoms of q exp(2 pi i k.s), from the
-// phasor tables of the current phase (ewald.cpp:1043-1244).
-__device__ __forceinline__ double2 candidateDelta(const Params& p, const Shared& sh, const double2* phasor, int c,
-                                                  char4 kv)
+// Structure-factor change of Ewald candidate c at the n <= kSegLen k-vectors kv[k0 ..] of one segment (they share kx
+// and ky): per k the sum over the candidate's atoms of q exp(2 pi i k.s) (ewald.cpp:1043-1244), from the phasor tables
+// of the current phase. Per atom the x and y phasors and the charge are multiplied once for the segment, then each k
+// takes its z phasor; the kSegLen sums are independent. Entries u >= n repeat the last k-vector and are not used.
+__device__ __forceinline__ void segmentDelta(const Params& p, const Shared& sh, const double2* phasor, const char4* kv,
+                                             int c, int k0, int n, double2 (&d)[kSegLen])
 {
-  double2 d = make_double2(0.0, 0.0);
+  const char4 kb = kv[k0];
+  int iz[kSegLen];
+  bool neg[kSegLen];
+#pragma unroll
+  for (int u = 0; u < kSegLen; ++u)
+  {
+    const char4 k = kv[k0 + min(u, n - 1)];
+    iz[u] = 2 * p.tabK + abs(k.z);
+    neg[u] = k.z < 0;
+    d[u] = make_double2(0.0, 0.0);
+  }
+  const int ix = abs(kb.x), iy = p.tabK + abs(kb.y);
   for (int a = 0; a < sh.cn[c]; ++a)
   {
     const double2* t = phasor + static_cast<long long>(c * p.cand_atoms + a) * 3 * p.tabK;
-    double2 ex = t[abs(kv.x)], ey = t[p.tabK + abs(kv.y)], ez = t[2 * p.tabK + abs(kv.z)];
-    if (kv.x < 0) ex.y = -ex.y;
-    if (kv.y < 0) ey.y = -ey.y;
-    if (kv.z < 0) ez.y = -ez.y;
-    const double2 exy = make_double2(ex.x * ey.x - ex.y * ey.y, ex.x * ey.y + ex.y * ey.x);
+    double2 ex = t[ix], ey = t[iy];
+    if (kb.x < 0) ex.y = -ex.y;
+    if (kb.y < 0) ey.y = -ey.y;
     const double q = sh.cq[c][a];
-    d.x += q * (exy.x * ez.x - exy.y * ez.y);
-    d.y += q * (exy.x * ez.y + exy.y * ez.x);
+    const double2 w = make_double2(q * (ex.x * ey.x - ex.y * ey.y), q * (ex.x * ey.y + ex.y * ey.x));
+#pragma unroll
+    for (int u = 0; u < kSegLen; ++u)
+    {
+      double2 z = t[iz[u]];
+      if (neg[u]) z.y = -z.y;
+      d[u].x += w.x * z.x - w.y * z.y;
+      d[u].y += w.x * z.y + w.y * z.x;
+    }
   }
-  return d;
 }
 
 // The accepted candidate's structure-factor change added to this CTA's S(k) range (the phasor tables of the phase
 // that evaluated it are still in shared memory).
 __device__ void addCandidate(const Params& p, const Shared& sh, const Dyn& dy, int c, int nkr)
 {
-  for (int kk = threadIdx.x; kk < nkr; kk += kThreads)
+  (void)nkr;
+  for (int sg = threadIdx.x; sg < sh.nseg; sg += kThreads)
   {
-    const double2 d = candidateDelta(p, sh, dy.phasor, c, dy.kv[kk]);
-    dy.ks[kk].x += d.x;
-    dy.ks[kk].y += d.y;
+    const int k0 = dy.segStart[sg], n = dy.segStart[sg + 1] - k0;
+    double2 d[kSegLen];
+    segmentDelta(p, sh, dy.phasor, dy.kv, c, k0, n, d);
+#pragma unroll
+    for (int u = 0; u < kSegLen; ++u)
+      if (u < n)
+      {
+        dy.ks[k0 + u].x += d[u].x;
+        dy.ks[k0 + u].y += d[u].y;
+      }
   }
 }
 
@@ -682,26 +711,33 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
       }
     }
     __syncthreads();
-    // energy change of each candidate over this CTA's k-range, in tiles of kEwTile k-vectors: one (candidate, k) task
-    // per thread, then warp w sums candidates w and w + kWarps, lane j over the tiles' k-vectors j, j + 32, ..
-    double esum0 = 0.0, esum1 = 0.0;
-    for (int t0 = 0; t0 < nkr; t0 += kEwTile)
+    // energy change of each candidate over this CTA's k-range: one (candidate, segment) task at a time per thread,
+    // its energy terms added to the thread's own sum for that candidate; then warp w sums candidates w and w + kWarps
+    // over the threads in a fixed order
+    const int nseg = sh.nseg;
+    for (int c = 0; c < ncand; ++c) dy.eacc[c * kThreads + tid] = 0.0;
+    for (int task = tid; task < ncand * nseg; task += kThreads)
     {
-      const int nt = min(kEwTile, nkr - t0);
-      for (int task = tid; task < ncand * nt; task += kThreads)
-      {
-        const int c = task / nt, j = task - c * nt, kk = t0 + j;
-        const double2 d = candidateDelta(p, sh, phasor, c, dy.kv[kk]);
-        const double2 sk = dy.ks[kk];
-        dy.ek[c * kEwTile + j] = dy.kt[kk] * (2.0 * (sk.x * d.x + sk.y * d.y) + (d.x * d.x + d.y * d.y));
-      }
-      __syncthreads();
-      if (warp < ncand)
-        for (int j = lane; j < nt; j += 32) esum0 += dy.ek[warp * kEwTile + j];
-      if (warp + kWarps < ncand)
-        for (int j = lane; j < nt; j += 32) esum1 += dy.ek[(warp + kWarps) * kEwTile + j];
-      __syncthreads();
+      const int c = task / nseg, sg = task - c * nseg;
+      const int k0 = dy.segStart[sg], n = dy.segStart[sg + 1] - k0;
+      double2 d[kSegLen];
+      segmentDelta(p, sh, phasor, dy.kv, c, k0, n, d);
+      double e = 0.0;
+#pragma unroll
+      for (int u = 0; u < kSegLen; ++u)
+        if (u < n)
+        {
+          const double2 sk = dy.ks[k0 + u];
+          e += dy.kt[k0 + u] * (2.0 * (sk.x * d[u].x + sk.y * d[u].y) + (d[u].x * d[u].x + d[u].y * d[u].y));
+        }
+      dy.eacc[c * kThreads + tid] += e;
     }
+    __syncthreads();
+    double esum0 = 0.0, esum1 = 0.0;
+    if (warp < ncand)
+      for (int j = lane; j < kThreads; j += 32) esum0 += dy.eacc[warp * kThreads + j];
+    if (warp + kWarps < ncand)
+      for (int j = lane; j < kThreads; j += 32) esum1 += dy.eacc[(warp + kWarps) * kThreads + j];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
     {
@@ -988,6 +1024,27 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
       dy.fws[i] = gs.fwx[fa + i];
       dy.fwq[i] = gs.fwq[fa + i];
     }
+  }
+  __syncthreads();
+  // the k-range cut into segments: runs of k-vectors with the same kx and ky, each split into pieces of at most
+  // kSegLen (the k-vectors are ordered by kx, ky, kz); the host sized nseg_max by the same rule
+  if (tid == 0)
+  {
+    int ns = 0, runStart = 0;
+    for (int kk = 0; kk < k1 - k0; ++kk)
+    {
+      const char4 a = dyk.kv[kk];
+      const bool newRun = kk == 0 || a.x != dyk.kv[kk - 1].x || a.y != dyk.kv[kk - 1].y;
+      if (newRun) runStart = kk;
+      if (newRun || (kk - runStart) % kSegLen == 0)
+      {
+        if (ns < p.nseg_max) dyk.segStart[ns] = kk;
+        ++ns;
+      }
+    }
+    if (ns > p.nseg_max) sh.fail = 1;
+    dyk.segStart[min(ns, p.nseg_max)] = max(0, k1 - k0);
+    sh.nseg = min(ns, p.nseg_max);
   }
   __syncthreads();
   if (sh.fail) return;
@@ -1711,6 +1768,33 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   x->blocks = std::min(kMaxBlocks, params->n_blocks > 0 ? std::min(params->n_blocks, sms) : sms);
   p.group = x->blocks;
   p.kpc = std::max(1, (p.nk + x->blocks - 1) / x->blocks);
+  // segments of each CTA's k-range, cut by the kernel's rule (runs of equal kx and ky, pieces of at most kSegLen):
+  // their largest count sizes the segment table in shared memory
+  p.nseg_max = 0;
+  if (p.use_charge && p.nk > 0)
+  {
+    std::vector<char4> hk(static_cast<size_t>(p.nk));
+    err = cudaMemcpyAsync(hk.data(), p.kvec, sizeof(char4) * hk.size(), cudaMemcpyDeviceToHost, ctx->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(ctx->stream);
+    if (err != cudaSuccess)
+    {
+      delete x;
+      return rg::cudaFail(ctx, err, "rg_mixture_create");
+    }
+    for (int cta = 0; cta < x->blocks; ++cta)
+    {
+      const int k0 = cta * p.kpc, k1 = std::min(p.nk, k0 + p.kpc);
+      int ns = 0, runStart = 0;
+      for (int kk = 0; kk < k1 - k0; ++kk)
+      {
+        const char4 a = hk[k0 + kk];
+        const bool newRun = kk == 0 || a.x != hk[k0 + kk - 1].x || a.y != hk[k0 + kk - 1].y;
+        if (newRun) runStart = kk;
+        if (newRun || (kk - runStart) % kSegLen == 0) ++ns;
+      }
+      p.nseg_max = std::max(p.nseg_max, ns);
+    }
+  }
   // shared memory: the k-range must fit; the staged slice of molecule sites takes what is left, up to a CTA's share of
   // a full system (sites beyond the slice are read from L2)
   cudaFuncAttributes fa{};
@@ -1751,7 +1835,7 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   const long long budget = static_cast<long long>(optin) - static_cast<long long>(fa.sharedSizeBytes) - 1024;
   auto fixedOf = [&](int cells) {
     return static_cast<long long>(
-               dynBytes(p.tabK, p.ncand_max, p.cand_atoms, p.kpc, 0, cells ? p.nc[0] * p.nc[1] * p.nc[2] : 0)) +
+               dynBytes(p.tabK, p.ncand_max, p.cand_atoms, p.kpc, p.nseg_max, 0, cells ? p.nc[0] * p.nc[1] * p.nc[2] : 0)) +
            16;
   };
   auto perSiteOf = [&](int cells) { return static_cast<long long>(sizeof(int4) + (cells ? sizeof(unsigned short) : 0)); };
@@ -1767,7 +1851,7 @@ extern "C" rg_status rg_mixture_create(rg_system* system, rg_ewald* ewald, const
   }
   const long long share = (static_cast<long long>(p.capacity) * na + x->blocks - 1) / x->blocks;
   p.nslice = static_cast<int>(std::max<long long>(64, std::min(std::min(share, (budget - fixedBytes) / perSite), 65535ll)));
-  x->smem = dynBytes(p.tabK, p.ncand_max, p.cand_atoms, p.kpc, p.nslice, ncell);
+  x->smem = dynBytes(p.tabK, p.ncand_max, p.cand_atoms, p.kpc, p.nseg_max, p.nslice, ncell);
   err = cudaFuncSetAttribute(p.quintic ? mixtureKernel<true> : mixtureKernel<false>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(x->smem));
   if (err == cudaSuccess)

@@ -559,6 +559,10 @@ rg_status rg_ewald_batch_delta(rg_ewald_batch* batch, const rg_atom* atoms, int 
                                const int32_t* n_old, double* delta_fourier);
 /* accept[s] != 0: system s's trial S(k) becomes its stored S(k). */
 rg_status rg_ewald_batch_accept(rg_ewald_batch* batch, const uint8_t* accept);
+/* Device time of the last rg_ewald_batch_delta in milliseconds, from CUDA events on the context's stream: the upload
+ * of the moved atoms and the update kernel (the host-side packing before them is not included). No reference
+ * counterpart: it reports the kernel's duration for a roofline. Either pointer may be NULL. */
+rg_status rg_ewald_batch_timing(rg_ewald_batch* batch, float* upload_ms, float* kernel_ms);
 /* Copies structure factors to the host, 2*(1+n_groups) doubles per k-vector in the reference's storedEik order
  * (total, then group sums; re, im). which: 0 = stored, 1 = trial, 2 = framework (2 doubles per k). */
 rg_status rg_ewald_get_structure_factors(rg_ewald* ewald, int which, double* host, int64_t n_doubles);

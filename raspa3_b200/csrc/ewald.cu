@@ -952,6 +952,9 @@ struct rg_ewald_batch
   int4* desc = nullptr;            // [blocks]: first k, end k, first (kx, ky) pair, pairs
   int* kinfo = nullptr;            // [nk]: pair * 256 + (kz + 128)
   char2* pairs = nullptr;          // [pairs]: (kx, ky)
+  // device time of the last rg_ewald_batch_delta: events before the atom upload, before and after the kernel
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  float upload_ms = 0.0f, kernel_ms = 0.0f;
 };
 
 namespace
@@ -1140,6 +1143,7 @@ rg_status rg_ewald_batch_create(rg_ewald* e, int n_systems, rg_ewald_batch** out
   if (!err) err = cudaMemsetAsync(b->counter, 0, sizeof(unsigned int) * n_systems, ctx->stream);
   if (!err) err = cudaHostAlloc(reinterpret_cast<void**>(&b->result_host), sizeof(double) * n_systems, cudaHostAllocMapped);
   if (!err) err = cudaHostGetDevicePointer(reinterpret_cast<void**>(&b->result), b->result_host, 0);
+  for (int i = 0; i < 3 && !err; ++i) err = cudaEventCreate(&b->ev[i]);
   if (!err) err = cudaStreamSynchronize(ctx->stream);
   if (err)
   {
@@ -1168,6 +1172,8 @@ rg_status rg_ewald_batch_destroy(rg_ewald_batch* b)
   if (b->atoms_host) cudaFreeHost(b->atoms_host);
   if (b->counts_host) cudaFreeHost(b->counts_host);
   if (b->result_host) cudaFreeHost(b->result_host);
+  for (cudaEvent_t ev : b->ev)
+    if (ev) cudaEventDestroy(ev);
   delete b;
   return RG_OK;
 }
@@ -1232,6 +1238,7 @@ rg_status rg_ewald_batch_delta(rg_ewald_batch* b, const rg_atom* atoms, int max_
     for (int s = 0; s < b->n; ++s) delta_fourier[s] = 0.0;
     return RG_OK;
   }
+  RG_CUDA(ctx, cudaEventRecord(b->ev[0], ctx->stream));
   RG_CUDA(ctx, cudaMemcpyAsync(b->atoms, b->atoms_host, sizeof(MovedAtom) * stride * b->n, cudaMemcpyHostToDevice,
                                ctx->stream));
   RG_CUDA(ctx, cudaMemcpyAsync(b->counts, b->counts_host, sizeof(int) * b->n, cudaMemcpyHostToDevice, ctx->stream));
@@ -1242,12 +1249,24 @@ rg_status rg_ewald_batch_delta(rg_ewald_batch* b, const rg_atom* atoms, int max_
   RG_CUDA(ctx, cudaFuncSetAttribute(ewaldBatchDeltaKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(shmem)));
   dim3 grid(b->blocks, b->n);
+  RG_CUDA(ctx, cudaEventRecord(b->ev[1], ctx->stream));
   ewaldBatchDeltaKernel<<<grid, kThreads, shmem, ctx->stream>>>(b->desc, b->kinfo, b->pairs, e->nk, b->n, e->temp,
                                                                b->sk, b->cur, b->atoms, stride, b->counts, kxm, kym,
                                                                kzm, b->partial, b->counter, b->result);
   RG_CUDA(ctx, cudaGetLastError());
+  RG_CUDA(ctx, cudaEventRecord(b->ev[2], ctx->stream));
   RG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  RG_CUDA(ctx, cudaEventElapsedTime(&b->upload_ms, b->ev[0], b->ev[1]));
+  RG_CUDA(ctx, cudaEventElapsedTime(&b->kernel_ms, b->ev[1], b->ev[2]));
   std::memcpy(delta_fourier, b->result_host, sizeof(double) * b->n);
+  return RG_OK;
+}
+
+rg_status rg_ewald_batch_timing(rg_ewald_batch* b, float* upload_ms, float* kernel_ms)
+{
+  if (!b) return RG_ERR_INVALID_ARGUMENT;
+  if (upload_ms) *upload_ms = b->upload_ms;
+  if (kernel_ms) *kernel_ms = b->kernel_ms;
   return RG_OK;
 }
 

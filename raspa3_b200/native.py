@@ -247,6 +247,7 @@ def lib():
         L.rg_ewald_batch_get.argtypes = [vp, i32, i32, vp]
         L.rg_ewald_batch_delta.argtypes = [vp, vp, i32, vp, vp, vp]
         L.rg_ewald_batch_accept.argtypes = [vp, vp]
+        L.rg_ewald_batch_timing.argtypes = [vp, P(ctypes.c_float), P(ctypes.c_float)]
         L.rg_mixture_get_positions.argtypes = [vp, vp, vp, i32, P(i32)]
         L.rg_mixture_get_structure_factors.argtypes = [vp, vp, i64]
         L.rg_mixture_set_proposal.argtypes = [vp, i32, vp, P(RgBox)]
@@ -736,6 +737,13 @@ class EwaldBatch:
         m = np.ascontiguousarray(mask, dtype=np.uint8)
         check(self.ctx.handle, lib().rg_ewald_batch_accept(self.handle, ctypes.c_void_p(m.ctypes.data)),
               "rg_ewald_batch_accept")
+
+    def timing(self) -> tuple[float, float]:
+        """Device time of the last delta in ms: (upload of the moved atoms, update kernel)."""
+        up, k = ctypes.c_float(), ctypes.c_float()
+        check(self.ctx.handle, lib().rg_ewald_batch_timing(self.handle, ctypes.byref(up), ctypes.byref(k)),
+              "rg_ewald_batch_timing")
+        return float(up.value), float(k.value)
 
 
 class Gcmc:

@@ -228,6 +228,8 @@ def test_batched_structure_factor_update(ctx, oracle, kmax, sphere):
         packed[6 * s:6 * s + len(new)] = new
         packed[6 * s + len(new):6 * s + len(new) + len(old)] = old
     d = batch.delta(packed, 6, [len(m[0]) for m in moves], [len(m[1]) for m in moves])
+    upload_ms, kernel_ms = batch.timing()
+    assert upload_ms >= 0.0 and kernel_ms > 0.0, (upload_ms, kernel_ms)
     trials = []
     for s in range(n_sys):
         new, old = moves[s]

@@ -39,6 +39,8 @@ METRIC = "grid pts/s"
 UNIT = "grid points/s"
 # FLOPs per in-cutoff pair of the restated formulas (add/mul = 1, FMA = 2, reciprocal/sqrt/erfc/exp = 1 each).
 FLOPS_PER_PAIR = {"lj": 55, "ewald": 65}
+# DRAM bytes (read + write) per launch of the grid kernels in their ncu capture (profiles/grid_build_config2.md)
+NCU_DRAM_BYTES = {"LJ C_co2+O_co2 (two-probe kernel)": 0.29e6 + 143e6, "Ewald-real": 0.17e6 + 44e6}
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -1288,9 +1290,10 @@ def run_ours(args):
                   for idx in calls]
     dom = int(np.argmax(mean_ms))
     achieved = call_flops[dom] / (mean_ms[dom] * 1e-3) / 1e12
-    # DRAM traffic is not measured in this run: the 100.75 MB a grid kernel writes is still in the 126 MB L2 when
-    # the kernel ends, so the kernel's own DRAM counters miss the write-back (the ncu capture is in profiles/)
-    traffic = None
+    # DRAM traffic per launch from the ncu capture of the same kernels (dram__bytes_read.sum + dram__bytes_write.sum,
+    # profiles/grid_build_config2.md): the images are L2-resident, and part of the 100.75 MB a grid kernel writes is
+    # still in the 126 MB L2 when the kernel ends, so the counters see less than the output
+    traffic = NCU_DRAM_BYTES.get(call_names[dom])
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -1306,12 +1309,13 @@ def run_ours(args):
                                     "images": stats[calls[c][0]]["n_images"],
                                     "tflops": call_flops[c] / (mean_ms[c] * 1e-3) / 1e12}
                     for c in range(len(calls))},
-        "roofline": {"kernel": f"gridKernel<float> ({call_names[dom]})", "bound": "fp32", "achieved": achieved,
+        "roofline": {"kernel": f"gridKernelPacked ({call_names[dom]})", "bound": "fp32", "achieved": achieved,
                      "peak": peak_fp32, "unit": "TFLOP/s", "frac": achieved / peak_fp32, "traffic": traffic,
                      "peak_source": "rg_probe_fma_peak: FP32 FMA chains on all SMs, measured in this run",
                      "flops_per_pair": FLOPS_PER_PAIR,
-                     "traffic_note": "null: the kernel's output (100.75 MB per grid) is still in L2 when it ends, so "
-                                     "its DRAM counters miss the write-back"},
+                     "traffic_note": "bytes per launch from one ncu capture of the kernel (profiles/grid_build_config2.md):"
+                                     " DRAM read + write; the output (100.75 MB per grid) is partly still in L2 when the "
+                                     "kernel ends, so the counters see less than it"},
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps, "step_ms": e2e_step_ms, "path": "rg_grid_build_set with pinned host outputs"},

@@ -383,9 +383,8 @@ __device__ __forceinline__ void segmentDelta(const Params& p, const Shared& sh, 
 
 // The accepted candidate's structure-factor change added to this CTA's S(k) range (the phasor tables of the phase
 // that evaluated it are still in shared memory).
-__device__ void addCandidate(const Params& p, const Shared& sh, const Dyn& dy, int c, int nkr)
+__device__ void addCandidate(const Params& p, const Shared& sh, const Dyn& dy, int c)
 {
-  (void)nkr;
   for (int sg = threadIdx.x; sg < sh.nseg; sg += kThreads)
   {
     const int k0 = dy.segStart[sg], n = dy.segStart[sg + 1] - k0;
@@ -1158,7 +1157,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
       if (sh.accept)
       {
         if (tid == 0) storeMolecule(p, sh, sh.m, c, sh.mol);
-        if (p.use_charge) addCandidate(p, sh, dyk, 0, k1 - k0);
+        if (p.use_charge) addCandidate(p, sh, dyk, 0);
       }
     }
     else if (kind == 2 && sh.n < p.capacity)
@@ -1265,7 +1264,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
             sh.count[c] += 1;
             sh.n += 1;
           }
-          if (p.use_charge) addCandidate(p, sh, dyk, sh.selOrient, k1 - k0);
+          if (p.use_charge) addCandidate(p, sh, dyk, sh.selOrient);
         }
       }
     }
@@ -1376,7 +1375,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
           }
           sh.n -= 1;
         }
-        if (p.use_charge) addCandidate(p, sh, dyk, 0, k1 - k0);
+        if (p.use_charge) addCandidate(p, sh, dyk, 0);
       }
     }
     else if (kind == 4 && p.n_comp > 1)
@@ -1502,7 +1501,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
             gs.list[newC * p.capacity + sh.count[newC]] = m;
             sh.count[newC] += 1;
           }
-          if (p.use_charge) addCandidate(p, sh, dyk, sh.selOrient, k1 - k0);
+          if (p.use_charge) addCandidate(p, sh, dyk, sh.selOrient);
         }
         c = oldC;
       }

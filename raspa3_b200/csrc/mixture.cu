@@ -1050,14 +1050,16 @@ __global__ void __launch_bounds__(kThreads, 1) mixtureKernel(const __grid_consta
   for (int mv = 0; mv < moves; ++mv)
   {
     const long long move = move0 + mv;
+    // the move's eight uniform numbers: four Philox draws, one per lane of warp 0
+    if (tid < 4)
+    {
+      const double2 u = urand(p, move, slot(kKindMove, 0, tid));
+      sh.u[2 * tid] = u.x;
+      sh.u[2 * tid + 1] = u.y;
+    }
+    if (tid < 32) __syncwarp();
     if (tid == 0)
     {
-      for (int q = 0; q < 4; ++q)
-      {
-        const double2 u = urand(p, move, slot(kKindMove, 0, q));
-        sh.u[2 * q] = u.x;
-        sh.u[2 * q + 1] = u.y;
-      }
       sh.c = min(p.n_comp - 1, static_cast<int>(sh.u[0] * p.n_comp));
       const double ptot = p.p_translation + p.p_rotation + p.p_swap + p.p_identity;
       const double v = sh.u[1] * ptot;

@@ -414,7 +414,31 @@ __device__ __forceinline__ int siteCell(const Params& p, int4 P)
 
 // Squared distance of trial atom B and partner P (fixed point) in FP32 from the exact fixed-point displacement (the
 // uint32 wrap is the minimum image).
-__device__ __forceinline__ float pairDistance2(const Params& p, int4 B, int4 P)
+// The launch constants the pair terms read, copied into registers once per phase by the pair warps (read through the
+// Params reference they would be loaded again for every pair)
+struct PairConst
+{
+  float hf[3][3];
+  float overlap_f, rc2_c, alpha, coul;
+  bool use_charge;
+};
+__device__ __forceinline__ PairConst pairConst(const Params& p)
+{
+  PairConst c;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) c.hf[a][b] = p.hf[a][b];
+  c.overlap_f = p.overlap_f;
+  c.rc2_c = p.rc2_c;
+  c.alpha = p.alpha;
+  c.coul = p.coul;
+  c.use_charge = p.use_charge;
+  return c;
+}
+
+template <class PC>
+__device__ __forceinline__ float pairDistance2(const PC& p, int4 B, int4 P)
 {
   const float f0 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.x) - static_cast<uint32_t>(P.x))) * kFix;
   const float f1 = static_cast<float>(static_cast<int>(static_cast<uint32_t>(B.y) - static_cast<uint32_t>(P.y))) * kFix;
@@ -427,7 +451,8 @@ __device__ __forceinline__ float pairDistance2(const Params& p, int4 B, int4 P)
 
 // Lennard-Jones + real-space Ewald of trial atom B (type bt, charge qb) with partner P at squared distance rr
 // (.w & 0xff = type; charge qP), FP32, added to acc in FP64.
-__device__ __forceinline__ void pairEnergy(const Params& p, const Shared& sh, int bt, float qb, int4 P, float qP,
+template <class PC>
+__device__ __forceinline__ void pairEnergy(const PC& p, const Shared& sh, int bt, float qb, int4 P, float qP,
                                            float rr, float rc2v, double& acc, bool& ov)
 {
   const int pt = P.w & 0xff;
@@ -457,7 +482,8 @@ __device__ __forceinline__ void pairEnergy(const Params& p, const Shared& sh, in
   }
 }
 
-__device__ __forceinline__ void pairTerm(const Params& p, const Shared& sh, int4 B, int bt, float qb, int4 P, float qP,
+template <class PC>
+__device__ __forceinline__ void pairTerm(const PC& p, const Shared& sh, int4 B, int bt, float qb, int4 P, float qP,
                                          float rc2v, double& acc, bool& ov)
 {
   pairEnergy(p, sh, bt, qb, P, qP, pairDistance2(p, B, P), rc2v, acc, ov);
@@ -495,33 +521,50 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
   int b = 0;
   if (warp == kWarps - 1)
   {
-    if (lane < 16)
-      for (int b = cta; b < nta; b += G)
+    // four trial atoms at a time, two per half-warp, so that their grid loads are in flight together
+    const int half = lane >> 4, l16 = lane & 15;
+    auto corner = [&](int b, double& q) -> double {
+      const double* vdw = atomGrid[b];
+      q = static_cast<double>(sh.qt[sh.tf[b].w & 0xff]);
+      const bool charged = p.use_charge && p.ewald_grid != nullptr && q != 0.0;
+      double v = 0.0;
+      if (vdw != nullptr && (l16 < 8 || charged))
       {
-        const double* vdw = atomGrid[b];
-        const double q = static_cast<double>(sh.qt[sh.tf[b].w & 0xff]);
-        const bool charged = p.use_charge && p.ewald_grid != nullptr && q != 0.0;
-        double v = 0.0;
-        if (vdw != nullptr && (lane < 8 || charged))
-        {
-          rgd::Grid g = p.grid;
-          g.data = lane < 8 ? vdw : p.ewald_grid;
-          const double3 r = sh.ta[b];
-          if (!QUINTIC)
-            v = rgd::interpolateCorner(g, rgd::gridCell(g, r.x, r.y, r.z), lane & 7);
-          else if ((lane & 7) == 0)  // triquintic grids: lanes 0 and 8 take the whole interpolant
-            v = rgd::interpolateQuintic(g, r.x, r.y, r.z, nullptr);
-        }
-        v += __shfl_xor_sync(0x0000ffffu, v, 1);
-        v += __shfl_xor_sync(0x0000ffffu, v, 2);
-        v += __shfl_xor_sync(0x0000ffffu, v, 4);
-        const double ew = __shfl_sync(0x0000ffffu, v, 8);
-        if (lane == 0)
-        {
-          sh.fwE[b] = v + q * ew;
-          if (v > p.overlap) atomicOr(&sh.ovl_bits[b >> 5], 1u << (b & 31));
-        }
+        rgd::Grid g = p.grid;
+        g.data = l16 < 8 ? vdw : p.ewald_grid;
+        const double3 r = sh.ta[b];
+        if (!QUINTIC)
+          v = rgd::interpolateCorner(g, rgd::gridCell(g, r.x, r.y, r.z), l16 & 7);
+        else if ((l16 & 7) == 0)  // triquintic grids: lanes 0 and 8 of the half take the whole interpolant
+          v = rgd::interpolateQuintic(g, r.x, r.y, r.z, nullptr);
       }
+      return v;
+    };
+    for (int b0 = cta; b0 < nta; b0 += 4 * G)
+    {
+      const int ba = b0 + half * G, bb = b0 + (2 + half) * G;
+      double qa = 0.0, qbb = 0.0;
+      double va = ba < nta ? corner(ba, qa) : 0.0;
+      double vb = bb < nta ? corner(bb, qbb) : 0.0;
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1)
+      {
+        va += __shfl_xor_sync(0xffffffffu, va, o);
+        vb += __shfl_xor_sync(0xffffffffu, vb, o);
+      }
+      const double ewa = __shfl_sync(0xffffffffu, va, (lane & 16) | 8);
+      const double ewb = __shfl_sync(0xffffffffu, vb, (lane & 16) | 8);
+      if (l16 == 0 && ba < nta)
+      {
+        sh.fwE[ba] = va + qa * ewa;
+        if (va > p.overlap) atomicOr(&sh.ovl_bits[ba >> 5], 1u << (ba & 31));
+      }
+      if (l16 == 0 && bb < nta)
+      {
+        sh.fwE[bb] = vb + qbb * ewb;
+        if (vb > p.overlap) atomicOr(&sh.ovl_bits[bb >> 5], 1u << (bb & 31));
+      }
+    }
   }
   else
   {
@@ -603,6 +646,8 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
       const float qb = sh.qt[bt];
       const int ns_staged = min(n, p.nslice);
       const float rcut2 = p.use_charge ? fmaxf(p.rc2_mm, p.rc2_c) : p.rc2_mm;
+      const float rc2mm = p.rc2_mm;
+      const PairConst pc = pairConst(p);
       double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
       if (useCells)
       {
@@ -618,10 +663,29 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
             const int c = wrapCell(cx + k % 3 - 1, p.nc[0]) +
                           p.nc[0] * (wrapCell(cy + (k / 3) % 3 - 1, p.nc[1]) + p.nc[1] * wrapCell(cz + k / 9 - 1, p.nc[2]));
             const int e = dy.cellStart[c + 1];
-            for (int j = dy.cellStart[c] + st / cstep; j < e; j += nsub)
+            int j = dy.cellStart[c] + st / cstep;
+            // four sites of the cell per iteration: their distances without branches, then the energies of the few
+            // within a cutoff, into four independent sums
+            for (; j + 3 * nsub < e; j += 4 * nsub)
+            {
+              const int4 P0 = dy.slice[dy.order[j]], P1 = dy.slice[dy.order[j + nsub]],
+                         P2 = dy.slice[dy.order[j + 2 * nsub]], P3 = dy.slice[dy.order[j + 3 * nsub]];
+              const float r0 = (P0.w >> 8) == skip ? INFINITY : pairDistance2(pc, B, P0);
+              const float r1 = (P1.w >> 8) == skip ? INFINITY : pairDistance2(pc, B, P1);
+              const float r2 = (P2.w >> 8) == skip ? INFINITY : pairDistance2(pc, B, P2);
+              const float r3 = (P3.w >> 8) == skip ? INFINITY : pairDistance2(pc, B, P3);
+              if (fminf(fminf(r0, r1), fminf(r2, r3)) < rcut2)
+              {
+                if (r0 < rcut2) pairEnergy(pc, sh, bt, qb, P0, sh.qt[P0.w & 0xff], r0, rc2mm, a0, ov);
+                if (r1 < rcut2) pairEnergy(pc, sh, bt, qb, P1, sh.qt[P1.w & 0xff], r1, rc2mm, a1, ov);
+                if (r2 < rcut2) pairEnergy(pc, sh, bt, qb, P2, sh.qt[P2.w & 0xff], r2, rc2mm, a2, ov);
+                if (r3 < rcut2) pairEnergy(pc, sh, bt, qb, P3, sh.qt[P3.w & 0xff], r3, rc2mm, a3, ov);
+              }
+            }
+            for (; j < e; j += nsub)
             {
               const int4 P = dy.slice[dy.order[j]];
-              if ((P.w >> 8) != skip) pairTerm(p, sh, B, bt, qb, P, sh.qt[P.w & 0xff], p.rc2_mm, a0, ov);
+              if ((P.w >> 8) != skip) pairTerm(pc, sh, B, bt, qb, P, sh.qt[P.w & 0xff], rc2mm, a0, ov);
             }
           }
         }
@@ -635,23 +699,23 @@ __device__ bool phase(const Params& p, Shared& sh, int skip, const double* const
         {
           const int4 P0 = dy.slice[i], P1 = dy.slice[i + streams], P2 = dy.slice[i + 2 * streams],
                      P3 = dy.slice[i + 3 * streams];
-          const float r0 = (P0.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P0);
-          const float r1 = (P1.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P1);
-          const float r2 = (P2.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P2);
-          const float r3 = (P3.w >> 8) == skip ? INFINITY : pairDistance2(p, B, P3);
+          const float r0 = (P0.w >> 8) == skip ? INFINITY : pairDistance2(pc, B, P0);
+          const float r1 = (P1.w >> 8) == skip ? INFINITY : pairDistance2(pc, B, P1);
+          const float r2 = (P2.w >> 8) == skip ? INFINITY : pairDistance2(pc, B, P2);
+          const float r3 = (P3.w >> 8) == skip ? INFINITY : pairDistance2(pc, B, P3);
           if (fminf(fminf(r0, r1), fminf(r2, r3)) < rcut2)
           {
-            if (r0 < rcut2) pairEnergy(p, sh, bt, qb, P0, sh.qt[P0.w & 0xff], r0, p.rc2_mm, a0, ov);
-            if (r1 < rcut2) pairEnergy(p, sh, bt, qb, P1, sh.qt[P1.w & 0xff], r1, p.rc2_mm, a1, ov);
-            if (r2 < rcut2) pairEnergy(p, sh, bt, qb, P2, sh.qt[P2.w & 0xff], r2, p.rc2_mm, a2, ov);
-            if (r3 < rcut2) pairEnergy(p, sh, bt, qb, P3, sh.qt[P3.w & 0xff], r3, p.rc2_mm, a3, ov);
+            if (r0 < rcut2) pairEnergy(pc, sh, bt, qb, P0, sh.qt[P0.w & 0xff], r0, rc2mm, a0, ov);
+            if (r1 < rcut2) pairEnergy(pc, sh, bt, qb, P1, sh.qt[P1.w & 0xff], r1, rc2mm, a1, ov);
+            if (r2 < rcut2) pairEnergy(pc, sh, bt, qb, P2, sh.qt[P2.w & 0xff], r2, rc2mm, a2, ov);
+            if (r3 < rcut2) pairEnergy(pc, sh, bt, qb, P3, sh.qt[P3.w & 0xff], r3, rc2mm, a3, ov);
           }
         }
         // the rest: remaining staged sites, then any beyond the staged slice from L2
         for (; i < n; i += streams)
         {
           const int4 P = i < p.nslice ? dy.slice[i] : __ldcg(gs.fx + s0 + i);
-          if ((P.w >> 8) != skip) pairTerm(p, sh, B, bt, qb, P, sh.qt[P.w & 0xff], p.rc2_mm, a0, ov);
+          if ((P.w >> 8) != skip) pairTerm(pc, sh, B, bt, qb, P, sh.qt[P.w & 0xff], rc2mm, a0, ov);
         }
       }
       acc = (a0 + a1) + (a2 + a3);

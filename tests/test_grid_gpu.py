@@ -10,7 +10,7 @@ from reference_systems import itq29, zeolite_forcefield
 
 pytestmark = pytest.mark.gpu
 
-E_LIMIT = 1e4 * KELVIN_TO_ENERGY  # north-star tolerance applies where |E| < 1e4 K
+E_LIMIT = 1e4 * KELVIN_TO_ENERGY  # the 1e-5 relative tolerance applies where |E| < 1e4 K
 # Absolute floor of the energy channel's relative error, in K: 1e-5 relative to max(|E|, 1000 K), i.e. at most 0.01 K
 # where the framework's terms (single terms up to ~5e5 K) cancel to |E| below 1000 K.
 ENERGY_FLOOR_K = 1000.0

@@ -1,5 +1,5 @@
 #!/usr/bin/env python
-"""Benchmark of the interpolation-grid build (path a) on the configuration-2 workload.
+"""Benchmark of the interpolation-grid build (path a) on the charged synthetic framework (three 133 x 133 x 89 grids).
 
 Workload (one "step"): the three tricubic grids of the charged synthetic framework — C_co2 Lennard-Jones, O_co2
 Lennard-Jones and the unit-charge real-space Ewald grid — 133 x 133 x 89 = 1,574,321 points each (0.15 Angstrom
@@ -39,7 +39,7 @@ METRIC = "grid pts/s"
 UNIT = "grid points/s"
 # FLOPs per in-cutoff pair of the restated formulas (add/mul = 1, FMA = 2, reciprocal/sqrt/erfc/exp = 1 each).
 FLOPS_PER_PAIR = {"lj": 55, "ewald": 65}
-# DRAM bytes (read + write) per launch of the grid kernels in their ncu capture (profiles/grid_build_config2.md)
+# DRAM bytes (read + write) per launch of the grid kernels in their ncu capture (profiles/grid_build_charged_framework.md)
 NCU_DRAM_BYTES = {"LJ C_co2+O_co2 (two-probe kernel)": 0.29e6 + 143e6, "Ewald-real": 0.17e6 + 44e6}
 L2_FLUSH_BYTES = 256 << 20
 
@@ -62,11 +62,11 @@ def parse():
 
 
 def workload():
-    from raspa3_b200.synthetic import config1_grid_dims, synthetic_forcefield, synthetic_framework
+    from raspa3_b200.synthetic import spacing_grid_dims, synthetic_forcefield, synthetic_framework
 
     ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=8)
     cell, atoms = synthetic_framework(ff, seed=42)
-    dims = config1_grid_dims(cell)
+    dims = spacing_grid_dims(cell)
     grids = [("C_co2-LJ", 0, ff.index("C_co2")), ("O_co2-LJ", 0, ff.index("O_co2")), ("Ewald-real", 1, 0)]
     return ff, cell, atoms, dims, grids
 
@@ -159,16 +159,16 @@ def cpu_oracle_rate(ff, cell, atoms, dims, grids, target_seconds, threads=0, see
     return pts1 / t1, pts1, t1, threads
 
 
-def run_config1(args, ctx, world, rank, dist, torch):
-    """Configuration 1 (plain method, small, FP64): the methane Lennard-Jones tricubic grid of the uncharged synthetic
+def run_methane_grid_fp64(args, ctx, world, rank, dist, torch):
+    """The plain small FP64 case: the methane Lennard-Jones tricubic grid of the uncharged synthetic
     framework, 133 x 133 x 89 points, FP64 pair terms and sums: grid points/s, the FP64-pipe roofline, end to end
     through rg_grid_build with a pinned host output, and the FP64 oracle on the host cores."""
     from raspa3_b200 import native
-    from raspa3_b200.synthetic import config1_grid_dims, synthetic_forcefield, synthetic_framework
+    from raspa3_b200.synthetic import spacing_grid_dims, synthetic_forcefield, synthetic_framework
 
     ff = synthetic_forcefield(charges=False)
     cell, atoms = synthetic_framework(ff, seed=42)
-    dims = config1_grid_dims(cell)
+    dims = spacing_grid_dims(cell)
     npts = dims[0] * dims[1] * dims[2]
     probe = ff.index("CH4")
     stream = torch.cuda.current_stream()
@@ -209,7 +209,7 @@ def run_config1(args, ctx, world, rank, dist, torch):
     for _ in range(e2e_steps):
         ctx.grid_build(0, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP64, out_host=host)
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, dist)
-    res = {"workload": "config1: CH4 Lennard-Jones tricubic grid of the uncharged synthetic framework (96 T + 192 O, "
+    res = {"workload": "CH4 Lennard-Jones tricubic grid of the uncharged synthetic framework (96 T + 192 O, "
                        "20.0 x 19.9 x 13.4 A), 133 x 133 x 89 points, rc 12 A, FP64",
            "value": value, "unit": UNIT, "ms_per_step": 1e3 * total_s / steps, "steps": steps, "dtype": "f64",
            "pairs": st["pair_count"], "images": st["n_images"],
@@ -244,7 +244,7 @@ def gcmc_setup(ff, cell, atoms):
 
 
 def run_gcmc(args, ctx, ff, cell, atoms, dims, grids, outs, world, rank, dist, torch):
-    """Device-resident GCMC of CO2 at 300 K and 1e5 Pa (configuration 2): move attempts per second over all chains."""
+    """Device-resident GCMC of CO2 at 300 K and 1e5 Pa in the charged 2x2x3 box: move attempts per second over all chains."""
     from raspa3_b200 import native
     from raspa3_b200.gcmc import beta_of, co2_component, fugacity_of
 
@@ -303,15 +303,15 @@ ALKANE_FLOPS_PER_PAIR = 16
 
 
 def run_alkane(args, ctx, peak_fp32, world, rank, dist, torch):
-    """Batched CBMC of flexible alkanes (configuration 3): 64 independent systems of uneven size (cells 12-40 A,
+    """Batched CBMC of flexible alkanes: 64 independent systems of uneven size (cells 12-40 A,
     96-1536 framework atoms, 4-8 bead chains) in one graph replay of persistent cluster kernels, GCMC at 300 K and
     1e5 Pa with translation and CBMC swap moves. Metric: move attempts per second over all systems, after
     equilibration, with the launch plan chosen by the autotuner."""
     from raspa3_b200 import native
-    from raspa3_b200.alkane import alkane_forcefield, config3_systems
+    from raspa3_b200.alkane import alkane_forcefield, alkane_batch_systems
 
     ff = alkane_forcefield()
-    systems = config3_systems(ff, n_systems=ALKANE_SYSTEMS, seed=1234, max_molecules=128)
+    systems = alkane_batch_systems(ff, n_systems=ALKANE_SYSTEMS, seed=1234, max_molecules=128)
     stream = torch.cuda.current_stream()
     w_ig = {}
     for q in systems:
@@ -380,14 +380,14 @@ MIXTURE_BLOCKS_PER_SYSTEM = 4  # CTAs per system in the many-systems run: 37 sys
 
 
 def run_mixture(args, ctx, world, rank, dist, torch):
-    """The large mixture (configuration 5): 2,000 CO2 + 2,000 N2 in the 18,432-atom framework, Ewald kmax 12
+    """The large mixture: 2,000 CO2 + 2,000 N2 in the 18,432-atom framework, Ewald kmax 12
     (8,124 k-vectors), translation : rotation : CBMC swap : identity change = 1 : 1 : 1 : 1 with the learned first-bead
     proposal of each component, one system advanced by all SMs. Metric: move attempts per second."""
     from raspa3_b200 import native
     from raspa3_b200.gcmc import beta_of, fugacity_of
-    from raspa3_b200.mixture import config5, total_energy
+    from raspa3_b200.mixture import large_mixture, total_energy
 
-    d = config5(ctx, torch)
+    d = large_mixture(ctx, torch)
     ff, comps = d["ff"], d["components"]
     beta = beta_of(300.0)
     e0 = total_energy(d["system"], d["ewald"], ff, comps, d["xyz"], d["comp"])
@@ -450,7 +450,7 @@ def run_mixture(args, ctx, world, rank, dist, torch):
     out = {"metric": "mixture GCMC steps/s", "value": moves_per_s, "unit": "MC move attempts/s",
            "moves": MIXTURE_MOVES, "ms": secs * 1e3, "blocks": info["blocks"], "n_kvectors": nk,
            "workload": "2,000 CO2 + 2,000 N2 (12,000 sites) in the 4x4x4 replica (18,432 atoms) of the synthetic "
-                       "charged cell at 1.5x the configuration-1 lengths, Ewald alpha 0.265 kmax 12, 300 K, 1e5 Pa "
+                       "charged cell at 1.5x the 20.0 x 19.9 x 13.4 A lengths, Ewald alpha 0.265 kmax 12, 300 K, 1e5 Pa "
                        "each, translation : rotation : CBMC swap : identity change 1:1:1:1, 10 + 10 trials, learned "
                        "first-bead proposal per component",
            "n_molecules": r["n_molecules"][:2], "attempted": r["attempted"], "accepted": r["accepted"],
@@ -545,7 +545,7 @@ LEARNED_MOVES = 40000
 
 
 def run_learned(args, ctx, world, rank, dist, torch):
-    """Learned vs uniform first-bead proposal (configuration 4): CO2 at 300 K and 1e6 Pa in the 2x2x3 box of the
+    """Learned vs uniform first-bead proposal: CO2 at 300 K and 1e6 Pa in the 2x2x3 box of the
     synthetic framework, with the framework charges set to zero (with them the binding wells of about -1e4 K make the
     system non-ergodic for every sampler); CO2 keeps its charges, Ewald on. The MLP is trained on 2^22 grid-sampled
     Boltzmann factors of the C atom. Both arms run the same number of chains and moves; the statistical error of the
@@ -553,14 +553,14 @@ def run_learned(args, ctx, world, rank, dist, torch):
     t_train + t_learned * (se_learned / se_uniform)^2, against t_uniform."""
     from raspa3_b200 import native
     from raspa3_b200.gcmc import beta_of, co2_component, fugacity_of
-    from raspa3_b200.synthetic import config1_grid_dims, replicate, synthetic_forcefield, synthetic_framework
+    from raspa3_b200.synthetic import spacing_grid_dims, replicate, synthetic_forcefield, synthetic_framework
 
     ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=8)
     for pa in ff.pseudo_atoms[:2]:
         pa.charge = 0.0
     ucell, ufw = synthetic_framework(ff, seed=42)
     scell, sfw = replicate(ucell, ufw, (2, 2, 3))
-    dims = config1_grid_dims(ucell)
+    dims = spacing_grid_dims(ucell)
     stream = torch.cuda.current_stream()
     sysg = native.System(ctx, ff, scell, sfw)
     keep = []
@@ -676,7 +676,7 @@ def run_grid_validation(args, ctx, ff, cell, atoms, dims, outs, rank, world, nat
            "energy_relative_error": res["energy_relative_error"],
            "charge_energy_relative_error": res["charge_energy_relative_error"],
            "gradient_relative_error": res["gradient_relative_error"],
-           "workload": "C_co2 FP32C grid of configuration 2 with its charge term, 2x2x3 box, weights at 300 K"}
+           "workload": "C_co2 FP32C grid of the charged synthetic framework with its charge term, 2x2x3 box, weights at 300 K"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
 
@@ -705,7 +705,7 @@ TRIQUINTIC_FLOPS_PER_PAIR = 257
 
 
 def run_triquintic(args, ctx, ff, cell, atoms, dims, world, rank, dist, torch):
-    """Triquintic grid (27 values per point, FP64) of the C_co2 Lennard-Jones probe on the configuration-2 framework and
+    """Triquintic grid (27 values per point, FP64) of the C_co2 Lennard-Jones probe on the charged synthetic framework and
     grid (133 x 133 x 89 points, 340 MB): grid points/s with the output on the device (CUDA events; each output is
     larger than L2), end to end with a pinned host output, and the FP64 roofline of the kernel. CPU baseline: the
     oracle of the reference's triquintic branch on a sample of points, all host cores."""
@@ -755,7 +755,7 @@ def run_triquintic(args, ctx, ff, cell, atoms, dims, world, rank, dist, torch):
     tflops = st["pair_count"] * TRIQUINTIC_FLOPS_PER_PAIR / secs / 1e12
     res = {"metric": "triquintic grid pts/s through rg_grid_build_triquintic", "unit": "grid points/s",
            "value": whole_job_rate(npts, world, secs), "ms": 1e3 * secs,
-           "workload": "C_co2 Lennard-Jones triquintic grid (27 channels, FP64) of configuration 2, 133 x 133 x 89 "
+           "workload": "C_co2 Lennard-Jones triquintic grid (27 channels, FP64) of the charged synthetic framework, 133 x 133 x 89 "
                        "points, 340 MB",
            "pairs": st["pair_count"], "pairs_per_s": st["pair_count"] / secs,
            "roofline": {"bound": "fp64", "achieved": tflops, "peak": peak64, "unit": "TFLOP/s",
@@ -798,15 +798,15 @@ EWALD_BATCH_STEPS = 20
 
 def run_ewald_batch(args, ctx, world, rank, dist, torch):
     """Path (c) batched: the Fourier energy difference of one CO2 translation in each of 1,184 systems that share the
-    configuration-5 box and k-vectors (kmax 12, the full half-box, 8,124 k-vectors), one rg_ewald_batch_delta call per
+    large-mixture box and k-vectors (kmax 12, the full half-box, 8,124 k-vectors), one rg_ewald_batch_delta call per
     step: every system's S(k) read and its trial S(k) written (32 bytes per k-vector and system), the HBM roofline of
     the structure-factor update."""
     from raspa3_b200 import native
-    from raspa3_b200.mixture import CONFIG5_CELL
+    from raspa3_b200.mixture import MIXTURE_CELL
     from raspa3_b200.synthetic import random_molecules, synthetic_forcefield
 
     ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=12, sphere=False)
-    cell = np.diag([4 * CONFIG5_CELL[0], 4 * CONFIG5_CELL[1], 4 * CONFIG5_CELL[2]])
+    cell = np.diag([4 * MIXTURE_CELL[0], 4 * MIXTURE_CELL[1], 4 * MIXTURE_CELL[2]])
     ew = native.Ewald(ctx, ff, cell)
     nk = ew.n_kvectors
     n_sys = EWALD_BATCH_SYSTEMS
@@ -864,7 +864,7 @@ def run_ewald_batch(args, ctx, world, rank, dist, torch):
         hbm = None
     gbs = sk_bytes / (dev_ms * 1e-3) / 1e9
     out = {"workload": f"{n_sys} systems x one CO2 translation, {nk} k-vectors (kmax 12, the full half-box), "
-                       "config-5 box, one rg_ewald_batch_delta call per step",
+                       "large-mixture box, one rg_ewald_batch_delta call per step",
            "value": world * n_sys / (dev_ms * 1e-3), "unit": "Fourier differences/s",
            "ms_per_step": dev_ms, "steps": EWALD_BATCH_STEPS,
            "value_note": "the update kernel's device time with the moved atoms already on the device (CUDA events "
@@ -907,19 +907,19 @@ def run_ewald_batch(args, ctx, world, rank, dist, torch):
 
 
 def run_paths(args, ctx, world, rank, dist, torch):
-    """Paths (b) and (c) on their own, through their C-ABI entry points with host buffers, on the configuration-5
+    """Paths (b) and (c) on their own, through their C-ABI entry points with host buffers, on the large-mixture
     system (18,432 framework atoms, 2,000 CO2 + 2,000 N2, Ewald kmax 12: 8,124 k-vectors):
     (b) the trial sets of one CBMC insertion of CO2 (10 first-bead C positions, then 10 orientations whose two O atoms
         are the trial atoms), each trial atom against the grids and the 12,000 adsorbate sites, in FP64 and FP32C;
-    (c) the Ewald Fourier difference of a CO2 translation (3 new + 3 old atoms) at the configuration-5 box and at the
-        configuration-2 box (1,152 k-vectors), and the full recompute of the configuration-5 structure factors."""
+    (c) the Ewald Fourier difference of a CO2 translation (3 new + 3 old atoms) at the large-mixture box (8,124 k-vectors) and at the
+        charged 2x2x3 box (1,152 k-vectors), and the full recompute of the large mixture's structure factors."""
     from raspa3_b200 import native
     from raspa3_b200.forcefield import make_atoms
-    from raspa3_b200.mixture import config5, molecules_as_atoms
+    from raspa3_b200.mixture import large_mixture, molecules_as_atoms
     from raspa3_b200.synthetic import (CO2_NAMES, CO2_OFFSETS, random_molecules, random_rotation, replicate,
                                        rigid_molecule, synthetic_forcefield, synthetic_framework)
 
-    d = config5(ctx, torch)
+    d = large_mixture(ctx, torch)
     ff, comps, sysg, ew = d["ff"], d["components"], d["system"], d["ewald"]
     atoms = molecules_as_atoms(ff, comps, d["xyz"], d["comp"])
     n_mol = len(d["comp"])
@@ -936,7 +936,7 @@ def run_paths(args, ctx, world, rank, dist, torch):
         inserts.append((first, orient))
     trial_atoms = 10 + 10 * 2
     stream = torch.cuda.current_stream()
-    out = {"workload": "configuration 5: 18,432 framework atoms, 12,000 adsorbate sites, grids for every adsorbate "
+    out = {"workload": "large mixture: 18,432 framework atoms, 12,000 adsorbate sites, grids for every adsorbate "
                        "type, Ewald alpha 0.265 kmax 12 (8,124 k)"}
 
     def time_trials():
@@ -971,7 +971,7 @@ def run_paths(args, ctx, world, rank, dist, torch):
         "e2e": {"value": trials["fp32c"]["pair_tests_per_s"], "unit": "pair tests/s",
                 "h2d_bytes_per_step": trial_atoms * 64 + 20 * 64, "d2h_bytes_per_step": 20 * 104}}
 
-    # (c) Fourier differences: configuration 5 and configuration 2
+    # (c) Fourier differences: the large-mixture box and the charged 2x2x3 box
     ew.full(atoms, np.full(n_mol, 3, dtype=np.int32))
     ff2 = synthetic_forcefield(charges=True, alpha=0.265, kmax=8)
     ucell2, ufw2 = synthetic_framework(ff2, seed=42)
@@ -995,7 +995,7 @@ def run_paths(args, ctx, world, rank, dist, torch):
         return mv
 
     deltas = {}
-    for name, e_, a_, n_ in (("config5", ew, atoms, n_mol), ("config2", ew2, ads2, 30)):
+    for name, e_, a_, n_ in (("large_mixture_8124k", ew, atoms, n_mol), ("charged_box_1152k", ew2, ads2, 30)):
         mv = moves(a_, n_, PATH_DELTAS)
         for new, old in mv[:10]:
             e_.delta(new, old)
@@ -1025,7 +1025,7 @@ def run_paths(args, ctx, world, rank, dist, torch):
                         "python_wrapper_us_per_delta": 1e6 * wall / PATH_DELTAS,
                         "algorithmic_bytes_per_delta": 40 * nk,
                         "achieved_gbs": 40 * nk * PATH_DELTAS / direct / 1e9}
-    # full recompute of configuration 5 (adsorbates on top of the rigid framework structure factor)
+    # full recompute of the large mixture (adsorbates on top of the rigid framework structure factor)
     sizes = np.full(n_mol, 3, dtype=np.int32)
     for _ in range(2):
         ew.full(atoms, sizes)
@@ -1038,7 +1038,7 @@ def run_paths(args, ctx, world, rank, dist, torch):
     full_tf = terms * EWALD_FLOPS_PER_TERM / full_s / 1e12
     out["ewald"] = {
         "metric": "Ewald Fourier differences/s through rg_ewald_delta", "unit": "differences/s",
-        "value": deltas["config5"]["deltas_per_s"], "per_box": deltas,
+        "value": deltas["large_mixture_8124k"]["deltas_per_s"], "per_box": deltas,
         "full_recompute": {"atoms": len(atoms), "n_kvectors": ew.n_kvectors, "ms": 1e3 * full_s,
                            "terms_per_s": terms / full_s, "tflops": full_tf, "fp64_peak_tflops": peak64,
                            "frac_of_fp64_peak": full_tf / peak64 if peak64 else None,
@@ -1090,8 +1090,8 @@ def run_paths(args, ctx, world, rank, dist, torch):
         # the oracle's Fourier difference: (i) one core, the reference's serial k loop (a single system's move is serial
         # there); (ii) all host cores, the same loop parallelised over k by us (OpenMP over a precomputed k table)
         cpu_d, cpu_all = {}, {}
-        for name, ff_, cell_, a_, n_, fw_ in (("config5", ff, d["cell"], atoms, n_mol, d["framework"]),
-                                              ("config2", ff2, cell2, ads2, 30, fw2)):
+        for name, ff_, cell_, a_, n_, fw_ in (("large_mixture_8124k", ff, d["cell"], atoms, n_mol, d["framework"]),
+                                              ("charged_box_1152k", ff2, cell2, ads2, 30, fw2)):
             s_rig = oracle.ewald_rigid(ff_, cell_, fw_)
             _, stored = oracle.ewald_fourier_energy(ff_, cell_, a_, np.full(n_, 3, dtype=np.int32), s_rigid=s_rig)
             mv = moves(a_, n_, 1000)
@@ -1106,7 +1106,7 @@ def run_paths(args, ctx, world, rank, dist, torch):
                     count += 1
                 target[name] = count / (time.perf_counter() - t0)
         out["ewald"]["cpu_baseline"] = {
-            "value": cpu_d["config5"], "unit": "differences/s", "cores": 1, "kind": "port",
+            "value": cpu_d["large_mixture_8124k"], "unit": "differences/s", "cores": 1, "kind": "port",
             "per_box": cpu_d, "sample": "FP64 oracle of energyDifferenceEwaldFourier on one core, same moves",
             "all_cores": {"cores": threads, "per_box": cpu_all,
                           "sample": "the same k loop parallelised over k with OpenMP (restated reference loop, "
@@ -1167,7 +1167,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "config2 grid build: C_co2-LJ + O_co2-LJ + unit-charge Ewald-real tricubic grids, "
+        "config": {"workload": "grid build: C_co2-LJ + O_co2-LJ + unit-charge Ewald-real tricubic grids, "
                                "133x133x89 points each", "grid_points_per_step_full": 3 * total,
                    "parallelism": "cpu"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
@@ -1291,7 +1291,7 @@ def run_ours(args):
     dom = int(np.argmax(mean_ms))
     achieved = call_flops[dom] / (mean_ms[dom] * 1e-3) / 1e12
     # DRAM traffic per launch from the ncu capture of the same kernels (dram__bytes_read.sum + dram__bytes_write.sum,
-    # profiles/grid_build_config2.md): the images are L2-resident, and part of the 100.75 MB a grid kernel writes is
+    # profiles/grid_build_charged_framework.md): the images are L2-resident, and part of the 100.75 MB a grid kernel writes is
     # still in the 126 MB L2 when the kernel ends, so the counters see less than the output
     traffic = NCU_DRAM_BYTES.get(call_names[dom])
 
@@ -1299,7 +1299,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "config2 grid build: C_co2-LJ + O_co2-LJ + unit-charge Ewald-real tricubic grids, "
+        "config": {"workload": "grid build: C_co2-LJ + O_co2-LJ + unit-charge Ewald-real tricubic grids, "
                                "133x133x89 points each, FP32C", "grid_points_per_step": len(grids) * npts,
                    "framework_atoms": int(len(atoms)), "cutoff": 12.0, "precision": "FP32 pairs, compensated FP32 "
                    "accumulation, FP64 epilogue", "l2": "256 MiB flush between timed steps; 302 MB output per step",
@@ -1313,7 +1313,7 @@ def run_ours(args):
                      "peak": peak_fp32, "unit": "TFLOP/s", "frac": achieved / peak_fp32, "traffic": traffic,
                      "peak_source": "rg_probe_fma_peak: FP32 FMA chains on all SMs, measured in this run",
                      "flops_per_pair": FLOPS_PER_PAIR,
-                     "traffic_note": "bytes per launch from one ncu capture of the kernel (profiles/grid_build_config2.md):"
+                     "traffic_note": "bytes per launch from one ncu capture of the kernel (profiles/grid_build_charged_framework.md):"
                                      " DRAM read + write; the output (100.75 MB per grid) is partly still in L2 when the "
                                      "kernel ends, so the counters see less than it"},
         "clocks": clocks,
@@ -1322,25 +1322,25 @@ def run_ours(args):
         "gpu_launches": len(calls) * args.steps,
         "grid_validation": validation,
     }
-    # ---- configuration 1: the methane grid in FP64 (FP64-pipe roofline) ----
-    line["config1_fp64"] = run_config1(args, ctx, world, rank, dist, torch)
+    # ---- the methane grid in FP64 (FP64-pipe roofline) ----
+    line["methane_grid_fp64"] = run_methane_grid_fp64(args, ctx, world, rank, dist, torch)
     # ---- GCMC steps/s on the same workload: CO2 in the 2x2x3 simulation box, the FP32C grids just built ----
     if not args.no_gcmc:
         line["gcmc"] = run_gcmc(args, ctx, ff, cell, atoms, dims, grids, outs, world, rank, dist, torch)
-    # ---- batched CBMC of flexible chains in 64 uneven systems (configuration 3) ----
+    # ---- batched CBMC of flexible chains in 64 uneven systems ----
     if not args.no_alkane:
         line["batched_cbmc"] = run_alkane(args, ctx, peak_fp32, world, rank, dist, torch)
-    # ---- one large two-component system on the whole GPU (configuration 5) ----
+    # ---- one large two-component system on the whole GPU ----
     if not args.no_mixture:
         line["mixture"] = run_mixture(args, ctx, world, rank, dist, torch)
-    # ---- triquintic grid of configuration 2 (27 channels, FP64) ----
+    # ---- triquintic grid of the charged synthetic framework (27 channels, FP64) ----
     if not args.no_triquintic:
         line["triquintic"] = run_triquintic(args, ctx, ff, cell, atoms, dims, world, rank, dist, torch)
-    # ---- paths (b) and (c) on their own through the C-ABI (configuration 5, and configuration 2 for the Ewald) ----
+    # ---- paths (b) and (c) on their own through the C-ABI (large mixture, and the charged 2x2x3 box for the Ewald) ----
     if not args.no_paths:
         line["paths"] = run_paths(args, ctx, world, rank, dist, torch)
         line["paths"]["ewald_batch"] = run_ewald_batch(args, ctx, world, rank, dist, torch)
-    # ---- learned vs uniform first-bead proposal at equal loading error (configuration 4) ----
+    # ---- learned vs uniform first-bead proposal at equal loading error ----
     if not args.no_learned:
         del flush
         line["learned_proposal"] = run_learned(args, ctx, world, rank, dist, torch)

@@ -92,16 +92,16 @@ def alkane_forcefield(rc: float = 12.0) -> ForceField:
     return synthetic_forcefield(rc=rc, charges=False)
 
 
-CONFIG3_DENSITY = 0.025  # framework atoms per cubic Angstrom
+ALKANE_FRAMEWORK_DENSITY = 0.025  # framework atoms per cubic Angstrom
 
 
-def config3_systems(ff: ForceField, n_systems: int = 64, seed: int = 1234, temperature: float = 300.0,
+def alkane_batch_systems(ff: ForceField, n_systems: int = 64, seed: int = 1234, temperature: float = 300.0,
                     pressure: float = 1e5, cutoff: float = 12.0, max_molecules: int = 64, chain_lengths=(4, 8),
-                    trials=None, density: float = CONFIG3_DENSITY):
+                    trials=None, density: float = ALKANE_FRAMEWORK_DENSITY):
     """The batched-CBMC workload: synthetic cells with lengths uniform in [12, 40] A and 96-1536 atoms
     (batched_frameworks; the count is density x volume clipped to that range), each replicated for the minimum image of
     the cutoff, with a chain of 4-8 beads drawn per system. The density of 0.025 per cubic Angstrom leaves channels
-    for CH2/CH3 beads between randomly placed atoms (at the 0.054 of the configuration-1 cell they are closed).
+    for CH2/CH3 beads between randomly placed atoms (at the 0.054 atoms per cubic Angstrom of the 20.0 x 19.9 x 13.4 A cell they are closed).
     trials: optional (n_first, n_directions) per system for uneven trial counts (default 10 / 10)."""
     from .gcmc import beta_of, fugacity_of
 

@@ -1,7 +1,7 @@
 """The large two-component system: CO2 and N2 in a synthetic charged framework replicated 4 x 4 x 4.
 
-The framework is the configuration-1/2 generator (96 T + 192 O per cell, T +2.05 e, O -1.025 e) on a cell 1.5 times
-the configuration-1/2 lengths (30.0 x 29.85 x 20.1 A), replicated 4 x 4 x 4: 18,432 atoms, holding 2,000 rigid CO2
+The framework is the synthetic charged generator (96 T + 192 O per cell, T +2.05 e, O -1.025 e) on a cell 1.5 times
+the 20.0 x 19.9 x 13.4 A cell's lengths (30.0 x 29.85 x 20.1 A), replicated 4 x 4 x 4: 18,432 atoms, holding 2,000 rigid CO2
 and 2,000 rigid 3-site N2 (N-N 1.10 A, N 36 K / 3.31 A / -0.482 e, massless centre +0.964 e); Ewald alpha = 0.265 per
 Angstrom and kmax 12 given explicitly, so every k of the half-box is used, as the reference does for explicit Ewald
 parameters (forcefield.cpp:388-418; 8,124 k-vectors; the integer sphere belongs to the automatic setting). Framework
@@ -100,11 +100,11 @@ def total_energy(system, ewald, ff, components, xyz, comp):
     return fw + mm + e["ewald_fourier"] + e["ewald_self"] + e["ewald_exclusion"]
 
 
-CONFIG5_CELL = (30.0, 29.85, 20.1)
+MIXTURE_CELL = (30.0, 29.85, 20.1)
 
 
-def config5(ctx, torch, reps=(4, 4, 4), counts=(2000, 2000), kmax: int = 12, seed: int = 5, dims=None,
-            lengths=CONFIG5_CELL, spacing: float = 0.15):
+def large_mixture(ctx, torch, reps=(4, 4, 4), counts=(2000, 2000), kmax: int = 12, seed: int = 5, dims=None,
+            lengths=MIXTURE_CELL, spacing: float = 0.15):
     """Builds the large mixture system: returns a dict with the force field, cells, framework, grids (device buffers
     kept alive), System, Ewald, components and the starting configuration."""
     from . import native

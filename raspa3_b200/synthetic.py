@@ -9,7 +9,7 @@ Framework placement algorithm (``synthetic_framework``), orthorhombic cell:
   2. O atoms: for each T atom in order, two O atoms at ``bond`` (1.6 Angstrom) along uniform random directions,
      accepted when the minimum-image distance to every other atom placed so far is at least ``min_sep``
      (1.5 Angstrom). Every T-O bonded pair is therefore at exactly 1.6 Angstrom and every other pair at >= 1.5.
-  The unit cell holds n_T T atoms and 2 n_T O atoms (96 + 192 for configurations 1, 2, 4, 5).
+  The unit cell holds n_T T atoms and 2 n_T O atoms (96 + 192 for the 20.0 x 19.9 x 13.4 A cell and its replicas).
 """
 
 from __future__ import annotations
@@ -20,7 +20,7 @@ import numpy as np
 
 from .forcefield import ForceField, PseudoAtom, grid_points_for_spacing, make_atoms
 
-CONFIG1_CELL = (20.0, 19.9, 13.4)
+SYNTHETIC_CELL = (20.0, 19.9, 13.4)
 GRID_SPACING = 0.15
 
 
@@ -54,7 +54,7 @@ def _min_image(d, L):
     return d - L * np.rint(d / L)
 
 
-def synthetic_framework(ff: ForceField, lengths=CONFIG1_CELL, n_t: int = 96, seed: int = 42, min_sep: float = 1.5,
+def synthetic_framework(ff: ForceField, lengths=SYNTHETIC_CELL, n_t: int = 96, seed: int = 42, min_sep: float = 1.5,
                         t_sep: float = 3.0, bond: float = 1.6, max_tries: int = 200000):
     """Returns (cell rows 3x3, unit-cell atom records). Charges come from the force field's pseudo-atoms."""
     rng = np.random.default_rng(seed)
@@ -117,15 +117,15 @@ def replicate(cell, atoms, reps):
     return big, np.concatenate(out)
 
 
-def config1_grid_dims(cell=None):
+def spacing_grid_dims(cell=None):
     """133 x 133 x 89 for the 20.0 x 19.9 x 13.4 Angstrom cell at 0.15 Angstrom spacing."""
-    return grid_points_for_spacing(np.diag(CONFIG1_CELL) if cell is None else cell, GRID_SPACING)
+    return grid_points_for_spacing(np.diag(SYNTHETIC_CELL) if cell is None else cell, GRID_SPACING)
 
 
 def batched_frameworks(ff: ForceField, n_systems: int = 64, seed: int = 1234, density: float = 288 / 5333.2,
                        lmin: float = 12.0, lmax: float = 40.0, nmin: int = 96, nmax: int = 1536):
-    """Configuration 3: cells with lengths uniform in [12, 40] Angstrom and 96-1536 atoms (count set by the
-    configuration-1 density, clipped to the range, rounded to a multiple of 3 so that T:O = 1:2)."""
+    """The batched-alkane frameworks: cells with lengths uniform in [12, 40] Angstrom and 96-1536 atoms (count set by the
+    density of the 20.0 x 19.9 x 13.4 A cell, clipped to the range, rounded to a multiple of 3 so that T:O = 1:2)."""
     rng = np.random.default_rng(seed)
     systems = []
     for s in range(n_systems):

@@ -17,7 +17,7 @@ from chain_statistics import assert_agree
 import pytest
 
 from raspa3_b200 import native
-from raspa3_b200.alkane import AlkaneChain, AlkaneSystem, alkane_forcefield, config3_systems, replicate_for_cutoff
+from raspa3_b200.alkane import AlkaneChain, AlkaneSystem, alkane_forcefield, alkane_batch_systems, replicate_for_cutoff
 from raspa3_b200.forcefield import make_atoms
 from raspa3_b200.gcmc import beta_of, fugacity_of
 from raspa3_b200.synthetic import synthetic_framework
@@ -193,11 +193,11 @@ def test_loading_matches_oracle_and_no_drift(ctx, oracle, plan):
 
 
 def test_batched_uneven_systems_autotune(ctx, oracle):
-    """Eight uneven configuration-3 systems (cells, chain lengths, trial counts): the autotuner picks a plan, the
+    """Eight uneven batched-alkane systems (cells, chain lengths, trial counts): the autotuner picks a plan, the
     run completes with every system's running energy equal to an FP64 recomputation of its final state."""
     ff = alkane_forcefield()
     trials = [(10, 10), (8, 12), (16, 6), (10, 10), (4, 16), (12, 8), (10, 10), (6, 14)]
-    systems = config3_systems(ff, n_systems=8, seed=77, trials=trials)
+    systems = alkane_batch_systems(ff, n_systems=8, seed=77, trials=trials)
     for q in systems:
         q.w_ig = native.alkane_grow_vacuum(ctx, ff, q.chain, BETA, 50000, seed=3)
     a = native.Alkane(ctx, ff, systems, seed=41)

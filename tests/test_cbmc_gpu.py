@@ -79,8 +79,8 @@ def test_golden_two_co2_mfi_charged(ctx):
 
 
 @pytest.fixture(scope="module")
-def config2(ctx):
-    """Configuration-2 system: charged framework in a 2x2x3 simulation box, FP64 grids on a 0.5 A mesh, 30 CO2."""
+def charged_box(ctx):
+    """The charged synthetic framework in a 2x2x3 simulation box, FP64 grids on a 0.5 A mesh, 30 CO2."""
     ff = synthetic_forcefield(charges=True)
     ucell, ufw = synthetic_framework(ff, seed=42)
     scell, sfw = replicate(ucell, ufw, (2, 2, 3))
@@ -122,8 +122,8 @@ def check(gpu, ok, ref):
         assert abs(getattr(gpu, k) - ref[k]) <= 1e-9 * max(1.0, abs(ref[k])), (k, getattr(gpu, k), ref[k])
 
 
-def test_first_bead_trials_grid_branch(config2, oracle):
-    c = config2
+def test_first_bead_trials_grid_branch(charged_box, oracle):
+    c = charged_box
     ff = c["ff"]
     rng = np.random.default_rng(21)
     pos = rng.random((10, 3)) @ c["scell"]
@@ -137,9 +137,9 @@ def test_first_bead_trials_grid_branch(config2, oracle):
     assert n_ok >= 1
 
 
-def test_orientation_trials_with_skip(config2, oracle):
+def test_orientation_trials_with_skip(charged_box, oracle):
     """Chain-growth trial sets (three CO2 atoms around a fixed first bead, first bead skipped)."""
-    c = config2
+    c = charged_box
     ff = c["ff"]
     rng = np.random.default_rng(5)
     center = rng.random(3) @ c["scell"]
@@ -151,9 +151,9 @@ def test_orientation_trials_with_skip(config2, oracle):
         check(got[t], ok, ref)
 
 
-def test_pair_loop_branch_fractional_and_groups(config2, oracle):
+def test_pair_loop_branch_fractional_and_groups(charged_box, oracle):
     """A fractional CFCMC molecule (no grid branch): framework pair loop over 3456 atoms, lambda 0.6, group 1."""
-    c = config2
+    c = charged_box
     ff = c["ff"]
     rng = np.random.default_rng(6)
     sets = [rigid_molecule(ff, CO2_NAMES, CO2_OFFSETS, rng.random(3) @ c["scell"], random_rotation(rng), 31, lam=0.6,
@@ -168,8 +168,8 @@ def test_pair_loop_branch_fractional_and_groups(config2, oracle):
             np.testing.assert_allclose(got[t].dudlambda_charge[:], ref["dudlambda_charge"], rtol=1e-9, atol=1e-9)
 
 
-def test_skip_background_molecule(config2, oracle):
-    c = config2
+def test_skip_background_molecule(charged_box, oracle):
+    c = charged_box
     ff = c["ff"]
     old = c["ads"][6:9]  # molecule 2, retraced: its own interactions are skipped by moleculeId
     trial = old.copy()
@@ -178,11 +178,11 @@ def test_skip_background_molecule(config2, oracle):
     check(got[0], ok, ref)
 
 
-def test_fp32c_trial_energies(config2, oracle):
+def test_fp32c_trial_energies(charged_box, oracle):
     """RG_PRECISION_FP32C: Lennard-Jones pair terms in FP32 from the FP64 minimum-image displacement with
     TwoSum-compensated FP32 sums; the real-space Coulomb pairs and the grid branch in FP64. Bound: the trial's energy
     within 1e-6 of itself, and each part within 1e-6 of itself (both with a floor of 1 K where a sum crosses zero)."""
-    c = config2
+    c = charged_box
     ff = c["ff"]
     rng = np.random.default_rng(23)
     first = make_atoms(rng.random((20, 3)) @ c["scell"], ff.index("C_co2"), 0.70, molecule_ids=np.full(20, 30))
@@ -253,10 +253,10 @@ def moved_molecules(c, seed, n=8, lam=1.0, fractional=False, step=0.8):
     return out
 
 
-def test_framework_energy_difference_translation_rotation(config2, oracle):
+def test_framework_energy_difference_translation_rotation(charged_box, oracle):
     """rg_framework_molecule_energy_difference against the oracle's restatement of
     Interactions::computeFrameworkMoleculeEnergyDifference: grid branch (Ewald charge method, integer molecules)."""
-    c = config2
+    c = charged_box
     c["sys"].set_precision(native.PRECISION_FP64)
     n_ok = n_overlap = 0
     # every stored molecule, moved by a small step: most random placements in this dense framework overlap, and both
@@ -272,10 +272,10 @@ def test_framework_energy_difference_translation_rotation(config2, oracle):
     assert n_ok >= 3 and n_overlap >= 1, (n_ok, n_overlap)
 
 
-def test_framework_energy_difference_cfcmc_and_charge_method(config2, oracle):
+def test_framework_energy_difference_cfcmc_and_charge_method(charged_box, oracle):
     """A fractional molecule (CFCMC lambda move) takes the framework pair loop with dU/dlambda groups; a charge method
     other than Ewald turns the grid branch off (framework_molecule.cpp:145-146) and, with charges on, is unsupported."""
-    c = config2
+    c = charged_box
     ff = c["ff"]
     for new, old in moved_molecules(c, 42, n=4, lam=0.55, fractional=True):
         got = c["sys"].framework_energy_difference(new, old)
@@ -307,8 +307,8 @@ def test_framework_energy_difference_cfcmc_and_charge_method(config2, oracle):
         sys2.close()
 
 
-def test_framework_energy_difference_overlap_only_for_new_atoms(config2, oracle):
-    c = config2
+def test_framework_energy_difference_overlap_only_for_new_atoms(charged_box, oracle):
+    c = charged_box
     ff = c["ff"]
     fw_atom = c["sfw"][c["sfw"]["type"] == ff.index("O")][0]
     # a stored molecule that does not overlap the framework where it stands
@@ -326,10 +326,10 @@ def test_framework_energy_difference_overlap_only_for_new_atoms(config2, oracle)
     assert got.overlap == 0
 
 
-def test_intermolecular_energy_difference_and_update(config2, oracle):
+def test_intermolecular_energy_difference_and_update(charged_box, oracle):
     """rg_intermolecular_energy_difference against Interactions::computeInterMolecularEnergyDifference, then an
     accepted move written back with rg_system_update_molecules is seen by the next difference."""
-    c = config2
+    c = charged_box
     ff = c["ff"]
     moves = moved_molecules(c, 44)
     for new, old in moves:
@@ -356,10 +356,10 @@ def test_intermolecular_energy_difference_and_update(config2, oracle):
 
 # ---- blocked pockets, the external field and the dual-cutoff correction (B1) ----
 
-def test_blocked_pockets(config2, oracle):
+def test_blocked_pockets(charged_box, oracle):
     """CBMC::insideBlockedPockets: pocket centres in unit-cell fractions, minimum image in the unit cell, radius scaled
     by the atom's VDW scaling; the trial is flagged 2 (dropped)."""
-    c = config2
+    c = charged_box
     ff = c["ff"]
     pockets = np.array([[0.5, 0.5, 0.5, 4.0], [0.1, 0.9, 0.2, 3.0]])
     rng = np.random.default_rng(51)
@@ -387,10 +387,10 @@ def test_blocked_pockets(config2, oracle):
                                               (native.SURFACE_CYLINDER_Z, (9.0, 0.0, 0.0, 0.0)),
                                               (native.SURFACE_RECTANGLE_X, (8.0, 12.0, 0.0, 0.0)),
                                               (native.SURFACE_RECTANGLE_Z, (8.0, 12.0, 0.0, 0.0))])
-def test_external_field_analytic(config2, oracle, surface, geometry):
+def test_external_field_analytic(charged_box, oracle, surface, geometry):
     """CBMC::computeExternalFieldEnergy without a grid: the energy of each trial atom and the confinements that drop
     trials outside them."""
-    c = config2
+    c = charged_box
     ff = c["ff"]
     rng = np.random.default_rng(52)
     if surface == native.SURFACE_MULLER_BROWN:
@@ -418,9 +418,9 @@ def test_external_field_analytic(config2, oracle, surface, geometry):
         assert 0 < n_out < 48
 
 
-def test_external_field_grid(config2, oracle):
+def test_external_field_grid(charged_box, oracle):
     """The external field from a tricubic grid over the simulation box, scaled by each atom's VDW scaling."""
-    c = config2
+    c = charged_box
     ff = c["ff"]
     dims = (17, 17, 18)
     grid, _ = c["sys"].ctx.grid_build(0, ff, c["scell"], c["sfw"], ff.index("C_co2"), 12.0, dims,
@@ -440,10 +440,10 @@ def test_external_field_grid(config2, oracle):
         assert abs(got[t].external_field_vdw - ef) <= 1e-9 * max(1.0, abs(ef)), (got[t].external_field_vdw, ef)
 
 
-def test_dual_cutoff_correction(config2, oracle):
+def test_dual_cutoff_correction(charged_box, oracle):
     """CBMC::computeDualCutOffCorrection: the set's energy with the force field's cutoffs minus with the dual cutoff,
     pair-loop (fractional) and grid-branch sets alike."""
-    c = config2
+    c = charged_box
     ff = c["ff"]
     rng = np.random.default_rng(54)
     sets = [rigid_molecule(ff, CO2_NAMES, CO2_OFFSETS, rng.random(3) @ c["scell"], random_rotation(rng), 31, lam=0.8,

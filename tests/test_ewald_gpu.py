@@ -77,7 +77,7 @@ def test_golden_mfi_with_framework(ctx, rep, single_ion, fourier):
     ew.close()
 
 
-def config2_system(n_mol=24, seed=3, sphere=True):
+def charged_co2_box(n_mol=24, seed=3, sphere=True):
     ff = synthetic_forcefield(charges=True, alpha=0.265, kmax=8, sphere=sphere)
     cell, fw = synthetic_framework(ff, seed=42)
     ads = random_molecules(ff, cell, n_mol, seed=seed)
@@ -85,8 +85,8 @@ def config2_system(n_mol=24, seed=3, sphere=True):
 
 
 @pytest.mark.parametrize("sphere,nk", [(True, 1152), (False, 2600)])
-def test_kvector_counts_config2(ctx, oracle, sphere, nk):
-    ff, cell, fw, ads = config2_system(sphere=sphere)
+def test_kvector_counts_charged_co2_box(ctx, oracle, sphere, nk):
+    ff, cell, fw, ads = charged_co2_box(sphere=sphere)
     ew = native.Ewald(ctx, ff, cell)
     kv, temp, s = oracle.ewald_kvectors(ff, cell)
     assert ew.n_kvectors == nk == len(kv)
@@ -94,7 +94,7 @@ def test_kvector_counts_config2(ctx, oracle, sphere, nk):
 
 
 def test_full_and_delta_match_oracle(ctx, oracle):
-    ff, cell, fw, ads = config2_system()
+    ff, cell, fw, ads = charged_co2_box()
     ew = native.Ewald(ctx, ff, cell, n_groups=0)
     ew.set_framework(fw)
     s_rigid = oracle.ewald_rigid(ff, cell, fw)
@@ -123,7 +123,7 @@ def test_full_and_delta_match_oracle(ctx, oracle):
 
 
 def test_insertion_and_deletion_deltas(ctx, oracle):
-    ff, cell, fw, ads = config2_system()
+    ff, cell, fw, ads = charged_co2_box()
     ew = native.Ewald(ctx, ff, cell)
     ew.set_framework(fw)
     s_rigid = oracle.ewald_rigid(ff, cell, fw)
@@ -142,7 +142,7 @@ def test_insertion_and_deletion_deltas(ctx, oracle):
 
 def test_fractional_molecule_dudlambda_groups(ctx, oracle):
     """A CFCMC fractional molecule (lambda = 0.7, group 1): dU/dlambda group sums (ewald.cpp:166-173, 1221-1238)."""
-    ff, cell, fw, ads = config2_system(n_mol=10)
+    ff, cell, fw, ads = charged_co2_box(n_mol=10)
     rng = np.random.default_rng(2)
     frac = rigid_molecule(ff, CO2_NAMES, CO2_OFFSETS, rng.random(3) @ cell, random_rotation(rng), 500, lam=0.7,
                           group=1, fractional=True)
@@ -168,7 +168,7 @@ def test_fractional_molecule_dudlambda_groups(ctx, oracle):
 def test_running_energy_drift_over_many_moves(ctx, oracle):
     """Running sum of accepted deltas vs a full recompute after 300 moves (the reference drift tests,
     tests/raspa3-tests/mc_*_drift.cpp, require < 1e-6 per term)."""
-    ff, cell, fw, ads = config2_system(n_mol=30, seed=4)
+    ff, cell, fw, ads = charged_co2_box(n_mol=30, seed=4)
     ew = native.Ewald(ctx, ff, cell)
     ew.set_framework(fw)
     sizes = [3] * (len(ads) // 3)
@@ -196,7 +196,7 @@ def test_running_energy_drift_over_many_moves(ctx, oracle):
 @pytest.mark.parametrize("kmax,sphere", [(12, False), (9, True)])
 def test_batched_structure_factor_update(ctx, oracle, kmax, sphere):
     """rg_ewald_batch: one CO2 move in each of 40 systems that share one set of k-vectors, in one launch: the
-    configuration-5 set (kmax 12, the full half-box) with translations, and a spherical set (kmax 9, runs of kz of
+    large-mixture set (kmax 12, the full half-box, 8,124 k-vectors) with translations, and a spherical set (kmax 9, runs of kz of
     every length) with insertions, deletions and translations. Each system's Fourier energy change and trial S(k)
     equal the oracle's energyDifferenceEwaldFourier on that system's own S(k) (1e-9), and accepting flips only the
     accepted systems."""

@@ -123,7 +123,7 @@ def framework_co2(ctx, oracle):
 
 
 def test_framework_co2_drift(ctx, oracle, framework_co2):
-    """Configuration-2 system (charged framework in a 2x2x3 box, grids, framework structure factor) at 1e5 Pa:
+    """The charged synthetic system (charged framework in a 2x2x3 box, grids, framework structure factor) at 1e5 Pa:
     every chain's running energy equals the oracle's recomputation of its final configuration."""
     c = framework_co2
     comp = co2_component()

@@ -5,7 +5,7 @@ import pytest
 
 from raspa3_b200 import native
 from raspa3_b200.forcefield import KELVIN_TO_ENERGY, make_atoms
-from raspa3_b200.synthetic import (config1_grid_dims, synthetic_forcefield, synthetic_framework)
+from raspa3_b200.synthetic import (spacing_grid_dims, synthetic_forcefield, synthetic_framework)
 from reference_systems import itq29, zeolite_forcefield
 
 pytestmark = pytest.mark.gpu
@@ -56,10 +56,10 @@ def grid_errors(gpu, ref, beta_scale=1.0, energy_floor_k=ENERGY_FLOOR_K):
     return rel, boltz, int(mask.sum())
 
 
-def test_config1_lj_fp64_full_grid_vs_oracle_sample(ctx, oracle):
+def test_methane_lj_fp64_full_grid_vs_oracle_sample(ctx, oracle):
     ff = synthetic_forcefield(charges=False)
     cell, atoms = synthetic_framework(ff)
-    dims = config1_grid_dims(cell)
+    dims = spacing_grid_dims(cell)
     assert dims == (133, 133, 89)
     probe = ff.index("CH4")
     out, stats = ctx.grid_build(native.GRID_LENNARD_JONES, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP64,
@@ -75,7 +75,7 @@ def test_config1_lj_fp64_full_grid_vs_oracle_sample(ctx, oracle):
     assert stats["pair_count"] > 0 and stats["n_images"] > 0
 
 
-def test_config1_pair_count_small_grid(ctx, oracle):
+def test_methane_pair_count_small_grid(ctx, oracle):
     ff = synthetic_forcefield(charges=False)
     cell, atoms = synthetic_framework(ff)
     dims = (21, 20, 14)
@@ -92,10 +92,10 @@ FP32C_TOL = {0: (1e-5, 1e-5), 1: (1e-5, 1e-5)}
 
 
 @pytest.mark.parametrize("grid_type,probe_name", [(0, "C_co2"), (0, "O_co2"), (1, None)])
-def test_config2_fp32c_vs_oracle_sample(ctx, oracle, grid_type, probe_name):
+def test_charged_fp32c_vs_oracle_sample(ctx, oracle, grid_type, probe_name):
     ff = synthetic_forcefield(charges=True)
     cell, atoms = synthetic_framework(ff)
-    dims = config1_grid_dims(cell)
+    dims = spacing_grid_dims(cell)
     probe = 0 if probe_name is None else ff.index(probe_name)
     out, _ = ctx.grid_build(grid_type, ff, cell, atoms, probe, 12.0, dims, native.PRECISION_FP32C)
     pts = sample_points(dims, 3000, seed=11)
@@ -188,7 +188,7 @@ def _close(d, o, scale, rel=1e-9):
 def test_grid_validation_matches_oracle(ctx, oracle):
     """rg_grid_validate (the reference's grid test, system_interpolation_grids.cpp:240-651) on the device against the
     oracle at the same 2,000 points: every Boltzmann-weighted sum of the C_co2 VDW grid and of its charge term (0.70 e
-    x the unit-charge Ewald grid), FP64 grids of the configuration-2 framework on a 0.5 A mesh in the 2x2x3 box.
+    x the unit-charge Ewald grid), FP64 grids of the charged synthetic framework on a 0.5 A mesh in the 2x2x3 box.
     Tolerance 1e-9 of each sum's scale (for a sum of w x, sqrt(sum w x^2 sum w))."""
     torch = pytest.importorskip("torch")
     from raspa3_b200.synthetic import replicate

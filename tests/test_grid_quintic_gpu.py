@@ -212,7 +212,7 @@ def _close(a, b, scale):
 def test_triquintic_grid_test_matches_oracle(ctx, oracle, torch):
     """rg_grid_validate_triquintic (the reference's grid test with the triquintic scheme, Hessians included) against
     the oracle at the same 600 points: every Boltzmann-weighted sum of the C_co2 VDW grid and of its charge term
-    (0.70 e x the unit-charge Ewald grid), configuration-2 framework on a 0.5 A mesh, 2x2x3 box. Tolerance 1e-9 of each
+    (0.70 e x the unit-charge Ewald grid), charged synthetic framework on a 0.5 A mesh, 2x2x3 box. Tolerance 1e-9 of each
     sum's scale (for a sum of w x, sqrt(sum w x^2 sum w))."""
     ff = synthetic_forcefield(charges=True)
     ucell, ufw = synthetic_framework(ff, seed=42)

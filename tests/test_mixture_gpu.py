@@ -20,7 +20,7 @@ import pytest
 from raspa3_b200 import native
 from raspa3_b200.forcefield import make_atoms
 from raspa3_b200.gcmc import beta_of, co2_component, fugacity_of, n2_component
-from raspa3_b200.mixture import config5, random_mixture, total_energy
+from raspa3_b200.mixture import large_mixture, random_mixture, total_energy
 from raspa3_b200.synthetic import replicate, synthetic_forcefield, synthetic_framework
 
 pytestmark = pytest.mark.gpu
@@ -164,7 +164,7 @@ def test_split_molecules_are_kept_whole(ctx, torch):
 
 
 def test_large_mixture_runs_without_drift(ctx, torch):
-    d = config5(ctx, torch)
+    d = large_mixture(ctx, torch)
     ff, comps = d["ff"], d["components"]
     e0 = total_energy(d["system"], d["ewald"], ff, comps, d["xyz"], d["comp"])
     sk0 = d["ewald"].structure_factors(0)
@@ -185,11 +185,11 @@ def test_large_mixture_runs_without_drift(ctx, torch):
 
 @pytest.mark.parametrize("blocks,n_systems", [(4, 3), (2, 2)])
 def test_large_mixtures_on_few_ctas_each(ctx, torch, blocks, n_systems):
-    """Configuration 5 with 2 or 4 CTAs per system (2,031 or 4,062 k-vectors per CTA: several tiles of the candidates'
+    """The large mixture (12,000 sites, 8,124 k-vectors) with 2 or 4 CTAs per system (2,031 or 4,062 k-vectors per CTA: several tiles of the candidates'
     energy sums; at 2 CTAs most of the 6,000 sites per CTA come from L2 beyond the staged slice), several systems per
     launch: each system equals the same system run on its own, its running energy equals an FP64 recomputation of its
     final configuration, and its structure factors equal a recomputation."""
-    d = config5(ctx, torch)
+    d = large_mixture(ctx, torch)
     ff, comps = d["ff"], d["components"]
     e0 = total_energy(d["system"], d["ewald"], ff, comps, d["xyz"], d["comp"])
     sk0 = d["ewald"].structure_factors(0)

@@ -25,7 +25,7 @@ def ctx():
 
 
 def triquintic_system(ctx, types, charges=True, kmax=8, dims=(33, 33, 23)):
-    """The configuration-2 framework in its 2x2x3 box with triquintic grids of the given pseudo-atom names and the
+    """The charged synthetic framework in its 2x2x3 box with triquintic grids of the given pseudo-atom names and the
     unit-charge Ewald grid."""
     ff = synthetic_forcefield(charges=charges, alpha=0.265, kmax=kmax)
     ucell, ufw = synthetic_framework(ff, seed=42)

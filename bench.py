@@ -39,7 +39,7 @@ METRIC = "grid pts/s"
 UNIT = "grid points/s"
 # FLOPs per in-cutoff pair of the restated formulas (add/mul = 1, FMA = 2, reciprocal/sqrt/erfc/exp = 1 each).
 FLOPS_PER_PAIR = {"lj": 55, "ewald": 65}
-# DRAM bytes (read + write) per launch of the grid kernels in their ncu capture (profiles/grid_build_charged_framework.md)
+# DRAM bytes (read + write) per launch of the grid kernels in their ncu capture (the grid-build summary in profiles/)
 NCU_DRAM_BYTES = {"LJ C_co2+O_co2 (two-probe kernel)": 0.29e6 + 143e6, "Ewald-real": 0.17e6 + 44e6}
 L2_FLUSH_BYTES = 256 << 20
 
@@ -1291,7 +1291,7 @@ def run_ours(args):
     dom = int(np.argmax(mean_ms))
     achieved = call_flops[dom] / (mean_ms[dom] * 1e-3) / 1e12
     # DRAM traffic per launch from the ncu capture of the same kernels (dram__bytes_read.sum + dram__bytes_write.sum,
-    # profiles/grid_build_charged_framework.md): the images are L2-resident, and part of the 100.75 MB a grid kernel writes is
+    # the grid-build summary in profiles/): the images are L2-resident, and part of the 100.75 MB a grid kernel writes is
     # still in the 126 MB L2 when the kernel ends, so the counters see less than the output
     traffic = NCU_DRAM_BYTES.get(call_names[dom])
 
@@ -1313,7 +1313,7 @@ def run_ours(args):
                      "peak": peak_fp32, "unit": "TFLOP/s", "frac": achieved / peak_fp32, "traffic": traffic,
                      "peak_source": "rg_probe_fma_peak: FP32 FMA chains on all SMs, measured in this run",
                      "flops_per_pair": FLOPS_PER_PAIR,
-                     "traffic_note": "bytes per launch from one ncu capture of the kernel (profiles/grid_build_charged_framework.md):"
+                     "traffic_note": "bytes per launch from one ncu capture of the kernel (the grid-build summary in profiles/):"
                                      " DRAM read + write; the output (100.75 MB per grid) is partly still in L2 when the "
                                      "kernel ends, so the counters see less than it"},
         "clocks": clocks,
